@@ -1,0 +1,334 @@
+"""Benchmark of the EMSES particle hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 128^3 periodic cells, electrons + ions x 64 particles per cell
+(268,435,456 particles), mass ratio 1836, ion drift 0.01 x, B0 = (0,0,0.1)
+plus 8 seeded dB modes and 8 seeded E modes of amplitude 1e-3, dt = 0.5,
+cell sort every 4 steps (seeded synthetic inputs in the reference's internal
+units, ctca_b200/inputs.py).  One step = field relocation (grdcrt), push,
+zigzag current and CIC charge into int64 fixed point, guard folding, FP64
+rho / J outputs, plus the sort + compaction on every 4th step.
+
+`value` is particle-steps per second of the FP32 / fixed-point form with the
+state resident in HBM (7.5 GB of particles, well above the 126 MB L2, so no
+L2 flush is needed).  `e2e` is the same metric through the C ABI with host
+buffers: every step uploads eb from pinned host memory and downloads rho and
+J.  `fp64_dropin` reports the plain FP64 drop-in (64-byte records) on the
+same workload.  With --gpus N every rank runs its own replica (the path has
+no data exchange on one rank: weak scaling, replicas only).
+
+--impl reference times the reference's CPU path (the oracle restatement of
+psolve1 + charge; the Fortran reference cannot be built here) on the host
+cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "push+deposit particles/s & % HBM roofline: FP32-fixedpt vs FP64 plain; adj/fwd"
+UNIT = "particle-steps/s"
+SORT_EVERY = 4
+# Algorithmic bytes of one particle-step (FP32 form, S = 4, 128 particles
+# per cell): 2*28 (push read+write) + (2*28+8)/4 (sort) + (24+32)/128 (grid).
+B_ALG_STEP = 2 * 28 + (2 * 28 + 8) / SORT_EVERY + (24 + 32) / 128
+B_ALG_PUSH = 2 * 28  # the fused push + deposit kernel, per particle
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (read only)."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.reader.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[1]))
+                mx = float(s[2])
+                for n, v in zip(names, s[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------- CPU baseline
+def cpu_sample(seconds: float, threads: int):
+    """The oracle's psolve1 + charge on the 128^3 grid with 1 particle per
+    cell per species (4.19 M particles): a bounded sample of the workload."""
+    from ctca_b200 import inputs
+    from oracle import oracle as O
+    case = inputs.baseline_case(2)
+    for s in case.species:
+        s.ppc = 1
+    cfg = inputs.make_config(case)
+    eb = inputs.make_fields(case)
+    pl = inputs.plasma(case)
+    pbuf, tp = O.load_plasma(cfg, pl)
+    o = O.Oracle(cfg, pbuf[:0], [0, 0], eb)
+    o.grdcrt()
+    wrk = o.f["wrk"]
+    n = int(tp.sum())
+    t_total, steps = 0.0, 0
+    while t_total < seconds or steps < 1:
+        dt, _, _ = O.step_timed(cfg, 2, wrk, pbuf, tp, threads)
+        t_total += dt
+        steps += 1
+    return n * steps / t_total, f"128^3 grid, 2 species x 1 ppc ({n} particles), psolve1+charge, {steps} steps", steps
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    secs = max(1.0, 3.0 * args.steps / max(args.steps, 1))
+    for _ in range(max(args.warmup, 0) and 1):
+        cpu_sample(0.1, threads)
+    value, sample, steps = cpu_sample(min(60.0, 2.0 * args.steps), threads)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 268435456 / value * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "128^3 periodic, 2 species x 64 ppc (268M particles), sort every 4",
+                   "sample": sample, "note": "oracle restatement of psolve1+charge (Fortran reference not "
+                                             "buildable: no Fortran/MPI/HDF5/FFTW toolchain)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- GPU arm
+def run_ours(args, world, rank, local):
+    import torch
+    from ctca_b200 import inputs
+    from ctca_b200.emses import Emses, select_device
+
+    torch.cuda.set_device(local)
+    select_device(local)
+    case = inputs.baseline_case(2)
+    cfg = inputs.make_config(case)
+    eb = inputs.make_fields(case)
+    npart = sum(cfg.capacity[i] for i in range(cfg.nspec))
+    g = Emses(cfg)
+    g.load_plasma(inputs.plasma(case, seed=case.seed + 1000 * rank))
+    g.upload_field("eb", eb)
+    stream = torch.cuda.ExternalStream(g.stream)
+
+    def timed(fn, steps):
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s in range(steps):
+            fn(s)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier(world)
+        return max_over_ranks(world, e0.elapsed_time(e1) / 1e3)
+
+    # ---- plain FP64 drop-in (64-byte records): grdcrt, psolve1, folds, charge, sort every 4
+    def fp64_step(s):
+        g.grdcrt(1)
+        g.zero_field("aj")
+        g.psolve1(1, 2, 0)
+        g.reduce_aj()
+        if s % SORT_EVERY == SORT_EVERY - 1:
+            g.spsort(1)
+        g.charge(1, 0)
+        g.reduce_rho("rho")
+
+    k64 = max(1, min(args.steps, args.fp64_steps))
+    for s in range(args.warmup):
+        fp64_step(s)
+    t64 = timed(fp64_step, k64)
+
+    # ---- FP32 / fixed-point form
+    g.fx_load()
+    step_i = [0]
+
+    def fx_step(s):
+        g.fx_step(2, (step_i[0] % SORT_EVERY) == SORT_EVERY - 1)
+        step_i[0] += 1
+
+    for s in range(args.warmup):
+        fx_step(s)
+    g.set_profiling(True)
+    g.profile_reset()
+    with Clocks(local) as clk:
+        t = timed(fx_step, args.steps)
+    prof = g.profile()
+    g.set_profiling(False)
+
+    # ---- end to end through the C ABI with host buffers
+    eb_host = torch.empty(eb.size, dtype=torch.float64, pin_memory=True)
+    eb_host.numpy()[:] = eb.reshape(-1)
+    nr = g.field_size("rho")
+    na = g.field_size("aj")
+    rho_host = torch.empty(nr, dtype=torch.float64, pin_memory=True)
+    aj_host = torch.empty(na, dtype=torch.float64, pin_memory=True)
+    lib = g.lib
+
+    def e2e_step(s):
+        lib.emsesg_upload_field(g.h, 0, eb_host.data_ptr())
+        fx_step(s)
+        lib.emsesg_download_field(g.h, 4, rho_host.data_ptr())
+        lib.emsesg_download_field(g.h, 2, aj_host.data_ptr())
+
+    ke2e = max(1, min(args.steps, args.e2e_steps))
+    te2e = timed(e2e_step, ke2e)
+    g.synchronize()
+
+    value = world * npart * args.steps / t
+    hbm, peak_kind = peaks()
+    ms, launches = prof.get("fx_push", (0.0, 0))
+    avg_launch_s = ms / 1e3 / max(launches, 1)
+    parts_per_launch = npart / cfg.nspec
+    achieved = B_ALG_PUSH * parts_per_launch / avg_launch_s / 1e9 if launches else None
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        tb = json.loads(tfile.read_text()).get("fx_push_bytes_per_particle")
+        if tb:
+            traffic = tb * parts_per_launch
+    step_time = t / args.steps
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_time * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+i64", "data": "synthetic",
+        "config": {"workload": "128^3 periodic, 2 species x 64 ppc (268,435,456 particles), mass ratio 1836, "
+                               "sort every 4; FP32 cell+offset particles, int64 rho/J at 2^40",
+                   "l2": "inputs larger than L2 (7.5 GB particle state)", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                     "kernel": "fx_push", "peak_kind": peak_kind,
+                     "bytes_per_particle_alg": B_ALG_PUSH,
+                     "step_frac": B_ALG_STEP * npart / step_time / 1e9 / hbm},
+        "e2e": {"value": world * npart * ke2e / te2e, "unit": UNIT,
+                "h2d_bytes_per_step": int(eb.size * 8), "d2h_bytes_per_step": int((nr + na) * 8)},
+        "fp64_dropin": {"value": world * npart * k64 / t64, "unit": UNIT, "steps": k64,
+                        "ms_per_step": t64 / k64 * 1e3,
+                        "fp32_over_fp64": (value / (world * npart * k64 / t64))},
+        "gpu_launches": int(sum(n for _, n in prof.values())),
+        "kernels_ms": {k: round(v[0], 3) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, sample, _ = cpu_sample(args.cpu_seconds, os.cpu_count() or 1)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": sample}
+    g.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--fp64-steps", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+// common.cuh -- shared internals of libemsesg (the B200 EMSES particle path).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/emses_gpu.h"
+
+namespace emsesg {
+
+// Fortran-layout field descriptor (nc, lo:n+hi per axis), component fastest.
+struct FieldDesc {
+  int nc, lo, ex, ey, ez;
+  __host__ __device__ int64_t at(int c, int i, int j, int k) const {
+    return c + (int64_t)nc * ((i - lo) + (int64_t)ex * ((j - lo) + (int64_t)ey * (k - lo)));
+  }
+  __host__ __device__ int64_t size() const { return (int64_t)nc * ex * ey * ez; }
+};
+
+// Guard extents from OhHelp's fsizes rule (ohhelp3.c:439-477) applied to
+// ftypes/ctypes of src/wrapper/ohinit.F90:98-122.
+FieldDesc field_desc(const emsesg_config& c, int field);
+
+// Per-species device segment: particles [base, base + count) of a region of
+// `capacity` slots.  The device keeps one region per species (the host
+// buffer packs them back to back, as pbuf/pbase/totalp do).
+struct Segments {
+  int64_t base[EMSESG_ISPEC];
+  int64_t capacity[EMSESG_ISPEC];
+};
+
+// Kernel launch timing (CUDA events on the context stream).
+struct KernelTimer {
+  bool on = false;
+  struct Entry { double ms = 0; int64_t launches = 0; };
+  std::map<std::string, Entry> total;
+  struct Pending { std::string name; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> pool;
+};
+
+struct SortScratch {
+  // Radix sort buffers sized for the largest species region.
+  uint32_t* keys[2] = {nullptr, nullptr};
+  uint32_t* vals[2] = {nullptr, nullptr};
+  uint32_t* hist = nullptr;       // digit-major block histograms
+  uint32_t* scan_tmp = nullptr;   // partial sums of the scans
+  int64_t cap = 0;
+  int64_t hist_cap = 0;
+  int64_t scan_tmp_cap = 0;
+};
+
+// FP32 / fixed-point particle state.
+struct FxState {
+  bool loaded = false;
+  float4* pos = nullptr;   // {ox, oy, oz, __int_as_float(cell)}
+  float* vx = nullptr;
+  float* vy = nullptr;
+  float* vz = nullptr;
+  float4* pos2 = nullptr;  // sort double buffer
+  float* vx2 = nullptr;
+  float* vy2 = nullptr;
+  float* vz2 = nullptr;
+  int64_t* count_d = nullptr;       // device particle counts per species
+  int64_t* tile_start = nullptr;    // [nspec][ntiles+1] offsets within the species region
+  int64_t* accum = nullptr;         // int64 (rho, jx, jy, jz) on the rho layout
+  float4* fnode = nullptr;          // node field {ex, ey, ez, bx} over (n+1)^3 nodes
+  float4* fnode2 = nullptr;         // {by, bz, 0, 0}
+  int bits[3] = {0, 0, 0};          // packed cell bit widths
+  int tile[3] = {8, 8, 8};
+  int ntile[3] = {0, 0, 0};
+  int64_t ntiles = 0;
+};
+
+}  // namespace emsesg
+
+struct emsesg_ctx {
+  emsesg_config cfg;
+  emsesg_config* d_cfg = nullptr;      // device copy of cfg for the kernels
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  emsesg::Segments seg;
+  int64_t totalp[EMSESG_ISPEC] = {0};  // host mirror of the species counts
+  int64_t* d_count = nullptr;          // device species counts (drop-in)
+  emsesg_particle* pbuf = nullptr;     // device pbuf, one region per species
+  emsesg_particle* pbuf2 = nullptr;    // scratch for sort / compaction
+  double* field[EMSESG_NFIELDS] = {nullptr};
+  double* node64 = nullptr;            // drop-in node field: 8 doubles / node
+  double* tj = nullptr;                // per-species zigzag scratch (aj layout)
+  emsesg_counter* d_counter = nullptr;
+  double* d_randoms = nullptr;
+  int64_t n_randoms = 0;
+  int64_t* d_rand_pos = nullptr;       // next pre-drawn number (device)
+  uint64_t rng_stream = 0;             // push call counter for the hash
+  int* d_status = nullptr;             // device error word
+  int64_t* d_scratch64 = nullptr;      // small scratch (counts, sums)
+  double* d_sum = nullptr;
+  emsesg::SortScratch sort;
+  emsesg::FxState fx;
+  emsesg::KernelTimer timer;
+};
+
+namespace emsesg {
+
+int set_error(emsesg_ctx* ctx, int code, const char* fmt, ...);
+int check_cuda(emsesg_ctx* ctx, cudaError_t e, const char* what);
+// Launch bracketing for the per-kernel profile.
+void timer_begin(emsesg_ctx* ctx, const char* name);
+void timer_end(emsesg_ctx* ctx);
+void timer_collect(emsesg_ctx* ctx);
+
+// Device status word codes.
+enum { ST_OK = 0, ST_BAD_INDEX = 1, ST_RANDOMS = 2, ST_OVERFLOW = 4 };
+
+// SplitMix64 finaliser (Steele, Lea, Flood 2014).
+__host__ __device__ inline uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+// U[0,1) with 53 random bits from (seed, stream, index).
+__host__ __device__ inline double hash_u01(uint64_t seed, uint64_t stream, uint64_t index) {
+  uint64_t a = mix64(seed ^ mix64(stream + 0x632BE59BD9B4E019ULL));
+  uint64_t b = mix64(a ^ (index * 0xD1B54A32D192ED03ULL));
+  return (double)(b >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// Internal entry points shared between translation units.
+int sort_pairs(emsesg_ctx* ctx, uint32_t* keys, uint32_t* vals, int64_t n, int key_bits,
+               uint32_t** keys_out, uint32_t** vals_out);
+int exclusive_scan_u32(emsesg_ctx* ctx, uint32_t* data, int64_t n);
+int exclusive_scan_i64(emsesg_ctx* ctx, int64_t* data, int64_t n);
+int ensure_sort_scratch(emsesg_ctx* ctx, int64_t n);
+
+int fx_alloc(emsesg_ctx* ctx);
+void fx_free(emsesg_ctx* ctx);
+
+}  // namespace emsesg
+
+#define EMSESG_CUDA(ctx, call)                                               \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) return emsesg::check_cuda((ctx), e_, #call);      \
+  } while (0)
+
+#define EMSESG_LAUNCH(ctx, name, kernel, grid, block, smem, ...)             \
+  do {                                                                       \
+    emsesg::timer_begin((ctx), (name));                                      \
+    kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);         \
+    emsesg::timer_end((ctx));                                                \
+    cudaError_t e_ = cudaGetLastError();                                     \
+    if (e_ != cudaSuccess) return emsesg::check_cuda((ctx), e_, name);       \
+  } while (0)

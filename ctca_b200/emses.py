@@ -1,0 +1,366 @@
+"""Host-side mirror of the reference's particle-path subroutines over the C ABI.
+
+The methods keep the reference's names and argument meaning:
+
+    Emses.grdcrt(ps)                 subroutine grdcrt(ps)          src/field/grdcrt.F90:125
+    Emses.psolve2(ps, ustep)         subroutine psolve2(ps, ustep)  src/pcl2field/psolve2.F90:4
+    Emses.psolve1(ps, ustep, func)   subroutine psolve1(...)        src/pcl2field/psolve1.F90:4
+    Emses.charge(ps, func)           subroutine charge(ps, func)    src/pcl2field/charge.F90:4
+    Emses.spsort(ps)                 subroutine spsort(ps)          src/etc/spsort.F90:4
+
+Every call goes through libemsesg.so (CUDA kernels for sm_100a); there is no
+CPU fallback, and the module refuses to load without the built library.
+Errors from the library raise EmsesError with the library's message, as the
+reference's `icon` / `errstop` paths report them.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+ISPEC = 10
+INPC = 15
+
+OK = 0
+ERR_ARG = 1
+ERR_UNSUPPORTED = 2
+ERR_CUDA = 3
+ERR_OVERFLOW = 4
+ERR_NOMEM = 5
+ERR_TIMEOUT = 6
+ERR_DEVICE = 7
+ERR_STATE = 8
+
+PCL_ALIVE = 0
+PCL_INJECTED = 1
+PCL_TO_BE_ACCUMULATED = -1
+PCL_TO_BE_ACCUMULATED_AS_ANTIPCL = -2
+
+FIELDS = {"eb": 0, "wrk": 1, "aj": 2, "ajdg": 3, "rho": 4, "rhodg": 5, "rhobk": 6, "rhobksp": 7}
+
+# oh_particle (lib/ohhelp/ohhelp-1.1.1/oh_type.F90:15-28): 64 bytes.
+PARTICLE_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("vx", "<f8"), ("vy", "<f8"),
+                           ("vz", "<f8"), ("pid", "<i4"), ("preside", "<i4"), ("nid", "<i4"), ("spec", "<i4")])
+assert PARTICLE_DTYPE.itemsize == 64
+
+
+class Body(ctypes.Structure):
+    _fields_ = [("geotype", ctypes.c_int32), ("ncond", ctypes.c_int32), ("cyl_align", ctypes.c_int32),
+                ("reserved_", ctypes.c_int32),
+                ("xlpc", ctypes.c_double), ("xupc", ctypes.c_double), ("ylpc", ctypes.c_double),
+                ("yupc", ctypes.c_double), ("zlpc", ctypes.c_double), ("zupc", ctypes.c_double),
+                ("cyl_axis", ctypes.c_double * 2), ("cyl_edge", ctypes.c_double * 2), ("radius", ctypes.c_double),
+                ("sph_center", ctypes.c_double * 3), ("sqdscaled", ctypes.c_double)]
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("nspec", ctypes.c_int32), ("nfbnd", ctypes.c_int32 * 3),
+                ("npbnd", (ctypes.c_int32 * 3) * ISPEC), ("npc", ctypes.c_int32), ("line_mode", ctypes.c_int32),
+                ("rng_mode", ctypes.c_int32), ("sort_tile", ctypes.c_int32 * 3), ("reserved_", ctypes.c_int32),
+                ("rng_seed", ctypes.c_uint64), ("q", ctypes.c_double * ISPEC), ("qm", ctypes.c_double * ISPEC),
+                ("rm", ctypes.c_double * ISPEC), ("e0", ctypes.c_double * 3), ("b0", ctypes.c_double * 3),
+                ("body", Body * INPC), ("capacity", ctypes.c_int64 * ISPEC)]
+
+
+class Counter(ctypes.Structure):
+    """The Fortran sequence type `counter` (src/main/paramt.F90:76-83)."""
+    _fields_ = [("globalp", (ctypes.c_int64 * ISPEC) * 2), ("influx", (ctypes.c_int32 * INPC) * ISPEC),
+                ("outflux", (ctypes.c_int32 * INPC) * ISPEC),
+                ("infhist", ((ctypes.c_int32 * (INPC + 1)) * INPC) * ISPEC),
+                ("nesc", ctypes.c_int32 * ((ISPEC + 1) // 2 * 2)), ("chgacm", (ctypes.c_double * 2) * INPC)]
+
+    def as_dict(self) -> dict:
+        return {
+            "influx": np.ctypeslib.as_array(self.influx).copy(),
+            "infhist": np.ctypeslib.as_array(self.infhist).copy(),
+            "nesc": np.ctypeslib.as_array(self.nesc).copy(),
+            "chgacm": np.ctypeslib.as_array(self.chgacm).copy(),
+        }
+
+
+class Plasma(ctypes.Structure):
+    _fields_ = [("ppc", ctypes.c_int32 * ISPEC), ("vth", ctypes.c_double * ISPEC),
+                ("vdrift", (ctypes.c_double * 3) * ISPEC), ("seed", ctypes.c_uint64)]
+
+
+# Declarations of include/emses_gpu.h, in order.
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_SIGS = {
+    "emsesg_select_device": (_I, [_I]),
+    "emsesg_create": (_I, [ctypes.POINTER(Config), ctypes.POINTER(_P)]),
+    "emsesg_destroy": (_I, [_P]),
+    "emsesg_last_error": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    "emsesg_stream": (_P, [_P]),
+    "emsesg_synchronize": (_I, [_P]),
+    "emsesg_field_size": (_I, [_P, _I, ctypes.POINTER(ctypes.c_int64)]),
+    "emsesg_upload_particles": (_I, [_P, _I, _P, ctypes.POINTER(ctypes.c_int64)]),
+    "emsesg_download_particles": (_I, [_P, _I, _P, ctypes.POINTER(ctypes.c_int64)]),
+    "emsesg_upload_field": (_I, [_P, _I, _P]),
+    "emsesg_download_field": (_I, [_P, _I, _P]),
+    "emsesg_zero_field": (_I, [_P, _I]),
+    "emsesg_set_counters": (_I, [_P, ctypes.POINTER(Counter)]),
+    "emsesg_get_counters": (_I, [_P, ctypes.POINTER(Counter)]),
+    "emsesg_set_randoms": (_I, [_P, _P, ctypes.c_int64]),
+    "emsesg_grdcrt": (_I, [_P, _I]),
+    "emsesg_psolve2": (_I, [_P, _I, _I, ctypes.POINTER(Counter)]),
+    "emsesg_psolve1": (_I, [_P, _I, _I, _I, ctypes.POINTER(Counter)]),
+    "emsesg_charge": (_I, [_P, _I, _I]),
+    "emsesg_reduce_rho": (_I, [_P, _I]),
+    "emsesg_reduce_aj": (_I, [_P]),
+    "emsesg_reduce_ajdg": (_I, [_P]),
+    "emsesg_spsort": (_I, [_P, _I]),
+    "emsesg_compact": (_I, [_P, _I, ctypes.POINTER(ctypes.c_int64)]),
+    "emsesg_rhoupd": (_I, [_P, _I]),
+    "emsesg_energy": (_I, [_P, ctypes.POINTER(ctypes.c_double)]),
+    "emsesg_fx_load": (_I, [_P]),
+    "emsesg_fx_store": (_I, [_P]),
+    "emsesg_fx_step": (_I, [_P, _I, _I]),
+    "emsesg_fx_sort": (_I, [_P]),
+    "emsesg_fx_counts": (_I, [_P, ctypes.POINTER(ctypes.c_int64)]),
+    "emsesg_fx_download_accum": (_I, [_P, _P]),
+    "emsesg_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
+    "emsesg_set_profiling": (_I, [_P, _I]),
+    "emsesg_profile_report": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    "emsesg_profile_reset": (_I, [_P]),
+}
+
+LIB_PATH = Path(__file__).resolve().parent / "libemsesg.so"
+_lib = None
+
+
+def library_path() -> Path:
+    return Path(os.environ.get("EMSESG_LIB", LIB_PATH))
+
+
+def load_library() -> ctypes.CDLL:
+    """Loads libemsesg.so; raises ImportError when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not path.exists():
+        raise ImportError(f"{path} is missing: build it with `python -m ctca_b200.build`")
+    lib = ctypes.CDLL(str(path))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def declared_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def select_device(device: int):
+    """CUDA device for the contexts this thread creates next (local rank)."""
+    rc = load_library().emsesg_select_device(int(device))
+    if rc != OK:
+        raise EmsesError(rc, f"cannot select CUDA device {device}")
+
+
+class EmsesError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def field_extents(cfg: Config, name: str) -> tuple[int, int, int, int, int]:
+    """(ncomp, lo, ext_x, ext_y, ext_z) of a field array (Fortran layout)."""
+    nx, ny, nz, ns = cfg.nx, cfg.ny, cfg.nz, cfg.nspec
+    return {
+        "eb": (6, -1, nx + 3, ny + 3, nz + 3),
+        "wrk": (9, -4, nx + 9, ny + 9, nz + 9),
+        "aj": (3, -4, nx + 9, ny + 9, nz + 9),
+        "ajdg": (3 * ns, -4, nx + 9, ny + 9, nz + 9),
+        "rho": (1, -1, nx + 3, ny + 3, nz + 3),
+        "rhodg": (2 * ns + 1, -1, nx + 3, ny + 3, nz + 3),
+        "rhobk": (1, -1, nx + 3, ny + 3, nz + 3),
+        "rhobksp": (1, -1, nx + 3, ny + 3, nz + 3),
+    }[name]
+
+
+def field_shape(cfg: Config, name: str) -> tuple[int, ...]:
+    """numpy (C-order) shape of a field: (z, y, x, comp), plus a leading
+    species axis for rhobksp.  Index [k-lo, j-lo, i-lo, c] is Fortran
+    field(c+1, i, j, k)."""
+    nc, lo, ex, ey, ez = field_extents(cfg, name)
+    shp = (ez, ey, ex, nc)
+    return (cfg.nspec,) + shp if name == "rhobksp" else shp
+
+
+class Emses:
+    """One device context (one rank, ps = 1) of the EMSES particle path."""
+
+    def __init__(self, cfg: Config):
+        self.lib = load_library()
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        rc = self.lib.emsesg_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != OK:
+            raise EmsesError(rc, "emsesg_create failed (bad configuration or no CUDA device)")
+        self.h = h
+
+    # -- plumbing
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.emsesg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != OK:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.emsesg_last_error(self.h, buf, 512)
+            raise EmsesError(rc, buf.value.decode(errors="replace"))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.emsesg_stream(self.h) or 0
+
+    def synchronize(self):
+        self._check(self.lib.emsesg_synchronize(self.h))
+
+    # -- explicit sync points
+    def upload_particles(self, pbuf: np.ndarray, totalp, ps: int = 1):
+        pbuf = np.ascontiguousarray(pbuf, dtype=PARTICLE_DTYPE)
+        tp = (ctypes.c_int64 * ISPEC)(*[int(t) for t in totalp])
+        self._check(self.lib.emsesg_upload_particles(self.h, ps, pbuf.ctypes.data, tp))
+
+    def download_particles(self, ps: int = 1):
+        tp = (ctypes.c_int64 * ISPEC)()
+        self._check(self.lib.emsesg_download_particles(self.h, ps, None, tp))
+        total = sum(tp[: self.cfg.nspec])
+        out = np.zeros(total, dtype=PARTICLE_DTYPE)
+        self._check(self.lib.emsesg_download_particles(self.h, ps, out.ctypes.data, tp))
+        return out, np.array(tp[: self.cfg.nspec], dtype=np.int64)
+
+    def field_size(self, name: str) -> int:
+        n = ctypes.c_int64()
+        self._check(self.lib.emsesg_field_size(self.h, FIELDS[name], ctypes.byref(n)))
+        return n.value
+
+    def upload_field(self, name: str, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        if a.size != self.field_size(name):
+            raise ValueError(f"{name}: expected {self.field_size(name)} doubles, got {a.size}")
+        self._check(self.lib.emsesg_upload_field(self.h, FIELDS[name], a.ctypes.data))
+
+    def download_field(self, name: str) -> np.ndarray:
+        out = np.zeros(field_shape(self.cfg, name), dtype=np.float64)
+        self._check(self.lib.emsesg_download_field(self.h, FIELDS[name], out.ctypes.data))
+        return out
+
+    def zero_field(self, name: str):
+        self._check(self.lib.emsesg_zero_field(self.h, FIELDS[name]))
+
+    def set_counters(self, gc: Counter):
+        self._check(self.lib.emsesg_set_counters(self.h, ctypes.byref(gc)))
+
+    def get_counters(self) -> Counter:
+        gc = Counter()
+        self._check(self.lib.emsesg_get_counters(self.h, ctypes.byref(gc)))
+        return gc
+
+    def set_randoms(self, u: np.ndarray):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        self._check(self.lib.emsesg_set_randoms(self.h, u.ctypes.data if u.size else None, u.size))
+
+    # -- the reference subroutines
+    def grdcrt(self, ps: int = 1):
+        self._check(self.lib.emsesg_grdcrt(self.h, ps))
+
+    def psolve2(self, ps: int, ustep: int, gcount: Counter | None = None):
+        self._check(self.lib.emsesg_psolve2(self.h, ps, ustep, ctypes.byref(gcount) if gcount else None))
+
+    def psolve1(self, ps: int, ustep: int, func: int, gcount: Counter | None = None):
+        self._check(self.lib.emsesg_psolve1(self.h, ps, ustep, func, ctypes.byref(gcount) if gcount else None))
+
+    def charge(self, ps: int, func: int):
+        self._check(self.lib.emsesg_charge(self.h, ps, func))
+
+    def reduce_rho(self, name: str = "rho"):
+        self._check(self.lib.emsesg_reduce_rho(self.h, FIELDS[name]))
+
+    def reduce_aj(self):
+        self._check(self.lib.emsesg_reduce_aj(self.h))
+
+    def reduce_ajdg(self):
+        self._check(self.lib.emsesg_reduce_ajdg(self.h))
+
+    def spsort(self, ps: int = 1):
+        self._check(self.lib.emsesg_spsort(self.h, ps))
+
+    def compact(self, ps: int = 1) -> np.ndarray:
+        tp = (ctypes.c_int64 * ISPEC)()
+        self._check(self.lib.emsesg_compact(self.h, ps, tp))
+        return np.array(tp[: self.cfg.nspec], dtype=np.int64)
+
+    def rhoupd(self, ps: int = 1):
+        self._check(self.lib.emsesg_rhoupd(self.h, ps))
+
+    def energy(self) -> np.ndarray:
+        e = (ctypes.c_double * (3 * ISPEC))()
+        self._check(self.lib.emsesg_energy(self.h, e))
+        return np.array(e[: 3 * self.cfg.nspec]).reshape(self.cfg.nspec, 3)
+
+    # -- FP32 / fixed-point form
+    def fx_load(self):
+        self._check(self.lib.emsesg_fx_load(self.h))
+
+    def fx_store(self):
+        self._check(self.lib.emsesg_fx_store(self.h))
+
+    def fx_step(self, ustep: int = 2, do_sort: bool = False):
+        self._check(self.lib.emsesg_fx_step(self.h, ustep, 1 if do_sort else 0))
+
+    def fx_sort(self):
+        self._check(self.lib.emsesg_fx_sort(self.h))
+
+    def fx_counts(self) -> np.ndarray:
+        tp = (ctypes.c_int64 * ISPEC)()
+        self._check(self.lib.emsesg_fx_counts(self.h, tp))
+        return np.array(tp[: self.cfg.nspec], dtype=np.int64)
+
+    def fx_download_accum(self) -> tuple[np.ndarray, np.ndarray]:
+        nr = int(np.prod(field_shape(self.cfg, "rho")))
+        nj = int(np.prod(field_shape(self.cfg, "aj")))
+        out = np.zeros(nr + nj, dtype=np.int64)
+        self._check(self.lib.emsesg_fx_download_accum(self.h, out.ctypes.data))
+        return out[:nr].reshape(field_shape(self.cfg, "rho")), out[nr:].reshape(field_shape(self.cfg, "aj"))
+
+    # -- synthetic loader and profile
+    def load_plasma(self, pl: Plasma):
+        self._check(self.lib.emsesg_load_plasma(self.h, ctypes.byref(pl)))
+
+    def set_profiling(self, on: bool):
+        self._check(self.lib.emsesg_set_profiling(self.h, 1 if on else 0))
+
+    def profile(self) -> dict[str, tuple[float, int]]:
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(self.lib.emsesg_profile_report(self.h, buf, 1 << 16))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, ms, n = line.split()
+            out[name] = (float(ms), int(n))
+        return out
+
+    def profile_reset(self):
+        self._check(self.lib.emsesg_profile_reset(self.h))

@@ -1,0 +1,248 @@
+/*
+ * emses_gpu.h -- C ABI of the B200 (sm_100a) particle hot path of EMSES
+ * (MPIEMSES3D): Buneman-Boris push with trilinear E/B gather and
+ * boundary/body handling, the particle cell sort, CIC charge deposition and
+ * the charge-conserving zigzag current deposition.
+ *
+ * The entry points keep the argument meaning of the reference's external
+ * Fortran subroutines so that an ISO_C_BINDING shim with the same subroutine
+ * names (grdcrt, psolve1, psolve2, charge, spsort) can forward to them:
+ *
+ *   emsesg_grdcrt    <- subroutine grdcrt(ps)            src/field/grdcrt.F90:125
+ *   emsesg_psolve2   <- subroutine psolve2(ps, ustep)     src/pcl2field/psolve2.F90:4
+ *   emsesg_psolve1   <- subroutine psolve1(ps,ustep,func) src/pcl2field/psolve1.F90:4
+ *   emsesg_charge    <- subroutine charge(ps, func)       src/pcl2field/charge.F90:4
+ *   emsesg_spsort    <- subroutine spsort(ps)             src/etc/spsort.F90:4
+ *                       (and the C symbol particle_sort_,  lib/psort/psort-struct.c:7)
+ *   emsesg_compact   <- single-rank part of oh3_transbound
+ *                       lib/ohhelp/ohhelp-1.1.1/ohhelp2.c:103-123
+ *   emsesg_reduce_rho / emsesg_reduce_aj / emsesg_reduce_ajdg
+ *                    <- oh3_exchange_borders (ohhelp3.c:1011) on one rank
+ *                       followed by add_boundary_charge (charge.F90:214),
+ *                       add_boundary_current (psolve1.F90:859) and
+ *                       add_boundary_current2 (psolve1.F90:1081)
+ *   emsesg_rhoupd    <- subroutine rhoupd(ps)             src/field/rhoupd.F90:4
+ *   emsesg_energy    <- kinetic part of energy            src/etc/energy.F90:29-47
+ *
+ * Single rank, one GPU: ps must be 1 (the helper subdomain ps=2 of OhHelp is
+ * not supported and returns EMSESG_ERR_UNSUPPORTED).  There is no CPU
+ * fallback: every compute entry point launches CUDA kernels.
+ *
+ * Data ownership: the context owns persistent device mirrors of pbuf, eb,
+ * wrk, rho, rhodg, rhobk, rhobksp, aj and ajdg.  Between calls the device
+ * copy is authoritative; host arrays are read or written only by the
+ * explicit upload/download calls.  Compute calls are asynchronous on the
+ * context's CUDA stream, except where a host output argument is given.
+ *
+ * Array layouts are the reference's Fortran (column-major) layouts with the
+ * guard extents that OhHelp gives them (ohhelp3.c:439-477, ftypes/ctypes in
+ * src/wrapper/ohinit.F90:98-122), for a subdomain of nx*ny*nz cells:
+ *
+ *   eb     (6,        -1:nx+1, -1:ny+1, -1:nz+1)   EMSESG_FIELD_EB
+ *   wrk    (9,        -4:nx+4, -4:ny+4, -4:nz+4)   EMSESG_FIELD_WRK
+ *   aj     (3,        -4:nx+4, -4:ny+4, -4:nz+4)   EMSESG_FIELD_AJ
+ *   ajdg   (3*nspec,  -4:nx+4, -4:ny+4, -4:nz+4)   EMSESG_FIELD_AJDG
+ *   rho    (1,        -1:nx+1, -1:ny+1, -1:nz+1)   EMSESG_FIELD_RHO
+ *   rhodg  (2*nspec+1,-1:nx+1, -1:ny+1, -1:nz+1)   EMSESG_FIELD_RHODG
+ *   rhobk  (1,        -1:nx+1, -1:ny+1, -1:nz+1)   EMSESG_FIELD_RHOBK
+ *   rhobksp(1,        -1:nx+1, -1:ny+1, -1:nz+1, nspec) EMSESG_FIELD_RHOBKSP
+ *
+ * Error convention: every function returns an int status (EMSESG_OK == 0);
+ * none of them exits, aborts or traps.  emsesg_last_error() gives the text.
+ * A context is not thread-safe; use one context per host thread.
+ */
+#ifndef EMSES_GPU_H
+#define EMSES_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Array caps of the reference, src/main/paramt.F90:55-60 (ispec, inpc). */
+#define EMSESG_ISPEC 10
+#define EMSESG_INPC 15
+
+/* Status codes. */
+#define EMSESG_OK 0
+#define EMSESG_ERR_ARG 1          /* bad argument or configuration */
+#define EMSESG_ERR_UNSUPPORTED 2  /* ps=2, disabled physics options */
+#define EMSESG_ERR_CUDA 3         /* a CUDA runtime call failed */
+#define EMSESG_ERR_OVERFLOW 4     /* particle capacity exceeded */
+#define EMSESG_ERR_NOMEM 5        /* device allocation failed */
+#define EMSESG_ERR_TIMEOUT 6      /* a bounded device wait gave up */
+#define EMSESG_ERR_DEVICE 7       /* a kernel reported a bad index */
+#define EMSESG_ERR_STATE 8        /* call out of order (e.g. no fixed state) */
+
+/* Particle states, lib/ohhelp/ohhelp-1.1.1/oh_type.F90:31-34. */
+#define EMSESG_PCL_ALIVE 0
+#define EMSESG_PCL_INJECTED 1
+#define EMSESG_PCL_TO_BE_ACCUMULATED (-1)
+#define EMSESG_PCL_TO_BE_ACCUMULATED_AS_ANTIPCL (-2)
+
+/* Field identifiers for upload/download. */
+#define EMSESG_FIELD_EB 0
+#define EMSESG_FIELD_WRK 1
+#define EMSESG_FIELD_AJ 2
+#define EMSESG_FIELD_AJDG 3
+#define EMSESG_FIELD_RHO 4
+#define EMSESG_FIELD_RHODG 5
+#define EMSESG_FIELD_RHOBK 6
+#define EMSESG_FIELD_RHOBKSP 7
+#define EMSESG_NFIELDS 8
+
+/* The OhHelp particle record oh_particle (oh_type.F90:15-28, oh_part.h:23-28,
+ * OH_BIG_SPACE off): 64 bytes. */
+typedef struct emsesg_particle {
+  double x, y, z, vx, vy, vz;
+  int32_t pid;
+  int32_t preside;
+  int32_t nid;
+  int32_t spec;
+} emsesg_particle;
+
+/* The Fortran sequence type `counter` (src/main/paramt.F90:76-83) with the
+ * same memory layout: Fortran (a,b,c) arrays appear as C [c][b][a]. */
+typedef struct emsesg_counter {
+  int64_t globalp[2][EMSESG_ISPEC];
+  int32_t influx[EMSESG_ISPEC][EMSESG_INPC];
+  int32_t outflux[EMSESG_ISPEC][EMSESG_INPC];
+  int32_t infhist[EMSESG_ISPEC][EMSESG_INPC][EMSESG_INPC + 1];
+  int32_t nesc[(EMSESG_ISPEC + 1) / 2 * 2];
+  double chgacm[EMSESG_INPC][2];
+} emsesg_counter;
+
+/* One internal body (&ptcond), as tested by psolve2.F90:465-531. */
+typedef struct emsesg_body {
+  int32_t geotype;   /* 0 or 1: box; 2: cylinder; 3: sphere; <0: none */
+  int32_t ncond;     /* >0: conductor, chgacm is accumulated */
+  int32_t cyl_align; /* cylinder axis 1=x 2=y 3=z */
+  int32_t reserved_;
+  double xlpc, xupc, ylpc, yupc, zlpc, zupc; /* box bounds, inclusive */
+  double cyl_axis[2];
+  double cyl_edge[2];
+  double radius;     /* cylinder / sphere radius */
+  double sph_center[3];
+  double sqdscaled;  /* chgacm weight (allcom.F90:132) */
+} emsesg_body;
+
+/* Run configuration in the reference's internal units (rescal.F90:47-81). */
+typedef struct emsesg_config {
+  int32_t nx, ny, nz;               /* subdomain cells = sdoms(2,d)-sdoms(1,d) */
+  int32_t nspec;                    /* number of species, <= EMSESG_ISPEC */
+  int32_t nfbnd[3];                 /* field BC per axis: 0 periodic */
+  int32_t npbnd[EMSESG_ISPEC][3];   /* particle BC per species, axis: 0 wrap,
+                                       1 reflect, 2 escape (npbnd(3,ispec)) */
+  int32_t npc;                      /* number of bodies, <= EMSESG_INPC */
+  int32_t line_mode;                /* 1 disables the body test */
+  int32_t rng_mode;                 /* 0 counter hash, 1 pre-drawn uniforms */
+  int32_t sort_tile[3];             /* cell tile of the sort key (0: whole grid) */
+  int32_t reserved_;
+  uint64_t rng_seed;                /* seed of the counter hash */
+  double q[EMSESG_ISPEC];           /* charge per macro-particle */
+  double qm[EMSESG_ISPEC];          /* charge-to-mass ratio */
+  double rm[EMSESG_ISPEC];          /* mass (energy.F90:44) */
+  double e0[3], b0[3];              /* background fields added by grdcrt */
+  emsesg_body body[EMSESG_INPC];
+  int64_t capacity[EMSESG_ISPEC];   /* device particle capacity per species */
+} emsesg_config;
+
+typedef struct emsesg_ctx emsesg_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+/* Makes `device` the CUDA device of the contexts created next by this host
+ * thread (one process per GPU: call it with the local rank). */
+int emsesg_select_device(int device);
+int emsesg_create(const emsesg_config* cfg, emsesg_ctx** out);
+int emsesg_destroy(emsesg_ctx* ctx);
+/* Copies the last error text (NUL-terminated) into buf. */
+int emsesg_last_error(const emsesg_ctx* ctx, char* buf, size_t len);
+/* The context's cudaStream_t, as an opaque pointer. */
+void* emsesg_stream(emsesg_ctx* ctx);
+int emsesg_synchronize(emsesg_ctx* ctx);
+/* Number of doubles of a field array in the layout above. */
+int emsesg_field_size(const emsesg_ctx* ctx, int field, int64_t* ndoubles);
+
+/* ---- explicit sync points (host <-> device) ---------------------------- */
+/* pbuf holds the species segments back to back (pbase = 0); totalp[is] is
+ * the count of species is (totalp(is,ps)). */
+int emsesg_upload_particles(emsesg_ctx* ctx, int ps, const emsesg_particle* pbuf,
+                            const int64_t* totalp);
+int emsesg_download_particles(emsesg_ctx* ctx, int ps, emsesg_particle* pbuf,
+                              int64_t* totalp);
+int emsesg_upload_field(emsesg_ctx* ctx, int field, const double* host);
+int emsesg_download_field(emsesg_ctx* ctx, int field, double* host);
+/* Sets a whole field array to 0.0, as `aj(:,:,:,:,1:2) = 0.0d0` at the start
+ * of a step (src/main/esses.F90:318-321, src/pcl/psuper1.F90:88-90). */
+int emsesg_zero_field(emsesg_ctx* ctx, int field);
+/* Counters (gcount(1)): set before a push, read after it. */
+int emsesg_set_counters(emsesg_ctx* ctx, const emsesg_counter* gcount);
+int emsesg_get_counters(emsesg_ctx* ctx, emsesg_counter* gcount);
+/* Pre-drawn U[0,1) numbers for injected particles (rng_mode 1): the k-th
+ * injected particle met by a push, in buffer order, takes u[k]; the index
+ * carries over from call to call until emsesg_set_randoms is called again. */
+int emsesg_set_randoms(emsesg_ctx* ctx, const double* u, int64_t n);
+
+/* ---- the reference subroutines (plain FP64 drop-in) --------------------- */
+int emsesg_grdcrt(emsesg_ctx* ctx, int ps);
+/* gcount may be NULL: counters then stay on the device (emsesg_get_counters). */
+int emsesg_psolve2(emsesg_ctx* ctx, int ps, int ustep, emsesg_counter* gcount);
+int emsesg_psolve1(emsesg_ctx* ctx, int ps, int ustep, int func,
+                   emsesg_counter* gcount);
+int emsesg_charge(emsesg_ctx* ctx, int ps, int func);
+int emsesg_reduce_rho(emsesg_ctx* ctx, int field);
+int emsesg_reduce_aj(emsesg_ctx* ctx);
+int emsesg_reduce_ajdg(emsesg_ctx* ctx);
+int emsesg_spsort(emsesg_ctx* ctx, int ps);
+/* Drops particles with nid == -1, keeps species segments contiguous and the
+ * survivors in buffer order; totalp (may be NULL) receives the new counts. */
+int emsesg_compact(emsesg_ctx* ctx, int ps, int64_t* totalp);
+int emsesg_rhoupd(emsesg_ctx* ctx, int ps);
+/* engk[is*3 + d] = 0.5*rm(is)*sum(v_d^2)/(slx*sly*slz), FP64. */
+int emsesg_energy(emsesg_ctx* ctx, double* engk);
+
+/* ---- FP32 / fixed-point form -------------------------------------------
+ * Particle state as SoA {packed int32 cell, 3 x FP32 in-cell offset,
+ * 3 x FP32 velocity} = 28 bytes, species segments, sorted by the tile-major
+ * cell key.  rho and J accumulate in int64 fixed point (scale 2^40), so the
+ * sums do not depend on the order in which threads add them. */
+/* Converts the FP64 pbuf mirror into the FP32 form and sorts it. */
+int emsesg_fx_load(emsesg_ctx* ctx);
+/* Converts the FP32 form back into the FP64 pbuf mirror (for download). */
+int emsesg_fx_store(emsesg_ctx* ctx);
+/* One step: FP32 field relocation (grdcrt), push, zigzag J and CIC rho into
+ * the fixed-point accumulators, guard folding, FP64 rho/aj outputs.  Sorts
+ * (and compacts) first when do_sort != 0. */
+int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort);
+int emsesg_fx_sort(emsesg_ctx* ctx);
+/* Particle counts of the FP32 form (nspec entries). */
+int emsesg_fx_counts(emsesg_ctx* ctx, int64_t* totalp);
+/* Raw fixed-point accumulators after the guard folding, int64 at 2^40:
+ * rho in the rho layout followed by (jx, jy, jz) in the aj layout. */
+int emsesg_fx_download_accum(emsesg_ctx* ctx, int64_t* host);
+
+/* ---- synthetic plasma loader (seeded, on the device) -------------------- */
+typedef struct emsesg_plasma {
+  int32_t ppc[EMSESG_ISPEC];     /* particles per cell per species */
+  double vth[EMSESG_ISPEC];      /* thermal speed (internal units) */
+  double vdrift[EMSESG_ISPEC][3];/* drift velocity (internal units) */
+  uint64_t seed;
+} emsesg_plasma;
+/* Fills the FP64 pbuf mirror: ppc particles uniform in every cell,
+ * Maxwellian velocities (Box-Muller on a SplitMix64 counter hash). */
+int emsesg_load_plasma(emsesg_ctx* ctx, const emsesg_plasma* pl);
+
+/* ---- profiling ----------------------------------------------------------- */
+/* When on, every kernel launch is bracketed by CUDA events on the context
+ * stream and its duration is summed per kernel name. */
+int emsesg_set_profiling(emsesg_ctx* ctx, int on);
+/* Writes "name total_ms launches\n" lines; returns EMSESG_OK. */
+int emsesg_profile_report(emsesg_ctx* ctx, char* buf, size_t len);
+int emsesg_profile_reset(emsesg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EMSES_GPU_H */

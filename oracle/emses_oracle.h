@@ -1,0 +1,85 @@
+/*
+ * emses_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A CPU FP64 restatement of the reference's particle hot path, written
+ * statement for statement from the Fortran sources and used only as the
+ * checker of the CUDA path (by tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference arm of bench.py).  Nothing in the product links
+ * or calls it.
+ *
+ * Parity status: the reference Fortran cannot be compiled in this
+ * environment (no Fortran compiler, MPI, HDF5 or FFTW), and the reference
+ * has no tests or golden vectors for this path.  The parts of the reference
+ * that are C (lib/mtarm/mt19937arm.c, lib/psort/psort-struct.c) are compiled
+ * from their own sources into oracle/_ref and checked against this file;
+ * the Fortran statements are pinned by the golden fixtures that
+ * tests/golden/make_golden.py produces by executing the reference's own
+ * Fortran source text with a small interpreter (see that script).
+ *
+ * Arithmetic: IEEE FP64, no FMA contraction (-ffp-contract=off), Fortran
+ * left-to-right expression order.  Fortran int() truncates toward zero,
+ * floor() rounds down; both are kept where the reference uses them.
+ */
+#ifndef EMSES_ORACLE_H
+#define EMSES_ORACLE_H
+#include "../include/emses_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Size in doubles of a field array (same layouts as emses_gpu.h). */
+int64_t orc_field_size(const emsesg_config* c, int field);
+
+/* Single-rank guard fill of eb (oh3_exchange_borders with CEB), periodic axes. */
+void orc_exchange_eb(const emsesg_config* c, double* eb);
+
+void orc_grdcrt(const emsesg_config* c, const double* eb, double* wrk);
+
+/* Random numbers for injected particles: rng_mode 1 consumes ranu[*ranu_pos]
+ * in buffer order; rng_mode 0 uses the counter hash of (seed, stream, m). */
+int orc_psolve2(const emsesg_config* c, int ustep, const double* wrk,
+                emsesg_particle* pbuf, const int64_t* totalp, const double* ranu,
+                int64_t nranu, int64_t* ranu_pos, uint64_t rng_stream,
+                emsesg_counter* gc);
+int orc_psolve1(const emsesg_config* c, int ustep, int func, double* wrk,
+                emsesg_particle* pbuf, const int64_t* totalp, const double* ranu,
+                int64_t nranu, int64_t* ranu_pos, uint64_t rng_stream,
+                double* aj, double* ajdg, emsesg_counter* gc);
+void orc_charge(const emsesg_config* c, int func, emsesg_particle* pbuf,
+                const int64_t* totalp, double* rho, double* rhodg, double* rhobk,
+                double* rhobksp);
+/* oh3_exchange_borders(CRH) + add_boundary_charge on an array of ncomp
+ * components with the rho layout. */
+void orc_reduce_rho(const emsesg_config* c, double* rh, int ncomp);
+/* oh3_exchange_borders(CAJ) + add_boundary_current; ncomp = 3. */
+void orc_reduce_aj(const emsesg_config* c, double* aj);
+/* oh3_exchange_borders(CJD) + add_boundary_current2; ncomp = 3*nspec. */
+void orc_reduce_ajdg(const emsesg_config* c, double* ajdg);
+void orc_rhoupd(const emsesg_config* c, double* rho, const double* aj);
+void orc_energy(const emsesg_config* c, const emsesg_particle* pbuf,
+                const int64_t* totalp, double* engk);
+
+/* Canonical sort key of a particle and the stable sort by it. */
+int64_t orc_sort_key(const emsesg_config* c, const emsesg_particle* p);
+void orc_spsort(const emsesg_config* c, emsesg_particle* pbuf, const int64_t* totalp);
+void orc_compact(const emsesg_config* c, emsesg_particle* pbuf, int64_t* totalp);
+
+/* Counter hash used for injected particles (rng_mode 0). */
+double orc_hash_u01(uint64_t seed, uint64_t stream, uint64_t index);
+
+/* Synthetic plasma loader, same hash streams as emsesg_load_plasma. */
+void orc_load_plasma(const emsesg_config* c, const emsesg_plasma* pl,
+                     emsesg_particle* pbuf, int64_t* totalp);
+
+/* Timed CPU baseline: one step psolve1 (zigzag J) + charge(func 0) on
+ * `threads` OpenMP threads with private rho/aj per thread.  Returns the
+ * wall time in seconds. */
+double orc_step_timed(const emsesg_config* c, int ustep, const double* wrk,
+                      emsesg_particle* pbuf, const int64_t* totalp, double* aj,
+                      double* rho, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

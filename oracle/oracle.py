@@ -1,0 +1,228 @@
+"""TEST INFRASTRUCTURE ONLY: Python binding of the CPU oracle (liboracle.so).
+
+The oracle is the FP64 restatement of the reference's particle path
+(emses_oracle.cpp).  Only tests/, __graft_entry__.smoke() and the CPU
+baseline of bench.py use it, and only as the checker or the timed CPU
+reference; the product (ctca_b200) never imports it.
+
+Also binds oracle/_ref/libemses_ref.so, the reference's own C sources for
+this path (MT19937 of lib/mtarm, particle_sort_ of lib/psort) when built.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from ctca_b200.emses import ISPEC, PARTICLE_DTYPE, Config, Counter, Plasma, field_shape
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libemses_ref.so"
+FIELD_IDS = {"eb": 0, "wrk": 1, "aj": 2, "ajdg": 3, "rho": 4, "rhodg": 5, "rhobk": 6, "rhobksp": 7}
+
+_P = ctypes.c_void_p
+_lib = None
+
+
+def build(reference: str | None = None):
+    """Builds liboracle.so (and _ref/ when the reference sources exist)."""
+    args = ["make", "-C", str(HERE), "liboracle.so"]
+    subprocess.run(args, check=True, capture_output=True)
+    ref = Path(reference or "/root/reference")
+    if (ref / "lib" / "mtarm" / "mt19937arm.c").exists():
+        subprocess.run(["make", "-C", str(HERE), "ref", f"REFERENCE={ref}"], check=True, capture_output=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB.exists():
+        build()
+    L = ctypes.CDLL(str(LIB))
+    cfgp = ctypes.POINTER(Config)
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    sigs = {
+        "orc_field_size": (ctypes.c_int64, [cfgp, ctypes.c_int]),
+        "orc_exchange_eb": (None, [cfgp, _P]),
+        "orc_grdcrt": (None, [cfgp, _P, _P]),
+        "orc_psolve2": (ctypes.c_int, [cfgp, ctypes.c_int, _P, _P, i64p, _P, ctypes.c_int64, i64p, ctypes.c_uint64,
+                                       ctypes.POINTER(Counter)]),
+        "orc_psolve1": (ctypes.c_int, [cfgp, ctypes.c_int, ctypes.c_int, _P, _P, i64p, _P, ctypes.c_int64, i64p,
+                                       ctypes.c_uint64, _P, _P, ctypes.POINTER(Counter)]),
+        "orc_charge": (None, [cfgp, ctypes.c_int, _P, i64p, _P, _P, _P, _P]),
+        "orc_reduce_rho": (None, [cfgp, _P, ctypes.c_int]),
+        "orc_reduce_aj": (None, [cfgp, _P]),
+        "orc_reduce_ajdg": (None, [cfgp, _P]),
+        "orc_rhoupd": (None, [cfgp, _P, _P]),
+        "orc_energy": (None, [cfgp, _P, i64p, _P]),
+        "orc_sort_key": (ctypes.c_int64, [cfgp, _P]),
+        "orc_spsort": (None, [cfgp, _P, i64p]),
+        "orc_compact": (None, [cfgp, _P, i64p]),
+        "orc_hash_u01": (ctypes.c_double, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+        "orc_load_plasma": (None, [cfgp, ctypes.POINTER(Plasma), _P, i64p]),
+        "orc_step_timed": (ctypes.c_double, [cfgp, ctypes.c_int, _P, _P, i64p, _P, _P, ctypes.c_int]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _tp(totalp) -> ctypes.Array:
+    return (ctypes.c_int64 * ISPEC)(*[int(t) for t in totalp])
+
+
+def zeros(cfg: Config, name: str) -> np.ndarray:
+    return np.zeros(field_shape(cfg, name), dtype=np.float64)
+
+
+class Oracle:
+    """Holds the CPU state of one rank: pbuf, wrk, aj, ajdg, rho, ... ."""
+
+    def __init__(self, cfg: Config, pbuf: np.ndarray, totalp, eb: np.ndarray):
+        self.cfg = cfg
+        self.L = lib()
+        self.pbuf = np.ascontiguousarray(pbuf, dtype=PARTICLE_DTYPE).copy()
+        self.totalp = np.array(totalp, dtype=np.int64)
+        self.eb = np.ascontiguousarray(eb, dtype=np.float64).copy()
+        self.f = {name: zeros(cfg, name) for name in FIELD_IDS if name != "eb"}
+        self.gc = Counter()
+        self.ranu = np.zeros(0)
+        self.ranu_pos = ctypes.c_int64(0)
+        self.rng_stream = 0
+
+    def _c(self):
+        return ctypes.byref(self.cfg)
+
+    def set_randoms(self, u):
+        self.ranu = np.ascontiguousarray(u, dtype=np.float64)
+        self.ranu_pos = ctypes.c_int64(0)
+
+    def grdcrt(self):
+        self.L.orc_grdcrt(self._c(), self.eb.ctypes.data, self.f["wrk"].ctypes.data)
+
+    def psolve2(self, ustep: int):
+        tp = _tp(self.totalp)
+        rc = self.L.orc_psolve2(self._c(), ustep, self.f["wrk"].ctypes.data, self.pbuf.ctypes.data, tp,
+                                self.ranu.ctypes.data if self.ranu.size else None, self.ranu.size,
+                                ctypes.byref(self.ranu_pos), self.rng_stream, ctypes.byref(self.gc))
+        self.rng_stream += 1
+        if rc:
+            raise RuntimeError("oracle psolve2: random numbers exhausted")
+
+    def psolve1(self, ustep: int, func: int = 0):
+        tp = _tp(self.totalp)
+        rc = self.L.orc_psolve1(self._c(), ustep, func, self.f["wrk"].ctypes.data, self.pbuf.ctypes.data, tp,
+                                self.ranu.ctypes.data if self.ranu.size else None, self.ranu.size,
+                                ctypes.byref(self.ranu_pos), self.rng_stream, self.f["aj"].ctypes.data,
+                                self.f["ajdg"].ctypes.data, ctypes.byref(self.gc))
+        self.rng_stream += 1
+        if rc:
+            raise RuntimeError("oracle psolve1: random numbers exhausted")
+
+    def charge(self, func: int = 0):
+        tp = _tp(self.totalp)
+        self.L.orc_charge(self._c(), func, self.pbuf.ctypes.data, tp, self.f["rho"].ctypes.data,
+                          self.f["rhodg"].ctypes.data, self.f["rhobk"].ctypes.data, self.f["rhobksp"].ctypes.data)
+
+    def reduce_rho(self, name: str = "rho"):
+        a = self.f[name]
+        nc = a.shape[-1]
+        if name == "rhobksp":
+            for s in range(a.shape[0]):
+                sub = np.ascontiguousarray(a[s])
+                self.L.orc_reduce_rho(self._c(), sub.ctypes.data, nc)
+                a[s] = sub
+        else:
+            self.L.orc_reduce_rho(self._c(), a.ctypes.data, nc)
+
+    def reduce_aj(self):
+        self.L.orc_reduce_aj(self._c(), self.f["aj"].ctypes.data)
+
+    def reduce_ajdg(self):
+        self.L.orc_reduce_ajdg(self._c(), self.f["ajdg"].ctypes.data)
+
+    def rhoupd(self):
+        self.L.orc_rhoupd(self._c(), self.f["rho"].ctypes.data, self.f["aj"].ctypes.data)
+
+    def energy(self) -> np.ndarray:
+        e = np.zeros(3 * ISPEC)
+        self.L.orc_energy(self._c(), self.pbuf.ctypes.data, _tp(self.totalp), e.ctypes.data)
+        return e[: 3 * self.cfg.nspec].reshape(self.cfg.nspec, 3)
+
+    def spsort(self):
+        self.L.orc_spsort(self._c(), self.pbuf.ctypes.data, _tp(self.totalp))
+
+    def compact(self):
+        tp = _tp(self.totalp)
+        self.L.orc_compact(self._c(), self.pbuf.ctypes.data, tp)
+        self.totalp = np.array(tp[: self.cfg.nspec], dtype=np.int64)
+        self.pbuf = self.pbuf[: int(self.totalp.sum())].copy()
+
+    def sort_keys(self) -> np.ndarray:
+        return np.array([self.L.orc_sort_key(self._c(), self.pbuf[m:m + 1].ctypes.data)
+                         for m in range(self.pbuf.size)], dtype=np.int64)
+
+
+def exchange_eb(cfg: Config, eb: np.ndarray) -> np.ndarray:
+    out = np.ascontiguousarray(eb, dtype=np.float64).copy()
+    lib().orc_exchange_eb(ctypes.byref(cfg), out.ctypes.data)
+    return out
+
+
+def hash_u01(seed: int, stream: int, index: int) -> float:
+    return lib().orc_hash_u01(seed, stream, index)
+
+
+def load_plasma(cfg: Config, pl: Plasma):
+    n = int(sum(pl.ppc[i] for i in range(cfg.nspec))) * cfg.nx * cfg.ny * cfg.nz
+    pbuf = np.zeros(n, dtype=PARTICLE_DTYPE)
+    tp = (ctypes.c_int64 * ISPEC)()
+    lib().orc_load_plasma(ctypes.byref(cfg), ctypes.byref(pl), pbuf.ctypes.data, tp)
+    return pbuf, np.array(tp[: cfg.nspec], dtype=np.int64)
+
+
+def step_timed(cfg: Config, ustep: int, wrk: np.ndarray, pbuf: np.ndarray, totalp, threads: int):
+    """One psolve1 + charge step on `threads` host threads; returns seconds."""
+    aj = zeros(cfg, "aj")
+    rho = zeros(cfg, "rho")
+    return lib().orc_step_timed(ctypes.byref(cfg), ustep, wrk.ctypes.data, pbuf.ctypes.data, _tp(totalp),
+                                aj.ctypes.data, rho.ctypes.data, threads), aj, rho
+
+
+# -- the reference's own C code (oracle/_ref) --------------------------------
+_ref = None
+
+
+def ref_lib():
+    """libemses_ref.so built from the reference's lib/mtarm and lib/psort."""
+    global _ref
+    if _ref is None:
+        if not REF_LIB.exists():
+            return None
+        L = ctypes.CDLL(str(REF_LIB))
+        L.mt_init_.argtypes = [ctypes.POINTER(ctypes.c_int)]
+        L.mt_init_.restype = ctypes.c_int
+        L.mtrand_real8_.argtypes = []
+        L.mtrand_real8_.restype = ctypes.c_double
+        L.particle_sort_.argtypes = [_P, ctypes.POINTER(ctypes.c_int)]
+        L.particle_sort_.restype = None
+        _ref = L
+    return _ref
+
+
+def ranu0_stream(seed: int, n: int) -> np.ndarray:
+    """n successive RANU0 draws of the reference (randinit0 + mtrand_real8,
+    src/wrapper/wrapper.F90:20-87 over lib/mtarm/mt19937arm.c)."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref not built")
+    s = ctypes.c_int(seed)
+    L.mt_init_(ctypes.byref(s))
+    return np.array([L.mtrand_real8_() for _ in range(n)])
