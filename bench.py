@@ -226,7 +226,9 @@ def run_ours(args, world, rank, local):
     k64 = max(1, min(args.steps, args.fp64_steps))
     for s in range(args.warmup):
         fp64_step(s)
+    g.synchronize()
     t64 = timed(fp64_step, k64)
+    g.synchronize()
 
     # ---- FP32 / fixed-point form
     g.fx_load()

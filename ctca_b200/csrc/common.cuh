@@ -99,6 +99,7 @@ struct emsesg_ctx {
   int64_t* d_rand_pos = nullptr;       // next pre-drawn number (device)
   uint64_t rng_stream = 0;             // push call counter for the hash
   int* d_status = nullptr;             // device error word
+  long long* d_diag = nullptr;         // first bad-index report {site, index, what, 0}
   int64_t* d_scratch64 = nullptr;      // small scratch (counts, sums)
   double* d_sum = nullptr;
   emsesg::SortScratch sort;
@@ -117,6 +118,19 @@ void timer_collect(emsesg_ctx* ctx);
 
 // Device status word codes.
 enum { ST_OK = 0, ST_BAD_INDEX = 1, ST_RANDOMS = 2, ST_OVERFLOW = 4 };
+
+// Sites that report ST_BAD_INDEX; the first report also leaves
+// {site, particle index, packed or truncated cell, 0} in the diag record.
+enum { SITE_PSOLVE2 = 1, SITE_PSOLVE1, SITE_CHARGE, SITE_FX_LOAD, SITE_FX_PUSH, SITE_FX_DEPOSIT, SITE_FX_FLUSH };
+
+__device__ __forceinline__ void report_bad(int* status, long long* diag, int site, long long index,
+                                           long long what) {
+  atomicOr(status, ST_BAD_INDEX);
+  if (diag && atomicCAS((unsigned long long*)&diag[0], 0ull, (unsigned long long)site) == 0ull) {
+    diag[1] = index;
+    diag[2] = what;
+  }
+}
 
 // SplitMix64 finaliser (Steele, Lea, Flood 2014).
 __host__ __device__ inline uint64_t mix64(uint64_t z) {

@@ -142,8 +142,9 @@ extern "C" int emsesg_create(const emsesg_config* cfg, emsesg_ctx** out) {
     if ((e = cudaMalloc(&ctx->field[f], n * sizeof(double)))) return fail(e, "field");
     if ((e = cudaMemsetAsync(ctx->field[f], 0, n * sizeof(double), ctx->stream))) return fail(e, "field");
   }
-  int64_t nn = (int64_t)(cfg->nx + 1) * (cfg->ny + 1) * (cfg->nz + 1);
+  int64_t nn = (int64_t)(cfg->nx + 2) * (cfg->ny + 2) * (cfg->nz + 2);
   if ((e = cudaMalloc(&ctx->node64, nn * 8 * sizeof(double)))) return fail(e, "node64");
+  if ((e = cudaMemsetAsync(ctx->node64, 0, nn * 8 * sizeof(double), ctx->stream))) return fail(e, "node64");
   if ((e = cudaMalloc(&ctx->tj, field_doubles(ctx->cfg, EMSESG_FIELD_AJ) * sizeof(double)))) return fail(e, "tj");
   if ((e = cudaMalloc(&ctx->d_counter, sizeof(emsesg_counter)))) return fail(e, "counter");
   if ((e = cudaMemsetAsync(ctx->d_counter, 0, sizeof(emsesg_counter), ctx->stream))) return fail(e, "counter");
@@ -153,6 +154,8 @@ extern "C" int emsesg_create(const emsesg_config* cfg, emsesg_ctx** out) {
   if ((e = cudaMemsetAsync(ctx->d_rand_pos, 0, sizeof(int64_t), ctx->stream))) return fail(e, "rand");
   if ((e = cudaMalloc(&ctx->d_status, sizeof(int)))) return fail(e, "status");
   if ((e = cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream))) return fail(e, "status");
+  if ((e = cudaMalloc(&ctx->d_diag, 4 * sizeof(long long)))) return fail(e, "diag");
+  if ((e = cudaMemsetAsync(ctx->d_diag, 0, 4 * sizeof(long long), ctx->stream))) return fail(e, "diag");
   if ((e = cudaMalloc(&ctx->d_scratch64, 64 * sizeof(int64_t)))) return fail(e, "scratch");
   if ((e = cudaMalloc(&ctx->d_sum, 64 * sizeof(double)))) return fail(e, "sum");
   if ((e = cudaStreamSynchronize(ctx->stream))) return fail(e, "create");
@@ -175,6 +178,7 @@ extern "C" int emsesg_destroy(emsesg_ctx* ctx) {
   cudaFree(ctx->d_randoms);
   cudaFree(ctx->d_rand_pos);
   cudaFree(ctx->d_status);
+  cudaFree(ctx->d_diag);
   cudaFree(ctx->d_scratch64);
   cudaFree(ctx->d_sum);
   for (int b = 0; b < 2; b++) { cudaFree(ctx->sort.keys[b]); cudaFree(ctx->sort.vals[b]); }
@@ -203,10 +207,18 @@ extern "C" int emsesg_synchronize(emsesg_ctx* ctx) {
   int st = 0;
   EMSESG_CUDA(ctx, cudaMemcpy(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
   if (st) {
+    long long diag[4] = {0, 0, 0, 0};
+    cudaMemcpy(diag, ctx->d_diag, sizeof diag, cudaMemcpyDeviceToHost);
     cudaMemset(ctx->d_status, 0, sizeof(int));
+    cudaMemset(ctx->d_diag, 0, sizeof diag);
     if (st & ST_RANDOMS) return set_error(ctx, EMSESG_ERR_ARG, "pre-drawn random numbers exhausted");
     if (st & ST_OVERFLOW) return set_error(ctx, EMSESG_ERR_OVERFLOW, "particle capacity exceeded");
-    return set_error(ctx, EMSESG_ERR_DEVICE, "a kernel met a particle outside the field arrays (status %d)", st);
+    static const char* sites[] = {"?", "psolve2", "psolve1", "charge", "fx_load", "fx_push", "fx_deposit",
+                                  "fx_flush"};
+    int site = (diag[0] >= 0 && diag[0] <= 7) ? (int)diag[0] : 0;
+    return set_error(ctx, EMSESG_ERR_DEVICE,
+                     "a kernel met a particle outside the field arrays (status %d, site %s, index %lld, cell %lld)",
+                     st, sites[site], diag[1], diag[2]);
   }
   return EMSESG_OK;
 }

@@ -54,16 +54,21 @@ struct PushArgs {
   const uint32_t* ordinal;
   emsesg_counter* gc;
   int* status;
+  long long* diag;
   double* tj;             // psolve1: per-species zigzag scratch (aj layout)
   FieldDesc fa;
 };
 
+// The drop-in node field covers nodes 0..n+1 per axis; grdcrt fills 0..n
+// (grdcrt.F90:158-160) and node n+1 stays 0.  A particle that a periodic
+// wrap leaves exactly on x = slx (x - slx + slx rounding) has i = n and gathers
+// node n+1 with weight 0, as the reference reads wrk(n+1) with weight 0.
 __device__ __forceinline__ int64_t node_index(const emsesg_config* c, int i, int j, int k) {
-  return (int64_t)i + (int64_t)(c->nx + 1) * ((int64_t)j + (int64_t)(c->ny + 1) * k);
+  return (int64_t)i + (int64_t)(c->nx + 2) * ((int64_t)j + (int64_t)(c->ny + 2) * k);
 }
 
 __device__ __forceinline__ bool cell_ok(const emsesg_config* c, int i, int j, int k) {
-  return i >= 0 && j >= 0 && k >= 0 && i < c->nx && j < c->ny && k < c->nz;
+  return i >= 0 && j >= 0 && k >= 0 && i <= c->nx && j <= c->ny && k <= c->nz;
 }
 
 // Gather + Buneman-Boris + move, psolve2.F90:185-318 (psolve1.F90:201-333).
@@ -71,7 +76,7 @@ __device__ __forceinline__ void gather_boris_move(const double* __restrict__ nod
                                                   emsesg_particle& p, int i, int j, int k, const W8& w,
                                                   double qmp, double gustep) {
   int64_t n1 = node_index(c, i, j, k + 1), n5 = node_index(c, i, j, k);
-  int64_t sx = 1, sy = c->nx + 1;
+  int64_t sx = 1, sy = c->nx + 2;
   const double* c1 = node + 8 * n1;            // (i,  j,  k1)
   const double* c2 = node + 8 * (n1 + sx);     // (i1, j,  k1)
   const double* c3 = node + 8 * (n1 + sx + sy);// (i1, j1, k1)
@@ -185,7 +190,7 @@ __global__ void k_psolve2(PushArgs a) {
   double xlocal = p.x - dxl, ylocal = p.y - dyl, zlocal = p.z - dzl;
   int i = (int)xlocal, j = (int)ylocal, k = (int)zlocal;
   if (!cell_ok(c, i, j, k) || !(xlocal >= 0.0 && ylocal >= 0.0 && zlocal >= 0.0)) {
-    atomicOr(a.status, ST_BAD_INDEX);
+    report_bad(a.status, a.diag, SITE_PSOLVE2, a.packed_base + m, i + 100000LL * j + 10000000000LL * k);
     return;
   }
   W8 w = weights(xlocal - i, ylocal - j, zlocal - k);
@@ -270,7 +275,7 @@ __global__ void k_psolve1(PushArgs a) {
   double xlocalb = p.x - dxl, ylocalb = p.y - dyl, zlocalb = p.z - dzl;
   int ib = (int)floor(xlocalb), jb = (int)floor(ylocalb), kb = (int)floor(zlocalb);
   if (!cell_ok(c, ib, jb, kb)) {
-    atomicOr(a.status, ST_BAD_INDEX);
+    report_bad(a.status, a.diag, SITE_PSOLVE1, a.packed_base + m, ib + 100000LL * jb + 10000000000LL * kb);
     return;
   }
   double xb = ib, yb = jb, zb = kb;
@@ -445,7 +450,7 @@ __global__ void k_grdcrt(const double* __restrict__ eb, double* __restrict__ nod
   int64_t ex = nx + 1, ey = ny + 1, ez = nz + 1;
   if (t >= ex * ey * ez) return;
   int i = (int)(t % ex), j = (int)((t / ex) % ey), k = (int)(t / (ex * ey));
-  double* o = node + 8 * t;
+  double* o = node + 8 * ((int64_t)i + (ex + 1) * ((int64_t)j + (ey + 1) * k));
   o[EX] = 0.5 * (eb[fe.at(EX, i, j, k)] + eb[fe.at(EX, i - 1, j, k)]) + e0x;
   o[EY] = 0.5 * (eb[fe.at(EY, i, j, k)] + eb[fe.at(EY, i, j - 1, k)]) + e0y;
   o[EZ] = 0.5 * (eb[fe.at(EZ, i, j, k)] + eb[fe.at(EZ, i, j, k - 1)]) + e0z;
@@ -465,7 +470,8 @@ __global__ void k_node_to_wrk(const double* __restrict__ node, double* wrk, Fiel
   int64_t ex = nx + 1, ey = ny + 1, ez = nz + 1;
   if (t >= ex * ey * ez) return;
   int i = (int)(t % ex), j = (int)((t / ex) % ey), k = (int)(t / (ex * ey));
-  for (int cc = 0; cc < 6; cc++) wrk[fw.at(cc, i, j, k)] = node[8 * t + cc];
+  int64_t nd = (int64_t)i + (ex + 1) * ((int64_t)j + (ey + 1) * k);
+  for (int cc = 0; cc < 6; cc++) wrk[fw.at(cc, i, j, k)] = node[8 * nd + cc];
 }
 
 struct ChargeArgs {
@@ -478,6 +484,7 @@ struct ChargeArgs {
   FieldDesc fr, fd;
   const emsesg_config* cfg;
   int* status;
+  long long* diag;
 };
 
 __device__ __forceinline__ void distribute(double* rh, const FieldDesc& f, int cc, int i, int j, int k, double qc,
@@ -502,7 +509,7 @@ __global__ void k_charge(ChargeArgs a) {
   int i = (int)xlocal, j = (int)ylocal, k = (int)zlocal;
   const emsesg_config* c = a.cfg;
   if (i < -1 || j < -1 || k < -1 || i > c->nx || j > c->ny || k > c->nz) {
-    atomicOr(a.status, ST_BAD_INDEX);
+    report_bad(a.status, a.diag, SITE_CHARGE, m, i + 100000LL * j + 10000000000LL * k);
     return;
   }
   W8 w = weights(xlocal - i, ylocal - j, zlocal - k);
@@ -718,6 +725,7 @@ PushArgs push_args(emsesg_ctx* ctx, int is, int ustep) {
   a.rand_pos = ctx->d_rand_pos;
   a.gc = ctx->d_counter;
   a.status = ctx->d_status;
+  a.diag = ctx->d_diag;
   a.tj = ctx->tj;
   a.fa = field_desc(ctx->cfg, EMSESG_FIELD_AJ);
   return a;
@@ -816,6 +824,7 @@ extern "C" int emsesg_charge(emsesg_ctx* ctx, int ps, int func) {
     a.fd = field_desc(c, EMSESG_FIELD_RHODG);
     a.cfg = ctx->d_cfg;
     a.status = ctx->d_status;
+    a.diag = ctx->d_diag;
     EMSESG_LAUNCH(ctx, "charge", k_charge, nblk(a.n), 256, 0, a);
   }
   return EMSESG_OK;

@@ -90,6 +90,7 @@ struct FxPushArgs {
   float qmp, gustep, rustep, qfix;  // qfix = q * 2^40
   int* nesc;
   int* status;
+  long long* diag;
 };
 
 // Per-axis move and outer boundary of psolve1.F90:366-606 on (cell, offset)
@@ -189,13 +190,13 @@ __device__ __forceinline__ void deposit_one(const FxPushArgs& a, const Box& bx, 
     atomicAdd(&box[((comp * bx.B + lk) * bx.B + lj) * bx.B + li], (unsigned long long)v);
   } else if (comp == 0) {
     if (i < -1 || j < -1 || k < -1 || i > a.g.nx + 1 || j > a.g.ny + 1 || k > a.g.nz + 1) {
-      atomicOr(a.status, ST_BAD_INDEX);
+      report_bad(a.status, a.diag, SITE_FX_DEPOSIT, -1, i + 100000LL * j + 10000000000LL * k);
       return;
     }
     atomicAdd(&a.acc_rho[a.fr.at(0, i, j, k)], (unsigned long long)v);
   } else {
     if (i < -4 || j < -4 || k < -4 || i > a.g.nx + 4 || j > a.g.ny + 4 || k > a.g.nz + 4) {
-      atomicOr(a.status, ST_BAD_INDEX);
+      report_bad(a.status, a.diag, SITE_FX_DEPOSIT, -2, i + 100000LL * j + 10000000000LL * k);
       return;
     }
     atomicAdd(&a.acc_j[a.fj.at(comp - 1, i, j, k)], (unsigned long long)v);
@@ -248,7 +249,10 @@ __global__ void __launch_bounds__(FX_THREADS) k_fx_push(FxPushArgs a) {
     int ib = 0, jb = 0, kb = 0;
     if (live) {
       unpack(g, cell, ib, jb, kb);
-      if (ib >= g.nx || jb >= g.ny || kb >= g.nz) { atomicOr(a.status, ST_BAD_INDEX); live = false; }
+      if (ib >= g.nx || jb >= g.ny || kb >= g.nz) {
+        report_bad(a.status, a.diag, SITE_FX_PUSH, m, (long long)cell);
+        live = false;
+      }
     }
     float J1[12], J2[12], R[8];
     Axis ax{}, ay{}, az{};
@@ -407,10 +411,16 @@ __global__ void __launch_bounds__(FX_THREADS) k_fx_push(FxPushArgs a) {
     int li = e % bx.B, lj = (e / bx.B) % bx.B, lk = (e / (bx.B * bx.B)) % bx.B, comp = e / (bx.B * bx.B * bx.B);
     int i = bx.o[0] + li, j = bx.o[1] + lj, k = bx.o[2] + lk;
     if (comp == 0) {
-      if (i < -1 || j < -1 || k < -1 || i > g.nx + 1 || j > g.ny + 1 || k > g.nz + 1) { atomicOr(a.status, ST_BAD_INDEX); continue; }
+      if (i < -1 || j < -1 || k < -1 || i > g.nx + 1 || j > g.ny + 1 || k > g.nz + 1) {
+        report_bad(a.status, a.diag, SITE_FX_FLUSH, t, i + 100000LL * j + 10000000000LL * k);
+        continue;
+      }
       atomicAdd(&a.acc_rho[a.fr.at(0, i, j, k)], v);
     } else {
-      if (i < -4 || j < -4 || k < -4 || i > g.nx + 4 || j > g.ny + 4 || k > g.nz + 4) { atomicOr(a.status, ST_BAD_INDEX); continue; }
+      if (i < -4 || j < -4 || k < -4 || i > g.nx + 4 || j > g.ny + 4 || k > g.nz + 4) {
+        report_bad(a.status, a.diag, SITE_FX_FLUSH, t, i + 100000LL * j + 10000000000LL * k);
+        continue;
+      }
       atomicAdd(&a.acc_j[a.fj.at(comp - 1, i, j, k)], v);
     }
   }
@@ -424,22 +434,31 @@ __global__ void k_fix_to_double(const long long* __restrict__ src, double* __res
 }
 
 // ---------------------------------------------------------------- load / store / sort
+// (cell, offset) of one FP64 coordinate.  An offset that rounds up to 1.0f,
+// or a coordinate exactly on the upper face x = n (left there by the
+// rounding of a periodic wrap), is kept in the last cell with the largest
+// FP32 offset below 1 (an error of at most 6e-8 cell).
+__device__ __forceinline__ bool split_coord(double x, int n, int& c, float& o) {
+  double f = floor(x);
+  c = (int)f;
+  o = (float)(x - f);
+  const float below_one = 0.99999994f;
+  if (o >= 1.0f) o = below_one;
+  if (c == n && x == (double)n) { c = n - 1; o = below_one; }
+  return c >= 0 && c < n;
+}
+
 __global__ void k_fx_from_aos(const emsesg_particle* __restrict__ p, int64_t n, Geo g, float4* pos, float* vx,
-                              float* vy, float* vz, int* status) {
+                              float* vy, float* vz, int* status, long long* diag) {
   int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n) return;
   emsesg_particle q = p[m];
   uint32_t cell = DEAD;
   float ox = 0.f, oy = 0.f, oz = 0.f;
   if (q.nid != -1) {
-    if (q.preside != 0) atomicOr(status, ST_BAD_INDEX);
-    double fx = floor(q.x), fy = floor(q.y), fz = floor(q.z);
-    int i = (int)fx, j = (int)fy, k = (int)fz;
-    ox = (float)(q.x - fx); oy = (float)(q.y - fy); oz = (float)(q.z - fz);
-    if (ox >= 1.0f) { ox = 0.f; i += 1; }
-    if (oy >= 1.0f) { oy = 0.f; j += 1; }
-    if (oz >= 1.0f) { oz = 0.f; k += 1; }
-    if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) atomicOr(status, ST_BAD_INDEX);
+    int i, j, k;
+    bool ok = split_coord(q.x, g.nx, i, ox) & split_coord(q.y, g.ny, j, oy) & split_coord(q.z, g.nz, k, oz);
+    if (!ok || q.preside != 0) report_bad(status, diag, SITE_FX_LOAD, m, i + 100000LL * j + 10000000000LL * k);
     else cell = pack(g, i, j, k);
   }
   pos[m] = make_float4(ox, oy, oz, __int_as_float((int)cell));
@@ -646,7 +665,7 @@ extern "C" int emsesg_fx_load(emsesg_ctx* ctx) {
     int64_t off = ctx->seg.base[is];
     if (n == 0) continue;
     EMSESG_LAUNCH(ctx, "fx_from_aos", k_fx_from_aos, nblk(n), 256, 0, ctx->pbuf + off, n, g, f.pos + off, f.vx + off,
-                  f.vy + off, f.vz + off, ctx->d_status);
+                  f.vy + off, f.vz + off, ctx->d_status, ctx->d_diag);
   }
   EMSESG_CUDA(ctx, cudaMemcpyAsync(f.count_d, ctx->totalp, EMSESG_ISPEC * sizeof(int64_t), cudaMemcpyHostToDevice,
                                    ctx->stream));
@@ -668,10 +687,11 @@ extern "C" int emsesg_fx_counts(emsesg_ctx* ctx, int64_t* totalp) {
 extern "C" int emsesg_fx_store(emsesg_ctx* ctx) {
   if (!ctx) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded");
-  int rc = emsesg_fx_sort(ctx);  // compacts: live particles first
-  if (rc) return rc;
+  // Current buffer order; particles that died since the last sort come out
+  // with nid = -1 in place, as the reference leaves them before transbound.
   int64_t cnt[EMSESG_ISPEC] = {0};
-  if ((rc = emsesg_fx_counts(ctx, cnt))) return rc;
+  int rc = emsesg_fx_counts(ctx, cnt);
+  if (rc) return rc;
   FxState& f = ctx->fx;
   Geo g = make_geo(ctx);
   for (int is = 0; is < ctx->cfg.nspec; is++) {
@@ -726,6 +746,7 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
     a.qfix = (float)(c.q[is] * 1099511627776.0);
     a.nesc = &ctx->d_counter->nesc[is];
     a.status = ctx->d_status;
+    a.diag = ctx->d_diag;
     EMSESG_LAUNCH(ctx, "fx_push", k_fx_push, (unsigned)f.ntiles, FX_THREADS, smem, a);
   }
   // guard folding on the exact integers, then FP64 outputs

@@ -210,7 +210,9 @@ int emsesg_energy(emsesg_ctx* ctx, double* engk);
  * sums do not depend on the order in which threads add them. */
 /* Converts the FP64 pbuf mirror into the FP32 form and sorts it. */
 int emsesg_fx_load(emsesg_ctx* ctx);
-/* Converts the FP32 form back into the FP64 pbuf mirror (for download). */
+/* Converts the FP32 form back into the FP64 pbuf mirror (for download), in
+ * the current buffer order; particles that died since the last sort come
+ * out in place with nid = -1. */
 int emsesg_fx_store(emsesg_ctx* ctx);
 /* One step: FP32 field relocation (grdcrt), push, zigzag J and CIC rho into
  * the fixed-point accumulators, guard folding, FP64 rho/aj outputs.  Sorts

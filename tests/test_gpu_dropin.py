@@ -162,6 +162,28 @@ def test_spsort_permutation_exact(gpu, tile):
     assert same_particles(pg, o.pbuf)
 
 
+def test_spsort_large_multi_block(gpu):
+    """~1M particles: many radix blocks and a two-level prefix sum."""
+    c = case(n=(64, 64, 64), ppc=(2, 2), tile=(8, 8, 8))
+    cfg, eb, p, tp = build(c)
+    rng = np.random.default_rng(2)
+    perm = np.concatenate([rng.permutation(tp[0]), tp[0] + rng.permutation(tp[1])])
+    p = p[perm]
+    g = Emses(cfg)
+    g.upload_particles(p, tp)
+    o = O.Oracle(cfg, p, tp, eb)
+    g.spsort(1)
+    o.spsort()
+    pg, _ = g.download_particles()
+    assert same_particles(pg, o.pbuf)
+    p["nid"][::3] = -1
+    g.upload_particles(p, tp)
+    o = O.Oracle(cfg, p, tp, eb)
+    assert np.array_equal(g.compact(1), (o.compact(), o.totalp)[1])
+    pg, _ = g.download_particles()
+    assert same_particles(pg, o.pbuf)
+
+
 def test_compact_exact(gpu):
     c = case()
     cfg, eb, p, tp = build(c)
