@@ -27,6 +27,7 @@ SOURCES = {
     "dropin.cu": ["--fmad=false"],
     "sort.cu": [],
     "fx.cu": [],
+    "noalloc.cu": [],
 }
 
 

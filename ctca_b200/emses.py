@@ -116,6 +116,7 @@ _SIGS = {
     "emsesg_spsort": (_I, [_P, _I]),
     "emsesg_compact": (_I, [_P, _I, ctypes.POINTER(ctypes.c_int64)]),
     "emsesg_rhoupd": (_I, [_P, _I]),
+    "emsesg_compact_noalloc": (_I, [_P, ctypes.c_int64, _P, _P, _P]),
     "emsesg_energy": (_I, [_P, ctypes.POINTER(ctypes.c_double)]),
     "emsesg_fx_load": (_I, [_P]),
     "emsesg_fx_store": (_I, [_P]),
