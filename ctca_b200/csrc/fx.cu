@@ -32,8 +32,6 @@ namespace emsesg {
 namespace {
 
 constexpr uint32_t DEAD = 0xFFFFFFFFu;
-constexpr int FX_THREADS = 256;
-constexpr int GUARD = 2;
 constexpr double FIX_INV = 1.0 / 1099511627776.0;
 
 struct Geo {
@@ -214,7 +212,8 @@ int fx_alloc(emsesg_ctx* ctx) {
   if (f.pos) return EMSESG_OK;
   const emsesg_config& c = ctx->cfg;
   int n[3] = {c.nx, c.ny, c.nz};
-  for (int d = 0; d < 3; d++) f.bits[d] = ceil_log2(n[d]);
+  // room for cells -1 .. n shifted by +1 (the push queue keys)
+  for (int d = 0; d < 3; d++) f.bits[d] = ceil_log2(n[d] + 2);
   if (f.bits[0] + f.bits[1] + f.bits[2] > 31)
     return set_error(ctx, EMSESG_ERR_ARG, "grid needs more than 31 bits of packed cell index");
   for (int d = 0; d < 3; d++) {
@@ -400,9 +399,9 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
   a.diag = ctx->d_diag;
   dim3 grid((unsigned)f.ntiles, (unsigned)c.nspec);
   if (fx_box_tile(tmax) == 4)
-    EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<4>, grid, FX_THREADS, smem, a);
+    EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<4>, grid, PUSH_THREADS, smem, a);
   else
-    EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<8>, grid, FX_THREADS, smem, a);
+    EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<8>, grid, PUSH_THREADS, smem, a);
   // guard folding on the exact integers, then FP64 outputs
   if ((rc = run_slab_ops(ctx, (long long*)acc_rho, fr, fold_ops(c, 0, 1), "fx_fold_rho"))) return rc;
   if ((rc = run_slab_ops(ctx, (long long*)acc_j, fj, fold_ops(c, 1, 3), "fx_fold_j"))) return rc;

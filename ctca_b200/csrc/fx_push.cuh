@@ -1,26 +1,34 @@
 // fx_push.cuh -- the fused push + zigzag current + CIC charge kernel of the
 // FP32 / fixed-point form (included by fx.cu inside its private namespace).
 //
-// One CTA pushes the particles that the last sort placed in one cell tile of
-// one species.  The tile's particles are split into 256 contiguous slices,
-// one per thread; because they are sorted by cell, a thread meets long runs
-// of particles in the same cell.  A thread keeps the 20 deposits of a cell
-// (12 zigzag-current and 8 CIC-charge node values) in FP32 registers while
-// the cell does not change, for up to two cells at a time (the least
-// recently used one is written out first), and writes a cell's sums into the
-// CTA's int64 tile accumulator (tile + 2-cell guard, shared memory) only when
-// the cell leaves the pair.  Particles that change cell in this step add
-// their "before" half (zigzag segment 1) to the run and write the rest
-// directly.  The CTA finally adds its accumulator into the global int64
-// arrays.  Particle records move through shared memory: slices are loaded
-// and stored with coalesced accesses in chunks of RUN particles per thread.
+// One CTA (512 threads) pushes the particles that the last sort placed in
+// one cell tile of one species.  At the start it copies the tile's FP32 E/B
+// nodes (tile + 1-node guard) into shared memory, so the 8-corner gathers
+// read shared memory.  The tile's particles are split into 512 contiguous
+// slices, one per thread; because they are sorted by cell, a thread meets
+// long runs of particles in the same cell.  A thread keeps the 20 deposits of
+// a cell (12 zigzag-current and 8 CIC-charge node values) in FP32 registers
+// while the cell does not change.  When the
+// cell changes (the thread's run moves on), or a particle changes cell
+// during the step (its "after" half), the thread appends the 20 values
+// and the cell to its warp's queue in shared memory; when the queue holds 16
+// or more entries the warp empties it together, one entry per lane, adding
+// the values into the CTA's int64 tile accumulator (tile + 1-cell guard).
+// So the conversions and atomics run with all lanes busy instead of one
+// lane at a time.  The CTA finally adds its accumulator into the global
+// int64 arrays.  Particle records move through shared memory: slices are
+// loaded and stored with coalesced accesses in chunks of RUN particles.
 //
 // The tile edge T is a template parameter, so every node offset inside the
-// accumulator is an immediate: a deposit is one FP32->int64 conversion and
-// one shared-memory atomic.  Deposits whose cell lies outside the tile box
-// (rare: particles that drifted more than the guard) take a separate,
-// non-inlined path into the global arrays.
+// accumulator is an immediate.  Deposits or gathers whose cell lies outside
+// the tile box (particles that drifted more than one cell since the sort)
+// take a separate path through the global arrays.
 
+constexpr int PUSH_THREADS = 512;
+constexpr int PUSH_WARPS = PUSH_THREADS / 32;
+constexpr int PG = 1;           // guard cells around the tile
+constexpr int QCAP = 48;        // queue entries per warp
+constexpr int QW = 21;          // words per entry: 20 values + cell
 constexpr int RUN = 4;          // particles per thread per staged chunk
 constexpr int SLOT = RUN + 1;   // padded slots per thread (conflict-free reads)
 constexpr int NJ = 12;          // zigzag node values of one cell
@@ -175,75 +183,125 @@ __device__ __forceinline__ int box_base(const int (&o)[3], int i, int j, int k) 
   return ok ? (lk * B + lj) * B + li : -1;
 }
 
-// 12 zigzag values starting at v[first] (compile-time indices only).
-template <int B, int N>
-__device__ __forceinline__ void put_j(const Sink& sk, unsigned long long* box, const int (&o)[3], int i, int j, int k,
-                                      const float (&v)[N], int first_unused, float qfix) {
-  int base = box_base<B>(o, i, j, k);
-  if (base >= 0) {
+template <bool SMEM>
+__device__ __forceinline__ void gather8(const float4* f0, const void* f1v, int64_t n5, int64_t sy, int64_t sz,
+                                        const float (&w)[8], float (&e)[3], float (&b)[3]) {
+  const int64_t idx[8] = {n5 + sz, n5 + sz + 1, n5 + sz + 1 + sy, n5 + sz + sy, n5, n5 + 1, n5 + 1 + sy, n5 + sy};
+  float ex = 0.f, ey = 0.f, ez = 0.f, bx = 0.f, by = 0.f, bz = 0.f;
 #pragma unroll
-    for (int q = 0; q < NJ; q++)
-      atomicAdd(&box[base + BoxT<B>::joff(q)], (unsigned long long)to_fix(v[q], qfix));
-  } else {
-    V12 w;
-#pragma unroll
-    for (int q = 0; q < NJ; q++) w.v[q] = v[q];
-    put_j_global(sk, i, j, k, w, qfix);
+  for (int c = 0; c < 8; c++) {
+    float4 p;
+    float2 q;
+    if (SMEM) {
+      p = f0[idx[c]];
+      q = reinterpret_cast<const float2*>(f1v)[idx[c]];
+    } else {
+      p = __ldg(&f0[idx[c]]);
+      float4 q4 = __ldg(&reinterpret_cast<const float4*>(f1v)[idx[c]]);
+      q = make_float2(q4.x, q4.y);
+    }
+    ex += p.x * w[c];
+    ey += p.y * w[c];
+    ez += p.z * w[c];
+    bx += p.w * w[c];
+    by += q.x * w[c];
+    bz += q.y * w[c];
   }
+  e[0] = ex; e[1] = ey; e[2] = ez;
+  b[0] = bx; b[1] = by; b[2] = bz;
 }
 
-// 8 charge values at v[OFF .. OFF+7].
-template <int B, int OFF, int N>
-__device__ __forceinline__ void put_r(const Sink& sk, unsigned long long* box, const int (&o)[3], int i, int j, int k,
-                                      const float (&v)[N], float qfix) {
-  int base = box_base<B>(o, i, j, k);
-  if (base >= 0) {
-#pragma unroll
-    for (int r = 0; r < NR; r++)
-      atomicAdd(&box[base + BoxT<B>::roff(r)], (unsigned long long)to_fix(v[OFF + r], qfix));
-  } else {
-    V8 w;
-#pragma unroll
-    for (int r = 0; r < NR; r++) w.v[r] = v[OFF + r];
-    put_r_global(sk, i, j, k, w, qfix);
-  }
+// A queued bundle whose cell lies outside the tile box (rare).
+__device__ __noinline__ void put_bundle_global(Sink sk, int i, int j, int k, const float* en, float qfix) {
+  V12 wj;
+  V8 wr;
+  for (int s = 0; s < NJ; s++) wj.v[s] = en[s];
+  for (int r = 0; r < NR; r++) wr.v[r] = en[NJ + r];
+  put_j_global(sk, i, j, k, wj, qfix);
+  put_r_global(sk, i, j, k, wr, qfix);
 }
 
-// Writes the 20 register sums of one cell (key) and clears them.
+// Empties a warp queue: lane l takes entries l, l+32, ...  Each lane walks
+// its entry's 20 slots starting at slot (lane mod 20), so lanes holding
+// entries of the same cell add to different nodes at the same time.
 template <int B>
-__device__ __forceinline__ void flush_cell(const Sink& sk, const Geo& g, unsigned long long* box, const int (&o)[3],
-                                           uint32_t key, float (&acc)[NJ + NR], float qfix) {
-  if (key == DEAD) return;
-  int i, j, k;
-  unpack(g, key, i, j, k);
-  put_j<B, NJ + NR>(sk, box, o, i, j, k, acc, 0, qfix);
-  put_r<B, NJ, NJ + NR>(sk, box, o, i, j, k, acc, qfix);
-#pragma unroll
-  for (int q = 0; q < NJ + NR; q++) acc[q] = 0.f;
+__device__ __forceinline__ void drain_queue(const Sink& sk, const Geo& g, unsigned long long* box, const int (&o)[3],
+                                            const int* slot_off, float* q, int qn, float qfix, int lane) {
+  __syncwarp();
+  const int rot = lane % (NJ + NR);
+  for (int p = 0; p < qn; p += 32) {
+    int e = p + lane;
+    if (e < qn) {
+      const float* en = q + e * QW;
+      uint32_t key = (uint32_t)__float_as_int(en[NJ + NR]);
+      int i, j, k;
+      unpack(g, key, i, j, k);
+      i -= 1; j -= 1; k -= 1;  // keys hold cells shifted by +1 (qkey)
+      int base = box_base<B>(o, i, j, k);
+      if (base >= 0) {
+#pragma unroll 4
+        for (int s = 0; s < NJ + NR; s++) {
+          int slot = s + rot;
+          slot -= slot >= NJ + NR ? NJ + NR : 0;
+          long long v = to_fix(en[slot], qfix);
+          if (v) atomicAdd(&box[base + slot_off[slot]], (unsigned long long)v);
+        }
+      } else {
+        put_bundle_global(sk, i, j, k, en, qfix);
+      }
+    }
+  }
+  __syncwarp();
 }
+
+// Cell key of an "after" bundle: cells may be -1 or n on an axis (the
+// reference's guard indices), so the queue stores the cell shifted by +1.
+__device__ __forceinline__ uint32_t qkey(const Geo& g, int i, int j, int k) { return pack(g, i + 1, j + 1, k + 1); }
 
 template <int T>
-__global__ void __launch_bounds__(FX_THREADS, 2) k_fx_push(FxPushArgs a) {
-  constexpr int B = T + 2 * GUARD + 1;
+__global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_push(FxPushArgs a) {
+  constexpr int B = T + 2 * PG + 1;  // box and field tile edge (nodes)
   constexpr int NBOX = 4 * B * B * B;
+  constexpr int NF = B * B * B;
   extern __shared__ unsigned long long smem[];
+  __shared__ int slot_off[NJ + NR];
   const Geo& g = a.g;
   const int is = blockIdx.y;
   const int t = blockIdx.x;
   const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const unsigned lt = (1u << lane) - 1u;
   int tx = t % g.nt[0], ty = (t / g.nt[0]) % g.nt[1], tz = t / (g.nt[0] * g.nt[1]);
   // T bounds every tile edge; the box may be larger than a thin tile needs
-  const int o[3] = {tx * g.t[0] - GUARD, ty * g.t[1] - GUARD, tz * g.t[2] - GUARD};
+  const int o[3] = {tx * g.t[0] - PG, ty * g.t[1] - PG, tz * g.t[2] - PG};
   unsigned long long* box = smem;
-  float4* spos = reinterpret_cast<float4*>(smem + NBOX);
-  float* svx = reinterpret_cast<float*>(spos + FX_THREADS * SLOT);
-  float* svy = svx + FX_THREADS * SLOT;
-  float* svz = svy + FX_THREADS * SLOT;
+  float4* sf0 = reinterpret_cast<float4*>(smem + NBOX);
+  float4* spos = sf0 + NF;
+  float2* sf1 = reinterpret_cast<float2*>(spos + PUSH_THREADS * SLOT);
+  float* svx = reinterpret_cast<float*>(sf1 + NF);
+  float* svy = svx + PUSH_THREADS * SLOT;
+  float* svz = svy + PUSH_THREADS * SLOT;
+  float* queue = svz + PUSH_THREADS * SLOT + warp * QCAP * QW;
 
   const int64_t* ts = a.tile_start + (int64_t)is * (a.ntiles + 1);
   const int64_t p0 = ts[t], n = ts[t + 1] - p0;
   if (n <= 0) return;
-  for (int e = tid; e < NBOX; e += FX_THREADS) box[e] = 0ull;
+  const int64_t sy = g.nx + 1, sz = (int64_t)(g.nx + 1) * (g.ny + 1);
+  if (tid < NJ + NR) slot_off[tid] = tid < NJ ? BoxT<B>::joff(tid) : BoxT<B>::roff(tid - NJ);
+  for (int e = tid; e < NBOX; e += PUSH_THREADS) box[e] = 0ull;
+  // field tile: nodes o .. o+B-1 (those inside 0..n)
+  for (int e = tid; e < NF; e += PUSH_THREADS) {
+    int li = e % B, lj = (e / B) % B, lk = e / (B * B);
+    int gi = o[0] + li, gj = o[1] + lj, gk = o[2] + lk;
+    float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p;
+    if (gi >= 0 && gj >= 0 && gk >= 0 && gi <= g.nx && gj <= g.ny && gk <= g.nz) {
+      int64_t gn = gi + sy * gj + sz * gk;
+      p = __ldg(&a.f0[gn]);
+      q = __ldg(&a.f1[gn]);
+    }
+    sf0[e] = p;
+    sf1[e] = make_float2(q.x, q.y);
+  }
 
   const int64_t off = a.off[is];
   float4* gpos = a.pos + off;
@@ -252,28 +310,27 @@ __global__ void __launch_bounds__(FX_THREADS, 2) k_fx_push(FxPushArgs a) {
   float* gvz = a.vz + off;
   const float qmp = a.qmp[is], qfix = a.qfix[is];
   const int nb0 = a.npbnd[is][0], nb1 = a.npbnd[is][1], nb2 = a.npbnd[is][2];
+  const Sink sk{a.acc_rho, a.acc_j, a.fr, a.fj, g.nx, g.ny, g.nz, a.status, a.diag};
   // thread slices of the tile's particles
-  const int64_t s0 = p0 + ((n * tid) >> 8);
-  const int64_t s1 = p0 + ((n * (tid + 1)) >> 8);
-  const int64_t maxlen = (n + FX_THREADS - 1) >> 8;
+  const int64_t s0 = p0 + (n * tid) / PUSH_THREADS;
+  const int64_t s1 = p0 + (n * (tid + 1)) / PUSH_THREADS;
+  const int64_t maxlen = (n + PUSH_THREADS - 1) / PUSH_THREADS;
   const int chunks = (int)((maxlen + RUN - 1) / RUN);
 
-  const Sink sk{a.acc_rho, a.acc_j, a.fr, a.fj, g.nx, g.ny, g.nz, a.status, a.diag};
-  float accA[NJ + NR], accB[NJ + NR];
+  float acc[NJ + NR];
 #pragma unroll
-  for (int s = 0; s < NJ + NR; s++) { accA[s] = 0.f; accB[s] = 0.f; }
-  uint32_t keyA = DEAD, keyB = DEAD;
-  bool lastA = true;
+  for (int s = 0; s < NJ + NR; s++) acc[s] = 0.f;
+  uint32_t acckey = DEAD;
   int nesc = 0;
-  const int64_t sy = g.nx + 1, sz = (int64_t)(g.nx + 1) * (g.ny + 1);
+  int qn = 0;  // warp-uniform queue length
 
   for (int c = 0; c < chunks; c++) {
-    __syncthreads();  // staging buffers free (and box zeroed, on the first pass)
+    __syncthreads();  // staging free; box and field tile ready on the first pass
 #pragma unroll
     for (int r = 0; r < RUN; r++) {
-      int e = tid + r * FX_THREADS;
+      int e = tid + r * PUSH_THREADS;
       int ow = e / RUN, j = e % RUN;
-      int64_t so = p0 + ((n * ow) >> 8), se = p0 + ((n * (ow + 1)) >> 8);
+      int64_t so = p0 + (n * ow) / PUSH_THREADS, se = p0 + (n * (ow + 1)) / PUSH_THREADS;
       int64_t m = so + (int64_t)c * RUN + j;
       if (m < se) {
         spos[ow * SLOT + j] = gpos[m];
@@ -286,126 +343,159 @@ __global__ void __launch_bounds__(FX_THREADS, 2) k_fx_push(FxPushArgs a) {
 #pragma unroll 1
     for (int j = 0; j < RUN; j++) {
       int64_t m = s0 + (int64_t)c * RUN + j;
-      if (m >= s1) break;
-      float4 ps = spos[tid * SLOT + j];
-      uint32_t cell = (uint32_t)__float_as_int(ps.w);
-      if (cell == DEAD) continue;
-      int ib, jb, kb;
-      unpack(g, cell, ib, jb, kb);
-      if (ib >= g.nx || jb >= g.ny || kb >= g.nz) {
-        report_bad(a.status, a.diag, SITE_FX_PUSH, m, (long long)cell);
-        continue;
+      bool act = m < s1;
+      float4 ps = act ? spos[tid * SLOT + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      uint32_t cell = act ? (uint32_t)__float_as_int(ps.w) : DEAD;
+      act = act && cell != DEAD;
+      int ib = 0, jb = 0, kb = 0;
+      if (act) {
+        unpack(g, cell, ib, jb, kb);
+        if (ib >= g.nx || jb >= g.ny || kb >= g.nz) {
+          report_bad(a.status, a.diag, SITE_FX_PUSH, m, (long long)cell);
+          act = false;
+        }
       }
-      float vx = svx[tid * SLOT + j], vy = svy[tid * SLOT + j], vz = svz[tid * SLOT + j];
-      // trilinear weights (psolve1.F90:186-199)
-      float x1 = ps.x, y1 = ps.y, z1 = ps.z;
-      float xy1 = x1 * y1, xz1 = x1 * z1, yz1 = y1 * z1, z2 = 1.0f - z1;
-      float xz2 = x1 * z2, yz2 = y1 * z2;
-      float v3 = xy1 * z1, v2 = xz1 - v3, v4 = yz1 - v3, v1 = z1 - xz1 - v4;
-      float v7 = xy1 * z2, v6 = xz2 - v7, v8 = yz2 - v7, v5 = z2 - xz2 - v8;
-      int64_t n5 = ib + sy * jb + sz * kb, n1 = n5 + sz;
-      float4 a1 = __ldg(&a.f0[n1]), a2 = __ldg(&a.f0[n1 + 1]), a3 = __ldg(&a.f0[n1 + 1 + sy]), a4 = __ldg(&a.f0[n1 + sy]);
-      float4 a5 = __ldg(&a.f0[n5]), a6 = __ldg(&a.f0[n5 + 1]), a7 = __ldg(&a.f0[n5 + 1 + sy]), a8 = __ldg(&a.f0[n5 + sy]);
-      float4 b1 = __ldg(&a.f1[n1]), b2 = __ldg(&a.f1[n1 + 1]), b3 = __ldg(&a.f1[n1 + 1 + sy]), b4 = __ldg(&a.f1[n1 + sy]);
-      float4 b5 = __ldg(&a.f1[n5]), b6 = __ldg(&a.f1[n5 + 1]), b7 = __ldg(&a.f1[n5 + 1 + sy]), b8 = __ldg(&a.f1[n5 + sy]);
-      float eex = a1.x * v1 + a2.x * v2 + a3.x * v3 + a4.x * v4 + a5.x * v5 + a6.x * v6 + a7.x * v7 + a8.x * v8;
-      float eey = a1.y * v1 + a2.y * v2 + a3.y * v3 + a4.y * v4 + a5.y * v5 + a6.y * v6 + a7.y * v7 + a8.y * v8;
-      float eez = a1.z * v1 + a2.z * v2 + a3.z * v3 + a4.z * v4 + a5.z * v5 + a6.z * v6 + a7.z * v7 + a8.z * v8;
-      float bbx = a1.w * v1 + a2.w * v2 + a3.w * v3 + a4.w * v4 + a5.w * v5 + a6.w * v6 + a7.w * v7 + a8.w * v8;
-      float bby = b1.x * v1 + b2.x * v2 + b3.x * v3 + b4.x * v4 + b5.x * v5 + b6.x * v6 + b7.x * v7 + b8.x * v8;
-      float bbz = b1.y * v1 + b2.y * v2 + b3.y * v3 + b4.y * v4 + b5.y * v5 + b6.y * v6 + b7.y * v7 + b8.y * v8;
-      // Buneman-Boris (psolve1.F90:247-272)
-      eex *= qmp; eey *= qmp; eez *= qmp;
-      bbx *= qmp; bby *= qmp; bbz *= qmp;
-      float boris = 2.0f / (1.0f + bbx * bbx + bby * bby + bbz * bbz);
-      vx += eex; vy += eey; vz += eez;
-      float vxt = vx + vy * bbz - vz * bby;
-      float vyt = vy + vz * bbx - vx * bbz;
-      float vzt = vz + vx * bby - vy * bbx;
-      vx += boris * (vyt * bbz - vzt * bby);
-      vy += boris * (vzt * bbx - vxt * bbz);
-      vz += boris * (vxt * bby - vyt * bbx);
-      vx += eex; vy += eey; vz += eez;
-      Axis ax = axis_move(ib, ps.x, vx * a.gustep, g.nx, nb0);
-      Axis ay = axis_move(jb, ps.y, vy * a.gustep, g.ny, nb1);
-      Axis az = axis_move(kb, ps.z, vz * a.gustep, g.nz, nb2);
-      if (ax.flip) vx = -vx;
-      if (ay.flip) vy = -vy;
-      if (az.flip) vz = -vz;
-      bool dead = ax.dead || ay.dead || az.dead;
-      // zigzag (psolve1.F90:717-757), integer parts first
-      float xd1 = ((float)(ax.rc - ib) + ax.rf + ps.x) * 0.5f;
-      float yd1 = ((float)(ay.rc - jb) + ay.rf + ps.y) * 0.5f;
-      float zd1 = ((float)(az.rc - kb) + az.rf + ps.z) * 0.5f;
-      float vvx1 = ((float)(ax.rc - ib) + (ax.rf - ps.x)) * a.rustep;
-      float vvy1 = ((float)(ay.rc - jb) + (ay.rf - ps.y)) * a.rustep;
-      float vvz1 = ((float)(az.rc - kb) + (az.rf - ps.z)) * a.rustep;
-      float xd2 = ((float)(ax.ac - ax.ia) + ax.af + (float)(ax.rc - ax.ia) + ax.rf) * 0.5f;
-      float yd2 = ((float)(ay.ac - ay.ia) + ay.af + (float)(ay.rc - ay.ia) + ay.rf) * 0.5f;
-      float zd2 = ((float)(az.ac - az.ia) + az.af + (float)(az.rc - az.ia) + az.rf) * 0.5f;
-      float vvx2 = ((float)(ax.ac - ax.rc) + (ax.af - ax.rf)) * a.rustep;
-      float vvy2 = ((float)(ay.ac - ay.rc) + (ay.af - ay.rf)) * a.rustep;
-      float vvz2 = ((float)(az.ac - az.rc) + (az.af - az.rf)) * a.rustep;
-      float J1[NJ], J2[NJ], R[NR];
-      float w;
-      w = yd1 * zd1; J1[3] = vvx1 * w; J1[1] = vvx1 * (yd1 - w); J1[2] = vvx1 * (zd1 - w); J1[0] = vvx1 * (1.0f - yd1 - (zd1 - w));
-      w = xd1 * zd1; J1[7] = vvy1 * w; J1[5] = vvy1 * (xd1 - w); J1[6] = vvy1 * (zd1 - w); J1[4] = vvy1 * (1.0f - xd1 - (zd1 - w));
-      w = xd1 * yd1; J1[11] = vvz1 * w; J1[9] = vvz1 * (xd1 - w); J1[10] = vvz1 * (yd1 - w); J1[8] = vvz1 * (1.0f - xd1 - (yd1 - w));
-      w = yd2 * zd2; J2[3] = vvx2 * w; J2[1] = vvx2 * (yd2 - w); J2[2] = vvx2 * (zd2 - w); J2[0] = vvx2 * (1.0f - yd2 - (zd2 - w));
-      w = xd2 * zd2; J2[7] = vvy2 * w; J2[5] = vvy2 * (xd2 - w); J2[6] = vvy2 * (zd2 - w); J2[4] = vvy2 * (1.0f - xd2 - (zd2 - w));
-      w = xd2 * yd2; J2[11] = vvz2 * w; J2[9] = vvz2 * (xd2 - w); J2[10] = vvz2 * (yd2 - w); J2[8] = vvz2 * (1.0f - xd2 - (yd2 - w));
+      // ---- the register run follows cell_b; a new cell sends the old sums
+      // through the warp queue
+      uint32_t key = qkey(g, ib, jb, kb);
       {
+        bool evict = act && key != acckey && acckey != DEAD;
+        unsigned mk = __ballot_sync(0xffffffffu, evict);
+        if (mk) {
+          if (evict) {
+            float* en = queue + (qn + __popc(mk & lt)) * QW;
+#pragma unroll
+            for (int s = 0; s < NJ + NR; s++) en[s] = acc[s];
+            en[NJ + NR] = __int_as_float((int)acckey);
+          }
+          qn += __popc(mk);
+          if (qn >= 16) {
+            drain_queue<B>(sk, g, box, o, slot_off, queue, qn, qfix, lane);
+            qn = 0;
+          }
+        }
+      }
+      if (act && key != acckey) {
+#pragma unroll
+        for (int s = 0; s < NJ + NR; s++) acc[s] = 0.f;
+        acckey = key;
+      }
+
+      // ---- push
+      Axis ax{}, ay{}, az{};
+      bool simple = true, dead = false;
+      float xd2 = 0.f, yd2 = 0.f, zd2 = 0.f, vvx2 = 0.f, vvy2 = 0.f, vvz2 = 0.f;
+      if (act) {
+        float vx = svx[tid * SLOT + j], vy = svy[tid * SLOT + j], vz = svz[tid * SLOT + j];
+        // trilinear weights (psolve1.F90:186-199)
+        float x1 = ps.x, y1 = ps.y, z1 = ps.z;
+        float xy1 = x1 * y1, xz1 = x1 * z1, yz1 = y1 * z1, z2 = 1.0f - z1;
+        float xz2 = x1 * z2, yz2 = y1 * z2;
+        float wv[8];
+        wv[2] = xy1 * z1; wv[1] = xz1 - wv[2]; wv[3] = yz1 - wv[2]; wv[0] = z1 - xz1 - wv[3];
+        wv[6] = xy1 * z2; wv[5] = xz2 - wv[6]; wv[7] = yz2 - wv[6]; wv[4] = z2 - xz2 - wv[7];
+        float eb_e[3], eb_b[3];
+        int li = ib - o[0], lj = jb - o[1], lk = kb - o[2];
+        if ((unsigned)li < (unsigned)(B - 1) && (unsigned)lj < (unsigned)(B - 1) && (unsigned)lk < (unsigned)(B - 1))
+          gather8<true>(sf0, sf1, li + B * lj + (int64_t)B * B * lk, B, (int64_t)B * B, wv, eb_e, eb_b);
+        else
+          gather8<false>(a.f0, a.f1, ib + sy * jb + sz * kb, sy, sz, wv, eb_e, eb_b);
+        // Buneman-Boris (psolve1.F90:247-272)
+        float eex = eb_e[0] * qmp, eey = eb_e[1] * qmp, eez = eb_e[2] * qmp;
+        float bbx = eb_b[0] * qmp, bby = eb_b[1] * qmp, bbz = eb_b[2] * qmp;
+        float boris = 2.0f / (1.0f + bbx * bbx + bby * bby + bbz * bbz);
+        vx += eex; vy += eey; vz += eez;
+        float vxt = vx + vy * bbz - vz * bby;
+        float vyt = vy + vz * bbx - vx * bbz;
+        float vzt = vz + vx * bby - vy * bbx;
+        vx += boris * (vyt * bbz - vzt * bby);
+        vy += boris * (vzt * bbx - vxt * bbz);
+        vz += boris * (vxt * bby - vyt * bbx);
+        vx += eex; vy += eey; vz += eez;
+        ax = axis_move(ib, ps.x, vx * a.gustep, g.nx, nb0);
+        ay = axis_move(jb, ps.y, vy * a.gustep, g.ny, nb1);
+        az = axis_move(kb, ps.z, vz * a.gustep, g.nz, nb2);
+        if (ax.flip) vx = -vx;
+        if (ay.flip) vy = -vy;
+        if (az.flip) vz = -vz;
+        dead = ax.dead || ay.dead || az.dead;
+        if (dead) nesc++;
+        uint32_t nc = dead ? DEAD : pack(g, ax.nc, ay.nc, az.nc);
+        spos[tid * SLOT + j] = make_float4(ax.nf, ay.nf, az.nf, __int_as_float((int)nc));
+        svx[tid * SLOT + j] = vx;
+        svy[tid * SLOT + j] = vy;
+        svz[tid * SLOT + j] = vz;
+        // zigzag (psolve1.F90:717-757), integer parts first; segment 1 goes
+        // to the run of cell_b
+        float xd1 = ((float)(ax.rc - ib) + ax.rf + ps.x) * 0.5f;
+        float yd1 = ((float)(ay.rc - jb) + ay.rf + ps.y) * 0.5f;
+        float zd1 = ((float)(az.rc - kb) + az.rf + ps.z) * 0.5f;
+        float vvx1 = ((float)(ax.rc - ib) + (ax.rf - ps.x)) * a.rustep;
+        float vvy1 = ((float)(ay.rc - jb) + (ay.rf - ps.y)) * a.rustep;
+        float vvz1 = ((float)(az.rc - kb) + (az.rf - ps.z)) * a.rustep;
+        float w;
+        w = yd1 * zd1; acc[3] += vvx1 * w; acc[1] += vvx1 * (yd1 - w); acc[2] += vvx1 * (zd1 - w); acc[0] += vvx1 * (1.0f - yd1 - (zd1 - w));
+        w = xd1 * zd1; acc[7] += vvy1 * w; acc[5] += vvy1 * (xd1 - w); acc[6] += vvy1 * (zd1 - w); acc[4] += vvy1 * (1.0f - xd1 - (zd1 - w));
+        w = xd1 * yd1; acc[11] += vvz1 * w; acc[9] += vvz1 * (xd1 - w); acc[10] += vvz1 * (yd1 - w); acc[8] += vvz1 * (1.0f - xd1 - (yd1 - w));
+        xd2 = ((float)(ax.ac - ax.ia) + ax.af + (float)(ax.rc - ax.ia) + ax.rf) * 0.5f;
+        yd2 = ((float)(ay.ac - ay.ia) + ay.af + (float)(ay.rc - ay.ia) + ay.rf) * 0.5f;
+        zd2 = ((float)(az.ac - az.ia) + az.af + (float)(az.rc - az.ia) + az.rf) * 0.5f;
+        vvx2 = ((float)(ax.ac - ax.rc) + (ax.af - ax.rf)) * a.rustep;
+        vvy2 = ((float)(ay.ac - ay.rc) + (ay.af - ay.rf)) * a.rustep;
+        vvz2 = ((float)(az.ac - az.rc) + (az.af - az.rf)) * a.rustep;
+        simple = !ax.crossed && !ay.crossed && !az.crossed && ax.ia == ib && ay.ia == jb && az.ia == kb;
+      }
+      // ---- segment 2 and the charge: into the run when the cell did not
+      // change, else through the warp queue
+      bool cross = act && !simple;
+      unsigned mk = __ballot_sync(0xffffffffu, cross);
+      float* en = cross ? queue + (qn + __popc(mk & lt)) * QW : nullptr;
+      if (act) {
+        float J2[NJ], R[NR];
+        float w;
+        w = yd2 * zd2; J2[3] = vvx2 * w; J2[1] = vvx2 * (yd2 - w); J2[2] = vvx2 * (zd2 - w); J2[0] = vvx2 * (1.0f - yd2 - (zd2 - w));
+        w = xd2 * zd2; J2[7] = vvy2 * w; J2[5] = vvy2 * (xd2 - w); J2[6] = vvy2 * (zd2 - w); J2[4] = vvy2 * (1.0f - xd2 - (zd2 - w));
+        w = xd2 * yd2; J2[11] = vvz2 * w; J2[9] = vvz2 * (xd2 - w); J2[10] = vvz2 * (yd2 - w); J2[8] = vvz2 * (1.0f - xd2 - (yd2 - w));
         float X = ax.nf, Y = ay.nf, Z = az.nf;
         float XY = X * Y, XZ = X * Z, YZ = Y * Z, Z2 = 1.0f - Z, XZ2 = X * Z2, YZ2 = Y * Z2;
         R[2] = XY * Z; R[1] = XZ - R[2]; R[3] = YZ - R[2]; R[0] = Z - XZ - R[3];
         R[6] = XY * Z2; R[5] = XZ2 - R[6]; R[7] = YZ2 - R[6]; R[4] = Z2 - XZ2 - R[7];
-      }
-      if (dead) nesc++;
-      uint32_t nc = dead ? DEAD : pack(g, ax.nc, ay.nc, az.nc);
-      spos[tid * SLOT + j] = make_float4(ax.nf, ay.nf, az.nf, __int_as_float((int)nc));
-      svx[tid * SLOT + j] = vx;
-      svy[tid * SLOT + j] = vy;
-      svz[tid * SLOT + j] = vz;
-
-      // ---- deposit: segment 1 (and, without a cell change, everything)
-      // goes to the register run of cell_b
-      bool simple = !ax.crossed && !ay.crossed && !az.crossed && ax.ia == ib && ay.ia == jb && az.ia == kb;
-      bool useA;
-      if (cell == keyA) useA = true;
-      else if (cell == keyB) useA = false;
-      else if (lastA) {  // evict B
-        flush_cell<B>(sk, g, box, o, keyB, accB, qfix);
-        keyB = cell;
-        useA = false;
-      } else {
-        flush_cell<B>(sk, g, box, o, keyA, accA, qfix);
-        keyA = cell;
-        useA = true;
-      }
-      lastA = useA;
-      float sm = simple ? 1.0f : 0.0f;
+        if (simple) {
 #pragma unroll
-      for (int s = 0; s < NJ; s++) {
-        float v = fmaf(sm, J2[s], J1[s]);
-        if (useA) accA[s] += v; else accB[s] += v;
-      }
+          for (int s = 0; s < NJ; s++) acc[s] += J2[s];
 #pragma unroll
-      for (int r = 0; r < NR; r++) {
-        float v = sm * R[r];
-        if (useA) accA[NJ + r] += v; else accB[NJ + r] += v;
+          for (int r = 0; r < NR; r++) acc[NJ + r] += R[r];
+        } else {
+          // the stored cell differs from the after cell only at an outer
+          // boundary (wrap or reflection): that charge goes out directly
+          bool rsplit = dead || ax.nc != ax.ia || ay.nc != ay.ia || az.nc != az.ia;
+          if (rsplit && !dead) {
+            V8 wr;
+#pragma unroll
+            for (int r = 0; r < NR; r++) wr.v[r] = R[r];
+            put_r_global(sk, ax.nc, ay.nc, az.nc, wr, qfix);
+          }
+#pragma unroll
+          for (int s = 0; s < NJ; s++) en[s] = J2[s];
+#pragma unroll
+          for (int r = 0; r < NR; r++) en[NJ + r] = rsplit ? 0.f : R[r];
+          en[NJ + NR] = __int_as_float((int)qkey(g, ax.ia, ay.ia, az.ia));
+        }
       }
-      if (!simple) {
-        // segment 2 at the after cell, charge at the stored position
-        put_j<B, NJ>(sk, box, o, ax.ia, ay.ia, az.ia, J2, 0, qfix);
-        if (!dead) put_r<B, 0, NR>(sk, box, o, ax.nc, ay.nc, az.nc, R, qfix);
+      if (mk) {
+        qn += __popc(mk);
+        if (qn >= 16) {
+          drain_queue<B>(sk, g, box, o, slot_off, queue, qn, qfix, lane);
+          qn = 0;
+        }
       }
     }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < RUN; r++) {
-      int e = tid + r * FX_THREADS;
+      int e = tid + r * PUSH_THREADS;
       int ow = e / RUN, j = e % RUN;
-      int64_t so = p0 + ((n * ow) >> 8), se = p0 + ((n * (ow + 1)) >> 8);
+      int64_t so = p0 + (n * ow) / PUSH_THREADS, se = p0 + (n * (ow + 1)) / PUSH_THREADS;
       int64_t m = so + (int64_t)c * RUN + j;
       if (m < se) {
         gpos[m] = spos[ow * SLOT + j];
@@ -415,12 +505,23 @@ __global__ void __launch_bounds__(FX_THREADS, 2) k_fx_push(FxPushArgs a) {
       }
     }
   }
-  flush_cell<B>(sk, g, box, o, keyA, accA, qfix);
-  flush_cell<B>(sk, g, box, o, keyB, accB, qfix);
+  // the last run of every thread
+  {
+    bool has = acckey != DEAD;
+    unsigned mk = __ballot_sync(0xffffffffu, has);
+    if (has) {
+      float* en = queue + (qn + __popc(mk & lt)) * QW;
+#pragma unroll
+      for (int s = 0; s < NJ + NR; s++) en[s] = acc[s];
+      en[NJ + NR] = __int_as_float((int)acckey);
+    }
+    qn += __popc(mk);
+    if (qn) drain_queue<B>(sk, g, box, o, slot_off, queue, qn, qfix, lane);
+  }
   if (nesc) atomicAdd(&a.nesc[is], nesc);
   __syncthreads();
   // add the tile accumulator into the global int64 arrays
-  for (int e = tid; e < NBOX; e += FX_THREADS) {
+  for (int e = tid; e < NBOX; e += PUSH_THREADS) {
     unsigned long long v = box[e];
     if (v == 0ull) continue;
     int li = e % B, lj = (e / B) % B, lk = (e / (B * B)) % B, comp = e / (B * B * B);
@@ -445,10 +546,8 @@ __global__ void __launch_bounds__(FX_THREADS, 2) k_fx_push(FxPushArgs a) {
 inline int fx_box_tile(int tmax) { return tmax <= 4 ? 4 : 8; }
 
 inline int fx_push_smem(int tmax) {
-  int B = fx_box_tile(tmax) + 2 * GUARD + 1;
-  return 4 * B * B * B * (int)sizeof(unsigned long long) + FX_THREADS * SLOT * (int)(sizeof(float4) + 3 * sizeof(float));
-}
-
-inline const void* fx_push_kernel(int tmax) {
-  return fx_box_tile(tmax) == 4 ? (const void*)k_fx_push<4> : (const void*)k_fx_push<8>;
+  int B = fx_box_tile(tmax) + 2 * PG + 1;
+  int nf = B * B * B;
+  return 4 * nf * (int)sizeof(unsigned long long) + nf * (int)(sizeof(float4) + sizeof(float2)) +
+         PUSH_THREADS * SLOT * (int)(sizeof(float4) + 3 * sizeof(float)) + PUSH_WARPS * QCAP * QW * (int)sizeof(float);
 }
