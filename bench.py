@@ -18,6 +18,9 @@ J.  `fp64_dropin` reports the plain FP64 drop-in (64-byte records) on the
 same workload.  With --gpus N every rank runs its own replica (the path has
 no data exchange on one rank: weak scaling, replicas only).
 
+--cells N [--ppc P] shrinks the grid (and particles per cell) for profiler
+captures; the headline line is the default 128^3 x 64 workload.
+
 --impl reference times the reference's CPU path (the oracle restatement of
 psolve1 + charge; the Fortran reference cannot be built here) on the host
 cores, on a bounded sample of the same workload.
@@ -190,6 +193,13 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(local)
     select_device(local)
     case = inputs.baseline_case(2)
+    if args.cells:
+        # smaller copy of the workload for profiler captures (not the headline)
+        n = args.cells
+        case.n = (n, n, n)
+        case.kmax = 4 * 2 * math.pi / n
+        for sp in case.species:
+            sp.ppc = args.ppc or sp.ppc
     cfg = inputs.make_config(case)
     eb = inputs.make_fields(case)
     npart = sum(cfg.capacity[i] for i in range(cfg.nspec))
@@ -283,9 +293,10 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_time * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+i64", "data": "synthetic",
-        "config": {"workload": "128^3 periodic, 2 species x 64 ppc (268,435,456 particles), mass ratio 1836, "
-                               "sort every 4; FP32 cell+offset particles, int64 rho/J at 2^40",
-                   "l2": "inputs larger than L2 (7.5 GB particle state)", "parallelism": f"replicas x{world}"},
+        "config": {"workload": f"{case.n[0]}^3 periodic, 2 species x {case.species[0].ppc} ppc ({npart:,} particles), "
+                               "mass ratio 1836, sort every 4; FP32 cell+offset particles, int64 rho/J at 2^40",
+                   "l2": f"inputs larger than L2 ({npart * 28 / 1e9:.2f} GB particle state)",
+                   "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                      "kernel": "fx_push", "peak_kind": peak_kind,
@@ -319,6 +330,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cells", type=int, default=0, help="grid side of a smaller profiling case (default 128)")
+    ap.add_argument("--ppc", type=int, default=0, help="particles per cell per species with --cells")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
