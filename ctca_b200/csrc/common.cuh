@@ -66,8 +66,23 @@ struct FxState {
   float* vx2 = nullptr;
   float* vy2 = nullptr;
   float* vz2 = nullptr;
-  int64_t* count_d = nullptr;       // device particle counts per species
-  int64_t* tile_start = nullptr;    // [nspec][ntiles+1] offsets within the species region
+  int64_t* count_d = nullptr;       // device live-particle counts per species (last sort)
+  int64_t* slots_d = nullptr;       // device slot counts per species (padded regions)
+  int64_t* tile_start = nullptr;    // [nspec][ntiles+1] sorted ranks of each tile's first particle
+  int64_t* tile_pad = nullptr;      // [nspec][ntiles+1] first slot of each tile's padded region
+  int64_t base[EMSESG_ISPEC] = {};  // species region offsets in pos / vx / vy / vz
+  int64_t cap[EMSESG_ISPEC] = {};   // species region sizes (capacity + tile padding)
+  bool tiled = false;               // regions hold the thread-major layout of a sort
+  // tile-local counting sort (fx_sort.cuh): per species
+  int64_t* tile_start2 = nullptr;   // the new tile_start / tile_pad, swapped in after
+  int64_t* tile_pad2 = nullptr;
+  uint32_t* lcs_cnt = nullptr;      // [nspec][ntiles][nbc]
+  uint32_t* lcs_base = nullptr;     // [nspec][ntiles][nbc]
+  uint16_t* lcs_wcnt = nullptr;     // [nspec][ntiles][warps][nbc]
+  uint32_t* lcs_celltot = nullptr;  // [ntiles][tile cells]
+  int64_t* lcs_tiletot = nullptr;   // [ntiles]
+  int* lcs_stray = nullptr;         // [nspec]
+  uint32_t* lcs_inv = nullptr;      // per slot: the old slot of its particle
   int64_t* accum = nullptr;         // int64 (rho, jx, jy, jz) on the rho layout
   float4* fnode = nullptr;          // node field {ex, ey, ez, bx} over (n+1)^3 nodes
   float4* fnode2 = nullptr;         // {by, bz, 0, 0}
@@ -121,7 +136,7 @@ enum { ST_OK = 0, ST_BAD_INDEX = 1, ST_RANDOMS = 2, ST_OVERFLOW = 4 };
 
 // Sites that report ST_BAD_INDEX; the first report also leaves
 // {site, particle index, packed or truncated cell, 0} in the diag record.
-enum { SITE_PSOLVE2 = 1, SITE_PSOLVE1, SITE_CHARGE, SITE_FX_LOAD, SITE_FX_PUSH, SITE_FX_DEPOSIT, SITE_FX_FLUSH };
+enum { SITE_PSOLVE2 = 1, SITE_PSOLVE1, SITE_CHARGE, SITE_FX_LOAD, SITE_FX_PUSH, SITE_FX_DEPOSIT, SITE_FX_FLUSH, SITE_FX_SORT };
 
 __device__ __forceinline__ void report_bad(int* status, long long* diag, int site, long long index,
                                            long long what) {

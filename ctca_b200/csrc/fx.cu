@@ -6,8 +6,9 @@
 //            marks a dead particle),
 //   vx[m], vy[m], vz[m]: FP32 velocities in internal units.
 // Particles stay sorted by the tile-major cell key (8x8x8 cell tiles by
-// default); tile_start[t] .. tile_start[t+1] is the slice of tile t at the
-// last sort, and one CTA pushes one tile of one species.
+// default): tile_start[t] .. tile_start[t+1] are the sorted ranks of tile t
+// at the last sort, stored thread-major in the padded slot region that starts
+// at tile_pad[t] (fx_push.cuh), and one CTA pushes one tile of one species.
 //
 // The step kernel fuses, per particle: the trilinear E/B gather from the
 // FP32 node field (grdcrt output), the Buneman-Boris push, the move and the
@@ -16,7 +17,7 @@
 // charge of charge.F90:59-80 at the new position (fx_push.cuh).  Deposits
 // are summed per cell in registers along each thread's sorted slice,
 // converted to int64 fixed point at 2^40 and added into a shared-memory
-// accumulator covering the tile plus a 2-cell guard; the CTA then adds its
+// accumulator covering the tile plus a 1-cell guard; the CTA then adds its
 // accumulator into the global int64 arrays.  Integer adds commute, so the
 // global sums do not depend on the order in which CTAs and atomics run, and
 // the FP32 partial sums depend only on the sorted order and the fixed thread
@@ -115,60 +116,63 @@ __global__ void k_fx_from_aos(const emsesg_particle* __restrict__ p, int64_t n, 
   vx[m] = (float)q.vx; vy[m] = (float)q.vy; vz[m] = (float)q.vz;
 }
 
-__global__ void k_fx_to_aos(const float4* __restrict__ pos, const float* __restrict__ vx, const float* __restrict__ vy,
-                            const float* __restrict__ vz, int64_t n, Geo g, int is, emsesg_particle* p) {
-  int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= n) return;
-  float4 ps = pos[m];
-  uint32_t cell = (uint32_t)__float_as_int(ps.w);
-  emsesg_particle q;
-  if (cell == DEAD) {
-    q.x = q.y = q.z = 0.0;
-    q.nid = -1;
-  } else {
-    int i, j, k;
-    unpack(g, cell, i, j, k);
-    q.x = (double)i + (double)ps.x;
-    q.y = (double)j + (double)ps.y;
-    q.z = (double)k + (double)ps.z;
-    q.nid = 0;
+// One tile region (thread-major, see fx_push.cuh) back to the FP64 records
+// of the tile's sorted ranks ts[t] .. ts[t+1]-1.
+__global__ void k_fx_to_aos_tm(const float4* __restrict__ pos, const float* __restrict__ vx,
+                               const float* __restrict__ vy, const float* __restrict__ vz,
+                               const int64_t* __restrict__ ts, const int64_t* __restrict__ tp, Geo g, int is,
+                               emsesg_particle* p) {
+  const int t = blockIdx.x, tid = threadIdx.x;
+  const int64_t n = ts[t + 1] - ts[t];
+  if (n <= 0) return;
+  const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
+  for (int r = 0; r < L; r++) {
+    const int64_t q = (int64_t)tid * L + r;
+    if (q >= n) continue;
+    const int64_t m = tp[t] + (int64_t)r * PUSH_THREADS + tid;
+    float4 ps = pos[m];
+    uint32_t cell = (uint32_t)__float_as_int(ps.w);
+    emsesg_particle o;
+    if (cell == DEAD) {
+      o.x = o.y = o.z = 0.0;
+      o.nid = -1;
+    } else {
+      int i, j, k;
+      unpack(g, cell, i, j, k);
+      o.x = (double)i + (double)ps.x;
+      o.y = (double)j + (double)ps.y;
+      o.z = (double)k + (double)ps.z;
+      o.nid = 0;
+    }
+    o.vx = vx[m]; o.vy = vy[m]; o.vz = vz[m];
+    o.pid = 0;
+    o.preside = 0;
+    o.spec = is + 1;
+    p[ts[t] + q] = o;
   }
-  q.vx = vx[m]; q.vy = vy[m]; q.vz = vz[m];
-  q.pid = 0;
-  q.preside = 0;
-  q.spec = is + 1;
-  p[m] = q;
 }
 
 // Sort key of the FP32 form: the tile-major cell key (as the FP64 spsort);
-// dead particles and slots past the live count get the largest key.
-__global__ void k_fx_keys(const float4* __restrict__ pos, int64_t n, const int64_t* count, Geo g, uint32_t deadkey,
+// dead particles, empty slots and slots past the region's slot count get the
+// largest key.
+__global__ void k_fx_keys(const float4* __restrict__ pos, int64_t n, const int64_t* slots, Geo g, uint32_t deadkey,
                           uint32_t* keys, uint32_t* vals) {
   int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n) return;
-  uint32_t cell = (uint32_t)__float_as_int(pos[m].w);
   uint32_t key = deadkey;
-  if (m < *count && cell != DEAD) {
-    int i, j, k;
-    unpack(g, cell, i, j, k);
-    uint32_t tile = (uint32_t)(i / g.t[0]) + (uint32_t)g.nt[0] * ((uint32_t)(j / g.t[1]) + (uint32_t)g.nt[1] * (uint32_t)(k / g.t[2]));
-    uint32_t in = (uint32_t)(i % g.t[0]) + (uint32_t)g.t[0] * ((uint32_t)(j % g.t[1]) + (uint32_t)g.t[1] * (uint32_t)(k % g.t[2]));
-    key = tile * (uint32_t)(g.t[0] * g.t[1] * g.t[2]) + in;
+  if (m < *slots) {
+    uint32_t cell = (uint32_t)__float_as_int(pos[m].w);
+    if (cell != DEAD) {
+      int i, j, k;
+      unpack(g, cell, i, j, k);
+      uint32_t tile = (uint32_t)(i / g.t[0]) +
+                      (uint32_t)g.nt[0] * ((uint32_t)(j / g.t[1]) + (uint32_t)g.nt[1] * (uint32_t)(k / g.t[2]));
+      uint32_t in = (uint32_t)(i % g.t[0]) + (uint32_t)g.t[0] * ((uint32_t)(j % g.t[1]) + (uint32_t)g.t[1] * (uint32_t)(k % g.t[2]));
+      key = tile * (uint32_t)(g.t[0] * g.t[1] * g.t[2]) + in;
+    }
   }
   keys[m] = key;
   vals[m] = (uint32_t)m;
-}
-
-__global__ void k_fx_gather(const float4* __restrict__ pos, const float* __restrict__ vx, const float* __restrict__ vy,
-                            const float* __restrict__ vz, const uint32_t* __restrict__ idx, int64_t n, float4* pos2,
-                            float* vx2, float* vy2, float* vz2) {
-  int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= n) return;
-  uint32_t s = idx[m];
-  pos2[m] = pos[s];
-  vx2[m] = vx[s];
-  vy2[m] = vy[s];
-  vz2[m] = vz[s];
 }
 
 // tile_start[t] = first sorted slot with tile >= t; tile_start[ntiles] and
@@ -184,6 +188,70 @@ __global__ void k_tile_starts(const uint32_t* __restrict__ keys, int64_t n, uint
   for (int64_t t = prev + 1; t <= cur; t++) tile_start[t] = m;
   if (cur == ntiles && prev < ntiles) *count = m;
 }
+
+// Padded region starts: tile t gets ceil(n_t / PUSH_THREADS) full rows.  One
+// block of 1024 threads scans the ntiles counts; slots = total.
+__global__ void __launch_bounds__(1024) k_tile_pad(const int64_t* __restrict__ ts, int64_t ntiles, int64_t* tp,
+                                                   int64_t* slots) {
+  __shared__ int64_t part[1024];
+  const int tid = threadIdx.x;
+  const int64_t per = (ntiles + 1023) / 1024;
+  const int64_t t0 = tid * per, t1 = min(ntiles, t0 + per);
+  int64_t sum = 0;
+  for (int64_t t = t0; t < t1; t++) {
+    int64_t n = ts[t + 1] - ts[t];
+    sum += (n + PUSH_THREADS - 1) / PUSH_THREADS * PUSH_THREADS;
+  }
+  part[tid] = sum;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    int64_t v = tid >= d ? part[tid - d] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  int64_t run = part[tid] - sum;  // exclusive prefix of this thread's chunk
+  for (int64_t t = t0; t < t1; t++) {
+    tp[t] = run;
+    int64_t n = ts[t + 1] - ts[t];
+    run += (n + PUSH_THREADS - 1) / PUSH_THREADS * PUSH_THREADS;
+  }
+  if (tid == 1023) {
+    tp[ntiles] = part[1023];
+    *slots = part[1023];
+  }
+}
+
+// Sorted ranks -> thread-major tile regions (fx_push.cuh): slot
+// tp[t] + r*PUSH_THREADS + c holds rank ts[t] + c*L + r; empty slots get a
+// DEAD cell.  One block per tile, coalesced writes.
+__global__ void k_fx_gather_tm(const float4* __restrict__ pos, const float* __restrict__ vx,
+                               const float* __restrict__ vy, const float* __restrict__ vz,
+                               const uint32_t* __restrict__ idx, const int64_t* __restrict__ ts,
+                               const int64_t* __restrict__ tp, float4* pos2, float* vx2, float* vy2, float* vz2) {
+  const int t = blockIdx.x, tid = threadIdx.x;
+  const int64_t n = ts[t + 1] - ts[t];
+  if (n <= 0) return;
+  const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
+  for (int r = 0; r < L; r++) {
+    const int64_t q = (int64_t)tid * L + r;
+    const int64_t m = tp[t] + (int64_t)r * PUSH_THREADS + tid;
+    if (q < n) {
+      const uint32_t src = idx[ts[t] + q];
+      pos2[m] = pos[src];
+      vx2[m] = vx[src];
+      vy2[m] = vy[src];
+      vz2[m] = vz[src];
+    } else {
+      pos2[m] = make_float4(0.f, 0.f, 0.f, __int_as_float((int)DEAD));
+      vx2[m] = 0.f;
+      vy2[m] = 0.f;
+      vz2[m] = 0.f;
+    }
+  }
+}
+
+#include "fx_sort.cuh"
 
 inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
 
@@ -224,8 +292,14 @@ int fx_alloc(emsesg_ctx* ctx) {
   int tmax = std::max(f.tile[0], std::max(f.tile[1], f.tile[2]));
   if (tmax > 8) return set_error(ctx, EMSESG_ERR_ARG, "FP32 form tiles are at most 8 cells per axis");
   f.ntiles = (int64_t)f.ntile[0] * f.ntile[1] * f.ntile[2];
+  // species regions: capacity plus one row of padding per tile, in whole rows
   int64_t cap = 0;
-  for (int is = 0; is < c.nspec; is++) cap += ctx->seg.capacity[is];
+  for (int is = 0; is < c.nspec; is++) {
+    f.base[is] = cap;
+    int64_t rows = (ctx->seg.capacity[is] + PUSH_THREADS - 1) / PUSH_THREADS + f.ntiles;
+    f.cap[is] = rows * PUSH_THREADS;
+    cap += f.cap[is];
+  }
   cap = std::max<int64_t>(cap, 1);
   EMSESG_CUDA(ctx, cudaMalloc(&f.pos, cap * sizeof(float4)));
   EMSESG_CUDA(ctx, cudaMalloc(&f.vx, cap * sizeof(float)));
@@ -236,12 +310,33 @@ int fx_alloc(emsesg_ctx* ctx) {
   EMSESG_CUDA(ctx, cudaMalloc(&f.vy2, cap * sizeof(float)));
   EMSESG_CUDA(ctx, cudaMalloc(&f.vz2, cap * sizeof(float)));
   EMSESG_CUDA(ctx, cudaMalloc(&f.count_d, EMSESG_ISPEC * sizeof(int64_t)));
+  EMSESG_CUDA(ctx, cudaMalloc(&f.slots_d, EMSESG_ISPEC * sizeof(int64_t)));
   EMSESG_CUDA(ctx, cudaMalloc(&f.tile_start, (int64_t)c.nspec * (f.ntiles + 1) * sizeof(int64_t)));
+  EMSESG_CUDA(ctx, cudaMalloc(&f.tile_pad, (int64_t)c.nspec * (f.ntiles + 1) * sizeof(int64_t)));
   FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
   EMSESG_CUDA(ctx, cudaMalloc(&f.accum, (fr.size() + fj.size()) * sizeof(int64_t)));
   int64_t nn = (int64_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
   EMSESG_CUDA(ctx, cudaMalloc(&f.fnode, nn * sizeof(float4)));
   EMSESG_CUDA(ctx, cudaMalloc(&f.fnode2, nn * sizeof(float4)));
+  // tile-local sort scratch (tiles of at most 8 cells a side)
+  {
+    const int64_t nbc = (int64_t)(f.tile[0] + 2) * (f.tile[1] + 2) * (f.tile[2] + 2);
+    const int64_t tcells = (int64_t)f.tile[0] * f.tile[1] * f.tile[2];
+    const int64_t ns = c.nspec;
+    EMSESG_CUDA(ctx, cudaMalloc(&f.tile_start2, ns * (f.ntiles + 1) * sizeof(int64_t)));
+    EMSESG_CUDA(ctx, cudaMalloc(&f.tile_pad2, ns * (f.ntiles + 1) * sizeof(int64_t)));
+    EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_cnt, ns * f.ntiles * nbc * sizeof(uint32_t)));
+    EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_base, ns * f.ntiles * nbc * sizeof(uint32_t)));
+    EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_wcnt, ns * f.ntiles * PUSH_WARPS * nbc * sizeof(uint16_t)));
+    EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_celltot, f.ntiles * tcells * sizeof(uint32_t)));
+    EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_tiletot, f.ntiles * sizeof(int64_t)));
+    EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_stray, EMSESG_ISPEC * sizeof(int)));
+    EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_inv, cap * sizeof(uint32_t)));
+    const int lsm = (int)(PUSH_WARPS * nbc * sizeof(uint32_t));
+    EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_count, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
+    EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
+    EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_move, cudaFuncAttributeMaxDynamicSharedMemorySize, move_smem()));
+  }
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(4)));
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(8)));
   return EMSESG_OK;
@@ -251,8 +346,10 @@ void fx_free(emsesg_ctx* ctx) {
   FxState& f = ctx->fx;
   cudaFree(f.pos); cudaFree(f.vx); cudaFree(f.vy); cudaFree(f.vz);
   cudaFree(f.pos2); cudaFree(f.vx2); cudaFree(f.vy2); cudaFree(f.vz2);
-  cudaFree(f.count_d); cudaFree(f.tile_start); cudaFree(f.accum);
+  cudaFree(f.count_d); cudaFree(f.slots_d); cudaFree(f.tile_start); cudaFree(f.tile_pad); cudaFree(f.accum);
   cudaFree(f.fnode); cudaFree(f.fnode2);
+  cudaFree(f.tile_start2); cudaFree(f.tile_pad2); cudaFree(f.lcs_cnt); cudaFree(f.lcs_base); cudaFree(f.lcs_wcnt);
+  cudaFree(f.lcs_celltot); cudaFree(f.lcs_tiletot); cudaFree(f.lcs_stray); cudaFree(f.lcs_inv);
   f = FxState();
 }
 
@@ -261,46 +358,133 @@ void fx_free(emsesg_ctx* ctx) {
 using namespace emsesg;
 
 namespace {
-int64_t max_cap(emsesg_ctx* ctx) {
-  int64_t m = 0;
-  for (int is = 0; is < ctx->cfg.nspec; is++) m = std::max(m, ctx->seg.capacity[is]);
-  return m;
+// Host-side bound of the slots the sort has to look at: the particles loaded
+// (no particle is added in this form) plus the padding, within the region.
+int64_t sort_slots(emsesg_ctx* ctx, int is) {
+  return std::min(ctx->fx.cap[is], ctx->totalp[is] + ctx->fx.ntiles * PUSH_THREADS);
 }
 }  // namespace
+
+// The tile-local counting sort (fx_sort.cuh).  Sets *done = false, having
+// changed nothing, when a particle left its tile's sort box; the caller then
+// sorts with the radix path.
+int fx_local_sort(emsesg_ctx* ctx, bool* done) {
+  *done = false;
+  FxState& f = ctx->fx;
+  const emsesg_config& c = ctx->cfg;
+  Geo g = make_geo(ctx);
+  LcsGeo G[EMSESG_ISPEC];
+  const int n[3] = {c.nx, c.ny, c.nz};
+  for (int is = 0; is < c.nspec; is++) {
+    G[is].nbc = 1;
+    G[is].tcells = 1;
+    for (int d = 0; d < 3; d++) {
+      G[is].n[d] = n[d];
+      G[is].t[d] = f.tile[d];
+      G[is].nt[d] = f.ntile[d];
+      G[is].bc[d] = f.tile[d] + 2;
+      G[is].nbc *= G[is].bc[d];
+      G[is].tcells *= f.tile[d];
+      G[is].wrap[d] = c.npbnd[is][d] == 0;
+    }
+  }
+  const int64_t nbc = G[0].nbc;
+  const int lsm = (int)(PUSH_WARPS * nbc * sizeof(uint32_t));
+  const int64_t T1 = f.ntiles + 1;
+  EMSESG_CUDA(ctx, cudaMemsetAsync(f.lcs_stray, 0, EMSESG_ISPEC * sizeof(int), ctx->stream));
+  for (int is = 0; is < c.nspec; is++) {
+    if (ctx->totalp[is] == 0) continue;
+    EMSESG_LAUNCH(ctx, "lcs_count", k_lcs_count, (unsigned)f.ntiles, PUSH_THREADS, lsm, f.pos + f.base[is],
+                  f.tile_start + is * T1, f.tile_pad + is * T1, g, G[is],
+                  f.lcs_wcnt + is * f.ntiles * PUSH_WARPS * nbc, f.lcs_cnt + is * f.ntiles * nbc, f.lcs_stray + is);
+  }
+  int stray[EMSESG_ISPEC] = {0};
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(stray, f.lcs_stray, EMSESG_ISPEC * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int is = 0; is < c.nspec; is++)
+    if (stray[is]) return EMSESG_OK;
+  for (int is = 0; is < c.nspec; is++) {
+    int64_t* ts2 = f.tile_start2 + is * T1;
+    int64_t* tp2 = f.tile_pad2 + is * T1;
+    if (ctx->totalp[is] == 0) {
+      EMSESG_CUDA(ctx, cudaMemsetAsync(ts2, 0, T1 * sizeof(int64_t), ctx->stream));
+      EMSESG_CUDA(ctx, cudaMemsetAsync(tp2, 0, T1 * sizeof(int64_t), ctx->stream));
+      EMSESG_CUDA(ctx, cudaMemsetAsync(f.count_d + is, 0, sizeof(int64_t), ctx->stream));
+      EMSESG_CUDA(ctx, cudaMemsetAsync(f.slots_d + is, 0, sizeof(int64_t), ctx->stream));
+      continue;
+    }
+    const int64_t off = f.base[is];
+    uint32_t* cnt = f.lcs_cnt + is * f.ntiles * nbc;
+    uint32_t* bas = f.lcs_base + is * f.ntiles * nbc;
+    EMSESG_LAUNCH(ctx, "lcs_celltot", k_lcs_celltot, (unsigned)f.ntiles, PUSH_THREADS, 0, cnt, g, G[is],
+                  f.lcs_celltot, f.lcs_tiletot);
+    EMSESG_LAUNCH(ctx, "lcs_tiles", k_lcs_tiles, 1, 1024, 0, f.lcs_tiletot, f.ntiles, ts2, tp2, f.count_d + is,
+                  f.slots_d + is);
+    EMSESG_LAUNCH(ctx, "lcs_bases", k_lcs_bases, (unsigned)f.ntiles, PUSH_THREADS, 0, cnt, f.lcs_celltot, g, G[is],
+                  ts2, tp2, bas, f.lcs_inv + off);
+    EMSESG_LAUNCH(ctx, "lcs_rank", k_lcs_rank, (unsigned)f.ntiles, PUSH_THREADS, lsm, f.pos + off,
+                  f.tile_start + is * T1, f.tile_pad + is * T1, g, G[is], f.lcs_wcnt + is * f.ntiles * PUSH_WARPS * nbc,
+                  bas, ts2, tp2, f.lcs_inv + off, ctx->d_status, ctx->d_diag);
+    EMSESG_LAUNCH(ctx, "lcs_move", k_lcs_move, (unsigned)f.ntiles, PUSH_THREADS, move_smem(), f.pos + off,
+                  f.vx + off, f.vy + off, f.vz + off, f.tile_start + is * T1, f.tile_pad + is * T1, ts2, tp2,
+                  f.lcs_inv + off, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off);
+  }
+  std::swap(f.pos, f.pos2);
+  std::swap(f.vx, f.vx2);
+  std::swap(f.vy, f.vy2);
+  std::swap(f.vz, f.vz2);
+  std::swap(f.tile_start, f.tile_start2);
+  std::swap(f.tile_pad, f.tile_pad2);
+  *done = true;
+  return EMSESG_OK;
+}
 
 extern "C" int emsesg_fx_sort(emsesg_ctx* ctx) {
   if (!ctx) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
-  int rc = ensure_sort_scratch(ctx, max_cap(ctx));
-  if (rc) return rc;
   FxState& f = ctx->fx;
+  if (f.tiled) {
+    bool done = false;
+    int lrc = fx_local_sort(ctx, &done);
+    if (lrc) return lrc;
+    if (done) return EMSESG_OK;
+  }
+  int64_t most = 1;
+  for (int is = 0; is < ctx->cfg.nspec; is++) most = std::max(most, sort_slots(ctx, is));
+  int rc = ensure_sort_scratch(ctx, most);
+  if (rc) return rc;
   Geo g = make_geo(ctx);
   uint32_t tilecells = (uint32_t)(f.tile[0] * f.tile[1] * f.tile[2]);
   uint32_t deadkey = (uint32_t)(f.ntiles * tilecells);
   int bits = 1;
   while (bits < 32 && (1ULL << bits) <= deadkey) bits++;
   for (int is = 0; is < ctx->cfg.nspec; is++) {
-    int64_t n = ctx->totalp[is];  // upper bound of the live count
-    int64_t off = ctx->seg.base[is];
+    int64_t n = sort_slots(ctx, is);
+    int64_t off = f.base[is];
     int64_t* ts = f.tile_start + (int64_t)is * (f.ntiles + 1);
-    if (n == 0) {
+    int64_t* tp = f.tile_pad + (int64_t)is * (f.ntiles + 1);
+    if (ctx->totalp[is] == 0) {
       EMSESG_CUDA(ctx, cudaMemsetAsync(ts, 0, (f.ntiles + 1) * sizeof(int64_t), ctx->stream));
+      EMSESG_CUDA(ctx, cudaMemsetAsync(tp, 0, (f.ntiles + 1) * sizeof(int64_t), ctx->stream));
       EMSESG_CUDA(ctx, cudaMemsetAsync(f.count_d + is, 0, sizeof(int64_t), ctx->stream));
+      EMSESG_CUDA(ctx, cudaMemsetAsync(f.slots_d + is, 0, sizeof(int64_t), ctx->stream));
       continue;
     }
-    EMSESG_LAUNCH(ctx, "fx_keys", k_fx_keys, nblk(n), 256, 0, f.pos + off, n, f.count_d + is, g, deadkey,
+    EMSESG_LAUNCH(ctx, "fx_keys", k_fx_keys, nblk(n), 256, 0, f.pos + off, n, f.slots_d + is, g, deadkey,
                   ctx->sort.keys[0], ctx->sort.vals[0]);
     uint32_t *ko, *vo;
     if ((rc = sort_pairs(ctx, ctx->sort.keys[0], ctx->sort.vals[0], n, bits, &ko, &vo))) return rc;
-    EMSESG_LAUNCH(ctx, "fx_gather", k_fx_gather, nblk(n), 256, 0, f.pos + off, f.vx + off, f.vy + off, f.vz + off, vo,
-                  n, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off);
     EMSESG_LAUNCH(ctx, "fx_tile_starts", k_tile_starts, nblk(n + 1), 256, 0, ko, n, tilecells, f.ntiles, ts,
                   f.count_d + is);
+    EMSESG_LAUNCH(ctx, "fx_tile_pad", k_tile_pad, 1, 1024, 0, ts, f.ntiles, tp, f.slots_d + is);
+    EMSESG_LAUNCH(ctx, "fx_gather", k_fx_gather_tm, (unsigned)f.ntiles, PUSH_THREADS, 0, f.pos + off, f.vx + off,
+                  f.vy + off, f.vz + off, vo, ts, tp, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off);
   }
   std::swap(f.pos, f.pos2);
   std::swap(f.vx, f.vx2);
   std::swap(f.vy, f.vy2);
   std::swap(f.vz, f.vz2);
+  f.tiled = true;
   return EMSESG_OK;
 }
 
@@ -312,14 +496,18 @@ extern "C" int emsesg_fx_load(emsesg_ctx* ctx) {
   Geo g = make_geo(ctx);
   for (int is = 0; is < ctx->cfg.nspec; is++) {
     int64_t n = ctx->totalp[is];
-    int64_t off = ctx->seg.base[is];
     if (n == 0) continue;
-    EMSESG_LAUNCH(ctx, "fx_from_aos", k_fx_from_aos, nblk(n), 256, 0, ctx->pbuf + off, n, g, f.pos + off, f.vx + off,
-                  f.vy + off, f.vz + off, ctx->d_status, ctx->d_diag);
+    EMSESG_LAUNCH(ctx, "fx_from_aos", k_fx_from_aos, nblk(n), 256, 0, ctx->pbuf + ctx->seg.base[is], n, g,
+                  f.pos + f.base[is], f.vx + f.base[is], f.vy + f.base[is], f.vz + f.base[is], ctx->d_status,
+                  ctx->d_diag);
   }
+  // before the first sort the regions hold the records in buffer order
   EMSESG_CUDA(ctx, cudaMemcpyAsync(f.count_d, ctx->totalp, EMSESG_ISPEC * sizeof(int64_t), cudaMemcpyHostToDevice,
                                    ctx->stream));
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(f.slots_d, ctx->totalp, EMSESG_ISPEC * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                   ctx->stream));
   f.loaded = true;
+  f.tiled = false;  // buffer order: the first sort is the radix path
   rc = emsesg_fx_sort(ctx);
   if (rc) return rc;
   return emsesg_synchronize(ctx);
@@ -337,19 +525,22 @@ extern "C" int emsesg_fx_counts(emsesg_ctx* ctx, int64_t* totalp) {
 extern "C" int emsesg_fx_store(emsesg_ctx* ctx) {
   if (!ctx) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded");
-  // Current buffer order; particles that died since the last sort come out
-  // with nid = -1 in place, as the reference leaves them before transbound.
+  // Sorted order of the last sort (tile-major cell order); particles that
+  // died since then come out with nid = -1 in place, as the reference leaves
+  // them before transbound.
   int64_t cnt[EMSESG_ISPEC] = {0};
   int rc = emsesg_fx_counts(ctx, cnt);
   if (rc) return rc;
   FxState& f = ctx->fx;
   Geo g = make_geo(ctx);
   for (int is = 0; is < ctx->cfg.nspec; is++) {
-    int64_t off = ctx->seg.base[is];
+    int64_t off = f.base[is];
     ctx->totalp[is] = cnt[is];
     if (cnt[is] == 0) continue;
-    EMSESG_LAUNCH(ctx, "fx_to_aos", k_fx_to_aos, nblk(cnt[is]), 256, 0, f.pos + off, f.vx + off, f.vy + off,
-                  f.vz + off, cnt[is], g, is, ctx->pbuf + off);
+    const int64_t* ts = f.tile_start + (int64_t)is * (f.ntiles + 1);
+    const int64_t* tp = f.tile_pad + (int64_t)is * (f.ntiles + 1);
+    EMSESG_LAUNCH(ctx, "fx_to_aos", k_fx_to_aos_tm, (unsigned)f.ntiles, PUSH_THREADS, 0, f.pos + off, f.vx + off,
+                  f.vy + off, f.vz + off, ts, tp, g, is, ctx->pbuf + ctx->seg.base[is]);
   }
   EMSESG_CUDA(ctx, cudaMemcpyAsync(ctx->d_count, ctx->totalp, EMSESG_ISPEC * sizeof(int64_t), cudaMemcpyHostToDevice,
                                    ctx->stream));
@@ -380,12 +571,13 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
   FxPushArgs a{};
   a.pos = f.pos; a.vx = f.vx; a.vy = f.vy; a.vz = f.vz;
   a.tile_start = f.tile_start;
+  a.tile_pad = f.tile_pad;
   a.ntiles = f.ntiles;
   double gustep = ustep;
   a.gustep = (float)gustep;
   a.rustep = (float)(1.0 / ustep);
   for (int is = 0; is < c.nspec; is++) {
-    a.off[is] = ctx->seg.base[is];
+    a.off[is] = f.base[is];
     for (int d = 0; d < 3; d++) a.npbnd[is][d] = c.npbnd[is][d];
     a.qmp[is] = (float)(c.qm[is] * gustep * 0.5);
     a.qfix[is] = (float)(c.q[is] * 1099511627776.0);
@@ -399,9 +591,9 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
   a.diag = ctx->d_diag;
   dim3 grid((unsigned)f.ntiles, (unsigned)c.nspec);
   if (fx_box_tile(tmax) == 4)
-    EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<4>, grid, PUSH_THREADS, smem, a);
+    EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<4>, grid, PUSH_BLOCK, smem, a);
   else
-    EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<8>, grid, PUSH_THREADS, smem, a);
+    EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<8>, grid, PUSH_BLOCK, smem, a);
   // guard folding on the exact integers, then FP64 outputs
   if ((rc = run_slab_ops(ctx, (long long*)acc_rho, fr, fold_ops(c, 0, 1), "fx_fold_rho"))) return rc;
   if ((rc = run_slab_ops(ctx, (long long*)acc_j, fj, fold_ops(c, 1, 3), "fx_fold_j"))) return rc;

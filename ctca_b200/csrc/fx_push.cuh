@@ -1,45 +1,58 @@
 // fx_push.cuh -- the fused push + zigzag current + CIC charge kernel of the
 // FP32 / fixed-point form (included by fx.cu inside its private namespace).
 //
-// One CTA (512 threads) pushes the particles that the last sort placed in
-// one cell tile of one species.  At the start it copies the tile's FP32 E/B
-// nodes (tile + 1-node guard) into shared memory, so the 8-corner gathers
-// read shared memory.  The tile's particles are split into 512 contiguous
-// slices, one per thread; because they are sorted by cell, a thread meets
-// long runs of particles in the same cell.  A thread keeps the 20 deposits of
-// a cell (12 zigzag-current and 8 CIC-charge node values) in FP32 registers
-// while the cell does not change.  When the
-// cell changes (the thread's run moves on), or a particle changes cell
-// during the step (its "after" half), the thread appends the 20 values
-// and the cell to its warp's queue in shared memory; when the queue holds 16
-// or more entries the warp empties it together, one entry per lane, adding
-// the values into the CTA's int64 tile accumulator (tile + 1-cell guard).
-// So the conversions and atomics run with all lanes busy instead of one
-// lane at a time.  The CTA finally adds its accumulator into the global
-// int64 arrays.  Particle records move through shared memory: slices are
-// loaded and stored with coalesced accesses in chunks of RUN particles.
+// Layout.  The sort leaves every (species, cell tile) in a padded region of
+// L rows x PUSH_THREADS slots, thread-major: the particle of sorted rank q in
+// the tile sits in row q % L, column q / L.  Column t of the region is thus
+// thread t's contiguous run of the cell-sorted order, and row r is one
+// coalesced stretch of PUSH_THREADS records.  Empty slots hold DEAD cells.
 //
-// The tile edge T is a template parameter, so every node offset inside the
-// accumulator is an immediate.  Deposits or gathers whose cell lies outside
-// the tile box (particles that drifted more than one cell since the sort)
-// take a separate path through the global arrays.
+// One CTA pushes one region with 512 threads; a 17th warp streams the rows
+// into a 4-stage shared-memory ring with cp.async.bulk (TMA 1-D copies
+// completing on mbarriers) and never computes, so a warp busy with its
+// queues never holds up the stream; pushing warps release a stage through an
+// "empty" mbarrier once they hold their particle.  The
+// tile's FP32 E/B nodes (tile + 1-cell guard) sit in shared memory.
+//
+// Per particle: trilinear gather, Buneman-Boris, move.  A particle that
+// stays inside its cell (the common case) adds its two zigzag segments and
+// its CIC charge to 20 FP32 registers that follow the thread's current cell
+// ("run"); when the run's cell changes the 20 sums go through a per-warp
+// queue and are added, converted to int64 fixed point, into the CTA's tile
+// accumulator by all lanes together.  A particle that leaves its cell (or
+// whose cell lies outside the tile box) is appended to a per-warp "cross"
+// queue; when 32 are queued, every lane takes one and runs the general path
+// (per-axis boundary rules, relay point, two segments in different cells,
+// charge at the new cell) with direct int64 atomics.  So the divergent work
+// of the few cell-crossing particles runs with all lanes busy.
+//
+// Determinism: a run's FP32 partial sums follow the thread's fixed order;
+// every conversion to fixed point is of one value; integer atomics commute.
+// Two runs on the same input give the same bits.
 
-constexpr int PUSH_THREADS = 512;
+constexpr int PUSH_THREADS = 512;           // pushing threads = slots per row
 constexpr int PUSH_WARPS = PUSH_THREADS / 32;
+constexpr int PUSH_BLOCK = PUSH_THREADS + 32;  // + one warp that streams the rows
 constexpr int PG = 1;           // guard cells around the tile
-constexpr int QCAP = 48;        // queue entries per warp
-constexpr int QW = 21;          // words per entry: 20 values + cell
-constexpr int RUN = 4;          // particles per thread per staged chunk
-constexpr int SLOT = RUN + 1;   // padded slots per thread (conflict-free reads)
+constexpr int NSTAGE = 4;       // row ring stages
+constexpr int PREFETCH = 2;     // rows issued ahead of the row being pushed
 constexpr int NJ = 12;          // zigzag node values of one cell
 constexpr int NR = 8;           // CIC node values of one cell
+constexpr int RQW = NJ + NR + 1;  // run-queue entry: 20 sums + cell
+constexpr int RQ_DRAIN = 8;     // drain the run queue at this many entries
+constexpr int RQCAP = RQ_DRAIN + 32;
+constexpr int XQW = 8;          // cross entry: slot, cell, 3 offsets, 3 velocities
+constexpr int XQ_DRAIN = 32;
+constexpr int XQCAP = XQ_DRAIN + 32;
+constexpr uint32_t ROW_BYTES = PUSH_THREADS * (16 + 3 * 4);
 
 struct FxPushArgs {
   float4* pos;                  // all species regions
   float* vx;
   float* vy;
   float* vz;
-  const int64_t* tile_start;    // [nspec][ntiles+1], offsets inside each region
+  const int64_t* tile_start;    // [nspec][ntiles+1] sorted ranks (live particles)
+  const int64_t* tile_pad;      // [nspec][ntiles+1] slot offsets of the padded regions
   int64_t off[EMSESG_ISPEC];    // region base per species
   int npbnd[EMSESG_ISPEC][3];
   float qmp[EMSESG_ISPEC], qfix[EMSESG_ISPEC];
@@ -56,6 +69,57 @@ struct FxPushArgs {
   long long* diag;
 };
 
+// ---------------------------------------------------------------- PTX
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(b)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait: gives up after about one second.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+  if (mbar_try_wait(b, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0;; it++) {
+    if (mbar_try_wait(b, parity)) return true;
+    if ((it & 255u) == 255u && global_ns() - t0 > 1000000000ull) return false;
+  }
+}
+// 1-D bulk copy global -> shared, completing on an mbarrier (both addresses
+// 16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// ---------------------------------------------------------------- moves
 // Per-axis move and outer boundary of psolve1.F90:366-606 on (cell, offset)
 // pairs.  In: cell ib, offset ob, displacement d.  Out: the "after" point
 // xlocala = (ac, af), its cell ia, the relay point xr = (rc, rf), the stored
@@ -66,18 +130,13 @@ struct Axis {
   bool dead, flip, crossed;
 };
 
-__device__ __forceinline__ Axis axis_move(int ib, float ob, float d, int n, int npbnd) {
+// The outer boundary rules for an "after" cell ac outside 0..n-1.
+__device__ __forceinline__ Axis axis_boundary(int ib, float ob, int ac, float af, int n, int npbnd) {
   Axis o;
-  float s = ob + d;
-  float fl = floorf(s);
-  int ac = ib + (int)fl;
-  float af = s - fl;
-  if (af >= 1.0f) { af = 0.0f; ac += 1; }
   o.dead = false;
   o.flip = false;
-  o.crossed = false;
+  o.crossed = true;
   if (ac < 0) {  // p%x < 0
-    o.crossed = true;
     if (npbnd == 0) {
       o.ac = ac; o.af = af; o.ia = -1; o.rc = 0; o.rf = 0.f;
       o.nc = ac + n; o.nf = af;
@@ -91,8 +150,7 @@ __device__ __forceinline__ Axis axis_move(int ib, float ob, float d, int n, int 
       o.ac = -1; o.af = 0.f; o.ia = -1; o.rc = 0; o.rf = 0.f;
       o.nc = 0; o.nf = 0.f; o.dead = true;
     }
-  } else if (ac >= n) {  // p%x >= slx
-    o.crossed = true;
+  } else {  // p%x >= slx
     if (npbnd == 0) {
       o.ac = ac; o.af = af; o.ia = n; o.rc = n; o.rf = 0.f;
       o.nc = ac - n; o.nf = af;
@@ -106,12 +164,25 @@ __device__ __forceinline__ Axis axis_move(int ib, float ob, float d, int n, int 
       o.ac = n + 1; o.af = 0.f; o.ia = n; o.rc = n; o.rf = 0.f;
       o.nc = 0; o.nf = 0.f; o.dead = true;
     }
-  } else {
-    o.ac = ac; o.af = af; o.ia = ac;
-    if (ac == ib) { o.rc = ib; o.rf = (ob + af) * 0.5f; }
-    else { o.rc = max(ib, ac); o.rf = 0.f; }
-    o.nc = ac; o.nf = af;
   }
+  return o;
+}
+
+__device__ __forceinline__ Axis axis_move(int ib, float ob, float d, int n, int npbnd) {
+  const float s = ob + d;
+  const float fl = floorf(s);
+  int ac = ib + (int)fl;
+  float af = s - fl;
+  if (af >= 1.0f) { af = 0.0f; ac += 1; }
+  if ((unsigned)ac >= (unsigned)n) return axis_boundary(ib, ob, ac, af, n, npbnd);
+  Axis o;
+  o.dead = false;
+  o.flip = false;
+  o.crossed = false;
+  o.ac = ac; o.af = af; o.ia = ac; o.nc = ac; o.nf = af;
+  const bool same = ac == ib;
+  o.rc = same ? ib : max(ib, ac);
+  o.rf = same ? (ob + af) * 0.5f : 0.f;
   return o;
 }
 
@@ -147,32 +218,6 @@ struct Sink {
   int* status;
   long long* diag;
 };
-struct V12 { float v[NJ]; };
-struct V8 { float v[NR]; };
-
-// Out-of-box bundles: global int64 atomics with bounds checks (rare path;
-// values come by value so the callers' register arrays keep no address).
-__device__ __noinline__ void put_j_global(Sink s, int i, int j, int k, V12 v, float qfix) {
-  for (int q = 0; q < NJ; q++) {
-    int ii = i + jdi(q), jj = j + jdj(q), kk = k + jdk(q);
-    if (ii < -4 || jj < -4 || kk < -4 || ii > s.nx + 4 || jj > s.ny + 4 || kk > s.nz + 4) {
-      report_bad(s.status, s.diag, SITE_FX_DEPOSIT, -2, ii + 100000LL * jj + 10000000000LL * kk);
-      continue;
-    }
-    atomicAdd(&s.acc_j[s.fj.at(jcomp(q) - 1, ii, jj, kk)], (unsigned long long)to_fix(v.v[q], qfix));
-  }
-}
-
-__device__ __noinline__ void put_r_global(Sink s, int i, int j, int k, V8 v, float qfix) {
-  for (int r = 0; r < NR; r++) {
-    int ii = i + rdi(r), jj = j + rdj(r), kk = k + rdk(r);
-    if (ii < -1 || jj < -1 || kk < -1 || ii > s.nx + 1 || jj > s.ny + 1 || kk > s.nz + 1) {
-      report_bad(s.status, s.diag, SITE_FX_DEPOSIT, -1, ii + 100000LL * jj + 10000000000LL * kk);
-      continue;
-    }
-    atomicAdd(&s.acc_rho[s.fr.at(0, ii, jj, kk)], (unsigned long long)to_fix(v.v[r], qfix));
-  }
-}
 
 // Box index of cell (i,j,k) when its 2x2x2 node block lies inside the box,
 // else -1.
@@ -181,6 +226,70 @@ __device__ __forceinline__ int box_base(const int (&o)[3], int i, int j, int k) 
   int li = i - o[0], lj = j - o[1], lk = k - o[2];
   bool ok = (unsigned)li < (unsigned)(B - 1) && (unsigned)lj < (unsigned)(B - 1) && (unsigned)lk < (unsigned)(B - 1);
   return ok ? (lk * B + lj) * B + li : -1;
+}
+
+struct V12 { float v[NJ]; };
+struct V8 { float v[NR]; };
+
+// Node sets whose cell lies outside the box: global int64 atomics with
+// bounds checks (rare; the values come by value so that the callers'
+// register arrays keep no address).
+__device__ __forceinline__ void put_j_global(Sink s, int i, int j, int k, V12 v, float qfix) {
+  for (int q = 0; q < NJ; q++) {
+    const long long f = to_fix(v.v[q], qfix);
+    if (f == 0) continue;
+    const int ii = i + jdi(q), jj = j + jdj(q), kk = k + jdk(q);
+    if (ii < -4 || jj < -4 || kk < -4 || ii > s.nx + 4 || jj > s.ny + 4 || kk > s.nz + 4) {
+      report_bad(s.status, s.diag, SITE_FX_DEPOSIT, -2, ii + 100000LL * jj + 10000000000LL * kk);
+      continue;
+    }
+    atomicAdd(&s.acc_j[s.fj.at(jcomp(q) - 1, ii, jj, kk)], (unsigned long long)f);
+  }
+}
+
+__device__ __forceinline__ void put_r_global(Sink s, int i, int j, int k, V8 v, float qfix) {
+  for (int r = 0; r < NR; r++) {
+    const long long f = to_fix(v.v[r], qfix);
+    if (f == 0) continue;
+    const int ii = i + rdi(r), jj = j + rdj(r), kk = k + rdk(r);
+    if (ii < -1 || jj < -1 || kk < -1 || ii > s.nx + 1 || jj > s.ny + 1 || kk > s.nz + 1) {
+      report_bad(s.status, s.diag, SITE_FX_DEPOSIT, -1, ii + 100000LL * jj + 10000000000LL * kk);
+      continue;
+    }
+    atomicAdd(&s.acc_rho[s.fr.at(0, ii, jj, kk)], (unsigned long long)f);
+  }
+}
+
+// One zigzag node set (12 values) of cell (i,j,k): into the box, or into the
+// global arrays when the cell lies outside the box.
+template <int B>
+__device__ __forceinline__ void put_j(unsigned long long* box, const int (&o)[3], const Sink& s, int i, int j, int k,
+                                      const float (&v)[NJ], float qfix) {
+  const int base = box_base<B>(o, i, j, k);
+  if (base >= 0) {
+#pragma unroll
+    for (int q = 0; q < NJ; q++) atomicAdd(&box[base + BoxT<B>::joff(q)], (unsigned long long)to_fix(v[q], qfix));
+  } else {
+    V12 w;
+#pragma unroll
+    for (int q = 0; q < NJ; q++) w.v[q] = v[q];
+    put_j_global(s, i, j, k, w, qfix);
+  }
+}
+
+template <int B>
+__device__ __forceinline__ void put_r(unsigned long long* box, const int (&o)[3], const Sink& s, int i, int j, int k,
+                                      const float (&v)[NR], float qfix) {
+  const int base = box_base<B>(o, i, j, k);
+  if (base >= 0) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) atomicAdd(&box[base + BoxT<B>::roff(r)], (unsigned long long)to_fix(v[r], qfix));
+  } else {
+    V8 w;
+#pragma unroll
+    for (int r = 0; r < NR; r++) w.v[r] = v[r];
+    put_r_global(s, i, j, k, w, qfix);
+  }
 }
 
 template <bool SMEM>
@@ -211,86 +320,208 @@ __device__ __forceinline__ void gather8(const float4* f0, const void* f1v, int64
   b[0] = bx; b[1] = by; b[2] = bz;
 }
 
-// A queued bundle whose cell lies outside the tile box (rare).
-__device__ __noinline__ void put_bundle_global(Sink sk, int i, int j, int k, const float* en, float qfix) {
-  V12 wj;
-  V8 wr;
-  for (int s = 0; s < NJ; s++) wj.v[s] = en[s];
-  for (int r = 0; r < NR; r++) wr.v[r] = en[NJ + r];
-  put_j_global(sk, i, j, k, wj, qfix);
-  put_r_global(sk, i, j, k, wr, qfix);
+// The same gather from the tile's shared-memory nodes (box index `base`,
+// compile-time strides).
+template <int B>
+__device__ __forceinline__ void gather8_smem(const float4* f0, const float2* f1, int base, const float (&w)[8],
+                                             float (&e)[3], float (&b)[3]) {
+  constexpr int SY = B, SZ = B * B;
+  constexpr int off[8] = {SZ, SZ + 1, SZ + 1 + SY, SZ + SY, 0, 1, 1 + SY, SY};
+  float ex = 0.f, ey = 0.f, ez = 0.f, bx = 0.f, by = 0.f, bz = 0.f;
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const float4 p = f0[base + off[c]];
+    const float2 q = f1[base + off[c]];
+    ex += p.x * w[c];
+    ey += p.y * w[c];
+    ez += p.z * w[c];
+    bx += p.w * w[c];
+    by += q.x * w[c];
+    bz += q.y * w[c];
+  }
+  e[0] = ex; e[1] = ey; e[2] = ez;
+  b[0] = bx; b[1] = by; b[2] = bz;
 }
 
-// Empties a warp queue: lane l takes entries l, l+32, ...  Each lane walks
-// its entry's 20 slots starting at slot (lane mod 20), so lanes holding
+// Empties a warp's run queue: lane l takes entries l, l+32, ...  Each lane
+// walks its entry's 20 slots starting at slot (lane mod 20), so lanes holding
 // entries of the same cell add to different nodes at the same time.
 template <int B>
-__device__ __forceinline__ void drain_queue(const Sink& sk, const Geo& g, unsigned long long* box, const int (&o)[3],
-                                            const int* slot_off, float* q, int qn, float qfix, int lane) {
+__device__ __forceinline__ void drain_runs(const Geo& g, unsigned long long* box, const int (&o)[3],
+                                           const int* slot_off, const float* q, int qn, float qfix, int lane) {
   __syncwarp();
   const int rot = lane % (NJ + NR);
   for (int p = 0; p < qn; p += 32) {
     int e = p + lane;
     if (e < qn) {
-      const float* en = q + e * QW;
+      const float* en = q + e * RQW;
       uint32_t key = (uint32_t)__float_as_int(en[NJ + NR]);
       int i, j, k;
       unpack(g, key, i, j, k);
-      i -= 1; j -= 1; k -= 1;  // keys hold cells shifted by +1 (qkey)
-      int base = box_base<B>(o, i, j, k);
-      if (base >= 0) {
+      int base = box_base<B>(o, i, j, k);  // runs are only kept for cells inside the box
 #pragma unroll 4
-        for (int s = 0; s < NJ + NR; s++) {
-          int slot = s + rot;
-          slot -= slot >= NJ + NR ? NJ + NR : 0;
-          long long v = to_fix(en[slot], qfix);
-          if (v) atomicAdd(&box[base + slot_off[slot]], (unsigned long long)v);
-        }
-      } else {
-        put_bundle_global(sk, i, j, k, en, qfix);
+      for (int s = 0; s < NJ + NR; s++) {
+        int slot = s + rot;
+        slot -= slot >= NJ + NR ? NJ + NR : 0;
+        atomicAdd(&box[base + slot_off[slot]], (unsigned long long)to_fix(en[slot], qfix));
       }
     }
   }
   __syncwarp();
 }
 
-// Cell key of an "after" bundle: cells may be -1 or n on an axis (the
-// reference's guard indices), so the queue stores the cell shifted by +1.
-__device__ __forceinline__ uint32_t qkey(const Geo& g, int i, int j, int k) { return pack(g, i + 1, j + 1, k + 1); }
+struct CrossCtx {
+  float4* gpos;                 // the tile region's first slot
+  float* gvx;
+  float* gvy;
+  float* gvz;
+  float gustep, rustep, qfix;
+  int nb[3];
+};
+
+// General path for one particle that left its cell (or whose cell lies
+// outside the box): boundary rules, zigzag with relay point, charge at the
+// stored cell; the final record is written here.
+template <int B>
+__device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, const int (&o)[3], const Sink& sk,
+                                         const CrossCtx& c, const float* en) {
+  const int loc = __float_as_int(en[0]);
+  const uint32_t cell = (uint32_t)__float_as_int(en[1]);
+  const float bx = en[2], by = en[3], bz = en[4];
+  float vx = en[5], vy = en[6], vz = en[7];
+  int ib, jb, kb;
+  unpack(g, cell, ib, jb, kb);
+  Axis ax = axis_move(ib, bx, vx * c.gustep, g.nx, c.nb[0]);
+  Axis ay = axis_move(jb, by, vy * c.gustep, g.ny, c.nb[1]);
+  Axis az = axis_move(kb, bz, vz * c.gustep, g.nz, c.nb[2]);
+  if (ax.flip) vx = -vx;
+  if (ay.flip) vy = -vy;
+  if (az.flip) vz = -vz;
+  const bool dead = ax.dead || ay.dead || az.dead;
+  const uint32_t nc = dead ? DEAD : pack(g, ax.nc, ay.nc, az.nc);
+  c.gpos[loc] = make_float4(ax.nf, ay.nf, az.nf, __int_as_float((int)nc));
+  c.gvx[loc] = vx;
+  c.gvy[loc] = vy;
+  c.gvz[loc] = vz;
+  // zigzag (psolve1.F90:717-757), integer parts first
+  float J[NJ];
+  {
+    float xd = ((float)(ax.rc - ib) + ax.rf + bx) * 0.5f;
+    float yd = ((float)(ay.rc - jb) + ay.rf + by) * 0.5f;
+    float zd = ((float)(az.rc - kb) + az.rf + bz) * 0.5f;
+    float vvx = ((float)(ax.rc - ib) + (ax.rf - bx)) * c.rustep;
+    float vvy = ((float)(ay.rc - jb) + (ay.rf - by)) * c.rustep;
+    float vvz = ((float)(az.rc - kb) + (az.rf - bz)) * c.rustep;
+    float w;
+    w = yd * zd; J[3] = vvx * w; J[1] = vvx * (yd - w); J[2] = vvx * (zd - w); J[0] = vvx * (1.0f - yd - (zd - w));
+    w = xd * zd; J[7] = vvy * w; J[5] = vvy * (xd - w); J[6] = vvy * (zd - w); J[4] = vvy * (1.0f - xd - (zd - w));
+    w = xd * yd; J[11] = vvz * w; J[9] = vvz * (xd - w); J[10] = vvz * (yd - w); J[8] = vvz * (1.0f - xd - (yd - w));
+  }
+  // both segments in the cell of the start point (a particle that did not
+  // change cell): one set of node values
+  const bool one = ax.ia == ib && ay.ia == jb && az.ia == kb;
+  if (!one) put_j<B>(box, o, sk, ib, jb, kb, J, c.qfix);
+  {
+    float J2[NJ];
+    float xd = ((float)(ax.ac - ax.ia) + ax.af + (float)(ax.rc - ax.ia) + ax.rf) * 0.5f;
+    float yd = ((float)(ay.ac - ay.ia) + ay.af + (float)(ay.rc - ay.ia) + ay.rf) * 0.5f;
+    float zd = ((float)(az.ac - az.ia) + az.af + (float)(az.rc - az.ia) + az.rf) * 0.5f;
+    float vvx = ((float)(ax.ac - ax.rc) + (ax.af - ax.rf)) * c.rustep;
+    float vvy = ((float)(ay.ac - ay.rc) + (ay.af - ay.rf)) * c.rustep;
+    float vvz = ((float)(az.ac - az.rc) + (az.af - az.rf)) * c.rustep;
+    float w;
+    w = yd * zd; J2[3] = vvx * w; J2[1] = vvx * (yd - w); J2[2] = vvx * (zd - w); J2[0] = vvx * (1.0f - yd - (zd - w));
+    w = xd * zd; J2[7] = vvy * w; J2[5] = vvy * (xd - w); J2[6] = vvy * (zd - w); J2[4] = vvy * (1.0f - xd - (zd - w));
+    w = xd * yd; J2[11] = vvz * w; J2[9] = vvz * (xd - w); J2[10] = vvz * (yd - w); J2[8] = vvz * (1.0f - xd - (yd - w));
+    if (one) {
+#pragma unroll
+      for (int q = 0; q < NJ; q++) J2[q] += J[q];
+    }
+    put_j<B>(box, o, sk, ax.ia, ay.ia, az.ia, J2, c.qfix);
+  }
+  if (!dead) {
+    // charge.F90:152-210 at the stored (wrapped / reflected) position
+    float X = ax.nf, Y = ay.nf, Z = az.nf;
+    float XY = X * Y, XZ = X * Z, YZ = Y * Z, Z2 = 1.0f - Z, XZ2 = X * Z2, YZ2 = Y * Z2;
+    float R[NR];
+    R[2] = XY * Z; R[1] = XZ - R[2]; R[3] = YZ - R[2]; R[0] = Z - XZ - R[3];
+    R[6] = XY * Z2; R[5] = XZ2 - R[6]; R[7] = YZ2 - R[6]; R[4] = Z2 - XZ2 - R[7];
+    put_r<B>(box, o, sk, ax.nc, ay.nc, az.nc, R, c.qfix);
+  }
+  return dead ? 1 : 0;
+}
+
+// Returns the number of this lane's particles that escaped.
+template <int B>
+__device__ __forceinline__ int drain_cross(const FxPushArgs& a, int is, int64_t slot0, unsigned long long* box,
+                                           const int (&o)[3], const float* q, int qn, int lane) {
+  __syncwarp();
+  // the context comes from the kernel parameters here, so that the pushing
+  // loop keeps none of it in registers
+  const Geo& g = a.g;
+  const Sink sk{a.acc_rho, a.acc_j, a.fr, a.fj, g.nx, g.ny, g.nz, a.status, a.diag};
+  const CrossCtx c{a.pos + slot0, a.vx + slot0, a.vy + slot0, a.vz + slot0, a.gustep, a.rustep, a.qfix[is],
+                   {a.npbnd[is][0], a.npbnd[is][1], a.npbnd[is][2]}};
+  int dead = 0;
+  for (int p = 0; p < qn; p += 32) {
+    int e = p + lane;
+    if (e < qn) dead += cross_one<B>(g, box, o, sk, c, q + e * XQW);
+  }
+  __syncwarp();
+  return dead;
+}
 
 template <int T>
-__global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_push(FxPushArgs a) {
+__global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   constexpr int B = T + 2 * PG + 1;  // box and field tile edge (nodes)
   constexpr int NBOX = 4 * B * B * B;
   constexpr int NF = B * B * B;
-  extern __shared__ unsigned long long smem[];
+  extern __shared__ __align__(128) unsigned long long smem[];
+  __shared__ __align__(8) uint64_t full_bar[NSTAGE];
+  __shared__ __align__(8) uint64_t empty_bar[NSTAGE];
   __shared__ int slot_off[NJ + NR];
+  __shared__ int rows_seen;
   const Geo& g = a.g;
   const int is = blockIdx.y;
   const int t = blockIdx.x;
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  int tx = t % g.nt[0], ty = (t / g.nt[0]) % g.nt[1], tz = t / (g.nt[0] * g.nt[1]);
-  // T bounds every tile edge; the box may be larger than a thin tile needs
-  const int o[3] = {tx * g.t[0] - PG, ty * g.t[1] - PG, tz * g.t[2] - PG};
-  unsigned long long* box = smem;
-  float4* sf0 = reinterpret_cast<float4*>(smem + NBOX);
-  float4* spos = sf0 + NF;
-  float2* sf1 = reinterpret_cast<float2*>(spos + PUSH_THREADS * SLOT);
-  float* svx = reinterpret_cast<float*>(sf1 + NF);
-  float* svy = svx + PUSH_THREADS * SLOT;
-  float* svz = svy + PUSH_THREADS * SLOT;
-  float* queue = svz + PUSH_THREADS * SLOT + warp * QCAP * QW;
 
   const int64_t* ts = a.tile_start + (int64_t)is * (a.ntiles + 1);
-  const int64_t p0 = ts[t], n = ts[t + 1] - p0;
+  const int64_t n = ts[t + 1] - ts[t];
   if (n <= 0) return;
-  const int64_t sy = g.nx + 1, sz = (int64_t)(g.nx + 1) * (g.ny + 1);
+  const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
+  const int64_t slot0 = a.off[is] + a.tile_pad[(int64_t)is * (a.ntiles + 1) + t];
+
+  int tx = t % g.nt[0], ty = (t / g.nt[0]) % g.nt[1], tz = t / (g.nt[0] * g.nt[1]);
+  const int o[3] = {tx * g.t[0] - PG, ty * g.t[1] - PG, tz * g.t[2] - PG};
+  unsigned long long* box = smem;
+  float4* stpos = reinterpret_cast<float4*>(smem + NBOX);
+  float* stvx = reinterpret_cast<float*>(stpos + NSTAGE * PUSH_THREADS);
+  float* stvy = stvx + NSTAGE * PUSH_THREADS;
+  float* stvz = stvy + NSTAGE * PUSH_THREADS;
+  float4* sf0 = reinterpret_cast<float4*>(stvz + NSTAGE * PUSH_THREADS);
+  float2* sf1 = reinterpret_cast<float2*>(sf0 + NF);
+  float* rq = reinterpret_cast<float*>(sf1 + NF) + warp * RQCAP * RQW;
+  float* xq = reinterpret_cast<float*>(sf1 + NF) + PUSH_WARPS * RQCAP * RQW + warp * XQCAP * XQW;
+
+  float4* gpos = a.pos + slot0;
+  float* gvx = a.vx + slot0;
+  float* gvy = a.vy + slot0;
+  float* gvz = a.vz + slot0;
+
+  if (tid == 0) {
+    for (int s = 0; s < NSTAGE; s++) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], PUSH_WARPS);
+    }
+    mbar_fence_init();
+  }
   if (tid < NJ + NR) slot_off[tid] = tid < NJ ? BoxT<B>::joff(tid) : BoxT<B>::roff(tid - NJ);
-  for (int e = tid; e < NBOX; e += PUSH_THREADS) box[e] = 0ull;
-  // field tile: nodes o .. o+B-1 (those inside 0..n)
-  for (int e = tid; e < NF; e += PUSH_THREADS) {
+  for (int e = tid; e < NBOX; e += PUSH_BLOCK) box[e] = 0ull;
+  const int64_t sy = g.nx + 1, sz = (int64_t)(g.nx + 1) * (g.ny + 1);
+  for (int e = tid; e < NF; e += PUSH_BLOCK) {
     int li = e % B, lj = (e / B) % B, lk = e / (B * B);
     int gi = o[0] + li, gj = o[1] + lj, gk = o[2] + lk;
     float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p;
@@ -302,226 +533,216 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_push(FxPushArgs a) {
     sf0[e] = p;
     sf1[e] = make_float2(q.x, q.y);
   }
+  __syncthreads();
 
-  const int64_t off = a.off[is];
-  float4* gpos = a.pos + off;
-  float* gvx = a.vx + off;
-  float* gvy = a.vy + off;
-  float* gvz = a.vz + off;
+  int issued = 0;  // rows issued (producer lane 0)
+  if (warp == PUSH_WARPS) {
+    // Row producer: row r goes to stage r % NSTAGE once every pushing warp
+    // released the row that used that stage before.
+    if (lane == 0) {
+      for (int r = 0; r < L; r++) {
+        const int s = r % NSTAGE;
+        if (r >= NSTAGE && !mbar_wait(&empty_bar[s], (uint32_t)((r / NSTAGE - 1) & 1))) {
+          report_bad(a.status, a.diag, SITE_FX_PUSH, -4, t);
+          break;
+        }
+        mbar_expect_tx(&full_bar[s], ROW_BYTES);
+        const int64_t ro = (int64_t)r * PUSH_THREADS;
+        bulk_g2s(stpos + s * PUSH_THREADS, gpos + ro, PUSH_THREADS * 16, &full_bar[s]);
+        bulk_g2s(stvx + s * PUSH_THREADS, gvx + ro, PUSH_THREADS * 4, &full_bar[s]);
+        bulk_g2s(stvy + s * PUSH_THREADS, gvy + ro, PUSH_THREADS * 4, &full_bar[s]);
+        bulk_g2s(stvz + s * PUSH_THREADS, gvz + ro, PUSH_THREADS * 4, &full_bar[s]);
+        issued = r + 1;
+      }
+    }
+    __syncwarp();
+  } else {
+
   const float qmp = a.qmp[is], qfix = a.qfix[is];
-  const int nb0 = a.npbnd[is][0], nb1 = a.npbnd[is][1], nb2 = a.npbnd[is][2];
-  const Sink sk{a.acc_rho, a.acc_j, a.fr, a.fj, g.nx, g.ny, g.nz, a.status, a.diag};
-  // thread slices of the tile's particles
-  const int64_t s0 = p0 + (n * tid) / PUSH_THREADS;
-  const int64_t s1 = p0 + (n * (tid + 1)) / PUSH_THREADS;
-  const int64_t maxlen = (n + PUSH_THREADS - 1) / PUSH_THREADS;
-  const int chunks = (int)((maxlen + RUN - 1) / RUN);
+  const float gustep = a.gustep, hr = 0.5f * a.rustep;
 
   float acc[NJ + NR];
 #pragma unroll
   for (int s = 0; s < NJ + NR; s++) acc[s] = 0.f;
-  uint32_t acckey = DEAD;
+  uint32_t runcell = DEAD;
+  int runbase = -1;
   int nesc = 0;
-  int qn = 0;  // warp-uniform queue length
+  int rqn = 0, xqn = 0;  // warp-uniform queue lengths
+  bool failed = false;
+  int seen = 0;  // rows observed complete (thread 0)
+  // Row r is pushed while row r+1 is already in shared memory: the cell of
+  // the thread's next particle decides whether a change of cell starts a new
+  // run or is a single particle out of place (one that changed cell since
+  // the sort), which then takes the cross path and leaves the run intact.
+  bool okme = false;
+  if (L > 0) {
+    okme = mbar_wait(&full_bar[0], 0u);
+    if (!__any_sync(0xffffffffu, okme)) failed = true;
+    for (int k = 0; !okme && k < 1024; k++) okme = mbar_try_wait(&full_bar[0], 0u);
+    if (tid == 0 && okme) seen = 1;
+  }
 
-  for (int c = 0; c < chunks; c++) {
-    __syncthreads();  // staging free; box and field tile ready on the first pass
-#pragma unroll
-    for (int r = 0; r < RUN; r++) {
-      int e = tid + r * PUSH_THREADS;
-      int ow = e / RUN, j = e % RUN;
-      int64_t so = p0 + (n * ow) / PUSH_THREADS, se = p0 + (n * (ow + 1)) / PUSH_THREADS;
-      int64_t m = so + (int64_t)c * RUN + j;
-      if (m < se) {
-        spos[ow * SLOT + j] = gpos[m];
-        svx[ow * SLOT + j] = gvx[m];
-        svy[ow * SLOT + j] = gvy[m];
-        svz[ow * SLOT + j] = gvz[m];
+  for (int r = 0; r < L && !failed; r++) {
+    const int s = r % NSTAGE;
+    uint32_t nextcell = DEAD;
+    bool oknext = false;
+    if (r + 1 < L) {
+      const int s1 = (r + 1) % NSTAGE;
+      const uint32_t par1 = (uint32_t)(((r + 1) / NSTAGE) & 1);
+      oknext = mbar_wait(&full_bar[s1], par1);
+      if (!__any_sync(0xffffffffu, oknext)) {
+        failed = true;
+        break;
+      }
+      for (int k = 0; !oknext && k < 1024; k++) oknext = mbar_try_wait(&full_bar[s1], par1);
+      if (tid == 0 && oknext) seen = r + 2;
+      if (oknext) nextcell = (uint32_t)__float_as_int(stpos[s1 * PUSH_THREADS + tid].w);
+    }
+    const float4 ps = stpos[s * PUSH_THREADS + tid];
+    float vx = stvx[s * PUSH_THREADS + tid];
+    float vy = stvy[s * PUSH_THREADS + tid];
+    float vz = stvz[s * PUSH_THREADS + tid];
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty_bar[s]);
+
+    const uint32_t cell = (uint32_t)__float_as_int(ps.w);
+    bool act = cell != DEAD && okme;
+    okme = oknext;
+    int ib = 0, jb = 0, kb = 0;
+    if (act) {
+      unpack(g, cell, ib, jb, kb);
+      if (ib >= g.nx || jb >= g.ny || kb >= g.nz) {
+        report_bad(a.status, a.diag, SITE_FX_PUSH, slot0 + (int64_t)r * PUSH_THREADS + tid, (long long)cell);
+        act = false;
       }
     }
-    __syncthreads();
-#pragma unroll 1
-    for (int j = 0; j < RUN; j++) {
-      int64_t m = s0 + (int64_t)c * RUN + j;
-      bool act = m < s1;
-      float4 ps = act ? spos[tid * SLOT + j] : make_float4(0.f, 0.f, 0.f, 0.f);
-      uint32_t cell = act ? (uint32_t)__float_as_int(ps.w) : DEAD;
-      act = act && cell != DEAD;
-      int ib = 0, jb = 0, kb = 0;
-      if (act) {
-        unpack(g, cell, ib, jb, kb);
-        if (ib >= g.nx || jb >= g.ny || kb >= g.nz) {
-          report_bad(a.status, a.diag, SITE_FX_PUSH, m, (long long)cell);
-          act = false;
-        }
-      }
-      // ---- the register run follows cell_b; a new cell sends the old sums
-      // through the warp queue
-      uint32_t key = qkey(g, ib, jb, kb);
-      {
-        bool evict = act && key != acckey && acckey != DEAD;
-        unsigned mk = __ballot_sync(0xffffffffu, evict);
-        if (mk) {
-          if (evict) {
-            float* en = queue + (qn + __popc(mk & lt)) * QW;
-#pragma unroll
-            for (int s = 0; s < NJ + NR; s++) en[s] = acc[s];
-            en[NJ + NR] = __int_as_float((int)acckey);
-          }
-          qn += __popc(mk);
-          if (qn >= 16) {
-            drain_queue<B>(sk, g, box, o, slot_off, queue, qn, qfix, lane);
-            qn = 0;
-          }
-        }
-      }
-      if (act && key != acckey) {
-#pragma unroll
-        for (int s = 0; s < NJ + NR; s++) acc[s] = 0.f;
-        acckey = key;
-      }
-
-      // ---- push
-      Axis ax{}, ay{}, az{};
-      bool simple = true, dead = false;
-      float xd2 = 0.f, yd2 = 0.f, zd2 = 0.f, vvx2 = 0.f, vvy2 = 0.f, vvz2 = 0.f;
-      if (act) {
-        float vx = svx[tid * SLOT + j], vy = svy[tid * SLOT + j], vz = svz[tid * SLOT + j];
-        // trilinear weights (psolve1.F90:186-199)
-        float x1 = ps.x, y1 = ps.y, z1 = ps.z;
-        float xy1 = x1 * y1, xz1 = x1 * z1, yz1 = y1 * z1, z2 = 1.0f - z1;
-        float xz2 = x1 * z2, yz2 = y1 * z2;
-        float wv[8];
-        wv[2] = xy1 * z1; wv[1] = xz1 - wv[2]; wv[3] = yz1 - wv[2]; wv[0] = z1 - xz1 - wv[3];
-        wv[6] = xy1 * z2; wv[5] = xz2 - wv[6]; wv[7] = yz2 - wv[6]; wv[4] = z2 - xz2 - wv[7];
-        float eb_e[3], eb_b[3];
-        int li = ib - o[0], lj = jb - o[1], lk = kb - o[2];
-        if ((unsigned)li < (unsigned)(B - 1) && (unsigned)lj < (unsigned)(B - 1) && (unsigned)lk < (unsigned)(B - 1))
-          gather8<true>(sf0, sf1, li + B * lj + (int64_t)B * B * lk, B, (int64_t)B * B, wv, eb_e, eb_b);
-        else
-          gather8<false>(a.f0, a.f1, ib + sy * jb + sz * kb, sy, sz, wv, eb_e, eb_b);
-        // Buneman-Boris (psolve1.F90:247-272)
-        float eex = eb_e[0] * qmp, eey = eb_e[1] * qmp, eez = eb_e[2] * qmp;
-        float bbx = eb_b[0] * qmp, bby = eb_b[1] * qmp, bbz = eb_b[2] * qmp;
-        float boris = 2.0f / (1.0f + bbx * bbx + bby * bby + bbz * bbz);
-        vx += eex; vy += eey; vz += eez;
-        float vxt = vx + vy * bbz - vz * bby;
-        float vyt = vy + vz * bbx - vx * bbz;
-        float vzt = vz + vx * bby - vy * bbx;
-        vx += boris * (vyt * bbz - vzt * bby);
-        vy += boris * (vzt * bbx - vxt * bbz);
-        vz += boris * (vxt * bby - vyt * bbx);
-        vx += eex; vy += eey; vz += eez;
-        ax = axis_move(ib, ps.x, vx * a.gustep, g.nx, nb0);
-        ay = axis_move(jb, ps.y, vy * a.gustep, g.ny, nb1);
-        az = axis_move(kb, ps.z, vz * a.gustep, g.nz, nb2);
-        if (ax.flip) vx = -vx;
-        if (ay.flip) vy = -vy;
-        if (az.flip) vz = -vz;
-        dead = ax.dead || ay.dead || az.dead;
-        if (dead) nesc++;
-        uint32_t nc = dead ? DEAD : pack(g, ax.nc, ay.nc, az.nc);
-        spos[tid * SLOT + j] = make_float4(ax.nf, ay.nf, az.nf, __int_as_float((int)nc));
-        svx[tid * SLOT + j] = vx;
-        svy[tid * SLOT + j] = vy;
-        svz[tid * SLOT + j] = vz;
-        // zigzag (psolve1.F90:717-757), integer parts first; segment 1 goes
-        // to the run of cell_b
-        float xd1 = ((float)(ax.rc - ib) + ax.rf + ps.x) * 0.5f;
-        float yd1 = ((float)(ay.rc - jb) + ay.rf + ps.y) * 0.5f;
-        float zd1 = ((float)(az.rc - kb) + az.rf + ps.z) * 0.5f;
-        float vvx1 = ((float)(ax.rc - ib) + (ax.rf - ps.x)) * a.rustep;
-        float vvy1 = ((float)(ay.rc - jb) + (ay.rf - ps.y)) * a.rustep;
-        float vvz1 = ((float)(az.rc - kb) + (az.rf - ps.z)) * a.rustep;
-        float w;
-        w = yd1 * zd1; acc[3] += vvx1 * w; acc[1] += vvx1 * (yd1 - w); acc[2] += vvx1 * (zd1 - w); acc[0] += vvx1 * (1.0f - yd1 - (zd1 - w));
-        w = xd1 * zd1; acc[7] += vvy1 * w; acc[5] += vvy1 * (xd1 - w); acc[6] += vvy1 * (zd1 - w); acc[4] += vvy1 * (1.0f - xd1 - (zd1 - w));
-        w = xd1 * yd1; acc[11] += vvz1 * w; acc[9] += vvz1 * (xd1 - w); acc[10] += vvz1 * (yd1 - w); acc[8] += vvz1 * (1.0f - xd1 - (yd1 - w));
-        xd2 = ((float)(ax.ac - ax.ia) + ax.af + (float)(ax.rc - ax.ia) + ax.rf) * 0.5f;
-        yd2 = ((float)(ay.ac - ay.ia) + ay.af + (float)(ay.rc - ay.ia) + ay.rf) * 0.5f;
-        zd2 = ((float)(az.ac - az.ia) + az.af + (float)(az.rc - az.ia) + az.rf) * 0.5f;
-        vvx2 = ((float)(ax.ac - ax.rc) + (ax.af - ax.rf)) * a.rustep;
-        vvy2 = ((float)(ay.ac - ay.rc) + (ay.af - ay.rf)) * a.rustep;
-        vvz2 = ((float)(az.ac - az.rc) + (az.af - az.rf)) * a.rustep;
-        simple = !ax.crossed && !ay.crossed && !az.crossed && ax.ia == ib && ay.ia == jb && az.ia == kb;
-      }
-      // ---- segment 2 and the charge: into the run when the cell did not
-      // change, else through the warp queue
-      bool cross = act && !simple;
-      unsigned mk = __ballot_sync(0xffffffffu, cross);
-      float* en = cross ? queue + (qn + __popc(mk & lt)) * QW : nullptr;
-      if (act) {
-        float J2[NJ], R[NR];
-        float w;
-        w = yd2 * zd2; J2[3] = vvx2 * w; J2[1] = vvx2 * (yd2 - w); J2[2] = vvx2 * (zd2 - w); J2[0] = vvx2 * (1.0f - yd2 - (zd2 - w));
-        w = xd2 * zd2; J2[7] = vvy2 * w; J2[5] = vvy2 * (xd2 - w); J2[6] = vvy2 * (zd2 - w); J2[4] = vvy2 * (1.0f - xd2 - (zd2 - w));
-        w = xd2 * yd2; J2[11] = vvz2 * w; J2[9] = vvz2 * (xd2 - w); J2[10] = vvz2 * (yd2 - w); J2[8] = vvz2 * (1.0f - xd2 - (yd2 - w));
-        float X = ax.nf, Y = ay.nf, Z = az.nf;
-        float XY = X * Y, XZ = X * Z, YZ = Y * Z, Z2 = 1.0f - Z, XZ2 = X * Z2, YZ2 = Y * Z2;
-        R[2] = XY * Z; R[1] = XZ - R[2]; R[3] = YZ - R[2]; R[0] = Z - XZ - R[3];
-        R[6] = XY * Z2; R[5] = XZ2 - R[6]; R[7] = YZ2 - R[6]; R[4] = Z2 - XZ2 - R[7];
-        if (simple) {
-#pragma unroll
-          for (int s = 0; s < NJ; s++) acc[s] += J2[s];
-#pragma unroll
-          for (int r = 0; r < NR; r++) acc[NJ + r] += R[r];
-        } else {
-          // the stored cell differs from the after cell only at an outer
-          // boundary (wrap or reflection): that charge goes out directly
-          bool rsplit = dead || ax.nc != ax.ia || ay.nc != ay.ia || az.nc != az.ia;
-          if (rsplit && !dead) {
-            V8 wr;
-#pragma unroll
-            for (int r = 0; r < NR; r++) wr.v[r] = R[r];
-            put_r_global(sk, ax.nc, ay.nc, az.nc, wr, qfix);
-          }
-#pragma unroll
-          for (int s = 0; s < NJ; s++) en[s] = J2[s];
-#pragma unroll
-          for (int r = 0; r < NR; r++) en[NJ + r] = rsplit ? 0.f : R[r];
-          en[NJ + NR] = __int_as_float((int)qkey(g, ax.ia, ay.ia, az.ia));
-        }
-      }
+    // ---- a new cell ends the thread's run (its sums go to the run queue)
+    // when the next particle is in that cell too, or when there is no run
+    const bool newrun = act && cell != runcell && (runbase < 0 || nextcell == cell || nextcell == DEAD);
+    {
+      const bool evict = newrun && runbase >= 0;
+      const unsigned mk = __ballot_sync(0xffffffffu, evict);
       if (mk) {
-        qn += __popc(mk);
-        if (qn >= 16) {
-          drain_queue<B>(sk, g, box, o, slot_off, queue, qn, qfix, lane);
-          qn = 0;
+        if (evict) {
+          float* en = rq + (rqn + __popc(mk & lt)) * RQW;
+#pragma unroll
+          for (int q = 0; q < NJ + NR; q++) en[q] = acc[q];
+          en[NJ + NR] = __int_as_float((int)runcell);
+        }
+        rqn += __popc(mk);
+        if (rqn >= RQ_DRAIN) {
+          drain_runs<B>(g, box, o, slot_off, rq, rqn, qfix, lane);
+          rqn = 0;
         }
       }
     }
-    __syncthreads();
+    if (newrun) {
 #pragma unroll
-    for (int r = 0; r < RUN; r++) {
-      int e = tid + r * PUSH_THREADS;
-      int ow = e / RUN, j = e % RUN;
-      int64_t so = p0 + (n * ow) / PUSH_THREADS, se = p0 + (n * (ow + 1)) / PUSH_THREADS;
-      int64_t m = so + (int64_t)c * RUN + j;
-      if (m < se) {
-        gpos[m] = spos[ow * SLOT + j];
-        gvx[m] = svx[ow * SLOT + j];
-        gvy[m] = svy[ow * SLOT + j];
-        gvz[m] = svz[ow * SLOT + j];
+      for (int q = 0; q < NJ + NR; q++) acc[q] = 0.f;
+      runcell = cell;
+      runbase = box_base<B>(o, ib, jb, kb);
+    }
+
+    // ---- gather + Buneman-Boris (psolve1.F90:186-272)
+    bool simple = false;
+    float sx = 0.f, syy = 0.f, szz = 0.f;
+    if (act) {
+      const float x1 = ps.x, y1 = ps.y, z1 = ps.z;
+      const float xy1 = x1 * y1, xz1 = x1 * z1, yz1 = y1 * z1, z2 = 1.0f - z1;
+      const float xz2 = x1 * z2, yz2 = y1 * z2;
+      float wv[8];
+      wv[2] = xy1 * z1; wv[1] = xz1 - wv[2]; wv[3] = yz1 - wv[2]; wv[0] = z1 - xz1 - wv[3];
+      wv[6] = xy1 * z2; wv[5] = xz2 - wv[6]; wv[7] = yz2 - wv[6]; wv[4] = z2 - xz2 - wv[7];
+      float fe[3], fb[3];
+      const int gb = cell == runcell ? runbase : box_base<B>(o, ib, jb, kb);
+      if (gb >= 0)
+        gather8_smem<B>(sf0, sf1, gb, wv, fe, fb);
+      else
+        gather8<false>(a.f0, a.f1, ib + sy * jb + sz * kb, sy, sz, wv, fe, fb);
+      const float eex = fe[0] * qmp, eey = fe[1] * qmp, eez = fe[2] * qmp;
+      const float bbx = fb[0] * qmp, bby = fb[1] * qmp, bbz = fb[2] * qmp;
+      const float boris = __fdividef(2.0f, 1.0f + bbx * bbx + bby * bby + bbz * bbz);
+      vx += eex; vy += eey; vz += eez;
+      const float vxt = vx + vy * bbz - vz * bby;
+      const float vyt = vy + vz * bbx - vx * bbz;
+      const float vzt = vz + vx * bby - vy * bbx;
+      vx += boris * (vyt * bbz - vzt * bby);
+      vy += boris * (vzt * bbx - vxt * bbz);
+      vz += boris * (vxt * bby - vyt * bbx);
+      vx += eex; vy += eey; vz += eez;
+      sx = x1 + vx * gustep;
+      syy = y1 + vy * gustep;
+      szz = z1 + vz * gustep;
+      simple = cell == runcell && runbase >= 0 && sx >= 0.f && sx < 1.0f && syy >= 0.f && syy < 1.0f && szz >= 0.f && szz < 1.0f;
+    }
+    if (simple) {
+      // both zigzag segments in the same cell: relay point at the midpoint,
+      // equal segment fluxes h = (a-b)/2/ustep, mid-points m -+ (a-b)/4; the
+      // sum of the two bilinear weight sets is written with S = a+b, D = a-b
+      const float Sx = sx + ps.x, Sy = syy + ps.y, Sz = szz + ps.z;
+      const float Dx = sx - ps.x, Dy = syy - ps.y, Dz = szz - ps.z;
+      const float hx = Dx * hr, hy = Dy * hr, hz = Dz * hr;
+      float P;
+      P = 0.5f * Sy * Sz + 0.125f * Dy * Dz;
+      acc[3] += hx * P; acc[1] += hx * (Sy - P); acc[2] += hx * (Sz - P); acc[0] += hx * (2.0f - Sy - Sz + P);
+      P = 0.5f * Sx * Sz + 0.125f * Dx * Dz;
+      acc[7] += hy * P; acc[5] += hy * (Sx - P); acc[6] += hy * (Sz - P); acc[4] += hy * (2.0f - Sx - Sz + P);
+      P = 0.5f * Sx * Sy + 0.125f * Dx * Dy;
+      acc[11] += hz * P; acc[9] += hz * (Sx - P); acc[10] += hz * (Sy - P); acc[8] += hz * (2.0f - Sx - Sy + P);
+      // CIC charge at the new position (charge.F90:152-210)
+      const float XY = sx * syy, XZ = sx * szz, YZ = syy * szz, Z2 = 1.0f - szz, XZ2 = sx * Z2, YZ2 = syy * Z2;
+      const float r2 = XY * szz, r6 = XY * Z2;
+      const float r3 = YZ - r2, r7 = YZ2 - r6;
+      acc[NJ + 2] += r2; acc[NJ + 1] += XZ - r2; acc[NJ + 3] += r3; acc[NJ + 0] += szz - XZ - r3;
+      acc[NJ + 6] += r6; acc[NJ + 5] += XZ2 - r6; acc[NJ + 7] += r7; acc[NJ + 4] += Z2 - XZ2 - r7;
+      const int m = r * PUSH_THREADS + tid;
+      gpos[m] = make_float4(sx, syy, szz, ps.w);
+      gvx[m] = vx;
+      gvy[m] = vy;
+      gvz[m] = vz;
+    }
+    // ---- cell-crossing particles: the warp's cross queue
+    const bool cross = act && !simple;
+    const unsigned xm = __ballot_sync(0xffffffffu, cross);
+    if (xm) {
+      if (cross) {
+        float* en = xq + (xqn + __popc(xm & lt)) * XQW;
+        en[0] = __int_as_float(r * PUSH_THREADS + tid);
+        en[1] = ps.w;
+        en[2] = ps.x; en[3] = ps.y; en[4] = ps.z;
+        en[5] = vx; en[6] = vy; en[7] = vz;
+      }
+      xqn += __popc(xm);
+      if (xqn >= XQ_DRAIN) {
+        nesc += drain_cross<B>(a, is, slot0, box, o, xq, xqn, lane);
+        xqn = 0;
       }
     }
   }
-  // the last run of every thread
+  if (failed) report_bad(a.status, a.diag, SITE_FX_PUSH, -3, t);
+  // the last run of every thread, and what is left in the queues
   {
-    bool has = acckey != DEAD;
-    unsigned mk = __ballot_sync(0xffffffffu, has);
+    const bool has = runbase >= 0;
+    const unsigned mk = __ballot_sync(0xffffffffu, has);
     if (has) {
-      float* en = queue + (qn + __popc(mk & lt)) * QW;
+      float* en = rq + (rqn + __popc(mk & lt)) * RQW;
 #pragma unroll
-      for (int s = 0; s < NJ + NR; s++) en[s] = acc[s];
-      en[NJ + NR] = __int_as_float((int)acckey);
+      for (int q = 0; q < NJ + NR; q++) en[q] = acc[q];
+      en[NJ + NR] = __int_as_float((int)runcell);
     }
-    qn += __popc(mk);
-    if (qn) drain_queue<B>(sk, g, box, o, slot_off, queue, qn, qfix, lane);
+    rqn += __popc(mk);
+    if (rqn) drain_runs<B>(g, box, o, slot_off, rq, rqn, qfix, lane);
+    if (xqn) nesc += drain_cross<B>(a, is, slot0, box, o, xq, xqn, lane);
   }
   if (nesc) atomicAdd(&a.nesc[is], nesc);
+  if (tid == 0) rows_seen = seen;
+  }  // pushing warps
   __syncthreads();
+  // copies still in flight after a failed wait complete before the CTA exits
+  if (warp == PUSH_WARPS && lane == 0)
+    for (int r = rows_seen; r < issued; r++) (void)mbar_wait(&full_bar[r % NSTAGE], (uint32_t)((r / NSTAGE) & 1));
   // add the tile accumulator into the global int64 arrays
-  for (int e = tid; e < NBOX; e += PUSH_THREADS) {
+  for (int e = tid; e < NBOX; e += PUSH_BLOCK) {
     unsigned long long v = box[e];
     if (v == 0ull) continue;
     int li = e % B, lj = (e / B) % B, lk = (e / (B * B)) % B, comp = e / (B * B * B);
@@ -548,6 +769,7 @@ inline int fx_box_tile(int tmax) { return tmax <= 4 ? 4 : 8; }
 inline int fx_push_smem(int tmax) {
   int B = fx_box_tile(tmax) + 2 * PG + 1;
   int nf = B * B * B;
-  return 4 * nf * (int)sizeof(unsigned long long) + nf * (int)(sizeof(float4) + sizeof(float2)) +
-         PUSH_THREADS * SLOT * (int)(sizeof(float4) + 3 * sizeof(float)) + PUSH_WARPS * QCAP * QW * (int)sizeof(float);
+  return 4 * nf * (int)sizeof(unsigned long long) + NSTAGE * (int)ROW_BYTES +
+         nf * (int)(sizeof(float4) + sizeof(float2)) +
+         PUSH_WARPS * (RQCAP * RQW + XQCAP * XQW) * (int)sizeof(float);
 }

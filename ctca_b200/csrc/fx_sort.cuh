@@ -1,0 +1,408 @@
+// fx_sort.cuh -- the tile-local counting sort of the FP32 form (included by
+// fx.cu inside its private namespace, after fx_push.cuh).
+//
+// Between two sorts a particle moves by a fraction of a cell per step, so
+// every particle of source tile t (its region of the last sort) lies in the
+// "sort box" of t: the tile's cells plus one cell on every side (wrapped on
+// the species' periodic axes).  The re-sort is then a counting sort whose
+// buckets are cells, organised per source tile:
+//
+//   count   per (source tile, warp, box cell) counts of the live particles;
+//   celltot per destination cell: the sum over the (at most 27) source tiles
+//           whose box holds the cell; per destination tile: its total;
+//   tiles   exclusive scan of the tile totals -> tile_start, tile_pad;
+//   bases   per destination cell: its first rank (tile_start + scan over the
+//           tile's cells), handed out to the source tiles in increasing tile
+//           index: base[t'][bc'] = first rank of the cell's particles that
+//           come from tile t'; empty slots of the new regions get DEAD;
+//   rank    per source tile: each particle's rank = base[t][bc] + the counts
+//           of the same cell in the tile's lower warps + its rank inside its
+//           warp (rows in order, lanes in order, __match_any_sync) gives its
+//           slot in the thread-major region of its new tile: inv[slot] = old
+//           slot (4-byte scattered writes);
+//   move    per destination tile, in groups of 32 columns: a window of the
+//           tile's old region is staged in shared memory (coalesced rows)
+//           and every slot takes its particle from the window or, for
+//           particles from other tiles, from global memory (coalesced
+//           writes).
+//
+// The order of equal-cell particles is thus (source tile, warp, row, lane):
+// fixed by the data, so the sort is deterministic, and a particle is read
+// twice (16 bytes to count and rank, 28 to move) and written once (28
+// bytes), plus 4-byte slot indices.  Dead
+// particles and empty slots are dropped (the compaction).  A particle outside
+// its tile's sort box, or more than 65535 particles of one cell in one warp,
+// sets the stray flag; the host then sorts with the radix path instead.
+
+struct LcsGeo {
+  int n[3];      // grid cells
+  int t[3];      // tile edge
+  int nt[3];     // tiles per axis
+  int bc[3];     // sort-box edge = t + 2
+  int nbc;       // box cells
+  int tcells;    // t[0]*t[1]*t[2]
+  bool wrap[3];  // periodic particle axis (npbnd == 0)
+};
+
+__device__ __forceinline__ int lcs_axis(const LcsGeo& G, int d, int tile, int i) {
+  int l = i - (tile * G.t[d] - 1);
+  if (G.wrap[d]) {
+    if (l < 0) l += G.n[d];
+    else if (l >= G.n[d]) l -= G.n[d];
+  }
+  return (l >= 0 && l < G.bc[d]) ? l : -1;
+}
+
+// Box cell of cell (i,j,k) in the sort box of tile (tx,ty,tz), or -1.
+__device__ __forceinline__ int lcs_box_cell(const LcsGeo& G, int tx, int ty, int tz, int i, int j, int k) {
+  int a = lcs_axis(G, 0, tx, i), b = lcs_axis(G, 1, ty, j), c = lcs_axis(G, 2, tz, k);
+  if (a < 0 || b < 0 || c < 0) return -1;
+  return a + G.bc[0] * (b + G.bc[1] * c);
+}
+
+// Tiles along one axis whose sort box may hold cell index i, ascending,
+// without repeats.
+__device__ __forceinline__ int lcs_cand(const LcsGeo& G, int d, int i, int (&out)[3]) {
+  const int c = i / G.t[d];
+  int m = 0;
+  int v[3] = {c - 1, c, c + 1};
+  int w[3];
+  for (int q = 0; q < 3; q++) {
+    int x = v[q];
+    if (x < 0 || x >= G.nt[d]) {
+      if (!G.wrap[d]) continue;
+      x = (x + G.nt[d]) % G.nt[d];
+    }
+    w[m++] = x;
+  }
+  // sort the (at most 3) entries and drop repeats
+  for (int a = 1; a < m; a++)
+    for (int b = a; b > 0 && w[b - 1] > w[b]; b--) { int s = w[b]; w[b] = w[b - 1]; w[b - 1] = s; }
+  int k = 0;
+  for (int a = 0; a < m; a++)
+    if (k == 0 || out[k - 1] != w[a]) out[k++] = w[a];
+  return k;
+}
+
+__device__ __forceinline__ void tile_xyz(const Geo& g, int64_t t, int& tx, int& ty, int& tz) {
+  tx = (int)(t % g.nt[0]);
+  ty = (int)((t / g.nt[0]) % g.nt[1]);
+  tz = (int)(t / ((int64_t)g.nt[0] * g.nt[1]));
+}
+
+// count: per (source tile, warp, box cell).  grid = ntiles, block = PUSH_THREADS.
+__global__ void __launch_bounds__(PUSH_THREADS) k_lcs_count(const float4* __restrict__ pos,
+                                                            const int64_t* __restrict__ ts,
+                                                            const int64_t* __restrict__ tp, Geo g, LcsGeo G,
+                                                            uint16_t* __restrict__ wcnt, uint32_t* __restrict__ cnt,
+                                                            int* stray) {
+  extern __shared__ uint32_t hist[];  // [PUSH_WARPS][nbc]
+  const int t = blockIdx.x, tid = threadIdx.x, warp = tid >> 5;
+  for (int e = tid; e < PUSH_WARPS * G.nbc; e += PUSH_THREADS) hist[e] = 0;
+  __syncthreads();
+  int tx, ty, tz;
+  tile_xyz(g, t, tx, ty, tz);
+  const int64_t n = ts[t + 1] - ts[t];
+  const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
+  bool bad = false;
+  const float4* src = pos + tp[t];
+#pragma unroll 4
+  for (int r = 0; r < L; r++) {
+    const uint32_t cell = (uint32_t)__float_as_int(src[r * PUSH_THREADS + tid].w);
+    if (cell == DEAD) continue;
+    int i, j, k;
+    unpack(g, cell, i, j, k);
+    const int bc = lcs_box_cell(G, tx, ty, tz, i, j, k);
+    if (bc < 0) { bad = true; continue; }
+    atomicAdd(&hist[warp * G.nbc + bc], 1u);
+  }
+  __syncthreads();
+  uint16_t* wc = wcnt + (int64_t)t * PUSH_WARPS * G.nbc;
+  uint32_t* c = cnt + (int64_t)t * G.nbc;
+  for (int b = tid; b < G.nbc; b += PUSH_THREADS) {
+    uint32_t sum = 0;
+    for (int w = 0; w < PUSH_WARPS; w++) {
+      uint32_t h = hist[w * G.nbc + b];
+      if (h > 65535u) bad = true;
+      wc[w * G.nbc + b] = (uint16_t)h;
+      sum += h;
+    }
+    c[b] = sum;
+  }
+  if (bad) atomicOr(stray, 1);
+}
+
+// celltot: per destination cell, the sum over the source tiles holding it;
+// per destination tile its total.  grid = ntiles, block = PUSH_THREADS (>= tcells).
+__global__ void __launch_bounds__(PUSH_THREADS) k_lcs_celltot(const uint32_t* __restrict__ cnt, Geo g, LcsGeo G,
+                                                              uint32_t* __restrict__ celltot,
+                                                              int64_t* __restrict__ tiletot) {
+  __shared__ uint32_t part[PUSH_WARPS];
+  const int t = blockIdx.x, tid = threadIdx.x;
+  int tx, ty, tz;
+  tile_xyz(g, t, tx, ty, tz);
+  uint32_t tot = 0;
+  if (tid < G.tcells) {
+    const int i = tx * G.t[0] + tid % G.t[0];
+    const int j = ty * G.t[1] + (tid / G.t[0]) % G.t[1];
+    const int k = tz * G.t[2] + tid / (G.t[0] * G.t[1]);
+    if (i < G.n[0] && j < G.n[1] && k < G.n[2]) {
+      int cx[3], cy[3], cz[3];
+      const int mx = lcs_cand(G, 0, i, cx), my = lcs_cand(G, 1, j, cy), mz = lcs_cand(G, 2, k, cz);
+      for (int c = 0; c < mz; c++)
+        for (int b = 0; b < my; b++)
+          for (int a = 0; a < mx; a++) {
+            const int bc = lcs_box_cell(G, cx[a], cy[b], cz[c], i, j, k);
+            if (bc < 0) continue;
+            const int64_t tt = cx[a] + (int64_t)g.nt[0] * (cy[b] + (int64_t)g.nt[1] * cz[c]);
+            tot += cnt[tt * G.nbc + bc];
+          }
+    }
+    celltot[(int64_t)t * G.tcells + tid] = tot;
+  }
+  // block sum
+  uint32_t v = tot;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((tid & 31) == 0) part[tid >> 5] = v;
+  __syncthreads();
+  if (tid == 0) {
+    int64_t s = 0;
+    for (int w = 0; w < PUSH_WARPS; w++) s += part[w];
+    tiletot[t] = s;
+  }
+}
+
+// tiles: exclusive scan of the tile totals (one block of 1024 threads):
+// tile_start, tile_pad (whole rows per tile), live count and slot count.
+__global__ void __launch_bounds__(1024) k_lcs_tiles(const int64_t* __restrict__ tiletot, int64_t ntiles,
+                                                    int64_t* ts, int64_t* tp, int64_t* count, int64_t* slots) {
+  __shared__ int64_t pa[1024], pb[1024];
+  const int tid = threadIdx.x;
+  const int64_t per = (ntiles + 1023) / 1024;
+  const int64_t t0 = tid * per, t1 = min(ntiles, t0 + per);
+  int64_t sa = 0, sb = 0;
+  for (int64_t t = t0; t < t1; t++) {
+    sa += tiletot[t];
+    sb += (tiletot[t] + PUSH_THREADS - 1) / PUSH_THREADS * PUSH_THREADS;
+  }
+  pa[tid] = sa;
+  pb[tid] = sb;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    int64_t va = tid >= d ? pa[tid - d] : 0, vb = tid >= d ? pb[tid - d] : 0;
+    __syncthreads();
+    pa[tid] += va;
+    pb[tid] += vb;
+    __syncthreads();
+  }
+  int64_t ra = pa[tid] - sa, rb = pb[tid] - sb;
+  for (int64_t t = t0; t < t1; t++) {
+    ts[t] = ra;
+    tp[t] = rb;
+    ra += tiletot[t];
+    rb += (tiletot[t] + PUSH_THREADS - 1) / PUSH_THREADS * PUSH_THREADS;
+  }
+  if (tid == 1023) {
+    ts[ntiles] = pa[1023];
+    tp[ntiles] = pb[1023];
+    *count = pa[1023];
+    *slots = pb[1023];
+  }
+}
+
+// bases: first rank of every (source tile, box cell); DEAD in the empty
+// slots of the new region.  grid = ntiles (destination tiles), block = PUSH_THREADS.
+__global__ void __launch_bounds__(PUSH_THREADS) k_lcs_bases(const uint32_t* __restrict__ cnt,
+                                                            const uint32_t* __restrict__ celltot, Geo g, LcsGeo G,
+                                                            const int64_t* __restrict__ ts,
+                                                            const int64_t* __restrict__ tp, uint32_t* __restrict__ base,
+                                                            uint32_t* __restrict__ inv) {
+  __shared__ uint32_t sc[PUSH_THREADS];
+  const int t = blockIdx.x, tid = threadIdx.x;
+  int tx, ty, tz;
+  tile_xyz(g, t, tx, ty, tz);
+  const uint32_t mine = tid < G.tcells ? celltot[(int64_t)t * G.tcells + tid] : 0u;
+  // exclusive scan over the tile's cells (cell order = the sort key order)
+  sc[tid] = mine;
+  __syncthreads();
+  for (int d = 1; d < PUSH_THREADS; d <<= 1) {
+    uint32_t v = tid >= d ? sc[tid - d] : 0u;
+    __syncthreads();
+    sc[tid] += v;
+    __syncthreads();
+  }
+  if (tid < G.tcells) {
+    const int i = tx * G.t[0] + tid % G.t[0];
+    const int j = ty * G.t[1] + (tid / G.t[0]) % G.t[1];
+    const int k = tz * G.t[2] + tid / (G.t[0] * G.t[1]);
+    if (i < G.n[0] && j < G.n[1] && k < G.n[2]) {
+      uint32_t run = (uint32_t)ts[t] + sc[tid] - mine;
+      int cx[3], cy[3], cz[3];
+      const int mx = lcs_cand(G, 0, i, cx), my = lcs_cand(G, 1, j, cy), mz = lcs_cand(G, 2, k, cz);
+      for (int c = 0; c < mz; c++)
+        for (int b = 0; b < my; b++)
+          for (int a = 0; a < mx; a++) {
+            const int bc = lcs_box_cell(G, cx[a], cy[b], cz[c], i, j, k);
+            if (bc < 0) continue;
+            const int64_t tt = cx[a] + (int64_t)g.nt[0] * (cy[b] + (int64_t)g.nt[1] * cz[c]);
+            base[tt * G.nbc + bc] = run;
+            run += cnt[tt * G.nbc + bc];
+          }
+    }
+  }
+  // empty slots of the new region
+  const int64_t n = ts[t + 1] - ts[t];
+  if (n > 0) {
+    const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
+    for (int64_t q = n + tid; q < (int64_t)L * PUSH_THREADS; q += PUSH_THREADS) {
+      const int64_t slot = tp[t] + (q % L) * PUSH_THREADS + q / L;
+      inv[slot] = DEAD;
+    }
+  }
+}
+
+// rank: every live particle of source tile t gets its slot in the new
+// regions; inv[new slot] = old slot.  grid = ntiles, block = PUSH_THREADS,
+// shared = PUSH_WARPS * nbc * 4.
+__global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restrict__ pos,
+                                                           const int64_t* __restrict__ ts,
+                                                           const int64_t* __restrict__ tp, Geo g, LcsGeo G,
+                                                           const uint16_t* __restrict__ wcnt,
+                                                           const uint32_t* __restrict__ base,
+                                                           const int64_t* __restrict__ ts2,
+                                                           const int64_t* __restrict__ tp2, uint32_t* __restrict__ inv,
+                                                           int* status, long long* diag) {
+  extern __shared__ uint32_t wb[];  // [PUSH_WARPS][nbc] next rank of (warp, box cell)
+  const int t = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const uint16_t* wc = wcnt + (int64_t)t * PUSH_WARPS * G.nbc;
+  for (int b = tid; b < G.nbc; b += PUSH_THREADS) {
+    uint32_t run = base[(int64_t)t * G.nbc + b];
+    for (int w = 0; w < PUSH_WARPS; w++) {
+      wb[w * G.nbc + b] = run;
+      run += wc[w * G.nbc + b];
+    }
+  }
+  __syncthreads();
+  int tx, ty, tz;
+  tile_xyz(g, t, tx, ty, tz);
+  const int64_t n = ts[t + 1] - ts[t];
+  const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
+  const int64_t s0 = tp[t];
+  uint32_t* mywb = wb + warp * G.nbc;
+  for (int r = 0; r < L; r++) {
+    const int64_t m = s0 + (int64_t)r * PUSH_THREADS + tid;
+    const uint32_t cell = (uint32_t)__float_as_int(pos[m].w);
+    int i = 0, j = 0, k = 0, bc = -1;
+    if (cell != DEAD) {
+      unpack(g, cell, i, j, k);
+      bc = lcs_box_cell(G, tx, ty, tz, i, j, k);  // >= 0: strays sort with the radix path
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, bc);
+    const uint32_t rank = bc >= 0 ? mywb[bc] + __popc(peers & lt) : 0u;
+    __syncwarp();
+    if (bc >= 0 && (peers & lt) == 0) mywb[bc] += __popc(peers);
+    __syncwarp();
+    if (bc < 0) continue;
+    // destination tile and its thread-major slot
+    const int64_t td = (int64_t)(i / g.t[0]) + (int64_t)g.nt[0] * ((j / g.t[1]) + (int64_t)g.nt[1] * (k / g.t[2]));
+    const int64_t q = (int64_t)rank - ts2[td];
+    const int64_t nd = ts2[td + 1] - ts2[td];
+    if (q < 0 || q >= nd) {
+      report_bad(status, diag, SITE_FX_SORT, m, (long long)cell);
+      continue;
+    }
+    const int64_t Ld = (nd + PUSH_THREADS - 1) / PUSH_THREADS;
+    inv[tp2[td] + (q % Ld) * PUSH_THREADS + q / Ld] = (uint32_t)m;
+  }
+}
+
+// move: the new region of destination tile t, in groups of 32 columns.  A
+// particle that stayed in its tile keeps about its column (its rank moves by
+// the net count change of the cells before it), so each group first stages a
+// window of MOVE_WCOLS source columns (all rows of the tile's old region,
+// coalesced rows) in shared memory, centred on the old column of the group's
+// middle slot, and then writes its slots row by row (coalesced), taking each
+// particle from the window or, when it came from elsewhere, from global
+// memory.  grid = ntiles, block = PUSH_THREADS, shared = move_smem().
+constexpr int MOVE_WCOLS = 40;
+constexpr int MOVE_MAXROWS = 80;  // two CTAs per SM
+inline int move_smem() { return MOVE_MAXROWS * MOVE_WCOLS * (16 + 3 * 4); }
+
+__global__ void __launch_bounds__(PUSH_THREADS) k_lcs_move(const float4* __restrict__ pos, const float* __restrict__ vx,
+                                                           const float* __restrict__ vy, const float* __restrict__ vz,
+                                                           const int64_t* __restrict__ ts,
+                                                           const int64_t* __restrict__ tp,
+                                                           const int64_t* __restrict__ ts2,
+                                                           const int64_t* __restrict__ tp2,
+                                                           const uint32_t* __restrict__ inv, float4* __restrict__ pos2,
+                                                           float* __restrict__ vx2, float* __restrict__ vy2,
+                                                           float* __restrict__ vz2) {
+  extern __shared__ float4 wpos[];  // [rows][MOVE_WCOLS], then wvx, wvy, wvz
+  __shared__ int wlo;
+  const int t = blockIdx.x, tid = threadIdx.x;
+  const int64_t nd = ts2[t + 1] - ts2[t];
+  if (nd <= 0) return;
+  const int Ld = (int)((nd + PUSH_THREADS - 1) / PUSH_THREADS);
+  const int64_t ns = ts[t + 1] - ts[t];
+  const int Ls = (int)((ns + PUSH_THREADS - 1) / PUSH_THREADS);
+  const int64_t sbase = tp[t], send = sbase + (int64_t)Ls * PUSH_THREADS;
+  const bool win = ns > 0 && Ls <= MOVE_MAXROWS;
+  float* wvx = reinterpret_cast<float*>(wpos + MOVE_MAXROWS * MOVE_WCOLS);
+  float* wvy = wvx + MOVE_MAXROWS * MOVE_WCOLS;
+  float* wvz = wvy + MOVE_MAXROWS * MOVE_WCOLS;
+  const int64_t d0 = tp2[t];
+  for (int c0 = 0; c0 < PUSH_THREADS; c0 += 32) {
+    if (win) {
+      if (tid == 0) {
+        const uint32_t s = inv[d0 + (int64_t)(Ld / 2) * PUSH_THREADS + c0 + 16];
+        int col = c0 + 16;
+        if (s != DEAD && (int64_t)s >= sbase && (int64_t)s < send) col = (int)(((int64_t)s - sbase) % PUSH_THREADS);
+        wlo = min(max(col - MOVE_WCOLS / 2, 0), PUSH_THREADS - MOVE_WCOLS);
+      }
+      __syncthreads();
+      const int lo = wlo;
+#pragma unroll 4
+      for (int e = tid; e < Ls * MOVE_WCOLS; e += PUSH_THREADS) {
+        const int64_t gs = sbase + (int64_t)(e / MOVE_WCOLS) * PUSH_THREADS + lo + e % MOVE_WCOLS;
+        wpos[e] = pos[gs];
+        wvx[e] = vx[gs];
+        wvy[e] = vy[gs];
+        wvz[e] = vz[gs];
+      }
+      __syncthreads();
+    }
+    const int lo = win ? wlo : 0;
+#pragma unroll 2
+    for (int e = tid; e < Ld * 32; e += PUSH_THREADS) {
+      const int64_t m = d0 + (int64_t)(e >> 5) * PUSH_THREADS + c0 + (e & 31);
+      const uint32_t src = inv[m];
+      float4 p;
+      float a, b, c;
+      if (src == DEAD) {
+        p = make_float4(0.f, 0.f, 0.f, __int_as_float((int)DEAD));
+        a = b = c = 0.f;
+      } else {
+        const int64_t rel = (int64_t)src - sbase;
+        const int cc = win && rel >= 0 && (int64_t)src < send ? (int)(rel % PUSH_THREADS) - lo : -1;
+        if (cc >= 0 && cc < MOVE_WCOLS) {
+          const int w = (int)(rel / PUSH_THREADS) * MOVE_WCOLS + cc;
+          p = wpos[w];
+          a = wvx[w];
+          b = wvy[w];
+          c = wvz[w];
+        } else {
+          p = pos[src];
+          a = vx[src];
+          b = vy[src];
+          c = vz[src];
+        }
+      }
+      pos2[m] = p;
+      vx2[m] = a;
+      vy2[m] = b;
+      vz2[m] = c;
+    }
+    if (win) __syncthreads();  // the window is reloaded for the next group
+  }
+}

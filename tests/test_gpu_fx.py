@@ -128,3 +128,58 @@ def test_fx_escape_counts(gpu):
     g.fx_sort()
     assert np.array_equal(g.fx_counts(), [(o.pbuf[:o.totalp[0]]["nid"] != -1).sum(),
                                           (o.pbuf[o.totalp[0]:]["nid"] != -1).sum()])
+
+
+def _tile_key(cfg, tile, p):
+    i, j, k = np.floor(p["x"]).astype(int), np.floor(p["y"]).astype(int), np.floor(p["z"]).astype(int)
+    nt = [-(-n // t) for n, t in zip((cfg.nx, cfg.ny, cfg.nz), tile)]
+    tid = i // tile[0] + nt[0] * (j // tile[1] + nt[1] * (k // tile[2]))
+    lin = i % tile[0] + tile[0] * (j % tile[1] + tile[1] * (k % tile[2]))
+    return tid * (tile[0] * tile[1] * tile[2]) + lin, tid
+
+
+@pytest.mark.parametrize("npbnd,tile", [((0, 0, 0), (8, 8, 8)), ((1, 2, 0), (8, 4, 8))])
+def test_fx_local_sort_is_a_stable_cell_sort(gpu, npbnd, tile):
+    """The re-sort after a step (the tile-local counting sort) orders the
+    live particles by the tile-major cell key; equal cells keep the order
+    (source tile, warp, row, lane) of the thread-major layout of the last
+    sort, computed here from the tile sizes of that sort."""
+    threads = 512
+    c = case(n=(16, 16, 16), ppc=(8, 8), npbnd=npbnd, vth_scale=6.0, tile=tile)
+    cfg, eb, p, tp = build(c)
+    g = Emses(cfg)
+    g.upload_particles(p, tp)
+    g.upload_field("eb", eb)
+    g.fx_load()
+    g.fx_store()
+    p0, tp0 = g.download_particles()   # sorted; cells of the last sort
+    g.fx_step(2, False)
+    g.fx_store()
+    p1, tp1 = g.download_particles()   # same order, moved
+    g.fx_sort()
+    g.fx_store()
+    p2, tp2 = g.download_particles()
+    base0 = np.concatenate([[0], np.cumsum(tp0)])
+    for s in range(cfg.nspec):
+        a0 = p0[base0[s]:base0[s] + tp0[s]]
+        a1 = p1[base0[s]:base0[s] + tp0[s]]
+        _, t0 = _tile_key(cfg, tile, a0)
+        ntile = int(t0.max()) + 1
+        counts = np.bincount(t0, minlength=ntile)
+        starts = np.concatenate([[0], np.cumsum(counts)])
+        q = np.arange(a0.size) - starts[t0]
+        L = -(-counts[t0] // threads)
+        col, row = q // L, q % L
+        src = np.lexsort((col % 32, row, col // 32, t0))  # (tile, warp, row, lane)
+        order_pos = np.empty(a0.size, dtype=np.int64)
+        order_pos[src] = np.arange(a0.size)
+        live = a1["nid"] != -1
+        key1, _ = _tile_key(cfg, tile, a1)
+        idx = np.flatnonzero(live)
+        exp = idx[np.lexsort((order_pos[idx], key1[idx]))]
+        base2 = int(np.sum(tp2[:s]))
+        got = p2[base2:base2 + tp2[s]]
+        assert tp2[s] == live.sum()
+        for f in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.array_equal(got[f], a1[exp][f]), (s, f)
+    g.close()
