@@ -255,6 +255,91 @@ __global__ void k_psolve2(PushArgs a) {
   a.p[m] = p;
 }
 
+// positn, src/pcl/positn.F90:50-355: position-only advance (x += v*ustep;
+// injected particles still draw, :97-101), outer boundary with nesc counted
+// per escaping axis (:228-268), body test with the box bounds as the
+// cylinder's axial extent (:283-316).  One thread per particle.
+__global__ void k_positn(PushArgs a) {
+  int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.n || m >= *a.count) return;
+  const emsesg_config* c = a.cfg;
+  emsesg_particle p = a.p[m];
+  double gustep, qmp;
+  if (!push_status(a, m, p, gustep, qmp)) { a.p[m] = p; return; }
+  const double dxl = 0.0, dyl = 0.0, dzl = 0.0;
+  const double dxu = c->nx, dyu = c->ny, dzu = c->nz;
+  const double slx = c->nx, sly = c->ny, slz = c->nz;
+  const double tslx = 2.0 * slx, tsly = 2.0 * sly, tslz = 2.0 * slz;
+  const double us = (double)a.ustep;
+  double xmove = p.vx * us, ymove = p.vy * us, zmove = p.vz * us;
+  p.x = p.x + xmove;
+  p.y = p.y + ymove;
+  p.z = p.z + zmove;
+  int nud = 14;
+  if (p.x < dxl) nud -= 1; else if (p.x >= dxu) nud += 1;
+  if (p.y < dyl) nud -= 3; else if (p.y >= dyu) nud += 3;
+  if (p.z < dzl) nud -= 9; else if (p.z >= dzu) nud += 9;
+  if (nud != 14) {
+    const int32_t* nb = c->npbnd[a.is];
+    p.nid = nborps_single(nb, p.x < dxl || p.x >= dxu, p.y < dyl || p.y >= dyu, p.z < dzl || p.z >= dzu);
+    int esc = 0;
+    if (p.x < 0.0) {
+      if (nb[0] == 0) p.x = p.x + slx;
+      else if (nb[0] == 1) { p.x = -p.x; p.vx = -p.vx; }
+      else esc++;
+    } else if (p.x >= slx) {
+      if (nb[0] == 0) p.x = p.x - slx;
+      else if (nb[0] == 1) { p.x = tslx - p.x; p.vx = -p.vx; }
+      else esc++;
+    }
+    if (p.y < 0.0) {
+      if (nb[1] == 0) p.y = p.y + sly;
+      else if (nb[1] == 1) { p.y = -p.y; p.vy = -p.vy; }
+      else esc++;
+    } else if (p.y >= sly) {
+      if (nb[1] == 0) p.y = p.y - sly;
+      else if (nb[1] == 1) { p.y = tsly - p.y; p.vy = -p.vy; }
+      else esc++;
+    }
+    if (p.z < 0.0) {
+      if (nb[2] == 0) p.z = p.z + slz;
+      else if (nb[2] == 1) { p.z = -p.z; p.vz = -p.vz; }
+      else esc++;
+    } else if (p.z >= slz) {
+      if (nb[2] == 0) p.z = p.z - slz;
+      else if (nb[2] == 1) { p.z = tslz - p.z; p.vz = -p.vz; }
+      else esc++;
+    }
+    if (esc) atomicAdd(&a.gc->nesc[a.is], esc);
+  }
+  if (c->line_mode != 1) {
+    for (int ipc = 0; ipc < c->npc; ipc++) {
+      if (p.nid == -1) continue;
+      const emsesg_body& b = c->body[ipc];
+      bool kill = false;
+      if ((b.geotype == 0 || b.geotype == 1) &&
+          (p.x >= b.xlpc && p.x <= b.xupc && p.y >= b.ylpc && p.y <= b.yupc && p.z >= b.zlpc && p.z <= b.zupc)) {
+        kill = true;
+      } else if (b.geotype == 2) {
+        double d1, d2, ax, lo, hi;
+        if (b.cyl_align == 1) { d1 = p.y - b.cyl_axis[0]; d2 = p.z - b.cyl_axis[1]; ax = p.x; lo = b.xlpc; hi = b.xupc; }
+        else if (b.cyl_align == 2) { d1 = p.z - b.cyl_axis[0]; d2 = p.x - b.cyl_axis[1]; ax = p.y; lo = b.ylpc; hi = b.yupc; }
+        else if (b.cyl_align == 3) { d1 = p.x - b.cyl_axis[0]; d2 = p.y - b.cyl_axis[1]; ax = p.z; lo = b.zlpc; hi = b.zupc; }
+        else continue;
+        if (ax >= lo && ax <= hi && d1 * d1 + d2 * d2 < b.radius * b.radius) kill = true;
+      } else if (b.geotype == 3) {
+        double d1 = p.x - b.sph_center[0], d2 = p.y - b.sph_center[1], d3 = p.z - b.sph_center[2];
+        if (d1 * d1 + d2 * d2 + d3 * d3 < b.radius * b.radius) kill = true;
+      }
+      if (kill) {
+        p.nid = -1;
+        absorb(a.gc, a.is, ipc, p.pid);
+      }
+    }
+  }
+  a.p[m] = p;
+}
+
 // psolve1, src/pcl2field/psolve1.F90:146-789: push with floor() indices and
 // the zigzag current into the per-species scratch tj (wrk(TJX:TJZ)).
 __global__ void k_psolve1(PushArgs a) {
@@ -770,6 +855,28 @@ extern "C" int emsesg_psolve2(emsesg_ctx* ctx, int ps, int ustep, emsesg_counter
     if ((rc = advance_randoms(ctx, is))) return rc;
   }
   return finish_push(ctx, gcount);
+}
+
+extern "C" int emsesg_positn(emsesg_ctx* ctx, int ps, int ustep, emsesg_counter* gcount) {
+  int rc = check_ps(ctx, ps);
+  if (rc) return rc;
+  if (ustep < 1) return set_error(ctx, EMSESG_ERR_ARG, "ustep must be >= 1");
+  if (gcount && (rc = emsesg_set_counters(ctx, gcount))) return rc;
+  for (int is = 0; is < ctx->cfg.nspec; is++) {
+    if (ctx->totalp[is] == 0) continue;
+    const uint32_t* ord;
+    if ((rc = prepare_ordinals(ctx, is, &ord))) return rc;
+    PushArgs a = push_args(ctx, is, ustep);
+    a.ordinal = ord;
+    EMSESG_LAUNCH(ctx, "positn", k_positn, nblk(a.n), 256, 0, a);
+    if ((rc = advance_randoms(ctx, is))) return rc;
+  }
+  ctx->rng_stream++;
+  if (gcount) {
+    if ((rc = emsesg_get_counters(ctx, gcount))) return rc;
+    return emsesg_synchronize(ctx);
+  }
+  return EMSESG_OK;
 }
 
 extern "C" int emsesg_psolve1(emsesg_ctx* ctx, int ps, int ustep, int func, emsesg_counter* gcount) {

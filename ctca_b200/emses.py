@@ -5,6 +5,7 @@ The methods keep the reference's names and argument meaning:
     Emses.grdcrt(ps)                 subroutine grdcrt(ps)          src/field/grdcrt.F90:125
     Emses.psolve2(ps, ustep)         subroutine psolve2(ps, ustep)  src/pcl2field/psolve2.F90:4
     Emses.psolve1(ps, ustep, func)   subroutine psolve1(...)        src/pcl2field/psolve1.F90:4
+    Emses.positn(ps, ustep)          subroutine positn(ps, ustep)   src/pcl/positn.F90:3
     Emses.charge(ps, func)           subroutine charge(ps, func)    src/pcl2field/charge.F90:4
     Emses.spsort(ps)                 subroutine spsort(ps)          src/etc/spsort.F90:4
 
@@ -108,6 +109,7 @@ _SIGS = {
     "emsesg_set_randoms": (_I, [_P, _P, ctypes.c_int64]),
     "emsesg_grdcrt": (_I, [_P, _I]),
     "emsesg_psolve2": (_I, [_P, _I, _I, ctypes.POINTER(Counter)]),
+    "emsesg_positn": (_I, [_P, _I, _I, ctypes.POINTER(Counter)]),
     "emsesg_psolve1": (_I, [_P, _I, _I, _I, ctypes.POINTER(Counter)]),
     "emsesg_charge": (_I, [_P, _I, _I]),
     "emsesg_reduce_rho": (_I, [_P, _I]),
@@ -290,6 +292,9 @@ class Emses:
 
     def psolve2(self, ps: int, ustep: int, gcount: Counter | None = None):
         self._check(self.lib.emsesg_psolve2(self.h, ps, ustep, ctypes.byref(gcount) if gcount else None))
+
+    def positn(self, ps: int, ustep: int, gcount: Counter | None = None):
+        self._check(self.lib.emsesg_positn(self.h, ps, ustep, ctypes.byref(gcount) if gcount else None))
 
     def psolve1(self, ps: int, ustep: int, func: int, gcount: Counter | None = None):
         self._check(self.lib.emsesg_psolve1(self.h, ps, ustep, func, ctypes.byref(gcount) if gcount else None))

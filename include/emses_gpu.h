@@ -11,6 +11,7 @@
  *   emsesg_grdcrt    <- subroutine grdcrt(ps)            src/field/grdcrt.F90:125
  *   emsesg_psolve2   <- subroutine psolve2(ps, ustep)     src/pcl2field/psolve2.F90:4
  *   emsesg_psolve1   <- subroutine psolve1(ps,ustep,func) src/pcl2field/psolve1.F90:4
+ *   emsesg_positn    <- subroutine positn(ps, ustep)     src/pcl/positn.F90:3
  *   emsesg_charge    <- subroutine charge(ps, func)       src/pcl2field/charge.F90:4
  *   emsesg_spsort    <- subroutine spsort(ps)             src/etc/spsort.F90:4
  *                       (and the C symbol particle_sort_,  lib/psort/psort-struct.c:7)
@@ -189,6 +190,8 @@ int emsesg_set_randoms(emsesg_ctx* ctx, const double* u, int64_t n);
 int emsesg_grdcrt(emsesg_ctx* ctx, int ps);
 /* gcount may be NULL: counters then stay on the device (emsesg_get_counters). */
 int emsesg_psolve2(emsesg_ctx* ctx, int ps, int ustep, emsesg_counter* gcount);
+/* Position-only advance of the initial state (no fields, no deposit). */
+int emsesg_positn(emsesg_ctx* ctx, int ps, int ustep, emsesg_counter* gcount);
 int emsesg_psolve1(emsesg_ctx* ctx, int ps, int ustep, int func,
                    emsesg_counter* gcount);
 int emsesg_charge(emsesg_ctx* ctx, int ps, int func);

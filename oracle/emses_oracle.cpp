@@ -384,6 +384,105 @@ int orc_psolve2(const emsesg_config* c, int ustep, const double* wrk,
   return rs.ok ? 0 : EMSESG_ERR_ARG;
 }
 
+// positn, src/pcl/positn.F90:50-355: the position-only advance of the
+// initial state.  x += v*ustep for every live particle (injected ones still
+// draw their random number, :97-101, but move by ustep, :109-114); the outer
+// boundary counts nesc once per escaping axis (:228-268); the body test takes
+// the box bounds xlpc..zupc as the cylinder's axial extent (:283-316); there
+// is no chgacm update.
+int orc_positn(const emsesg_config* c, int ustep, emsesg_particle* pbuf, const int64_t* totalp,
+               const double* ranu, int64_t nranu, int64_t* ranu_pos, uint64_t rng_stream, emsesg_counter* gc) {
+  double radsq[EMSESG_INPC];
+  radsq_of(c, radsq);
+  const double dxl = 0.0, dyl = 0.0, dzl = 0.0;
+  const double dxu = c->nx, dyu = c->ny, dzu = c->nz;
+  const double slx = c->nx, sly = c->ny, slz = c->nz;
+  const double tslx = 2.0 * slx, tsly = 2.0 * sly, tslz = 2.0 * slz;
+  RandSource rs{c, ranu, nranu, ranu_pos, rng_stream};
+  int64_t nee = 0;
+  for (int is = 0; is < c->nspec; is++) {
+    int64_t ns = nee, ne = nee + totalp[is];
+    nee = ne;
+    for (int64_t m = ns; m < ne; m++) {
+      emsesg_particle& p = pbuf[m];
+      if (p.preside < 0) {
+        p.nid = -1;
+        p.preside = 0;
+      } else if (p.preside == EMSESG_PCL_INJECTED) {
+        (void)rs.draw(m);
+        p.preside = 0;
+      }
+      if (p.nid == -1) continue;
+      double xmove = p.vx * ustep, ymove = p.vy * ustep, zmove = p.vz * ustep;
+      p.x = p.x + xmove;
+      p.y = p.y + ymove;
+      p.z = p.z + zmove;
+      int nud = 14;
+      if (p.x < dxl) nud -= 1; else if (p.x >= dxu) nud += 1;
+      if (p.y < dyl) nud -= 3; else if (p.y >= dyu) nud += 3;
+      if (p.z < dzl) nud -= 9; else if (p.z >= dzu) nud += 9;
+      if (nud != 14) {
+        bool cx = p.x < dxl || p.x >= dxu, cy = p.y < dyl || p.y >= dyu, cz = p.z < dzl || p.z >= dzu;
+        p.nid = nborps_single(c, is, cx, cy, cz);
+        const int32_t* nb = c->npbnd[is];
+        if (p.x < 0.0) {
+          if (nb[0] == 0) p.x = p.x + slx;
+          else if (nb[0] == 1) { p.x = -p.x; p.vx = -p.vx; }
+          else gc->nesc[is] += 1;
+        } else if (p.x >= slx) {
+          if (nb[0] == 0) p.x = p.x - slx;
+          else if (nb[0] == 1) { p.x = tslx - p.x; p.vx = -p.vx; }
+          else gc->nesc[is] += 1;
+        }
+        if (p.y < 0.0) {
+          if (nb[1] == 0) p.y = p.y + sly;
+          else if (nb[1] == 1) { p.y = -p.y; p.vy = -p.vy; }
+          else gc->nesc[is] += 1;
+        } else if (p.y >= sly) {
+          if (nb[1] == 0) p.y = p.y - sly;
+          else if (nb[1] == 1) { p.y = tsly - p.y; p.vy = -p.vy; }
+          else gc->nesc[is] += 1;
+        }
+        if (p.z < 0.0) {
+          if (nb[2] == 0) p.z = p.z + slz;
+          else if (nb[2] == 1) { p.z = -p.z; p.vz = -p.vz; }
+          else gc->nesc[is] += 1;
+        } else if (p.z >= slz) {
+          if (nb[2] == 0) p.z = p.z - slz;
+          else if (nb[2] == 1) { p.z = tslz - p.z; p.vz = -p.vz; }
+          else gc->nesc[is] += 1;
+        }
+      }
+      if (c->line_mode == 1) continue;
+      for (int ipc = 0; ipc < c->npc; ipc++) {
+        if (p.nid == -1) continue;
+        const emsesg_body& b = c->body[ipc];
+        bool kill = false;
+        if ((b.geotype == 0 || b.geotype == 1) &&
+            (p.x >= b.xlpc && p.x <= b.xupc && p.y >= b.ylpc && p.y <= b.yupc && p.z >= b.zlpc && p.z <= b.zupc)) {
+          kill = true;
+        } else if (b.geotype == 2) {
+          double d1, d2, a, lo, hi;
+          if (b.cyl_align == 1) { d1 = p.y - b.cyl_axis[0]; d2 = p.z - b.cyl_axis[1]; a = p.x; lo = b.xlpc; hi = b.xupc; }
+          else if (b.cyl_align == 2) { d1 = p.z - b.cyl_axis[0]; d2 = p.x - b.cyl_axis[1]; a = p.y; lo = b.ylpc; hi = b.yupc; }
+          else if (b.cyl_align == 3) { d1 = p.x - b.cyl_axis[0]; d2 = p.y - b.cyl_axis[1]; a = p.z; lo = b.zlpc; hi = b.zupc; }
+          else continue;
+          if (a >= lo && a <= hi && d1 * d1 + d2 * d2 < radsq[ipc]) kill = true;
+        } else if (b.geotype == 3) {
+          double d1 = p.x - b.sph_center[0], d2 = p.y - b.sph_center[1], d3 = p.z - b.sph_center[2];
+          if (d1 * d1 + d2 * d2 + d3 * d3 < radsq[ipc]) kill = true;
+        }
+        if (kill) {
+          p.nid = -1;
+          gc->influx[is][ipc] += 1;
+          if (p.pid >= 0 && p.pid <= EMSESG_INPC) gc->infhist[is][ipc][p.pid] += 1;
+        }
+      }
+    }
+  }
+  return rs.ok ? 0 : EMSESG_ERR_ARG;
+}
+
 // psolve1, src/pcl2field/psolve1.F90:85-828: the push of psolve2 with floor()
 // cell indices and the zigzag current (Umeda 2003) into wrk(TJX:TJZ), flushed
 // into aj (and ajdg when func == 1) with q(is) per species.

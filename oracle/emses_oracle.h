@@ -42,6 +42,9 @@ int orc_psolve2(const emsesg_config* c, int ustep, const double* wrk,
                 emsesg_particle* pbuf, const int64_t* totalp, const double* ranu,
                 int64_t nranu, int64_t* ranu_pos, uint64_t rng_stream,
                 emsesg_counter* gc);
+int orc_positn(const emsesg_config* c, int ustep, emsesg_particle* pbuf, const int64_t* totalp,
+               const double* ranu, int64_t nranu, int64_t* ranu_pos, uint64_t rng_stream,
+               emsesg_counter* gc);
 int orc_psolve1(const emsesg_config* c, int ustep, int func, double* wrk,
                 emsesg_particle* pbuf, const int64_t* totalp, const double* ranu,
                 int64_t nranu, int64_t* ranu_pos, uint64_t rng_stream,

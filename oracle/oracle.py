@@ -51,6 +51,8 @@ def lib() -> ctypes.CDLL:
         "orc_grdcrt": (None, [cfgp, _P, _P]),
         "orc_psolve2": (ctypes.c_int, [cfgp, ctypes.c_int, _P, _P, i64p, _P, ctypes.c_int64, i64p, ctypes.c_uint64,
                                        ctypes.POINTER(Counter)]),
+        "orc_positn": (ctypes.c_int, [cfgp, ctypes.c_int, _P, i64p, _P, ctypes.c_int64, i64p, ctypes.c_uint64,
+                                      ctypes.POINTER(Counter)]),
         "orc_psolve1": (ctypes.c_int, [cfgp, ctypes.c_int, ctypes.c_int, _P, _P, i64p, _P, ctypes.c_int64, i64p,
                                        ctypes.c_uint64, _P, _P, ctypes.POINTER(Counter)]),
         "orc_charge": (None, [cfgp, ctypes.c_int, _P, i64p, _P, _P, _P, _P]),
@@ -115,6 +117,15 @@ class Oracle:
         self.rng_stream += 1
         if rc:
             raise RuntimeError("oracle psolve2: random numbers exhausted")
+
+    def positn(self, ustep: int):
+        tp = _tp(self.totalp)
+        rc = self.L.orc_positn(self._c(), ustep, self.pbuf.ctypes.data, tp,
+                               self.ranu.ctypes.data if self.ranu.size else None, self.ranu.size,
+                               ctypes.byref(self.ranu_pos), self.rng_stream, ctypes.byref(self.gc))
+        self.rng_stream += 1
+        if rc:
+            raise RuntimeError("oracle positn: random numbers exhausted")
 
     def psolve1(self, ustep: int, func: int = 0):
         tp = _tp(self.totalp)

@@ -12,6 +12,7 @@ these files use) runs them from the text of
     src/pcl2field/psolve1.F90    psolve1, add_boundary_current(2)
     src/pcl2field/charge.F90     charge, add_boundary_charge
     src/field/rhoupd.F90         rhoupd
+    src/pcl/positn.F90           positn
 
 with IEEE double arithmetic in source order (Python floats: no fused
 multiply-add, no reassociation), Fortran integer division and int()
@@ -58,7 +59,7 @@ from ctca_b200 import inputs  # noqa: E402
 from ctca_b200.emses import INPC, ISPEC, PARTICLE_DTYPE, Body, Config, field_shape  # noqa: E402
 
 SOURCES = ["src/field/grdcrt.F90", "src/pcl2field/psolve2.F90", "src/pcl2field/psolve1.F90",
-           "src/pcl2field/charge.F90", "src/field/rhoupd.F90"]
+           "src/pcl2field/charge.F90", "src/field/rhoupd.F90", "src/pcl/positn.F90"]
 
 # src/main/paramt.F90:44-48
 CEB, CAJ, CRH, CRD, CJD, CPH = 1, 2, 3, 4, 5, 6
@@ -355,6 +356,16 @@ def run_case(units, name, c, ustep, opts):
     out["psolve2_nranu"] = np.int64(pos[0])
     for k, v in counters(gc).items():
         out["psolve2_" + k] = v
+    # positn: the position-only advance of the initial state
+    f = fields()
+    pb = p0.copy()
+    g, ext, gc, pos = make_env(cfg, pb, tp, f, uniforms)
+    it = Interpreter(units, g, ext)
+    it.call("positn", [1, ustep])
+    out["positn_pbuf"] = pb.copy()
+    out["positn_nranu"] = np.int64(pos[0])
+    for k, v in counters(gc).items():
+        out["positn_" + k] = v
     # grdcrt + psolve1(func=1): zigzag current, then the J border reduction
     f = fields()
     pb = p0.copy()

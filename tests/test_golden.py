@@ -1,6 +1,6 @@
 """The oracle against the golden fixtures of tests/golden/: outputs of the
 reference's own Fortran subroutines (grdcrt, psolve2, psolve1,
-add_boundary_current(2), charge, add_boundary_charge, rhoupd), executed from
+add_boundary_current(2), charge, add_boundary_charge, rhoupd, positn), executed from
 their source text by tests/golden/make_golden.py on small seeded cases.
 
 Every comparison is bit-for-bit: particles (all 64 bytes of each record),
@@ -94,3 +94,14 @@ def test_psolve1_charge_and_reductions(path):
     assert same(o.f["rhodg"], d["reduced_rhodg"]), first_diff(o.f["rhodg"], d["reduced_rhodg"])
     o.rhoupd()
     assert same(o.f["rho"], d["rhoupd_rho"]), first_diff(o.f["rho"], d["rhoupd_rho"])
+
+
+@pytest.mark.parametrize("path", CASES, ids=lambda p: p.stem)
+def test_positn(path):
+    d, cfg = load(path)
+    o = oracle_for(d, cfg, d["pbuf0"])
+    o.positn(int(d["ustep"]))
+    assert o.ranu_pos.value == int(d["positn_nranu"])
+    for fld in d["pbuf0"].dtype.names:
+        assert same(o.pbuf[fld], d["positn_pbuf"][fld]), (fld, first_diff(o.pbuf[fld], d["positn_pbuf"][fld]))
+    check_counters(o, d, "positn_")

@@ -85,3 +85,14 @@ def test_dropin_psolve1_charge_golden(gpu, path):
         assert rel_l2(g.download_field("rhodg"), d["reduced_rhodg"]) < TOL
         g.rhoupd(1)
         assert rel_l2(g.download_field("rho"), d["rhoupd_rho"]) < TOL
+
+
+@pytest.mark.parametrize("path", CASES, ids=lambda p: p.stem)
+def test_dropin_positn_golden(gpu, path):
+    d, cfg = load(path)
+    with device(d, cfg, d["pbuf0"]) as g:
+        gc = Counter()
+        g.positn(1, int(d["ustep"]), gc)
+        p, _ = g.download_particles()
+        assert same_particles(p, d["positn_pbuf"])
+        counters_match(gc, d, "positn_")
