@@ -416,11 +416,11 @@ int fx_local_sort(emsesg_ctx* ctx, bool* done) {
     const int64_t off = f.base[is];
     uint32_t* cnt = f.lcs_cnt + is * f.ntiles * nbc;
     uint32_t* bas = f.lcs_base + is * f.ntiles * nbc;
-    EMSESG_LAUNCH(ctx, "lcs_celltot", k_lcs_celltot, (unsigned)f.ntiles, PUSH_THREADS, 0, cnt, g, G[is],
+    EMSESG_LAUNCH(ctx, "lcs_celltot", k_lcs_celltot, (unsigned)f.ntiles, CELL_THREADS, 0, cnt, g, G[is],
                   f.lcs_celltot, f.lcs_tiletot);
     EMSESG_LAUNCH(ctx, "lcs_tiles", k_lcs_tiles, 1, 1024, 0, f.lcs_tiletot, f.ntiles, ts2, tp2, f.count_d + is,
                   f.slots_d + is);
-    EMSESG_LAUNCH(ctx, "lcs_bases", k_lcs_bases, (unsigned)f.ntiles, PUSH_THREADS, 0, cnt, f.lcs_celltot, g, G[is],
+    EMSESG_LAUNCH(ctx, "lcs_bases", k_lcs_bases, (unsigned)f.ntiles, CELL_THREADS, 0, cnt, f.lcs_celltot, g, G[is],
                   ts2, tp2, bas, f.lcs_inv + off);
     EMSESG_LAUNCH(ctx, "lcs_rank", k_lcs_rank, (unsigned)f.ntiles, PUSH_THREADS, lsm, f.pos + off,
                   f.tile_start + is * T1, f.tile_pad + is * T1, g, G[is], f.lcs_wcnt + is * f.ntiles * PUSH_WARPS * nbc,

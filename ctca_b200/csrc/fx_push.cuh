@@ -7,7 +7,7 @@
 // thread t's contiguous run of the cell-sorted order, and row r is one
 // coalesced stretch of PUSH_THREADS records.  Empty slots hold DEAD cells.
 //
-// One CTA pushes one region with 512 threads; a 17th warp streams the rows
+// One CTA pushes one region with 480 threads; a 16th warp streams the rows
 // into a 4-stage shared-memory ring with cp.async.bulk (TMA 1-D copies
 // completing on mbarriers) and never computes, so a warp busy with its
 // queues never holds up the stream; pushing warps release a stage through an
@@ -30,7 +30,9 @@
 // every conversion to fixed point is of one value; integer atomics commute.
 // Two runs on the same input give the same bits.
 
-constexpr int PUSH_THREADS = 512;           // pushing threads = slots per row
+// 15 pushing warps + 1 streaming warp: 16 warps, so that each SM sub-partition
+// holds 4 of them and the kernel keeps 128 registers a thread.
+constexpr int PUSH_THREADS = 480;           // pushing threads = slots per row
 constexpr int PUSH_WARPS = PUSH_THREADS / 32;
 constexpr int PUSH_BLOCK = PUSH_THREADS + 32;  // + one warp that streams the rows
 constexpr int PG = 1;           // guard cells around the tile
@@ -45,6 +47,8 @@ constexpr int XQW = 8;          // cross entry: slot, cell, 3 offsets, 3 velocit
 constexpr int XQ_DRAIN = 32;
 constexpr int XQCAP = XQ_DRAIN + 32;
 constexpr uint32_t ROW_BYTES = PUSH_THREADS * (16 + 3 * 4);
+static_assert(PUSH_THREADS == EMSESG_FX_ROW_SLOTS, "row width of the thread-major layout");
+static_assert(ROW_BYTES % 16 == 0 && (PUSH_THREADS * 4) % 16 == 0, "bulk copies move whole 16-byte units");
 
 struct FxPushArgs {
   float4* pos;                  // all species regions

@@ -44,6 +44,10 @@ struct LcsGeo {
   bool wrap[3];  // periodic particle axis (npbnd == 0)
 };
 
+// Block size of the per-cell kernels (one thread per cell of a tile of at
+// most 8x8x8 cells).
+constexpr int CELL_THREADS = 512;
+
 __device__ __forceinline__ int lcs_axis(const LcsGeo& G, int d, int tile, int i) {
   int l = i - (tile * G.t[d] - 1);
   if (G.wrap[d]) {
@@ -133,11 +137,11 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_count(const float4* __rest
 }
 
 // celltot: per destination cell, the sum over the source tiles holding it;
-// per destination tile its total.  grid = ntiles, block = PUSH_THREADS (>= tcells).
-__global__ void __launch_bounds__(PUSH_THREADS) k_lcs_celltot(const uint32_t* __restrict__ cnt, Geo g, LcsGeo G,
+// per destination tile its total.  grid = ntiles, block = CELL_THREADS (>= tcells).
+__global__ void __launch_bounds__(CELL_THREADS) k_lcs_celltot(const uint32_t* __restrict__ cnt, Geo g, LcsGeo G,
                                                               uint32_t* __restrict__ celltot,
                                                               int64_t* __restrict__ tiletot) {
-  __shared__ uint32_t part[PUSH_WARPS];
+  __shared__ uint32_t part[CELL_THREADS / 32];
   const int t = blockIdx.x, tid = threadIdx.x;
   int tx, ty, tz;
   tile_xyz(g, t, tx, ty, tz);
@@ -167,7 +171,7 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_celltot(const uint32_t* __
   __syncthreads();
   if (tid == 0) {
     int64_t s = 0;
-    for (int w = 0; w < PUSH_WARPS; w++) s += part[w];
+    for (int w = 0; w < CELL_THREADS / 32; w++) s += part[w];
     tiletot[t] = s;
   }
 }
@@ -211,13 +215,13 @@ __global__ void __launch_bounds__(1024) k_lcs_tiles(const int64_t* __restrict__ 
 }
 
 // bases: first rank of every (source tile, box cell); DEAD in the empty
-// slots of the new region.  grid = ntiles (destination tiles), block = PUSH_THREADS.
-__global__ void __launch_bounds__(PUSH_THREADS) k_lcs_bases(const uint32_t* __restrict__ cnt,
+// slots of the new region.  grid = ntiles (destination tiles), block = CELL_THREADS.
+__global__ void __launch_bounds__(CELL_THREADS) k_lcs_bases(const uint32_t* __restrict__ cnt,
                                                             const uint32_t* __restrict__ celltot, Geo g, LcsGeo G,
                                                             const int64_t* __restrict__ ts,
                                                             const int64_t* __restrict__ tp, uint32_t* __restrict__ base,
                                                             uint32_t* __restrict__ inv) {
-  __shared__ uint32_t sc[PUSH_THREADS];
+  __shared__ uint32_t sc[CELL_THREADS];
   const int t = blockIdx.x, tid = threadIdx.x;
   int tx, ty, tz;
   tile_xyz(g, t, tx, ty, tz);
@@ -225,7 +229,7 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_bases(const uint32_t* __re
   // exclusive scan over the tile's cells (cell order = the sort key order)
   sc[tid] = mine;
   __syncthreads();
-  for (int d = 1; d < PUSH_THREADS; d <<= 1) {
+  for (int d = 1; d < CELL_THREADS; d <<= 1) {
     uint32_t v = tid >= d ? sc[tid - d] : 0u;
     __syncthreads();
     sc[tid] += v;
@@ -254,7 +258,7 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_bases(const uint32_t* __re
   const int64_t n = ts[t + 1] - ts[t];
   if (n > 0) {
     const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
-    for (int64_t q = n + tid; q < (int64_t)L * PUSH_THREADS; q += PUSH_THREADS) {
+    for (int64_t q = n + tid; q < (int64_t)L * PUSH_THREADS; q += CELL_THREADS) {
       const int64_t slot = tp[t] + (q % L) * PUSH_THREADS + q / L;
       inv[slot] = DEAD;
     }

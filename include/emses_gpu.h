@@ -227,6 +227,10 @@ int emsesg_energy(emsesg_ctx* ctx, double* engk);
  * cell key.  rho and J accumulate in int64 fixed point (scale 2^40), so the
  * sums do not depend on the order in which threads add them. */
 /* Converts the FP64 pbuf mirror into the FP32 form and sorts it. */
+/* Slots per row of the FP32 form's thread-major tile regions: after a sort
+ * the particle of sorted rank q of a tile of n particles sits in row q % L,
+ * column q / L of its region, L = ceil(n / EMSESG_FX_ROW_SLOTS). */
+#define EMSESG_FX_ROW_SLOTS 480
 int emsesg_fx_load(emsesg_ctx* ctx);
 /* Converts the FP32 form back into the FP64 pbuf mirror (for download), in
  * the current buffer order; particles that died since the last sort come

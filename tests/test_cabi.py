@@ -79,3 +79,10 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(emses, "_lib", None)
     with pytest.raises(ImportError):
         emses.load_library()
+
+
+def test_fx_row_slots_match_the_header():
+    import re
+    from ctca_b200.emses import FX_ROW_SLOTS
+    text = (Path(__file__).resolve().parent.parent / "include" / "emses_gpu.h").read_text()
+    assert int(re.search(r"#define EMSESG_FX_ROW_SLOTS (\d+)", text).group(1)) == FX_ROW_SLOTS

@@ -11,7 +11,7 @@ accumulators."""
 import numpy as np
 import pytest
 
-from ctca_b200.emses import Emses
+from ctca_b200.emses import FX_ROW_SLOTS, Emses
 from oracle import oracle as O
 
 from helpers import build, case, rel_l2
@@ -144,7 +144,7 @@ def test_fx_local_sort_is_a_stable_cell_sort(gpu, npbnd, tile):
     live particles by the tile-major cell key; equal cells keep the order
     (source tile, warp, row, lane) of the thread-major layout of the last
     sort, computed here from the tile sizes of that sort."""
-    threads = 512
+    threads = FX_ROW_SLOTS
     c = case(n=(16, 16, 16), ppc=(8, 8), npbnd=npbnd, vth_scale=6.0, tile=tile)
     cfg, eb, p, tp = build(c)
     g = Emses(cfg)
