@@ -83,6 +83,20 @@ struct FxState {
   int64_t* lcs_tiletot = nullptr;   // [ntiles]
   int* lcs_stray = nullptr;         // [nspec]
   uint32_t* lcs_inv = nullptr;      // per slot: the old slot of its particle
+  // box bodies: absorbed minus emitted particles per surface cell
+  unsigned long long* surf = nullptr;  // [nspec][nsurf]
+  int64_t nsurf = 0;
+  // injected particles (oh2_inject_particle): a tail zone at the end of each
+  // species region, pushed by the general path until the next sort
+  int64_t tail0[EMSESG_ISPEC] = {};    // first slot of the tail zone
+  int64_t tailcap[EMSESG_ISPEC] = {};
+  int64_t ntail[EMSESG_ISPEC] = {};
+  int32_t* tailord = nullptr;          // per tail slot: 1 + ordinal of a pending random step, or 0
+  int64_t tailord_base[EMSESG_ISPEC] = {};  // offset of each species' tail in tailord
+  int64_t pending[EMSESG_ISPEC] = {};  // injected particles still to take their random step
+  emsesg_particle* stage = nullptr;    // device staging of injected records
+  int32_t* stage_ord = nullptr;
+  int64_t stage_cap = 0;
   int64_t* accum = nullptr;         // int64 (rho, jx, jy, jz) on the rho layout
   float4* fnode = nullptr;          // node field {ex, ey, ez, bx} over (n+1)^3 nodes
   float4* fnode2 = nullptr;         // {by, bz, 0, 0}

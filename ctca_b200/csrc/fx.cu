@@ -23,6 +23,9 @@
 // the FP32 partial sums depend only on the sorted order and the fixed thread
 // slicing, so every run gives the same bits.
 #include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
 #include <cstring>
 
 #include "common.cuh"
@@ -118,6 +121,68 @@ __global__ void k_fx_from_aos(const emsesg_particle* __restrict__ p, int64_t n, 
 
 // One tile region (thread-major, see fx_push.cuh) back to the FP64 records
 // of the tile's sorted ranks ts[t] .. ts[t+1]-1.
+// Injected records into the tail zone (oh2_inject_particle, ohhelp2.c:549):
+// preside +1 takes a random fraction of its first step (ord > 0), an
+// anti-particle (preside -2, an emitted particle's image on the body face,
+// psuper3.F90:203-206) removes one count from the surface cell it lies on
+// and takes no slot's place in the push (DEAD).
+__global__ void k_fx_inject(const emsesg_particle* __restrict__ q, const int32_t* __restrict__ qord, int64_t n,
+                            Geo g, Bodies bd, int64_t slot0, float4* pos, float* vx, float* vy, float* vz,
+                            int32_t* ord, unsigned long long* surf, int* status, long long* diag) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const emsesg_particle r = q[k];
+  const int64_t m = slot0 + k;
+  uint32_t cell = DEAD;
+  float ox = 0.f, oy = 0.f, oz = 0.f;
+  if (r.preside == EMSESG_PCL_TO_BE_ACCUMULATED_AS_ANTIPCL) {
+    const double p3[3] = {r.x, r.y, r.z};
+    for (int b = 0; b < bd.n; b++) {
+      int64_t hit = -1;
+      for (int d = 0; d < 3 && hit < 0; d++) {
+        const int e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;
+        if (p3[e1] < bd.lo[b][e1] || p3[e1] > bd.hi[b][e1] || p3[e2] < bd.lo[b][e2] || p3[e2] > bd.hi[b][e2]) continue;
+        int side = -1;
+        if (p3[d] == (double)bd.lo[b][d]) side = 0;
+        else if (p3[d] == (double)bd.hi[b][d]) side = 1;
+        if (side < 0) continue;
+        int u = (int)floor(p3[e1]), v = (int)floor(p3[e2]);
+        u = min(max(u, bd.lo[b][e1]), bd.hi[b][e1] - 1) - bd.lo[b][e1];
+        v = min(max(v, bd.lo[b][e2]), bd.hi[b][e2] - 1) - bd.lo[b][e2];
+        hit = bd.off[b][2 * d + side] + u + (int64_t)(bd.hi[b][e1] - bd.lo[b][e1]) * v;
+      }
+      if (hit >= 0) {
+        atomicAdd(&surf[hit], (unsigned long long)(-1LL));
+        break;
+      }
+    }
+  } else if (r.nid != -1) {
+    int i, j, kk;
+    bool ok = split_coord(r.x, g.nx, i, ox) & split_coord(r.y, g.ny, j, oy) & split_coord(r.z, g.nz, kk, oz);
+    if (!ok) report_bad(status, diag, SITE_FX_LOAD, m, i + 100000LL * j + 10000000000LL * kk);
+    else cell = pack(g, i, j, kk);
+  }
+  pos[m] = make_float4(ox, oy, oz, __int_as_float((int)cell));
+  vx[m] = (float)r.vx;
+  vy[m] = (float)r.vy;
+  vz[m] = (float)r.vz;
+  ord[k] = cell == DEAD ? 0 : qord[k];
+}
+
+// chgacm += influx * q * sqdscaled for conductors (psolve1.F90:821-828).
+__global__ void k_fx_chgacm(const emsesg_config* c, emsesg_counter* gc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int is = 0; is < c->nspec; is++)
+    for (int ipc = 0; ipc < c->npc; ipc++)
+      if (c->body[ipc].ncond > 0) {
+        double add = (double)gc->influx[is][ipc] * c->q[is] * c->body[ipc].sqdscaled;
+        gc->chgacm[ipc][0] = gc->chgacm[ipc][0] + add;
+        gc->chgacm[ipc][1] = gc->chgacm[ipc][1] + add;
+      }
+}
+
+__global__ void k_add_i64(int64_t* p, int64_t v) { *p += v; }
+
 __global__ void k_fx_to_aos_tm(const float4* __restrict__ pos, const float* __restrict__ vx,
                                const float* __restrict__ vy, const float* __restrict__ vz,
                                const int64_t* __restrict__ ts, const int64_t* __restrict__ tp, Geo g, int is,
@@ -155,13 +220,15 @@ __global__ void k_fx_to_aos_tm(const float4* __restrict__ pos, const float* __re
 // Sort key of the FP32 form: the tile-major cell key (as the FP64 spsort);
 // dead particles, empty slots and slots past the region's slot count get the
 // largest key.
-__global__ void k_fx_keys(const float4* __restrict__ pos, int64_t n, const int64_t* slots, Geo g, uint32_t deadkey,
-                          uint32_t* keys, uint32_t* vals) {
+__global__ void k_fx_keys(const float4* __restrict__ pos, int64_t n, const int64_t* slots, int64_t tail0,
+                          int64_t ntail, Geo g, uint32_t deadkey, uint32_t* keys, uint32_t* vals) {
   int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= n) return;
+  if (m >= n + ntail) return;
   uint32_t key = deadkey;
-  if (m < *slots) {
-    uint32_t cell = (uint32_t)__float_as_int(pos[m].w);
+  // indices past n are the tail zone's slots
+  const int64_t slot = m < n ? m : tail0 + (m - n);
+  if (m >= n || m < *slots) {
+    uint32_t cell = (uint32_t)__float_as_int(pos[slot].w);
     if (cell != DEAD) {
       int i, j, k;
       unpack(g, cell, i, j, k);
@@ -172,7 +239,7 @@ __global__ void k_fx_keys(const float4* __restrict__ pos, int64_t n, const int64
     }
   }
   keys[m] = key;
-  vals[m] = (uint32_t)m;
+  vals[m] = (uint32_t)slot;
 }
 
 // tile_start[t] = first sorted slot with tile >= t; tile_start[ntiles] and
@@ -275,6 +342,51 @@ Geo make_geo(emsesg_ctx* ctx) {
 
 }  // namespace
 
+// Box bodies usable by the FP32 form: geotype 0/1 with integer bounds.
+// Returns false (with the reason) when a body cannot be handled.
+bool bodies_supported(const emsesg_config& c, std::string* why) {
+  if (c.npc <= 0 || c.line_mode == 1) return true;
+  for (int ipc = 0; ipc < c.npc; ipc++) {
+    const emsesg_body& b = c.body[ipc];
+    if (!(b.geotype == 0 || b.geotype == 1)) {
+      if (why) *why = "the FP32 form handles box bodies (geotype 0/1) only";
+      return false;
+    }
+    const double v[6] = {b.xlpc, b.xupc, b.ylpc, b.yupc, b.zlpc, b.zupc};
+    for (int q = 0; q < 6; q++)
+      if (v[q] != std::floor(v[q])) {
+        if (why) *why = "the FP32 form needs integer box bounds";
+        return false;
+      }
+    if (!(b.xupc > b.xlpc && b.yupc > b.ylpc && b.zupc > b.zlpc)) {
+      if (why) *why = "empty box body";
+      return false;
+    }
+  }
+  return true;
+}
+
+Bodies make_bodies(const emsesg_config& c) {
+  Bodies bd{};
+  bd.n = 0;
+  bd.nsurf = 0;
+  if (c.line_mode == 1 || !bodies_supported(c, nullptr)) return bd;
+  for (int ipc = 0; ipc < c.npc; ipc++) {
+    const emsesg_body& b = c.body[ipc];
+    const int q = bd.n++;
+    bd.ipc[q] = ipc;
+    bd.lo[q][0] = (int)b.xlpc; bd.hi[q][0] = (int)b.xupc;
+    bd.lo[q][1] = (int)b.ylpc; bd.hi[q][1] = (int)b.yupc;
+    bd.lo[q][2] = (int)b.zlpc; bd.hi[q][2] = (int)b.zupc;
+    for (int f = 0; f < 6; f++) {
+      const int d = f / 2, e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;
+      bd.off[q][f] = bd.nsurf;
+      bd.nsurf += (int64_t)(bd.hi[q][e1] - bd.lo[q][e1]) * (bd.hi[q][e2] - bd.lo[q][e2]);
+    }
+  }
+  return bd;
+}
+
 int fx_alloc(emsesg_ctx* ctx) {
   FxState& f = ctx->fx;
   if (f.pos) return EMSESG_OK;
@@ -292,15 +404,31 @@ int fx_alloc(emsesg_ctx* ctx) {
   int tmax = std::max(f.tile[0], std::max(f.tile[1], f.tile[2]));
   if (tmax > 8) return set_error(ctx, EMSESG_ERR_ARG, "FP32 form tiles are at most 8 cells per axis");
   f.ntiles = (int64_t)f.ntile[0] * f.ntile[1] * f.ntile[2];
-  // species regions: capacity plus one row of padding per tile, in whole rows
-  int64_t cap = 0;
+  // species regions: capacity plus one row of padding per tile, in whole
+  // rows, then the tail zone of injected particles (an eighth of capacity)
+  int64_t cap = 0, ntailall = 0;
   for (int is = 0; is < c.nspec; is++) {
     f.base[is] = cap;
     int64_t rows = (ctx->seg.capacity[is] + PUSH_THREADS - 1) / PUSH_THREADS + f.ntiles;
-    f.cap[is] = rows * PUSH_THREADS;
+    f.tail0[is] = rows * PUSH_THREADS;
+    f.tailcap[is] = ((ctx->seg.capacity[is] / 8 + PUSH_THREADS - 1) / PUSH_THREADS + 1) * PUSH_THREADS;
+    f.tailord_base[is] = ntailall;
+    ntailall += f.tailcap[is];
+    f.ntail[is] = 0;
+    f.pending[is] = 0;
+    f.cap[is] = f.tail0[is] + f.tailcap[is];
     cap += f.cap[is];
   }
   cap = std::max<int64_t>(cap, 1);
+  EMSESG_CUDA(ctx, cudaMalloc(&f.tailord, std::max<int64_t>(ntailall, 1) * sizeof(int32_t)));
+  EMSESG_CUDA(ctx, cudaMemsetAsync(f.tailord, 0, std::max<int64_t>(ntailall, 1) * sizeof(int32_t), ctx->stream));
+  {
+    Bodies bd = make_bodies(c);
+    f.nsurf = bd.nsurf;
+    const int64_t ns = std::max<int64_t>((int64_t)c.nspec * f.nsurf, 1);
+    EMSESG_CUDA(ctx, cudaMalloc(&f.surf, ns * sizeof(unsigned long long)));
+    EMSESG_CUDA(ctx, cudaMemsetAsync(f.surf, 0, ns * sizeof(unsigned long long), ctx->stream));
+  }
   EMSESG_CUDA(ctx, cudaMalloc(&f.pos, cap * sizeof(float4)));
   EMSESG_CUDA(ctx, cudaMalloc(&f.vx, cap * sizeof(float)));
   EMSESG_CUDA(ctx, cudaMalloc(&f.vy, cap * sizeof(float)));
@@ -350,6 +478,7 @@ void fx_free(emsesg_ctx* ctx) {
   cudaFree(f.fnode); cudaFree(f.fnode2);
   cudaFree(f.tile_start2); cudaFree(f.tile_pad2); cudaFree(f.lcs_cnt); cudaFree(f.lcs_base); cudaFree(f.lcs_wcnt);
   cudaFree(f.lcs_celltot); cudaFree(f.lcs_tiletot); cudaFree(f.lcs_stray); cudaFree(f.lcs_inv);
+  cudaFree(f.surf); cudaFree(f.tailord); cudaFree(f.stage); cudaFree(f.stage_ord);
   f = FxState();
 }
 
@@ -361,7 +490,7 @@ namespace {
 // Host-side bound of the slots the sort has to look at: the particles loaded
 // (no particle is added in this form) plus the padding, within the region.
 int64_t sort_slots(emsesg_ctx* ctx, int is) {
-  return std::min(ctx->fx.cap[is], ctx->totalp[is] + ctx->fx.ntiles * PUSH_THREADS);
+  return std::min(ctx->fx.tail0[is], ctx->totalp[is] + ctx->fx.ntiles * PUSH_THREADS);
 }
 }  // namespace
 
@@ -443,14 +572,19 @@ extern "C" int emsesg_fx_sort(emsesg_ctx* ctx) {
   if (!ctx) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
   FxState& f = ctx->fx;
-  if (f.tiled) {
+  bool tail = false;
+  for (int is = 0; is < ctx->cfg.nspec; is++) {
+    if (f.pending[is]) return set_error(ctx, EMSESG_ERR_STATE, "injected particles are sorted before their first push");
+    tail = tail || f.ntail[is] > 0;
+  }
+  if (f.tiled && !tail) {
     bool done = false;
     int lrc = fx_local_sort(ctx, &done);
     if (lrc) return lrc;
     if (done) return EMSESG_OK;
   }
   int64_t most = 1;
-  for (int is = 0; is < ctx->cfg.nspec; is++) most = std::max(most, sort_slots(ctx, is));
+  for (int is = 0; is < ctx->cfg.nspec; is++) most = std::max(most, sort_slots(ctx, is) + f.ntail[is]);
   int rc = ensure_sort_scratch(ctx, most);
   if (rc) return rc;
   Geo g = make_geo(ctx);
@@ -470,8 +604,11 @@ extern "C" int emsesg_fx_sort(emsesg_ctx* ctx) {
       EMSESG_CUDA(ctx, cudaMemsetAsync(f.slots_d + is, 0, sizeof(int64_t), ctx->stream));
       continue;
     }
-    EMSESG_LAUNCH(ctx, "fx_keys", k_fx_keys, nblk(n), 256, 0, f.pos + off, n, f.slots_d + is, g, deadkey,
-                  ctx->sort.keys[0], ctx->sort.vals[0]);
+    const int64_t nt = f.ntail[is];
+    EMSESG_LAUNCH(ctx, "fx_keys", k_fx_keys, nblk(n + nt), 256, 0, f.pos + off, n, f.slots_d + is, f.tail0[is], nt,
+                  g, deadkey, ctx->sort.keys[0], ctx->sort.vals[0]);
+    n += nt;
+    f.ntail[is] = 0;
     uint32_t *ko, *vo;
     if ((rc = sort_pairs(ctx, ctx->sort.keys[0], ctx->sort.vals[0], n, bits, &ko, &vo))) return rc;
     EMSESG_LAUNCH(ctx, "fx_tile_starts", k_tile_starts, nblk(n + 1), 256, 0, ko, n, tilecells, f.ntiles, ts,
@@ -528,8 +665,15 @@ extern "C" int emsesg_fx_store(emsesg_ctx* ctx) {
   // Sorted order of the last sort (tile-major cell order); particles that
   // died since then come out with nid = -1 in place, as the reference leaves
   // them before transbound.
+  int rc;
+  // injected particles still in the tail zone join the regions first
+  for (int is = 0; is < ctx->cfg.nspec; is++)
+    if (ctx->fx.ntail[is] > 0) {
+      if ((rc = emsesg_fx_sort(ctx))) return rc;
+      break;
+    }
   int64_t cnt[EMSESG_ISPEC] = {0};
-  int rc = emsesg_fx_counts(ctx, cnt);
+  rc = emsesg_fx_counts(ctx, cnt);
   if (rc) return rc;
   FxState& f = ctx->fx;
   Geo g = make_geo(ctx);
@@ -552,10 +696,9 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
   if (ustep < 1) return set_error(ctx, EMSESG_ERR_ARG, "ustep must be >= 1");
   const emsesg_config& c = ctx->cfg;
-  if (c.npc > 0 && c.line_mode != 1)
-    return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "the FP32 form has no body absorption yet");
+  std::string why;
+  if (!bodies_supported(c, &why)) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "%s", why.c_str());
   int rc;
-  if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
   FxState& f = ctx->fx;
   Geo g = make_geo(ctx);
   int64_t nn = (int64_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
@@ -587,6 +730,9 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
   a.fr = fr; a.fj = fj;
   a.g = g;
   a.nesc = ctx->d_counter->nesc;
+  a.gc = ctx->d_counter;
+  a.surf = f.surf;
+  a.bd = make_bodies(c);
   a.status = ctx->d_status;
   a.diag = ctx->d_diag;
   dim3 grid((unsigned)f.ntiles, (unsigned)c.nspec);
@@ -594,6 +740,18 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
     EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<4>, grid, PUSH_BLOCK, smem, a);
   else
     EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<8>, grid, PUSH_BLOCK, smem, a);
+  // injected particles of the tail zones (general path, global deposits)
+  int64_t drawn = 0;
+  for (int is = 0; is < c.nspec; is++) {
+    if (f.ntail[is] == 0) continue;
+    EMSESG_LAUNCH(ctx, "fx_tail", k_fx_tail, nblk(f.ntail[is]), 256, 0, a, is, f.tail0[is], f.ntail[is],
+                  f.tailord + f.tailord_base[is], ustep, c.rng_mode == 1 ? ctx->d_randoms : nullptr, ctx->n_randoms,
+                  ctx->d_rand_pos, drawn, c.rng_seed, ctx->rng_stream, ctx->d_counter->nesc + is);
+    drawn += f.pending[is];
+    f.pending[is] = 0;
+  }
+  if (drawn && c.rng_mode == 1) EMSESG_LAUNCH(ctx, "fx_rand_advance", k_add_i64, 1, 1, 0, ctx->d_rand_pos, drawn);
+  if (a.bd.n > 0) EMSESG_LAUNCH(ctx, "fx_chgacm", k_fx_chgacm, 1, 32, 0, ctx->d_cfg, ctx->d_counter);
   // guard folding on the exact integers, then FP64 outputs
   if ((rc = run_slab_ops(ctx, (long long*)acc_rho, fr, fold_ops(c, 0, 1), "fx_fold_rho"))) return rc;
   if ((rc = run_slab_ops(ctx, (long long*)acc_j, fj, fold_ops(c, 1, 3), "fx_fold_j"))) return rc;
@@ -602,6 +760,63 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
   EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_double, nblk(fj.size()), 256, 0, (const long long*)acc_j,
                 ctx->field[EMSESG_FIELD_AJ], fj.size());
   ctx->rng_stream++;
+  // the re-sort after the push (so that injected particles take their
+  // first, partial step before they join the tile regions)
+  if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int64_t n) {
+  if (!ctx || n < 0 || (n > 0 && !host)) return EMSESG_ERR_ARG;
+  if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
+  const int is = spec - 1;
+  if (is < 0 || is >= ctx->cfg.nspec) return set_error(ctx, EMSESG_ERR_ARG, "species %d out of range", spec);
+  if (n == 0) return EMSESG_OK;
+  FxState& f = ctx->fx;
+  if (f.ntail[is] + n > f.tailcap[is])
+    return set_error(ctx, EMSESG_ERR_OVERFLOW, "tail zone of species %d full (%lld + %lld > %lld)", spec,
+                     (long long)f.ntail[is], (long long)n, (long long)f.tailcap[is]);
+  if (ctx->totalp[is] + n > ctx->seg.capacity[is])
+    return set_error(ctx, EMSESG_ERR_OVERFLOW, "species %d capacity %lld exceeded", spec,
+                     (long long)ctx->seg.capacity[is]);
+  if (n > f.stage_cap) {
+    cudaFree(f.stage);
+    cudaFree(f.stage_ord);
+    f.stage = nullptr;
+    f.stage_ord = nullptr;
+    f.stage_cap = 0;
+    EMSESG_CUDA(ctx, cudaMalloc(&f.stage, n * sizeof(emsesg_particle)));
+    EMSESG_CUDA(ctx, cudaMalloc(&f.stage_ord, n * sizeof(int32_t)));
+    f.stage_cap = n;
+  }
+  // ordinal of each injected particle's random step, in buffer order
+  std::vector<int32_t> ord((size_t)n, 0);
+  int64_t k1 = f.pending[is];
+  for (int64_t k = 0; k < n; k++)
+    if (host[k].preside == EMSESG_PCL_INJECTED && host[k].nid != -1) ord[(size_t)k] = (int32_t)(++k1);
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(f.stage, host, n * sizeof(emsesg_particle), cudaMemcpyHostToDevice, ctx->stream));
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(f.stage_ord, ord.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+  const int64_t off = f.base[is], slot0 = f.tail0[is] + f.ntail[is];
+  Bodies bd = make_bodies(ctx->cfg);
+  EMSESG_LAUNCH(ctx, "fx_inject", k_fx_inject, nblk(n), 256, 0, f.stage, f.stage_ord, n, make_geo(ctx), bd, slot0,
+                f.pos + off, f.vx + off, f.vy + off, f.vz + off, f.tailord + f.tailord_base[is] + f.ntail[is],
+                f.surf + (int64_t)is * f.nsurf, ctx->d_status, ctx->d_diag);
+  f.ntail[is] += n;
+  f.pending[is] = k1;
+  ctx->totalp[is] += n;
+  // the host copy of ord must outlive the asynchronous upload
+  return emsesg_synchronize(ctx);
+}
+
+extern "C" int emsesg_fx_surface(emsesg_ctx* ctx, int64_t* counts, int64_t* nsurf) {
+  if (!ctx || !nsurf) return EMSESG_ERR_ARG;
+  if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded");
+  *nsurf = ctx->fx.nsurf;
+  if (counts && ctx->fx.nsurf > 0) {
+    EMSESG_CUDA(ctx, cudaMemcpyAsync(counts, ctx->fx.surf, ctx->cfg.nspec * ctx->fx.nsurf * sizeof(int64_t),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   return EMSESG_OK;
 }
 

@@ -50,6 +50,18 @@ constexpr uint32_t ROW_BYTES = PUSH_THREADS * (16 + 3 * 4);
 static_assert(PUSH_THREADS == EMSESG_FX_ROW_SLOTS, "row width of the thread-major layout");
 static_assert(ROW_BYTES % 16 == 0 && (PUSH_THREADS * 4) % 16 == 0, "bulk copies move whole 16-byte units");
 
+// Box bodies of the FP32 form (geotype 0/1 with integer bounds): the
+// absorption test and the per-surface-cell counts.  Faces -x,+x,-y,+y,-z,+z;
+// a face's cells with its first tangential axis fastest (x faces: y then z;
+// y faces: x then z; z faces: x then y).
+struct Bodies {
+  int n;                        // box bodies
+  int ipc[EMSESG_INPC];         // their index in cfg.body
+  int lo[EMSESG_INPC][3], hi[EMSESG_INPC][3];
+  int64_t off[EMSESG_INPC][6];  // first surface cell of each face
+  int64_t nsurf;                // surface cells of all bodies
+};
+
 struct FxPushArgs {
   float4* pos;                  // all species regions
   float* vx;
@@ -69,6 +81,9 @@ struct FxPushArgs {
   Geo g;
   int64_t ntiles;
   int* nesc;                    // counter nesc(is), one int per species
+  emsesg_counter* gc;           // influx / infhist of the body absorption
+  unsigned long long* surf;     // [nspec][nsurf] absorbed - emitted counts
+  Bodies bd;
   int* status;
   long long* diag;
 };
@@ -381,7 +396,61 @@ struct CrossCtx {
   float* gvz;
   float gustep, rustep, qfix;
   int nb[3];
+  const Bodies* bd;
+  emsesg_counter* gc;
+  unsigned long long* surf;     // this species' surface counts
+  int is;
 };
+
+// Box absorption of the end point a = (ac, af) per axis (psolve1.F90:
+// 644-662, inclusive bounds); counts influx, infhist and the surface cell of
+// the face crossed last on the way from b = (ib, ob) (the rule of the oracle's
+// orc_surface_cell).  Returns true when the particle was absorbed.
+__device__ __forceinline__ bool body_absorb(const CrossCtx& c, const int (&ib)[3], const float (&ob)[3],
+                                            const Axis* a3) {
+  const Bodies& bd = *c.bd;
+  for (int q = 0; q < bd.n; q++) {
+    bool in = true;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const int ac = a3[d].ac;
+      in = in && ac >= bd.lo[q][d] && (ac < bd.hi[q][d] || (ac == bd.hi[q][d] && a3[d].af == 0.0f));
+    }
+    if (!in) continue;
+    const int ipc = bd.ipc[q];
+    atomicAdd(&c.gc->influx[c.is][ipc], 1);
+    atomicAdd(&c.gc->infhist[c.is][ipc][0], 1);
+    // face crossed last: the largest entry time along b -> a
+    int best = -1, side = 0;
+    float tb = -1.0f;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const int lo = bd.lo[q][d], hi = bd.hi[q][d];
+      const float den = (float)(a3[d].ac - ib[d]) + (a3[d].af - ob[d]);
+      float t = -1.0f;
+      int sd = 0;
+      if (ib[d] < lo) { t = ((float)(lo - ib[d]) - ob[d]) / den; sd = 0; }
+      else if (ib[d] > hi || (ib[d] == hi && ob[d] > 0.0f)) { t = ((float)(hi - ib[d]) - ob[d]) / den; sd = 1; }
+      if (t > tb) { tb = t; best = d; side = sd; }
+    }
+    if (best < 0) {  // start point inside: the nearest face of the end point
+      float dm = 3.0e38f;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const float x = (float)a3[d].ac + a3[d].af;
+        if (x - (float)bd.lo[q][d] < dm) { dm = x - (float)bd.lo[q][d]; best = d; side = 0; }
+        if ((float)bd.hi[q][d] - x < dm) { dm = (float)bd.hi[q][d] - x; best = d; side = 1; }
+      }
+    }
+    const int e1 = best == 0 ? 1 : 0, e2 = best == 2 ? 1 : 2;
+    const int u = min(max(a3[e1].ac, bd.lo[q][e1]), bd.hi[q][e1] - 1) - bd.lo[q][e1];
+    const int v = min(max(a3[e2].ac, bd.lo[q][e2]), bd.hi[q][e2] - 1) - bd.lo[q][e2];
+    const int64_t cellx = bd.off[q][2 * best + side] + u + (int64_t)(bd.hi[q][e1] - bd.lo[q][e1]) * v;
+    atomicAdd(&c.surf[cellx], 1ull);
+    return true;
+  }
+  return false;
+}
 
 // General path for one particle that left its cell (or whose cell lies
 // outside the box): boundary rules, zigzag with relay point, charge at the
@@ -401,7 +470,15 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
   if (ax.flip) vx = -vx;
   if (ay.flip) vy = -vy;
   if (az.flip) vz = -vz;
-  const bool dead = ax.dead || ay.dead || az.dead;
+  const bool escaped = ax.dead || ay.dead || az.dead;
+  bool absorbed = false;
+  if (!escaped && c.bd->n > 0) {
+    const int ib3[3] = {ib, jb, kb};
+    const float ob3[3] = {bx, by, bz};
+    const Axis a3[3] = {ax, ay, az};
+    absorbed = body_absorb(c, ib3, ob3, a3);
+  }
+  const bool dead = escaped || absorbed;
   const uint32_t nc = dead ? DEAD : pack(g, ax.nc, ay.nc, az.nc);
   c.gpos[loc] = make_float4(ax.nf, ay.nf, az.nf, __int_as_float((int)nc));
   c.gvx[loc] = vx;
@@ -422,10 +499,11 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
     w = xd * yd; J[11] = vvz * w; J[9] = vvz * (xd - w); J[10] = vvz * (yd - w); J[8] = vvz * (1.0f - xd - (yd - w));
   }
   // both segments in the cell of the start point (a particle that did not
-  // change cell): one set of node values
-  const bool one = ax.ia == ib && ay.ia == jb && az.ia == kb;
+  // change cell): one set of node values.  An absorbed particle stops at the
+  // relay point (psolve1.F90:660-662): no second segment.
+  const bool one = !absorbed && ax.ia == ib && ay.ia == jb && az.ia == kb;
   if (!one) put_j<B>(box, o, sk, ib, jb, kb, J, c.qfix);
-  {
+  if (!absorbed) {
     float J2[NJ];
     float xd = ((float)(ax.ac - ax.ia) + ax.af + (float)(ax.rc - ax.ia) + ax.rf) * 0.5f;
     float yd = ((float)(ay.ac - ay.ia) + ay.af + (float)(ay.rc - ay.ia) + ay.rf) * 0.5f;
@@ -452,7 +530,7 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
     R[6] = XY * Z2; R[5] = XZ2 - R[6]; R[7] = YZ2 - R[6]; R[4] = Z2 - XZ2 - R[7];
     put_r<B>(box, o, sk, ax.nc, ay.nc, az.nc, R, c.qfix);
   }
-  return dead ? 1 : 0;
+  return escaped ? 1 : 0;
 }
 
 // Returns the number of this lane's particles that escaped.
@@ -465,7 +543,8 @@ __device__ __forceinline__ int drain_cross(const FxPushArgs& a, int is, int64_t 
   const Geo& g = a.g;
   const Sink sk{a.acc_rho, a.acc_j, a.fr, a.fj, g.nx, g.ny, g.nz, a.status, a.diag};
   const CrossCtx c{a.pos + slot0, a.vx + slot0, a.vy + slot0, a.vz + slot0, a.gustep, a.rustep, a.qfix[is],
-                   {a.npbnd[is][0], a.npbnd[is][1], a.npbnd[is][2]}};
+                   {a.npbnd[is][0], a.npbnd[is][1], a.npbnd[is][2]}, &a.bd, a.gc,
+                   a.surf + (int64_t)is * a.bd.nsurf, is};
   int dead = 0;
   for (int p = 0; p < qn; p += 32) {
     int e = p + lane;
@@ -677,7 +756,10 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       sx = x1 + vx * gustep;
       syy = y1 + vy * gustep;
       szz = z1 + vz * gustep;
-      simple = cell == runcell && runbase >= 0 && sx >= 0.f && sx < 1.0f && syy >= 0.f && syy < 1.0f && szz >= 0.f && szz < 1.0f;
+      // an end point exactly on a cell face takes the general path (it may
+      // lie on a body face: inclusive bounds)
+      simple = cell == runcell && runbase >= 0 && sx > 0.f && sx < 1.0f && syy > 0.f && syy < 1.0f && szz > 0.f &&
+               szz < 1.0f;
     }
     if (simple) {
       // both zigzag segments in the same cell: relay point at the midpoint,
@@ -765,6 +847,78 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       atomicAdd(&a.acc_j[a.fj.at(comp - 1, i, j, k)], v);
     }
   }
+}
+
+// Injected particles of the tail zone of species `is`, one thread each: the
+// random fraction of the step for a particle injected since the last push
+// (psolve1.F90:150-156: gustep = ustep * U), gather from the global node
+// field, Buneman-Boris, and the general path with global deposits.
+__global__ void k_fx_tail(FxPushArgs a, int is, int64_t tail0, int64_t ntail, int32_t* ord, int ustep,
+                          const double* randoms, int64_t nrand, const int64_t* rand_pos, int64_t ord_base,
+                          uint64_t seed, uint64_t stream, int* nesc_out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ntail) return;
+  const Geo& g = a.g;
+  const int64_t base = a.off[is];
+  const int64_t slot = tail0 + k;
+  const float4 ps = a.pos[base + slot];
+  const uint32_t cell = (uint32_t)__float_as_int(ps.w);
+  if (cell == DEAD) return;
+  int ib, jb, kb;
+  unpack(g, cell, ib, jb, kb);
+  if (ib >= g.nx || jb >= g.ny || kb >= g.nz) {
+    report_bad(a.status, a.diag, SITE_FX_PUSH, base + slot, (long long)cell);
+    return;
+  }
+  float gus = (float)ustep;
+  const int32_t o1 = ord[k];
+  if (o1 > 0) {
+    double u;
+    const int64_t j = ord_base + o1 - 1;
+    if (randoms) {
+      const int64_t r = *rand_pos + j;
+      if (r >= nrand) {
+        atomicOr(a.status, ST_RANDOMS);
+        u = 0.0;
+      } else {
+        u = randoms[r];
+      }
+    } else {
+      u = hash_u01(seed, stream, (uint64_t)j);
+    }
+    gus = (float)((double)ustep * u);
+    ord[k] = 0;
+  }
+  const float qmp = (float)((double)a.qmp[is] / (double)a.gustep * (double)gus);
+  float vx = a.vx[base + slot], vy = a.vy[base + slot], vz = a.vz[base + slot];
+  const float x1 = ps.x, y1 = ps.y, z1 = ps.z;
+  const float xy1 = x1 * y1, xz1 = x1 * z1, yz1 = y1 * z1, z2 = 1.0f - z1;
+  const float xz2 = x1 * z2, yz2 = y1 * z2;
+  float wv[8];
+  wv[2] = xy1 * z1; wv[1] = xz1 - wv[2]; wv[3] = yz1 - wv[2]; wv[0] = z1 - xz1 - wv[3];
+  wv[6] = xy1 * z2; wv[5] = xz2 - wv[6]; wv[7] = yz2 - wv[6]; wv[4] = z2 - xz2 - wv[7];
+  float fe[3], fb[3];
+  const int64_t sy = g.nx + 1, sz = (int64_t)(g.nx + 1) * (g.ny + 1);
+  gather8<false>(a.f0, a.f1, ib + sy * jb + sz * kb, sy, sz, wv, fe, fb);
+  const float eex = fe[0] * qmp, eey = fe[1] * qmp, eez = fe[2] * qmp;
+  const float bbx = fb[0] * qmp, bby = fb[1] * qmp, bbz = fb[2] * qmp;
+  const float boris = 2.0f / (1.0f + bbx * bbx + bby * bby + bbz * bbz);
+  vx += eex; vy += eey; vz += eez;
+  const float vxt = vx + vy * bbz - vz * bby;
+  const float vyt = vy + vz * bbx - vx * bbz;
+  const float vzt = vz + vx * bby - vy * bbx;
+  vx += boris * (vyt * bbz - vzt * bby);
+  vy += boris * (vzt * bbx - vxt * bbz);
+  vz += boris * (vxt * bby - vyt * bbx);
+  vx += eex; vy += eey; vz += eez;
+  const Sink sk{a.acc_rho, a.acc_j, a.fr, a.fj, g.nx, g.ny, g.nz, a.status, a.diag};
+  const CrossCtx c{a.pos + base, a.vx + base, a.vy + base, a.vz + base, gus, a.rustep, a.qfix[is],
+                   {a.npbnd[is][0], a.npbnd[is][1], a.npbnd[is][2]}, &a.bd, a.gc,
+                   a.surf + (int64_t)is * a.bd.nsurf, is};
+  const float en[XQW] = {__int_as_float((int)slot), ps.w, ps.x, ps.y, ps.z, vx, vy, vz};
+  const int far[3] = {-(1 << 28), -(1 << 28), -(1 << 28)};  // no box: global deposits
+  const int esc = cross_one<11>(g, nullptr, far, sk, c, en);
+  if (esc) atomicAdd(nesc_out, esc);
 }
 
 // The compiled box edge for the largest tile edge tmax (<= 8).

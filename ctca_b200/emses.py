@@ -129,6 +129,8 @@ _SIGS = {
     "emsesg_fx_sort": (_I, [_P]),
     "emsesg_fx_counts": (_I, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "emsesg_fx_download_accum": (_I, [_P, _P]),
+    "emsesg_fx_inject": (_I, [_P, _I, _P, ctypes.c_int64]),
+    "emsesg_fx_surface": (_I, [_P, _P, ctypes.POINTER(ctypes.c_int64)]),
     "emsesg_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
     "emsesg_set_profiling": (_I, [_P, _I]),
     "emsesg_profile_report": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t]),
@@ -356,6 +358,20 @@ class Emses:
         return out[:nr].reshape(field_shape(self.cfg, "rho")), out[nr:].reshape(field_shape(self.cfg, "aj"))
 
     # -- synthetic loader and profile
+    def fx_inject(self, spec: int, records: np.ndarray):
+        """Injected particles of species `spec` (1-based): oh2_inject_particle."""
+        rec = np.ascontiguousarray(records, dtype=PARTICLE_DTYPE)
+        self._check(self.lib.emsesg_fx_inject(self.h, spec, rec.ctypes.data if rec.size else None, rec.size))
+
+    def fx_surface(self) -> np.ndarray:
+        """Absorbed minus emitted particles per surface cell, [nspec, nsurf]."""
+        n = ctypes.c_int64(0)
+        self._check(self.lib.emsesg_fx_surface(self.h, None, ctypes.byref(n)))
+        out = np.zeros((self.cfg.nspec, max(n.value, 0)), dtype=np.int64)
+        if n.value:
+            self._check(self.lib.emsesg_fx_surface(self.h, out.ctypes.data, ctypes.byref(n)))
+        return out
+
     def load_plasma(self, pl: Plasma):
         self._check(self.lib.emsesg_load_plasma(self.h, ctypes.byref(pl)))
 

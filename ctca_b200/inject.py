@@ -1,0 +1,128 @@
+"""Host-side particle supervisors of the injection rows: face emission from a
+box body (psuper3.F90:142-239) and open-boundary inflow along z
+(psuper2.F90:236-292).  They produce oh_particle records for
+Emses.fx_inject (emsesg_fx_inject); the reference's supervisors also run on
+the host and hand each new particle to oh2_inject_particle.
+
+Velocity tables.  The reference fills vnormf / vtangf / vzf / vzb / vxr / vyr
+at initialisation (src/main/inipin.F90:476-583) with npr samples of the flux
+distributions and draws table entries with addr = nprs + npr*U.  Here the
+tables hold the npr quantiles (k + 1/2)/npr of the same distributions:
+
+  tangential   Maxwellian N(drift, vth^2)
+  normal flux  v * exp(-(v - vd)^2 / (2 vth^2)) on v > 0 (flux through a face)
+
+Random numbers come from a numpy Generator (the reference uses MT19937
+through RANU0); the number and order of draws per particle follow the
+reference: 6 per emitted particle (u(4) unused), 5 per inflow particle.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+from scipy.special import erfinv
+
+from .emses import PARTICLE_DTYPE
+
+PCL_INJECTED = 1
+PCL_ANTI = -2
+
+
+def maxwell_table(vth: float, drift: float, npr: int) -> np.ndarray:
+    """npr quantiles of N(drift, vth^2)."""
+    p = (np.arange(npr) + 0.5) / npr
+    return drift + vth * math.sqrt(2.0) * erfinv(2.0 * p - 1.0)
+
+
+def flux_table(vth: float, vd: float, npr: int, sign: float = 1.0) -> np.ndarray:
+    """npr quantiles of the one-sided flux distribution along an axis:
+    f(v) ~ |v| exp(-(v - vd)^2 / (2 vth^2)) for sign*v > 0, with vd the
+    signed drift along the axis and sign the side of the flux (+1: v > 0,
+    -1: v < 0).  With vd = 0 it is the Rayleigh distribution
+    sign*vth*sqrt(-2 ln(1-p))."""
+    p = (np.arange(npr) + 0.5) / npr
+    vd = sign * vd
+    if vd == 0.0:
+        return sign * vth * np.sqrt(-2.0 * np.log1p(-p))
+    hi = max(vd, 0.0) + 12.0 * vth
+    v = np.linspace(0.0, hi, 200001)
+    f = v * np.exp(-0.5 * ((v - vd) / vth) ** 2)
+    cdf = np.concatenate([[0.0], np.cumsum(0.5 * (f[1:] + f[:-1]) * np.diff(v))])
+    cdf /= cdf[-1]
+    return sign * np.interp(p, cdf, v)
+
+
+def emission_count(istep: int, lstep: int, fluxf: float, injct: int, ustep: int) -> int:
+    """nemit of psuper3.F90:64-66."""
+    return (int((istep + lstep) * fluxf) - int((istep + lstep - injct) * fluxf)) * ustep
+
+
+# nemd -> (normal axis, sign); tangential axes follow psuper3.F90:152-185:
+# +-1: (vx | vy, vz), +-2: (vy | vz, vx), +-3: (vz | vx, vy)
+_ORDER = {1: (0, 1, 2), 2: (1, 2, 0), 3: (2, 0, 1)}
+
+
+def emit_rectangle(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int, vnormf: np.ndarray,
+                   vtangf: np.ndarray, rng: np.random.Generator, spec: int) -> np.ndarray:
+    """n emitted particles from a rectangular face (emit_from_rectangle,
+    psuper3.F90:142-208): each gives an anti-particle (preside -2) on the
+    face and its twin 1e-5 off the face along the normal (preside +1).
+    bounds1 / bounds2 are the face extents along the first / second
+    tangential axis of nemd.  Returns 2n records, anti-particle first."""
+    axis = _ORDER[abs(nemd)]
+    ud = 1.0 if nemd > 0 else -1.0
+    npr = vnormf.size
+    u = rng.random((n, 6))
+    out = np.zeros(2 * n, dtype=PARTICLE_DTYPE)
+    coords = [("x", "vx"), ("y", "vy"), ("z", "vz")]
+    a0 = (npr * u[:, 0]).astype(np.int64)
+    a1 = (npr * u[:, 1]).astype(np.int64)
+    a2 = (npr * u[:, 2]).astype(np.int64)
+    vn = ud * vnormf[a0]
+    vt1 = vtangf[a1]
+    vt2 = vtangf[a2]
+    rn = np.full(n, grd)
+    rt1 = bounds1[0] + (bounds1[1] - bounds1[0]) * u[:, 4]
+    rt2 = bounds2[0] + (bounds2[1] - bounds2[0]) * u[:, 5]
+    for val_r, val_v, ax in ((rn, vn, axis[0]), (rt1, vt1, axis[1]), (rt2, vt2, axis[2])):
+        c, v = coords[ax]
+        out[c][0::2] = val_r
+        out[c][1::2] = val_r
+        out[v][0::2] = val_v
+        out[v][1::2] = val_v
+    out[coords[axis[0]][0]][1::2] += ud * 1e-5
+    out["preside"][0::2] = PCL_ANTI
+    out["preside"][1::2] = PCL_INJECTED
+    out["spec"] = spec
+    out["pid"] = 0
+    out["nid"] = 0
+    return out
+
+
+def inflow_count(istep: int, lstep: int, arr: float, injct: int, ustep: int) -> int:
+    """narrzf / narrzb of psuper2.F90:238-239, 266-267."""
+    return (int((istep + lstep) * arr) - int((istep + lstep - injct) * arr)) * ustep
+
+
+def inflow_z(front: bool, n: int, nx: int, ny: int, nz: int, vz_table: np.ndarray, vx_table: np.ndarray,
+             vy_table: np.ndarray, injctisw: float, rng: np.random.Generator, spec: int,
+             zssurf: float = -1.0e30) -> np.ndarray:
+    """Particles entering through the z = 0 face (front) or z = nz face
+    (back), psuper2.F90:236-292: x, y uniform on the face, z = the distance
+    covered within the last injctisw steps, preside 0."""
+    npr = vz_table.size
+    u = rng.random((n, 5))
+    a1 = (npr * u[:, 0]).astype(np.int64)
+    a2 = (npr * u[:, 1]).astype(np.int64)
+    out = np.zeros(n, dtype=PARTICLE_DTYPE)
+    out["x"] = 0.0 + nx * u[:, 2]
+    out["y"] = 0.0 + ny * u[:, 3]
+    vz = vz_table[a1]
+    out["z"] = (vz * injctisw * u[:, 4]) if front else (nz + vz * injctisw * u[:, 4])
+    out["vx"] = vx_table[a2]
+    out["vy"] = vy_table[a2]
+    out["vz"] = vz
+    out["spec"] = spec
+    keep = out["z"] > zssurf
+    return out[keep]

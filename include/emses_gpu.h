@@ -239,6 +239,9 @@ int emsesg_fx_store(emsesg_ctx* ctx);
 /* One step: FP32 field relocation (grdcrt), push, zigzag J and CIC rho into
  * the fixed-point accumulators, guard folding, FP64 rho/aj outputs.  Sorts
  * (and compacts) first when do_sort != 0. */
+/* One step of the FP32 form: push of the tile regions and of the tail zone,
+ * zigzag J and CIC rho into int64 fixed point, guard folds, FP64 rho / aj;
+ * with do_sort, the re-sort after the push. */
 int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort);
 int emsesg_fx_sort(emsesg_ctx* ctx);
 /* Particle counts of the FP32 form (nspec entries). */
@@ -246,6 +249,24 @@ int emsesg_fx_counts(emsesg_ctx* ctx, int64_t* totalp);
 /* Raw fixed-point accumulators after the guard folding, int64 at 2^40:
  * rho in the rho layout followed by (jx, jy, jz) in the aj layout. */
 int emsesg_fx_download_accum(emsesg_ctx* ctx, int64_t* host);
+/* Injected particles of species `spec` (1-based), oh2_inject_particle
+ * (lib/ohhelp/ohhelp-1.1.1/ohhelp2.c:549) for the FP32 form: the records go
+ * to a tail zone that the next emsesg_fx_step pushes with the general path
+ * (preside +1: a random fraction U of the first step, psolve1.F90:150-156;
+ * drawn in buffer order after the species before it); an anti-particle
+ * (preside -2, the image of an emitted particle on a body face,
+ * psuper3.F90:203-206) removes one count from that face cell.  The next
+ * sort merges the tail into the tile regions (sorting with particles still
+ * waiting for their first push is an error). */
+int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int64_t n);
+/* Absorbed minus emitted particles per surface cell of the box bodies
+ * (geotype 0/1, integer bounds), int64 [nspec][nsurf]: body by body, faces
+ * -x,+x,-y,+y,-z,+z, each face's cells with its first tangential axis
+ * fastest (x faces: y then z; y faces: x then z; z faces: x then y).  A
+ * particle entering a box between two positions counts on the face it
+ * crossed last, in the cell holding its end point.  counts may be NULL to
+ * query nsurf. */
+int emsesg_fx_surface(emsesg_ctx* ctx, int64_t* counts, int64_t* nsurf);
 
 /* ---- synthetic plasma loader (seeded, on the device) -------------------- */
 typedef struct emsesg_plasma {

@@ -134,6 +134,106 @@ void radsq_of(const emsesg_config* c, double* radsq) {
   }
 }
 
+// Per-surface-cell absorbed-charge counts of the box bodies (a rule of this
+// project; the reference's own per-cell absorbed charge comes from its
+// finbound route only).  Bodies with geotype 0/1 and integer bounds have six
+// faces -x,+x,-y,+y,-z,+z; a face's cells are numbered with its first
+// tangential axis fastest (x faces: y then z; y faces: x then z; z faces:
+// x then y).  A particle entering the box between its start point b and its
+// end point a is counted on the face it crossed last (largest entry time
+// along the segment; ties take the lower axis), in the cell that holds a's
+// tangential coordinates.
+bool box_surface(const emsesg_body& b) {
+  if (!(b.geotype == 0 || b.geotype == 1)) return false;
+  const double v[6] = {b.xlpc, b.xupc, b.ylpc, b.yupc, b.zlpc, b.zupc};
+  for (int q = 0; q < 6; q++)
+    if (v[q] != std::floor(v[q])) return false;
+  return b.xupc > b.xlpc && b.yupc > b.ylpc && b.zupc > b.zlpc;
+}
+
+void body_bounds(const emsesg_body& b, int lo[3], int hi[3]) {
+  lo[0] = (int)b.xlpc; hi[0] = (int)b.xupc;
+  lo[1] = (int)b.ylpc; hi[1] = (int)b.yupc;
+  lo[2] = (int)b.zlpc; hi[2] = (int)b.zupc;
+}
+
+const int TAN1[3] = {1, 0, 0}, TAN2[3] = {2, 2, 1};
+
+int64_t face_cells(const int lo[3], const int hi[3], int d) {
+  return (int64_t)(hi[TAN1[d]] - lo[TAN1[d]]) * (hi[TAN2[d]] - lo[TAN2[d]]);
+}
+
+int64_t face_index(const int lo[3], const int hi[3], int d, const double a[3]) {
+  const int e1 = TAN1[d], e2 = TAN2[d];
+  int u = (int)std::floor(a[e1]), v = (int)std::floor(a[e2]);
+  u = std::min(std::max(u, lo[e1]), hi[e1] - 1) - lo[e1];
+  v = std::min(std::max(v, lo[e2]), hi[e2] - 1) - lo[e2];
+  return u + (int64_t)(hi[e1] - lo[e1]) * v;
+}
+
+}  // namespace
+
+extern "C" int64_t orc_surface_layout(const emsesg_config* c, int64_t* offsets) {
+  int64_t n = 0;
+  for (int ipc = 0; ipc < c->npc; ipc++) {
+    const emsesg_body& b = c->body[ipc];
+    bool on = box_surface(b);
+    int lo[3], hi[3];
+    if (on) body_bounds(b, lo, hi);
+    for (int f = 0; f < 6; f++) {
+      if (offsets) offsets[ipc * 6 + f] = n;
+      if (on) n += face_cells(lo, hi, f / 2);
+    }
+  }
+  return n;
+}
+
+extern "C" int64_t orc_surface_cell(const emsesg_config* c, int ipc, const double* bp, const double* ap) {
+  const emsesg_body& b = c->body[ipc];
+  if (!box_surface(b)) return -1;
+  int lo[3], hi[3];
+  body_bounds(b, lo, hi);
+  int64_t off[6 * EMSESG_INPC];
+  orc_surface_layout(c, off);
+  int best = -1, side = 0;
+  double tb = -1.0;
+  for (int d = 0; d < 3; d++) {
+    double t = -1.0;
+    int sd = 0;
+    if (bp[d] < lo[d]) { t = (lo[d] - bp[d]) / (ap[d] - bp[d]); sd = 0; }
+    else if (bp[d] > hi[d]) { t = (hi[d] - bp[d]) / (ap[d] - bp[d]); sd = 1; }
+    if (t > tb) { tb = t; best = d; side = sd; }
+  }
+  if (best < 0) {  // start point inside: the nearest face of the end point
+    double dm = 1e300;
+    for (int d = 0; d < 3; d++) {
+      if (ap[d] - lo[d] < dm) { dm = ap[d] - lo[d]; best = d; side = 0; }
+      if (hi[d] - ap[d] < dm) { dm = hi[d] - ap[d]; best = d; side = 1; }
+    }
+  }
+  return off[ipc * 6 + 2 * best + side] + face_index(lo, hi, best, ap);
+}
+
+// Face cell of a point lying on a box face (an emitted particle's
+// anti-particle), or -1.
+extern "C" int64_t orc_surface_point(const emsesg_config* c, int ipc, const double* p) {
+  const emsesg_body& b = c->body[ipc];
+  if (!box_surface(b)) return -1;
+  int lo[3], hi[3];
+  body_bounds(b, lo, hi);
+  int64_t off[6 * EMSESG_INPC];
+  orc_surface_layout(c, off);
+  for (int d = 0; d < 3; d++) {
+    const int e1 = TAN1[d], e2 = TAN2[d];
+    if (p[e1] < lo[e1] || p[e1] > hi[e1] || p[e2] < lo[e2] || p[e2] > hi[e2]) continue;
+    if (p[d] == (double)lo[d]) return off[ipc * 6 + 2 * d] + face_index(lo, hi, d, p);
+    if (p[d] == (double)hi[d]) return off[ipc * 6 + 2 * d + 1] + face_index(lo, hi, d, p);
+  }
+  return -1;
+}
+
+namespace {
+
 // Trilinear weights v1..v8 (psolve2.F90:166-183, charge.F90:173-192).
 struct W8 { double v1, v2, v3, v4, v5, v6, v7, v8; };
 inline W8 weights(double x1, double y1, double z1) {
@@ -489,7 +589,8 @@ int orc_positn(const emsesg_config* c, int ustep, emsesg_particle* pbuf, const i
 int orc_psolve1(const emsesg_config* c, int ustep, int func, double* wrk,
                 emsesg_particle* pbuf, const int64_t* totalp, const double* ranu,
                 int64_t nranu, int64_t* ranu_pos, uint64_t rng_stream,
-                double* aj, double* ajdg, emsesg_counter* gc) {
+                double* aj, double* ajdg, emsesg_counter* gc, int64_t* surf) {
+  const int64_t nsurf = orc_surface_layout(c, nullptr);
   FD fw = fd_of(c, EMSESG_FIELD_WRK), fa = fd_of(c, EMSESG_FIELD_AJ), fj = fd_of(c, EMSESG_FIELD_AJDG);
   double radsq[EMSESG_INPC];
   radsq_of(c, radsq);
@@ -535,6 +636,7 @@ int orc_psolve1(const emsesg_config* c, int ustep, int func, double* wrk,
       if (p.nid == -1) continue;
 
       double xlocalb = p.x - dxl, ylocalb = p.y - dyl, zlocalb = p.z - dzl;
+      const double xlocalb0 = xlocalb, ylocalb0 = ylocalb, zlocalb0 = zlocalb;
       int ib = (int)std::floor(xlocalb), jb = (int)std::floor(ylocalb), kb = (int)std::floor(zlocalb);
       double xb = ib, yb = jb, zb = kb;
       int i1b = ib + 1, j1b = jb + 1, k1b = kb + 1;
@@ -617,6 +719,12 @@ int orc_psolve1(const emsesg_config* c, int ustep, int func, double* wrk,
               p.nid = -1;
               gc->influx[is][ipc] += 1;
               if (p.pid >= 0 && p.pid <= EMSESG_INPC) gc->infhist[is][ipc][p.pid] += 1;
+              if (surf) {
+                const double bp[3] = {xlocalb0 + dxl, ylocalb0 + dyl, zlocalb0 + dzl};
+                const double ap[3] = {xlocala + dxl, ylocala + dyl, zlocala + dzl};
+                const int64_t sc = orc_surface_cell(c, ipc, bp, ap);
+                if (sc >= 0) surf[(int64_t)is * nsurf + sc] += 1;
+              }
               xlocala = xr; ylocala = yr; zlocala = zr;
             }
           } else if (b.geotype == 2) {
@@ -1094,7 +1202,7 @@ double orc_step_timed(const emsesg_config* c, int ustep, const double* wrk,
       tp[is] = hi - lo;
       int64_t pos = 0;
       orc_psolve1(c, ustep, 0, w.data(), pbuf + base + lo, tp.data(), nullptr, 0, &pos, 0,
-                  a.data(), nullptr, &gc);
+                  a.data(), nullptr, &gc, nullptr);
       std::vector<double> rr(rsz, 0.0);
       orc_charge(c, 0, pbuf + base + lo, tp.data(), rr.data(), nullptr, nullptr, nullptr);
       for (int64_t x = 0; x < rsz; x++) r[x] += rr[x];

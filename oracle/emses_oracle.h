@@ -48,7 +48,14 @@ int orc_positn(const emsesg_config* c, int ustep, emsesg_particle* pbuf, const i
 int orc_psolve1(const emsesg_config* c, int ustep, int func, double* wrk,
                 emsesg_particle* pbuf, const int64_t* totalp, const double* ranu,
                 int64_t nranu, int64_t* ranu_pos, uint64_t rng_stream,
-                double* aj, double* ajdg, emsesg_counter* gc);
+                double* aj, double* ajdg, emsesg_counter* gc, int64_t* surf);
+/* Per-surface-cell counts of box bodies (geotype 0/1, integer bounds):
+ * layout (faces -x,+x,-y,+y,-z,+z per body, first tangential axis fastest)
+ * and the cell of an entering particle (b -> a) or of a point on a face.
+ * surf in orc_psolve1 may be NULL; else [nspec][nsurf] counts are added. */
+int64_t orc_surface_layout(const emsesg_config* c, int64_t* offsets);
+int64_t orc_surface_cell(const emsesg_config* c, int ipc, const double* b, const double* a);
+int64_t orc_surface_point(const emsesg_config* c, int ipc, const double* p);
 void orc_charge(const emsesg_config* c, int func, emsesg_particle* pbuf,
                 const int64_t* totalp, double* rho, double* rhodg, double* rhobk,
                 double* rhobksp);

@@ -54,7 +54,10 @@ def lib() -> ctypes.CDLL:
         "orc_positn": (ctypes.c_int, [cfgp, ctypes.c_int, _P, i64p, _P, ctypes.c_int64, i64p, ctypes.c_uint64,
                                       ctypes.POINTER(Counter)]),
         "orc_psolve1": (ctypes.c_int, [cfgp, ctypes.c_int, ctypes.c_int, _P, _P, i64p, _P, ctypes.c_int64, i64p,
-                                       ctypes.c_uint64, _P, _P, ctypes.POINTER(Counter)]),
+                                       ctypes.c_uint64, _P, _P, ctypes.POINTER(Counter), _P]),
+        "orc_surface_layout": (ctypes.c_int64, [cfgp, _P]),
+        "orc_surface_cell": (ctypes.c_int64, [cfgp, ctypes.c_int, _P, _P]),
+        "orc_surface_point": (ctypes.c_int64, [cfgp, ctypes.c_int, _P]),
         "orc_charge": (None, [cfgp, ctypes.c_int, _P, i64p, _P, _P, _P, _P]),
         "orc_reduce_rho": (None, [cfgp, _P, ctypes.c_int]),
         "orc_reduce_aj": (None, [cfgp, _P]),
@@ -95,6 +98,8 @@ class Oracle:
         self.eb = np.ascontiguousarray(eb, dtype=np.float64).copy()
         self.f = {name: zeros(cfg, name) for name in FIELD_IDS if name != "eb"}
         self.gc = Counter()
+        self.nsurf = int(self.L.orc_surface_layout(ctypes.byref(cfg), None))
+        self.surf = np.zeros((cfg.nspec, max(self.nsurf, 1)), dtype=np.int64)
         self.ranu = np.zeros(0)
         self.ranu_pos = ctypes.c_int64(0)
         self.rng_stream = 0
@@ -132,7 +137,7 @@ class Oracle:
         rc = self.L.orc_psolve1(self._c(), ustep, func, self.f["wrk"].ctypes.data, self.pbuf.ctypes.data, tp,
                                 self.ranu.ctypes.data if self.ranu.size else None, self.ranu.size,
                                 ctypes.byref(self.ranu_pos), self.rng_stream, self.f["aj"].ctypes.data,
-                                self.f["ajdg"].ctypes.data, ctypes.byref(self.gc))
+                                self.f["ajdg"].ctypes.data, ctypes.byref(self.gc), self.surf.ctypes.data)
         self.rng_stream += 1
         if rc:
             raise RuntimeError("oracle psolve1: random numbers exhausted")

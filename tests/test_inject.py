@@ -1,0 +1,86 @@
+"""Host-side injection supervisors (ctca_b200/inject.py) and the oracle's
+surface-cell rule of the box bodies."""
+import ctypes
+import math
+
+import numpy as np
+
+from ctca_b200 import inject, inputs
+from oracle import oracle as O
+
+from helpers import case
+
+
+def test_flux_tables():
+    vth, npr = 0.3, 4000
+    r = inject.flux_table(vth, 0.0, npr)
+    assert np.all(np.diff(r) > 0) and r[0] > 0
+    assert abs(r.mean() - vth * math.sqrt(math.pi / 2)) < 2e-3 * vth
+    t = inject.maxwell_table(vth, 0.1, npr)
+    assert abs(t.mean() - 0.1) < 1e-6 and abs(t.std() - vth) < 5e-3 * vth
+    # drifting flux toward -z: all negative, faster than the drift on average
+    b = inject.flux_table(vth, -0.5, npr, sign=-1.0)
+    assert np.all(b < 0) and b.mean() < -0.5
+
+
+def test_emission_count_matches_the_reference_formula():
+    # (int((istep+lstep)*fluxf) - int((istep+lstep-injct)*fluxf)) * ustep
+    assert inject.emission_count(10, 0, 3.7, 1, 2) == (int(10 * 3.7) - int(9 * 3.7)) * 2
+    assert sum(inject.emission_count(s, 0, 0.25, 1, 1) for s in range(1, 9)) == 2
+
+
+def test_emit_rectangle_pairs():
+    rng = np.random.default_rng(3)
+    vn = inject.flux_table(0.01, 0.0, 256)
+    vt = inject.maxwell_table(0.01, 0.0, 256)
+    for nemd, ax in ((1, "x"), (-2, "y"), (3, "z")):
+        rec = inject.emit_rectangle(nemd, 16.0, (8.0, 16.0), (14.0, 18.0), 50, vn, vt, rng, spec=1)
+        anti, twin = rec[0::2], rec[1::2]
+        assert np.all(anti["preside"] == -2) and np.all(twin["preside"] == 1)
+        assert np.all(anti[ax] == 16.0)
+        assert np.allclose(twin[ax] - anti[ax], np.sign(nemd) * 1e-5)
+        assert np.all(np.sign(twin["v" + ax]) == np.sign(nemd))
+        for c in "xyz":
+            if c != ax:
+                assert np.array_equal(anti[c], twin[c])
+
+
+def test_inflow_positions():
+    rng = np.random.default_rng(4)
+    vz = inject.flux_table(0.05, -0.08, 512, sign=-1.0)
+    vx = inject.maxwell_table(0.05, 0.0, 512)
+    rec = inject.inflow_z(False, 1000, 24, 24, 32, vz, vx, vx, 1.0, rng, spec=1)
+    assert np.all(rec["z"] <= 32) and np.all(rec["z"] >= 32 + vz.min())
+    assert np.all(rec["vz"] < 0) and np.all(rec["preside"] == 0)
+    assert np.all((rec["x"] >= 0) & (rec["x"] < 24))
+
+
+def _box_cfg():
+    c = case(n=(24, 24, 32))
+    c.bodies = [dict(geotype=0, ncond=1, xlpc=8.0, xupc=16.0, ylpc=8.0, yupc=16.0, zlpc=14.0, zupc=18.0,
+                     sqdscaled=1.0)]
+    return inputs.make_config(c)
+
+
+def test_surface_layout_and_rule():
+    cfg = _box_cfg()
+    L = O.lib()
+    off = (ctypes.c_int64 * (6 * 15))()
+    n = L.orc_surface_layout(ctypes.byref(cfg), off)
+    # x faces 8x4, y faces 8x4, z faces 8x8
+    assert n == 2 * 32 + 2 * 32 + 2 * 64
+    assert list(off[:6]) == [0, 32, 64, 96, 128, 192]
+
+    def cell(b, a):
+        bb = (ctypes.c_double * 3)(*b)
+        aa = (ctypes.c_double * 3)(*a)
+        return L.orc_surface_cell(ctypes.byref(cfg), 0, bb, aa)
+
+    # through the +x face (x = 16) into cell y=10, z=15
+    assert cell((16.3, 10.5, 15.5), (15.8, 10.5, 15.5)) == 32 + (10 - 8) + 8 * (15 - 14)
+    # through the -z face (z = 14) at x=9, y=12
+    assert cell((9.5, 12.2, 13.9), (9.5, 12.2, 14.1)) == 128 + (9 - 8) + 8 * (12 - 8)
+    # corner: crosses x = 8 at t = 0.75, z = 14 at t = 0.5: the x face is crossed last
+    assert cell((7.7, 9.5, 13.8), (8.1, 9.5, 14.2)) == 0 + (9 - 8) + 8 * (14 - 14)
+    p = (ctypes.c_double * 3)(16.0, 11.25, 17.5)
+    assert L.orc_surface_point(ctypes.byref(cfg), 0, p) == 32 + 3 + 8 * 3
