@@ -443,8 +443,10 @@ __device__ __forceinline__ bool body_absorb(const CrossCtx& c, const int (&ib)[3
       }
     }
     const int e1 = best == 0 ? 1 : 0, e2 = best == 2 ? 1 : 2;
-    const int u = min(max(a3[e1].ac, bd.lo[q][e1]), bd.hi[q][e1] - 1) - bd.lo[q][e1];
-    const int v = min(max(a3[e2].ac, bd.lo[q][e2]), bd.hi[q][e2] - 1) - bd.lo[q][e2];
+    const int c1 = best == 0 ? a3[1].ac : a3[0].ac;  // selects keep a3 in registers
+    const int c2 = best == 2 ? a3[1].ac : a3[2].ac;
+    const int u = min(max(c1, bd.lo[q][e1]), bd.hi[q][e1] - 1) - bd.lo[q][e1];
+    const int v = min(max(c2, bd.lo[q][e2]), bd.hi[q][e2] - 1) - bd.lo[q][e2];
     const int64_t cellx = bd.off[q][2 * best + side] + u + (int64_t)(bd.hi[q][e1] - bd.lo[q][e1]) * v;
     atomicAdd(&c.surf[cellx], 1ull);
     return true;

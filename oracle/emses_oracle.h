@@ -89,6 +89,15 @@ double orc_step_timed(const emsesg_config* c, int ustep, const double* wrk,
                       emsesg_particle* pbuf, const int64_t* totalp, double* aj,
                       double* rho, int threads);
 
+/* Loss sum_steps sum_probe Jx^2 of K periodic steps and, when gE is not
+ * NULL, its gradients with respect to the node fields (gE, gB: [n^3][3],
+ * x fastest), the uniform e0 / b0 (g0[6]) and the initial velocities
+ * (gv[np][3]); particles are advanced in place.  Node fields exclude e0/b0.
+ * adjoint.cpp. */
+double orc_adjoint(const emsesg_config* c, int K, int ustep, const double* enode, const double* bnode,
+                   const double* e0b0, emsesg_particle* p, int64_t np, const int* probe_lo,
+                   const int* probe_hi, double* gE, double* gB, double* g0, double* gv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,8 @@ def lib() -> ctypes.CDLL:
         "orc_compact": (None, [cfgp, _P, i64p]),
         "orc_hash_u01": (ctypes.c_double, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
         "orc_load_plasma": (None, [cfgp, ctypes.POINTER(Plasma), _P, i64p]),
+        "orc_adjoint": (ctypes.c_double, [cfgp, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, ctypes.c_int64, _P, _P,
+                                          _P, _P, _P, _P]),
         "orc_step_timed": (ctypes.c_double, [cfgp, ctypes.c_int, _P, _P, i64p, _P, _P, ctypes.c_int]),
     }
     for name, (res, args) in sigs.items():
@@ -242,3 +244,25 @@ def ranu0_stream(seed: int, n: int) -> np.ndarray:
     s = ctypes.c_int(seed)
     L.mt_init_(ctypes.byref(s))
     return np.array([L.mtrand_real8_() for _ in range(n)])
+
+
+def adjoint(cfg: Config, K: int, ustep: int, enode: np.ndarray, bnode: np.ndarray, e0b0, pbuf: np.ndarray,
+            probe_lo, probe_hi, grad: bool = True):
+    """FP64 loss sum_steps sum_probe Jx^2 of K periodic steps and its
+    gradients (adjoint.cpp): returns (loss, gE, gB, g0, gv); node fields are
+    [n^3][3] with x fastest and exclude e0 / b0."""
+    p = np.ascontiguousarray(pbuf, dtype=PARTICLE_DTYPE).copy()
+    en = np.ascontiguousarray(enode, dtype=np.float64)
+    bn = np.ascontiguousarray(bnode, dtype=np.float64)
+    e0 = np.ascontiguousarray(e0b0, dtype=np.float64)
+    lo = (ctypes.c_int * 3)(*probe_lo)
+    hi = (ctypes.c_int * 3)(*probe_hi)
+    nn = cfg.nx * cfg.ny * cfg.nz
+    gE = np.zeros((nn, 3)) if grad else None
+    gB = np.zeros((nn, 3)) if grad else None
+    g0 = np.zeros(6) if grad else None
+    gv = np.zeros((p.size, 3)) if grad else None
+    ptr = (lambda a: a.ctypes.data if a is not None else None)
+    loss = lib().orc_adjoint(ctypes.byref(cfg), K, ustep, en.ctypes.data, bn.ctypes.data, e0.ctypes.data,
+                             p.ctypes.data, p.size, lo, hi, ptr(gE), ptr(gB), ptr(g0), ptr(gv))
+    return loss, gE, gB, g0, gv
