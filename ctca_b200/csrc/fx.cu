@@ -295,7 +295,8 @@ __global__ void __launch_bounds__(1024) k_tile_pad(const int64_t* __restrict__ t
 __global__ void k_fx_gather_tm(const float4* __restrict__ pos, const float* __restrict__ vx,
                                const float* __restrict__ vy, const float* __restrict__ vz,
                                const uint32_t* __restrict__ idx, const int64_t* __restrict__ ts,
-                               const int64_t* __restrict__ tp, float4* pos2, float* vx2, float* vy2, float* vz2) {
+                               const int64_t* __restrict__ tp, float4* pos2, float* vx2, float* vy2, float* vz2,
+                               uint32_t* inv) {
   const int t = blockIdx.x, tid = threadIdx.x;
   const int64_t n = ts[t + 1] - ts[t];
   if (n <= 0) return;
@@ -309,16 +310,19 @@ __global__ void k_fx_gather_tm(const float4* __restrict__ pos, const float* __re
       vx2[m] = vx[src];
       vy2[m] = vy[src];
       vz2[m] = vz[src];
+      inv[m] = src;
     } else {
       pos2[m] = make_float4(0.f, 0.f, 0.f, __int_as_float((int)DEAD));
       vx2[m] = 0.f;
       vy2[m] = 0.f;
       vz2[m] = 0.f;
+      inv[m] = DEAD;
     }
   }
 }
 
 #include "fx_sort.cuh"
+#include "fx_adjoint.cuh"
 
 inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
 
@@ -615,7 +619,8 @@ extern "C" int emsesg_fx_sort(emsesg_ctx* ctx) {
                   f.count_d + is);
     EMSESG_LAUNCH(ctx, "fx_tile_pad", k_tile_pad, 1, 1024, 0, ts, f.ntiles, tp, f.slots_d + is);
     EMSESG_LAUNCH(ctx, "fx_gather", k_fx_gather_tm, (unsigned)f.ntiles, PUSH_THREADS, 0, f.pos + off, f.vx + off,
-                  f.vy + off, f.vz + off, vo, ts, tp, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off);
+                  f.vy + off, f.vz + off, vo, ts, tp, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off,
+                  f.lcs_inv + off);
   }
   std::swap(f.pos, f.pos2);
   std::swap(f.vx, f.vx2);
@@ -828,4 +833,228 @@ extern "C" int emsesg_fx_download_accum(emsesg_ctx* ctx, int64_t* host) {
                                    cudaMemcpyDeviceToHost, ctx->stream));
   EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return EMSESG_OK;
+}
+
+namespace {
+
+// Device copy of the FP32 state (particle arrays of every species region and
+// the region layout) for the checkpoints of the adjoint.
+struct FxSnap {
+  float4* pos = nullptr;
+  float* vx = nullptr;
+  float* vy = nullptr;
+  float* vz = nullptr;
+  int64_t* ts = nullptr;
+  int64_t* tp = nullptr;
+  int64_t* counts = nullptr;  // count_d, slots_d
+};
+
+int snap_alloc(emsesg_ctx* ctx, FxSnap& sn, int64_t cap, int64_t nl) {
+  EMSESG_CUDA(ctx, cudaMalloc(&sn.pos, cap * sizeof(float4)));
+  EMSESG_CUDA(ctx, cudaMalloc(&sn.vx, cap * sizeof(float)));
+  EMSESG_CUDA(ctx, cudaMalloc(&sn.vy, cap * sizeof(float)));
+  EMSESG_CUDA(ctx, cudaMalloc(&sn.vz, cap * sizeof(float)));
+  EMSESG_CUDA(ctx, cudaMalloc(&sn.ts, nl * sizeof(int64_t)));
+  EMSESG_CUDA(ctx, cudaMalloc(&sn.tp, nl * sizeof(int64_t)));
+  EMSESG_CUDA(ctx, cudaMalloc(&sn.counts, 2 * EMSESG_ISPEC * sizeof(int64_t)));
+  return EMSESG_OK;
+}
+
+void snap_free(FxSnap& sn) {
+  cudaFree(sn.pos); cudaFree(sn.vx); cudaFree(sn.vy); cudaFree(sn.vz);
+  cudaFree(sn.ts); cudaFree(sn.tp); cudaFree(sn.counts);
+  sn = FxSnap();
+}
+
+int snap_copy(emsesg_ctx* ctx, bool save, FxSnap& sn, int64_t cap, int64_t nl) {
+  FxState& f = ctx->fx;
+  const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+  cudaStream_t st = ctx->stream;
+#define EMSESG_SNAP(dst, src, bytes) EMSESG_CUDA(ctx, cudaMemcpyAsync(save ? (void*)(dst) : (void*)(src), \
+                                                 save ? (const void*)(src) : (const void*)(dst), bytes, k, st))
+  EMSESG_SNAP(sn.pos, f.pos, cap * sizeof(float4));
+  EMSESG_SNAP(sn.vx, f.vx, cap * sizeof(float));
+  EMSESG_SNAP(sn.vy, f.vy, cap * sizeof(float));
+  EMSESG_SNAP(sn.vz, f.vz, cap * sizeof(float));
+  EMSESG_SNAP(sn.ts, f.tile_start, nl * sizeof(int64_t));
+  EMSESG_SNAP(sn.tp, f.tile_pad, nl * sizeof(int64_t));
+  EMSESG_SNAP(sn.counts, f.count_d, EMSESG_ISPEC * sizeof(int64_t));
+  EMSESG_SNAP(sn.counts + EMSESG_ISPEC, f.slots_d, EMSESG_ISPEC * sizeof(int64_t));
+#undef EMSESG_SNAP
+  return EMSESG_OK;
+}
+
+}  // namespace
+
+extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, int sort_every,
+                                 const int32_t* probe_lo, const int32_t* probe_hi, double* loss, double* gE,
+                                 double* gB, double* g0, double* gv) {
+  if (!ctx || !probe_lo || !probe_hi || !loss) return EMSESG_ERR_ARG;
+  FxState& f = ctx->fx;
+  if (!f.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
+  const emsesg_config& c = ctx->cfg;
+  if (K < 1 || ckpt < 1 || ckpt > 64 || K % ckpt != 0 || ustep < 1 || sort_every < 1)
+    return set_error(ctx, EMSESG_ERR_ARG, "adjoint: K >= 1 a multiple of ckpt (1..64), ustep, sort_every >= 1");
+  for (int is = 0; is < c.nspec; is++) {
+    for (int d = 0; d < 3; d++)
+      if (c.npbnd[is][d] != 0) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "adjoint: periodic particles only");
+    if (f.ntail[is]) return set_error(ctx, EMSESG_ERR_STATE, "adjoint: injected particles pending");
+  }
+  for (int d = 0; d < 3; d++)
+    if (c.nfbnd[d] != 0) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "adjoint: periodic fields only");
+  if (c.npc > 0 && c.line_mode != 1) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "adjoint: no bodies");
+  int tmax = std::max(f.tile[0], std::max(f.tile[1], f.tile[2]));
+  int64_t cap = 0;
+  for (int is = 0; is < c.nspec; is++) cap += f.cap[is];
+  const int64_t nl = (int64_t)c.nspec * (f.ntiles + 1);
+  const int64_t nn = (int64_t)c.nx * c.ny * c.nz;
+  const int nseg = K / ckpt;
+  Geo g = make_geo(ctx);
+  FieldDesc fj = field_desc(c, EMSESG_FIELD_AJ);
+  const int3 lo = make_int3(probe_lo[0], probe_lo[1], probe_lo[2]);
+  const int3 hi = make_int3(probe_hi[0], probe_hi[1], probe_hi[2]);
+  // buffers: checkpoints, the states and sort maps of one segment, the
+  // probe Jx of one segment, lambda, g, node-field gradients
+  std::vector<FxSnap> ck((size_t)nseg + 1), seg((size_t)ckpt);
+  std::vector<uint32_t*> inv((size_t)ckpt, nullptr);
+  float *lam = nullptr, *lam2 = nullptr, *jx = nullptr, *gd = nullptr, *gEd = nullptr, *gBd = nullptr;
+  double *lossd = nullptr, *gvd = nullptr;
+  int rc = EMSESG_OK;
+  auto cleanup = [&]() {
+    for (auto& s : ck) snap_free(s);
+    for (auto& s : seg) snap_free(s);
+    for (auto* p : inv) cudaFree(p);
+    cudaFree(lam); cudaFree(lam2); cudaFree(jx); cudaFree(gd); cudaFree(gEd); cudaFree(gBd);
+    cudaFree(lossd); cudaFree(gvd);
+  };
+#define EMSESG_ADJ(call) do { rc = (call); if (rc) { cleanup(); return rc; } } while (0)
+  for (auto& s : ck) EMSESG_ADJ(snap_alloc(ctx, s, cap, nl));
+  for (auto& s : seg) EMSESG_ADJ(snap_alloc(ctx, s, cap, nl));
+  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&lam, 6 * cap * sizeof(float)), "adjoint lambda"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&lam2, 6 * cap * sizeof(float)), "adjoint lambda"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&jx, (size_t)ckpt * nn * sizeof(float)), "adjoint jx"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&gd, 3 * nn * sizeof(float)), "adjoint g"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&gEd, 3 * nn * sizeof(float)), "adjoint gE"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&gBd, 3 * nn * sizeof(float)), "adjoint gB"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&lossd, sizeof(double)), "adjoint loss"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(lossd, 0, sizeof(double), ctx->stream), "adjoint loss"));
+  // forward: K steps with a checkpoint every ckpt steps, the loss on the way
+  for (int n = 0; n < K; n++) {
+    if (n % ckpt == 0) EMSESG_ADJ(snap_copy(ctx, true, ck[(size_t)(n / ckpt)], cap, nl));
+    EMSESG_ADJ(emsesg_fx_step(ctx, ustep, (n + 1) % sort_every == 0 ? 1 : 0));
+    EMSESG_LAUNCH(ctx, "adj_probe", k_adj_probe, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_AJ], fj, g, lo, hi,
+                  lossd, (float*)nullptr);
+  }
+  EMSESG_ADJ(snap_copy(ctx, true, ck[(size_t)nseg], cap, nl));  // the state after K steps, restored at the end
+  // backward
+  float* lx = lam;
+  EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(lam, 0, 6 * cap * sizeof(float), ctx->stream), "adjoint lambda"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(gEd, 0, 3 * nn * sizeof(float), ctx->stream), "adjoint gE"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(gBd, 0, 3 * nn * sizeof(float), ctx->stream), "adjoint gB"));
+  AdjArgs a{};
+  for (int is = 0; is < c.nspec; is++) {
+    a.off[is] = f.base[is];
+    a.qmp[is] = (float)(c.qm[is] * ustep * 0.5);
+    a.q[is] = (float)c.q[is];
+  }
+  a.us = (float)ustep;
+  a.rustep = (float)(1.0 / ustep);
+  a.f0 = f.fnode;
+  a.f1 = f.fnode2;
+  a.g = gd;
+  a.gE = gEd;
+  a.gB = gBd;
+  a.geo = g;
+  a.ntiles = f.ntiles;
+  const int asmem = fx_adjoint_smem(tmax);
+  dim3 grid((unsigned)f.ntiles, (unsigned)c.nspec);
+  for (int sgi = nseg - 1; sgi >= 0; sgi--) {
+    EMSESG_ADJ(snap_copy(ctx, false, ck[(size_t)sgi], cap, nl));
+    bool sorted[64] = {false};
+    for (int j = 0; j < ckpt; j++) {
+      const int n = sgi * ckpt + j;
+      EMSESG_ADJ(snap_copy(ctx, true, seg[(size_t)j], cap, nl));
+      const bool srt = (n + 1) % sort_every == 0;
+      // slots past the new regions keep no map from an earlier sort
+      if (srt) EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(f.lcs_inv, 0xFF, cap * sizeof(uint32_t), ctx->stream), "inv"));
+      EMSESG_ADJ(emsesg_fx_step(ctx, ustep, srt ? 1 : 0));
+      EMSESG_LAUNCH(ctx, "adj_probe", k_adj_probe, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_AJ], fj, g, lo, hi,
+                    (double*)nullptr, jx + (int64_t)j * nn);
+      if (srt && j < 64) {
+        if (!inv[(size_t)j]) EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&inv[(size_t)j], cap * sizeof(uint32_t)), "inv"));
+        EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(inv[(size_t)j], f.lcs_inv, cap * sizeof(uint32_t),
+                                                   cudaMemcpyDeviceToDevice, ctx->stream), "inv"));
+        sorted[j] = true;
+      }
+    }
+    for (int j = ckpt - 1; j >= 0; j--) {
+      if (j < 64 && sorted[j]) {
+        // lambda of S_{n+1} (sorted layout) back to the layout of S_n
+        EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(lam2, 0, 6 * cap * sizeof(float), ctx->stream), "lambda"));
+        for (int is = 0; is < c.nspec; is++) {
+          const int64_t off = f.base[is];
+          EMSESG_LAUNCH(ctx, "adj_unsort", k_adj_unsort, nblk(f.cap[is]), 256, 0, inv[(size_t)j] + off, f.cap[is],
+                        lx + off, lx + cap + off, lx + 2 * cap + off, lx + 3 * cap + off, lx + 4 * cap + off,
+                        lx + 5 * cap + off, lam2 + off, lam2 + cap + off, lam2 + 2 * cap + off, lam2 + 3 * cap + off,
+                        lam2 + 4 * cap + off, lam2 + 5 * cap + off);
+        }
+        std::swap(lam, lam2);
+        lx = lam;
+      }
+      EMSESG_LAUNCH(ctx, "adj_g", k_adj_g, nblk(nn), 256, 0, jx + (int64_t)j * nn, nn, gd);
+      const FxSnap& sn = seg[(size_t)j];
+      a.pos = sn.pos; a.vx = sn.vx; a.vy = sn.vy; a.vz = sn.vz;
+      a.tile_start = sn.ts; a.tile_pad = sn.tp;
+      a.lx = lx; a.ly = lx + cap; a.lz = lx + 2 * cap; a.lvx = lx + 3 * cap; a.lvy = lx + 4 * cap; a.lvz = lx + 5 * cap;
+      if (fx_box_tile(tmax) == 4) {
+        EMSESG_ADJ(check_cuda(ctx, cudaFuncSetAttribute(k_fx_adjoint<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        asmem), "adjoint smem"));
+        EMSESG_LAUNCH(ctx, "fx_adjoint", k_fx_adjoint<4>, grid, PUSH_THREADS, asmem, a);
+      } else {
+        EMSESG_ADJ(check_cuda(ctx, cudaFuncSetAttribute(k_fx_adjoint<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        asmem), "adjoint smem"));
+        EMSESG_LAUNCH(ctx, "fx_adjoint", k_fx_adjoint<8>, grid, PUSH_THREADS, asmem, a);
+      }
+    }
+  }
+  // outputs: lambda_v of the start state in canonical order, node gradients
+  int64_t ntot = 0, rank0[EMSESG_ISPEC];
+  int64_t cnt0[2 * EMSESG_ISPEC];
+  EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(cnt0, ck[0].counts, sizeof(cnt0), cudaMemcpyDeviceToHost, ctx->stream),
+                        "counts"));
+  EMSESG_ADJ(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "sync"));
+  for (int is = 0; is < c.nspec; is++) { rank0[is] = ntot; ntot += cnt0[is]; }
+  if (gv) {
+    EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&gvd, std::max<int64_t>(ntot, 1) * 3 * sizeof(double)), "gv"));
+    for (int is = 0; is < c.nspec; is++) {
+      const int64_t off = f.base[is];
+      EMSESG_LAUNCH(ctx, "adj_canonical", k_adj_canonical, (unsigned)f.ntiles, PUSH_THREADS, 0, lx + 3 * cap + off,
+                    lx + 4 * cap + off, lx + 5 * cap + off, ck[0].ts + (int64_t)is * (f.ntiles + 1),
+                    ck[0].tp + (int64_t)is * (f.ntiles + 1), rank0[is], gvd);
+    }
+    EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(gv, gvd, ntot * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                                               ctx->stream), "gv"));
+  }
+  std::vector<float> hE((size_t)(3 * nn)), hB((size_t)(3 * nn));
+  EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(hE.data(), gEd, 3 * nn * sizeof(float), cudaMemcpyDeviceToHost,
+                                             ctx->stream), "gE"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(hB.data(), gBd, 3 * nn * sizeof(float), cudaMemcpyDeviceToHost,
+                                             ctx->stream), "gB"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(loss, lossd, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+                        "loss"));
+  EMSESG_ADJ(snap_copy(ctx, false, ck[(size_t)nseg], cap, nl));
+  EMSESG_ADJ(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "sync"));
+  double s0[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t u = 0; u < nn; u++)
+    for (int k = 0; k < 3; k++) {
+      s0[k] += hE[(size_t)(3 * u + k)];
+      s0[3 + k] += hB[(size_t)(3 * u + k)];
+      if (gE) gE[3 * u + k] = hE[(size_t)(3 * u + k)];
+      if (gB) gB[3 * u + k] = hB[(size_t)(3 * u + k)];
+    }
+  if (g0)
+    for (int k = 0; k < 6; k++) g0[k] = s0[k];
+  cleanup();
+#undef EMSESG_ADJ
+  return emsesg_synchronize(ctx);
 }

@@ -1,0 +1,357 @@
+// fx_adjoint.cuh -- reverse-mode (adjoint) step of the FP32 form on a
+// periodic grid (included by fx.cu after fx_push.cuh).
+//
+// One CTA per (tile, species) region of the thread-major layout, one thread
+// per column as in the push.  For the particle state S_n of step n and the
+// adjoint (lambda_x, lambda_v) of S_{n+1}, each particle recomputes its
+// forward step (trilinear gather of the node fields, Buneman-Boris, move,
+// zigzag relay points) and runs it backwards:
+//   zigzag     dS/da, dS/db of S = sum_nodes g . J_particle, g = dL/dJ of
+//              this step on the nodes (2 Jx on the probe nodes)
+//   move       a = b + v_{n+1} ustep: lambda_v += ustep lambda_a,
+//              lambda_b += lambda_a
+//   Boris      the rotation transposed term by term -> lambda_v_n,
+//              lambda_E, lambda_B at the particle
+//   gather     w_c lambda_E, w_c lambda_B added to the node-field gradients
+//              (shared-memory box, then global float atomics);
+//              sum_c grad(w_c) (E_c . lambda_E + B_c . lambda_B) added to
+//              lambda_x
+// The same formulas in FP64 are the CPU checker (oracle/adjoint.cpp).
+
+struct AdjArgs {
+  const float4* pos;
+  const float* vx;
+  const float* vy;
+  const float* vz;
+  float* lx;                    // adjoint of the position (x, y, z)
+  float* ly;
+  float* lz;
+  float* lvx;                   // adjoint of the velocity
+  float* lvy;
+  float* lvz;
+  const int64_t* tile_start;
+  const int64_t* tile_pad;
+  int64_t off[EMSESG_ISPEC];
+  float qmp[EMSESG_ISPEC], q[EMSESG_ISPEC];
+  float us, rustep;
+  const float4* __restrict__ f0;  // node fields (nodes 0..n per axis)
+  const float4* __restrict__ f1;
+  const float* __restrict__ g;    // dL/dJ per unique node, 3 components
+  float* gE;                      // node-field gradients per unique node, 3 + 3
+  float* gB;
+  Geo geo;
+  int64_t ntiles;
+};
+
+__device__ __forceinline__ int64_t unique_node(const Geo& G, int i, int j, int k) {
+  i %= G.nx; if (i < 0) i += G.nx;
+  j %= G.ny; if (j < 0) j += G.ny;
+  k %= G.nz; if (k < 0) k += G.nz;
+  return (int64_t)i + (int64_t)G.nx * ((int64_t)j + (int64_t)G.ny * k);
+}
+
+template <int B>
+struct AdjBox {
+  const int* o;
+  const float* gs;  // box g, 3 per node
+  const Geo* G;
+  const float* gglob;
+  __device__ float g(int comp, int i, int j, int k) const {
+    const int li = i - o[0], lj = j - o[1], lk = k - o[2];
+    if ((unsigned)li < (unsigned)B && (unsigned)lj < (unsigned)B && (unsigned)lk < (unsigned)B)
+      return gs[3 * ((lk * B + lj) * B + li) + comp];
+    return gglob[3 * unique_node(*G, i, j, k) + comp];
+  }
+};
+
+// dS/da and dS/db (local coordinates of cell b) of the zigzag deposit.
+template <int B>
+__device__ __forceinline__ void zigzag_adj(const AdjBox<B>& bx, const int (&cb)[3], const int (&ca)[3],
+                                           const float (&bl)[3], const float (&al)[3], float q, float rustep,
+                                           float (&dSda)[3], float (&dSdb)[3]) {
+  float r[3], drd[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const bool same = ca[k] == cb[k];
+    r[k] = same ? 0.5f * (al[k] + bl[k]) : (ca[k] > cb[k] ? 1.0f : 0.0f);
+    drd[k] = same ? 0.5f : 0.0f;
+    dSda[k] = 0.f;
+    dSdb[k] = 0.f;
+  }
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    float F[3], d[3], dFa[3], dFb[3], dda[3], ddb[3];
+    int cell[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      if (s == 0) {
+        F[k] = (r[k] - bl[k]) * rustep;
+        d[k] = 0.5f * (r[k] + bl[k]);
+        dFa[k] = drd[k] * rustep; dFb[k] = (drd[k] - 1.0f) * rustep;
+        dda[k] = 0.5f * drd[k]; ddb[k] = 0.5f * (drd[k] + 1.0f);
+        cell[k] = cb[k];
+      } else {
+        const float sh = (float)(ca[k] - cb[k]);
+        F[k] = (al[k] - r[k]) * rustep;
+        d[k] = 0.5f * (al[k] + r[k]) - sh;
+        dFa[k] = (1.0f - drd[k]) * rustep; dFb[k] = -drd[k] * rustep;
+        dda[k] = 0.5f * (1.0f + drd[k]); ddb[k] = 0.5f * drd[k];
+        cell[k] = ca[k];
+      }
+    }
+#pragma unroll
+    for (int comp = 0; comp < 3; comp++) {
+      const int p1 = comp == 0 ? 1 : 0, p2 = comp == 2 ? 1 : 2;
+      float Gv = 0.f, dG1 = 0.f, dG2 = 0.f;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int u = e & 1, v = e >> 1;
+        int nd[3] = {cell[0], cell[1], cell[2]};
+        nd[p1] += u;
+        nd[p2] += v;
+        const float W1 = u ? d[p1] : 1.0f - d[p1], W2 = v ? d[p2] : 1.0f - d[p2];
+        const float gn = bx.g(comp, nd[0], nd[1], nd[2]);
+        Gv += gn * W1 * W2;
+        dG1 += gn * (u ? 1.0f : -1.0f) * W2;
+        dG2 += gn * W1 * (v ? 1.0f : -1.0f);
+      }
+      dSda[comp] += q * Gv * dFa[comp];
+      dSdb[comp] += q * Gv * dFb[comp];
+      dSda[p1] += q * F[comp] * dG1 * dda[p1];
+      dSdb[p1] += q * F[comp] * dG1 * ddb[p1];
+      dSda[p2] += q * F[comp] * dG2 * dda[p2];
+      dSdb[p2] += q * F[comp] * dG2 * ddb[p2];
+    }
+  }
+}
+
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 mul3(float s, float3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+template <int T>
+__global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
+  constexpr int B = T + 2 * PG + 1;
+  constexpr int NF = B * B * B;
+  extern __shared__ __align__(16) float4 adj_smem[];
+  float4* sf0 = adj_smem;
+  float4* sf1 = sf0 + NF;
+  float* sg = reinterpret_cast<float*>(sf1 + NF);  // 3 per node
+  float* sgr = sg + 3 * NF;                        // 6 per node: dE (3), dB (3)
+  const Geo& G = a.geo;
+  const int is = blockIdx.y, t = blockIdx.x, tid = threadIdx.x;
+  const int64_t* ts = a.tile_start + (int64_t)is * (a.ntiles + 1);
+  const int64_t n = ts[t + 1] - ts[t];
+  if (n <= 0) return;
+  const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
+  const int64_t slot0 = a.off[is] + a.tile_pad[(int64_t)is * (a.ntiles + 1) + t];
+  const int tx = t % G.nt[0], ty = (t / G.nt[0]) % G.nt[1], tz = t / (G.nt[0] * G.nt[1]);
+  const int o[3] = {tx * G.t[0] - PG, ty * G.t[1] - PG, tz * G.t[2] - PG};
+  const int64_t sy = G.nx + 1, sz = (int64_t)(G.nx + 1) * (G.ny + 1);
+  for (int e = tid; e < NF; e += PUSH_THREADS) {
+    const int li = e % B, lj = (e / B) % B, lk = e / (B * B);
+    const int gi = o[0] + li, gj = o[1] + lj, gk = o[2] + lk;
+    float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p;
+    if (gi >= 0 && gj >= 0 && gk >= 0 && gi <= G.nx && gj <= G.ny && gk <= G.nz) {
+      const int64_t gn = gi + sy * gj + sz * gk;
+      p = __ldg(&a.f0[gn]);
+      q = __ldg(&a.f1[gn]);
+    }
+    sf0[e] = p;
+    sf1[e] = q;
+    const int64_t un = unique_node(G, gi, gj, gk);
+#pragma unroll
+    for (int c = 0; c < 3; c++) sg[3 * e + c] = a.g[3 * un + c];
+#pragma unroll
+    for (int c = 0; c < 6; c++) sgr[6 * e + c] = 0.f;
+  }
+  __syncthreads();
+  const AdjBox<B> bx{o, sg, &G, a.g};
+  const float qmp = a.qmp[is], qq = a.q[is], us = a.us, rustep = a.rustep;
+  for (int r = 0; r < L; r++) {
+    const int64_t m = slot0 + (int64_t)r * PUSH_THREADS + tid;
+    const float4 ps = a.pos[m];
+    const uint32_t cell = (uint32_t)__float_as_int(ps.w);
+    if (cell == DEAD) continue;
+    int cb[3];
+    unpack(G, cell, cb[0], cb[1], cb[2]);
+    const float bl[3] = {ps.x, ps.y, ps.z};
+    const float3 v0 = f3(a.vx[m], a.vy[m], a.vz[m]);
+    // forward recompute: gather (corner c = di + 2 dj + 4 dk)
+    float3 E = f3(0.f, 0.f, 0.f), Bf = E;
+    float4 cp[8], cq[8];
+    const int li = cb[0] - o[0], lj = cb[1] - o[1], lk = cb[2] - o[2];
+    const bool inb = (unsigned)li < (unsigned)(B - 1) && (unsigned)lj < (unsigned)(B - 1) && (unsigned)lk < (unsigned)(B - 1);
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int di = c & 1, dj = (c >> 1) & 1, dk = c >> 2;
+      if (inb) {
+        const int e = ((lk + dk) * B + (lj + dj)) * B + (li + di);
+        cp[c] = sf0[e];
+        cq[c] = sf1[e];
+      } else {
+        const int64_t gn = (cb[0] + di) + sy * (cb[1] + dj) + sz * (cb[2] + dk);
+        cp[c] = __ldg(&a.f0[gn]);
+        cq[c] = __ldg(&a.f1[gn]);
+      }
+      const float X = di ? bl[0] : 1.0f - bl[0], Y = dj ? bl[1] : 1.0f - bl[1], Z = dk ? bl[2] : 1.0f - bl[2];
+      const float w = X * Y * Z;
+      E = add3(E, mul3(w, f3(cp[c].x, cp[c].y, cp[c].z)));
+      Bf = add3(Bf, mul3(w, f3(cp[c].w, cq[c].x, cq[c].y)));
+    }
+    const float3 ee = mul3(qmp, E), tt = mul3(qmp, Bf);
+    const float sfac = 2.0f / (1.0f + dot3(tt, tt));
+    const float3 uu = add3(v0, ee);
+    const float3 ww = add3(uu, cross3(uu, tt));
+    const float3 cc = cross3(ww, tt);
+    const float3 pp = add3(uu, mul3(sfac, cc));
+    const float3 vn = add3(pp, ee);
+    const float vnv[3] = {vn.x, vn.y, vn.z};
+    float al[3];
+    int ca[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      al[k] = bl[k] + vnv[k] * us;
+      ca[k] = cb[k] + (int)floorf(al[k]);
+    }
+    float dSda[3], dSdb[3];
+    zigzag_adj<B>(bx, cb, ca, bl, al, qq, rustep, dSda, dSdb);
+    // move: a = b + vnew * ustep
+    const float3 la = f3(a.lx[m] + dSda[0], a.ly[m] + dSda[1], a.lz[m] + dSda[2]);
+    const float3 lvn = add3(f3(a.lvx[m], a.lvy[m], a.lvz[m]), mul3(us, la));
+    float3 lb = add3(f3(dSdb[0], dSdb[1], dSdb[2]), la);
+    // Boris, reversed
+    float3 le = lvn;
+    const float3 lp = lvn;
+    float3 lu = lp;
+    const float ls = dot3(lp, cc);
+    const float3 lc = mul3(sfac, lp);
+    const float3 lw = cross3(tt, lc);
+    float3 lt = cross3(lc, ww);
+    lu = add3(add3(lu, lw), cross3(tt, lw));
+    lt = add3(lt, cross3(lw, uu));
+    lt = add3(lt, mul3(-ls * sfac * sfac, tt));
+    le = add3(le, lu);
+    const float3 lE = mul3(qmp, le), lB = mul3(qmp, lt);
+    // gather, reversed
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int di = c & 1, dj = (c >> 1) & 1, dk = c >> 2;
+      const float X = di ? bl[0] : 1.0f - bl[0], Y = dj ? bl[1] : 1.0f - bl[1], Z = dk ? bl[2] : 1.0f - bl[2];
+      const float dX = di ? 1.0f : -1.0f, dY = dj ? 1.0f : -1.0f, dZ = dk ? 1.0f : -1.0f;
+      const float w = X * Y * Z;
+      const float sdot = cp[c].x * lE.x + cp[c].y * lE.y + cp[c].z * lE.z + cp[c].w * lB.x + cq[c].x * lB.y +
+                         cq[c].y * lB.z;
+      lb = add3(lb, mul3(sdot, f3(dX * Y * Z, X * dY * Z, X * Y * dZ)));
+      const float gv[6] = {w * lE.x, w * lE.y, w * lE.z, w * lB.x, w * lB.y, w * lB.z};
+      if (inb) {
+        const int e = ((lk + dk) * B + (lj + dj)) * B + (li + di);
+#pragma unroll
+        for (int q = 0; q < 6; q++) atomicAdd(&sgr[6 * e + q], gv[q]);
+      } else {
+        const int64_t un = unique_node(G, cb[0] + di, cb[1] + dj, cb[2] + dk);
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          atomicAdd(&a.gE[3 * un + q], gv[q]);
+          atomicAdd(&a.gB[3 * un + q], gv[3 + q]);
+        }
+      }
+    }
+    a.lx[m] = lb.x;
+    a.ly[m] = lb.y;
+    a.lz[m] = lb.z;
+    a.lvx[m] = lu.x;
+    a.lvy[m] = lu.y;
+    a.lvz[m] = lu.z;
+  }
+  __syncthreads();
+  for (int e = tid; e < NF; e += PUSH_THREADS) {
+    const int li = e % B, lj = (e / B) % B, lk = e / (B * B);
+    const int gi = o[0] + li, gj = o[1] + lj, gk = o[2] + lk;
+    if (gi < 0 || gj < 0 || gk < 0 || gi > G.nx || gj > G.ny || gk > G.nz) continue;
+    const int64_t un = unique_node(G, gi, gj, gk);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const float vE = sgr[6 * e + q], vB = sgr[6 * e + 3 + q];
+      if (vE != 0.f) atomicAdd(&a.gE[3 * un + q], vE);
+      if (vB != 0.f) atomicAdd(&a.gB[3 * un + q], vB);
+    }
+  }
+}
+
+inline int fx_adjoint_smem(int tmax) {
+  const int B = fx_box_tile(tmax) + 2 * PG + 1;
+  const int nf = B * B * B;
+  return nf * (int)(2 * sizeof(float4) + 9 * sizeof(float));
+}
+
+// lambda through a sort: the adjoint of S_{n+1} (new layout) back to the
+// layout before the sort (inv[new slot] = old slot).
+__global__ void k_adj_unsort(const uint32_t* __restrict__ inv, int64_t n, const float* __restrict__ src0,
+                             const float* __restrict__ src1, const float* __restrict__ src2,
+                             const float* __restrict__ src3, const float* __restrict__ src4,
+                             const float* __restrict__ src5, float* d0, float* d1, float* d2, float* d3, float* d4,
+                             float* d5) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const uint32_t s = inv[m];
+  if (s == DEAD) return;
+  d0[s] = src0[m]; d1[s] = src1[m]; d2[s] = src2[m];
+  d3[s] = src3[m]; d4[s] = src4[m]; d5[s] = src5[m];
+}
+
+__device__ __forceinline__ bool in_probe(const Geo& G, int64_t un, int3 lo, int3 hi, int& i, int& j, int& k) {
+  i = (int)(un % G.nx);
+  j = (int)((un / G.nx) % G.ny);
+  k = (int)(un / ((int64_t)G.nx * G.ny));
+  return i >= lo.x && i < hi.x && j >= lo.y && j < hi.y && k >= lo.z && k < hi.z;
+}
+
+// The loss of one step, sum over the probe nodes of aj_x^2 (aj: the folded
+// FP64 current), and, when jx_keep is given, the probe Jx of the step.
+__global__ void k_adj_probe(const double* __restrict__ aj, FieldDesc fj, Geo G, int3 lo, int3 hi, double* loss,
+                            float* jx_keep) {
+  const int64_t un = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (un >= (int64_t)G.nx * G.ny * G.nz) return;
+  int i, j, k;
+  if (!in_probe(G, un, lo, hi, i, j, k)) {
+    if (jx_keep) jx_keep[un] = 0.f;
+    return;
+  }
+  const double jx = aj[fj.at(0, i, j, k)];
+  if (loss) atomicAdd(loss, jx * jx);
+  if (jx_keep) jx_keep[un] = (float)jx;
+}
+
+// g = dL/dJ of one step: 2 Jx on the probe nodes, 0 elsewhere.
+__global__ void k_adj_g(const float* __restrict__ jx, int64_t nn, float* g) {
+  const int64_t un = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (un >= nn) return;
+  g[3 * un] = 2.0f * jx[un];
+  g[3 * un + 1] = 0.f;
+  g[3 * un + 2] = 0.f;
+}
+
+// lambda_v of the start state (thread-major regions) in canonical order
+// (tile-major sorted ranks): out[(rank0 + q) * 3 + c].
+__global__ void k_adj_canonical(const float* __restrict__ lvx, const float* __restrict__ lvy,
+                                const float* __restrict__ lvz, const int64_t* __restrict__ ts,
+                                const int64_t* __restrict__ tp, int64_t rank0, double* out) {
+  const int t = blockIdx.x, tid = threadIdx.x;
+  const int64_t n = ts[t + 1] - ts[t];
+  if (n <= 0) return;
+  const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
+  for (int r = 0; r < L; r++) {
+    const int64_t q = (int64_t)tid * L + r;
+    if (q >= n) continue;
+    const int64_t m = tp[t] + (int64_t)r * PUSH_THREADS + tid;
+    double* o = out + 3 * (rank0 + ts[t] + q);
+    o[0] = lvx[m];
+    o[1] = lvy[m];
+    o[2] = lvz[m];
+  }
+}

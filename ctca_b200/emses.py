@@ -131,6 +131,7 @@ _SIGS = {
     "emsesg_fx_download_accum": (_I, [_P, _P]),
     "emsesg_fx_inject": (_I, [_P, _I, _P, ctypes.c_int64]),
     "emsesg_fx_surface": (_I, [_P, _P, ctypes.POINTER(ctypes.c_int64)]),
+    "emsesg_fx_adjoint": (_I, [_P, _I, _I, _I, _I, _P, _P, ctypes.POINTER(ctypes.c_double), _P, _P, _P, _P]),
     "emsesg_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
     "emsesg_set_profiling": (_I, [_P, _I]),
     "emsesg_profile_report": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t]),
@@ -371,6 +372,22 @@ class Emses:
         if n.value:
             self._check(self.lib.emsesg_fx_surface(self.h, out.ctypes.data, ctypes.byref(n)))
         return out
+
+    def fx_adjoint(self, K: int, ustep: int, ckpt: int, sort_every: int, probe_lo, probe_hi, nparticles: int):
+        """Loss sum_steps sum_probe aj_x^2 over K steps and its gradients:
+        returns (loss, gE, gB, g0, gv) with node gradients [n^3, 3] and gv
+        [nparticles, 3] in emsesg_fx_store order."""
+        nn = self.cfg.nx * self.cfg.ny * self.cfg.nz
+        gE = np.zeros((nn, 3))
+        gB = np.zeros((nn, 3))
+        g0 = np.zeros(6)
+        gv = np.zeros((nparticles, 3))
+        loss = ctypes.c_double(0.0)
+        lo = (ctypes.c_int32 * 3)(*probe_lo)
+        hi = (ctypes.c_int32 * 3)(*probe_hi)
+        self._check(self.lib.emsesg_fx_adjoint(self.h, K, ustep, ckpt, sort_every, lo, hi, ctypes.byref(loss),
+                                               gE.ctypes.data, gB.ctypes.data, g0.ctypes.data, gv.ctypes.data))
+        return loss.value, gE, gB, g0, gv
 
     def load_plasma(self, pl: Plasma):
         self._check(self.lib.emsesg_load_plasma(self.h, ctypes.byref(pl)))

@@ -267,6 +267,18 @@ int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int
  * crossed last, in the cell holding its end point.  counts may be NULL to
  * query nsurf. */
 int emsesg_fx_surface(emsesg_ctx* ctx, int64_t* counts, int64_t* nsurf);
+/* Reverse mode through K steps of the FP32 form on a periodic grid (no
+ * bodies, no injection): runs the K forward steps (re-sort every sort_every
+ * steps), then the adjoint sweep with the particle state checkpointed every
+ * ckpt steps (K a multiple of ckpt, ckpt <= 64) and recomputed in between.
+ * Loss: L = sum over the K steps and the probe nodes lo <= (i,j,k) < hi of
+ * aj_x(i,j,k)^2 (the folded current).  Gradients, each optional: gE, gB of
+ * the FP32 node fields E, B used by the push, [nx*ny*nz][3] with x fastest;
+ * g0[6] of the uniform e0, b0 (the node sums); gv[N][3] of the initial
+ * velocities, in the order emsesg_fx_store writes the particles (species by
+ * species, tile-major sorted ranks).  The state ends as after the forward. */
+int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, int sort_every, const int32_t* probe_lo,
+                      const int32_t* probe_hi, double* loss, double* gE, double* gB, double* g0, double* gv);
 
 /* ---- synthetic plasma loader (seeded, on the device) -------------------- */
 typedef struct emsesg_plasma {
