@@ -97,6 +97,13 @@ struct FxState {
   emsesg_particle* stage = nullptr;    // device staging of injected records
   int32_t* stage_ord = nullptr;
   int64_t stage_cap = 0;
+  // CUDA graph of a block of steps (emsesg_fx_run)
+  bool capture = false;                // inside a stream capture: no host syncs
+  cudaGraphExec_t gexec = nullptr;
+  int g_ustep = 0, g_sort = 0;
+  const float4* g_pos = nullptr;       // buffers and configuration it was captured with
+  const int64_t* g_ts = nullptr;
+  emsesg_config g_cfg{};
   int64_t* accum = nullptr;         // int64 (rho, jx, jy, jz) on the rho layout
   float4* fnode = nullptr;          // node field {ex, ey, ez, bx} over (n+1)^3 nodes
   float4* fnode2 = nullptr;         // {by, bz, 0, 0}

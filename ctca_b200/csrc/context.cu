@@ -214,8 +214,8 @@ extern "C" int emsesg_synchronize(emsesg_ctx* ctx) {
     if (st & ST_RANDOMS) return set_error(ctx, EMSESG_ERR_ARG, "pre-drawn random numbers exhausted");
     if (st & ST_OVERFLOW) return set_error(ctx, EMSESG_ERR_OVERFLOW, "particle capacity exceeded");
     static const char* sites[] = {"?", "psolve2", "psolve1", "charge", "fx_load", "fx_push", "fx_deposit",
-                                  "fx_flush"};
-    int site = (diag[0] >= 0 && diag[0] <= 7) ? (int)diag[0] : 0;
+                                  "fx_flush", "fx_sort"};
+    int site = (diag[0] >= 0 && diag[0] <= 8) ? (int)diag[0] : 0;
     return set_error(ctx, EMSESG_ERR_DEVICE,
                      "a kernel met a particle outside the field arrays (status %d, site %s, index %lld, cell %lld)",
                      st, sites[site], diag[1], diag[2]);

@@ -464,7 +464,9 @@ int fx_alloc(emsesg_ctx* ctx) {
     EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_tiletot, f.ntiles * sizeof(int64_t)));
     EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_stray, EMSESG_ISPEC * sizeof(int)));
     EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_inv, cap * sizeof(uint32_t)));
-    const int lsm = (int)(PUSH_WARPS * nbc * sizeof(uint32_t));
+    // kernel attributes hold for every context of the process: allow the
+    // largest box (8-cell tiles), whatever this context's tile
+    const int lsm = (int)(PUSH_WARPS * 10 * 10 * 10 * sizeof(uint32_t));
     EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_count, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
     EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
     EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_move, cudaFuncAttributeMaxDynamicSharedMemorySize, move_smem()));
@@ -483,6 +485,7 @@ void fx_free(emsesg_ctx* ctx) {
   cudaFree(f.tile_start2); cudaFree(f.tile_pad2); cudaFree(f.lcs_cnt); cudaFree(f.lcs_base); cudaFree(f.lcs_wcnt);
   cudaFree(f.lcs_celltot); cudaFree(f.lcs_tiletot); cudaFree(f.lcs_stray); cudaFree(f.lcs_inv);
   cudaFree(f.surf); cudaFree(f.tailord); cudaFree(f.stage); cudaFree(f.stage_ord);
+  if (f.gexec) cudaGraphExecDestroy(f.gexec);
   f = FxState();
 }
 
@@ -531,11 +534,18 @@ int fx_local_sort(emsesg_ctx* ctx, bool* done) {
                   f.tile_start + is * T1, f.tile_pad + is * T1, g, G[is],
                   f.lcs_wcnt + is * f.ntiles * PUSH_WARPS * nbc, f.lcs_cnt + is * f.ntiles * nbc, f.lcs_stray + is);
   }
-  int stray[EMSESG_ISPEC] = {0};
-  EMSESG_CUDA(ctx, cudaMemcpyAsync(stray, f.lcs_stray, EMSESG_ISPEC * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  for (int is = 0; is < c.nspec; is++)
-    if (stray[is]) return EMSESG_OK;
+  // Outside a stream capture the host reads the stray flags and falls back
+  // to the radix sort.  Inside one (emsesg_fx_run's graph) it cannot: the
+  // sort kernels of a species with a stray then return at once and
+  // k_lcs_keep carries its current order over to the new buffers.
+  if (!f.capture) {
+    int stray[EMSESG_ISPEC] = {0};
+    EMSESG_CUDA(ctx, cudaMemcpyAsync(stray, f.lcs_stray, EMSESG_ISPEC * sizeof(int), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int is = 0; is < c.nspec; is++)
+      if (stray[is]) return EMSESG_OK;
+  }
   for (int is = 0; is < c.nspec; is++) {
     int64_t* ts2 = f.tile_start2 + is * T1;
     int64_t* tp2 = f.tile_pad2 + is * T1;
@@ -549,18 +559,23 @@ int fx_local_sort(emsesg_ctx* ctx, bool* done) {
     const int64_t off = f.base[is];
     uint32_t* cnt = f.lcs_cnt + is * f.ntiles * nbc;
     uint32_t* bas = f.lcs_base + is * f.ntiles * nbc;
+    const int* stray = f.lcs_stray + is;
     EMSESG_LAUNCH(ctx, "lcs_celltot", k_lcs_celltot, (unsigned)f.ntiles, CELL_THREADS, 0, cnt, g, G[is],
-                  f.lcs_celltot, f.lcs_tiletot);
+                  f.lcs_celltot, f.lcs_tiletot, stray);
     EMSESG_LAUNCH(ctx, "lcs_tiles", k_lcs_tiles, 1, 1024, 0, f.lcs_tiletot, f.ntiles, ts2, tp2, f.count_d + is,
-                  f.slots_d + is);
+                  f.slots_d + is, stray);
     EMSESG_LAUNCH(ctx, "lcs_bases", k_lcs_bases, (unsigned)f.ntiles, CELL_THREADS, 0, cnt, f.lcs_celltot, g, G[is],
-                  ts2, tp2, bas, f.lcs_inv + off);
+                  ts2, tp2, bas, f.lcs_inv + off, stray);
     EMSESG_LAUNCH(ctx, "lcs_rank", k_lcs_rank, (unsigned)f.ntiles, PUSH_THREADS, lsm, f.pos + off,
                   f.tile_start + is * T1, f.tile_pad + is * T1, g, G[is], f.lcs_wcnt + is * f.ntiles * PUSH_WARPS * nbc,
-                  bas, ts2, tp2, f.lcs_inv + off, ctx->d_status, ctx->d_diag);
+                  bas, ts2, tp2, f.lcs_inv + off, ctx->d_status, ctx->d_diag, stray);
     EMSESG_LAUNCH(ctx, "lcs_move", k_lcs_move, (unsigned)f.ntiles, PUSH_THREADS, move_smem(), f.pos + off,
                   f.vx + off, f.vy + off, f.vz + off, f.tile_start + is * T1, f.tile_pad + is * T1, ts2, tp2,
-                  f.lcs_inv + off, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off);
+                  f.lcs_inv + off, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off, stray);
+    if (f.capture)
+      EMSESG_LAUNCH(ctx, "lcs_keep", k_lcs_keep, 4 * 148, 256, 0, stray, f.pos + off, f.vx + off, f.vy + off,
+                    f.vz + off, f.tile_start + is * T1, f.tile_pad + is * T1, f.ntiles, f.pos2 + off, f.vx2 + off,
+                    f.vy2 + off, f.vz2 + off, ts2, tp2, f.lcs_inv + off);
   }
   std::swap(f.pos, f.pos2);
   std::swap(f.vx, f.vx2);
@@ -1058,3 +1073,201 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
 #undef EMSESG_ADJ
   return emsesg_synchronize(ctx);
 }
+
+namespace {
+
+// Captures `block` steps of ctx (do_sort on every sort_every-th) into a new
+// graph.  Capturing runs no kernel; the host state that the steps touch
+// (buffer swaps of the sorts, the step counter of the random hash) is
+// checked, or put back, so that it matches the state after a replay.
+int capture_steps(emsesg_ctx* ctx, int ustep, int block, int sort_every, cudaGraph_t* out) {
+  FxState& f = ctx->fx;
+  *out = nullptr;
+  const bool timing = ctx->timer.on;
+  float4* pos0 = f.pos;
+  const int64_t* ts0 = f.tile_start;
+  const uint64_t rs0 = ctx->rng_stream;
+  ctx->timer.on = false;
+  EMSESG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  f.capture = true;
+  int rc = EMSESG_OK;
+  for (int s = 0; s < block && !rc; s++) rc = emsesg_fx_step(ctx, ustep, (s + 1) % sort_every == 0);
+  f.capture = false;
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+  ctx->timer.on = timing;
+  ctx->rng_stream = rs0;
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return check_cuda(ctx, e, "cudaStreamEndCapture");
+  if (f.pos != pos0 || f.tile_start != ts0) {
+    cudaGraphDestroy(graph);
+    return set_error(ctx, EMSESG_ERR_STATE, "captured block does not return to its buffers");
+  }
+  *out = graph;
+  return EMSESG_OK;
+}
+
+bool graph_ready(const emsesg_ctx* ctx) {
+  const FxState& f = ctx->fx;
+  bool tail = false;
+  for (int is = 0; is < ctx->cfg.nspec; is++) tail = tail || f.ntail[is] > 0 || f.pending[is] > 0;
+  return f.tiled && !tail;
+}
+
+}  // namespace
+
+// nsteps steps of the FP32 form with a re-sort every sort_every steps.  With
+// use_graph the block of 2*sort_every steps (two sorts, so that the buffer
+// swaps of the sorts cancel) is captured once into a CUDA graph and replayed;
+// steps that do not fill a block run one by one.  Asynchronous.
+extern "C" int emsesg_fx_run(emsesg_ctx* ctx, int ustep, int nsteps, int sort_every, int use_graph) {
+  if (!ctx || nsteps < 0 || sort_every < 1) return EMSESG_ERR_ARG;
+  FxState& f = ctx->fx;
+  if (!f.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
+  int rc;
+  const int block = 2 * sort_every;
+  if (!use_graph || !graph_ready(ctx) || nsteps < block) {
+    for (int s = 0; s < nsteps; s++)
+      if ((rc = emsesg_fx_step(ctx, ustep, (s + 1) % sort_every == 0))) return rc;
+    return EMSESG_OK;
+  }
+  if (f.gexec && (f.g_ustep != ustep || f.g_sort != sort_every || f.g_pos != f.pos || f.g_ts != f.tile_start ||
+                  memcmp(&f.g_cfg, &ctx->cfg, sizeof(emsesg_config)) != 0)) {
+    cudaGraphExecDestroy(f.gexec);
+    f.gexec = nullptr;
+  }
+  if (!f.gexec) {
+    cudaGraph_t graph;
+    if ((rc = capture_steps(ctx, ustep, block, sort_every, &graph))) return rc;
+    cudaError_t e = cudaGraphInstantiate(&f.gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      f.gexec = nullptr;
+      return check_cuda(ctx, e, "cudaGraphInstantiate");
+    }
+    f.g_ustep = ustep;
+    f.g_sort = sort_every;
+    f.g_pos = f.pos;
+    f.g_ts = f.tile_start;
+    f.g_cfg = ctx->cfg;
+  }
+  const int nblock = nsteps / block;
+  for (int b = 0; b < nblock; b++) EMSESG_CUDA(ctx, cudaGraphLaunch(f.gexec, ctx->stream));
+  ctx->rng_stream += (uint64_t)nblock * block;
+  for (int s = 0; s < nsteps - nblock * block; s++)
+    if ((rc = emsesg_fx_step(ctx, ustep, (s + 1) % sort_every == 0))) return rc;
+  return EMSESG_OK;
+}
+
+// ---- ensembles: one graph holding a block of steps of many runs ----------
+// Each run (context) is captured on its own stream into a child graph; the
+// children sit side by side in one parent graph with no edges between them,
+// so one cudaGraphLaunch starts every run and the GPU runs their kernels
+// concurrently, small runs filling the SMs that one run leaves idle.
+struct emsesg_batch {
+  std::vector<emsesg_ctx*> ctxs;
+  std::vector<cudaEvent_t> ev;      // one per context: its stream's last work
+  std::vector<float4*> pos;         // buffers each run was captured with
+  std::vector<const int64_t*> ts;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int block = 0;
+};
+
+extern "C" int emsesg_batch_destroy(emsesg_batch* b) {
+  if (!b) return EMSESG_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
+  if (b->done) cudaEventDestroy(b->done);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_batch_create(emsesg_ctx* const* ctxs, int n, int ustep, int block, const int* sort_every,
+                                   emsesg_batch** out) {
+  if (!ctxs || n < 1 || !sort_every || !out || block < 2) return EMSESG_ERR_ARG;
+  *out = nullptr;
+  emsesg_ctx* c0 = ctxs[0];
+  if (!c0) return EMSESG_ERR_ARG;
+  for (int r = 0; r < n; r++) {
+    emsesg_ctx* c = ctxs[r];
+    if (!c) return EMSESG_ERR_ARG;
+    for (int q = 0; q < r; q++)
+      if (ctxs[q] == c) return set_error(c, EMSESG_ERR_ARG, "a context appears twice in the batch");
+    if (c->device != c0->device) return set_error(c, EMSESG_ERR_ARG, "batch contexts must share one device");
+    if (sort_every[r] < 1 || block % (2 * sort_every[r]) != 0)
+      return set_error(c, EMSESG_ERR_ARG, "block %d is not a multiple of 2*sort_every (%d)", block, sort_every[r]);
+    if (!c->fx.loaded) return set_error(c, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
+    if (!graph_ready(c)) return set_error(c, EMSESG_ERR_STATE, "run is not tile-sorted or has injected particles");
+  }
+  emsesg_batch* b = new emsesg_batch();
+  b->ctxs.assign(ctxs, ctxs + n);
+  b->block = block;
+  int rc = EMSESG_OK;
+  cudaGraph_t parent = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaGraphCreate(&parent, 0);
+  for (int r = 0; r < n && e == cudaSuccess; r++) {
+    cudaEvent_t ev;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) b->ev.push_back(ev);
+  }
+  if (e != cudaSuccess) rc = check_cuda(c0, e, "batch resources");
+  for (int r = 0; r < n && !rc; r++) {
+    cudaGraph_t child = nullptr;
+    if ((rc = capture_steps(ctxs[r], ustep, block, sort_every[r], &child))) break;
+    cudaGraphNode_t node;
+    e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
+    cudaGraphDestroy(child);
+    if (e != cudaSuccess) rc = check_cuda(ctxs[r], e, "cudaGraphAddChildGraphNode");
+    b->pos.push_back(ctxs[r]->fx.pos);
+    b->ts.push_back(ctxs[r]->fx.tile_start);
+  }
+  if (!rc) {
+    e = cudaGraphInstantiate(&b->exec, parent, 0);
+    if (e != cudaSuccess) {
+      b->exec = nullptr;
+      rc = check_cuda(c0, e, "cudaGraphInstantiate");
+    }
+  }
+  if (parent) cudaGraphDestroy(parent);
+  if (rc) {
+    emsesg_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_batch_launch(emsesg_batch* b, int nrep) {
+  if (!b || nrep < 0) return EMSESG_ERR_ARG;
+  emsesg_ctx* c0 = b->ctxs[0];
+  const int n = (int)b->ctxs.size();
+  for (int r = 0; r < n; r++) {
+    emsesg_ctx* c = b->ctxs[r];
+    if (c->fx.pos != b->pos[r] || c->fx.tile_start != b->ts[r] || graph_ready(c) == false)
+      return set_error(c, EMSESG_ERR_STATE, "run changed since the batch was captured");
+  }
+  // the graph starts after each run's earlier work ...
+  for (int r = 0; r < n; r++) {
+    EMSESG_CUDA(c0, cudaEventRecord(b->ev[r], b->ctxs[r]->stream));
+    EMSESG_CUDA(c0, cudaStreamWaitEvent(b->stream, b->ev[r], 0));
+  }
+  for (int k = 0; k < nrep; k++) EMSESG_CUDA(c0, cudaGraphLaunch(b->exec, b->stream));
+  // ... and each run's later work starts after the graph
+  EMSESG_CUDA(c0, cudaEventRecord(b->done, b->stream));
+  for (int r = 0; r < n; r++) {
+    EMSESG_CUDA(c0, cudaStreamWaitEvent(b->ctxs[r]->stream, b->done, 0));
+    b->ctxs[r]->rng_stream += (uint64_t)nrep * b->block;
+  }
+  return EMSESG_OK;
+}
+
+extern "C" void* emsesg_batch_stream(emsesg_batch* b) { return b ? (void*)b->stream : nullptr; }

@@ -140,8 +140,9 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_count(const float4* __rest
 // per destination tile its total.  grid = ntiles, block = CELL_THREADS (>= tcells).
 __global__ void __launch_bounds__(CELL_THREADS) k_lcs_celltot(const uint32_t* __restrict__ cnt, Geo g, LcsGeo G,
                                                               uint32_t* __restrict__ celltot,
-                                                              int64_t* __restrict__ tiletot) {
+                                                              int64_t* __restrict__ tiletot, const int* stray) {
   __shared__ uint32_t part[CELL_THREADS / 32];
+  if (*stray) return;  // a particle left its sort box: this sort is skipped (see fx_local_sort)
   const int t = blockIdx.x, tid = threadIdx.x;
   int tx, ty, tz;
   tile_xyz(g, t, tx, ty, tz);
@@ -179,8 +180,10 @@ __global__ void __launch_bounds__(CELL_THREADS) k_lcs_celltot(const uint32_t* __
 // tiles: exclusive scan of the tile totals (one block of 1024 threads):
 // tile_start, tile_pad (whole rows per tile), live count and slot count.
 __global__ void __launch_bounds__(1024) k_lcs_tiles(const int64_t* __restrict__ tiletot, int64_t ntiles,
-                                                    int64_t* ts, int64_t* tp, int64_t* count, int64_t* slots) {
+                                                    int64_t* ts, int64_t* tp, int64_t* count, int64_t* slots,
+                                                    const int* stray) {
   __shared__ int64_t pa[1024], pb[1024];
+  if (*stray) return;
   const int tid = threadIdx.x;
   const int64_t per = (ntiles + 1023) / 1024;
   const int64_t t0 = tid * per, t1 = min(ntiles, t0 + per);
@@ -220,8 +223,9 @@ __global__ void __launch_bounds__(CELL_THREADS) k_lcs_bases(const uint32_t* __re
                                                             const uint32_t* __restrict__ celltot, Geo g, LcsGeo G,
                                                             const int64_t* __restrict__ ts,
                                                             const int64_t* __restrict__ tp, uint32_t* __restrict__ base,
-                                                            uint32_t* __restrict__ inv) {
+                                                            uint32_t* __restrict__ inv, const int* stray) {
   __shared__ uint32_t sc[CELL_THREADS];
+  if (*stray) return;
   const int t = blockIdx.x, tid = threadIdx.x;
   int tx, ty, tz;
   tile_xyz(g, t, tx, ty, tz);
@@ -275,8 +279,9 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restr
                                                            const uint32_t* __restrict__ base,
                                                            const int64_t* __restrict__ ts2,
                                                            const int64_t* __restrict__ tp2, uint32_t* __restrict__ inv,
-                                                           int* status, long long* diag) {
+                                                           int* status, long long* diag, const int* stray) {
   extern __shared__ uint32_t wb[];  // [PUSH_WARPS][nbc] next rank of (warp, box cell)
+  if (*stray) return;
   const int t = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned lt = (1u << lane) - 1u;
   const uint16_t* wc = wcnt + (int64_t)t * PUSH_WARPS * G.nbc;
@@ -341,9 +346,10 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_move(const float4* __restr
                                                            const int64_t* __restrict__ tp2,
                                                            const uint32_t* __restrict__ inv, float4* __restrict__ pos2,
                                                            float* __restrict__ vx2, float* __restrict__ vy2,
-                                                           float* __restrict__ vz2) {
+                                                           float* __restrict__ vz2, const int* stray) {
   extern __shared__ float4 wpos[];  // [rows][MOVE_WCOLS], then wvx, wvy, wvz
   __shared__ int wlo;
+  if (*stray) return;
   const int t = blockIdx.x, tid = threadIdx.x;
   const int64_t nd = ts2[t + 1] - ts2[t];
   if (nd <= 0) return;
@@ -408,5 +414,35 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_move(const float4* __restr
       vz2[m] = c;
     }
     if (win) __syncthreads();  // the window is reloaded for the next group
+  }
+}
+
+// Inside a CUDA graph the host cannot switch to the radix sort when a
+// particle has left its tile's sort box; the sort kernels above then return
+// at once and this one keeps the current order instead: the new buffers get
+// the old regions slot for slot (inv = identity).  The push handles a
+// particle outside its tile's box on its general path (global gather and
+// deposits), so the step stays correct, only slower, until the next sort
+// outside a graph.  Does nothing when no particle strayed.
+__global__ void __launch_bounds__(256) k_lcs_keep(const int* stray, const float4* __restrict__ pos,
+                                                  const float* __restrict__ vx, const float* __restrict__ vy,
+                                                  const float* __restrict__ vz, const int64_t* __restrict__ ts,
+                                                  const int64_t* __restrict__ tp, int64_t ntiles, float4* pos2,
+                                                  float* vx2, float* vy2, float* vz2, int64_t* ts2, int64_t* tp2,
+                                                  uint32_t* inv) {
+  if (!*stray) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t t = i0; t <= ntiles; t += stride) {
+    ts2[t] = ts[t];
+    tp2[t] = tp[t];
+  }
+  const int64_t n = tp[ntiles];
+  for (int64_t i = i0; i < n; i += stride) {
+    pos2[i] = pos[i];
+    vx2[i] = vx[i];
+    vy2[i] = vy[i];
+    vz2[i] = vz[i];
+    inv[i] = __float_as_uint(pos[i].w) == DEAD ? DEAD : (uint32_t)i;
   }
 }

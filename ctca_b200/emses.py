@@ -127,6 +127,11 @@ _SIGS = {
     "emsesg_fx_store": (_I, [_P]),
     "emsesg_fx_step": (_I, [_P, _I, _I]),
     "emsesg_fx_sort": (_I, [_P]),
+    "emsesg_fx_run": (_I, [_P, _I, _I, _I, _I]),
+    "emsesg_batch_create": (_I, [_P, _I, _I, _I, _P, ctypes.POINTER(_P)]),
+    "emsesg_batch_launch": (_I, [_P, _I]),
+    "emsesg_batch_stream": (_P, [_P]),
+    "emsesg_batch_destroy": (_I, [_P]),
     "emsesg_fx_counts": (_I, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "emsesg_fx_download_accum": (_I, [_P, _P]),
     "emsesg_fx_inject": (_I, [_P, _I, _P, ctypes.c_int64]),
@@ -343,6 +348,10 @@ class Emses:
     def fx_step(self, ustep: int = 2, do_sort: bool = False):
         self._check(self.lib.emsesg_fx_step(self.h, ustep, 1 if do_sort else 0))
 
+    def fx_run(self, ustep: int, nsteps: int, sort_every: int, use_graph: bool = True):
+        """nsteps steps, re-sort every sort_every, replayed from a CUDA graph."""
+        self._check(self.lib.emsesg_fx_run(self.h, ustep, nsteps, sort_every, 1 if use_graph else 0))
+
     def fx_sort(self):
         self._check(self.lib.emsesg_fx_sort(self.h))
 
@@ -406,3 +415,56 @@ class Emses:
 
     def profile_reset(self):
         self._check(self.lib.emsesg_profile_reset(self.h))
+
+
+class Batch:
+    """One CUDA graph holding `block` steps of each of several runs
+    (emsesg_batch_create); `launch(nrep)` replays it nrep times."""
+
+    def __init__(self, runs: list, ustep: int, block: int, sort_every: list):
+        self.lib = load_library()
+        self.runs = list(runs)
+        n = len(self.runs)
+        hs = (ctypes.c_void_p * n)(*[r.h.value for r in self.runs])
+        se = (ctypes.c_int * n)(*[int(x) for x in sort_every])
+        h = ctypes.c_void_p()
+        rc = self.lib.emsesg_batch_create(ctypes.cast(hs, ctypes.c_void_p), n, ustep, block,
+                                          ctypes.cast(se, ctypes.c_void_p), ctypes.byref(h))
+        if rc != OK:
+            self._raise(rc)
+        self.h = h
+        self.block = block
+
+    def _raise(self, rc: int):
+        for r in self.runs:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.emsesg_last_error(r.h, buf, 512)
+            if buf.value:
+                raise EmsesError(rc, buf.value.decode(errors="replace"))
+        raise EmsesError(rc, "emsesg_batch call failed")
+
+    @property
+    def stream(self) -> int:
+        return self.lib.emsesg_batch_stream(self.h) or 0
+
+    def launch(self, nrep: int):
+        rc = self.lib.emsesg_batch_launch(self.h, int(nrep))
+        if rc != OK:
+            self._raise(rc)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.emsesg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

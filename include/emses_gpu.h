@@ -244,6 +244,37 @@ int emsesg_fx_store(emsesg_ctx* ctx);
  * with do_sort, the re-sort after the push. */
 int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort);
 int emsesg_fx_sort(emsesg_ctx* ctx);
+/* nsteps steps of the FP32 form, re-sorting every sort_every steps
+ * (emsesg_fx_step with do_sort on every sort_every-th step).  With use_graph,
+ * a block of 2*sort_every steps is captured once into a CUDA graph (cached
+ * per ustep and sort_every) and replayed; the remaining steps run one by one.
+ * Inside the graph a tile sort that meets a particle outside its tile's sort
+ * box cannot switch to the global sort: it keeps the current order for that
+ * species (the push handles such particles on its general path), so rho/J
+ * stay the same physics, though their FP32 partial sums may round in a
+ * different order than emsesg_fx_step's.  Injected particles waiting in the
+ * tail zone, or an unsorted layout, make it run step by step.  Asynchronous
+ * on the context's stream. */
+int emsesg_fx_run(emsesg_ctx* ctx, int ustep, int nsteps, int sort_every, int use_graph);
+
+/* Ensembles (no counterpart in the reference, which runs one job per run):
+ * one CUDA graph holding `block` steps of each of n independent runs
+ * (contexts on one device, FP32 form loaded, no injected particles
+ * waiting), run r re-sorting every sort_every[r] steps; block must be a
+ * multiple of 2*sort_every[r] for every r.  The runs are independent
+ * branches of the graph, so the GPU runs their kernels side by side. */
+typedef struct emsesg_batch emsesg_batch;
+int emsesg_batch_create(emsesg_ctx* const* ctxs, int n, int ustep, int block, const int* sort_every,
+                        emsesg_batch** out);
+/* Replays the graph nrep times (nrep*block steps of every run) on the
+ * batch's own stream, after the earlier work of every run's stream and
+ * before its later work.  Errors are reported through the run contexts
+ * (emsesg_last_error of the first one for launch errors). */
+int emsesg_batch_launch(emsesg_batch* b, int nrep);
+/* The batch's cudaStream_t, as an opaque pointer (for timing events). */
+void* emsesg_batch_stream(emsesg_batch* b);
+/* Waits for the batch's work and releases it (the runs stay). */
+int emsesg_batch_destroy(emsesg_batch* b);
 /* Particle counts of the FP32 form (nspec entries). */
 int emsesg_fx_counts(emsesg_ctx* ctx, int64_t* totalp);
 /* Raw fixed-point accumulators after the guard folding, int64 at 2^40:
