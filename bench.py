@@ -21,6 +21,15 @@ no data exchange on one rank: weak scaling, replicas only).
 --cells N [--ppc P] shrinks the grid (and particles per cell) for profiler
 captures; the headline line is the default 128^3 x 64 workload.
 
+Two more workloads ride on the headline line (skip them with --no-extras):
+`adjoint` times the reverse mode through K = 256 steps of a 64^3 periodic
+grid with 32 particles per cell per species (checkpoints every 16 steps,
+loss = sum of Jx^2 over an 8^3 probe) against the same K forward steps;
+`ensemble` runs a bounded sample of the ensemble workload (independent runs
+of side 16..64 in one CUDA graph) against the same runs launched one after
+the other.  --workload ensemble prints the full ensemble line instead
+(512 runs x 200 steps by default).
+
 --impl reference times the reference's CPU path (the oracle restatement of
 psolve1 + charge; the Fortran reference cannot be built here) on the host
 cores, on a bounded sample of the same workload.
@@ -185,6 +194,64 @@ def run_reference(args, world, rank):
 
 
 # --------------------------------------------------------------- GPU arm
+def time_adjoint(K: int = 256, ckpt: int = 16, sort_every: int = SORT_EVERY) -> dict:
+    """Forward K steps vs the reverse mode through them (emsesg_fx_adjoint)
+    on the 64^3 x 32 ppc adjoint workload."""
+    import torch
+    from ctca_b200 import inputs
+    from ctca_b200.emses import Emses
+    case = inputs.baseline_case(4)
+    cfg = inputs.make_config(case)
+    eb = inputs.make_fields(case)
+    lo = tuple(case.n[d] // 2 - 4 for d in range(3))
+    hi = tuple(x + 8 for x in lo)
+    with Emses(cfg) as g:
+        g.upload_field("eb", eb)
+        g.load_plasma(inputs.plasma(case))
+        g.fx_load()
+        npart = int(g.fx_counts().sum())
+        st = torch.cuda.ExternalStream(g.stream)
+        g.fx_run(2, 2 * sort_every, sort_every, use_graph=False)  # warm-up
+        g.synchronize()
+        g.load_plasma(inputs.plasma(case))
+        g.fx_load()
+        g.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(st)
+        g.fx_run(2, K, sort_every, use_graph=False)
+        e1.record(st)
+        e1.synchronize()
+        g.load_plasma(inputs.plasma(case))
+        g.fx_load()
+        g.synchronize()
+        e1b = torch.cuda.Event(enable_timing=True)
+        e1b.record(st)
+        loss, gE, gB, g0, gv = g.fx_adjoint(K, 2, ckpt, sort_every, lo, hi, npart)
+        e2.record(st)
+        e2.synchronize()
+        fwd = e0.elapsed_time(e1) / 1e3
+        adj = e1b.elapsed_time(e2) / 1e3
+    return {"workload": f"{case.n[0]}^3 periodic, 2 species x 32 ppc ({npart:,} particles), K={K}, "
+                        f"checkpoint every {ckpt}, sort every {sort_every}, loss = sum Jx^2 over an 8^3 probe",
+            "forward_s": fwd, "adjoint_call_s": adj,
+            "reverse_over_forward": (adj - fwd) / fwd, "call_over_forward": adj / fwd,
+            "note": "the adjoint call runs the forward (with checkpoints) and then the reverse sweep, "
+                    "which recomputes each checkpoint segment; reverse_over_forward = (call - forward) / forward",
+            "loss": loss}
+
+
+def ensemble_sample(runs: int, steps: int) -> dict:
+    from ctca_b200 import ensemble
+    cases = ensemble.ensemble_cases(runs)
+    tuner = ensemble.Autotuner()
+    out = ensemble.run_ensemble(cases, steps, tuner, modes=("batch", "each"))
+    v = out["particle_steps_per_s"]
+    out["batch_over_each"] = v["batch"] / v["each"]
+    out["workload"] = (f"first {runs} of the 512 seeded ensemble runs (cubic periodic, side 16..64, "
+                       f"ppc U[8,64] per species, mass ratio 100), {steps} steps each")
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
     from ctca_b200 import inputs
@@ -280,7 +347,7 @@ def run_ours(args, world, rank, local):
     hbm, peak_kind = peaks()
     ms, launches = prof.get("fx_push", (0.0, 0))
     avg_launch_s = ms / 1e3 / max(launches, 1)
-    parts_per_launch = npart / cfg.nspec
+    parts_per_launch = npart  # one launch pushes every species (grid.y = species)
     achieved = B_ALG_PUSH * parts_per_launch / avg_launch_s / 1e9 if launches else None
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
@@ -311,6 +378,9 @@ def run_ours(args, world, rank, local):
         "kernels_ms": {k: round(v[0], 3) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
         "clocks": clk.summary(),
     }
+    if world == 1 and not args.no_extras and not args.cells:
+        out["adjoint"] = time_adjoint()
+        out["ensemble"] = ensemble_sample(args.ensemble_runs, args.ensemble_steps)
     if rank == 0 and world == 1 and not args.no_cpu:
         v, sample, _ = cpu_sample(args.cpu_seconds, os.cpu_count() or 1)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
@@ -318,6 +388,50 @@ def run_ours(args, world, rank, local):
     g.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def run_ensemble_line(args, world, rank, local):
+    """The ensemble workload: runs split across ranks (round robin), each
+    rank's runs in one graph per wave; value = all runs' particle-steps over
+    the slowest rank's device time."""
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no ensemble runner: each "
+                              "run is a separate job of the CPU path, timed by --impl reference"}), flush=True)
+        return
+    import torch
+    from ctca_b200 import ensemble
+    from ctca_b200.emses import select_device
+    torch.cuda.set_device(local)
+    select_device(local)
+    cases = ensemble.ensemble_cases(args.ensemble_runs)
+    mine = cases[rank::world]
+    tuner = ensemble.Autotuner()
+    with Clocks(local) as clk:
+        out = ensemble.run_ensemble(mine, args.ensemble_steps, tuner, modes=("batch", "each"))
+    t_batch = max_over_ranks(world, out["seconds"]["batch"])
+    t_each = max_over_ranks(world, out["seconds"]["each"])
+    total = sum(ensemble.particles(c) for c in cases) * args.ensemble_steps
+    line = {
+        "metric": METRIC, "value": total / t_batch, "unit": UNIT, "n_gpus": world, "steps": args.ensemble_steps,
+        "warmup": 4, "ms_per_step": t_batch / args.ensemble_steps * 1e3, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32+i64", "data": "synthetic",
+        "config": {"workload": f"ensemble of {len(cases)} independent periodic runs (side 16..64, ppc U[8,64] per "
+                               f"species, mass ratio 100), {args.ensemble_steps} steps each, one CUDA graph per "
+                               "wave of runs that fit in memory",
+                   "l2": "runs larger than L2 together (GBs of particle state per wave)",
+                   "parallelism": f"runs split over {world} GPU(s)"},
+        "one_launch_per_run": {"value": total / t_each, "unit": UNIT, "seconds": t_each},
+        "batch_over_each": t_each / t_batch,
+        "autotuner": out["choices"], "waves": out["waves"],
+        "e2e": {"value": total / out["e2e_seconds"], "unit": UNIT, "note": "setup + batch + rho/J download, wall",
+                "h2d_bytes_per_step": int(out["h2d_bytes"] / args.ensemble_steps),
+                "d2h_bytes_per_step": int(out["d2h_bytes"] / args.ensemble_steps)},
+        "gpu_launches": max_over_ranks(world, out["batch_kernels"]),
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def main():
@@ -332,12 +446,22 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cells", type=int, default=0, help="grid side of a smaller profiling case (default 128)")
     ap.add_argument("--ppc", type=int, default=0, help="particles per cell per species with --cells")
+    ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and ensemble sections")
+    ap.add_argument("--workload", default="particle_step", choices=["particle_step", "ensemble"])
+    ap.add_argument("--ensemble-runs", type=int, default=None)
+    ap.add_argument("--ensemble-steps", type=int, default=None)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
-        if args.impl == "reference":
+        if args.workload == "ensemble":
+            args.ensemble_runs = args.ensemble_runs or 512
+            args.ensemble_steps = args.ensemble_steps or 200
+            run_ensemble_line(args, world, rank, local)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
+            args.ensemble_runs = args.ensemble_runs or 64
+            args.ensemble_steps = args.ensemble_steps or 40
             run_ours(args, world, rank, local)
     finally:
         if world > 1:

@@ -1176,6 +1176,7 @@ struct emsesg_batch {
   cudaEvent_t done = nullptr;
   cudaGraphExec_t exec = nullptr;
   int block = 0;
+  int64_t kernels = 0;              // kernel nodes in one replay
 };
 
 extern "C" int emsesg_batch_destroy(emsesg_batch* b) {
@@ -1223,8 +1224,19 @@ extern "C" int emsesg_batch_create(emsesg_ctx* const* ctxs, int n, int ustep, in
   for (int r = 0; r < n && !rc; r++) {
     cudaGraph_t child = nullptr;
     if ((rc = capture_steps(ctxs[r], ustep, block, sort_every[r], &child))) break;
+    size_t nn = 0;
+    e = cudaGraphGetNodes(child, nullptr, &nn);
+    if (e == cudaSuccess && nn) {
+      std::vector<cudaGraphNode_t> nodes(nn);
+      e = cudaGraphGetNodes(child, nodes.data(), &nn);
+      for (size_t q = 0; q < nn && e == cudaSuccess; q++) {
+        cudaGraphNodeType t;
+        e = cudaGraphNodeGetType(nodes[q], &t);
+        if (t == cudaGraphNodeTypeKernel) b->kernels++;
+      }
+    }
     cudaGraphNode_t node;
-    e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
+    if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
     cudaGraphDestroy(child);
     if (e != cudaSuccess) rc = check_cuda(ctxs[r], e, "cudaGraphAddChildGraphNode");
     b->pos.push_back(ctxs[r]->fx.pos);
@@ -1271,3 +1283,9 @@ extern "C" int emsesg_batch_launch(emsesg_batch* b, int nrep) {
 }
 
 extern "C" void* emsesg_batch_stream(emsesg_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+extern "C" int emsesg_batch_kernels(const emsesg_batch* b, int64_t* n) {
+  if (!b || !n) return EMSESG_ERR_ARG;
+  *n = b->kernels;
+  return EMSESG_OK;
+}

@@ -131,6 +131,7 @@ _SIGS = {
     "emsesg_batch_create": (_I, [_P, _I, _I, _I, _P, ctypes.POINTER(_P)]),
     "emsesg_batch_launch": (_I, [_P, _I]),
     "emsesg_batch_stream": (_P, [_P]),
+    "emsesg_batch_kernels": (_I, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "emsesg_batch_destroy": (_I, [_P]),
     "emsesg_fx_counts": (_I, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "emsesg_fx_download_accum": (_I, [_P, _P]),
@@ -446,6 +447,15 @@ class Batch:
     @property
     def stream(self) -> int:
         return self.lib.emsesg_batch_stream(self.h) or 0
+
+    @property
+    def kernels(self) -> int:
+        """Kernel launches in one replay of the graph."""
+        n = ctypes.c_int64(0)
+        rc = self.lib.emsesg_batch_kernels(self.h, ctypes.byref(n))
+        if rc != OK:
+            self._raise(rc)
+        return n.value
 
     def launch(self, nrep: int):
         rc = self.lib.emsesg_batch_launch(self.h, int(nrep))

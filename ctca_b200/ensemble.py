@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import json
 import math
+import time
 from dataclasses import dataclass, replace
 from pathlib import Path
 
@@ -97,13 +98,15 @@ def _ext(stream_ptr: int):
     return torch.cuda.ExternalStream(stream_ptr)
 
 
-def run_batch(runs: list[Emses], sorts: list[int], steps: int, warm_blocks: int = 1) -> float:
+def run_batch(runs: list[Emses], sorts: list[int], steps: int, warm_blocks: int = 1, stats: dict | None = None) -> float:
     """Seconds of device time for `steps` steps of every run through one graph
     (after warm_blocks untimed replays).  Steps beyond whole blocks run on the
     runs' own streams inside the timed region."""
     import torch
     block = block_steps(sorts)
     with Batch(runs, USTEP, block, sorts) as b:
+        if stats is not None:
+            stats["kernels"] = stats.get("kernels", 0) + b.kernels * (steps // block)
         bs = _ext(b.stream)
         if warm_blocks:
             b.launch(warm_blocks)
@@ -238,14 +241,28 @@ def run_ensemble(cases: list[inputs.Case], steps: int, tuner: Autotuner, modes=(
     choice = [tuner.choose(c) for c in cases]
     secs = {m: 0.0 for m in modes}
     plan = waves(cases, budget)
+    stats = {"kernels": 0}
+    e2e = 0.0
+    h2d = d2h = 0
     for w in plan:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         runs = [open_run(cases[i], choice[i].tile) for i in w]
         sorts = [choice[i].sort_every for i in w]
+        torch.cuda.synchronize()
+        e2e += time.perf_counter() - t0
+        h2d += sum(g.field_size("eb") * 8 for g in runs)
         try:
-            torch.cuda.synchronize()
             for m in modes:
                 if m == "batch":
-                    secs[m] += run_batch(runs, sorts, steps, warm_blocks=max(1, -(-warm // block_steps(sorts))))
+                    secs[m] += run_batch(runs, sorts, steps, warm_blocks=max(1, -(-warm // block_steps(sorts))),
+                                         stats=stats)
+                    t0 = time.perf_counter()
+                    for g in runs:
+                        g.download_field("rho")
+                        g.download_field("aj")
+                    e2e += time.perf_counter() - t0
+                    d2h += sum((g.field_size("rho") + g.field_size("aj")) * 8 for g in runs)
                 elif m == "each":
                     secs[m] += run_each(runs, sorts, steps, use_graph=False, warm=warm)
                 elif m == "each_graph":
@@ -258,7 +275,11 @@ def run_ensemble(cases: list[inputs.Case], steps: int, tuner: Autotuner, modes=(
             for g in runs:
                 g.close()
     total = sum(particles(c) for c in cases) * steps
+    if "batch" in secs:
+        e2e += secs["batch"]  # device time of the batches; setup and downloads are wall time
     return {
+        "e2e_seconds": e2e if "batch" in secs else None, "h2d_bytes": h2d, "d2h_bytes": d2h,
+        "batch_kernels": stats["kernels"],
         "runs": len(cases), "steps": steps, "particles": sum(particles(c) for c in cases),
         "particle_steps": total, "waves": len(plan),
         "seconds": secs, "particle_steps_per_s": {m: total / t for m, t in secs.items() if t > 0},

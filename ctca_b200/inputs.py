@@ -92,6 +92,17 @@ def baseline_case(idx: int, scale: float = 1.0) -> Case:
                              Species(ppc, 1.0 / 1836.0, 0.05 / math.sqrt(1836.0), drift=(0.01, 0.0, 0.0))],
                     b0=(0.0, 0.0, 0.1), e_modes=8, e_amp=1e-3, b_modes=8, b_amp=1e-3,
                     kmax=4 * 2 * math.pi / n, seed=1002, sort_tile=(8, 8, 8))
+    if idx == 4:
+        # the adjoint workload: 64^3, the plasma of case 1 at 32 ppc
+        c = baseline_case(1)
+        n = max(8, int(round(64 * scale)))
+        c.n = (n, n, n)
+        for sp in c.species:
+            sp.ppc = 32
+        c.kmax = 4 * 2 * math.pi / n
+        c.seed = 1004
+        c.sort_tile = (8, 8, 8)
+        return c
     raise ValueError(f"no baseline case {idx}")
 
 

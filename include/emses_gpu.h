@@ -273,6 +273,8 @@ int emsesg_batch_create(emsesg_ctx* const* ctxs, int n, int ustep, int block, co
 int emsesg_batch_launch(emsesg_batch* b, int nrep);
 /* The batch's cudaStream_t, as an opaque pointer (for timing events). */
 void* emsesg_batch_stream(emsesg_batch* b);
+/* Kernel launches in one replay of the batch's graph. */
+int emsesg_batch_kernels(const emsesg_batch* b, int64_t* n);
 /* Waits for the batch's work and releases it (the runs stay). */
 int emsesg_batch_destroy(emsesg_batch* b);
 /* Particle counts of the FP32 form (nspec entries). */

@@ -133,10 +133,12 @@ def test_small_ensemble_runs_and_tunes(gpu):
         for s in c.species:
             s.ppc = min(s.ppc, 12)
     tuner = ensemble.Autotuner(steps=4, trial_particles=1 << 20)
-    out = ensemble.run_ensemble(cases, 8, tuner, modes=("batch", "each", "each_graph"), warm=2)
-    assert out["particle_steps"] == 8 * sum(ensemble.particles(c) for c in cases)
+    out = ensemble.run_ensemble(cases, 16, tuner, modes=("batch", "each", "each_graph"), warm=2)
+    assert out["particle_steps"] == 16 * sum(ensemble.particles(c) for c in cases)
     for m in ("batch", "each", "each_graph"):
         assert out["particle_steps_per_s"][m] > 0
+    assert out["batch_kernels"] > 0
+    assert out["e2e_seconds"] > out["seconds"]["batch"]
     assert set(out["choices"]) <= {"side16", "side24"}
     for ch in out["choices"].values():
         assert ch["tile"] in ensemble.TILES and ch["sort_every"] in ensemble.SORTS
