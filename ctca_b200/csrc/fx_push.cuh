@@ -19,12 +19,15 @@
 // its CIC charge to 20 FP32 registers that follow the thread's current cell
 // ("run"); when the run's cell changes the 20 sums go through a per-warp
 // queue and are added, converted to int64 fixed point, into the CTA's tile
-// accumulator by all lanes together.  A particle that leaves its cell (or
-// whose cell lies outside the tile box) is appended to a per-warp "cross"
-// queue; when 32 are queued, every lane takes one and runs the general path
-// (per-axis boundary rules, relay point, two segments in different cells,
-// charge at the new cell) with direct int64 atomics.  So the divergent work
-// of the few cell-crossing particles runs with all lanes busy.
+// accumulator by all lanes together.  A particle that stays in its cell
+// but is out of place in the thread's run (it changed cell since the sort)
+// puts its 20 values into the same queue as a one-particle run.  A particle
+// that leaves its cell (or whose cell lies outside the tile box) is appended
+// to a per-warp "cross" queue; when 32 are queued, every lane takes one and
+// runs the general path (per-axis boundary rules, relay point, two segments
+// in different cells, charge at the new cell) with direct int64 atomics.  So
+// the divergent work of the few cell-crossing particles runs with all lanes
+// busy.
 //
 // Determinism: a run's FP32 partial sums follow the thread's fixed order;
 // every conversion to fixed point is of one value; integer atomics commute.
@@ -36,11 +39,10 @@ constexpr int PUSH_THREADS = 480;           // pushing threads = slots per row
 constexpr int PUSH_WARPS = PUSH_THREADS / 32;
 constexpr int PUSH_BLOCK = PUSH_THREADS + 32;  // + one warp that streams the rows
 constexpr int PG = 1;           // guard cells around the tile
-constexpr int NSTAGE = 4;       // row ring stages
-constexpr int PREFETCH = 2;     // rows issued ahead of the row being pushed
+constexpr int NSTAGE = 5;       // row ring stages (up to NSTAGE - 1 rows in flight)
 constexpr int NJ = 12;          // zigzag node values of one cell
 constexpr int NR = 8;           // CIC node values of one cell
-constexpr int RQW = NJ + NR + 1;  // run-queue entry: 20 sums + cell
+constexpr int RQW = NJ + NR + 1;  // run-queue entry: 20 sums + box index of the cell
 constexpr int RQ_DRAIN = 8;     // drain the run queue at this many entries
 constexpr int RQCAP = RQ_DRAIN + 32;
 constexpr int XQW = 8;          // cross entry: slot, cell, 3 offsets, 3 velocities
@@ -362,28 +364,27 @@ __device__ __forceinline__ void gather8_smem(const float4* f0, const float2* f1,
   b[0] = bx; b[1] = by; b[2] = bz;
 }
 
-// Empties a warp's run queue: lane l takes entries l, l+32, ...  Each lane
-// walks its entry's 20 slots starting at slot (lane mod 20), so lanes holding
-// entries of the same cell add to different nodes at the same time.
-template <int B>
-__device__ __forceinline__ void drain_runs(const Geo& g, unsigned long long* box, const int (&o)[3],
-                                           const int* slot_off, const float* q, int qn, float qfix, int lane) {
+// Empties a warp's run queue.  The queue's (entry, slot) items are dealt
+// out to the lanes in order, item m to lane m mod 32, so every pass keeps all
+// 32 lanes busy however few entries are queued; the items of one entry go
+// to 20 different nodes.  An entry holds its 20 sums and the box index of
+// its cell (only cells inside the box are queued).
+__device__ __forceinline__ void drain_runs(unsigned long long* box, const int* slot_off, const float* q, int qn,
+                                           float qfix, int lane) {
   __syncwarp();
-  const int rot = lane % (NJ + NR);
-  for (int p = 0; p < qn; p += 32) {
-    int e = p + lane;
-    if (e < qn) {
-      const float* en = q + e * RQW;
-      uint32_t key = (uint32_t)__float_as_int(en[NJ + NR]);
-      int i, j, k;
-      unpack(g, key, i, j, k);
-      int base = box_base<B>(o, i, j, k);  // runs are only kept for cells inside the box
-#pragma unroll 4
-      for (int s = 0; s < NJ + NR; s++) {
-        int slot = s + rot;
-        slot -= slot >= NJ + NR ? NJ + NR : 0;
-        atomicAdd(&box[base + slot_off[slot]], (unsigned long long)to_fix(en[slot], qfix));
-      }
+  const int items = qn * (NJ + NR);
+  int e = lane / (NJ + NR), sl = lane % (NJ + NR);
+  for (int m = lane; m < items; m += 32) {
+    const float* en = q + e * RQW;
+    const int base = __float_as_int(en[NJ + NR]);
+    const long long f = to_fix(en[sl], qfix);
+    if (f) atomicAdd(&box[base + slot_off[sl]], (unsigned long long)f);
+    // m += 32: 32 = 1 * 20 + 12
+    sl += 32 - (NJ + NR);
+    e += 1;
+    if (sl >= NJ + NR) {
+      sl -= NJ + NR;
+      e += 1;
     }
   }
   __syncwarp();
@@ -712,11 +713,11 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
           float* en = rq + (rqn + __popc(mk & lt)) * RQW;
 #pragma unroll
           for (int q = 0; q < NJ + NR; q++) en[q] = acc[q];
-          en[NJ + NR] = __int_as_float((int)runcell);
+          en[NJ + NR] = __int_as_float(runbase);
         }
         rqn += __popc(mk);
         if (rqn >= RQ_DRAIN) {
-          drain_runs<B>(g, box, o, slot_off, rq, rqn, qfix, lane);
+          drain_runs(box, slot_off, rq, rqn, qfix, lane);
           rqn = 0;
         }
       }
@@ -729,7 +730,8 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     }
 
     // ---- gather + Buneman-Boris (psolve1.F90:186-272)
-    bool simple = false;
+    bool simple = false, oop = false;
+    int gb = -1;
     float sx = 0.f, syy = 0.f, szz = 0.f;
     if (act) {
       const float x1 = ps.x, y1 = ps.y, z1 = ps.z;
@@ -739,7 +741,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       wv[2] = xy1 * z1; wv[1] = xz1 - wv[2]; wv[3] = yz1 - wv[2]; wv[0] = z1 - xz1 - wv[3];
       wv[6] = xy1 * z2; wv[5] = xz2 - wv[6]; wv[7] = yz2 - wv[6]; wv[4] = z2 - xz2 - wv[7];
       float fe[3], fb[3];
-      const int gb = cell == runcell ? runbase : box_base<B>(o, ib, jb, kb);
+      gb = cell == runcell ? runbase : box_base<B>(o, ib, jb, kb);
       if (gb >= 0)
         gather8_smem<B>(sf0, sf1, gb, wv, fe, fb);
       else
@@ -760,37 +762,58 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       szz = z1 + vz * gustep;
       // an end point exactly on a cell face takes the general path (it may
       // lie on a body face: inclusive bounds)
-      simple = cell == runcell && runbase >= 0 && sx > 0.f && sx < 1.0f && syy > 0.f && syy < 1.0f && szz > 0.f &&
-               szz < 1.0f;
+      const bool incell = sx > 0.f && sx < 1.0f && syy > 0.f && syy < 1.0f && szz > 0.f && szz < 1.0f;
+      simple = incell && cell == runcell && runbase >= 0;
+      // a particle that stays in its cell but is out of place in the thread's
+      // run (it changed cell since the sort): its 20 sums go to the run queue
+      oop = incell && !simple && gb >= 0;
     }
-    if (simple) {
+    const unsigned om = __ballot_sync(0xffffffffu, oop);
+    float* oen = oop ? rq + (rqn + __popc(om & lt)) * RQW : nullptr;
+    if (simple || oop) {
       // both zigzag segments in the same cell: relay point at the midpoint,
       // equal segment fluxes h = (a-b)/2/ustep, mid-points m -+ (a-b)/4; the
       // sum of the two bilinear weight sets is written with S = a+b, D = a-b
       const float Sx = sx + ps.x, Sy = syy + ps.y, Sz = szz + ps.z;
       const float Dx = sx - ps.x, Dy = syy - ps.y, Dz = szz - ps.z;
       const float hx = Dx * hr, hy = Dy * hr, hz = Dz * hr;
+      float cv[NJ + NR];
       float P;
       P = 0.5f * Sy * Sz + 0.125f * Dy * Dz;
-      acc[3] += hx * P; acc[1] += hx * (Sy - P); acc[2] += hx * (Sz - P); acc[0] += hx * (2.0f - Sy - Sz + P);
+      cv[3] = hx * P; cv[1] = hx * (Sy - P); cv[2] = hx * (Sz - P); cv[0] = hx * (2.0f - Sy - Sz + P);
       P = 0.5f * Sx * Sz + 0.125f * Dx * Dz;
-      acc[7] += hy * P; acc[5] += hy * (Sx - P); acc[6] += hy * (Sz - P); acc[4] += hy * (2.0f - Sx - Sz + P);
+      cv[7] = hy * P; cv[5] = hy * (Sx - P); cv[6] = hy * (Sz - P); cv[4] = hy * (2.0f - Sx - Sz + P);
       P = 0.5f * Sx * Sy + 0.125f * Dx * Dy;
-      acc[11] += hz * P; acc[9] += hz * (Sx - P); acc[10] += hz * (Sy - P); acc[8] += hz * (2.0f - Sx - Sy + P);
+      cv[11] = hz * P; cv[9] = hz * (Sx - P); cv[10] = hz * (Sy - P); cv[8] = hz * (2.0f - Sx - Sy + P);
       // CIC charge at the new position (charge.F90:152-210)
       const float XY = sx * syy, XZ = sx * szz, YZ = syy * szz, Z2 = 1.0f - szz, XZ2 = sx * Z2, YZ2 = syy * Z2;
       const float r2 = XY * szz, r6 = XY * Z2;
       const float r3 = YZ - r2, r7 = YZ2 - r6;
-      acc[NJ + 2] += r2; acc[NJ + 1] += XZ - r2; acc[NJ + 3] += r3; acc[NJ + 0] += szz - XZ - r3;
-      acc[NJ + 6] += r6; acc[NJ + 5] += XZ2 - r6; acc[NJ + 7] += r7; acc[NJ + 4] += Z2 - XZ2 - r7;
+      cv[NJ + 2] = r2; cv[NJ + 1] = XZ - r2; cv[NJ + 3] = r3; cv[NJ + 0] = szz - XZ - r3;
+      cv[NJ + 6] = r6; cv[NJ + 5] = XZ2 - r6; cv[NJ + 7] = r7; cv[NJ + 4] = Z2 - XZ2 - r7;
+      if (oop) {
+#pragma unroll
+        for (int q = 0; q < NJ + NR; q++) oen[q] = cv[q];
+        oen[NJ + NR] = __int_as_float(gb);
+      } else {
+#pragma unroll
+        for (int q = 0; q < NJ + NR; q++) acc[q] += cv[q];
+      }
       const int m = r * PUSH_THREADS + tid;
       gpos[m] = make_float4(sx, syy, szz, ps.w);
       gvx[m] = vx;
       gvy[m] = vy;
       gvz[m] = vz;
     }
+    if (om) {
+      rqn += __popc(om);
+      if (rqn >= RQ_DRAIN) {
+        drain_runs(box, slot_off, rq, rqn, qfix, lane);
+        rqn = 0;
+      }
+    }
     // ---- cell-crossing particles: the warp's cross queue
-    const bool cross = act && !simple;
+    const bool cross = act && !simple && !oop;
     const unsigned xm = __ballot_sync(0xffffffffu, cross);
     if (xm) {
       if (cross) {
@@ -816,10 +839,10 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       float* en = rq + (rqn + __popc(mk & lt)) * RQW;
 #pragma unroll
       for (int q = 0; q < NJ + NR; q++) en[q] = acc[q];
-      en[NJ + NR] = __int_as_float((int)runcell);
+      en[NJ + NR] = __int_as_float(runbase);
     }
     rqn += __popc(mk);
-    if (rqn) drain_runs<B>(g, box, o, slot_off, rq, rqn, qfix, lane);
+    if (rqn) drain_runs(box, slot_off, rq, rqn, qfix, lane);
     if (xqn) nesc += drain_cross<B>(a, is, slot0, box, o, xq, xqn, lane);
   }
   if (nesc) atomicAdd(&a.nesc[is], nesc);
