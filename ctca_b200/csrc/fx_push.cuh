@@ -45,9 +45,8 @@ constexpr int NR = 8;           // CIC node values of one cell
 constexpr int RQW = NJ + NR + 1;  // run-queue entry: 20 sums + box index of the cell
 constexpr int RQ_DRAIN = 8;     // drain the run queue at this many entries
 constexpr int RQCAP = RQ_DRAIN + 32;
-constexpr int XQW = 8;          // cross entry: slot, cell, 3 offsets, 3 velocities
-constexpr int XQ_DRAIN = 32;
-constexpr int XQCAP = XQ_DRAIN + 32;
+constexpr int XQW = 8;          // general-path entry: slot, cell, 3 offsets, 3 velocities
+constexpr int XLCAP = 512;      // per-warp list of cross slots
 constexpr uint32_t ROW_BYTES = PUSH_THREADS * (16 + 3 * 4);
 static_assert(PUSH_THREADS == EMSESG_FX_ROW_SLOTS, "row width of the thread-major layout");
 static_assert(ROW_BYTES % 16 == 0 && (PUSH_THREADS * 4) % 16 == 0, "bulk copies move whole 16-byte units");
@@ -364,6 +363,38 @@ __device__ __forceinline__ void gather8_smem(const float4* f0, const float2* f1,
   b[0] = bx; b[1] = by; b[2] = bz;
 }
 
+// Trilinear gather of E and B at the particle (from the tile's shared nodes
+// when its cell lies in the box, gb >= 0, else from the global node field)
+// and the Buneman-Boris velocity update (psolve1.F90:186-272).
+template <int B>
+__device__ __forceinline__ void kick(const FxPushArgs& a, const float4* sf0, const float2* sf1, int gb, int ib, int jb,
+                                     int kb, const float4& ps, float qmp, float& vx, float& vy, float& vz) {
+  const float x1 = ps.x, y1 = ps.y, z1 = ps.z;
+  const float xy1 = x1 * y1, xz1 = x1 * z1, yz1 = y1 * z1, z2 = 1.0f - z1;
+  const float xz2 = x1 * z2, yz2 = y1 * z2;
+  float wv[8];
+  wv[2] = xy1 * z1; wv[1] = xz1 - wv[2]; wv[3] = yz1 - wv[2]; wv[0] = z1 - xz1 - wv[3];
+  wv[6] = xy1 * z2; wv[5] = xz2 - wv[6]; wv[7] = yz2 - wv[6]; wv[4] = z2 - xz2 - wv[7];
+  float fe[3], fb[3];
+  if (gb >= 0) {
+    gather8_smem<B>(sf0, sf1, gb, wv, fe, fb);
+  } else {
+    const int64_t sy = a.g.nx + 1, sz = (int64_t)(a.g.nx + 1) * (a.g.ny + 1);
+    gather8<false>(a.f0, a.f1, ib + sy * jb + sz * kb, sy, sz, wv, fe, fb);
+  }
+  const float eex = fe[0] * qmp, eey = fe[1] * qmp, eez = fe[2] * qmp;
+  const float bbx = fb[0] * qmp, bby = fb[1] * qmp, bbz = fb[2] * qmp;
+  const float boris = __fdividef(2.0f, 1.0f + bbx * bbx + bby * bby + bbz * bbz);
+  vx += eex; vy += eey; vz += eez;
+  const float vxt = vx + vy * bbz - vz * bby;
+  const float vyt = vy + vz * bbx - vx * bbz;
+  const float vzt = vz + vx * bby - vy * bbx;
+  vx += boris * (vyt * bbz - vzt * bby);
+  vy += boris * (vzt * bbx - vxt * bbz);
+  vz += boris * (vxt * bby - vyt * bbx);
+  vx += eex; vy += eey; vz += eez;
+}
+
 // Empties a warp's run queue.  The queue's (entry, slot) items are dealt
 // out to the lanes in order, item m to lane m mod 32, so every pass keeps all
 // 32 lanes busy however few entries are queued; the items of one entry go
@@ -536,10 +567,15 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
   return escaped ? 1 : 0;
 }
 
-// Returns the number of this lane's particles that escaped.
+// The particles of a warp's cross list (slots in the tile region, still
+// holding their state before this step): each lane takes one, repeats the
+// gather and Buneman-Boris of the row loop on it (the same code, so the same
+// velocity) and runs the general path.  Returns the number of this lane's
+// particles that escaped.
 template <int B>
-__device__ __forceinline__ int drain_cross(const FxPushArgs& a, int is, int64_t slot0, unsigned long long* box,
-                                           const int (&o)[3], const float* q, int qn, int lane) {
+__device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t slot0, unsigned long long* box,
+                                          const int (&o)[3], const float4* sf0, const float2* sf1, const int* xl,
+                                          int xn, int lane) {
   __syncwarp();
   // the context comes from the kernel parameters here, so that the pushing
   // loop keeps none of it in registers
@@ -549,9 +585,16 @@ __device__ __forceinline__ int drain_cross(const FxPushArgs& a, int is, int64_t 
                    {a.npbnd[is][0], a.npbnd[is][1], a.npbnd[is][2]}, &a.bd, a.gc,
                    a.surf + (int64_t)is * a.bd.nsurf, is};
   int dead = 0;
-  for (int p = 0; p < qn; p += 32) {
-    int e = p + lane;
-    if (e < qn) dead += cross_one<B>(g, box, o, sk, c, q + e * XQW);
+  for (int e = lane; e < xn; e += 32) {
+    const int loc = xl[e];
+    const float4 ps = c.gpos[loc];
+    float vx = c.gvx[loc], vy = c.gvy[loc], vz = c.gvz[loc];
+    const uint32_t cell = (uint32_t)__float_as_int(ps.w);
+    int ib, jb, kb;
+    unpack(g, cell, ib, jb, kb);
+    kick<B>(a, sf0, sf1, box_base<B>(o, ib, jb, kb), ib, jb, kb, ps, a.qmp[is], vx, vy, vz);
+    const float en[XQW] = {__int_as_float(loc), ps.w, ps.x, ps.y, ps.z, vx, vy, vz};
+    dead += cross_one<B>(g, box, o, sk, c, en);
   }
   __syncwarp();
   return dead;
@@ -590,7 +633,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   float4* sf0 = reinterpret_cast<float4*>(stvz + NSTAGE * PUSH_THREADS);
   float2* sf1 = reinterpret_cast<float2*>(sf0 + NF);
   float* rq = reinterpret_cast<float*>(sf1 + NF) + warp * RQCAP * RQW;
-  float* xq = reinterpret_cast<float*>(sf1 + NF) + PUSH_WARPS * RQCAP * RQW + warp * XQCAP * XQW;
+  int* xl = reinterpret_cast<int*>(reinterpret_cast<float*>(sf1 + NF) + PUSH_WARPS * RQCAP * RQW) + warp * XLCAP;
 
   float4* gpos = a.pos + slot0;
   float* gvx = a.vx + slot0;
@@ -668,7 +711,9 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     if (tid == 0 && okme) seen = 1;
   }
 
-  for (int r = 0; r < L && !failed; r++) {
+  int r = 0;
+  for (;;) {
+  for (; r < L && !failed; r++) {
     const int s = r % NSTAGE;
     uint32_t nextcell = DEAD;
     bool oknext = false;
@@ -734,32 +779,11 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     int gb = -1;
     float sx = 0.f, syy = 0.f, szz = 0.f;
     if (act) {
-      const float x1 = ps.x, y1 = ps.y, z1 = ps.z;
-      const float xy1 = x1 * y1, xz1 = x1 * z1, yz1 = y1 * z1, z2 = 1.0f - z1;
-      const float xz2 = x1 * z2, yz2 = y1 * z2;
-      float wv[8];
-      wv[2] = xy1 * z1; wv[1] = xz1 - wv[2]; wv[3] = yz1 - wv[2]; wv[0] = z1 - xz1 - wv[3];
-      wv[6] = xy1 * z2; wv[5] = xz2 - wv[6]; wv[7] = yz2 - wv[6]; wv[4] = z2 - xz2 - wv[7];
-      float fe[3], fb[3];
       gb = cell == runcell ? runbase : box_base<B>(o, ib, jb, kb);
-      if (gb >= 0)
-        gather8_smem<B>(sf0, sf1, gb, wv, fe, fb);
-      else
-        gather8<false>(a.f0, a.f1, ib + sy * jb + sz * kb, sy, sz, wv, fe, fb);
-      const float eex = fe[0] * qmp, eey = fe[1] * qmp, eez = fe[2] * qmp;
-      const float bbx = fb[0] * qmp, bby = fb[1] * qmp, bbz = fb[2] * qmp;
-      const float boris = __fdividef(2.0f, 1.0f + bbx * bbx + bby * bby + bbz * bbz);
-      vx += eex; vy += eey; vz += eez;
-      const float vxt = vx + vy * bbz - vz * bby;
-      const float vyt = vy + vz * bbx - vx * bbz;
-      const float vzt = vz + vx * bby - vy * bbx;
-      vx += boris * (vyt * bbz - vzt * bby);
-      vy += boris * (vzt * bbx - vxt * bbz);
-      vz += boris * (vxt * bby - vyt * bbx);
-      vx += eex; vy += eey; vz += eez;
-      sx = x1 + vx * gustep;
-      syy = y1 + vy * gustep;
-      szz = z1 + vz * gustep;
+      kick<B>(a, sf0, sf1, gb, ib, jb, kb, ps, qmp, vx, vy, vz);
+      sx = ps.x + vx * gustep;
+      syy = ps.y + vy * gustep;
+      szz = ps.z + vz * gustep;
       // an end point exactly on a cell face takes the general path (it may
       // lie on a body face: inclusive bounds)
       const bool incell = sx > 0.f && sx < 1.0f && syy > 0.f && syy < 1.0f && szz > 0.f && szz < 1.0f;
@@ -812,23 +836,24 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
         rqn = 0;
       }
     }
-    // ---- cell-crossing particles: the warp's cross queue
+    // ---- cell-crossing particles: the warp's cross list (their records
+    // stay as they were; the general path after the row loop redoes them)
     const bool cross = act && !simple && !oop;
     const unsigned xm = __ballot_sync(0xffffffffu, cross);
     if (xm) {
-      if (cross) {
-        float* en = xq + (xqn + __popc(xm & lt)) * XQW;
-        en[0] = __int_as_float(r * PUSH_THREADS + tid);
-        en[1] = ps.w;
-        en[2] = ps.x; en[3] = ps.y; en[4] = ps.z;
-        en[5] = vx; en[6] = vy; en[7] = vz;
-      }
+      if (cross) xl[xqn + __popc(xm & lt)] = r * PUSH_THREADS + tid;
       xqn += __popc(xm);
-      if (xqn >= XQ_DRAIN) {
-        nesc += drain_cross<B>(a, is, slot0, box, o, xq, xqn, lane);
-        xqn = 0;
+      if (xqn > XLCAP - 32) {  // full: empty it, then go on with the next row
+        r++;
+        break;
       }
     }
+  }
+  if (xqn) {
+    nesc += cross_list<B>(a, is, slot0, box, o, sf0, sf1, xl, xqn, lane);
+    xqn = 0;
+  }
+  if (r >= L || failed) break;
   }
   if (failed) report_bad(a.status, a.diag, SITE_FX_PUSH, -3, t);
   // the last run of every thread, and what is left in the queues
@@ -843,7 +868,6 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     }
     rqn += __popc(mk);
     if (rqn) drain_runs(box, slot_off, rq, rqn, qfix, lane);
-    if (xqn) nesc += drain_cross<B>(a, is, slot0, box, o, xq, xqn, lane);
   }
   if (nesc) atomicAdd(&a.nesc[is], nesc);
   if (tid == 0) rows_seen = seen;
@@ -954,5 +978,5 @@ inline int fx_push_smem(int tmax) {
   int nf = B * B * B;
   return 4 * nf * (int)sizeof(unsigned long long) + NSTAGE * (int)ROW_BYTES +
          nf * (int)(sizeof(float4) + sizeof(float2)) +
-         PUSH_WARPS * (RQCAP * RQW + XQCAP * XQW) * (int)sizeof(float);
+         PUSH_WARPS * (RQCAP * RQW * (int)sizeof(float) + XLCAP * (int)sizeof(int));
 }
