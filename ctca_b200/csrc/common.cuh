@@ -56,6 +56,10 @@ struct SortScratch {
 };
 
 // FP32 / fixed-point particle state.
+struct AdjWork;  // reverse-mode workspace (fx.cu), kept between calls
+struct FxState;
+void adj_free(FxState& f);
+
 struct FxState {
   bool loaded = false;
   float4* pos = nullptr;   // {ox, oy, oz, __int_as_float(cell)}
@@ -104,6 +108,7 @@ struct FxState {
   const float4* g_pos = nullptr;       // buffers and configuration it was captured with
   const int64_t* g_ts = nullptr;
   emsesg_config g_cfg{};
+  AdjWork* adj = nullptr;
   int64_t* accum = nullptr;         // int64 (rho, jx, jy, jz) on the rho layout
   float4* fnode = nullptr;          // node field {ex, ey, ez, bx} over (n+1)^3 nodes
   float4* fnode2 = nullptr;         // {by, bz, 0, 0}

@@ -473,6 +473,10 @@ int fx_alloc(emsesg_ctx* ctx) {
   }
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(4)));
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(8)));
+  EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        fx_push_smem(4)));
+  EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        fx_push_smem(8)));
   return EMSESG_OK;
 }
 
@@ -486,6 +490,7 @@ void fx_free(emsesg_ctx* ctx) {
   cudaFree(f.lcs_celltot); cudaFree(f.lcs_tiletot); cudaFree(f.lcs_stray); cudaFree(f.lcs_inv);
   cudaFree(f.surf); cudaFree(f.tailord); cudaFree(f.stage); cudaFree(f.stage_ord);
   if (f.gexec) cudaGraphExecDestroy(f.gexec);
+  adj_free(f);
   f = FxState();
 }
 
@@ -711,7 +716,18 @@ extern "C" int emsesg_fx_store(emsesg_ctx* ctx) {
   return emsesg_synchronize(ctx);
 }
 
+namespace {
+int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit);
+}
+
 extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
+  return fx_step_impl(ctx, ustep, do_sort, true);
+}
+
+namespace {
+// One step; without `deposit` the move only (no rho / J): for recomputing
+// particle states on a grid without bodies or injected particles.
+int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   if (!ctx) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
   if (ustep < 1) return set_error(ctx, EMSESG_ERR_ARG, "ustep must be >= 1");
@@ -728,7 +744,8 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
   FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
   unsigned long long* acc_rho = (unsigned long long*)f.accum;
   unsigned long long* acc_j = acc_rho + fr.size();
-  EMSESG_CUDA(ctx, cudaMemsetAsync(f.accum, 0, (fr.size() + fj.size()) * sizeof(int64_t), ctx->stream));
+  if (deposit)
+    EMSESG_CUDA(ctx, cudaMemsetAsync(f.accum, 0, (fr.size() + fj.size()) * sizeof(int64_t), ctx->stream));
   int tmax = std::max(f.tile[0], std::max(f.tile[1], f.tile[2]));
   int smem = fx_push_smem(tmax);
   FxPushArgs a{};
@@ -756,6 +773,18 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
   a.status = ctx->d_status;
   a.diag = ctx->d_diag;
   dim3 grid((unsigned)f.ntiles, (unsigned)c.nspec);
+  if (!deposit) {
+    for (int is = 0; is < c.nspec; is++)
+      if (f.ntail[is]) return set_error(ctx, EMSESG_ERR_STATE, "move-only step with injected particles");
+    if (a.bd.n > 0) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "move-only step with bodies");
+    if (fx_box_tile(tmax) == 4)
+      EMSESG_LAUNCH(ctx, "fx_move", (k_fx_push<4, false>), grid, PUSH_BLOCK, smem, a);
+    else
+      EMSESG_LAUNCH(ctx, "fx_move", (k_fx_push<8, false>), grid, PUSH_BLOCK, smem, a);
+    ctx->rng_stream++;
+    if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
+    return EMSESG_OK;
+  }
   if (fx_box_tile(tmax) == 4)
     EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<4>, grid, PUSH_BLOCK, smem, a);
   else
@@ -785,6 +814,7 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
   if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
   return EMSESG_OK;
 }
+}  // namespace
 
 extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int64_t n) {
   if (!ctx || n < 0 || (n > 0 && !host)) return EMSESG_ERR_ARG;
@@ -881,6 +911,71 @@ void snap_free(FxSnap& sn) {
   sn = FxSnap();
 }
 
+}  // namespace
+
+// Buffers of emsesg_fx_adjoint, kept from call to call (allocating some
+// thirty snapshots of the particle state costs more than a sweep) and
+// released with the FP32 form.
+struct emsesg::AdjWork {
+  int64_t cap = 0, nl = 0, nn = 0;
+  std::vector<FxSnap> ck, seg;     // checkpoints; the states of one segment
+  std::vector<uint32_t*> inv;      // sort maps of one segment
+  float *lam = nullptr, *lam2 = nullptr, *gd = nullptr, *gEd = nullptr, *gBd = nullptr;
+  float* jx = nullptr;             // probe Jx of each step
+  int jx_steps = 0;
+  double* lossd = nullptr;
+  double* gvd = nullptr;
+  int64_t gv_n = 0;
+  void release() {
+    for (auto& sn : ck) snap_free(sn);
+    for (auto& sn : seg) snap_free(sn);
+    for (auto* q : inv) cudaFree(q);
+    cudaFree(lam); cudaFree(lam2); cudaFree(gd); cudaFree(gEd); cudaFree(gBd); cudaFree(jx);
+    cudaFree(lossd); cudaFree(gvd);
+    *this = AdjWork();
+  }
+};
+
+void emsesg::adj_free(FxState& f) {
+  if (f.adj) {
+    f.adj->release();
+    delete f.adj;
+    f.adj = nullptr;
+  }
+}
+
+namespace {
+
+int adj_reserve(emsesg_ctx* ctx, AdjWork& w, int nseg, int ckpt, int jsteps, int64_t cap, int64_t nl, int64_t nn) {
+  if (w.cap != cap || w.nl != nl || w.nn != nn) w.release();
+  w.cap = cap; w.nl = nl; w.nn = nn;
+  while ((int)w.ck.size() < nseg + 1) {
+    w.ck.emplace_back();
+    int rc = snap_alloc(ctx, w.ck.back(), cap, nl);
+    if (rc) return rc;
+  }
+  while ((int)w.seg.size() < ckpt) {
+    w.seg.emplace_back();
+    int rc = snap_alloc(ctx, w.seg.back(), cap, nl);
+    if (rc) return rc;
+  }
+  if ((int)w.inv.size() < ckpt) w.inv.resize((size_t)ckpt, nullptr);
+  if (!w.lam) EMSESG_CUDA(ctx, cudaMalloc(&w.lam, 6 * cap * sizeof(float)));
+  if (!w.lam2) EMSESG_CUDA(ctx, cudaMalloc(&w.lam2, 6 * cap * sizeof(float)));
+  if (!w.gd) EMSESG_CUDA(ctx, cudaMalloc(&w.gd, 3 * nn * sizeof(float)));
+  if (!w.gEd) EMSESG_CUDA(ctx, cudaMalloc(&w.gEd, 3 * nn * sizeof(float)));
+  if (!w.gBd) EMSESG_CUDA(ctx, cudaMalloc(&w.gBd, 3 * nn * sizeof(float)));
+  if (!w.lossd) EMSESG_CUDA(ctx, cudaMalloc(&w.lossd, sizeof(double)));
+  if (w.jx_steps < jsteps) {
+    cudaFree(w.jx);
+    w.jx = nullptr;
+    w.jx_steps = 0;
+    EMSESG_CUDA(ctx, cudaMalloc(&w.jx, (size_t)jsteps * nn * sizeof(float)));
+    w.jx_steps = jsteps;
+  }
+  return EMSESG_OK;
+}
+
 int snap_copy(emsesg_ctx* ctx, bool save, FxSnap& sn, int64_t cap, int64_t nl) {
   FxState& f = ctx->fx;
   const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
@@ -928,37 +1023,32 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
   FieldDesc fj = field_desc(c, EMSESG_FIELD_AJ);
   const int3 lo = make_int3(probe_lo[0], probe_lo[1], probe_lo[2]);
   const int3 hi = make_int3(probe_hi[0], probe_hi[1], probe_hi[2]);
-  // buffers: checkpoints, the states and sort maps of one segment, the
-  // probe Jx of one segment, lambda, g, node-field gradients
-  std::vector<FxSnap> ck((size_t)nseg + 1), seg((size_t)ckpt);
-  std::vector<uint32_t*> inv((size_t)ckpt, nullptr);
-  float *lam = nullptr, *lam2 = nullptr, *jx = nullptr, *gd = nullptr, *gEd = nullptr, *gBd = nullptr;
-  double *lossd = nullptr, *gvd = nullptr;
-  int rc = EMSESG_OK;
-  auto cleanup = [&]() {
-    for (auto& s : ck) snap_free(s);
-    for (auto& s : seg) snap_free(s);
-    for (auto* p : inv) cudaFree(p);
-    cudaFree(lam); cudaFree(lam2); cudaFree(jx); cudaFree(gd); cudaFree(gEd); cudaFree(gBd);
-    cudaFree(lossd); cudaFree(gvd);
-  };
-#define EMSESG_ADJ(call) do { rc = (call); if (rc) { cleanup(); return rc; } } while (0)
-  for (auto& s : ck) EMSESG_ADJ(snap_alloc(ctx, s, cap, nl));
-  for (auto& s : seg) EMSESG_ADJ(snap_alloc(ctx, s, cap, nl));
-  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&lam, 6 * cap * sizeof(float)), "adjoint lambda"));
-  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&lam2, 6 * cap * sizeof(float)), "adjoint lambda"));
-  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&jx, (size_t)ckpt * nn * sizeof(float)), "adjoint jx"));
-  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&gd, 3 * nn * sizeof(float)), "adjoint g"));
-  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&gEd, 3 * nn * sizeof(float)), "adjoint gE"));
-  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&gBd, 3 * nn * sizeof(float)), "adjoint gB"));
-  EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&lossd, sizeof(double)), "adjoint loss"));
+  // buffers (kept between calls): checkpoints, the states and sort maps of
+  // one segment, lambda, g, node-field gradients, and the probe Jx of every
+  // step, kept from the forward pass so that the recompute of a segment only
+  // moves the particles (no rho / J)
+  if (!f.adj) f.adj = new AdjWork();
+  AdjWork& w = *f.adj;
+  int rc = adj_reserve(ctx, w, nseg, ckpt, K, cap, nl, nn);
+  if (rc) return rc;
+  std::vector<FxSnap>& ck = w.ck;
+  std::vector<FxSnap>& seg = w.seg;
+  std::vector<uint32_t*>& inv = w.inv;
+  float* lam = w.lam;
+  float* lam2 = w.lam2;
+  float* const jx = w.jx;
+  float* const gd = w.gd;
+  float* const gEd = w.gEd;
+  float* const gBd = w.gBd;
+  double* const lossd = w.lossd;
+#define EMSESG_ADJ(call) do { rc = (call); if (rc) return rc; } while (0)
   EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(lossd, 0, sizeof(double), ctx->stream), "adjoint loss"));
   // forward: K steps with a checkpoint every ckpt steps, the loss on the way
   for (int n = 0; n < K; n++) {
     if (n % ckpt == 0) EMSESG_ADJ(snap_copy(ctx, true, ck[(size_t)(n / ckpt)], cap, nl));
     EMSESG_ADJ(emsesg_fx_step(ctx, ustep, (n + 1) % sort_every == 0 ? 1 : 0));
     EMSESG_LAUNCH(ctx, "adj_probe", k_adj_probe, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_AJ], fj, g, lo, hi,
-                  lossd, (float*)nullptr);
+                  lossd, jx + (int64_t)n * nn);
   }
   EMSESG_ADJ(snap_copy(ctx, true, ck[(size_t)nseg], cap, nl));  // the state after K steps, restored at the end
   // backward
@@ -992,9 +1082,7 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
       const bool srt = (n + 1) % sort_every == 0;
       // slots past the new regions keep no map from an earlier sort
       if (srt) EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(f.lcs_inv, 0xFF, cap * sizeof(uint32_t), ctx->stream), "inv"));
-      EMSESG_ADJ(emsesg_fx_step(ctx, ustep, srt ? 1 : 0));
-      EMSESG_LAUNCH(ctx, "adj_probe", k_adj_probe, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_AJ], fj, g, lo, hi,
-                    (double*)nullptr, jx + (int64_t)j * nn);
+      EMSESG_ADJ(fx_step_impl(ctx, ustep, srt ? 1 : 0, false));
       if (srt && j < 64) {
         if (!inv[(size_t)j]) EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&inv[(size_t)j], cap * sizeof(uint32_t)), "inv"));
         EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(inv[(size_t)j], f.lcs_inv, cap * sizeof(uint32_t),
@@ -1016,7 +1104,7 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
         std::swap(lam, lam2);
         lx = lam;
       }
-      EMSESG_LAUNCH(ctx, "adj_g", k_adj_g, nblk(nn), 256, 0, jx + (int64_t)j * nn, nn, gd);
+      EMSESG_LAUNCH(ctx, "adj_g", k_adj_g, nblk(nn), 256, 0, jx + (int64_t)(sgi * ckpt + j) * nn, nn, gd);
       const FxSnap& sn = seg[(size_t)j];
       a.pos = sn.pos; a.vx = sn.vx; a.vy = sn.vy; a.vz = sn.vz;
       a.tile_start = sn.ts; a.tile_pad = sn.tp;
@@ -1040,7 +1128,14 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
   EMSESG_ADJ(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "sync"));
   for (int is = 0; is < c.nspec; is++) { rank0[is] = ntot; ntot += cnt0[is]; }
   if (gv) {
-    EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&gvd, std::max<int64_t>(ntot, 1) * 3 * sizeof(double)), "gv"));
+    if (w.gv_n < ntot) {
+      cudaFree(w.gvd);
+      w.gvd = nullptr;
+      w.gv_n = 0;
+      EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&w.gvd, std::max<int64_t>(ntot, 1) * 3 * sizeof(double)), "gv"));
+      w.gv_n = ntot;
+    }
+    double* const gvd = w.gvd;
     for (int is = 0; is < c.nspec; is++) {
       const int64_t off = f.base[is];
       EMSESG_LAUNCH(ctx, "adj_canonical", k_adj_canonical, (unsigned)f.ntiles, PUSH_THREADS, 0, lx + 3 * cap + off,
@@ -1069,7 +1164,9 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
     }
   if (g0)
     for (int k = 0; k < 6; k++) g0[k] = s0[k];
-  cleanup();
+  // lambda buffers swap in the sweep: keep them with the workspace
+  w.lam = lam;
+  w.lam2 = lam2;
 #undef EMSESG_ADJ
   return emsesg_synchronize(ctx);
 }

@@ -13,7 +13,8 @@
 //   Boris      the rotation transposed term by term -> lambda_v_n,
 //              lambda_E, lambda_B at the particle
 //   gather     w_c lambda_E, w_c lambda_B added to the node-field gradients
-//              (shared-memory box, then global float atomics);
+//              (per-thread run sums in registers, added into a shared-memory
+//              box when the thread's cell changes, then global float atomics);
 //              sum_c grad(w_c) (E_c . lambda_E + B_c . lambda_B) added to
 //              lambda_x
 // The same formulas in FP64 are the CPU checker (oracle/adjoint.cpp).
@@ -152,6 +153,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
   const int tx = t % G.nt[0], ty = (t / G.nt[0]) % G.nt[1], tz = t / (G.nt[0] * G.nt[1]);
   const int o[3] = {tx * G.t[0] - PG, ty * G.t[1] - PG, tz * G.t[2] - PG};
   const int64_t sy = G.nx + 1, sz = (int64_t)(G.nx + 1) * (G.ny + 1);
+  bool anyg = false;
   for (int e = tid; e < NF; e += PUSH_THREADS) {
     const int li = e % B, lj = (e / B) % B, lk = e / (B * B);
     const int gi = o[0] + li, gj = o[1] + lj, gk = o[2] + lk;
@@ -165,12 +167,36 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
     sf1[e] = q;
     const int64_t un = unique_node(G, gi, gj, gk);
 #pragma unroll
-    for (int c = 0; c < 3; c++) sg[3 * e + c] = a.g[3 * un + c];
+    for (int c = 0; c < 3; c++) {
+      sg[3 * e + c] = a.g[3 * un + c];
+      anyg = anyg || sg[3 * e + c] != 0.f;
+    }
 #pragma unroll
     for (int c = 0; c < 6; c++) sgr[6 * e + c] = 0.f;
   }
-  __syncthreads();
+  // dL/dJ is zero on every node of most boxes (the loss sees a probe region
+  // only): their particles' zigzag terms are zero and are skipped
+  anyg = __syncthreads_or(anyg) != 0;
   const AdjBox<B> bx{o, sg, &G, a.g};
+  // the node-field gradient of the thread's current run (its particles of
+  // one cell), 6 values for each of the 8 corners, in registers; added into
+  // sgr when the run ends, so the shared atomics go per run, not per particle
+  float pacc[48];
+#pragma unroll
+  for (int q = 0; q < 48; q++) pacc[q] = 0.f;
+  int runbase = -1;  // box index of the run cell's first corner
+  auto flush = [&]() {
+    if (runbase < 0) return;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int e = runbase + (c >> 2) * B * B + ((c >> 1) & 1) * B + (c & 1);
+#pragma unroll
+      for (int q = 0; q < 6; q++) {
+        if (pacc[6 * c + q] != 0.f) atomicAdd(&sgr[6 * e + q], pacc[6 * c + q]);
+        pacc[6 * c + q] = 0.f;
+      }
+    }
+  };
   const float qmp = a.qmp[is], qq = a.q[is], us = a.us, rustep = a.rustep;
   for (int r = 0; r < L; r++) {
     const int64_t m = slot0 + (int64_t)r * PUSH_THREADS + tid;
@@ -183,25 +209,30 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
     const float3 v0 = f3(a.vx[m], a.vy[m], a.vz[m]);
     // forward recompute: gather (corner c = di + 2 dj + 4 dk)
     float3 E = f3(0.f, 0.f, 0.f), Bf = E;
-    float4 cp[8], cq[8];
     const int li = cb[0] - o[0], lj = cb[1] - o[1], lk = cb[2] - o[2];
     const bool inb = (unsigned)li < (unsigned)(B - 1) && (unsigned)lj < (unsigned)(B - 1) && (unsigned)lk < (unsigned)(B - 1);
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
+    // corner c's node fields (read again by the reversed gather)
+    auto corner = [&](int c, float4& cp, float4& cq) {
       const int di = c & 1, dj = (c >> 1) & 1, dk = c >> 2;
       if (inb) {
         const int e = ((lk + dk) * B + (lj + dj)) * B + (li + di);
-        cp[c] = sf0[e];
-        cq[c] = sf1[e];
+        cp = sf0[e];
+        cq = sf1[e];
       } else {
         const int64_t gn = (cb[0] + di) + sy * (cb[1] + dj) + sz * (cb[2] + dk);
-        cp[c] = __ldg(&a.f0[gn]);
-        cq[c] = __ldg(&a.f1[gn]);
+        cp = __ldg(&a.f0[gn]);
+        cq = __ldg(&a.f1[gn]);
       }
+    };
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int di = c & 1, dj = (c >> 1) & 1, dk = c >> 2;
+      float4 cp, cq;
+      corner(c, cp, cq);
       const float X = di ? bl[0] : 1.0f - bl[0], Y = dj ? bl[1] : 1.0f - bl[1], Z = dk ? bl[2] : 1.0f - bl[2];
       const float w = X * Y * Z;
-      E = add3(E, mul3(w, f3(cp[c].x, cp[c].y, cp[c].z)));
-      Bf = add3(Bf, mul3(w, f3(cp[c].w, cq[c].x, cq[c].y)));
+      E = add3(E, mul3(w, f3(cp.x, cp.y, cp.z)));
+      Bf = add3(Bf, mul3(w, f3(cp.w, cq.x, cq.y)));
     }
     const float3 ee = mul3(qmp, E), tt = mul3(qmp, Bf);
     const float sfac = 2.0f / (1.0f + dot3(tt, tt));
@@ -218,8 +249,10 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
       al[k] = bl[k] + vnv[k] * us;
       ca[k] = cb[k] + (int)floorf(al[k]);
     }
-    float dSda[3], dSdb[3];
-    zigzag_adj<B>(bx, cb, ca, bl, al, qq, rustep, dSda, dSdb);
+    float dSda[3] = {0.f, 0.f, 0.f}, dSdb[3] = {0.f, 0.f, 0.f};
+    const bool ina = (unsigned)(ca[0] - o[0]) < (unsigned)(B - 1) && (unsigned)(ca[1] - o[1]) < (unsigned)(B - 1) &&
+                     (unsigned)(ca[2] - o[2]) < (unsigned)(B - 1);
+    if (anyg || !inb || !ina) zigzag_adj<B>(bx, cb, ca, bl, al, qq, rustep, dSda, dSdb);
     // move: a = b + vnew * ustep
     const float3 la = f3(a.lx[m] + dSda[0], a.ly[m] + dSda[1], a.lz[m] + dSda[2]);
     const float3 lvn = add3(f3(a.lvx[m], a.lvy[m], a.lvz[m]), mul3(us, la));
@@ -237,6 +270,13 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
     lt = add3(lt, mul3(-ls * sfac * sfac, tt));
     le = add3(le, lu);
     const float3 lE = mul3(qmp, le), lB = mul3(qmp, lt);
+    if (inb) {
+      const int base = (lk * B + lj) * B + li;
+      if (base != runbase) {
+        flush();
+        runbase = base;
+      }
+    }
     // gather, reversed
 #pragma unroll
     for (int c = 0; c < 8; c++) {
@@ -244,14 +284,14 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
       const float X = di ? bl[0] : 1.0f - bl[0], Y = dj ? bl[1] : 1.0f - bl[1], Z = dk ? bl[2] : 1.0f - bl[2];
       const float dX = di ? 1.0f : -1.0f, dY = dj ? 1.0f : -1.0f, dZ = dk ? 1.0f : -1.0f;
       const float w = X * Y * Z;
-      const float sdot = cp[c].x * lE.x + cp[c].y * lE.y + cp[c].z * lE.z + cp[c].w * lB.x + cq[c].x * lB.y +
-                         cq[c].y * lB.z;
+      float4 cp, cq;
+      corner(c, cp, cq);
+      const float sdot = cp.x * lE.x + cp.y * lE.y + cp.z * lE.z + cp.w * lB.x + cq.x * lB.y + cq.y * lB.z;
       lb = add3(lb, mul3(sdot, f3(dX * Y * Z, X * dY * Z, X * Y * dZ)));
       const float gv[6] = {w * lE.x, w * lE.y, w * lE.z, w * lB.x, w * lB.y, w * lB.z};
       if (inb) {
-        const int e = ((lk + dk) * B + (lj + dj)) * B + (li + di);
 #pragma unroll
-        for (int q = 0; q < 6; q++) atomicAdd(&sgr[6 * e + q], gv[q]);
+        for (int q = 0; q < 6; q++) pacc[6 * c + q] += gv[q];
       } else {
         const int64_t un = unique_node(G, cb[0] + di, cb[1] + dj, cb[2] + dk);
 #pragma unroll
@@ -268,6 +308,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
     a.lvy[m] = lu.y;
     a.lvz[m] = lu.z;
   }
+  flush();
   __syncthreads();
   for (int e = tid; e < NF; e += PUSH_THREADS) {
     const int li = e % B, lj = (e / B) % B, lk = e / (B * B);

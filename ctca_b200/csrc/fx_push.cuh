@@ -489,7 +489,7 @@ __device__ __forceinline__ bool body_absorb(const CrossCtx& c, const int (&ib)[3
 // General path for one particle that left its cell (or whose cell lies
 // outside the box): boundary rules, zigzag with relay point, charge at the
 // stored cell; the final record is written here.
-template <int B>
+template <int B, bool DEP = true>
 __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, const int (&o)[3], const Sink& sk,
                                          const CrossCtx& c, const float* en) {
   const int loc = __float_as_int(en[0]);
@@ -518,6 +518,7 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
   c.gvx[loc] = vx;
   c.gvy[loc] = vy;
   c.gvz[loc] = vz;
+  if (!DEP) return escaped ? 1 : 0;
   // zigzag (psolve1.F90:717-757), integer parts first
   float J[NJ];
   {
@@ -572,7 +573,7 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
 // gather and Buneman-Boris of the row loop on it (the same code, so the same
 // velocity) and runs the general path.  Returns the number of this lane's
 // particles that escaped.
-template <int B>
+template <int B, bool DEP>
 __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t slot0, unsigned long long* box,
                                           const int (&o)[3], const float4* sf0, const float2* sf1, const int* xl,
                                           int xn, int lane) {
@@ -594,13 +595,15 @@ __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t s
     unpack(g, cell, ib, jb, kb);
     kick<B>(a, sf0, sf1, box_base<B>(o, ib, jb, kb), ib, jb, kb, ps, a.qmp[is], vx, vy, vz);
     const float en[XQW] = {__int_as_float(loc), ps.w, ps.x, ps.y, ps.z, vx, vy, vz};
-    dead += cross_one<B>(g, box, o, sk, c, en);
+    dead += cross_one<B, DEP>(g, box, o, sk, c, en);
   }
   __syncwarp();
   return dead;
 }
 
-template <int T>
+// DEP = false: the move only (positions, velocities, boundary rules; no
+// current, no charge), for recomputing particle states.
+template <int T, bool DEP = true>
 __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   constexpr int B = T + 2 * PG + 1;  // box and field tile edge (nodes)
   constexpr int NBOX = 4 * B * B * B;
@@ -648,7 +651,8 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     mbar_fence_init();
   }
   if (tid < NJ + NR) slot_off[tid] = tid < NJ ? BoxT<B>::joff(tid) : BoxT<B>::roff(tid - NJ);
-  for (int e = tid; e < NBOX; e += PUSH_BLOCK) box[e] = 0ull;
+  if (DEP)
+    for (int e = tid; e < NBOX; e += PUSH_BLOCK) box[e] = 0ull;
   const int64_t sy = g.nx + 1, sz = (int64_t)(g.nx + 1) * (g.ny + 1);
   for (int e = tid; e < NF; e += PUSH_BLOCK) {
     int li = e % B, lj = (e / B) % B, lk = e / (B * B);
@@ -749,8 +753,8 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     }
     // ---- a new cell ends the thread's run (its sums go to the run queue)
     // when the next particle is in that cell too, or when there is no run
-    const bool newrun = act && cell != runcell && (runbase < 0 || nextcell == cell || nextcell == DEAD);
-    {
+    const bool newrun = DEP && act && cell != runcell && (runbase < 0 || nextcell == cell || nextcell == DEAD);
+    if (DEP) {
       const bool evict = newrun && runbase >= 0;
       const unsigned mk = __ballot_sync(0xffffffffu, evict);
       if (mk) {
@@ -787,14 +791,14 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       // an end point exactly on a cell face takes the general path (it may
       // lie on a body face: inclusive bounds)
       const bool incell = sx > 0.f && sx < 1.0f && syy > 0.f && syy < 1.0f && szz > 0.f && szz < 1.0f;
-      simple = incell && cell == runcell && runbase >= 0;
+      simple = incell && (!DEP || (cell == runcell && runbase >= 0));
       // a particle that stays in its cell but is out of place in the thread's
       // run (it changed cell since the sort): its 20 sums go to the run queue
-      oop = incell && !simple && gb >= 0;
+      oop = DEP && incell && !simple && gb >= 0;
     }
-    const unsigned om = __ballot_sync(0xffffffffu, oop);
+    const unsigned om = DEP ? __ballot_sync(0xffffffffu, oop) : 0u;
     float* oen = oop ? rq + (rqn + __popc(om & lt)) * RQW : nullptr;
-    if (simple || oop) {
+    if (DEP && (simple || oop)) {
       // both zigzag segments in the same cell: relay point at the midpoint,
       // equal segment fluxes h = (a-b)/2/ustep, mid-points m -+ (a-b)/4; the
       // sum of the two bilinear weight sets is written with S = a+b, D = a-b
@@ -823,6 +827,8 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
 #pragma unroll
         for (int q = 0; q < NJ + NR; q++) acc[q] += cv[q];
       }
+    }
+    if (simple || oop) {
       const int m = r * PUSH_THREADS + tid;
       gpos[m] = make_float4(sx, syy, szz, ps.w);
       gvx[m] = vx;
@@ -850,14 +856,14 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     }
   }
   if (xqn) {
-    nesc += cross_list<B>(a, is, slot0, box, o, sf0, sf1, xl, xqn, lane);
+    nesc += cross_list<B, DEP>(a, is, slot0, box, o, sf0, sf1, xl, xqn, lane);
     xqn = 0;
   }
   if (r >= L || failed) break;
   }
   if (failed) report_bad(a.status, a.diag, SITE_FX_PUSH, -3, t);
   // the last run of every thread, and what is left in the queues
-  {
+  if (DEP) {
     const bool has = runbase >= 0;
     const unsigned mk = __ballot_sync(0xffffffffu, has);
     if (has) {
@@ -877,23 +883,25 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   if (warp == PUSH_WARPS && lane == 0)
     for (int r = rows_seen; r < issued; r++) (void)mbar_wait(&full_bar[r % NSTAGE], (uint32_t)((r / NSTAGE) & 1));
   // add the tile accumulator into the global int64 arrays
-  for (int e = tid; e < NBOX; e += PUSH_BLOCK) {
-    unsigned long long v = box[e];
-    if (v == 0ull) continue;
-    int li = e % B, lj = (e / B) % B, lk = (e / (B * B)) % B, comp = e / (B * B * B);
-    int i = o[0] + li, j = o[1] + lj, k = o[2] + lk;
-    if (comp == 0) {
-      if (i < -1 || j < -1 || k < -1 || i > g.nx + 1 || j > g.ny + 1 || k > g.nz + 1) {
-        report_bad(a.status, a.diag, SITE_FX_FLUSH, t, i + 100000LL * j + 10000000000LL * k);
-        continue;
+  if (DEP) {
+    for (int e = tid; e < NBOX; e += PUSH_BLOCK) {
+      unsigned long long v = box[e];
+      if (v == 0ull) continue;
+      int li = e % B, lj = (e / B) % B, lk = (e / (B * B)) % B, comp = e / (B * B * B);
+      int i = o[0] + li, j = o[1] + lj, k = o[2] + lk;
+      if (comp == 0) {
+        if (i < -1 || j < -1 || k < -1 || i > g.nx + 1 || j > g.ny + 1 || k > g.nz + 1) {
+          report_bad(a.status, a.diag, SITE_FX_FLUSH, t, i + 100000LL * j + 10000000000LL * k);
+          continue;
+        }
+        atomicAdd(&a.acc_rho[a.fr.at(0, i, j, k)], v);
+      } else {
+        if (i < -4 || j < -4 || k < -4 || i > g.nx + 4 || j > g.ny + 4 || k > g.nz + 4) {
+          report_bad(a.status, a.diag, SITE_FX_FLUSH, t, i + 100000LL * j + 10000000000LL * k);
+          continue;
+        }
+        atomicAdd(&a.acc_j[a.fj.at(comp - 1, i, j, k)], v);
       }
-      atomicAdd(&a.acc_rho[a.fr.at(0, i, j, k)], v);
-    } else {
-      if (i < -4 || j < -4 || k < -4 || i > g.nx + 4 || j > g.ny + 4 || k > g.nz + 4) {
-        report_bad(a.status, a.diag, SITE_FX_FLUSH, t, i + 100000LL * j + 10000000000LL * k);
-        continue;
-      }
-      atomicAdd(&a.acc_j[a.fj.at(comp - 1, i, j, k)], v);
     }
   }
 }
