@@ -440,6 +440,173 @@ def run_ensemble_line(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def _flux(mu, sig, sign):
+    """E[(sign v)+] for v ~ N(mu, sig^2)."""
+    from math import erf, exp, pi, sqrt
+    m = sign * mu
+    return sig * exp(-0.5 * (m / sig) ** 2) / sqrt(2 * pi) + m * 0.5 * (1 + erf(m / sig / sqrt(2)))
+
+
+def _body_step(job):
+    """The injected records of one step of the body workload (see
+    body_injection); runs in a worker process."""
+    case, scale, seed, step = job
+    from ctca_b200 import inject, inputs
+    renv = inputs.units()["renv"]
+    nx, ny, nz = case.n
+    rng = np.random.default_rng([seed, step])
+    body = case.bodies[0]
+    nemit = int(round((1 << 20) * scale ** 3))
+    recs = []
+    for isp, s in enumerate(case.species):
+        vd = s.drift[2]
+        vxt = inject.maxwell_table(s.vth * renv, 0.0, 4096)
+        vyt = np.random.default_rng([seed, 99, isp]).permutation(vxt)  # tables drawn apart, as vxr / vyr
+        parts = []
+        for front, sgn in ((True, +1.0), (False, -1.0)):
+            cnt = s.ppc * nx * ny * _flux(vd, s.vth, sgn) * case.dt
+            n = int(cnt) + (1 if rng.random() < cnt - int(cnt) else 0)
+            if n:
+                vz = inject.flux_table(s.vth * renv, vd * renv, 4096, sign=sgn)
+                parts.append(inject.inflow_z(front, n, nx, ny, nz, vz, vxt, vyt, 2.0, rng, spec=isp + 1))
+        if isp == 0 and nemit:
+            vn = inject.flux_table(0.01 * renv, 0.0, 4096)
+            vt = inject.maxwell_table(0.01 * renv, 0.0, 4096)
+            parts.append(inject.emit_rectangle(1, body["xupc"], (body["ylpc"], body["yupc"]),
+                                               (body["zlpc"], body["zupc"]), nemit, vn, vt, rng, spec=1))
+        recs.append(np.concatenate(parts))
+    return recs
+
+
+def body_injection(case, steps: int, scale: float, seed: int):
+    """Records injected before each step of the body workload: inflow of
+    both species through the z faces at the rate of their drifting
+    Maxwellian flux (particles per step = ppc * face cells * flux * dt), and
+    2^20 (x scale^3) photoelectrons from the body's +x face with vth = 0.01
+    (pairs of an anti-particle on the face and a particle just off it).
+    Drawn in worker processes (started before any CUDA call).  Returns
+    [step][species] record arrays."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    jobs = [(case, scale, seed, k) for k in range(steps)]
+    workers = max(1, min(len(jobs), (os.cpu_count() or 2) - 1, 32))
+    with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_body_step, jobs))
+
+
+def run_body_line(args, world, rank, local):
+    """The body workload: 256x256x512 cells, open z, solar-wind electrons and
+    ions (24 ppc each, 1.61e9 particles) drifting along -z past a 32x32x16
+    conducting box that absorbs them (int64 counts per surface cell) and
+    emits 2^20 photoelectrons a step from its +x face, inflow through the z
+    faces; B0 = (0.05, 0, 0.1), E = 0.  An FP32-only context (no FP64
+    particle buffer) holds it on one GPU.  Each timed step injects the
+    step's records (host -> device) and pushes; sort every 4 steps."""
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the body workload (1.6e9 particles) is timed on "
+                              "the GPU only; the reference CPU path is timed by the default workload"}), flush=True)
+        return
+    import torch
+    from ctca_b200 import inputs
+    from ctca_b200.emses import Emses, select_device
+    torch.cuda.set_device(local)
+    select_device(local)
+    scale = args.body_scale
+    case = inputs.baseline_case(3, scale)
+    steps, warm = args.steps, args.warmup
+    inj = body_injection(case, warm + steps + 5, scale, seed=case.seed + 17 * rank)
+    add = [sum(int(st[i].size) for st in inj) for i in range(2)]
+    ncell = case.n[0] * case.n[1] * case.n[2]
+    cap = [int(s.ppc * ncell * 1.01) + add[i] + (1 << 20) for i, s in enumerate(case.species)]
+    cfg = inputs.make_config(case, capacity=cap)
+    cfg.flags = 1  # EMSESG_FLAG_FP32_ONLY
+    g = Emses(cfg)
+    g.fx_load_plasma(inputs.plasma(case, seed=case.seed + 1000 * rank))
+    stream = torch.cuda.ExternalStream(g.stream)
+    k = [0]
+
+    def step():
+        recs = inj[k[0]]
+        for isp in range(2):
+            if recs[isp].size:
+                g.fx_inject(isp + 1, recs[isp])
+        g.fx_step(2, k[0] % SORT_EVERY == SORT_EVERY - 1)
+        k[0] += 1
+
+    for _ in range(warm):
+        step()
+    g.synchronize()
+    n0 = int(g.fx_counts().sum())
+    g.set_profiling(True)
+    g.profile_reset()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    t = max_over_ranks(world, e0.elapsed_time(e1) / 1e3)
+    prof = g.profile()
+    g.set_profiling(False)
+    n1 = int(g.fx_counts().sum())
+    inj_bytes = sum(int(r.nbytes) for st in inj[warm:warm + steps] for r in st)
+    # end to end: the same steps plus rho and J to host after each one
+    nr, na = g.field_size("rho"), g.field_size("aj")
+    rho_h = torch.empty(nr, dtype=torch.float64, pin_memory=True)
+    aj_h = torch.empty(na, dtype=torch.float64, pin_memory=True)
+    ke = min(5, len(inj) - k[0])
+    ne0 = int(g.fx_counts().sum())
+    g.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        step()
+        g.lib.emsesg_download_field(g.h, 4, rho_h.data_ptr())
+        g.lib.emsesg_download_field(g.h, 2, aj_h.data_ptr())
+    g.synchronize()
+    te = time.perf_counter() - t0
+    ne1 = int(g.fx_counts().sum())
+    surf = g.fx_surface()
+    counters = g.get_counters().as_dict()
+    hbm, peak_kind = peaks()
+    ms, launches = prof.get("fx_push", (0.0, 0))
+    npart = 0.5 * (n0 + n1)
+    achieved = B_ALG_PUSH * npart / (ms / 1e3 / launches) / 1e9 if launches else None
+    out = {
+        "metric": METRIC, "value": world * npart * steps / t, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": warm, "ms_per_step": t / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+i64", "data": "synthetic",
+        "config": {"workload": f"{case.n[0]}x{case.n[1]}x{case.n[2]} cells, open z, 2 species x 24 ppc "
+                               f"({n0:,} particles at the start), drift -0.08 z, box body "
+                               f"{int(case.bodies[0]['xupc'] - case.bodies[0]['xlpc'])}x"
+                               f"{int(case.bodies[0]['yupc'] - case.bodies[0]['ylpc'])}x"
+                               f"{int(case.bodies[0]['zupc'] - case.bodies[0]['zlpc'])} absorbing with int64 "
+                               f"surface counts, {inj[0][0].size:,} electron and {inj[0][1].size:,} ion records "
+                               "injected a step (z inflow + photoemission pairs), sort every 4, FP32-only context",
+                   "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (achieved / hbm) if achieved else None, "traffic": None, "kernel": "fx_push",
+                     "peak_kind": peak_kind, "bytes_per_particle_alg": B_ALG_PUSH},
+        "e2e": {"value": world * 0.5 * (ne0 + ne1) * ke / te, "unit": UNIT, "steps": ke,
+                "h2d_bytes_per_step": int(inj_bytes / steps), "d2h_bytes_per_step": int((nr + na) * 8)},
+        "particles": {"start": n0, "end": n1},
+        "absorbed": {"influx_e": int(counters["influx"][0].sum()), "influx_i": int(counters["influx"][1].sum()),
+                     "surface_net_e": int(surf[0].sum()), "surface_net_i": int(surf[1].sum()),
+                     "escaped_e": int(counters["nesc"][0]), "escaped_i": int(counters["nesc"][1])},
+        "gpu_launches": int(sum(n for _, n in prof.values())),
+        "kernels_ms": {kk: round(v[0], 3) for kk, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+        "clocks": clk.summary(),
+    }
+    g.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -453,13 +620,16 @@ def main():
     ap.add_argument("--cells", type=int, default=0, help="grid side of a smaller profiling case (default 128)")
     ap.add_argument("--ppc", type=int, default=0, help="particles per cell per species with --cells")
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and ensemble sections")
-    ap.add_argument("--workload", default="particle_step", choices=["particle_step", "ensemble"])
+    ap.add_argument("--workload", default="particle_step", choices=["particle_step", "ensemble", "body"])
+    ap.add_argument("--body-scale", type=float, default=1.0, help="grid scale of the body workload (1: 256x256x512)")
     ap.add_argument("--ensemble-runs", type=int, default=None)
     ap.add_argument("--ensemble-steps", type=int, default=None)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
-        if args.workload == "ensemble":
+        if args.workload == "body":
+            run_body_line(args, world, rank, local)
+        elif args.workload == "ensemble":
             args.ensemble_runs = args.ensemble_runs or 512
             args.ensemble_steps = args.ensemble_steps or 200
             run_ensemble_line(args, world, rank, local)

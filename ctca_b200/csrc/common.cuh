@@ -151,6 +151,9 @@ struct emsesg_ctx {
 namespace emsesg {
 
 int set_error(emsesg_ctx* ctx, int code, const char* fmt, ...);
+// Records m0 .. m0+n-1 of species `is` of the seeded plasma of
+// emsesg_load_plasma, into the device array dst (n records).
+int plasma_records(emsesg_ctx* ctx, emsesg_particle* dst, int is, int64_t m0, int64_t n, const emsesg_plasma* pl);
 int check_cuda(emsesg_ctx* ctx, cudaError_t e, const char* what);
 // Launch bracketing for the per-kernel profile.
 void timer_begin(emsesg_ctx* ctx, const char* name);

@@ -98,6 +98,7 @@ static int validate_config(emsesg_ctx* ctx, const emsesg_config* c) {
   }
   for (int d = 0; d < 3; d++)
     if (c->sort_tile[d] < 0) return set_error(ctx, EMSESG_ERR_ARG, "sort_tile must be >= 0");
+  if (c->flags & ~EMSESG_FLAG_FP32_ONLY) return set_error(ctx, EMSESG_ERR_ARG, "unknown config flags");
   return EMSESG_OK;
 }
 
@@ -136,7 +137,9 @@ extern "C" int emsesg_create(const emsesg_config* cfg, emsesg_ctx** out) {
   if ((e = cudaMalloc(&ctx->d_cfg, sizeof(emsesg_config)))) return fail(e, "cfg");
   if ((e = cudaMemcpyAsync(ctx->d_cfg, &ctx->cfg, sizeof(emsesg_config), cudaMemcpyHostToDevice, ctx->stream)))
     return fail(e, "cfg");
-  if ((e = cudaMalloc(&ctx->pbuf, std::max<int64_t>(cap, 1) * sizeof(emsesg_particle)))) return fail(e, "pbuf");
+  // no FP64 particle buffer in FP32-only contexts (a one-record placeholder)
+  const int64_t cap64 = (cfg->flags & EMSESG_FLAG_FP32_ONLY) ? 1 : std::max<int64_t>(cap, 1);
+  if ((e = cudaMalloc(&ctx->pbuf, cap64 * sizeof(emsesg_particle)))) return fail(e, "pbuf");
   for (int f = 0; f < EMSESG_NFIELDS; f++) {
     int64_t n = field_doubles(ctx->cfg, f);
     if ((e = cudaMalloc(&ctx->field[f], n * sizeof(double)))) return fail(e, "field");
@@ -241,6 +244,8 @@ extern "C" int emsesg_upload_particles(emsesg_ctx* ctx, int ps, const emsesg_par
   int rc = check_ps(ctx, ps);
   if (rc) return rc;
   if (!pbuf || !totalp) return set_error(ctx, EMSESG_ERR_ARG, "null argument");
+  if (ctx->cfg.flags & EMSESG_FLAG_FP32_ONLY)
+    return set_error(ctx, EMSESG_ERR_STATE, "FP32-only context: no FP64 particle records");
   for (int is = 0; is < ctx->cfg.nspec; is++)
     if (totalp[is] < 0 || totalp[is] > ctx->seg.capacity[is])
       return set_error(ctx, EMSESG_ERR_OVERFLOW, "species %d: %lld particles exceed capacity %lld", is + 1,
@@ -263,6 +268,8 @@ extern "C" int emsesg_upload_particles(emsesg_ctx* ctx, int ps, const emsesg_par
 extern "C" int emsesg_download_particles(emsesg_ctx* ctx, int ps, emsesg_particle* pbuf, int64_t* totalp) {
   int rc = check_ps(ctx, ps);
   if (rc) return rc;
+  if (ctx->cfg.flags & EMSESG_FLAG_FP32_ONLY)
+    return set_error(ctx, EMSESG_ERR_STATE, "FP32-only context: no FP64 particle records");
   EMSESG_CUDA(ctx, cudaMemcpyAsync(ctx->totalp, ctx->d_count, EMSESG_ISPEC * sizeof(int64_t), cudaMemcpyDeviceToHost,
                                    ctx->stream));
   EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

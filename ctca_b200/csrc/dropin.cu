@@ -706,10 +706,12 @@ __global__ void k_advance(int64_t* pos, const uint32_t* total) { *pos += *total;
 __global__ void k_set_count(int64_t* count, const uint32_t* total) { *count = *total; }
 
 // Synthetic plasma, same streams as orc_load_plasma (oracle/emses_oracle.cpp).
-__global__ void k_load_plasma(emsesg_particle* p, int64_t n, int ppc, int nx, int ny, int is, uint64_t seed,
-                              double vth, double vdx, double vdy, double vdz) {
-  int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= n) return;
+// Particles m0 .. m0+n-1 of species `is` into p[0 .. n).
+__global__ void k_load_plasma(emsesg_particle* p, int64_t m0, int64_t n, int ppc, int nx, int ny, int is,
+                              uint64_t seed, double vth, double vdx, double vdy, double vdz) {
+  const int64_t loc = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (loc >= n) return;
+  const int64_t m = m0 + loc;
   int64_t cell = m / ppc;
   int i = (int)(cell % nx), j = (int)((cell / nx) % ny), k = (int)(cell / ((int64_t)nx * ny));
   uint64_t st = 1000 + is;
@@ -729,7 +731,7 @@ __global__ void k_load_plasma(emsesg_particle* p, int64_t n, int ppc, int nx, in
   q.preside = 0;
   q.nid = 0;
   q.spec = is + 1;
-  p[m] = q;
+  p[loc] = q;
 }
 
 inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
@@ -1073,8 +1075,18 @@ extern "C" int emsesg_compact(emsesg_ctx* ctx, int ps, int64_t* totalp) {
   return emsesg_synchronize(ctx);
 }
 
+int emsesg::plasma_records(emsesg_ctx* ctx, emsesg_particle* dst, int is, int64_t m0, int64_t n,
+                           const emsesg_plasma* pl) {
+  const emsesg_config& c = ctx->cfg;
+  EMSESG_LAUNCH(ctx, "load_plasma", k_load_plasma, nblk(n), 256, 0, dst, m0, n, pl->ppc[is], c.nx, c.ny, is,
+                pl->seed, pl->vth[is], pl->vdrift[is][0], pl->vdrift[is][1], pl->vdrift[is][2]);
+  return EMSESG_OK;
+}
+
 extern "C" int emsesg_load_plasma(emsesg_ctx* ctx, const emsesg_plasma* pl) {
   if (!ctx || !pl) return EMSESG_ERR_ARG;
+  if (ctx->cfg.flags & EMSESG_FLAG_FP32_ONLY)
+    return set_error(ctx, EMSESG_ERR_STATE, "FP32-only context: use emsesg_fx_load_plasma");
   const emsesg_config& c = ctx->cfg;
   int64_t ncell = (int64_t)c.nx * c.ny * c.nz;
   for (int is = 0; is < c.nspec; is++) {
@@ -1086,9 +1098,8 @@ extern "C" int emsesg_load_plasma(emsesg_ctx* ctx, const emsesg_plasma* pl) {
     int64_t n = ncell * pl->ppc[is];
     ctx->totalp[is] = n;
     if (n == 0) continue;
-    EMSESG_LAUNCH(ctx, "load_plasma", k_load_plasma, nblk(n), 256, 0, ctx->pbuf + ctx->seg.base[is], n,
-                  pl->ppc[is], c.nx, c.ny, is, pl->seed, pl->vth[is], pl->vdrift[is][0], pl->vdrift[is][1],
-                  pl->vdrift[is][2]);
+    int rc = plasma_records(ctx, ctx->pbuf + ctx->seg.base[is], is, 0, n, pl);
+    if (rc) return rc;
   }
   EMSESG_CUDA(ctx, cudaMemcpyAsync(ctx->d_count, ctx->totalp, EMSESG_ISPEC * sizeof(int64_t), cudaMemcpyHostToDevice,
                                    ctx->stream));

@@ -652,6 +652,8 @@ extern "C" int emsesg_fx_sort(emsesg_ctx* ctx) {
 
 extern "C" int emsesg_fx_load(emsesg_ctx* ctx) {
   if (!ctx) return EMSESG_ERR_ARG;
+  if (ctx->cfg.flags & EMSESG_FLAG_FP32_ONLY)
+    return set_error(ctx, EMSESG_ERR_STATE, "FP32-only context: use emsesg_fx_load_plasma");
   int rc = fx_alloc(ctx);
   if (rc) return rc;
   FxState& f = ctx->fx;
@@ -675,6 +677,92 @@ extern "C" int emsesg_fx_load(emsesg_ctx* ctx) {
   return emsesg_synchronize(ctx);
 }
 
+namespace emsesg {
+namespace {
+// Particles whose start point lies inside a box body (inclusive bounds, the
+// absorption test of the push) are not placed: DEAD.
+__global__ void k_fx_clear_bodies(float4* pos, int64_t n, Geo g, Bodies bd) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const float4 p = pos[m];
+  const uint32_t cell = (uint32_t)__float_as_int(p.w);
+  if (cell == DEAD) return;
+  int c3[3];
+  unpack(g, cell, c3[0], c3[1], c3[2]);
+  const float f3v[3] = {p.x, p.y, p.z};
+  for (int q = 0; q < bd.n; q++) {
+    bool in = true;
+    for (int d = 0; d < 3; d++)
+      in = in && c3[d] >= bd.lo[q][d] && (c3[d] < bd.hi[q][d] || (c3[d] == bd.hi[q][d] && f3v[d] == 0.0f));
+    if (in) {
+      pos[m].w = __int_as_float((int)DEAD);
+      return;
+    }
+  }
+}
+}  // namespace
+}  // namespace emsesg
+
+// The records come through a bounded device scratch in chunks and are
+// converted by the same kernel as emsesg_fx_load, so the state is the one
+// emsesg_load_plasma + emsesg_fx_load give (without bodies: particles that
+// start inside a box body are left out here).
+extern "C" int emsesg_fx_load_plasma(emsesg_ctx* ctx, const emsesg_plasma* pl) {
+  if (!ctx || !pl) return EMSESG_ERR_ARG;
+  const emsesg_config& c = ctx->cfg;
+  std::string why;
+  if (!bodies_supported(c, &why)) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "%s", why.c_str());
+  const int64_t ncell = (int64_t)c.nx * c.ny * c.nz;
+  for (int is = 0; is < c.nspec; is++) {
+    const int64_t n = ncell * pl->ppc[is];
+    if (pl->ppc[is] < 0 || n > ctx->seg.capacity[is])
+      return set_error(ctx, EMSESG_ERR_OVERFLOW, "species %d: %lld particles exceed capacity", is + 1, (long long)n);
+  }
+  int rc = fx_alloc(ctx);
+  if (rc) return rc;
+  FxState& f = ctx->fx;
+  Geo g = make_geo(ctx);
+  int64_t most = 0;
+  for (int is = 0; is < c.nspec; is++) most = std::max(most, ncell * pl->ppc[is]);
+  const int64_t chunk = std::min<int64_t>(std::max<int64_t>(most, 1), 1 << 25);  // 2 GiB of records at most
+  emsesg_particle* tmp = nullptr;
+  EMSESG_CUDA(ctx, cudaMalloc(&tmp, chunk * sizeof(emsesg_particle)));
+  for (int is = 0; is < c.nspec && !rc; is++) {
+    const int64_t n = ncell * pl->ppc[is];
+    ctx->totalp[is] = n;
+    for (int64_t m0 = 0; m0 < n && !rc; m0 += chunk) {
+      const int64_t k = std::min(chunk, n - m0);
+      rc = plasma_records(ctx, tmp, is, m0, k, pl);
+      if (rc) break;
+      const int64_t o = f.base[is] + m0;
+      cudaError_t e;
+      k_fx_from_aos<<<nblk(k), 256, 0, ctx->stream>>>(tmp, k, g, f.pos + o, f.vx + o, f.vy + o, f.vz + o,
+                                                     ctx->d_status, ctx->d_diag);
+      if ((e = cudaGetLastError()) != cudaSuccess) rc = check_cuda(ctx, e, "fx_from_aos");
+    }
+  }
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(tmp);
+  if (rc) return rc;
+  const Bodies bd = make_bodies(c);
+  if (bd.n > 0)
+    for (int is = 0; is < c.nspec; is++)
+      if (ctx->totalp[is])
+        EMSESG_LAUNCH(ctx, "fx_clear_bodies", k_fx_clear_bodies, nblk(ctx->totalp[is]), 256, 0, f.pos + f.base[is],
+                      ctx->totalp[is], g, bd);
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(ctx->d_count, ctx->totalp, EMSESG_ISPEC * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                   ctx->stream));
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(f.count_d, ctx->totalp, EMSESG_ISPEC * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                   ctx->stream));
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(f.slots_d, ctx->totalp, EMSESG_ISPEC * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                   ctx->stream));
+  f.loaded = true;
+  f.tiled = false;
+  rc = emsesg_fx_sort(ctx);
+  if (rc) return rc;
+  return emsesg_synchronize(ctx);
+}
+
 extern "C" int emsesg_fx_counts(emsesg_ctx* ctx, int64_t* totalp) {
   if (!ctx || !totalp) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded");
@@ -687,6 +775,8 @@ extern "C" int emsesg_fx_counts(emsesg_ctx* ctx, int64_t* totalp) {
 extern "C" int emsesg_fx_store(emsesg_ctx* ctx) {
   if (!ctx) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded");
+  if (ctx->cfg.flags & EMSESG_FLAG_FP32_ONLY)
+    return set_error(ctx, EMSESG_ERR_STATE, "FP32-only context: no FP64 particle records");
   // Sorted order of the last sort (tile-major cell order); particles that
   // died since then come out with nid = -1 in place, as the reference leaves
   // them before transbound.

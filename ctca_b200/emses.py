@@ -64,7 +64,7 @@ class Config(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
                 ("nspec", ctypes.c_int32), ("nfbnd", ctypes.c_int32 * 3),
                 ("npbnd", (ctypes.c_int32 * 3) * ISPEC), ("npc", ctypes.c_int32), ("line_mode", ctypes.c_int32),
-                ("rng_mode", ctypes.c_int32), ("sort_tile", ctypes.c_int32 * 3), ("reserved_", ctypes.c_int32),
+                ("rng_mode", ctypes.c_int32), ("sort_tile", ctypes.c_int32 * 3), ("flags", ctypes.c_int32),
                 ("rng_seed", ctypes.c_uint64), ("q", ctypes.c_double * ISPEC), ("qm", ctypes.c_double * ISPEC),
                 ("rm", ctypes.c_double * ISPEC), ("e0", ctypes.c_double * 3), ("b0", ctypes.c_double * 3),
                 ("body", Body * INPC), ("capacity", ctypes.c_int64 * ISPEC)]
@@ -139,6 +139,7 @@ _SIGS = {
     "emsesg_fx_surface": (_I, [_P, _P, ctypes.POINTER(ctypes.c_int64)]),
     "emsesg_fx_adjoint": (_I, [_P, _I, _I, _I, _I, _P, _P, ctypes.POINTER(ctypes.c_double), _P, _P, _P, _P]),
     "emsesg_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
+    "emsesg_fx_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
     "emsesg_set_profiling": (_I, [_P, _I]),
     "emsesg_profile_report": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     "emsesg_profile_reset": (_I, [_P]),
@@ -401,6 +402,10 @@ class Emses:
 
     def load_plasma(self, pl: Plasma):
         self._check(self.lib.emsesg_load_plasma(self.h, ctypes.byref(pl)))
+
+    def fx_load_plasma(self, pl: Plasma):
+        """The plasma of load_plasma straight into the FP32 form (no FP64 records)."""
+        self._check(self.lib.emsesg_fx_load_plasma(self.h, ctypes.byref(pl)))
 
     def set_profiling(self, on: bool):
         self._check(self.lib.emsesg_set_profiling(self.h, 1 if on else 0))

@@ -74,7 +74,7 @@ def emit_rectangle(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int
     ud = 1.0 if nemd > 0 else -1.0
     npr = vnormf.size
     u = rng.random((n, 6))
-    out = np.zeros(2 * n, dtype=PARTICLE_DTYPE)
+    out = np.zeros(2 * n, dtype=PARTICLE_DTYPE)  # pid = nid = 0
     coords = [("x", "vx"), ("y", "vy"), ("z", "vz")]
     a0 = (npr * u[:, 0]).astype(np.int64)
     a1 = (npr * u[:, 1]).astype(np.int64)
@@ -85,18 +85,16 @@ def emit_rectangle(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int
     rn = np.full(n, grd)
     rt1 = bounds1[0] + (bounds1[1] - bounds1[0]) * u[:, 4]
     rt2 = bounds2[0] + (bounds2[1] - bounds2[0]) * u[:, 5]
+    # whole-field writes of the interleaved pairs (anti-particle, twin)
     for val_r, val_v, ax in ((rn, vn, axis[0]), (rt1, vt1, axis[1]), (rt2, vt2, axis[2])):
         c, v = coords[ax]
-        out[c][0::2] = val_r
-        out[c][1::2] = val_r
-        out[v][0::2] = val_v
-        out[v][1::2] = val_v
-    out[coords[axis[0]][0]][1::2] += ud * 1e-5
-    out["preside"][0::2] = PCL_ANTI
-    out["preside"][1::2] = PCL_INJECTED
+        r2 = np.repeat(val_r, 2)
+        if ax == axis[0]:
+            r2[1::2] += ud * 1e-5
+        out[c] = r2
+        out[v] = np.repeat(val_v, 2)
+    out["preside"] = np.tile(np.array([PCL_ANTI, PCL_INJECTED], dtype=np.int32), n)
     out["spec"] = spec
-    out["pid"] = 0
-    out["nid"] = 0
     return out
 
 

@@ -92,6 +92,19 @@ def baseline_case(idx: int, scale: float = 1.0) -> Case:
                              Species(ppc, 1.0 / 1836.0, 0.05 / math.sqrt(1836.0), drift=(0.01, 0.0, 0.0))],
                     b0=(0.0, 0.0, 0.1), e_modes=8, e_amp=1e-3, b_modes=8, b_amp=1e-3,
                     kmax=4 * 2 * math.pi / n, seed=1002, sort_tile=(8, 8, 8))
+    if idx == 3:
+        # the body workload: solar wind along -z past a conducting box
+        nx, ny, nz = (max(16, int(round(256 * scale))), max(16, int(round(256 * scale))),
+                      max(32, int(round(512 * scale))))
+        c = Case(n=(nx, ny, nz),
+                 species=[Species(24, -1.0, 0.05, drift=(0.0, 0.0, -0.08), npbnd=(0, 0, 2)),
+                          Species(24, 1.0 / 100.0, 0.005, drift=(0.0, 0.0, -0.08), npbnd=(0, 0, 2))],
+                 b0=(0.05, 0.0, 0.1), nfbnd=(0, 0, 1), seed=1003, sort_tile=(8, 8, 8))
+        bx, by, bz = max(2, int(round(32 * scale))), max(2, int(round(32 * scale))), max(2, int(round(16 * scale)))
+        x0, y0, z0 = (nx - bx) // 2, (ny - by) // 2, (nz - bz) // 2
+        c.bodies = [dict(geotype=0, ncond=1, xlpc=float(x0), xupc=float(x0 + bx), ylpc=float(y0),
+                         yupc=float(y0 + by), zlpc=float(z0), zupc=float(z0 + bz), sqdscaled=1.0)]
+        return c
     if idx == 4:
         # the adjoint workload: 64^3, the plasma of case 1 at 32 ppc
         c = baseline_case(1)

@@ -140,7 +140,7 @@ typedef struct emsesg_config {
   int32_t line_mode;                /* 1 disables the body test */
   int32_t rng_mode;                 /* 0 counter hash, 1 pre-drawn uniforms */
   int32_t sort_tile[3];             /* cell tile of the sort key (0: whole grid) */
-  int32_t reserved_;
+  int32_t flags;                    /* EMSESG_FLAG_* (0: none) */
   uint64_t rng_seed;                /* seed of the counter hash */
   double q[EMSESG_ISPEC];           /* charge per macro-particle */
   double qm[EMSESG_ISPEC];          /* charge-to-mass ratio */
@@ -149,6 +149,14 @@ typedef struct emsesg_config {
   emsesg_body body[EMSESG_INPC];
   int64_t capacity[EMSESG_ISPEC];   /* device particle capacity per species */
 } emsesg_config;
+
+/* Config flags.  EMSESG_FLAG_FP32_ONLY: the context keeps no FP64 particle
+ * buffer (64 bytes a particle); particles live in the FP32 form only, loaded
+ * by emsesg_fx_load_plasma and added by emsesg_fx_inject, so that runs of
+ * some 1.6e9 particles fit one GPU.  The calls that move FP64 particle
+ * records (emsesg_upload/download_particles, emsesg_load_plasma,
+ * emsesg_fx_load, emsesg_fx_store) then return EMSESG_ERR_STATE. */
+#define EMSESG_FLAG_FP32_ONLY 1
 
 typedef struct emsesg_ctx emsesg_ctx;
 
@@ -323,6 +331,10 @@ typedef struct emsesg_plasma {
 /* Fills the FP64 pbuf mirror: ppc particles uniform in every cell,
  * Maxwellian velocities (Box-Muller on a SplitMix64 counter hash). */
 int emsesg_load_plasma(emsesg_ctx* ctx, const emsesg_plasma* pl);
+/* The same plasma (the same draws, particle for particle) straight into the
+ * FP32 form, tile-sorted, without the FP64 records: emsesg_load_plasma then
+ * emsesg_fx_load give the same state.  Works with EMSESG_FLAG_FP32_ONLY. */
+int emsesg_fx_load_plasma(emsesg_ctx* ctx, const emsesg_plasma* pl);
 
 /* ---- profiling ----------------------------------------------------------- */
 /* When on, every kernel launch is bracketed by CUDA events on the context
