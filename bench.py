@@ -517,6 +517,8 @@ def run_body_line(args, world, rank, local):
     steps, warm = args.steps, args.warmup
     inj = body_injection(case, warm + steps + 5, scale, seed=case.seed + 17 * rank)
     add = [sum(int(st[i].size) for st in inj) for i in range(2)]
+    # the step's records come from pinned host memory (asynchronous uploads)
+    pinned = [[torch.from_numpy(r.view(np.uint8)).pin_memory() for r in st] for st in inj]
     ncell = case.n[0] * case.n[1] * case.n[2]
     cap = [int(s.ppc * ncell * 1.01) + add[i] + (1 << 20) for i, s in enumerate(case.species)]
     cfg = inputs.make_config(case, capacity=cap)
@@ -530,7 +532,7 @@ def run_body_line(args, world, rank, local):
         recs = inj[k[0]]
         for isp in range(2):
             if recs[isp].size:
-                g.fx_inject(isp + 1, recs[isp])
+                g.fx_inject_raw(isp + 1, pinned[k[0]][isp].data_ptr(), recs[isp].size)
         g.fx_step(2, k[0] % SORT_EVERY == SORT_EVERY - 1)
         k[0] += 1
 

@@ -74,6 +74,7 @@ struct FxState {
   int64_t* slots_d = nullptr;       // device slot counts per species (padded regions)
   int64_t* tile_start = nullptr;    // [nspec][ntiles+1] sorted ranks of each tile's first particle
   int64_t* tile_pad = nullptr;      // [nspec][ntiles+1] first slot of each tile's padded region
+  int64_t* chunk_start = nullptr;   // [nspec][ntiles+1] first push CTA of each tile
   int64_t base[EMSESG_ISPEC] = {};  // species region offsets in pos / vx / vy / vz
   int64_t cap[EMSESG_ISPEC] = {};   // species region sizes (capacity + tile padding)
   bool tiled = false;               // regions hold the thread-major layout of a sort
@@ -82,7 +83,7 @@ struct FxState {
   int64_t* tile_pad2 = nullptr;
   uint32_t* lcs_cnt = nullptr;      // [nspec][ntiles][nbc]
   uint32_t* lcs_base = nullptr;     // [nspec][ntiles][nbc]
-  uint16_t* lcs_wcnt = nullptr;     // [nspec][ntiles][warps][nbc]
+  uint32_t* lcs_wcnt = nullptr;     // [ntiles][warps][nbc] of the species being sorted
   uint32_t* lcs_celltot = nullptr;  // [ntiles][tile cells]
   int64_t* lcs_tiletot = nullptr;   // [ntiles]
   int* lcs_stray = nullptr;         // [nspec]
@@ -101,6 +102,9 @@ struct FxState {
   emsesg_particle* stage = nullptr;    // device staging of injected records
   int32_t* stage_ord = nullptr;
   int64_t stage_cap = 0;
+  int32_t* ord_host = nullptr;         // pinned host staging of the ordinals
+  int64_t ord_host_cap = 0;
+  cudaEvent_t ord_ev = nullptr;        // the last upload from ord_host
   // CUDA graph of a block of steps (emsesg_fx_run)
   bool capture = false;                // inside a stream capture: no host syncs
   cudaGraphExec_t gexec = nullptr;

@@ -445,6 +445,7 @@ int fx_alloc(emsesg_ctx* ctx) {
   EMSESG_CUDA(ctx, cudaMalloc(&f.slots_d, EMSESG_ISPEC * sizeof(int64_t)));
   EMSESG_CUDA(ctx, cudaMalloc(&f.tile_start, (int64_t)c.nspec * (f.ntiles + 1) * sizeof(int64_t)));
   EMSESG_CUDA(ctx, cudaMalloc(&f.tile_pad, (int64_t)c.nspec * (f.ntiles + 1) * sizeof(int64_t)));
+  EMSESG_CUDA(ctx, cudaMalloc(&f.chunk_start, (int64_t)c.nspec * (f.ntiles + 1) * sizeof(int64_t)));
   FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
   EMSESG_CUDA(ctx, cudaMalloc(&f.accum, (fr.size() + fj.size()) * sizeof(int64_t)));
   int64_t nn = (int64_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
@@ -459,7 +460,7 @@ int fx_alloc(emsesg_ctx* ctx) {
     EMSESG_CUDA(ctx, cudaMalloc(&f.tile_pad2, ns * (f.ntiles + 1) * sizeof(int64_t)));
     EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_cnt, ns * f.ntiles * nbc * sizeof(uint32_t)));
     EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_base, ns * f.ntiles * nbc * sizeof(uint32_t)));
-    EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_wcnt, ns * f.ntiles * PUSH_WARPS * nbc * sizeof(uint16_t)));
+    EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_wcnt, f.ntiles * PUSH_WARPS * nbc * sizeof(uint32_t)));  // one species
     EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_celltot, f.ntiles * tcells * sizeof(uint32_t)));
     EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_tiletot, f.ntiles * sizeof(int64_t)));
     EMSESG_CUDA(ctx, cudaMalloc(&f.lcs_stray, EMSESG_ISPEC * sizeof(int)));
@@ -485,10 +486,13 @@ void fx_free(emsesg_ctx* ctx) {
   cudaFree(f.pos); cudaFree(f.vx); cudaFree(f.vy); cudaFree(f.vz);
   cudaFree(f.pos2); cudaFree(f.vx2); cudaFree(f.vy2); cudaFree(f.vz2);
   cudaFree(f.count_d); cudaFree(f.slots_d); cudaFree(f.tile_start); cudaFree(f.tile_pad); cudaFree(f.accum);
+  cudaFree(f.chunk_start);
   cudaFree(f.fnode); cudaFree(f.fnode2);
   cudaFree(f.tile_start2); cudaFree(f.tile_pad2); cudaFree(f.lcs_cnt); cudaFree(f.lcs_base); cudaFree(f.lcs_wcnt);
   cudaFree(f.lcs_celltot); cudaFree(f.lcs_tiletot); cudaFree(f.lcs_stray); cudaFree(f.lcs_inv);
   cudaFree(f.surf); cudaFree(f.tailord); cudaFree(f.stage); cudaFree(f.stage_ord);
+  cudaFreeHost(f.ord_host);
+  if (f.ord_ev) cudaEventDestroy(f.ord_ev);
   if (f.gexec) cudaGraphExecDestroy(f.gexec);
   adj_free(f);
   f = FxState();
@@ -532,25 +536,20 @@ int fx_local_sort(emsesg_ctx* ctx, bool* done) {
   const int64_t nbc = G[0].nbc;
   const int lsm = (int)(PUSH_WARPS * nbc * sizeof(uint32_t));
   const int64_t T1 = f.ntiles + 1;
+  // injected particles of the tail zones: sorted alone by cell key
+  const uint32_t tcells = (uint32_t)(f.tile[0] * f.tile[1] * f.tile[2]);
+  const uint32_t deadkey = (uint32_t)(f.ntiles * tcells);
+  int kbits = 1;
+  while (kbits < 32 && (1ULL << kbits) <= deadkey) kbits++;
+  {
+    int64_t most = 0;
+    for (int is = 0; is < c.nspec; is++) most = std::max(most, f.ntail[is]);
+    if (most > 0) {
+      int rc = ensure_sort_scratch(ctx, most);
+      if (rc) return rc;
+    }
+  }
   EMSESG_CUDA(ctx, cudaMemsetAsync(f.lcs_stray, 0, EMSESG_ISPEC * sizeof(int), ctx->stream));
-  for (int is = 0; is < c.nspec; is++) {
-    if (ctx->totalp[is] == 0) continue;
-    EMSESG_LAUNCH(ctx, "lcs_count", k_lcs_count, (unsigned)f.ntiles, PUSH_THREADS, lsm, f.pos + f.base[is],
-                  f.tile_start + is * T1, f.tile_pad + is * T1, g, G[is],
-                  f.lcs_wcnt + is * f.ntiles * PUSH_WARPS * nbc, f.lcs_cnt + is * f.ntiles * nbc, f.lcs_stray + is);
-  }
-  // Outside a stream capture the host reads the stray flags and falls back
-  // to the radix sort.  Inside one (emsesg_fx_run's graph) it cannot: the
-  // sort kernels of a species with a stray then return at once and
-  // k_lcs_keep carries its current order over to the new buffers.
-  if (!f.capture) {
-    int stray[EMSESG_ISPEC] = {0};
-    EMSESG_CUDA(ctx, cudaMemcpyAsync(stray, f.lcs_stray, EMSESG_ISPEC * sizeof(int), cudaMemcpyDeviceToHost,
-                                     ctx->stream));
-    EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    for (int is = 0; is < c.nspec; is++)
-      if (stray[is]) return EMSESG_OK;
-  }
   for (int is = 0; is < c.nspec; is++) {
     int64_t* ts2 = f.tile_start2 + is * T1;
     int64_t* tp2 = f.tile_pad2 + is * T1;
@@ -565,15 +564,44 @@ int fx_local_sort(emsesg_ctx* ctx, bool* done) {
     uint32_t* cnt = f.lcs_cnt + is * f.ntiles * nbc;
     uint32_t* bas = f.lcs_base + is * f.ntiles * nbc;
     const int* stray = f.lcs_stray + is;
+    // per-warp counts (one species at a time)
+    EMSESG_LAUNCH(ctx, "lcs_count", k_lcs_count, (unsigned)f.ntiles, PUSH_THREADS, lsm, f.pos + off,
+                  f.tile_start + is * T1, f.tile_pad + is * T1, g, G[is], f.lcs_wcnt, cnt, f.lcs_stray + is);
+    // Outside a stream capture the host reads the stray flag and falls back
+    // to the radix sort (which redoes every species).  Inside one
+    // (emsesg_fx_run's graph) it cannot: the sort kernels of a species with
+    // a stray then return at once and k_lcs_keep carries its current order
+    // over to the new buffers.
+    if (!f.capture) {
+      int st = 0;
+      EMSESG_CUDA(ctx, cudaMemcpyAsync(&st, f.lcs_stray + is, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+      EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      if (st) return EMSESG_OK;
+    }
+    // the species' tail zone, sorted by cell key
+    const int64_t nt = f.ntail[is];
+    uint32_t *tk = nullptr, *tv = nullptr;
+    if (nt > 0) {
+      EMSESG_LAUNCH(ctx, "lcs_tail_keys", k_fx_keys, nblk(nt), 256, 0, f.pos + off, (int64_t)0, f.slots_d + is,
+                    f.tail0[is], nt, g, deadkey, ctx->sort.keys[0], ctx->sort.vals[0]);
+      int rc = sort_pairs(ctx, ctx->sort.keys[0], ctx->sort.vals[0], nt, kbits, &tk, &tv);
+      if (rc) return rc;
+    }
     EMSESG_LAUNCH(ctx, "lcs_celltot", k_lcs_celltot, (unsigned)f.ntiles, CELL_THREADS, 0, cnt, g, G[is],
                   f.lcs_celltot, f.lcs_tiletot, stray);
+    if (nt > 0)
+      EMSESG_LAUNCH(ctx, "lcs_tail_count", k_lcs_tail_count, nblk(nt), 256, 0, tk, nt, deadkey, (int)tcells,
+                    f.lcs_celltot, (unsigned long long*)f.lcs_tiletot, stray);
     EMSESG_LAUNCH(ctx, "lcs_tiles", k_lcs_tiles, 1, 1024, 0, f.lcs_tiletot, f.ntiles, ts2, tp2, f.count_d + is,
                   f.slots_d + is, stray);
     EMSESG_LAUNCH(ctx, "lcs_bases", k_lcs_bases, (unsigned)f.ntiles, CELL_THREADS, 0, cnt, f.lcs_celltot, g, G[is],
                   ts2, tp2, bas, f.lcs_inv + off, stray);
     EMSESG_LAUNCH(ctx, "lcs_rank", k_lcs_rank, (unsigned)f.ntiles, PUSH_THREADS, lsm, f.pos + off,
-                  f.tile_start + is * T1, f.tile_pad + is * T1, g, G[is], f.lcs_wcnt + is * f.ntiles * PUSH_WARPS * nbc,
+                  f.tile_start + is * T1, f.tile_pad + is * T1, g, G[is], f.lcs_wcnt,
                   bas, ts2, tp2, f.lcs_inv + off, ctx->d_status, ctx->d_diag, stray);
+    if (nt > 0)
+      EMSESG_LAUNCH(ctx, "lcs_tail_inv", k_lcs_tail_inv, nblk(nt), 256, 0, tk, tv, nt, deadkey, (int)tcells,
+                    f.lcs_celltot, ts2, tp2, f.lcs_inv + off, stray);
     EMSESG_LAUNCH(ctx, "lcs_move", k_lcs_move, (unsigned)f.ntiles, PUSH_THREADS, move_smem(), f.pos + off,
                   f.vx + off, f.vy + off, f.vz + off, f.tile_start + is * T1, f.tile_pad + is * T1, ts2, tp2,
                   f.lcs_inv + off, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off, stray);
@@ -588,6 +616,7 @@ int fx_local_sort(emsesg_ctx* ctx, bool* done) {
   std::swap(f.vz, f.vz2);
   std::swap(f.tile_start, f.tile_start2);
   std::swap(f.tile_pad, f.tile_pad2);
+  for (int is = 0; is < c.nspec; is++) f.ntail[is] = 0;  // merged into the regions
   *done = true;
   return EMSESG_OK;
 }
@@ -596,12 +625,9 @@ extern "C" int emsesg_fx_sort(emsesg_ctx* ctx) {
   if (!ctx) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
   FxState& f = ctx->fx;
-  bool tail = false;
-  for (int is = 0; is < ctx->cfg.nspec; is++) {
+  for (int is = 0; is < ctx->cfg.nspec; is++)
     if (f.pending[is]) return set_error(ctx, EMSESG_ERR_STATE, "injected particles are sorted before their first push");
-    tail = tail || f.ntail[is] > 0;
-  }
-  if (f.tiled && !tail) {
+  if (f.tiled) {
     bool done = false;
     int lrc = fx_local_sort(ctx, &done);
     if (lrc) return lrc;
@@ -842,6 +868,7 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   a.pos = f.pos; a.vx = f.vx; a.vy = f.vy; a.vz = f.vz;
   a.tile_start = f.tile_start;
   a.tile_pad = f.tile_pad;
+  a.chunk_start = f.chunk_start;
   a.ntiles = f.ntiles;
   double gustep = ustep;
   a.gustep = (float)gustep;
@@ -862,7 +889,11 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   a.bd = make_bodies(c);
   a.status = ctx->d_status;
   a.diag = ctx->d_diag;
-  dim3 grid((unsigned)f.ntiles, (unsigned)c.nspec);
+  // row chunks of the tile regions: at most ntiles + rows / CHUNK_ROWS
+  int64_t rows = 0;
+  for (int is = 0; is < c.nspec; is++) rows = std::max(rows, (f.cap[is] + PUSH_THREADS - 1) / PUSH_THREADS);
+  EMSESG_LAUNCH(ctx, "fx_chunks", k_push_chunks, (unsigned)c.nspec, 1024, 0, f.tile_start, f.ntiles, f.chunk_start);
+  dim3 grid((unsigned)(f.ntiles + rows / CHUNK_ROWS + 1), (unsigned)c.nspec);
   if (!deposit) {
     for (int is = 0; is < c.nspec; is++)
       if (f.ntail[is]) return set_error(ctx, EMSESG_ERR_STATE, "move-only step with injected particles");
@@ -929,13 +960,26 @@ extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle
     EMSESG_CUDA(ctx, cudaMalloc(&f.stage_ord, n * sizeof(int32_t)));
     f.stage_cap = n;
   }
-  // ordinal of each injected particle's random step, in buffer order
-  std::vector<int32_t> ord((size_t)n, 0);
+  // ordinal of each injected particle's random step, in buffer order, staged
+  // in pinned host memory that the previous call's upload has released
+  if (!f.ord_ev) EMSESG_CUDA(ctx, cudaEventCreateWithFlags(&f.ord_ev, cudaEventDisableTiming));
+  EMSESG_CUDA(ctx, cudaEventSynchronize(f.ord_ev));
+  if (n > f.ord_host_cap) {
+    cudaFreeHost(f.ord_host);
+    f.ord_host = nullptr;
+    f.ord_host_cap = 0;
+    EMSESG_CUDA(ctx, cudaHostAlloc((void**)&f.ord_host, n * sizeof(int32_t), cudaHostAllocDefault));
+    f.ord_host_cap = n;
+  }
+  int32_t* ord = f.ord_host;
   int64_t k1 = f.pending[is];
   for (int64_t k = 0; k < n; k++)
-    if (host[k].preside == EMSESG_PCL_INJECTED && host[k].nid != -1) ord[(size_t)k] = (int32_t)(++k1);
+    ord[k] = (host[k].preside == EMSESG_PCL_INJECTED && host[k].nid != -1) ? (int32_t)(++k1) : 0;
+  // records from pinned host memory go asynchronously; from pageable memory
+  // the copy returns once the records are staged
   EMSESG_CUDA(ctx, cudaMemcpyAsync(f.stage, host, n * sizeof(emsesg_particle), cudaMemcpyHostToDevice, ctx->stream));
-  EMSESG_CUDA(ctx, cudaMemcpyAsync(f.stage_ord, ord.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(f.stage_ord, ord, n * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+  EMSESG_CUDA(ctx, cudaEventRecord(f.ord_ev, ctx->stream));
   const int64_t off = f.base[is], slot0 = f.tail0[is] + f.ntail[is];
   Bodies bd = make_bodies(ctx->cfg);
   EMSESG_LAUNCH(ctx, "fx_inject", k_fx_inject, nblk(n), 256, 0, f.stage, f.stage_ord, n, make_geo(ctx), bd, slot0,
@@ -944,8 +988,7 @@ extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle
   f.ntail[is] += n;
   f.pending[is] = k1;
   ctx->totalp[is] += n;
-  // the host copy of ord must outlive the asynchronous upload
-  return emsesg_synchronize(ctx);
+  return EMSESG_OK;
 }
 
 extern "C" int emsesg_fx_surface(emsesg_ctx* ctx, int64_t* counts, int64_t* nsurf) {

@@ -47,6 +47,7 @@ constexpr int RQ_DRAIN = 8;     // drain the run queue at this many entries
 constexpr int RQCAP = RQ_DRAIN + 32;
 constexpr int XQW = 8;          // general-path entry: slot, cell, 3 offsets, 3 velocities
 constexpr int XLCAP = 512;      // per-warp list of cross slots
+constexpr int CHUNK_ROWS = 256;  // rows of a tile region per CTA (crowded tiles take several)
 constexpr uint32_t ROW_BYTES = PUSH_THREADS * (16 + 3 * 4);
 static_assert(PUSH_THREADS == EMSESG_FX_ROW_SLOTS, "row width of the thread-major layout");
 static_assert(ROW_BYTES % 16 == 0 && (PUSH_THREADS * 4) % 16 == 0, "bulk copies move whole 16-byte units");
@@ -70,6 +71,7 @@ struct FxPushArgs {
   float* vz;
   const int64_t* tile_start;    // [nspec][ntiles+1] sorted ranks (live particles)
   const int64_t* tile_pad;      // [nspec][ntiles+1] slot offsets of the padded regions
+  const int64_t* chunk_start;   // [nspec][ntiles+1] first CTA (row chunk) of each tile
   int64_t off[EMSESG_ISPEC];    // region base per species
   int npbnd[EMSESG_ISPEC][3];
   float qmp[EMSESG_ISPEC], qfix[EMSESG_ISPEC];
@@ -615,16 +617,30 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   __shared__ int rows_seen;
   const Geo& g = a.g;
   const int is = blockIdx.y;
-  const int t = blockIdx.x;
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const unsigned lt = (1u << lane) - 1u;
 
+  // this CTA's chunk: tile t, rows r0 .. r0 + L - 1 of its region (a tile of
+  // more than CHUNK_ROWS rows is pushed by several CTAs, which add their
+  // sums into the same global arrays)
   const int64_t* ts = a.tile_start + (int64_t)is * (a.ntiles + 1);
+  const int64_t* cs = a.chunk_start + (int64_t)is * (a.ntiles + 1);
+  const int64_t b = blockIdx.x;
+  if (b >= cs[a.ntiles]) return;
+  int64_t tlo = 0, thi = a.ntiles;  // the last tile with cs[t] <= b
+  while (thi - tlo > 1) {
+    const int64_t mid = (tlo + thi) >> 1;
+    if (cs[mid] <= b) tlo = mid;
+    else thi = mid;
+  }
+  const int t = (int)tlo;
   const int64_t n = ts[t + 1] - ts[t];
   if (n <= 0) return;
-  const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
-  const int64_t slot0 = a.off[is] + a.tile_pad[(int64_t)is * (a.ntiles + 1) + t];
+  const int r0 = (int)(b - cs[t]) * CHUNK_ROWS;
+  const int L = min((int)((n + PUSH_THREADS - 1) / PUSH_THREADS) - r0, CHUNK_ROWS);
+  if (L <= 0) return;
+  const int64_t slot0 = a.off[is] + a.tile_pad[(int64_t)is * (a.ntiles + 1) + t] + (int64_t)r0 * PUSH_THREADS;
 
   int tx = t % g.nt[0], ty = (t / g.nt[0]) % g.nt[1], tz = t / (g.nt[0] * g.nt[1]);
   const int o[3] = {tx * g.t[0] - PG, ty * g.t[1] - PG, tz * g.t[2] - PG};
@@ -904,6 +920,38 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       }
     }
   }
+}
+
+// The row chunks of every tile region: cs[t] = first chunk of tile t,
+// cs[ntiles] = the number of chunks (one block of 1024 threads per species).
+__global__ void __launch_bounds__(1024) k_push_chunks(const int64_t* __restrict__ tile_start, int64_t ntiles,
+                                                      int64_t* chunk_start) {
+  __shared__ int64_t pa[1024];
+  const int64_t* ts = tile_start + (int64_t)blockIdx.x * (ntiles + 1);
+  int64_t* cs = chunk_start + (int64_t)blockIdx.x * (ntiles + 1);
+  const int tid = threadIdx.x;
+  const int64_t per = (ntiles + 1023) / 1024;
+  const int64_t t0 = tid * per, t1 = min(ntiles, t0 + per);
+  auto chunks = [&](int64_t t) {
+    const int64_t rows = (ts[t + 1] - ts[t] + PUSH_THREADS - 1) / PUSH_THREADS;
+    return (rows + CHUNK_ROWS - 1) / CHUNK_ROWS;
+  };
+  int64_t sa = 0;
+  for (int64_t t = t0; t < t1; t++) sa += chunks(t);
+  pa[tid] = sa;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    const int64_t v = tid >= d ? pa[tid - d] : 0;
+    __syncthreads();
+    pa[tid] += v;
+    __syncthreads();
+  }
+  int64_t ra = pa[tid] - sa;
+  for (int64_t t = t0; t < t1; t++) {
+    cs[t] = ra;
+    ra += chunks(t);
+  }
+  if (tid == 1023) cs[ntiles] = pa[1023];
 }
 
 // Injected particles of the tail zone of species `is`, one thread each: the

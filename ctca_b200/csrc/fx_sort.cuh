@@ -26,13 +26,19 @@
 //           particles from other tiles, from global memory (coalesced
 //           writes).
 //
+// Injected particles waiting in the tail zone join the same sort: the tail
+// alone is radix-sorted by the tile-major cell key (a few million keys), its
+// particles are added to the per-cell totals, and they take the last ranks
+// of their cell, in the tail's sorted order (cell range end - (upper bound
+// of the key - index)); the move then fetches them like particles of
+// another tile.
+//
 // The order of equal-cell particles is thus (source tile, warp, row, lane):
 // fixed by the data, so the sort is deterministic, and a particle is read
 // twice (16 bytes to count and rank, 28 to move) and written once (28
-// bytes), plus 4-byte slot indices.  Dead
-// particles and empty slots are dropped (the compaction).  A particle outside
-// its tile's sort box, or more than 65535 particles of one cell in one warp,
-// sets the stray flag; the host then sorts with the radix path instead.
+// bytes), plus 4-byte slot indices.  Dead particles and empty slots are
+// dropped (the compaction).  A particle outside its tile's sort box sets the
+// stray flag; the host then sorts with the radix path instead.
 
 struct LcsGeo {
   int n[3];      // grid cells
@@ -98,7 +104,7 @@ __device__ __forceinline__ void tile_xyz(const Geo& g, int64_t t, int& tx, int& 
 __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_count(const float4* __restrict__ pos,
                                                             const int64_t* __restrict__ ts,
                                                             const int64_t* __restrict__ tp, Geo g, LcsGeo G,
-                                                            uint16_t* __restrict__ wcnt, uint32_t* __restrict__ cnt,
+                                                            uint32_t* __restrict__ wcnt, uint32_t* __restrict__ cnt,
                                                             int* stray) {
   extern __shared__ uint32_t hist[];  // [PUSH_WARPS][nbc]
   const int t = blockIdx.x, tid = threadIdx.x, warp = tid >> 5;
@@ -121,14 +127,13 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_count(const float4* __rest
     atomicAdd(&hist[warp * G.nbc + bc], 1u);
   }
   __syncthreads();
-  uint16_t* wc = wcnt + (int64_t)t * PUSH_WARPS * G.nbc;
+  uint32_t* wc = wcnt + (int64_t)t * PUSH_WARPS * G.nbc;
   uint32_t* c = cnt + (int64_t)t * G.nbc;
   for (int b = tid; b < G.nbc; b += PUSH_THREADS) {
     uint32_t sum = 0;
     for (int w = 0; w < PUSH_WARPS; w++) {
       uint32_t h = hist[w * G.nbc + b];
-      if (h > 65535u) bad = true;
-      wc[w * G.nbc + b] = (uint16_t)h;
+      wc[w * G.nbc + b] = h;
       sum += h;
     }
     c[b] = sum;
@@ -220,7 +225,7 @@ __global__ void __launch_bounds__(1024) k_lcs_tiles(const int64_t* __restrict__ 
 // bases: first rank of every (source tile, box cell); DEAD in the empty
 // slots of the new region.  grid = ntiles (destination tiles), block = CELL_THREADS.
 __global__ void __launch_bounds__(CELL_THREADS) k_lcs_bases(const uint32_t* __restrict__ cnt,
-                                                            const uint32_t* __restrict__ celltot, Geo g, LcsGeo G,
+                                                            uint32_t* celltot, Geo g, LcsGeo G,
                                                             const int64_t* __restrict__ ts,
                                                             const int64_t* __restrict__ tp, uint32_t* __restrict__ base,
                                                             uint32_t* __restrict__ inv, const int* stray) {
@@ -257,6 +262,8 @@ __global__ void __launch_bounds__(CELL_THREADS) k_lcs_bases(const uint32_t* __re
             run += cnt[tt * G.nbc + bc];
           }
     }
+    // the cell's end rank (its tail particles take the ranks before it)
+    celltot[(int64_t)t * G.tcells + tid] = (uint32_t)ts[t] + sc[tid];
   }
   // empty slots of the new region
   const int64_t n = ts[t + 1] - ts[t];
@@ -275,7 +282,7 @@ __global__ void __launch_bounds__(CELL_THREADS) k_lcs_bases(const uint32_t* __re
 __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restrict__ pos,
                                                            const int64_t* __restrict__ ts,
                                                            const int64_t* __restrict__ tp, Geo g, LcsGeo G,
-                                                           const uint16_t* __restrict__ wcnt,
+                                                           const uint32_t* __restrict__ wcnt,
                                                            const uint32_t* __restrict__ base,
                                                            const int64_t* __restrict__ ts2,
                                                            const int64_t* __restrict__ tp2, uint32_t* __restrict__ inv,
@@ -284,7 +291,7 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restr
   if (*stray) return;
   const int t = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned lt = (1u << lane) - 1u;
-  const uint16_t* wc = wcnt + (int64_t)t * PUSH_WARPS * G.nbc;
+  const uint32_t* wc = wcnt + (int64_t)t * PUSH_WARPS * G.nbc;
   for (int b = tid; b < G.nbc; b += PUSH_THREADS) {
     uint32_t run = base[(int64_t)t * G.nbc + b];
     for (int w = 0; w < PUSH_WARPS; w++) {
@@ -445,4 +452,43 @@ __global__ void __launch_bounds__(256) k_lcs_keep(const int* stray, const float4
     vz2[i] = vz[i];
     inv[i] = __float_as_uint(pos[i].w) == DEAD ? DEAD : (uint32_t)i;
   }
+}
+
+// The tail's particles in the per-cell and per-tile totals.  keys: the
+// tail's sorted tile-major cell keys (deadkey for dead particles).
+__global__ void __launch_bounds__(256) k_lcs_tail_count(const uint32_t* __restrict__ keys, int64_t nt,
+                                                        uint32_t deadkey, int tcells, uint32_t* celltot,
+                                                        unsigned long long* tiletot, const int* stray) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nt || *stray) return;
+  const uint32_t key = keys[i];
+  if (key >= deadkey) return;
+  atomicAdd(&celltot[key], 1u);
+  atomicAdd(&tiletot[key / (uint32_t)tcells], 1ull);
+}
+
+// The new slot of every live tail particle: the last ranks of its cell, in
+// the tail's sorted order.  cellend: per (tile, cell) the end rank (from
+// k_lcs_bases); inv[new slot] = old (tail) slot.
+__global__ void __launch_bounds__(256) k_lcs_tail_inv(const uint32_t* __restrict__ keys,
+                                                      const uint32_t* __restrict__ vals, int64_t nt, uint32_t deadkey,
+                                                      int tcells, const uint32_t* __restrict__ cellend,
+                                                      const int64_t* __restrict__ ts, const int64_t* __restrict__ tp,
+                                                      uint32_t* inv, const int* stray) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nt || *stray) return;
+  const uint32_t key = keys[i];
+  if (key >= deadkey) return;
+  // upper bound of the key in the sorted tail
+  int64_t lo = i + 1, hi = nt;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (keys[mid] <= key) lo = mid + 1;
+    else hi = mid;
+  }
+  const int64_t t = key / (uint32_t)tcells;
+  const int64_t q = (int64_t)cellend[key] - (lo - i) - ts[t];  // rank inside the tile
+  const int64_t n = ts[t + 1] - ts[t];
+  const int64_t L = (n + PUSH_THREADS - 1) / PUSH_THREADS;
+  inv[tp[t] + (q % L) * PUSH_THREADS + q / L] = vals[i];
 }

@@ -375,6 +375,11 @@ class Emses:
         rec = np.ascontiguousarray(records, dtype=PARTICLE_DTYPE)
         self._check(self.lib.emsesg_fx_inject(self.h, spec, rec.ctypes.data if rec.size else None, rec.size))
 
+    def fx_inject_raw(self, spec: int, ptr: int, n: int):
+        """fx_inject from a host address of n records (pinned memory: the
+        upload is asynchronous; keep the records until the stream is past it)."""
+        self._check(self.lib.emsesg_fx_inject(self.h, spec, ptr if n else None, n))
+
     def fx_surface(self) -> np.ndarray:
         """Absorbed minus emitted particles per surface cell, [nspec, nsurf]."""
         n = ctypes.c_int64(0)

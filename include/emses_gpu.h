@@ -299,6 +299,9 @@ int emsesg_fx_download_accum(emsesg_ctx* ctx, int64_t* host);
  * psuper3.F90:203-206) removes one count from that face cell.  The next
  * sort merges the tail into the tile regions (sorting with particles still
  * waiting for their first push is an error). */
+/* Asynchronous: from pinned host memory the upload overlaps the GPU's work
+ * (keep the records unchanged until the stream has passed the call); from
+ * pageable memory the call returns once the records are copied. */
 int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int64_t n);
 /* Absorbed minus emitted particles per surface cell of the box bodies
  * (geotype 0/1, integer bounds), int64 [nspec][nsurf]: body by body, faces
