@@ -627,6 +627,43 @@ __global__ void k_rhoupd(double* rho, const double* __restrict__ aj, FieldDesc f
        aj[fa.at(JZ, i, j, k)] - aj[fa.at(JZ, i, j, k - 1)]) * 2.0;
 }
 
+// bfield, src/field/bfield.F90:37-53: B(i,j,k) for i,j,k in -1..n, from E
+// (the reference's statement order; B written, E read only).
+__global__ void k_bfield(double* eb, FieldDesc f, int nx, int ny, int nz) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t ex = nx + 2, ey = ny + 2, ez = nz + 2;
+  if (t >= ex * ey * ez) return;
+  const int i = (int)(t % ex) - 1, j = (int)((t / ex) % ey) - 1, k = (int)(t / (ex * ey)) - 1;
+  eb[f.at(BX, i, j, k)] = eb[f.at(BX, i, j, k)] + eb[f.at(EY, i, j, k + 1)] - eb[f.at(EY, i, j, k)] -
+                          eb[f.at(EZ, i, j + 1, k)] + eb[f.at(EZ, i, j, k)];
+  eb[f.at(BY, i, j, k)] = eb[f.at(BY, i, j, k)] + eb[f.at(EZ, i + 1, j, k)] - eb[f.at(EZ, i, j, k)] -
+                          eb[f.at(EX, i, j, k + 1)] + eb[f.at(EX, i, j, k)];
+  eb[f.at(BZ, i, j, k)] = eb[f.at(BZ, i, j, k)] + eb[f.at(EX, i, j + 1, k)] - eb[f.at(EX, i, j, k)] -
+                          eb[f.at(EY, i + 1, j, k)] + eb[f.at(EY, i, j, k)];
+}
+
+// efield, src/field/efield.F90:54-70 (no lumped elements): E(i,j,k) for
+// i,j,k in 0..n, from B and J (E written, B and J read only).
+__global__ void k_efield(double* eb, const double* __restrict__ aj, FieldDesc f, FieldDesc fa, int nx, int ny,
+                         int nz, double tcs, double dlt) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t ex = nx + 1, ey = ny + 1, ez = nz + 1;
+  if (t >= ex * ey * ez) return;
+  const int i = (int)(t % ex), j = (int)((t / ex) % ey), k = (int)(t / (ex * ey));
+  eb[f.at(EX, i, j, k)] = eb[f.at(EX, i, j, k)] +
+                          tcs * (eb[f.at(BZ, i, j, k)] - eb[f.at(BZ, i, j - 1, k)] - eb[f.at(BY, i, j, k)] +
+                                 eb[f.at(BY, i, j, k - 1)]) -
+                          dlt * aj[fa.at(JX, i, j, k)];
+  eb[f.at(EY, i, j, k)] = eb[f.at(EY, i, j, k)] +
+                          tcs * (eb[f.at(BX, i, j, k)] - eb[f.at(BX, i, j, k - 1)] - eb[f.at(BZ, i, j, k)] +
+                                 eb[f.at(BZ, i - 1, j, k)]) -
+                          dlt * aj[fa.at(JY, i, j, k)];
+  eb[f.at(EZ, i, j, k)] = eb[f.at(EZ, i, j, k)] +
+                          tcs * (eb[f.at(BY, i, j, k)] - eb[f.at(BY, i - 1, j, k)] - eb[f.at(BX, i, j, k)] +
+                                 eb[f.at(BX, i, j - 1, k)]) -
+                          dlt * aj[fa.at(JZ, i, j, k)];
+}
+
 // Sum of v_d^2 of live particles (energy.F90:38-43); FP64 block partials.
 __global__ void k_energy(const emsesg_particle* __restrict__ p, int64_t n, const int64_t* count, double* out) {
   __shared__ double s[3][256];
@@ -975,6 +1012,32 @@ extern "C" int emsesg_rhoupd(emsesg_ctx* ctx, int ps) {
                 ctx->field[EMSESG_FIELD_AJ], field_desc(c, EMSESG_FIELD_RHO), field_desc(c, EMSESG_FIELD_AJ), c.nx,
                 c.ny, c.nz);
   return EMSESG_OK;
+}
+
+extern "C" int emsesg_bfield(emsesg_ctx* ctx, int ps) {
+  int rc = check_ps(ctx, ps);
+  if (rc) return rc;
+  const emsesg_config& c = ctx->cfg;
+  const int64_t nn = (int64_t)(c.nx + 2) * (c.ny + 2) * (c.nz + 2);
+  EMSESG_LAUNCH(ctx, "bfield", k_bfield, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_EB],
+                field_desc(c, EMSESG_FIELD_EB), c.nx, c.ny, c.nz);
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_efield(emsesg_ctx* ctx, int ps, double tcs, double dlt) {
+  int rc = check_ps(ctx, ps);
+  if (rc) return rc;
+  const emsesg_config& c = ctx->cfg;
+  const int64_t nn = (int64_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
+  EMSESG_LAUNCH(ctx, "efield", k_efield, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_EB], ctx->field[EMSESG_FIELD_AJ],
+                field_desc(c, EMSESG_FIELD_EB), field_desc(c, EMSESG_FIELD_AJ), c.nx, c.ny, c.nz, tcs, dlt);
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_exchange_eb(emsesg_ctx* ctx) {
+  if (!ctx) return EMSESG_ERR_ARG;
+  const FieldDesc f = field_desc(ctx->cfg, EMSESG_FIELD_EB);
+  return run_slab_ops(ctx, ctx->field[EMSESG_FIELD_EB], f, fold_ops(ctx->cfg, 2, 6), "exchange_eb");
 }
 
 extern "C" int emsesg_energy(emsesg_ctx* ctx, double* engk) {

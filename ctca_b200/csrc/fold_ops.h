@@ -28,12 +28,14 @@ struct SlabOp {
 
 // kind 0: rho-type arrays (ctypes CRH, add_boundary_charge), ncomp components.
 // kind 1: aj / ajdg (ctypes CAJ / CJD, add_boundary_current{,2}), ncomp = 3*k.
+// kind 2: eb (ctypes CEB): the border exchange only, ncomp = 6.
 inline std::vector<SlabOp> fold_ops(const emsesg_config& c, int kind, int ncomp) {
   std::vector<SlabOp> ops;
   const int n[3] = {c.nx, c.ny, c.nz};
   // ctypes as (from, to, size) of the lower and upper sends (ohinit.F90:113-118)
   int fromL, toL, sizeL, fromU, toU, sizeU;
   if (kind == 0) { fromL = 0; toL = 1; sizeL = 1; fromU = 0; toU = -1; sizeU = 1; }
+  else if (kind == 2) { fromL = 0; toL = 0; sizeL = 2; fromU = -1; toU = -1; sizeU = 1; }
   else { fromL = -1; toL = 2; sizeL = 3; fromU = -1; toU = -4; sizeU = 3; }
   // Exchange: x, then y, then z; the other axes span exti (inner) or exto
   // (outer) ranges.
@@ -51,6 +53,7 @@ inline std::vector<SlabOp> fold_ops(const emsesg_config& c, int kind, int ncomp)
     o.src0 = n[d] + fromU; o.dst0 = toU; o.depth = sizeU;
     ops.push_back(o);
   }
+  if (kind == 2) return ops;
   const int sl = toU, su = toL, nl = sizeU, nu = sizeL;
   const int dl = sl + nl, du = su - nu;
   auto box = [&](int axis, int op, int dst0, int src0, int depth, int loa, int hia, int lob, int hib,

@@ -937,6 +937,21 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
 }
 }  // namespace
 
+extern "C" int emsesg_fx_em_step(emsesg_ctx* ctx, int ustep, int do_sort, double tcs) {
+  if (!ctx) return EMSESG_ERR_ARG;
+  const emsesg_config& c = ctx->cfg;
+  for (int d = 0; d < 3; d++)
+    if (c.nfbnd[d] != 0) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "field step: periodic fields only");
+  if (c.npc > 0 && c.line_mode != 1)
+    return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "field step: no body field corrections (bdyfld)");
+  int rc;
+  if ((rc = emsesg_bfield(ctx, 1))) return rc;  // b(n-1/2) -> b(n)
+  if ((rc = emsesg_fx_step(ctx, ustep, do_sort))) return rc;
+  if ((rc = emsesg_bfield(ctx, 1))) return rc;  // b(n) -> b(n+1/2)
+  if ((rc = emsesg_efield(ctx, 1, tcs, 2.0))) return rc;
+  return emsesg_exchange_eb(ctx);
+}
+
 extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int64_t n) {
   if (!ctx || n < 0 || (n > 0 && !host)) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");

@@ -122,6 +122,10 @@ _SIGS = {
     "emsesg_compact": (_I, [_P, _I, ctypes.POINTER(ctypes.c_int64)]),
     "emsesg_rhoupd": (_I, [_P, _I]),
     "emsesg_compact_noalloc": (_I, [_P, ctypes.c_int64, _P, _P, _P]),
+    "emsesg_bfield": (_I, [_P, _I]),
+    "emsesg_efield": (_I, [_P, _I, ctypes.c_double, ctypes.c_double]),
+    "emsesg_exchange_eb": (_I, [_P]),
+    "emsesg_fx_em_step": (_I, [_P, _I, _I, ctypes.c_double]),
     "emsesg_energy": (_I, [_P, ctypes.POINTER(ctypes.c_double)]),
     "emsesg_fx_load": (_I, [_P]),
     "emsesg_fx_store": (_I, [_P]),
@@ -334,6 +338,19 @@ class Emses:
 
     def rhoupd(self, ps: int = 1):
         self._check(self.lib.emsesg_rhoupd(self.h, ps))
+
+    def bfield(self, ps: int = 1):
+        self._check(self.lib.emsesg_bfield(self.h, ps))
+
+    def efield(self, ps: int, tcs: float, dlt: float = 2.0):
+        self._check(self.lib.emsesg_efield(self.h, ps, tcs, dlt))
+
+    def exchange_eb(self):
+        self._check(self.lib.emsesg_exchange_eb(self.h))
+
+    def fx_em_step(self, ustep: int, do_sort: bool, tcs: float):
+        """bfield, fx_step, bfield, efield, exchange_eb (the main loop's order)."""
+        self._check(self.lib.emsesg_fx_em_step(self.h, ustep, 1 if do_sort else 0, tcs))
 
     def energy(self) -> np.ndarray:
         e = (ctypes.c_double * (3 * ISPEC))()

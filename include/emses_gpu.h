@@ -226,6 +226,20 @@ int emsesg_rhoupd(emsesg_ctx* ctx, int ps);
 #define EMSESG_NOALLOC_MAX_PARTICLES (1 << 20)
 int emsesg_compact_noalloc(const emsesg_particle* d_in, int64_t n, emsesg_particle* d_out, int64_t* d_kept,
                            void* stream);
+/* The EM field step around the push (src/main/emses.F90:365-430, 536-540):
+ * bfield (src/field/bfield.F90:4) advances B by half a step from E;
+ * efield (src/field/efield.F90:4, no lumped elements) advances E from B and
+ * the reduced aj, E += tcs curl B - dlt J (tcs of inital.F90:78 /
+ * rescal.F90:132; dlt = 2, or 0 for test-particle runs); exchange_eb is
+ * oh3_exchange_borders(eb, CEB) on one rank.  FP64 on the eb mirror,
+ * bit-identical to the reference's statement order. */
+int emsesg_bfield(emsesg_ctx* ctx, int ps);
+int emsesg_efield(emsesg_ctx* ctx, int ps, double tcs, double dlt);
+int emsesg_exchange_eb(emsesg_ctx* ctx);
+/* One EM step of the FP32 form with the fields on the device (periodic
+ * fields, no bodies): bfield, emsesg_fx_step (push, J, rho), bfield,
+ * efield, exchange_eb -- the order of the reference's main loop. */
+int emsesg_fx_em_step(emsesg_ctx* ctx, int ustep, int do_sort, double tcs);
 /* engk[is*3 + d] = 0.5*rm(is)*sum(v_d^2)/(slx*sly*slz), FP64. */
 int emsesg_energy(emsesg_ctx* ctx, double* engk);
 

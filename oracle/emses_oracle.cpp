@@ -380,6 +380,44 @@ void orc_exchange_eb(const emsesg_config* c, double* eb) {
   exchange_single(c, fd_of(c, EMSESG_FIELD_EB), eb, CT_EB);
 }
 
+// bfield, src/field/bfield.F90:37-53 (statement order of the reference;
+// the loop writes B only and reads E only).
+void orc_bfield(const emsesg_config* c, double* eb) {
+  FD f = fd_of(c, EMSESG_FIELD_EB);
+  for (int k = -1; k <= c->nz; k++)
+    for (int j = -1; j <= c->ny; j++)
+      for (int i = -1; i <= c->nx; i++) {
+        eb[f.at(BX, i, j, k)] = eb[f.at(BX, i, j, k)] + eb[f.at(EY, i, j, k + 1)] - eb[f.at(EY, i, j, k)] -
+                                eb[f.at(EZ, i, j + 1, k)] + eb[f.at(EZ, i, j, k)];
+        eb[f.at(BY, i, j, k)] = eb[f.at(BY, i, j, k)] + eb[f.at(EZ, i + 1, j, k)] - eb[f.at(EZ, i, j, k)] -
+                                eb[f.at(EX, i, j, k + 1)] + eb[f.at(EX, i, j, k)];
+        eb[f.at(BZ, i, j, k)] = eb[f.at(BZ, i, j, k)] + eb[f.at(EX, i, j + 1, k)] - eb[f.at(EX, i, j, k)] -
+                                eb[f.at(EY, i + 1, j, k)] + eb[f.at(EY, i, j, k)];
+      }
+}
+
+// efield, src/field/efield.F90:54-70 (mode_dipole != 3: no lumped
+// elements; the loop writes E only and reads B and J).
+void orc_efield(const emsesg_config* c, double* eb, const double* aj, double tcs, double dlt) {
+  FD f = fd_of(c, EMSESG_FIELD_EB), fa = fd_of(c, EMSESG_FIELD_AJ);
+  for (int k = 0; k <= c->nz; k++)
+    for (int j = 0; j <= c->ny; j++)
+      for (int i = 0; i <= c->nx; i++) {
+        eb[f.at(EX, i, j, k)] = eb[f.at(EX, i, j, k)] +
+                                tcs * (eb[f.at(BZ, i, j, k)] - eb[f.at(BZ, i, j - 1, k)] - eb[f.at(BY, i, j, k)] +
+                                       eb[f.at(BY, i, j, k - 1)]) -
+                                dlt * aj[fa.at(JX, i, j, k)];
+        eb[f.at(EY, i, j, k)] = eb[f.at(EY, i, j, k)] +
+                                tcs * (eb[f.at(BX, i, j, k)] - eb[f.at(BX, i, j, k - 1)] - eb[f.at(BZ, i, j, k)] +
+                                       eb[f.at(BZ, i - 1, j, k)]) -
+                                dlt * aj[fa.at(JY, i, j, k)];
+        eb[f.at(EZ, i, j, k)] = eb[f.at(EZ, i, j, k)] +
+                                tcs * (eb[f.at(BY, i, j, k)] - eb[f.at(BY, i - 1, j, k)] - eb[f.at(BX, i, j, k)] +
+                                       eb[f.at(BX, i, j - 1, k)]) -
+                                dlt * aj[fa.at(JZ, i, j, k)];
+      }
+}
+
 // grdcrt main relocations, src/field/grdcrt.F90:156-169 (E) and :214-230 (B).
 // The hole (zurechole) and sfecrrct surface corrections are not part of the
 // path (off in every configuration).

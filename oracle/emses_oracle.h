@@ -33,6 +33,10 @@ int64_t orc_field_size(const emsesg_config* c, int field);
 
 /* Single-rank guard fill of eb (oh3_exchange_borders with CEB), periodic axes. */
 void orc_exchange_eb(const emsesg_config* c, double* eb);
+// bfield, src/field/bfield.F90:37-53: B += curl-E step (half time step).
+void orc_bfield(const emsesg_config* c, double* eb);
+// efield, src/field/efield.F90:54-70 (no lumped elements): E += tcs curl B - dlt J.
+void orc_efield(const emsesg_config* c, double* eb, const double* aj, double tcs, double dlt);
 
 void orc_grdcrt(const emsesg_config* c, const double* eb, double* wrk);
 

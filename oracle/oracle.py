@@ -48,6 +48,8 @@ def lib() -> ctypes.CDLL:
     sigs = {
         "orc_field_size": (ctypes.c_int64, [cfgp, ctypes.c_int]),
         "orc_exchange_eb": (None, [cfgp, _P]),
+        "orc_bfield": (None, [cfgp, _P]),
+        "orc_efield": (None, [cfgp, _P, _P, ctypes.c_double, ctypes.c_double]),
         "orc_grdcrt": (None, [cfgp, _P, _P]),
         "orc_psolve2": (ctypes.c_int, [cfgp, ctypes.c_int, _P, _P, i64p, _P, ctypes.c_int64, i64p, ctypes.c_uint64,
                                        ctypes.POINTER(Counter)]),
@@ -159,6 +161,15 @@ class Oracle:
                 a[s] = sub
         else:
             self.L.orc_reduce_rho(self._c(), a.ctypes.data, nc)
+
+    def bfield(self):
+        self.L.orc_bfield(self._c(), self.eb.ctypes.data)
+
+    def efield(self, tcs: float, dlt: float = 2.0):
+        self.L.orc_efield(self._c(), self.eb.ctypes.data, self.f["aj"].ctypes.data, tcs, dlt)
+
+    def exchange_eb(self):
+        self.L.orc_exchange_eb(self._c(), self.eb.ctypes.data)
 
     def reduce_aj(self):
         self.L.orc_reduce_aj(self._c(), self.f["aj"].ctypes.data)

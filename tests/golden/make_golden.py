@@ -13,6 +13,8 @@ these files use) runs them from the text of
     src/pcl2field/charge.F90     charge, add_boundary_charge
     src/field/rhoupd.F90         rhoupd
     src/pcl/positn.F90           positn
+    src/field/bfield.F90         bfield
+    src/field/efield.F90         efield
 
 with IEEE double arithmetic in source order (Python floats: no fused
 multiply-add, no reassociation), Fortran integer division and int()
@@ -59,7 +61,11 @@ from ctca_b200 import inputs  # noqa: E402
 from ctca_b200.emses import INPC, ISPEC, PARTICLE_DTYPE, Body, Config, field_shape  # noqa: E402
 
 SOURCES = ["src/field/grdcrt.F90", "src/pcl2field/psolve2.F90", "src/pcl2field/psolve1.F90",
-           "src/pcl2field/charge.F90", "src/field/rhoupd.F90", "src/pcl/positn.F90"]
+           "src/pcl2field/charge.F90", "src/field/rhoupd.F90", "src/pcl/positn.F90",
+           "src/field/bfield.F90", "src/field/efield.F90"]
+# tcs of efield (src/main/inital.F90:78, rescal.F90:132) for the field-step
+# fixtures: 2 (c dt)^2 in internal units with c dt / dx = 0.5
+TCS = 0.125
 
 # src/main/paramt.F90:44-48
 CEB, CAJ, CRH, CRD, CJD, CPH = 1, 2, 3, 4, 5, 6
@@ -416,6 +422,16 @@ def run_case(units, name, c, ustep, opts):
     # rhoupd with the reduced rho and aj
     it.call("rhoupd", [1])
     out["rhoupd_rho"] = f["rho"].copy()
+    # the field step around the push: bfield, efield with the reduced aj
+    # (no test particles: dlt = 2; no lumped elements), eb border exchange
+    g.update(juncan=0, nflag_testp=0, tcs=TCS, ngap=0, mode_dipole=0)
+    it.call("bfield", [1])
+    out["bfield_eb"] = f["eb"].copy()
+    it.call("efield", [1])
+    out["efield_eb"] = f["eb"].copy()
+    exchange(Field(f["eb"], -1), n, list(cfg.nfbnd), CTYPES[CEB])
+    out["exchange_eb"] = f["eb"].copy()
+    out["tcs"] = np.float64(TCS)
     print(f"{name}: {p0.size} particles, {time.time() - t0:.1f} s", flush=True)
     return out
 

@@ -1,7 +1,8 @@
 """The oracle against the golden fixtures of tests/golden/: outputs of the
 reference's own Fortran subroutines (grdcrt, psolve2, psolve1,
-add_boundary_current(2), charge, add_boundary_charge, rhoupd, positn), executed from
-their source text by tests/golden/make_golden.py on small seeded cases.
+add_boundary_current(2), charge, add_boundary_charge, rhoupd, positn,
+bfield, efield), executed from their source text by
+tests/golden/make_golden.py on small seeded cases.
 
 Every comparison is bit-for-bit: particles (all 64 bytes of each record),
 every field element, every counter, and the number of random numbers drawn.
@@ -105,3 +106,17 @@ def test_positn(path):
     for fld in d["pbuf0"].dtype.names:
         assert same(o.pbuf[fld], d["positn_pbuf"][fld]), (fld, first_diff(o.pbuf[fld], d["positn_pbuf"][fld]))
     check_counters(o, d, "positn_")
+
+
+@pytest.mark.parametrize("path", CASES, ids=lambda p: p.stem)
+def test_field_step(path):
+    """bfield, efield (with the reduced aj) and the eb border exchange."""
+    d, cfg = load(path)
+    o = oracle_for(d, cfg, d["pbuf0"])
+    o.bfield()
+    assert same(o.eb, d["bfield_eb"]), first_diff(o.eb, d["bfield_eb"])
+    o.f["aj"][...] = d["reduced_aj"]
+    o.efield(float(d["tcs"]))
+    assert same(o.eb, d["efield_eb"]), first_diff(o.eb, d["efield_eb"])
+    o.exchange_eb()
+    assert same(o.eb, d["exchange_eb"]), first_diff(o.eb, d["exchange_eb"])

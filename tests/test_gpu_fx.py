@@ -183,3 +183,24 @@ def test_fx_local_sort_is_a_stable_cell_sort(gpu, npbnd, tile):
         for f in ("x", "y", "z", "vx", "vy", "vz"):
             assert np.array_equal(got[f], a1[exp][f]), (s, f)
     g.close()
+
+
+def test_fx_em_step_vs_oracle(gpu):
+    """One EM step with the fields on the device (bfield, push, J, bfield,
+    efield, border exchange) against the oracle's FP64 sequence on the same
+    FP32-rounded start: the fields agree to the FP32 form's J tolerance."""
+    c = case(n=(16, 16, 16), ppc=(8, 8), vth_scale=3.0, tile=(8, 8, 8))
+    cfg, g, o, p32, tp32 = fx_pair(c)
+    tcs = 0.125
+    g.fx_em_step(2, False, tcs)
+    o.bfield()
+    oracle_step(o)
+    o.bfield()
+    o.efield(tcs)
+    o.exchange_eb()
+    eb = g.download_field("eb")
+    err = rel_l2(eb, o.eb)
+    print(f"eb L2 rel {err:.3e}")
+    assert err < 1e-6
+    assert rel_l2(g.download_field("aj"), o.f["aj"]) < RHOJ_TOL
+    g.close()

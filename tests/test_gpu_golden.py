@@ -96,3 +96,16 @@ def test_dropin_positn_golden(gpu, path):
         p, _ = g.download_particles()
         assert same_particles(p, d["positn_pbuf"])
         counters_match(gc, d, "positn_")
+
+
+@pytest.mark.parametrize("path", CASES, ids=lambda p: p.stem)
+def test_dropin_field_step_golden(gpu, path):
+    d, cfg = load(path)
+    with device(d, cfg, d["pbuf0"]) as g:
+        g.bfield(1)
+        assert np.array_equal(g.download_field("eb"), d["bfield_eb"])
+        g.upload_field("aj", d["reduced_aj"])
+        g.efield(1, float(d["tcs"]))
+        assert np.array_equal(g.download_field("eb"), d["efield_eb"])
+        g.exchange_eb()
+        assert np.array_equal(g.download_field("eb"), d["exchange_eb"])
