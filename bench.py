@@ -609,6 +609,71 @@ def run_body_line(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
+def run_em_line(args, world, rank, local):
+    """The headline workload run self-consistently with the fields on the
+    device: each step is bfield, push + J + rho, bfield, efield and the eb
+    border exchange (emsesg_fx_em_step; tcs = 2 (c dt)^2 = 0.125 in internal
+    units for c dt / dx = 0.5); sort every 4 steps."""
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's field solver is not built (no "
+                              "Fortran toolchain); its CPU particle path is timed by the default workload"}),
+                  flush=True)
+        return
+    import torch
+    from ctca_b200 import inputs
+    from ctca_b200.emses import Emses, select_device
+    torch.cuda.set_device(local)
+    select_device(local)
+    case = inputs.baseline_case(2)
+    cfg = inputs.make_config(case)
+    g = Emses(cfg)
+    g.upload_field("eb", inputs.make_fields(case))
+    g.fx_load_plasma(inputs.plasma(case, seed=case.seed + 1000 * rank))
+    npart = int(g.fx_counts().sum())
+    stream = torch.cuda.ExternalStream(g.stream)
+    k = [0]
+
+    def step():
+        g.fx_em_step(2, k[0] % SORT_EVERY == SORT_EVERY - 1, 0.125)
+        k[0] += 1
+
+    for _ in range(args.warmup):
+        step()
+    g.synchronize()
+    g.set_profiling(True)
+    g.profile_reset()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    t = max_over_ranks(world, e0.elapsed_time(e1) / 1e3)
+    prof = g.profile()
+    field_ms = sum(prof.get(n, (0.0, 0))[0] for n in ("bfield", "efield", "exchange_eb"))
+    out = {"metric": METRIC, "value": world * npart * args.steps / t, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64 (fields f64)",
+           "data": "synthetic",
+           "config": {"workload": f"{case.n[0]}^3 periodic, 2 species x {case.species[0].ppc} ppc ({npart:,} "
+                                  "particles), EM fields advanced on the device each step (bfield, push, bfield, "
+                                  "efield, border exchange), sort every 4",
+                      "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
+           "field_step_ms": field_ms / args.steps,
+           "gpu_launches": int(sum(n for _, n in prof.values())),
+           "kernels_ms": {kk: round(v[0], 3) for kk, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+           "clocks": clk.summary()}
+    g.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -622,7 +687,7 @@ def main():
     ap.add_argument("--cells", type=int, default=0, help="grid side of a smaller profiling case (default 128)")
     ap.add_argument("--ppc", type=int, default=0, help="particles per cell per species with --cells")
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and ensemble sections")
-    ap.add_argument("--workload", default="particle_step", choices=["particle_step", "ensemble", "body"])
+    ap.add_argument("--workload", default="particle_step", choices=["particle_step", "ensemble", "body", "em"])
     ap.add_argument("--body-scale", type=float, default=1.0, help="grid scale of the body workload (1: 256x256x512)")
     ap.add_argument("--ensemble-runs", type=int, default=None)
     ap.add_argument("--ensemble-steps", type=int, default=None)
@@ -631,6 +696,8 @@ def main():
     try:
         if args.workload == "body":
             run_body_line(args, world, rank, local)
+        elif args.workload == "em":
+            run_em_line(args, world, rank, local)
         elif args.workload == "ensemble":
             args.ensemble_runs = args.ensemble_runs or 512
             args.ensemble_steps = args.ensemble_steps or 200
