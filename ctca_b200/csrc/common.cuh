@@ -102,6 +102,8 @@ struct FxState {
   emsesg_particle* stage = nullptr;    // device staging of injected records
   int32_t* stage_ord = nullptr;
   int64_t stage_cap = 0;
+  double* inj_tab = nullptr;           // velocity tables of the device supervisors
+  int64_t inj_tab_cap = 0;
   int32_t* ord_host = nullptr;         // pinned host staging of the ordinals
   int64_t ord_host_cap = 0;
   cudaEvent_t ord_ev = nullptr;        // the last upload from ord_host

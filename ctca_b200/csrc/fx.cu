@@ -493,6 +493,7 @@ void fx_free(emsesg_ctx* ctx) {
   cudaFree(f.surf); cudaFree(f.tailord); cudaFree(f.stage); cudaFree(f.stage_ord);
   cudaFreeHost(f.ord_host);
   if (f.ord_ev) cudaEventDestroy(f.ord_ev);
+  cudaFree(f.inj_tab);
   if (f.gexec) cudaGraphExecDestroy(f.gexec);
   adj_free(f);
   f = FxState();
@@ -952,18 +953,18 @@ extern "C" int emsesg_fx_em_step(emsesg_ctx* ctx, int ustep, int do_sort, double
   return emsesg_exchange_eb(ctx);
 }
 
-extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int64_t n) {
-  if (!ctx || n < 0 || (n > 0 && !host)) return EMSESG_ERR_ARG;
-  if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
-  const int is = spec - 1;
-  if (is < 0 || is >= ctx->cfg.nspec) return set_error(ctx, EMSESG_ERR_ARG, "species %d out of range", spec);
-  if (n == 0) return EMSESG_OK;
+namespace emsesg {
+namespace {
+
+// Checks of an injection of n records of species index is, and room in the
+// device staging buffers.
+int inject_reserve(emsesg_ctx* ctx, int is, int64_t n) {
   FxState& f = ctx->fx;
   if (f.ntail[is] + n > f.tailcap[is])
-    return set_error(ctx, EMSESG_ERR_OVERFLOW, "tail zone of species %d full (%lld + %lld > %lld)", spec,
+    return set_error(ctx, EMSESG_ERR_OVERFLOW, "tail zone of species %d full (%lld + %lld > %lld)", is + 1,
                      (long long)f.ntail[is], (long long)n, (long long)f.tailcap[is]);
   if (ctx->totalp[is] + n > ctx->seg.capacity[is])
-    return set_error(ctx, EMSESG_ERR_OVERFLOW, "species %d capacity %lld exceeded", spec,
+    return set_error(ctx, EMSESG_ERR_OVERFLOW, "species %d capacity %lld exceeded", is + 1,
                      (long long)ctx->seg.capacity[is]);
   if (n > f.stage_cap) {
     cudaFree(f.stage);
@@ -975,6 +976,121 @@ extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle
     EMSESG_CUDA(ctx, cudaMalloc(&f.stage_ord, n * sizeof(int32_t)));
     f.stage_cap = n;
   }
+  return EMSESG_OK;
+}
+
+// The staged records (and ordinals) into the tail zone of species is; k1 is
+// the pending ordinal count after them.
+int inject_staged(emsesg_ctx* ctx, int is, int64_t n, int64_t k1) {
+  FxState& f = ctx->fx;
+  const int64_t off = f.base[is], slot0 = f.tail0[is] + f.ntail[is];
+  Bodies bd = make_bodies(ctx->cfg);
+  EMSESG_LAUNCH(ctx, "fx_inject", k_fx_inject, nblk(n), 256, 0, f.stage, f.stage_ord, n, make_geo(ctx), bd, slot0,
+                f.pos + off, f.vx + off, f.vy + off, f.vz + off, f.tailord + f.tailord_base[is] + f.ntail[is],
+                f.surf + (int64_t)is * f.nsurf, ctx->d_status, ctx->d_diag);
+  f.ntail[is] += n;
+  f.pending[is] = k1;
+  ctx->totalp[is] += n;
+  return EMSESG_OK;
+}
+
+// The supervisors' arithmetic without fused multiply-adds, so that the
+// records equal those of the host supervisors (ctca_b200/inject.py).
+__device__ __forceinline__ double lin(double lo, double hi, double u) {
+  return __dadd_rn(lo, __dmul_rn(__dsub_rn(hi, lo), u));
+}
+
+// Emitted pairs (psuper3.F90:142-208): pair k -> records 2k (anti-particle
+// on the face) and 2k+1 (its twin 1e-5 off the face, preside 1).
+__global__ void k_gen_emit(emsesg_particle* out, int32_t* ord, int64_t n, int nemd, double grd, double b1lo,
+                           double b1hi, double b2lo, double b2hi, const double* __restrict__ vnorm,
+                           const double* __restrict__ vtang, int npr, uint64_t seed, uint64_t stream,
+                           uint64_t index0, int spec, int64_t pending) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double u[6];
+  for (int c = 0; c < 6; c++) u[c] = hash_u01(seed, stream, (index0 + (uint64_t)k) * 6 + c);
+  const int an = abs(nemd);
+  const int ax0 = an - 1, ax1 = an % 3, ax2 = (an + 1) % 3;  // (0,1,2), (1,2,0), (2,0,1)
+  const double ud = nemd > 0 ? 1.0 : -1.0;
+  const int a0 = (int)(npr * u[0]), a1 = (int)(npr * u[1]), a2 = (int)(npr * u[2]);
+  const double vn = ud * vnorm[a0], vt1 = vtang[a1], vt2 = vtang[a2];
+  const double rt1 = lin(b1lo, b1hi, u[4]), rt2 = lin(b2lo, b2hi, u[5]);
+  emsesg_particle p;
+  double* r = &p.x;
+  double* v = &p.vx;
+  r[ax0] = grd; r[ax1] = rt1; r[ax2] = rt2;
+  v[ax0] = vn; v[ax1] = vt1; v[ax2] = vt2;
+  p.pid = 0; p.nid = 0; p.spec = spec;
+  p.preside = EMSESG_PCL_TO_BE_ACCUMULATED_AS_ANTIPCL;
+  out[2 * k] = p;
+  ord[2 * k] = 0;
+  r[ax0] = __dadd_rn(grd, __dmul_rn(ud, 1e-5));
+  p.preside = EMSESG_PCL_INJECTED;
+  out[2 * k + 1] = p;
+  ord[2 * k + 1] = (int32_t)(pending + k + 1);
+}
+
+// Inflow through a z face (psuper2.F90:236-292), preside 0.
+__global__ void k_gen_inflow_z(emsesg_particle* out, int32_t* ord, int64_t n, int front, int nx, int ny, int nz,
+                               const double* __restrict__ vzt, const double* __restrict__ vxt,
+                               const double* __restrict__ vyt, int npr, double injctisw, uint64_t seed,
+                               uint64_t stream, uint64_t index0, int spec) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double u[5];
+  for (int c = 0; c < 5; c++) u[c] = hash_u01(seed, stream, (index0 + (uint64_t)k) * 5 + c);
+  const int a1 = (int)(npr * u[0]), a2 = (int)(npr * u[1]);
+  emsesg_particle p;
+  p.x = __dadd_rn(0.0, __dmul_rn((double)nx, u[2]));
+  p.y = __dadd_rn(0.0, __dmul_rn((double)ny, u[3]));
+  const double vz = vzt[a1];
+  const double dz = __dmul_rn(__dmul_rn(vz, injctisw), u[4]);
+  p.z = front ? dz : __dadd_rn((double)nz, dz);
+  p.vx = vxt[a2];
+  p.vy = vyt[a2];
+  p.vz = vz;
+  p.pid = 0; p.preside = 0; p.nid = 0; p.spec = spec;
+  out[k] = p;
+  ord[k] = 0;
+}
+
+int inject_tables(emsesg_ctx* ctx, int ntab, int npr, const double* const* tabs) {
+  FxState& f = ctx->fx;
+  const int64_t need = (int64_t)ntab * npr;
+  if (need > f.inj_tab_cap) {
+    EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(f.inj_tab);
+    f.inj_tab = nullptr;
+    f.inj_tab_cap = 0;
+    EMSESG_CUDA(ctx, cudaMalloc(&f.inj_tab, need * sizeof(double)));
+    f.inj_tab_cap = need;
+  }
+  for (int t = 0; t < ntab; t++)
+    EMSESG_CUDA(ctx, cudaMemcpyAsync(f.inj_tab + (int64_t)t * npr, tabs[t], npr * sizeof(double),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+  return EMSESG_OK;
+}
+
+int inject_check(emsesg_ctx* ctx, int spec, int64_t n, int npr, const void* t0, const void* t1, const void* t2) {
+  if (!ctx || n < 0 || npr < 1 || !t0 || !t1 || !t2) return EMSESG_ERR_ARG;
+  if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
+  if (spec < 1 || spec > ctx->cfg.nspec) return set_error(ctx, EMSESG_ERR_ARG, "species %d out of range", spec);
+  return EMSESG_OK;
+}
+
+}  // namespace
+}  // namespace emsesg
+
+extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int64_t n) {
+  if (!ctx || n < 0 || (n > 0 && !host)) return EMSESG_ERR_ARG;
+  if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
+  const int is = spec - 1;
+  if (is < 0 || is >= ctx->cfg.nspec) return set_error(ctx, EMSESG_ERR_ARG, "species %d out of range", spec);
+  if (n == 0) return EMSESG_OK;
+  FxState& f = ctx->fx;
+  int rc = inject_reserve(ctx, is, n);
+  if (rc) return rc;
   // ordinal of each injected particle's random step, in buffer order, staged
   // in pinned host memory that the previous call's upload has released
   if (!f.ord_ev) EMSESG_CUDA(ctx, cudaEventCreateWithFlags(&f.ord_ev, cudaEventDisableTiming));
@@ -995,15 +1111,42 @@ extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle
   EMSESG_CUDA(ctx, cudaMemcpyAsync(f.stage, host, n * sizeof(emsesg_particle), cudaMemcpyHostToDevice, ctx->stream));
   EMSESG_CUDA(ctx, cudaMemcpyAsync(f.stage_ord, ord, n * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
   EMSESG_CUDA(ctx, cudaEventRecord(f.ord_ev, ctx->stream));
-  const int64_t off = f.base[is], slot0 = f.tail0[is] + f.ntail[is];
-  Bodies bd = make_bodies(ctx->cfg);
-  EMSESG_LAUNCH(ctx, "fx_inject", k_fx_inject, nblk(n), 256, 0, f.stage, f.stage_ord, n, make_geo(ctx), bd, slot0,
-                f.pos + off, f.vx + off, f.vy + off, f.vz + off, f.tailord + f.tailord_base[is] + f.ntail[is],
-                f.surf + (int64_t)is * f.nsurf, ctx->d_status, ctx->d_diag);
-  f.ntail[is] += n;
-  f.pending[is] = k1;
-  ctx->totalp[is] += n;
-  return EMSESG_OK;
+  return inject_staged(ctx, is, n, k1);
+}
+
+extern "C" int emsesg_fx_emit(emsesg_ctx* ctx, int spec, int nemd, double grd, const double* b1, const double* b2,
+                              int64_t n, const double* vnorm, const double* vtang, int npr, uint64_t seed,
+                              uint64_t stream, uint64_t index0) {
+  int rc = inject_check(ctx, spec, n, npr, vnorm, vtang, vnorm);
+  if (rc) return rc;
+  if (!b1 || !b2 || nemd == 0 || nemd < -3 || nemd > 3) return set_error(ctx, EMSESG_ERR_ARG, "bad emission face");
+  if (n == 0) return EMSESG_OK;
+  const int is = spec - 1;
+  FxState& f = ctx->fx;
+  if ((rc = inject_reserve(ctx, is, 2 * n))) return rc;
+  const double* tabs[2] = {vnorm, vtang};
+  if ((rc = inject_tables(ctx, 2, npr, tabs))) return rc;
+  const int64_t pending = f.pending[is];
+  EMSESG_LAUNCH(ctx, "fx_gen_emit", k_gen_emit, nblk(n), 256, 0, f.stage, f.stage_ord, n, nemd, grd, b1[0], b1[1],
+                b2[0], b2[1], f.inj_tab, f.inj_tab + npr, npr, seed, stream, index0, spec, pending);
+  return inject_staged(ctx, is, 2 * n, pending + n);
+}
+
+extern "C" int emsesg_fx_inflow_z(emsesg_ctx* ctx, int spec, int front, int64_t n, const double* vz_t,
+                                  const double* vx_t, const double* vy_t, int npr, double injctisw, uint64_t seed,
+                                  uint64_t stream, uint64_t index0) {
+  int rc = inject_check(ctx, spec, n, npr, vz_t, vx_t, vy_t);
+  if (rc) return rc;
+  if (n == 0) return EMSESG_OK;
+  const int is = spec - 1;
+  FxState& f = ctx->fx;
+  if ((rc = inject_reserve(ctx, is, n))) return rc;
+  const double* tabs[3] = {vz_t, vx_t, vy_t};
+  if ((rc = inject_tables(ctx, 3, npr, tabs))) return rc;
+  const emsesg_config& c = ctx->cfg;
+  EMSESG_LAUNCH(ctx, "fx_gen_inflow", k_gen_inflow_z, nblk(n), 256, 0, f.stage, f.stage_ord, n, front, c.nx, c.ny,
+                c.nz, f.inj_tab, f.inj_tab + npr, f.inj_tab + 2 * npr, npr, injctisw, seed, stream, index0, spec);
+  return inject_staged(ctx, is, n, f.pending[is]);
 }
 
 extern "C" int emsesg_fx_surface(emsesg_ctx* ctx, int64_t* counts, int64_t* nsurf) {

@@ -141,6 +141,10 @@ _SIGS = {
     "emsesg_fx_download_accum": (_I, [_P, _P]),
     "emsesg_fx_inject": (_I, [_P, _I, _P, ctypes.c_int64]),
     "emsesg_fx_surface": (_I, [_P, _P, ctypes.POINTER(ctypes.c_int64)]),
+    "emsesg_fx_emit": (_I, [_P, _I, _I, ctypes.c_double, _P, _P, ctypes.c_int64, _P, _P, _I, ctypes.c_uint64,
+                            ctypes.c_uint64, ctypes.c_uint64]),
+    "emsesg_fx_inflow_z": (_I, [_P, _I, _I, ctypes.c_int64, _P, _P, _P, _I, ctypes.c_double, ctypes.c_uint64,
+                                ctypes.c_uint64, ctypes.c_uint64]),
     "emsesg_fx_adjoint": (_I, [_P, _I, _I, _I, _I, _P, _P, ctypes.POINTER(ctypes.c_double), _P, _P, _P, _P]),
     "emsesg_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
     "emsesg_fx_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
@@ -396,6 +400,28 @@ class Emses:
         """fx_inject from a host address of n records (pinned memory: the
         upload is asynchronous; keep the records until the stream is past it)."""
         self._check(self.lib.emsesg_fx_inject(self.h, spec, ptr if n else None, n))
+
+    def fx_emit(self, spec: int, nemd: int, grd: float, bounds1, bounds2, n: int, vnormf, vtangf,
+                seed: int, stream: int, index0: int = 0):
+        """n emitted pairs from a body face drawn on the device
+        (emit_rectangle with hash_uniforms(seed, stream, index0, n, 6))."""
+        b1 = (ctypes.c_double * 2)(*bounds1)
+        b2 = (ctypes.c_double * 2)(*bounds2)
+        vn = np.ascontiguousarray(vnormf, dtype=np.float64)
+        vt = np.ascontiguousarray(vtangf, dtype=np.float64)
+        assert vn.size == vt.size
+        self._check(self.lib.emsesg_fx_emit(self.h, spec, nemd, grd, b1, b2, n, vn.ctypes.data, vt.ctypes.data,
+                                            vn.size, seed, stream, index0))
+
+    def fx_inflow_z(self, spec: int, front: bool, n: int, vz_table, vx_table, vy_table, injctisw: float,
+                    seed: int, stream: int, index0: int = 0):
+        """n inflow particles through a z face drawn on the device
+        (inflow_z with hash_uniforms(seed, stream, index0, n, 5))."""
+        t = [np.ascontiguousarray(x, dtype=np.float64) for x in (vz_table, vx_table, vy_table)]
+        assert t[0].size == t[1].size == t[2].size
+        self._check(self.lib.emsesg_fx_inflow_z(self.h, spec, 1 if front else 0, n, t[0].ctypes.data,
+                                                t[1].ctypes.data, t[2].ctypes.data, t[0].size, injctisw, seed,
+                                                stream, index0))
 
     def fx_surface(self) -> np.ndarray:
         """Absorbed minus emitted particles per surface cell, [nspec, nsurf]."""

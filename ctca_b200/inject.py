@@ -13,8 +13,11 @@ tables hold the npr quantiles (k + 1/2)/npr of the same distributions:
   normal flux  v * exp(-(v - vd)^2 / (2 vth^2)) on v > 0 (flux through a face)
 
 Random numbers come from a numpy Generator (the reference uses MT19937
-through RANU0); the number and order of draws per particle follow the
-reference: 6 per emitted particle (u(4) unused), 5 per inflow particle.
+through RANU0), or, with `uniforms=`, from a given array; the number and
+order of draws per particle follow the reference: 6 per emitted particle
+(u(4) unused), 5 per inflow particle.  `hash_uniforms` gives the draws of
+the device supervisors (emsesg_fx_emit / emsesg_fx_inflow_z), so the two
+produce the same records.
 """
 from __future__ import annotations
 
@@ -27,6 +30,30 @@ from .emses import PARTICLE_DTYPE
 
 PCL_INJECTED = 1
 PCL_ANTI = -2
+
+
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def _mix64(z: np.ndarray) -> np.ndarray:
+    """SplitMix64 finaliser (Steele, Lea, Flood 2014) on uint64 arrays."""
+    z = z + np.uint64(0x9E3779B97F4A7C15)
+    z = (z ^ (z >> np.uint64(30))) * _M1
+    z = (z ^ (z >> np.uint64(27))) * _M2
+    return z ^ (z >> np.uint64(31))
+
+
+def hash_uniforms(seed: int, stream: int, index0: int, n: int, per: int) -> np.ndarray:
+    """[n, per] U[0,1) numbers with 53 random bits: element (k, c) is the
+    counter hash of (seed, stream, (index0 + k) * per + c), the draws of the
+    device supervisors."""
+    with np.errstate(over="ignore"):
+        a = _mix64(np.uint64(seed) ^ _mix64(np.array([stream], dtype=np.uint64) + np.uint64(0x632BE59BD9B4E019)))
+        idx = (np.uint64(index0) + np.arange(n, dtype=np.uint64)[:, None]) * np.uint64(per) + \
+            np.arange(per, dtype=np.uint64)[None, :]
+        b = _mix64(a ^ (idx * np.uint64(0xD1B54A32D192ED03)))
+    return (b >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
 
 
 def maxwell_table(vth: float, drift: float, npr: int) -> np.ndarray:
@@ -64,7 +91,8 @@ _ORDER = {1: (0, 1, 2), 2: (1, 2, 0), 3: (2, 0, 1)}
 
 
 def emit_rectangle(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int, vnormf: np.ndarray,
-                   vtangf: np.ndarray, rng: np.random.Generator, spec: int) -> np.ndarray:
+                   vtangf: np.ndarray, rng: np.random.Generator | None, spec: int,
+                   uniforms: np.ndarray | None = None) -> np.ndarray:
     """n emitted particles from a rectangular face (emit_from_rectangle,
     psuper3.F90:142-208): each gives an anti-particle (preside -2) on the
     face and its twin 1e-5 off the face along the normal (preside +1).
@@ -73,7 +101,7 @@ def emit_rectangle(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int
     axis = _ORDER[abs(nemd)]
     ud = 1.0 if nemd > 0 else -1.0
     npr = vnormf.size
-    u = rng.random((n, 6))
+    u = rng.random((n, 6)) if uniforms is None else uniforms
     out = np.zeros(2 * n, dtype=PARTICLE_DTYPE)  # pid = nid = 0
     coords = [("x", "vx"), ("y", "vy"), ("z", "vz")]
     a0 = (npr * u[:, 0]).astype(np.int64)
@@ -104,13 +132,13 @@ def inflow_count(istep: int, lstep: int, arr: float, injct: int, ustep: int) -> 
 
 
 def inflow_z(front: bool, n: int, nx: int, ny: int, nz: int, vz_table: np.ndarray, vx_table: np.ndarray,
-             vy_table: np.ndarray, injctisw: float, rng: np.random.Generator, spec: int,
-             zssurf: float = -1.0e30) -> np.ndarray:
+             vy_table: np.ndarray, injctisw: float, rng: np.random.Generator | None, spec: int,
+             zssurf: float = -1.0e30, uniforms: np.ndarray | None = None) -> np.ndarray:
     """Particles entering through the z = 0 face (front) or z = nz face
     (back), psuper2.F90:236-292: x, y uniform on the face, z = the distance
     covered within the last injctisw steps, preside 0."""
     npr = vz_table.size
-    u = rng.random((n, 5))
+    u = rng.random((n, 5)) if uniforms is None else uniforms
     a1 = (npr * u[:, 0]).astype(np.int64)
     a2 = (npr * u[:, 1]).astype(np.int64)
     out = np.zeros(n, dtype=PARTICLE_DTYPE)

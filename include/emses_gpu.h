@@ -317,6 +317,25 @@ int emsesg_fx_download_accum(emsesg_ctx* ctx, int64_t* host);
  * (keep the records unchanged until the stream has passed the call); from
  * pageable memory the call returns once the records are copied. */
 int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int64_t n);
+/* The injection supervisors on the device (records drawn, converted and
+ * put into the tail zone without a host round trip).  U[0,1) numbers come
+ * from a counter hash of (seed, stream, index0 + k) per particle k;
+ * ctca_b200/inject.py computes the same records on the host
+ * (hash_uniforms), to which these are bit-identical.
+ * emsesg_fx_emit: n emitted pairs from the face nemd (+-1: x, +-2: y, +-3:
+ * z) at grd, extents b1 / b2 along its first / second tangential axis:
+ * an anti-particle (preside -2) on the face and its twin 1e-5 off it
+ * (preside 1), normal speed vnorm[int(npr*u0)], tangential vtang[int(npr*u1)],
+ * vtang[int(npr*u2)] (psuper3.F90:142-208).  emsesg_fx_inflow_z: n
+ * particles through z = 0 (front) or z = nz: x, y uniform on the face, z =
+ * the distance vz * injctisw * u4 from it, vz = vz_t[int(npr*u0)],
+ * vx / vy = vx_t / vy_t[int(npr*u1)], preside 0 (psuper2.F90:236-292). */
+int emsesg_fx_emit(emsesg_ctx* ctx, int spec, int nemd, double grd, const double* b1, const double* b2, int64_t n,
+                   const double* vnorm, const double* vtang, int npr, uint64_t seed, uint64_t stream,
+                   uint64_t index0);
+int emsesg_fx_inflow_z(emsesg_ctx* ctx, int spec, int front, int64_t n, const double* vz_t, const double* vx_t,
+                       const double* vy_t, int npr, double injctisw, uint64_t seed, uint64_t stream,
+                       uint64_t index0);
 /* Absorbed minus emitted particles per surface cell of the box bodies
  * (geotype 0/1, integer bounds), int64 [nspec][nsurf]: body by body, faces
  * -x,+x,-y,+y,-z,+z, each face's cells with its first tangential axis

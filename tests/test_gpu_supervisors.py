@@ -1,0 +1,73 @@
+"""The injection supervisors on the device (emsesg_fx_emit,
+emsesg_fx_inflow_z) against the host supervisors of ctca_b200/inject.py fed
+the same counter-hash draws (inject.hash_uniforms): the injected records,
+and everything downstream (the step's rho/J accumulators, the surface
+counts, the particle records after the sort), are bit-identical."""
+import numpy as np
+import pytest
+
+from ctca_b200 import inject, inputs
+from ctca_b200.emses import Emses
+
+from helpers import build, case
+
+pytestmark = pytest.mark.gpu
+
+BOX = dict(geotype=0, ncond=1, xlpc=8.0, xupc=16.0, ylpc=8.0, yupc=16.0, zlpc=14.0, zupc=18.0, sqdscaled=1.0)
+
+
+def setup():
+    c = case(n=(24, 24, 32), ppc=(3, 3), npbnd=(0, 0, 2), nfbnd=(0, 0, 1), vth_scale=3.0, tile=(8, 8, 8))
+    for s in c.species:
+        s.drift = (0.0, 0.0, -0.08)
+    c.bodies = [BOX]
+    cfg, eb, p, tp = build(c, capacity_factor=1.5)
+    return c, cfg, eb
+
+
+def loaded(c, cfg, eb):
+    g = Emses(cfg)
+    g.upload_field("eb", eb)
+    g.fx_load_plasma(inputs.plasma(c, seed=5))
+    return g
+
+
+def test_device_supervisors_match_host(gpu):
+    c, cfg, eb = setup()
+    renv = inputs.units()["renv"]
+    vn = inject.flux_table(0.01 * renv, 0.0, 512)
+    vt = inject.maxwell_table(0.01 * renv, 0.0, 512)
+    s0 = c.species[0]
+    vz = inject.flux_table(s0.vth * renv, -0.08 * renv, 512, sign=-1.0)
+    vx = inject.maxwell_table(s0.vth * renv, 0.0, 512)
+    vy = vx[::-1].copy()
+    seed = 99
+    with loaded(c, cfg, eb) as a, loaded(c, cfg, eb) as b:
+        for step in range(3):
+            ne, ni = 40 + step, 70 + 3 * step
+            # host: the same draws as the device
+            ue = inject.hash_uniforms(seed, 1, 1000 * step, ne, 6)
+            ui = inject.hash_uniforms(seed, 2, 1000 * step, ni, 5)
+            rec_e = inject.emit_rectangle(1, 16.0, (8.0, 16.0), (14.0, 18.0), ne, vn, vt, None, spec=1,
+                                          uniforms=ue)
+            rec_i = inject.inflow_z(False, ni, cfg.nx, cfg.ny, cfg.nz, vz, vx, vy, 2.0, None, spec=1, uniforms=ui)
+            a.fx_inject(1, rec_e)
+            a.fx_inject(1, rec_i)
+            b.fx_emit(1, 1, 16.0, (8.0, 16.0), (14.0, 18.0), ne, vn, vt, seed, 1, 1000 * step)
+            b.fx_inflow_z(1, False, ni, vz, vx, vy, 2.0, seed, 2, 1000 * step)
+            a.fx_step(2, step == 1)
+            b.fx_step(2, step == 1)
+            ra, ja = a.fx_download_accum()
+            rb, jb = b.fx_download_accum()
+            assert np.array_equal(ra, rb), step
+            assert np.array_equal(ja, jb), step
+        assert np.array_equal(a.fx_surface(), b.fx_surface())
+        assert np.abs(a.fx_surface()).sum() > 0
+        a.fx_sort()
+        b.fx_sort()
+        a.fx_store()
+        b.fx_store()
+        pa, ta = a.download_particles()
+        pb, tb = b.download_particles()
+        assert np.array_equal(ta, tb)
+        assert np.array_equal(pa.view(np.uint8), pb.view(np.uint8))
