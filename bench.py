@@ -440,6 +440,41 @@ def run_ensemble_line(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def body_plan(case, scale: float) -> dict:
+    """Per-step injection of the body workload drawn on the device: tables
+    and counts (the rates of body_injection)."""
+    from ctca_b200 import inject, inputs
+    renv = inputs.units()["renv"]
+    nx, ny, nz = case.n
+    plan = {"nemit": int(round((1 << 20) * scale ** 3)),
+            "vn": inject.flux_table(0.01 * renv, 0.0, 4096), "vt": inject.maxwell_table(0.01 * renv, 0.0, 4096),
+            "inflow": []}
+    counts = [0, 0]
+    for isp, s in enumerate(case.species):
+        vd = s.drift[2]
+        vxt = inject.maxwell_table(s.vth * renv, 0.0, 4096)
+        vyt = np.random.default_rng([case.seed, 99, isp]).permutation(vxt)
+        for front, sgn in ((True, +1.0), (False, -1.0)):
+            n = int(round(s.ppc * nx * ny * _flux(vd, s.vth, sgn) * case.dt))
+            if n:
+                plan["inflow"].append((isp + 1, front, n, inject.flux_table(s.vth * renv, vd * renv, 4096, sign=sgn),
+                                       vxt, vyt))
+                counts[isp] += n
+    counts[0] += 2 * plan["nemit"]
+    plan["counts"] = counts
+    return plan
+
+
+def body_inject_device(g, case, plan, seed: int, step: int):
+    """One step's injection of the body workload with the device supervisors."""
+    body = case.bodies[0]
+    for q, (spec, front, n, vz, vx, vy) in enumerate(plan["inflow"]):
+        g.fx_inflow_z(spec, front, n, vz, vx, vy, 2.0, seed, 10 + q, step * n)
+    if plan["nemit"]:
+        g.fx_emit(1, 1, body["xupc"], (body["ylpc"], body["yupc"]), (body["zlpc"], body["zupc"]), plan["nemit"],
+                  plan["vn"], plan["vt"], seed, 1, step * plan["nemit"])
+
+
 def _flux(mu, sig, sign):
     """E[(sign v)+] for v ~ N(mu, sig^2)."""
     from math import erf, exp, pi, sqrt
@@ -501,7 +536,9 @@ def run_body_line(args, world, rank, local):
     emits 2^20 photoelectrons a step from its +x face, inflow through the z
     faces; B0 = (0.05, 0, 0.1), E = 0.  An FP32-only context (no FP64
     particle buffer) holds it on one GPU.  Each timed step injects the
-    step's records (host -> device) and pushes; sort every 4 steps."""
+    step's records -- drawn on the device (emsesg_fx_emit,
+    emsesg_fx_inflow_z), or with --host-inject drawn on the host and
+    uploaded from pinned memory -- and pushes; sort every 4 steps."""
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the body workload (1.6e9 particles) is timed on "
@@ -515,10 +552,17 @@ def run_body_line(args, world, rank, local):
     scale = args.body_scale
     case = inputs.baseline_case(3, scale)
     steps, warm = args.steps, args.warmup
-    inj = body_injection(case, warm + steps + 5, scale, seed=case.seed + 17 * rank)
-    add = [sum(int(st[i].size) for st in inj) for i in range(2)]
-    # the step's records come from pinned host memory (asynchronous uploads)
-    pinned = [[torch.from_numpy(r.view(np.uint8)).pin_memory() for r in st] for st in inj]
+    nstep_all = warm + steps + 5
+    seed = case.seed + 17 * rank
+    if args.host_inject:
+        inj = body_injection(case, nstep_all, scale, seed=seed)
+        counts = [[int(r.size) for r in st] for st in inj]
+        # the step's records come from pinned host memory (asynchronous uploads)
+        pinned = [[torch.from_numpy(r.view(np.uint8)).pin_memory() for r in st] for st in inj]
+    else:
+        plan = body_plan(case, scale)
+        counts = [plan["counts"]] * nstep_all
+    add = [sum(st[i] for st in counts) for i in range(2)]
     ncell = case.n[0] * case.n[1] * case.n[2]
     cap = [int(s.ppc * ncell * 1.01) + add[i] + (1 << 20) for i, s in enumerate(case.species)]
     cfg = inputs.make_config(case, capacity=cap)
@@ -529,10 +573,13 @@ def run_body_line(args, world, rank, local):
     k = [0]
 
     def step():
-        recs = inj[k[0]]
-        for isp in range(2):
-            if recs[isp].size:
-                g.fx_inject_raw(isp + 1, pinned[k[0]][isp].data_ptr(), recs[isp].size)
+        if args.host_inject:
+            recs = inj[k[0]]
+            for isp in range(2):
+                if recs[isp].size:
+                    g.fx_inject_raw(isp + 1, pinned[k[0]][isp].data_ptr(), recs[isp].size)
+        else:
+            body_inject_device(g, case, plan, seed, k[0])
         g.fx_step(2, k[0] % SORT_EVERY == SORT_EVERY - 1)
         k[0] += 1
 
@@ -557,12 +604,13 @@ def run_body_line(args, world, rank, local):
     prof = g.profile()
     g.set_profiling(False)
     n1 = int(g.fx_counts().sum())
-    inj_bytes = sum(int(r.nbytes) for st in inj[warm:warm + steps] for r in st)
+    inj_bytes = (sum(int(r.nbytes) for st in inj[warm:warm + steps] for r in st) if args.host_inject
+                 else 0)
     # end to end: the same steps plus rho and J to host after each one
     nr, na = g.field_size("rho"), g.field_size("aj")
     rho_h = torch.empty(nr, dtype=torch.float64, pin_memory=True)
     aj_h = torch.empty(na, dtype=torch.float64, pin_memory=True)
-    ke = min(5, len(inj) - k[0])
+    ke = min(5, nstep_all - k[0])
     ne0 = int(g.fx_counts().sum())
     g.synchronize()
     t0 = time.perf_counter()
@@ -588,8 +636,9 @@ def run_body_line(args, world, rank, local):
                                f"{int(case.bodies[0]['xupc'] - case.bodies[0]['xlpc'])}x"
                                f"{int(case.bodies[0]['yupc'] - case.bodies[0]['ylpc'])}x"
                                f"{int(case.bodies[0]['zupc'] - case.bodies[0]['zlpc'])} absorbing with int64 "
-                               f"surface counts, {inj[0][0].size:,} electron and {inj[0][1].size:,} ion records "
-                               "injected a step (z inflow + photoemission pairs), sort every 4, FP32-only context",
+                               f"surface counts, {counts[0][0]:,} electron and {counts[0][1]:,} ion records "
+                               "injected a step (z inflow + photoemission pairs, drawn on the "
+                               f"{'host' if args.host_inject else 'device'}), sort every 4, FP32-only context",
                    "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": None, "kernel": "fx_push",
@@ -689,6 +738,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and ensemble sections")
     ap.add_argument("--workload", default="particle_step", choices=["particle_step", "ensemble", "body", "em"])
     ap.add_argument("--body-scale", type=float, default=1.0, help="grid scale of the body workload (1: 256x256x512)")
+    ap.add_argument("--host-inject", action="store_true",
+                    help="body workload: draw the injected records on the host (else on the device)")
     ap.add_argument("--ensemble-runs", type=int, default=None)
     ap.add_argument("--ensemble-steps", type=int, default=None)
     args = ap.parse_args()
