@@ -571,14 +571,12 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
 }
 
 // The particles of a warp's cross list (slots in the tile region, still
-// holding their state before this step): each lane takes one, repeats the
-// gather and Buneman-Boris of the row loop on it (the same code, so the same
-// velocity) and runs the general path.  Returns the number of this lane's
-// particles that escaped.
+// holding their position before this step and the velocity the row loop
+// gave them): each lane takes one and runs the general path.  Returns the
+// number of this lane's particles that escaped.
 template <int B, bool DEP>
 __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t slot0, unsigned long long* box,
-                                          const int (&o)[3], const float4* sf0, const float2* sf1, const int* xl,
-                                          int xn, int lane) {
+                                          const int (&o)[3], const int* xl, int xn, int lane) {
   __syncwarp();
   // the context comes from the kernel parameters here, so that the pushing
   // loop keeps none of it in registers
@@ -591,11 +589,7 @@ __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t s
   for (int e = lane; e < xn; e += 32) {
     const int loc = xl[e];
     const float4 ps = c.gpos[loc];
-    float vx = c.gvx[loc], vy = c.gvy[loc], vz = c.gvz[loc];
-    const uint32_t cell = (uint32_t)__float_as_int(ps.w);
-    int ib, jb, kb;
-    unpack(g, cell, ib, jb, kb);
-    kick<B>(a, sf0, sf1, box_base<B>(o, ib, jb, kb), ib, jb, kb, ps, a.qmp[is], vx, vy, vz);
+    const float vx = c.gvx[loc], vy = c.gvy[loc], vz = c.gvz[loc];
     const float en[XQW] = {__int_as_float(loc), ps.w, ps.x, ps.y, ps.z, vx, vy, vz};
     dead += cross_one<B, DEP>(g, box, o, sk, c, en);
   }
@@ -844,9 +838,11 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
         for (int q = 0; q < NJ + NR; q++) acc[q] += cv[q];
       }
     }
-    if (simple || oop) {
+    // the new velocity of every particle (a cell-crossing one keeps its old
+    // position until the general path writes the whole record)
+    if (act) {
       const int m = r * PUSH_THREADS + tid;
-      gpos[m] = make_float4(sx, syy, szz, ps.w);
+      if (simple || oop) gpos[m] = make_float4(sx, syy, szz, ps.w);
       gvx[m] = vx;
       gvy[m] = vy;
       gvz[m] = vz;
@@ -858,8 +854,8 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
         rqn = 0;
       }
     }
-    // ---- cell-crossing particles: the warp's cross list (their records
-    // stay as they were; the general path after the row loop redoes them)
+    // ---- cell-crossing particles: the warp's cross list (their positions
+    // stay as they were; the general path after the row loop moves them)
     const bool cross = act && !simple && !oop;
     const unsigned xm = __ballot_sync(0xffffffffu, cross);
     if (xm) {
@@ -872,7 +868,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     }
   }
   if (xqn) {
-    nesc += cross_list<B, DEP>(a, is, slot0, box, o, sf0, sf1, xl, xqn, lane);
+    nesc += cross_list<B, DEP>(a, is, slot0, box, o, xl, xqn, lane);
     xqn = 0;
   }
   if (r >= L || failed) break;

@@ -276,17 +276,29 @@ __global__ void __launch_bounds__(CELL_THREADS) k_lcs_bases(const uint32_t* __re
   }
 }
 
+// q / d for 32-bit q and d >= 1 by one 64-bit high multiply with
+// M = ceil(2^64 / d) (Lemire, Kaser and Kurz, "Faster remainder by direct
+// computation", 2019); d = 1 is passed through.
+__host__ __device__ __forceinline__ uint64_t fastdiv_mul(uint32_t d) {
+  return d > 1 ? ~0ull / d + 1 : 0ull;
+}
+__device__ __forceinline__ uint32_t fastdiv(uint32_t q, uint32_t d, uint64_t M) {
+  return d > 1 ? (uint32_t)__umul64hi(M, (uint64_t)q) : q;
+}
+
 // rank: every live particle of source tile t gets its slot in the new
-// regions; inv[new slot] = old slot.  grid = ntiles, block = PUSH_THREADS,
-// shared = PUSH_WARPS * nbc * 4.
+// regions; inv[new slot] = old slot (4-byte scattered writes).  grid =
+// ntiles, block = PUSH_THREADS, shared = PUSH_WARPS * nbc * 4.
+
 __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restrict__ pos,
-                                                           const int64_t* __restrict__ ts,
-                                                           const int64_t* __restrict__ tp, Geo g, LcsGeo G,
-                                                           const uint32_t* __restrict__ wcnt,
-                                                           const uint32_t* __restrict__ base,
-                                                           const int64_t* __restrict__ ts2,
-                                                           const int64_t* __restrict__ tp2, uint32_t* __restrict__ inv,
-                                                           int* status, long long* diag, const int* stray) {
+                                                              const int64_t* __restrict__ ts,
+                                                              const int64_t* __restrict__ tp, Geo g, LcsGeo G,
+                                                              const uint32_t* __restrict__ wcnt,
+                                                              const uint32_t* __restrict__ base,
+                                                              const int64_t* __restrict__ ts2,
+                                                              const int64_t* __restrict__ tp2,
+                                                              uint32_t* __restrict__ inv, int* status,
+                                                              long long* diag, const int* stray) {
   extern __shared__ uint32_t wb[];  // [PUSH_WARPS][nbc] next rank of (warp, box cell)
   if (*stray) return;
   const int t = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -299,20 +311,64 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restr
       run += wc[w * G.nbc + b];
     }
   }
-  __syncthreads();
   int tx, ty, tz;
   tile_xyz(g, t, tx, ty, tz);
+  // the 27 tiles around this one (the destinations of its particles): first
+  // rank, count, rows with their division multiplier, region start; a
+  // sort-box cell's side on each axis (below, inside, above the tile) picks
+  // the entry
+  __shared__ uint32_t nq0[27], nnd[27], nld[27];
+  __shared__ uint64_t nmul[27];
+  __shared__ int64_t ntp[27];
+  if (tid < 27) {
+    const int d3[3] = {tid % 3 - 1, (tid / 3) % 3 - 1, tid / 9 - 1};
+    const int c3[3] = {tx, ty, tz};
+    bool ok = true;
+    int64_t td = 0, mul = 1;
+    for (int d = 0; d < 3; d++) {
+      int x = c3[d] + d3[d];
+      if (x < 0 || x >= g.nt[d]) {
+        if (G.wrap[d]) x = (x + g.nt[d]) % g.nt[d];
+        else ok = false;
+      }
+      td += mul * x;
+      mul *= g.nt[d];
+    }
+    const int64_t nd = ok ? ts2[td + 1] - ts2[td] : 0;
+    nq0[tid] = ok ? (uint32_t)ts2[td] : 0u;
+    nnd[tid] = (uint32_t)nd;
+    const uint32_t ld = (uint32_t)((nd + PUSH_THREADS - 1) / PUSH_THREADS);
+    nld[tid] = ld;
+    nmul[tid] = fastdiv_mul(ld);
+    ntp[tid] = ok ? tp2[td] : 0;
+  }
+  __syncthreads();
   const int64_t n = ts[t + 1] - ts[t];
   const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
   const int64_t s0 = tp[t];
   uint32_t* mywb = wb + warp * G.nbc;
+  // the cells of the next rows are loaded ahead
+  constexpr int AHEAD = 4;
+  uint32_t cr[AHEAD];
+#pragma unroll
+  for (int q = 0; q < AHEAD; q++)
+    cr[q] = q < L ? (uint32_t)__float_as_int(pos[s0 + (int64_t)q * PUSH_THREADS + tid].w) : DEAD;
   for (int r = 0; r < L; r++) {
     const int64_t m = s0 + (int64_t)r * PUSH_THREADS + tid;
-    const uint32_t cell = (uint32_t)__float_as_int(pos[m].w);
-    int i = 0, j = 0, k = 0, bc = -1;
+    const uint32_t cell = cr[0];
+#pragma unroll
+    for (int q = 0; q < AHEAD - 1; q++) cr[q] = cr[q + 1];
+    cr[AHEAD - 1] = r + AHEAD < L ? (uint32_t)__float_as_int(pos[m + (int64_t)AHEAD * PUSH_THREADS].w) : DEAD;
+    int bc = -1, nb = 0;
     if (cell != DEAD) {
+      int i, j, k;
       unpack(g, cell, i, j, k);
-      bc = lcs_box_cell(G, tx, ty, tz, i, j, k);  // >= 0: strays sort with the radix path
+      const int a = lcs_axis(G, 0, tx, i), b = lcs_axis(G, 1, ty, j), c = lcs_axis(G, 2, tz, k);
+      if ((a | b | c) >= 0) {  // else a stray: the radix path sorts
+        bc = a + G.bc[0] * (b + G.bc[1] * c);
+        nb = (a == 0 ? 0 : (a == G.bc[0] - 1 ? 2 : 1)) + 3 * (b == 0 ? 0 : (b == G.bc[1] - 1 ? 2 : 1)) +
+             9 * (c == 0 ? 0 : (c == G.bc[2] - 1 ? 2 : 1));
+      }
     }
     const unsigned peers = __match_any_sync(0xffffffffu, bc);
     const uint32_t rank = bc >= 0 ? mywb[bc] + __popc(peers & lt) : 0u;
@@ -320,42 +376,60 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restr
     if (bc >= 0 && (peers & lt) == 0) mywb[bc] += __popc(peers);
     __syncwarp();
     if (bc < 0) continue;
-    // destination tile and its thread-major slot
-    const int64_t td = (int64_t)(i / g.t[0]) + (int64_t)g.nt[0] * ((j / g.t[1]) + (int64_t)g.nt[1] * (k / g.t[2]));
-    const int64_t q = (int64_t)rank - ts2[td];
-    const int64_t nd = ts2[td + 1] - ts2[td];
-    if (q < 0 || q >= nd) {
+    // the destination tile's thread-major slot
+    const uint32_t q = rank - nq0[nb];
+    if (q >= nnd[nb]) {
       report_bad(status, diag, SITE_FX_SORT, m, (long long)cell);
       continue;
     }
-    const int64_t Ld = (nd + PUSH_THREADS - 1) / PUSH_THREADS;
-    inv[tp2[td] + (q % Ld) * PUSH_THREADS + q / Ld] = (uint32_t)m;
+    const uint32_t Ld = nld[nb];
+    const uint32_t col = fastdiv(q, Ld, nmul[nb]);
+    inv[ntp[nb] + (q - col * Ld) * PUSH_THREADS + col] = (uint32_t)m;
   }
 }
 
 // move: the new region of destination tile t, in groups of 32 columns.  A
 // particle that stayed in its tile keeps about its column (its rank moves by
-// the net count change of the cells before it), so each group first stages a
-// window of MOVE_WCOLS source columns (all rows of the tile's old region,
-// coalesced rows) in shared memory, centred on the old column of the group's
-// middle slot, and then writes its slots row by row (coalesced), taking each
-// particle from the window or, when it came from elsewhere, from global
-// memory.  grid = ntiles, block = PUSH_THREADS, shared = move_smem().
-constexpr int MOVE_WCOLS = 40;
-constexpr int MOVE_MAXROWS = 80;  // two CTAs per SM
-inline int move_smem() { return MOVE_MAXROWS * MOVE_WCOLS * (16 + 3 * 4); }
+// the net count change of the cells before it), so each group takes its
+// particles from a window of MOVE_WCOLS source columns (all rows of the
+// tile's old region), centred on the old column of the group's middle slot,
+// or, when one came from elsewhere, from global memory; the writes go row by
+// row (coalesced).  The window and the group's 32 columns of inv are staged
+// in shared memory with cp.async, double-buffered: group g+1's copies are in
+// flight while group g is written.  grid = ntiles, block = PUSH_THREADS (one
+// CTA per SM), shared = move_smem().
+constexpr int MOVE_WCOLS = 40;  // a multiple of 4: 16-byte rows of the velocity arrays
+constexpr int MOVE_MAXROWS = 80;
+constexpr int MOVE_GROUPS = PUSH_THREADS / 32;
+constexpr int MOVE_K = (MOVE_MAXROWS * 32 + PUSH_THREADS - 1) / PUSH_THREADS;  // slots of a thread per group
+constexpr int MOVE_WIN = MOVE_MAXROWS * MOVE_WCOLS;
+constexpr int MOVE_BUF = MOVE_WIN * (16 + 3 * 4) + MOVE_MAXROWS * 32 * 4;  // bytes of one buffer
+inline int move_smem() { return 2 * MOVE_BUF; }
+static_assert(MOVE_WCOLS % 4 == 0 && PUSH_THREADS % 32 == 0, "16-byte window rows");
 
-__global__ void __launch_bounds__(PUSH_THREADS) k_lcs_move(const float4* __restrict__ pos, const float* __restrict__ vx,
-                                                           const float* __restrict__ vy, const float* __restrict__ vz,
-                                                           const int64_t* __restrict__ ts,
-                                                           const int64_t* __restrict__ tp,
-                                                           const int64_t* __restrict__ ts2,
-                                                           const int64_t* __restrict__ tp2,
-                                                           const uint32_t* __restrict__ inv, float4* __restrict__ pos2,
-                                                           float* __restrict__ vx2, float* __restrict__ vy2,
-                                                           float* __restrict__ vz2, const int* stray) {
-  extern __shared__ float4 wpos[];  // [rows][MOVE_WCOLS], then wvx, wvy, wvz
-  __shared__ int wlo;
+__device__ __forceinline__ void cpa16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+__global__ void __launch_bounds__(PUSH_THREADS, 1) k_lcs_move(const float4* __restrict__ pos,
+                                                              const float* __restrict__ vx,
+                                                              const float* __restrict__ vy,
+                                                              const float* __restrict__ vz,
+                                                              const int64_t* __restrict__ ts,
+                                                              const int64_t* __restrict__ tp,
+                                                              const int64_t* __restrict__ ts2,
+                                                              const int64_t* __restrict__ tp2,
+                                                              const uint32_t* __restrict__ inv, float4* __restrict__ pos2,
+                                                              float* __restrict__ vx2, float* __restrict__ vy2,
+                                                              float* __restrict__ vz2, const int* stray) {
+  extern __shared__ float4 msm[];  // two buffers: window pos, vx, vy, vz, then the group's inv
+  __shared__ int wlo[MOVE_GROUPS];
   if (*stray) return;
   const int t = blockIdx.x, tid = threadIdx.x;
   const int64_t nd = ts2[t + 1] - ts2[t];
@@ -364,63 +438,126 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_move(const float4* __restr
   const int64_t ns = ts[t + 1] - ts[t];
   const int Ls = (int)((ns + PUSH_THREADS - 1) / PUSH_THREADS);
   const int64_t sbase = tp[t], send = sbase + (int64_t)Ls * PUSH_THREADS;
-  const bool win = ns > 0 && Ls <= MOVE_MAXROWS;
-  float* wvx = reinterpret_cast<float*>(wpos + MOVE_MAXROWS * MOVE_WCOLS);
-  float* wvy = wvx + MOVE_MAXROWS * MOVE_WCOLS;
-  float* wvz = wvy + MOVE_MAXROWS * MOVE_WCOLS;
   const int64_t d0 = tp2[t];
-  for (int c0 = 0; c0 < PUSH_THREADS; c0 += 32) {
+  const bool win = ns > 0 && Ls <= MOVE_MAXROWS && al16(pos + sbase) && al16(vx + sbase) && al16(vy + sbase) &&
+                   al16(vz + sbase);
+  const bool sinv = Ld <= MOVE_MAXROWS && al16(inv + d0);
+  // the window of every group, from the old slot of the group's middle slot
+  if (win && tid < MOVE_GROUPS) {
+    const int c0 = tid * 32;
+    const uint32_t s = inv[d0 + (int64_t)(Ld / 2) * PUSH_THREADS + c0 + 16];
+    int col = c0 + 16;
+    if (s != DEAD && (int64_t)s >= sbase && (int64_t)s < send) col = (int)(((int64_t)s - sbase) % PUSH_THREADS);
+    wlo[tid] = min(max(col - MOVE_WCOLS / 2, 0), PUSH_THREADS - MOVE_WCOLS) & ~3;
+  }
+  __syncthreads();
+  auto stage = [&](int grp) {
+    char* buf = reinterpret_cast<char*>(msm) + (grp & 1) * MOVE_BUF;
+    float4* wpos = reinterpret_cast<float4*>(buf);
+    float* wv = reinterpret_cast<float*>(wpos + MOVE_WIN);
+    uint32_t* winv = reinterpret_cast<uint32_t*>(wv + 3 * MOVE_WIN);
     if (win) {
-      if (tid == 0) {
-        const uint32_t s = inv[d0 + (int64_t)(Ld / 2) * PUSH_THREADS + c0 + 16];
-        int col = c0 + 16;
-        if (s != DEAD && (int64_t)s >= sbase && (int64_t)s < send) col = (int)(((int64_t)s - sbase) % PUSH_THREADS);
-        wlo = min(max(col - MOVE_WCOLS / 2, 0), PUSH_THREADS - MOVE_WCOLS);
-      }
-      __syncthreads();
-      const int lo = wlo;
-#pragma unroll 4
+      const int lo = wlo[grp];
+      constexpr int VCH = MOVE_WCOLS / 4;  // 16-byte chunks of a velocity row
+      const float4* ps = pos + sbase + lo;
       for (int e = tid; e < Ls * MOVE_WCOLS; e += PUSH_THREADS) {
-        const int64_t gs = sbase + (int64_t)(e / MOVE_WCOLS) * PUSH_THREADS + lo + e % MOVE_WCOLS;
-        wpos[e] = pos[gs];
-        wvx[e] = vx[gs];
-        wvy[e] = vy[gs];
-        wvz[e] = vz[gs];
+        const int row = e / MOVE_WCOLS, col = e - row * MOVE_WCOLS;
+        cpa16(wpos + e, ps + row * PUSH_THREADS + col);
       }
-      __syncthreads();
+      const float* v3[3] = {vx + sbase + lo, vy + sbase + lo, vz + sbase + lo};
+#pragma unroll
+      for (int arr = 0; arr < 3; arr++)
+        for (int h = tid; h < Ls * VCH; h += PUSH_THREADS) {
+          const int row = h / VCH, ch = h - row * VCH;
+          cpa16(wv + arr * MOVE_WIN + row * MOVE_WCOLS + 4 * ch, v3[arr] + row * PUSH_THREADS + 4 * ch);
+        }
     }
-    const int lo = win ? wlo : 0;
-#pragma unroll 2
-    for (int e = tid; e < Ld * 32; e += PUSH_THREADS) {
-      const int64_t m = d0 + (int64_t)(e >> 5) * PUSH_THREADS + c0 + (e & 31);
-      const uint32_t src = inv[m];
-      float4 p;
-      float a, b, c;
-      if (src == DEAD) {
-        p = make_float4(0.f, 0.f, 0.f, __int_as_float((int)DEAD));
-        a = b = c = 0.f;
-      } else {
-        const int64_t rel = (int64_t)src - sbase;
-        const int cc = win && rel >= 0 && (int64_t)src < send ? (int)(rel % PUSH_THREADS) - lo : -1;
-        if (cc >= 0 && cc < MOVE_WCOLS) {
-          const int w = (int)(rel / PUSH_THREADS) * MOVE_WCOLS + cc;
-          p = wpos[w];
-          a = wvx[w];
-          b = wvy[w];
-          c = wvz[w];
-        } else {
-          p = pos[src];
-          a = vx[src];
-          b = vy[src];
-          c = vz[src];
+    if (sinv) {
+      const uint32_t* is = inv + d0 + grp * 32;
+      for (int e = tid; e < Ld * 8; e += PUSH_THREADS) {
+        const int row = e >> 3, ch = e & 7;
+        cpa16(winv + row * 32 + 4 * ch, is + row * PUSH_THREADS + 4 * ch);
+      }
+    }
+    cpa_commit();
+  };
+  stage(0);
+  for (int grp = 0; grp < MOVE_GROUPS; grp++) {
+    if (grp + 1 < MOVE_GROUPS) {
+      stage(grp + 1);
+      cpa_wait<1>();
+    } else {
+      cpa_wait<0>();
+    }
+    __syncthreads();
+    const char* buf = reinterpret_cast<const char*>(msm) + (grp & 1) * MOVE_BUF;
+    const float4* wpos = reinterpret_cast<const float4*>(buf);
+    const float* wvx = reinterpret_cast<const float*>(wpos + MOVE_WIN);
+    const float* wvy = wvx + MOVE_WIN;
+    const float* wvz = wvy + MOVE_WIN;
+    const uint32_t* winv = reinterpret_cast<const uint32_t*>(wvz + MOVE_WIN);
+    const int c0 = grp * 32;
+    const int lo = win ? wlo[grp] : 0;
+    // a thread's slots of the group (at most MOVE_K): every load is issued
+    // before the first store, so the particles gathered from global memory
+    // are in flight together
+    float4 p[MOVE_K];
+    float a[MOVE_K], b[MOVE_K], c[MOVE_K];
+#pragma unroll
+    for (int k = 0; k < MOVE_K; k++) {
+      const int e = tid + k * PUSH_THREADS;
+      p[k] = make_float4(0.f, 0.f, 0.f, __int_as_float((int)DEAD));
+      a[k] = b[k] = c[k] = 0.f;
+      if (e < Ld * 32) {
+        const uint32_t src = sinv ? winv[e] : inv[d0 + (int64_t)(e >> 5) * PUSH_THREADS + c0 + (e & 31)];
+        if (src != DEAD) {
+          // 32-bit offset into the old region (regions hold fewer than 2^31 slots)
+          const uint32_t rel = src - (uint32_t)sbase;
+          const int cc = win && rel < (uint32_t)(send - sbase) ? (int)(rel % PUSH_THREADS) - lo : -1;
+          if (cc >= 0 && cc < MOVE_WCOLS) {
+            const int w = (int)(rel / PUSH_THREADS) * MOVE_WCOLS + cc;
+            p[k] = wpos[w];
+            a[k] = wvx[w];
+            b[k] = wvy[w];
+            c[k] = wvz[w];
+          } else {
+            p[k] = pos[src];
+            a[k] = vx[src];
+            b[k] = vy[src];
+            c[k] = vz[src];
+          }
         }
       }
-      pos2[m] = p;
-      vx2[m] = a;
-      vy2[m] = b;
-      vz2[m] = c;
     }
-    if (win) __syncthreads();  // the window is reloaded for the next group
+#pragma unroll
+    for (int k = 0; k < MOVE_K; k++) {
+      const int e = tid + k * PUSH_THREADS;
+      if (e < Ld * 32) {
+        const int64_t m = d0 + (int64_t)(e >> 5) * PUSH_THREADS + c0 + (e & 31);
+        pos2[m] = p[k];
+        vx2[m] = a[k];
+        vy2[m] = b[k];
+        vz2[m] = c[k];
+      }
+    }
+    // rows beyond MOVE_MAXROWS (a tile whose window and inv are not staged)
+    for (int e = tid + MOVE_K * PUSH_THREADS; e < Ld * 32; e += PUSH_THREADS) {
+      const int64_t m = d0 + (int64_t)(e >> 5) * PUSH_THREADS + c0 + (e & 31);
+      const uint32_t src = inv[m];
+      float4 q = make_float4(0.f, 0.f, 0.f, __int_as_float((int)DEAD));
+      float x = 0.f, y = 0.f, z = 0.f;
+      if (src != DEAD) {
+        q = pos[src];
+        x = vx[src];
+        y = vy[src];
+        z = vz[src];
+      }
+      pos2[m] = q;
+      vx2[m] = x;
+      vy2[m] = y;
+      vz2[m] = z;
+    }
+    __syncthreads();  // this buffer is staged again for group grp + 2
   }
 }
 
