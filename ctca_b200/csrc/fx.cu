@@ -470,7 +470,10 @@ int fx_alloc(emsesg_ctx* ctx) {
     const int lsm = (int)(PUSH_WARPS * 10 * 10 * 10 * sizeof(uint32_t));
     EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_count, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
     EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
-    EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_move, cudaFuncAttributeMaxDynamicSharedMemorySize, move_smem()));
+    EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_move<MoveBig>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          move_smem<MoveBig>()));
+    EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_move<MoveSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          move_smem<MoveSmall>()));
   }
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(4)));
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(8)));
@@ -603,9 +606,16 @@ int fx_local_sort(emsesg_ctx* ctx, bool* done) {
     if (nt > 0)
       EMSESG_LAUNCH(ctx, "lcs_tail_inv", k_lcs_tail_inv, nblk(nt), 256, 0, tk, tv, nt, deadkey, (int)tcells,
                     f.lcs_celltot, ts2, tp2, f.lcs_inv + off, stray);
-    EMSESG_LAUNCH(ctx, "lcs_move", k_lcs_move, (unsigned)f.ntiles, PUSH_THREADS, move_smem(), f.pos + off,
-                  f.vx + off, f.vy + off, f.vz + off, f.tile_start + is * T1, f.tile_pad + is * T1, ts2, tp2,
-                  f.lcs_inv + off, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off, stray);
+    // the move's shape from the mean rows per tile (the host's count is an
+    // upper bound between synchronisations: escapes are not in it)
+    if (ctx->totalp[is] + nt <= (int64_t)MOVE_SMALL_ROWS * PUSH_THREADS * f.ntiles)
+      EMSESG_LAUNCH(ctx, "lcs_move", k_lcs_move<MoveSmall>, (unsigned)f.ntiles, PUSH_THREADS, move_smem<MoveSmall>(),
+                    f.pos + off, f.vx + off, f.vy + off, f.vz + off, f.tile_start + is * T1, f.tile_pad + is * T1, ts2,
+                    tp2, f.lcs_inv + off, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off, stray);
+    else
+      EMSESG_LAUNCH(ctx, "lcs_move", k_lcs_move<MoveBig>, (unsigned)f.ntiles, PUSH_THREADS, move_smem<MoveBig>(),
+                    f.pos + off, f.vx + off, f.vy + off, f.vz + off, f.tile_start + is * T1, f.tile_pad + is * T1, ts2,
+                    tp2, f.lcs_inv + off, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off, stray);
     if (f.capture)
       EMSESG_LAUNCH(ctx, "lcs_keep", k_lcs_keep, 4 * 148, 256, 0, stray, f.pos + off, f.vx + off, f.vy + off,
                     f.vz + off, f.tile_start + is * T1, f.tile_pad + is * T1, f.ntiles, f.pos2 + off, f.vx2 + off,

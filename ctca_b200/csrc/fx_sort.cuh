@@ -388,27 +388,48 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restr
   }
 }
 
-// move: the new region of destination tile t, in groups of 32 columns.  A
+// move: the new region of destination tile t, in groups of GW columns.  A
 // particle that stayed in its tile keeps about its column (its rank moves by
 // the net count change of the cells before it), so each group takes its
-// particles from a window of MOVE_WCOLS source columns (all rows of the
-// tile's old region), centred on the old column of the group's middle slot,
-// or, when one came from elsewhere, from global memory; the writes go row by
-// row (coalesced).  The window and the group's 32 columns of inv are staged
-// in shared memory with cp.async, double-buffered: group g+1's copies are in
-// flight while group g is written.  grid = ntiles, block = PUSH_THREADS (one
-// CTA per SM), shared = move_smem().
-constexpr int MOVE_WCOLS = 40;  // a multiple of 4: 16-byte rows of the velocity arrays
-constexpr int MOVE_MAXROWS = 80;
-constexpr int MOVE_GROUPS = PUSH_THREADS / 32;
-constexpr int MOVE_K = (MOVE_MAXROWS * 32 + PUSH_THREADS - 1) / PUSH_THREADS;  // slots of a thread per group
-constexpr int MOVE_WIN = MOVE_MAXROWS * MOVE_WCOLS;
-constexpr int MOVE_BUF = MOVE_WIN * (16 + 3 * 4) + MOVE_MAXROWS * 32 * 4;  // bytes of one buffer
-inline int move_smem() { return 2 * MOVE_BUF; }
-static_assert(MOVE_WCOLS % 4 == 0 && PUSH_THREADS % 32 == 0, "16-byte window rows");
+// particles from a window of GW + 8 source columns (all rows of the tile's
+// old region), centred on the old column of the group's middle slot, or,
+// when one came from elsewhere, from global memory; the writes go row by row
+// (coalesced).  The window and the group's columns of inv are staged in
+// shared memory with cp.async, double-buffered: group g+1's copies are in
+// flight while group g is written.  The group width is the widest of 32,
+// 96, 160 and 480 columns whose group fits the staged slots at the tile's
+// row count, so that a tile of few rows is moved in few groups.
+//
+// Two shapes (MoveBig, MoveSmall), picked per sort by the mean rows per
+// tile: tiles of many rows need big windows (80 rows: 200 KB of shared
+// memory, copies that skip L1); for tiles of at most 40 rows the buffers
+// take half that, and the copies go through L1, which then holds the
+// recent columns of the old region: the particles that changed cell along
+// z (whose rank moves by a z-layer, tens of columns) are found there.
+// grid = ntiles, block = PUSH_THREADS (one CTA per SM), shared =
+// 2 * Cfg::BUF.
+template <int WIN_, int SLOTS_, bool CA_>
+struct MoveCfg {
+  static constexpr int WIN = WIN_;      // window particles of one buffer
+  static constexpr int SLOTS = SLOTS_;  // slots of one group (staged inv)
+  static constexpr bool CA = CA_;       // copies cached in L1
+  static constexpr int K = (SLOTS + PUSH_THREADS - 1) / PUSH_THREADS;  // slots of a thread per group
+  static constexpr int BUF = WIN * (16 + 3 * 4) + SLOTS * 4;          // bytes of one buffer
+};
+using MoveBig = MoveCfg<3200, 2560, false>;   // up to 80 rows of 40 columns
+using MoveSmall = MoveCfg<1600, 1280, true>;  // up to 40 rows of 40 columns
+constexpr int MOVE_SMALL_ROWS = 32;           // mean rows per tile up to which MoveSmall is used
+constexpr int MOVE_MAXGROUPS = PUSH_THREADS / 32;
+template <class Cfg>
+inline int move_smem() { return 2 * Cfg::BUF; }
+static_assert(PUSH_THREADS == 480, "the group widths 32, 96, 160 and 480 divide the row");
 
+template <bool CA>
 __device__ __forceinline__ void cpa16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+  if (CA)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -417,38 +438,32 @@ __device__ __forceinline__ void cpa_wait() {
 }
 __device__ __forceinline__ bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
-__global__ void __launch_bounds__(PUSH_THREADS, 1) k_lcs_move(const float4* __restrict__ pos,
-                                                              const float* __restrict__ vx,
-                                                              const float* __restrict__ vy,
-                                                              const float* __restrict__ vz,
-                                                              const int64_t* __restrict__ ts,
-                                                              const int64_t* __restrict__ tp,
-                                                              const int64_t* __restrict__ ts2,
-                                                              const int64_t* __restrict__ tp2,
-                                                              const uint32_t* __restrict__ inv, float4* __restrict__ pos2,
-                                                              float* __restrict__ vx2, float* __restrict__ vy2,
-                                                              float* __restrict__ vz2, const int* stray) {
-  extern __shared__ float4 msm[];  // two buffers: window pos, vx, vy, vz, then the group's inv
-  __shared__ int wlo[MOVE_GROUPS];
-  if (*stray) return;
-  const int t = blockIdx.x, tid = threadIdx.x;
-  const int64_t nd = ts2[t + 1] - ts2[t];
-  if (nd <= 0) return;
-  const int Ld = (int)((nd + PUSH_THREADS - 1) / PUSH_THREADS);
-  const int64_t ns = ts[t + 1] - ts[t];
-  const int Ls = (int)((ns + PUSH_THREADS - 1) / PUSH_THREADS);
-  const int64_t sbase = tp[t], send = sbase + (int64_t)Ls * PUSH_THREADS;
-  const int64_t d0 = tp2[t];
-  const bool win = ns > 0 && Ls <= MOVE_MAXROWS && al16(pos + sbase) && al16(vx + sbase) && al16(vy + sbase) &&
+// One destination tile with groups of GW columns (see k_lcs_move).
+template <class Cfg, int GW>
+__device__ __forceinline__ void move_tile(const float4* __restrict__ pos, const float* __restrict__ vx,
+                                          const float* __restrict__ vy, const float* __restrict__ vz,
+                                          const uint32_t* __restrict__ inv, float4* __restrict__ pos2,
+                                          float* __restrict__ vx2, float* __restrict__ vy2, float* __restrict__ vz2,
+                                          int Ld, int Ls, int64_t sbase, int64_t d0, bool any_src, float4* msm,
+                                          int* wlo) {
+  constexpr int WC = GW + 8 < PUSH_THREADS ? GW + 8 : PUSH_THREADS;  // window columns, a multiple of 4
+  constexpr int NG = PUSH_THREADS / GW;
+  constexpr int VCH = WC / 4;  // 16-byte chunks of a velocity row
+  constexpr int GCH = GW / 4;  // 16-byte chunks of a group's inv row
+  static_assert(PUSH_THREADS % GW == 0 && WC % 4 == 0 && GW % 32 == 0, "group shape");
+  const int tid = threadIdx.x;
+  const int64_t send = sbase + (int64_t)Ls * PUSH_THREADS;
+  constexpr int MOVE_WIN = Cfg::WIN, MOVE_K = Cfg::K, MOVE_BUF = Cfg::BUF;
+  const bool win = any_src && Ls * WC <= MOVE_WIN && al16(pos + sbase) && al16(vx + sbase) && al16(vy + sbase) &&
                    al16(vz + sbase);
-  const bool sinv = Ld <= MOVE_MAXROWS && al16(inv + d0);
+  const bool sinv = Ld * GW <= Cfg::SLOTS && al16(inv + d0);
   // the window of every group, from the old slot of the group's middle slot
-  if (win && tid < MOVE_GROUPS) {
-    const int c0 = tid * 32;
-    const uint32_t s = inv[d0 + (int64_t)(Ld / 2) * PUSH_THREADS + c0 + 16];
-    int col = c0 + 16;
+  if (win && tid < NG) {
+    const int c0 = tid * GW;
+    const uint32_t s = inv[d0 + (int64_t)(Ld / 2) * PUSH_THREADS + c0 + GW / 2];
+    int col = c0 + GW / 2;
     if (s != DEAD && (int64_t)s >= sbase && (int64_t)s < send) col = (int)(((int64_t)s - sbase) % PUSH_THREADS);
-    wlo[tid] = min(max(col - MOVE_WCOLS / 2, 0), PUSH_THREADS - MOVE_WCOLS) & ~3;
+    wlo[tid] = min(max(col - WC / 2, 0), PUSH_THREADS - WC) & ~3;
   }
   __syncthreads();
   auto stage = [&](int grp) {
@@ -458,32 +473,31 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_lcs_move(const float4* __re
     uint32_t* winv = reinterpret_cast<uint32_t*>(wv + 3 * MOVE_WIN);
     if (win) {
       const int lo = wlo[grp];
-      constexpr int VCH = MOVE_WCOLS / 4;  // 16-byte chunks of a velocity row
       const float4* ps = pos + sbase + lo;
-      for (int e = tid; e < Ls * MOVE_WCOLS; e += PUSH_THREADS) {
-        const int row = e / MOVE_WCOLS, col = e - row * MOVE_WCOLS;
-        cpa16(wpos + e, ps + row * PUSH_THREADS + col);
+      for (int e = tid; e < Ls * WC; e += PUSH_THREADS) {
+        const int row = e / WC, col = e - row * WC;
+        cpa16<Cfg::CA>(wpos + e, ps + row * PUSH_THREADS + col);
       }
       const float* v3[3] = {vx + sbase + lo, vy + sbase + lo, vz + sbase + lo};
 #pragma unroll
       for (int arr = 0; arr < 3; arr++)
         for (int h = tid; h < Ls * VCH; h += PUSH_THREADS) {
           const int row = h / VCH, ch = h - row * VCH;
-          cpa16(wv + arr * MOVE_WIN + row * MOVE_WCOLS + 4 * ch, v3[arr] + row * PUSH_THREADS + 4 * ch);
+          cpa16<Cfg::CA>(wv + arr * MOVE_WIN + row * WC + 4 * ch, v3[arr] + row * PUSH_THREADS + 4 * ch);
         }
     }
     if (sinv) {
-      const uint32_t* is = inv + d0 + grp * 32;
-      for (int e = tid; e < Ld * 8; e += PUSH_THREADS) {
-        const int row = e >> 3, ch = e & 7;
-        cpa16(winv + row * 32 + 4 * ch, is + row * PUSH_THREADS + 4 * ch);
+      const uint32_t* is = inv + d0 + grp * GW;
+      for (int e = tid; e < Ld * GCH; e += PUSH_THREADS) {
+        const int row = e / GCH, ch = e - row * GCH;
+        cpa16<Cfg::CA>(winv + row * GW + 4 * ch, is + row * PUSH_THREADS + 4 * ch);
       }
     }
     cpa_commit();
   };
   stage(0);
-  for (int grp = 0; grp < MOVE_GROUPS; grp++) {
-    if (grp + 1 < MOVE_GROUPS) {
+  for (int grp = 0; grp < NG; grp++) {
+    if (grp + 1 < NG) {
       stage(grp + 1);
       cpa_wait<1>();
     } else {
@@ -496,69 +510,88 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_lcs_move(const float4* __re
     const float* wvy = wvx + MOVE_WIN;
     const float* wvz = wvy + MOVE_WIN;
     const uint32_t* winv = reinterpret_cast<const uint32_t*>(wvz + MOVE_WIN);
-    const int c0 = grp * 32;
+    const int64_t g0 = d0 + grp * GW;
     const int lo = win ? wlo[grp] : 0;
-    // a thread's slots of the group (at most MOVE_K): every load is issued
-    // before the first store, so the particles gathered from global memory
-    // are in flight together
-    float4 p[MOVE_K];
-    float a[MOVE_K], b[MOVE_K], c[MOVE_K];
+    // MOVE_K slots of a thread at a time (all of the group's when its inv is
+    // staged): every load is issued before the first store, so the
+    // particles gathered from global memory are in flight together
+    for (int e0 = 0; e0 < Ld * GW; e0 += MOVE_K * PUSH_THREADS) {
+      float4 p[MOVE_K];
+      float a[MOVE_K], b[MOVE_K], c[MOVE_K];
 #pragma unroll
-    for (int k = 0; k < MOVE_K; k++) {
-      const int e = tid + k * PUSH_THREADS;
-      p[k] = make_float4(0.f, 0.f, 0.f, __int_as_float((int)DEAD));
-      a[k] = b[k] = c[k] = 0.f;
-      if (e < Ld * 32) {
-        const uint32_t src = sinv ? winv[e] : inv[d0 + (int64_t)(e >> 5) * PUSH_THREADS + c0 + (e & 31)];
-        if (src != DEAD) {
-          // 32-bit offset into the old region (regions hold fewer than 2^31 slots)
-          const uint32_t rel = src - (uint32_t)sbase;
-          const int cc = win && rel < (uint32_t)(send - sbase) ? (int)(rel % PUSH_THREADS) - lo : -1;
-          if (cc >= 0 && cc < MOVE_WCOLS) {
-            const int w = (int)(rel / PUSH_THREADS) * MOVE_WCOLS + cc;
-            p[k] = wpos[w];
-            a[k] = wvx[w];
-            b[k] = wvy[w];
-            c[k] = wvz[w];
-          } else {
-            p[k] = pos[src];
-            a[k] = vx[src];
-            b[k] = vy[src];
-            c[k] = vz[src];
+      for (int k = 0; k < MOVE_K; k++) {
+        const int e = e0 + tid + k * PUSH_THREADS;
+        p[k] = make_float4(0.f, 0.f, 0.f, __int_as_float((int)DEAD));
+        a[k] = b[k] = c[k] = 0.f;
+        if (e < Ld * GW) {
+          const int row = e / GW;
+          const uint32_t src = sinv ? winv[e] : inv[g0 + (int64_t)row * PUSH_THREADS + (e - row * GW)];
+          if (src != DEAD) {
+            // 32-bit offset into the old region (regions hold fewer than 2^31 slots)
+            const uint32_t rel = src - (uint32_t)sbase;
+            const int cc = win && rel < (uint32_t)(send - sbase) ? (int)(rel % PUSH_THREADS) - lo : -1;
+            if (cc >= 0 && cc < WC) {
+              const int w = (int)(rel / PUSH_THREADS) * WC + cc;
+              p[k] = wpos[w];
+              a[k] = wvx[w];
+              b[k] = wvy[w];
+              c[k] = wvz[w];
+            } else {
+              p[k] = pos[src];
+              a[k] = vx[src];
+              b[k] = vy[src];
+              c[k] = vz[src];
+            }
           }
         }
       }
-    }
 #pragma unroll
-    for (int k = 0; k < MOVE_K; k++) {
-      const int e = tid + k * PUSH_THREADS;
-      if (e < Ld * 32) {
-        const int64_t m = d0 + (int64_t)(e >> 5) * PUSH_THREADS + c0 + (e & 31);
-        pos2[m] = p[k];
-        vx2[m] = a[k];
-        vy2[m] = b[k];
-        vz2[m] = c[k];
+      for (int k = 0; k < MOVE_K; k++) {
+        const int e = e0 + tid + k * PUSH_THREADS;
+        if (e < Ld * GW) {
+          const int row = e / GW;
+          const int64_t m = g0 + (int64_t)row * PUSH_THREADS + (e - row * GW);
+          pos2[m] = p[k];
+          vx2[m] = a[k];
+          vy2[m] = b[k];
+          vz2[m] = c[k];
+        }
       }
-    }
-    // rows beyond MOVE_MAXROWS (a tile whose window and inv are not staged)
-    for (int e = tid + MOVE_K * PUSH_THREADS; e < Ld * 32; e += PUSH_THREADS) {
-      const int64_t m = d0 + (int64_t)(e >> 5) * PUSH_THREADS + c0 + (e & 31);
-      const uint32_t src = inv[m];
-      float4 q = make_float4(0.f, 0.f, 0.f, __int_as_float((int)DEAD));
-      float x = 0.f, y = 0.f, z = 0.f;
-      if (src != DEAD) {
-        q = pos[src];
-        x = vx[src];
-        y = vy[src];
-        z = vz[src];
-      }
-      pos2[m] = q;
-      vx2[m] = x;
-      vy2[m] = y;
-      vz2[m] = z;
     }
     __syncthreads();  // this buffer is staged again for group grp + 2
   }
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(PUSH_THREADS, 1) k_lcs_move(const float4* __restrict__ pos,
+                                                              const float* __restrict__ vx,
+                                                              const float* __restrict__ vy,
+                                                              const float* __restrict__ vz,
+                                                              const int64_t* __restrict__ ts,
+                                                              const int64_t* __restrict__ tp,
+                                                              const int64_t* __restrict__ ts2,
+                                                              const int64_t* __restrict__ tp2,
+                                                              const uint32_t* __restrict__ inv, float4* __restrict__ pos2,
+                                                              float* __restrict__ vx2, float* __restrict__ vy2,
+                                                              float* __restrict__ vz2, const int* stray) {
+  extern __shared__ float4 msm[];  // two buffers: window pos, vx, vy, vz, then the group's inv
+  __shared__ int wlo[MOVE_MAXGROUPS];
+  if (*stray) return;
+  const int t = blockIdx.x;
+  const int64_t nd = ts2[t + 1] - ts2[t];
+  if (nd <= 0) return;
+  const int Ld = (int)((nd + PUSH_THREADS - 1) / PUSH_THREADS);
+  const int64_t ns = ts[t + 1] - ts[t];
+  const int Ls = (int)((ns + PUSH_THREADS - 1) / PUSH_THREADS);
+  const int R = max(Ls, Ld);
+  if (R * 480 <= Cfg::SLOTS)
+    move_tile<Cfg, 480>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
+  else if (R * 160 <= Cfg::SLOTS)
+    move_tile<Cfg, 160>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
+  else if (R * 96 <= Cfg::SLOTS)
+    move_tile<Cfg, 96>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
+  else
+    move_tile<Cfg, 32>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
 }
 
 // Inside a CUDA graph the host cannot switch to the radix sort when a
