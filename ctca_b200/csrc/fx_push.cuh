@@ -231,6 +231,19 @@ struct BoxT {
 
 __device__ __forceinline__ long long to_fix(float v, float scale) { return __float2ll_rn(v * scale); }
 
+// Adds v to a 64-bit accumulator in shared memory with 32-bit atomics (a
+// 64-bit shared-memory atomic add is much slower): the low word first, its
+// carry out then goes with the high word.  The carries counted by all
+// additions add up to the wraps of the low word, so the final value is the
+// 64-bit sum in any order; only the final value is read.
+__device__ __forceinline__ void box_add(unsigned long long* p, unsigned long long v) {
+  unsigned int* w = reinterpret_cast<unsigned int*>(p);  // little-endian: low word first
+  const unsigned int lo = (unsigned int)v, hi = (unsigned int)(v >> 32);
+  const unsigned int old = atomicAdd(w, lo);
+  const unsigned int h = hi + (old + lo < old ? 1u : 0u);
+  if (h) atomicAdd(w + 1, h);
+}
+
 // Global arrays for deposits whose cell lies outside the tile box.
 struct Sink {
   unsigned long long* acc_rho;
@@ -290,7 +303,7 @@ __device__ __forceinline__ void put_j(unsigned long long* box, const int (&o)[3]
   const int base = box_base<B>(o, i, j, k);
   if (base >= 0) {
 #pragma unroll
-    for (int q = 0; q < NJ; q++) atomicAdd(&box[base + BoxT<B>::joff(q)], (unsigned long long)to_fix(v[q], qfix));
+    for (int q = 0; q < NJ; q++) box_add(&box[base + BoxT<B>::joff(q)], (unsigned long long)to_fix(v[q], qfix));
   } else {
     V12 w;
 #pragma unroll
@@ -305,7 +318,7 @@ __device__ __forceinline__ void put_r(unsigned long long* box, const int (&o)[3]
   const int base = box_base<B>(o, i, j, k);
   if (base >= 0) {
 #pragma unroll
-    for (int r = 0; r < NR; r++) atomicAdd(&box[base + BoxT<B>::roff(r)], (unsigned long long)to_fix(v[r], qfix));
+    for (int r = 0; r < NR; r++) box_add(&box[base + BoxT<B>::roff(r)], (unsigned long long)to_fix(v[r], qfix));
   } else {
     V8 w;
 #pragma unroll
@@ -411,7 +424,7 @@ __device__ __forceinline__ void drain_runs(unsigned long long* box, const int* s
     const float* en = q + e * RQW;
     const int base = __float_as_int(en[NJ + NR]);
     const long long f = to_fix(en[sl], qfix);
-    if (f) atomicAdd(&box[base + slot_off[sl]], (unsigned long long)f);
+    if (f) box_add(&box[base + slot_off[sl]], (unsigned long long)f);
     // m += 32: 32 = 1 * 20 + 12
     sl += 32 - (NJ + NR);
     e += 1;
