@@ -60,8 +60,17 @@ struct AdjWork;  // reverse-mode workspace (fx.cu), kept between calls
 struct FxState;
 void adj_free(FxState& f);
 
+// Arrays a move-only step reads instead of the live ones (see FxPushArgs).
+struct FxSrc {
+  const float4* pos = nullptr;
+  const float* vx = nullptr;
+  const float* vy = nullptr;
+  const float* vz = nullptr;
+};
+
 struct FxState {
   bool loaded = false;
+  FxSrc move_src;          // set around the adjoint's recompute steps only
   float4* pos = nullptr;   // {ox, oy, oz, __int_as_float(cell)}
   float* vx = nullptr;
   float* vy = nullptr;

@@ -877,6 +877,10 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   int smem = fx_push_smem(tmax);
   FxPushArgs a{};
   a.pos = f.pos; a.vx = f.vx; a.vy = f.vy; a.vz = f.vz;
+  a.rpos = f.pos; a.rvx = f.vx; a.rvy = f.vy; a.rvz = f.vz;
+  if (!deposit && f.move_src.pos) {
+    a.rpos = f.move_src.pos; a.rvx = f.move_src.vx; a.rvy = f.move_src.vy; a.rvz = f.move_src.vz;
+  }
   a.tile_start = f.tile_start;
   a.tile_pad = f.tile_pad;
   a.chunk_start = f.chunk_start;
@@ -1277,16 +1281,20 @@ int adj_reserve(emsesg_ctx* ctx, AdjWork& w, int nseg, int ckpt, int jsteps, int
   return EMSESG_OK;
 }
 
-int snap_copy(emsesg_ctx* ctx, bool save, FxSnap& sn, int64_t cap, int64_t nl) {
+// Copies the live state into sn (save) or back; without `particles` only
+// the tile starts and counts.
+int snap_copy(emsesg_ctx* ctx, bool save, FxSnap& sn, int64_t cap, int64_t nl, bool particles = true) {
   FxState& f = ctx->fx;
   const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
   cudaStream_t st = ctx->stream;
 #define EMSESG_SNAP(dst, src, bytes) EMSESG_CUDA(ctx, cudaMemcpyAsync(save ? (void*)(dst) : (void*)(src), \
                                                  save ? (const void*)(src) : (const void*)(dst), bytes, k, st))
-  EMSESG_SNAP(sn.pos, f.pos, cap * sizeof(float4));
-  EMSESG_SNAP(sn.vx, f.vx, cap * sizeof(float));
-  EMSESG_SNAP(sn.vy, f.vy, cap * sizeof(float));
-  EMSESG_SNAP(sn.vz, f.vz, cap * sizeof(float));
+  if (particles) {
+    EMSESG_SNAP(sn.pos, f.pos, cap * sizeof(float4));
+    EMSESG_SNAP(sn.vx, f.vx, cap * sizeof(float));
+    EMSESG_SNAP(sn.vy, f.vy, cap * sizeof(float));
+    EMSESG_SNAP(sn.vz, f.vz, cap * sizeof(float));
+  }
   EMSESG_SNAP(sn.ts, f.tile_start, nl * sizeof(int64_t));
   EMSESG_SNAP(sn.tp, f.tile_pad, nl * sizeof(int64_t));
   EMSESG_SNAP(sn.counts, f.count_d, EMSESG_ISPEC * sizeof(int64_t));
@@ -1294,6 +1302,43 @@ int snap_copy(emsesg_ctx* ctx, bool save, FxSnap& sn, int64_t cap, int64_t nl) {
 #undef EMSESG_SNAP
   return EMSESG_OK;
 }
+
+// Puts the arrays o / o2 back into a / a2 (the live and the sort buffer),
+// taking them from whichever holder (live, sort buffer, a segment state)
+// has them: the recompute steps of the adjoint pass arrays around.
+template <class T>
+void reclaim(T*& a, T*& a2, T* o, T* o2, std::vector<FxSnap>& seg, T* FxSnap::*mem) {
+  auto take = [&](T*& slot, T* want) {
+    if (slot == want) return;
+    if (a == want) { std::swap(slot, a); return; }
+    if (a2 == want) { std::swap(slot, a2); return; }
+    for (FxSnap& s : seg)
+      if (s.*mem == want) { std::swap(slot, s.*mem); return; }
+  };
+  take(a, o);
+  take(a2, o2);
+}
+
+// The particle arrays of the context as they were when the adjoint began;
+// given back to their owners on every way out (the context frees them, and
+// captured graphs hold their addresses).
+struct ArrayOwners {
+  FxState& f;
+  std::vector<FxSnap>& seg;
+  float4 *p0, *p1;
+  float *x0, *x1, *y0, *y1, *z0, *z1;
+  ArrayOwners(FxState& f_, std::vector<FxSnap>& s)
+      : f(f_), seg(s), p0(f_.pos), p1(f_.pos2), x0(f_.vx), x1(f_.vx2), y0(f_.vy), y1(f_.vy2), z0(f_.vz),
+        z1(f_.vz2) {}
+  void give_back() {
+    f.move_src = FxSrc{};
+    reclaim(f.pos, f.pos2, p0, p1, seg, &FxSnap::pos);
+    reclaim(f.vx, f.vx2, x0, x1, seg, &FxSnap::vx);
+    reclaim(f.vy, f.vy2, y0, y1, seg, &FxSnap::vy);
+    reclaim(f.vz, f.vz2, z0, z1, seg, &FxSnap::vz);
+  }
+  ~ArrayOwners() { give_back(); }
+};
 
 }  // namespace
 
@@ -1342,6 +1387,7 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
   float* const gEd = w.gEd;
   float* const gBd = w.gBd;
   double* const lossd = w.lossd;
+  ArrayOwners owners(f, seg);
 #define EMSESG_ADJ(call) do { rc = (call); if (rc) return rc; } while (0)
   EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(lossd, 0, sizeof(double), ctx->stream), "adjoint loss"));
   // forward: K steps with a checkpoint every ckpt steps, the loss on the way
@@ -1379,11 +1425,21 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
     bool sorted[64] = {false};
     for (int j = 0; j < ckpt; j++) {
       const int n = sgi * ckpt + j;
-      EMSESG_ADJ(snap_copy(ctx, true, seg[(size_t)j], cap, nl));
+      // the state before step n is kept in seg[j]: its particle arrays take
+      // the live ones (no copy), and the move-only step reads them and
+      // writes the arrays seg[j] gave up
+      FxSnap& sj = seg[(size_t)j];
+      EMSESG_ADJ(snap_copy(ctx, true, sj, cap, nl, false));
+      std::swap(f.pos, sj.pos);
+      std::swap(f.vx, sj.vx);
+      std::swap(f.vy, sj.vy);
+      std::swap(f.vz, sj.vz);
+      f.move_src = FxSrc{sj.pos, sj.vx, sj.vy, sj.vz};
       const bool srt = (n + 1) % sort_every == 0;
       // slots past the new regions keep no map from an earlier sort
       if (srt) EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(f.lcs_inv, 0xFF, cap * sizeof(uint32_t), ctx->stream), "inv"));
       EMSESG_ADJ(fx_step_impl(ctx, ustep, srt ? 1 : 0, false));
+      f.move_src = FxSrc{};
       if (srt && j < 64) {
         if (!inv[(size_t)j]) EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&inv[(size_t)j], cap * sizeof(uint32_t)), "inv"));
         EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(inv[(size_t)j], f.lcs_inv, cap * sizeof(uint32_t),
@@ -1453,6 +1509,7 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
                                              ctx->stream), "gB"));
   EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(loss, lossd, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
                         "loss"));
+  owners.give_back();
   EMSESG_ADJ(snap_copy(ctx, false, ck[(size_t)nseg], cap, nl));
   EMSESG_ADJ(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "sync"));
   double s0[6] = {0, 0, 0, 0, 0, 0};

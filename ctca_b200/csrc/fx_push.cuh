@@ -65,10 +65,14 @@ struct Bodies {
 };
 
 struct FxPushArgs {
-  float4* pos;                  // all species regions
+  float4* pos;                  // all species regions (the step's result)
   float* vx;
   float* vy;
   float* vz;
+  const float4* rpos;           // the state read (the same arrays, or for a
+  const float* rvx;             // move-only step, those of a kept copy)
+  const float* rvy;
+  const float* rvz;
   const int64_t* tile_start;    // [nspec][ntiles+1] sorted ranks (live particles)
   const int64_t* tile_pad;      // [nspec][ntiles+1] slot offsets of the padded regions
   const int64_t* chunk_start;   // [nspec][ntiles+1] first CTA (row chunk) of each tile
@@ -601,7 +605,7 @@ __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t s
   int dead = 0;
   for (int e = lane; e < xn; e += 32) {
     const int loc = xl[e];
-    const float4 ps = c.gpos[loc];
+    const float4 ps = a.rpos[slot0 + loc];  // the position before the step
     const float vx = c.gvx[loc], vy = c.gvy[loc], vz = c.gvz[loc];
     const float en[XQW] = {__int_as_float(loc), ps.w, ps.x, ps.y, ps.z, vx, vy, vz};
     dead += cross_one<B, DEP>(g, box, o, sk, c, en);
@@ -665,6 +669,10 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   float* gvx = a.vx + slot0;
   float* gvy = a.vy + slot0;
   float* gvz = a.vz + slot0;
+  const float4* rgpos = a.rpos + slot0;
+  const float* rgvx = a.rvx + slot0;
+  const float* rgvy = a.rvy + slot0;
+  const float* rgvz = a.rvz + slot0;
 
   if (tid == 0) {
     for (int s = 0; s < NSTAGE; s++) {
@@ -704,10 +712,10 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
         }
         mbar_expect_tx(&full_bar[s], ROW_BYTES);
         const int64_t ro = (int64_t)r * PUSH_THREADS;
-        bulk_g2s(stpos + s * PUSH_THREADS, gpos + ro, PUSH_THREADS * 16, &full_bar[s]);
-        bulk_g2s(stvx + s * PUSH_THREADS, gvx + ro, PUSH_THREADS * 4, &full_bar[s]);
-        bulk_g2s(stvy + s * PUSH_THREADS, gvy + ro, PUSH_THREADS * 4, &full_bar[s]);
-        bulk_g2s(stvz + s * PUSH_THREADS, gvz + ro, PUSH_THREADS * 4, &full_bar[s]);
+        bulk_g2s(stpos + s * PUSH_THREADS, rgpos + ro, PUSH_THREADS * 16, &full_bar[s]);
+        bulk_g2s(stvx + s * PUSH_THREADS, rgvx + ro, PUSH_THREADS * 4, &full_bar[s]);
+        bulk_g2s(stvy + s * PUSH_THREADS, rgvy + ro, PUSH_THREADS * 4, &full_bar[s]);
+        bulk_g2s(stvz + s * PUSH_THREADS, rgvz + ro, PUSH_THREADS * 4, &full_bar[s]);
         issued = r + 1;
       }
     }
@@ -856,6 +864,14 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     if (act) {
       const int m = r * PUSH_THREADS + tid;
       if (simple || oop) gpos[m] = make_float4(sx, syy, szz, ps.w);
+      gvx[m] = vx;
+      gvy[m] = vy;
+      gvz[m] = vz;
+    } else if (!DEP) {
+      // a move-only step may write into other arrays than it reads: empty
+      // and dead slots are carried over
+      const int m = r * PUSH_THREADS + tid;
+      gpos[m] = ps;
       gvx[m] = vx;
       gvy[m] = vy;
       gvz[m] = vz;
