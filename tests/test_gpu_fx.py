@@ -138,14 +138,23 @@ def _tile_key(cfg, tile, p):
     return tid * (tile[0] * tile[1] * tile[2]) + lin, tid
 
 
-@pytest.mark.parametrize("npbnd,tile", [((0, 0, 0), (8, 8, 8)), ((1, 2, 0), (8, 4, 8))])
-def test_fx_local_sort_is_a_stable_cell_sort(gpu, npbnd, tile):
+@pytest.mark.parametrize("npbnd,tile,ppc", [
+    ((0, 0, 0), (8, 8, 8), (8, 8)),
+    ((1, 2, 0), (8, 4, 8), (8, 8)),
+    # tiles of 43 rows: the move's large shape with 40-column windows; and
+    # of 1 row: one group of all 480 columns
+    ((0, 0, 0), (8, 8, 8), (40, 1)),
+    # tiles of 103 rows: no window, inv read from global memory, several
+    # batches of slots per group
+    ((0, 0, 0), (8, 8, 8), (96, 4)),
+])
+def test_fx_local_sort_is_a_stable_cell_sort(gpu, npbnd, tile, ppc):
     """The re-sort after a step (the tile-local counting sort) orders the
     live particles by the tile-major cell key; equal cells keep the order
     (source tile, warp, row, lane) of the thread-major layout of the last
     sort, computed here from the tile sizes of that sort."""
     threads = FX_ROW_SLOTS
-    c = case(n=(16, 16, 16), ppc=(8, 8), npbnd=npbnd, vth_scale=6.0, tile=tile)
+    c = case(n=(16, 16, 16), ppc=ppc, npbnd=npbnd, vth_scale=6.0, tile=tile)
     cfg, eb, p, tp = build(c)
     g = Emses(cfg)
     g.upload_particles(p, tp)
