@@ -1046,24 +1046,32 @@ __global__ void k_gen_emit(emsesg_particle* out, int32_t* ord, int64_t n, int ne
 }
 
 // Inflow through a z face (psuper2.F90:236-292), preside 0.
-__global__ void k_gen_inflow_z(emsesg_particle* out, int32_t* ord, int64_t n, int front, int nx, int ny, int nz,
-                               const double* __restrict__ vzt, const double* __restrict__ vxt,
-                               const double* __restrict__ vyt, int npr, double injctisw, uint64_t seed,
-                               uint64_t stream, uint64_t index0, int spec) {
+// Inflow through the lower (front) or upper face of `axis`
+// (psuper2.F90:114-292): u2, u3, u4 give x, y, z -- uniform on the face
+// along the tangential axes; along the normal the distance vn * injctisw * u
+// from the face.  vnt: normal speeds [int(npr*u0)]; vat / vbt: the
+// tangential ones of the two other axes in increasing order [int(npr*u1)].
+__global__ void k_gen_inflow(emsesg_particle* out, int32_t* ord, int64_t n, int axis, int front, int nx, int ny,
+                             int nz, const double* __restrict__ vnt, const double* __restrict__ vat,
+                             const double* __restrict__ vbt, int npr, double injctisw, uint64_t seed,
+                             uint64_t stream, uint64_t index0, int spec) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   double u[5];
   for (int c = 0; c < 5; c++) u[c] = hash_u01(seed, stream, (index0 + (uint64_t)k) * 5 + c);
   const int a1 = (int)(npr * u[0]), a2 = (int)(npr * u[1]);
+  const int ext[3] = {nx, ny, nz};
+  double x[3], v[3];
+  for (int d = 0; d < 3; d++) x[d] = __dadd_rn(0.0, __dmul_rn((double)ext[d], u[2 + d]));
+  const double vn = vnt[a1];
+  const double dn = __dmul_rn(__dmul_rn(vn, injctisw), u[2 + axis]);
+  x[axis] = front ? dn : __dadd_rn((double)ext[axis], dn);
+  v[axis] = vn;
+  v[axis == 0 ? 1 : 0] = vat[a2];
+  v[axis == 2 ? 1 : 2] = vbt[a2];
   emsesg_particle p;
-  p.x = __dadd_rn(0.0, __dmul_rn((double)nx, u[2]));
-  p.y = __dadd_rn(0.0, __dmul_rn((double)ny, u[3]));
-  const double vz = vzt[a1];
-  const double dz = __dmul_rn(__dmul_rn(vz, injctisw), u[4]);
-  p.z = front ? dz : __dadd_rn((double)nz, dz);
-  p.vx = vxt[a2];
-  p.vy = vyt[a2];
-  p.vz = vz;
+  p.x = x[0]; p.y = x[1]; p.z = x[2];
+  p.vx = v[0]; p.vy = v[1]; p.vz = v[2];
   p.pid = 0; p.preside = 0; p.nid = 0; p.spec = spec;
   out[k] = p;
   ord[k] = 0;
@@ -1146,21 +1154,29 @@ extern "C" int emsesg_fx_emit(emsesg_ctx* ctx, int spec, int nemd, double grd, c
   return inject_staged(ctx, is, 2 * n, pending + n);
 }
 
-extern "C" int emsesg_fx_inflow_z(emsesg_ctx* ctx, int spec, int front, int64_t n, const double* vz_t,
-                                  const double* vx_t, const double* vy_t, int npr, double injctisw, uint64_t seed,
-                                  uint64_t stream, uint64_t index0) {
-  int rc = inject_check(ctx, spec, n, npr, vz_t, vx_t, vy_t);
+extern "C" int emsesg_fx_inflow(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n, const double* vn_t,
+                                const double* va_t, const double* vb_t, int npr, double injctisw, uint64_t seed,
+                                uint64_t stream, uint64_t index0) {
+  int rc = inject_check(ctx, spec, n, npr, vn_t, va_t, vb_t);
   if (rc) return rc;
+  if (axis < 0 || axis > 2) return set_error(ctx, EMSESG_ERR_ARG, "inflow axis %d (0, 1 or 2)", axis);
   if (n == 0) return EMSESG_OK;
   const int is = spec - 1;
   FxState& f = ctx->fx;
   if ((rc = inject_reserve(ctx, is, n))) return rc;
-  const double* tabs[3] = {vz_t, vx_t, vy_t};
+  const double* tabs[3] = {vn_t, va_t, vb_t};
   if ((rc = inject_tables(ctx, 3, npr, tabs))) return rc;
   const emsesg_config& c = ctx->cfg;
-  EMSESG_LAUNCH(ctx, "fx_gen_inflow", k_gen_inflow_z, nblk(n), 256, 0, f.stage, f.stage_ord, n, front, c.nx, c.ny,
-                c.nz, f.inj_tab, f.inj_tab + npr, f.inj_tab + 2 * npr, npr, injctisw, seed, stream, index0, spec);
+  EMSESG_LAUNCH(ctx, "fx_gen_inflow", k_gen_inflow, nblk(n), 256, 0, f.stage, f.stage_ord, n, axis, front, c.nx,
+                c.ny, c.nz, f.inj_tab, f.inj_tab + npr, f.inj_tab + 2 * npr, npr, injctisw, seed, stream, index0,
+                spec);
   return inject_staged(ctx, is, n, f.pending[is]);
+}
+
+extern "C" int emsesg_fx_inflow_z(emsesg_ctx* ctx, int spec, int front, int64_t n, const double* vz_t,
+                                  const double* vx_t, const double* vy_t, int npr, double injctisw, uint64_t seed,
+                                  uint64_t stream, uint64_t index0) {
+  return emsesg_fx_inflow(ctx, spec, 2, front, n, vz_t, vx_t, vy_t, npr, injctisw, seed, stream, index0);
 }
 
 extern "C" int emsesg_fx_surface(emsesg_ctx* ctx, int64_t* counts, int64_t* nsurf) {

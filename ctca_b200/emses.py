@@ -145,6 +145,8 @@ _SIGS = {
                             ctypes.c_uint64, ctypes.c_uint64]),
     "emsesg_fx_inflow_z": (_I, [_P, _I, _I, ctypes.c_int64, _P, _P, _P, _I, ctypes.c_double, ctypes.c_uint64,
                                 ctypes.c_uint64, ctypes.c_uint64]),
+    "emsesg_fx_inflow": (_I, [_P, _I, _I, _I, ctypes.c_int64, _P, _P, _P, _I, ctypes.c_double, ctypes.c_uint64,
+                              ctypes.c_uint64, ctypes.c_uint64]),
     "emsesg_fx_adjoint": (_I, [_P, _I, _I, _I, _I, _P, _P, ctypes.POINTER(ctypes.c_double), _P, _P, _P, _P]),
     "emsesg_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
     "emsesg_fx_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
@@ -422,6 +424,17 @@ class Emses:
         self._check(self.lib.emsesg_fx_inflow_z(self.h, spec, 1 if front else 0, n, t[0].ctypes.data,
                                                 t[1].ctypes.data, t[2].ctypes.data, t[0].size, injctisw, seed,
                                                 stream, index0))
+
+    def fx_inflow(self, spec: int, axis: int, front: bool, n: int, vn_table, va_table, vb_table, injctisw: float,
+                  seed: int, stream: int, index0: int = 0):
+        """n inflow particles through a face of `axis` (0 x, 1 y, 2 z) drawn
+        on the device (inject.inflow with hash_uniforms(seed, stream, index0,
+        n, 5)); va / vb: the tangential tables of the other axes in order."""
+        t = [np.ascontiguousarray(x, dtype=np.float64) for x in (vn_table, va_table, vb_table)]
+        assert t[0].size == t[1].size == t[2].size
+        self._check(self.lib.emsesg_fx_inflow(self.h, spec, axis, 1 if front else 0, n, t[0].ctypes.data,
+                                              t[1].ctypes.data, t[2].ctypes.data, t[0].size, injctisw, seed,
+                                              stream, index0))
 
     def fx_surface(self) -> np.ndarray:
         """Absorbed minus emitted particles per surface cell, [nspec, nsurf]."""

@@ -131,24 +131,43 @@ def inflow_count(istep: int, lstep: int, arr: float, injct: int, ustep: int) -> 
     return (int((istep + lstep) * arr) - int((istep + lstep - injct) * arr)) * ustep
 
 
-def inflow_z(front: bool, n: int, nx: int, ny: int, nz: int, vz_table: np.ndarray, vx_table: np.ndarray,
-             vy_table: np.ndarray, injctisw: float, rng: np.random.Generator | None, spec: int,
-             zssurf: float = -1.0e30, uniforms: np.ndarray | None = None) -> np.ndarray:
-    """Particles entering through the z = 0 face (front) or z = nz face
-    (back), psuper2.F90:236-292: x, y uniform on the face, z = the distance
-    covered within the last injctisw steps, preside 0."""
-    npr = vz_table.size
+def inflow(axis: int, front: bool, n: int, nx: int, ny: int, nz: int, vn_table: np.ndarray, va_table: np.ndarray,
+           vb_table: np.ndarray, injctisw: float, rng: np.random.Generator | None, spec: int,
+           zssurf: float = -1.0e30, uniforms: np.ndarray | None = None) -> np.ndarray:
+    """Particles entering through the lower (front) or upper face of `axis`
+    (0: x, 1: y, 2: z), psuper2.F90:114-292 (x faces :114-173, y :175-233, z
+    :236-292).  Per particle five uniforms: u0 picks the normal speed
+    vn_table[int(npr*u0)], u1 the tangential ones va_table / vb_table
+    [int(npr*u1)] (the two other axes in increasing order), u2 / u3 / u4 give
+    x / y / z: uniform on the face along the tangential axes, and along the
+    normal the distance vn * injctisw * u covered within the last injctisw
+    steps, from 0 or from the upper face.  preside 0.  Like the reference,
+    a particle with z <= zssurf is dropped whatever the face."""
+    npr = vn_table.size
     u = rng.random((n, 5)) if uniforms is None else uniforms
     a1 = (npr * u[:, 0]).astype(np.int64)
     a2 = (npr * u[:, 1]).astype(np.int64)
     out = np.zeros(n, dtype=PARTICLE_DTYPE)
-    out["x"] = 0.0 + nx * u[:, 2]
-    out["y"] = 0.0 + ny * u[:, 3]
-    vz = vz_table[a1]
-    out["z"] = (vz * injctisw * u[:, 4]) if front else (nz + vz * injctisw * u[:, 4])
-    out["vx"] = vx_table[a2]
-    out["vy"] = vy_table[a2]
-    out["vz"] = vz
+    ext = (nx, ny, nz)
+    names = ("x", "y", "z")
+    vn = vn_table[a1]
+    tang = [d for d in range(3) if d != axis]
+    for d in range(3):
+        if d == axis:
+            out[names[d]] = (vn * injctisw * u[:, 2 + d]) if front else (ext[d] + vn * injctisw * u[:, 2 + d])
+        else:
+            out[names[d]] = 0.0 + ext[d] * u[:, 2 + d]
+    out["v" + names[axis]] = vn
+    out["v" + names[tang[0]]] = va_table[a2]
+    out["v" + names[tang[1]]] = vb_table[a2]
     out["spec"] = spec
     keep = out["z"] > zssurf
     return out[keep]
+
+
+def inflow_z(front: bool, n: int, nx: int, ny: int, nz: int, vz_table: np.ndarray, vx_table: np.ndarray,
+             vy_table: np.ndarray, injctisw: float, rng: np.random.Generator | None, spec: int,
+             zssurf: float = -1.0e30, uniforms: np.ndarray | None = None) -> np.ndarray:
+    """Particles entering through the z = 0 face (front) or z = nz face
+    (back), psuper2.F90:236-292: inflow(2, ...)."""
+    return inflow(2, front, n, nx, ny, nz, vz_table, vx_table, vy_table, injctisw, rng, spec, zssurf, uniforms)

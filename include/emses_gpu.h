@@ -336,6 +336,16 @@ int emsesg_fx_emit(emsesg_ctx* ctx, int spec, int nemd, double grd, const double
 int emsesg_fx_inflow_z(emsesg_ctx* ctx, int spec, int front, int64_t n, const double* vz_t, const double* vx_t,
                        const double* vy_t, int npr, double injctisw, uint64_t seed, uint64_t stream,
                        uint64_t index0);
+/* emsesg_fx_inflow: the same through the lower (front) or upper face of
+ * any axis (0: x, 1: y, 2: z; psuper2.F90:114-173 x faces, :175-233 y
+ * faces, :236-292 z faces): u2 / u3 / u4 give x / y / z, uniform on the
+ * face along the tangential axes, the distance vn * injctisw * u from the
+ * face along the normal; vn = vn_t[int(npr*u0)], the tangential speeds of
+ * the two other axes in increasing order va_t / vb_t[int(npr*u1)].
+ * emsesg_fx_inflow_z(..., vz_t, vx_t, vy_t, ...) is
+ * emsesg_fx_inflow(..., 2, ..., vz_t, vx_t, vy_t, ...). */
+int emsesg_fx_inflow(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n, const double* vn_t, const double* va_t,
+                     const double* vb_t, int npr, double injctisw, uint64_t seed, uint64_t stream, uint64_t index0);
 /* Absorbed minus emitted particles per surface cell of the box bodies
  * (geotype 0/1, integer bounds), int64 [nspec][nsurf]: body by body, faces
  * -x,+x,-y,+y,-z,+z, each face's cells with its first tangential axis

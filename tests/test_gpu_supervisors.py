@@ -1,5 +1,5 @@
 """The injection supervisors on the device (emsesg_fx_emit,
-emsesg_fx_inflow_z) against the host supervisors of ctca_b200/inject.py fed
+emsesg_fx_inflow_z, emsesg_fx_inflow) against the host supervisors of ctca_b200/inject.py fed
 the same counter-hash draws (inject.hash_uniforms): the injected records,
 and everything downstream (the step's rho/J accumulators, the surface
 counts, the particle records after the sort), are bit-identical."""
@@ -63,6 +63,49 @@ def test_device_supervisors_match_host(gpu):
             assert np.array_equal(ja, jb), step
         assert np.array_equal(a.fx_surface(), b.fx_surface())
         assert np.abs(a.fx_surface()).sum() > 0
+        a.fx_sort()
+        b.fx_sort()
+        a.fx_store()
+        b.fx_store()
+        pa, ta = a.download_particles()
+        pb, tb = b.download_particles()
+        assert np.array_equal(ta, tb)
+        assert np.array_equal(pa.view(np.uint8), pb.view(np.uint8))
+
+
+@pytest.mark.parametrize("axis", [0, 1])
+def test_device_inflow_x_y_faces_match_host(gpu, axis):
+    """Inflow through both faces of x or y (open along that axis): device
+    records against the host supervisor on the same draws, through a step
+    and a sort."""
+    npb = [0, 0, 0]
+    npb[axis] = 2
+    nfb = [0, 0, 0]
+    nfb[axis] = 1
+    c = case(n=(24, 16, 16), ppc=(3, 3), npbnd=tuple(npb), nfbnd=tuple(nfb), vth_scale=3.0, tile=(8, 8, 8))
+    cfg, eb, p, tp = build(c, capacity_factor=1.5)
+    renv = inputs.units()["renv"]
+    s0 = c.species[0]
+    va = inject.maxwell_table(s0.vth * renv, 0.0, 512)
+    vb = va[::-1].copy()
+    ext = (cfg.nx, cfg.ny, cfg.nz)
+    seed = 7
+    with loaded(c, cfg, eb) as a, loaded(c, cfg, eb) as b:
+        for step in range(2):
+            for q, front in enumerate((True, False)):
+                vn = inject.flux_table(s0.vth * renv, 0.0, 512, sign=1.0 if front else -1.0)
+                n = 50 + 7 * step + q
+                st = 10 + q
+                u = inject.hash_uniforms(seed, st, 1000 * step, n, 5)
+                rec = inject.inflow(axis, front, n, *ext, vn, va, vb, 2.0, None, spec=1, uniforms=u)
+                a.fx_inject(1, rec)
+                b.fx_inflow(1, axis, front, n, vn, va, vb, 2.0, seed, st, 1000 * step)
+            a.fx_step(2, step == 1)
+            b.fx_step(2, step == 1)
+            ra, ja = a.fx_download_accum()
+            rb, jb = b.fx_download_accum()
+            assert np.array_equal(ra, rb), step
+            assert np.array_equal(ja, jb), step
         a.fx_sort()
         b.fx_sort()
         a.fx_store()

@@ -4,6 +4,7 @@ import ctypes
 import math
 
 import numpy as np
+import pytest
 
 from ctca_b200 import inject, inputs
 from oracle import oracle as O
@@ -53,6 +54,38 @@ def test_inflow_positions():
     assert np.all(rec["z"] <= 32) and np.all(rec["z"] >= 32 + vz.min())
     assert np.all(rec["vz"] < 0) and np.all(rec["preside"] == 0)
     assert np.all((rec["x"] >= 0) & (rec["x"] < 24))
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+@pytest.mark.parametrize("front", [True, False])
+def test_inflow_faces(axis, front):
+    """Inflow through every face (psuper2.F90:114-292): the normal coordinate
+    within vn * injctisw of the face, the tangential ones uniform on it, the
+    normal speed from the normal table and the tangential ones from one draw
+    of the tangential tables; the z faces are inflow_z."""
+    ext = (24, 20, 32)
+    names = "xyz"
+    sgn = 1.0 if front else -1.0
+    vn = inject.flux_table(0.05, 0.0, 512, sign=sgn)
+    va = inject.maxwell_table(0.05, 0.0, 512)
+    vb = va[::-1].copy()
+    u = inject.hash_uniforms(3, 4, 0, 2000, 5)
+    rec = inject.inflow(axis, front, 2000, *ext, vn, va, vb, 2.0, None, spec=2, uniforms=u)
+    assert rec.size == 2000 and np.all(rec["spec"] == 2) and np.all(rec["preside"] == 0)
+    n = names[axis]
+    depth = rec[n] if front else rec[n] - ext[axis]
+    assert np.all(sgn * depth >= 0) and np.all(np.abs(depth) <= 2.0 * np.abs(vn).max())
+    assert np.allclose(depth, rec["v" + n] * 2.0 * u[:, 2 + axis])
+    tang = [d for d in range(3) if d != axis]
+    for d in tang:
+        assert np.all((rec[names[d]] >= 0) & (rec[names[d]] < ext[d]))
+        assert np.array_equal(rec[names[d]], 0.0 + ext[d] * u[:, 2 + d])
+    a2 = (512 * u[:, 1]).astype(np.int64)
+    assert np.array_equal(rec["v" + names[tang[0]]], va[a2])
+    assert np.array_equal(rec["v" + names[tang[1]]], vb[a2])
+    if axis == 2:
+        z = inject.inflow_z(front, 2000, *ext, vn, va, vb, 2.0, None, spec=2, uniforms=u)
+        assert np.array_equal(z.view(np.uint8), rec.view(np.uint8))
 
 
 def _box_cfg():
