@@ -20,11 +20,11 @@
 //           warp (rows in order, lanes in order, __match_any_sync) gives its
 //           slot in the thread-major region of its new tile: inv[slot] = old
 //           slot (4-byte scattered writes);
-//   move    per destination tile, in groups of 32 columns: a window of the
-//           tile's old region is staged in shared memory (coalesced rows)
-//           and every slot takes its particle from the window or, for
-//           particles from other tiles, from global memory (coalesced
-//           writes).
+//   move    per destination tile, in groups of 32 to 480 columns: a window
+//           of the tile's old region and the group's inv are staged in
+//           shared memory (cp.async, double-buffered) and every slot takes
+//           its particle from the window or, for particles from other tiles
+//           or columns, from global memory (coalesced writes).
 //
 // Injected particles waiting in the tail zone join the same sort: the tail
 // alone is radix-sorted by the tile-major cell key (a few million keys), its
