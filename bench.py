@@ -152,7 +152,7 @@ def cpu_sample(seconds: float, threads: int):
     cell per species (4.19 M particles): a bounded sample of the workload."""
     from ctca_b200 import inputs
     from oracle import oracle as O
-    case = inputs.baseline_case(2)
+    case = inputs.workload_case(2)
     for s in case.species:
         s.ppc = 1
     cfg = inputs.make_config(case)
@@ -200,7 +200,7 @@ def time_adjoint(K: int = 256, ckpt: int = 16, sort_every: int = SORT_EVERY) -> 
     import torch
     from ctca_b200 import inputs
     from ctca_b200.emses import Emses
-    case = inputs.baseline_case(4)
+    case = inputs.workload_case(4)
     cfg = inputs.make_config(case)
     eb = inputs.make_fields(case)
     lo = tuple(case.n[d] // 2 - 4 for d in range(3))
@@ -265,7 +265,7 @@ def run_ours(args, world, rank, local):
 
     torch.cuda.set_device(local)
     select_device(local)
-    case = inputs.baseline_case(2)
+    case = inputs.workload_case(2)
     if args.cells:
         # smaller copy of the workload for profiler captures (not the headline)
         n = args.cells
@@ -550,7 +550,7 @@ def run_body_line(args, world, rank, local):
     torch.cuda.set_device(local)
     select_device(local)
     scale = args.body_scale
-    case = inputs.baseline_case(3, scale)
+    case = inputs.workload_case(3, scale)
     steps, warm = args.steps, args.warmup
     nstep_all = warm + steps + 5
     seed = case.seed + 17 * rank
@@ -674,7 +674,7 @@ def run_em_line(args, world, rank, local):
     from ctca_b200.emses import Emses, select_device
     torch.cuda.set_device(local)
     select_device(local)
-    case = inputs.baseline_case(2)
+    case = inputs.workload_case(2)
     cfg = inputs.make_config(case)
     g = Emses(cfg)
     g.upload_field("eb", inputs.make_fields(case))

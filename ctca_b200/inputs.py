@@ -77,8 +77,16 @@ def units(dt: float = 0.5, dr: float = 1.0, qm1: float = -1.0) -> dict:
     }
 
 
-# The benchmark configurations (normalized units), see the docstring.
-def baseline_case(idx: int, scale: float = 1.0) -> Case:
+def workload_case(idx: int, scale: float = 1.0) -> Case:
+    """The benchmark workloads (normalized units):
+    1: 32^3 periodic, 2 species x 16 ppc, mass ratio 100, B0 along z, E0 plus
+       4 Fourier modes (the CPU-sized case);
+    2: 128^3 periodic, 2 species x 64 ppc, mass ratio 1836, ion drift, 8 E
+       and 8 B modes (the headline particle step);
+    3: 256x256x512, open z, 2 species x 24 ppc drifting along -z past a
+       32x32x16 conducting box (the body workload);
+    4: 64^3 periodic, the plasma of case 1 at 32 ppc (the adjoint workload).
+    `scale` shrinks the grid of cases 2-4."""
     if idx == 1:
         return Case(n=(32, 32, 32),
                     species=[Species(16, -1.0, 0.05), Species(16, 1.0 / 100.0, 0.005)],
@@ -107,7 +115,7 @@ def baseline_case(idx: int, scale: float = 1.0) -> Case:
         return c
     if idx == 4:
         # the adjoint workload: 64^3, the plasma of case 1 at 32 ppc
-        c = baseline_case(1)
+        c = workload_case(1)
         n = max(8, int(round(64 * scale)))
         c.n = (n, n, n)
         for sp in c.species:
@@ -116,7 +124,7 @@ def baseline_case(idx: int, scale: float = 1.0) -> Case:
         c.seed = 1004
         c.sort_tile = (8, 8, 8)
         return c
-    raise ValueError(f"no baseline case {idx}")
+    raise ValueError(f"no workload case {idx}")
 
 
 def charges(case: Case) -> tuple[list, list, list]:

@@ -270,7 +270,7 @@ def counters(gc: DerivedObj) -> dict:
 
 # ------------------------------------------------------------ the cases
 def base_case(name):
-    c = inputs.baseline_case(1)
+    c = inputs.workload_case(1)
     c.n = (6, 5, 4)
     c.species[0].ppc, c.species[1].ppc = 3, 2
     c.kmax = 2 * np.pi / 4 * 2

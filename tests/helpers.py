@@ -8,7 +8,7 @@ from ctca_b200.emses import PARTICLE_DTYPE
 
 def case(n=(8, 8, 8), ppc=(6, 6), seed=11, b0=(0.0, 0.0, 0.2), e=True, vth_scale=1.0, npbnd=(0, 0, 0),
          nfbnd=(0, 0, 0), tile=(0, 0, 0)):
-    c = inputs.baseline_case(1)
+    c = inputs.workload_case(1)
     c.n = tuple(n)
     c.species[0].ppc, c.species[1].ppc = ppc
     c.species[0].vth *= vth_scale

@@ -11,7 +11,7 @@ from oracle import oracle as O
 
 
 def small_case(n=(8, 8, 8), ppc=(4, 4), seed=7, e=True, b0=(0.0, 0.0, 0.2)):
-    c = inputs.baseline_case(1)
+    c = inputs.workload_case(1)
     c.n = n
     c.species[0].ppc, c.species[1].ppc = ppc
     c.kmax = 2 * np.pi / min(n) * 2
