@@ -135,8 +135,10 @@ def charges(case: Case) -> tuple[list, list, list]:
     for s in case.species:
         if s is e:
             qs = qe
-        else:
+        elif s.ppc > 0:
             qs = -qe * e.ppc / s.ppc  # neutralising
+        else:
+            qs = -qe  # a species without particles: any finite charge
         q.append(qs)
         qm.append(s.qm)
         rm.append(qs / s.qm)

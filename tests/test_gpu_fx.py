@@ -213,3 +213,66 @@ def test_fx_em_step_vs_oracle(gpu):
     assert err < 1e-6
     assert rel_l2(g.download_field("aj"), o.f["aj"]) < RHOJ_TOL
     g.close()
+
+
+def test_fx_empty_species_tracks_oracle(gpu):
+    """A species without particles: steps and sorts (tile-local) leave it
+    empty and the other species tracks the oracle."""
+    c = case(n=(16, 16, 16), ppc=(8, 0), tile=(8, 8, 8))
+    cfg, g, o, p32, tp32 = fx_pair(c)
+    assert tp32[1] == 0
+    for step in range(4):
+        g.fx_step(2, step == 1)
+        if step == 1:
+            o.spsort()
+        oracle_step(o)
+    assert rel_l2(g.download_field("rho"), o.f["rho"]) < RHOJ_TOL
+    assert rel_l2(g.download_field("aj"), o.f["aj"]) < RHOJ_TOL
+    assert np.array_equal(g.fx_counts(), o.totalp)
+    g.close()
+
+
+def test_fx_stray_particles_fall_back_to_the_radix_sort(gpu):
+    """Particles that left their tile's sort box (tile + one cell) between
+    sorts: the tile-local sort gives way to the radix sort, which keeps every
+    live particle and orders them by the tile-major cell key; the next step
+    still tracks the oracle."""
+    tile = (8, 8, 8)
+    c = case(n=(16, 16, 16), ppc=(4, 4), vth_scale=20.0, tile=tile)
+    cfg, g, o, p32, tp32 = fx_pair(c)
+    for _ in range(3):
+        g.fx_step(2, False)
+        oracle_step(o)
+    g.fx_store()
+    pa, ta = g.download_particles()     # slot order of the load: same as p32
+    # some particle is out of the sort box of the tile it was sorted into
+    ext = np.array([cfg.nx, cfg.ny, cfg.nz])
+    c0 = np.stack([np.floor(p32[f]) for f in "xyz"], 1).astype(int)
+    c1 = np.stack([np.floor(pa[f]) for f in "xyz"], 1).astype(int)
+    lo = (c0 // tile) * tile - 1
+    off = (c1 - lo) % ext              # periodic
+    stray = (pa["nid"] != -1) & np.any(off >= np.array(tile) + 2, axis=1)
+    assert stray.sum() > 0
+    g.fx_sort()
+    g.fx_store()
+    pb, tb = g.download_particles()
+    fields = ("x", "y", "z", "vx", "vy", "vz")
+    base_a = np.concatenate([[0], np.cumsum(ta)])
+    base_b = np.concatenate([[0], np.cumsum(tb)])
+    for s in range(cfg.nspec):
+        a = pa[base_a[s]:base_a[s + 1]]
+        a = a[a["nid"] != -1]
+        b = pb[base_b[s]:base_b[s + 1]]
+        assert b.size == a.size
+        key, _ = _tile_key(cfg, tile, b)
+        assert np.all(np.diff(key) >= 0)
+        ka = np.lexsort([a[f] for f in fields])
+        kb = np.lexsort([b[f] for f in fields])
+        for f in fields:
+            assert np.array_equal(a[f][ka], b[f][kb]), (s, f)
+    g.fx_step(2, False)
+    o.spsort()
+    oracle_step(o)
+    assert rel_l2(g.download_field("rho"), o.f["rho"]) < RHOJ_TOL
+    assert rel_l2(g.download_field("aj"), o.f["aj"]) < RHOJ_TOL
+    g.close()
