@@ -938,8 +938,9 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   if (drawn && c.rng_mode == 1) EMSESG_LAUNCH(ctx, "fx_rand_advance", k_add_i64, 1, 1, 0, ctx->d_rand_pos, drawn);
   if (a.bd.n > 0) EMSESG_LAUNCH(ctx, "fx_chgacm", k_fx_chgacm, 1, 32, 0, ctx->d_cfg, ctx->d_counter);
   // guard folding on the exact integers, then FP64 outputs
-  if ((rc = run_slab_ops(ctx, (long long*)acc_rho, fr, fold_ops(c, 0, 1), "fx_fold_rho"))) return rc;
-  if ((rc = run_slab_ops(ctx, (long long*)acc_j, fj, fold_ops(c, 1, 3), "fx_fold_j"))) return rc;
+  if ((rc = run_slab_ops2(ctx, (long long*)acc_rho, fr, fold_ops(c, 0, 1), (long long*)acc_j, fj,
+                          fold_ops(c, 1, 3), "fx_fold")))
+    return rc;
   EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_double, nblk(fr.size()), 256, 0, (const long long*)acc_rho,
                 ctx->field[EMSESG_FIELD_RHO], fr.size());
   EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_double, nblk(fj.size()), 256, 0, (const long long*)acc_j,
