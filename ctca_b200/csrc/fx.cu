@@ -1046,7 +1046,35 @@ __global__ void k_gen_emit(emsesg_particle* out, int32_t* ord, int64_t n, int ne
   ord[2 * k + 1] = (int32_t)(pending + k + 1);
 }
 
-// Inflow through a z face (psuper2.F90:236-292), preside 0.
+// Particles emitted from a rectangular plane (psuper2.F90:330-360,
+// 554-576): the normal coordinate grd + vn * injctisw * u3, the tangential
+// ones uniform on the plane plus vt * injctisw * u3; preside 0, pid = the
+// body.  One record per particle.
+__global__ void k_gen_emit_plane(emsesg_particle* out, int32_t* ord, int64_t n, int nemd, double grd, double b1lo,
+                                 double b1hi, double b2lo, double b2hi, const double* __restrict__ vnorm,
+                                 const double* __restrict__ vtang, int npr, double injctisw, int pid,
+                                 uint64_t seed, uint64_t stream, uint64_t index0, int spec) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double u[6];
+  for (int c = 0; c < 6; c++) u[c] = hash_u01(seed, stream, (index0 + (uint64_t)k) * 6 + c);
+  const int an = abs(nemd);
+  const int ax0 = an - 1, ax1 = an % 3, ax2 = (an + 1) % 3;
+  const double ud = nemd > 0 ? 1.0 : -1.0;
+  const int a0 = (int)(npr * u[0]), a1 = (int)(npr * u[1]), a2 = (int)(npr * u[2]);
+  const double vn = ud * vnorm[a0], vt1 = vtang[a1], vt2 = vtang[a2];
+  emsesg_particle p;
+  double* r = &p.x;
+  double* v = &p.vx;
+  r[ax0] = __dadd_rn(grd, __dmul_rn(__dmul_rn(vn, injctisw), u[3]));
+  r[ax1] = __dadd_rn(lin(b1lo, b1hi, u[4]), __dmul_rn(__dmul_rn(vt1, injctisw), u[3]));
+  r[ax2] = __dadd_rn(lin(b2lo, b2hi, u[5]), __dmul_rn(__dmul_rn(vt2, injctisw), u[3]));
+  v[ax0] = vn; v[ax1] = vt1; v[ax2] = vt2;
+  p.pid = pid; p.preside = 0; p.nid = 0; p.spec = spec;
+  out[k] = p;
+  ord[k] = 0;
+}
+
 // Inflow through the lower (front) or upper face of `axis`
 // (psuper2.F90:114-292): u2, u3, u4 give x, y, z -- uniform on the face
 // along the tangential axes; along the normal the distance vn * injctisw * u
@@ -1153,6 +1181,24 @@ extern "C" int emsesg_fx_emit(emsesg_ctx* ctx, int spec, int nemd, double grd, c
   EMSESG_LAUNCH(ctx, "fx_gen_emit", k_gen_emit, nblk(n), 256, 0, f.stage, f.stage_ord, n, nemd, grd, b1[0], b1[1],
                 b2[0], b2[1], f.inj_tab, f.inj_tab + npr, npr, seed, stream, index0, spec, pending);
   return inject_staged(ctx, is, 2 * n, pending + n);
+}
+
+extern "C" int emsesg_fx_emit_plane(emsesg_ctx* ctx, int spec, int nemd, double grd, const double* b1,
+                                    const double* b2, int64_t n, const double* vnorm, const double* vtang, int npr,
+                                    double injctisw, int pid, uint64_t seed, uint64_t stream, uint64_t index0) {
+  int rc = inject_check(ctx, spec, n, npr, vnorm, vtang, vnorm);
+  if (rc) return rc;
+  if (!b1 || !b2 || nemd == 0 || nemd < -3 || nemd > 3) return set_error(ctx, EMSESG_ERR_ARG, "bad emission face");
+  if (n == 0) return EMSESG_OK;
+  const int is = spec - 1;
+  FxState& f = ctx->fx;
+  if ((rc = inject_reserve(ctx, is, n))) return rc;
+  const double* tabs[2] = {vnorm, vtang};
+  if ((rc = inject_tables(ctx, 2, npr, tabs))) return rc;
+  EMSESG_LAUNCH(ctx, "fx_gen_emit_plane", k_gen_emit_plane, nblk(n), 256, 0, f.stage, f.stage_ord, n, nemd, grd,
+                b1[0], b1[1], b2[0], b2[1], f.inj_tab, f.inj_tab + npr, npr, injctisw, pid, seed, stream, index0,
+                spec);
+  return inject_staged(ctx, is, n, f.pending[is]);
 }
 
 extern "C" int emsesg_fx_inflow(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n, const double* vn_t,

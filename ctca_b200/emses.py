@@ -147,6 +147,8 @@ _SIGS = {
                                 ctypes.c_uint64, ctypes.c_uint64]),
     "emsesg_fx_inflow": (_I, [_P, _I, _I, _I, ctypes.c_int64, _P, _P, _P, _I, ctypes.c_double, ctypes.c_uint64,
                               ctypes.c_uint64, ctypes.c_uint64]),
+    "emsesg_fx_emit_plane": (_I, [_P, _I, _I, ctypes.c_double, _P, _P, ctypes.c_int64, _P, _P, _I, ctypes.c_double,
+                                  _I, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
     "emsesg_fx_adjoint": (_I, [_P, _I, _I, _I, _I, _P, _P, ctypes.POINTER(ctypes.c_double), _P, _P, _P, _P]),
     "emsesg_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
     "emsesg_fx_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
@@ -424,6 +426,18 @@ class Emses:
         self._check(self.lib.emsesg_fx_inflow_z(self.h, spec, 1 if front else 0, n, t[0].ctypes.data,
                                                 t[1].ctypes.data, t[2].ctypes.data, t[0].size, injctisw, seed,
                                                 stream, index0))
+
+    def fx_emit_plane(self, spec: int, nemd: int, grd: float, b1, b2, n: int, vnorm, vtang, injctisw: float,
+                      pid: int, seed: int, stream: int, index0: int = 0):
+        """n particles emitted from a rectangular plane, drawn on the device
+        (inject.emit_plane with hash_uniforms(seed, stream, index0, n, 6))."""
+        vn = np.ascontiguousarray(vnorm, dtype=np.float64)
+        vt = np.ascontiguousarray(vtang, dtype=np.float64)
+        assert vn.size == vt.size
+        cb1 = (ctypes.c_double * 2)(*b1)
+        cb2 = (ctypes.c_double * 2)(*b2)
+        self._check(self.lib.emsesg_fx_emit_plane(self.h, spec, nemd, grd, cb1, cb2, n, vn.ctypes.data,
+                                                  vt.ctypes.data, vn.size, injctisw, pid, seed, stream, index0))
 
     def fx_inflow(self, spec: int, axis: int, front: bool, n: int, vn_table, va_table, vb_table, injctisw: float,
                   seed: int, stream: int, index0: int = 0):

@@ -126,6 +126,41 @@ def emit_rectangle(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int
     return out
 
 
+def emit_plane(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int, vnormf: np.ndarray,
+               vtangf: np.ndarray, injctisw: float, rng: np.random.Generator | None, spec: int, pid: int = 0,
+               uniforms: np.ndarray | None = None) -> np.ndarray:
+    """n particles emitted from a rectangular plane of a body
+    (emit_from_rectangular_surf, psuper2.F90:330-360, 554-576): per particle
+    six uniforms; normal speed ud * vnormf[int(npr*u0)], tangential speeds
+    vtangf[int(npr*u1)], vtangf[int(npr*u2)]; the normal coordinate
+    grd + vnorm * injctisw * u3 and the tangential ones uniform on the plane
+    (u4, u5) plus vtang * injctisw * u3: the particle has flown for the
+    fraction u3 of the injection interval.  One record per particle (no
+    anti-particle), pid = the body, preside 0."""
+    axis = _ORDER[abs(nemd)]
+    ud = 1.0 if nemd > 0 else -1.0
+    npr = vnormf.size
+    u = rng.random((n, 6)) if uniforms is None else uniforms
+    out = np.zeros(n, dtype=PARTICLE_DTYPE)
+    coords = [("x", "vx"), ("y", "vy"), ("z", "vz")]
+    a0 = (npr * u[:, 0]).astype(np.int64)
+    a1 = (npr * u[:, 1]).astype(np.int64)
+    a2 = (npr * u[:, 2]).astype(np.int64)
+    vn = ud * vnormf[a0]
+    vt1 = vtangf[a1]
+    vt2 = vtangf[a2]
+    rn = grd + vn * injctisw * u[:, 3]
+    rt1 = bounds1[0] + (bounds1[1] - bounds1[0]) * u[:, 4] + vt1 * injctisw * u[:, 3]
+    rt2 = bounds2[0] + (bounds2[1] - bounds2[0]) * u[:, 5] + vt2 * injctisw * u[:, 3]
+    for val_r, val_v, ax in ((rn, vn, axis[0]), (rt1, vt1, axis[1]), (rt2, vt2, axis[2])):
+        c, v = coords[ax]
+        out[c] = val_r
+        out[v] = val_v
+    out["spec"] = spec
+    out["pid"] = pid
+    return out
+
+
 def inflow_count(istep: int, lstep: int, arr: float, injct: int, ustep: int) -> int:
     """narrzf / narrzb of psuper2.F90:238-239, 266-267."""
     return (int((istep + lstep) * arr) - int((istep + lstep - injct) * arr)) * ustep

@@ -346,6 +346,16 @@ int emsesg_fx_inflow_z(emsesg_ctx* ctx, int spec, int front, int64_t n, const do
  * emsesg_fx_inflow(..., 2, ..., vz_t, vx_t, vy_t, ...). */
 int emsesg_fx_inflow(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n, const double* vn_t, const double* va_t,
                      const double* vb_t, int npr, double injctisw, uint64_t seed, uint64_t stream, uint64_t index0);
+/* emsesg_fx_emit_plane: n particles from a rectangular plane of body pid
+ * (psuper2.F90:330-360 with emit_from_rectangular_surf, :554-576): six
+ * uniforms each; normal speed ud * vnorm[int(npr*u0)], tangential
+ * vtang[int(npr*u1)], vtang[int(npr*u2)]; normal coordinate
+ * grd + vnorm * injctisw * u3, tangential b1 / b2 uniform (u4, u5) plus
+ * vtang * injctisw * u3; one record each, preside 0.  The outflux and
+ * chgacm bookkeeping of psuper2.F90:494-498 (n per call) is the caller's. */
+int emsesg_fx_emit_plane(emsesg_ctx* ctx, int spec, int nemd, double grd, const double* b1, const double* b2,
+                         int64_t n, const double* vnorm, const double* vtang, int npr, double injctisw, int pid,
+                         uint64_t seed, uint64_t stream, uint64_t index0);
 /* Absorbed minus emitted particles per surface cell of the box bodies
  * (geotype 0/1, integer bounds), int64 [nspec][nsurf]: body by body, faces
  * -x,+x,-y,+y,-z,+z, each face's cells with its first tangential axis

@@ -1,5 +1,5 @@
 """The injection supervisors on the device (emsesg_fx_emit,
-emsesg_fx_inflow_z, emsesg_fx_inflow) against the host supervisors of ctca_b200/inject.py fed
+emsesg_fx_inflow_z, emsesg_fx_inflow, emsesg_fx_emit_plane) against the host supervisors of ctca_b200/inject.py fed
 the same counter-hash draws (inject.hash_uniforms): the injected records,
 and everything downstream (the step's rho/J accumulators, the surface
 counts, the particle records after the sort), are bit-identical."""
@@ -100,6 +100,42 @@ def test_device_inflow_x_y_faces_match_host(gpu, axis):
                 rec = inject.inflow(axis, front, n, *ext, vn, va, vb, 2.0, None, spec=1, uniforms=u)
                 a.fx_inject(1, rec)
                 b.fx_inflow(1, axis, front, n, vn, va, vb, 2.0, seed, st, 1000 * step)
+            a.fx_step(2, step == 1)
+            b.fx_step(2, step == 1)
+            ra, ja = a.fx_download_accum()
+            rb, jb = b.fx_download_accum()
+            assert np.array_equal(ra, rb), step
+            assert np.array_equal(ja, jb), step
+        a.fx_sort()
+        b.fx_sort()
+        a.fx_store()
+        b.fx_store()
+        pa, ta = a.download_particles()
+        pb, tb = b.download_particles()
+        assert np.array_equal(ta, tb)
+        assert np.array_equal(pa.view(np.uint8), pb.view(np.uint8))
+
+
+def test_device_plane_emission_matches_host(gpu):
+    """Plane emission (psuper2) from two planes inside a periodic box:
+    device records against the host supervisor on the same draws, through
+    steps and a sort."""
+    c = case(n=(24, 24, 24), ppc=(3, 3), vth_scale=3.0, tile=(8, 8, 8))
+    cfg, eb, p, tp = build(c, capacity_factor=1.5)
+    renv = inputs.units()["renv"]
+    vn = inject.flux_table(0.01 * renv, 0.0, 512)
+    vt = inject.maxwell_table(0.01 * renv, 0.0, 512)
+    seed = 31
+    planes = [(1, 12.0, (4.0, 20.0), (6.0, 18.0), 1), (-3, 9.5, (2.0, 22.0), (3.0, 21.0), 2)]
+    with loaded(c, cfg, eb) as a, loaded(c, cfg, eb) as b:
+        for step in range(3):
+            for q, (nemd, grd, b1, b2, pid) in enumerate(planes):
+                n = 60 + 5 * step + q
+                st = 20 + q
+                u = inject.hash_uniforms(seed, st, 1000 * step, n, 6)
+                rec = inject.emit_plane(nemd, grd, b1, b2, n, vn, vt, 2.0, None, spec=1, pid=pid, uniforms=u)
+                a.fx_inject(1, rec)
+                b.fx_emit_plane(1, nemd, grd, b1, b2, n, vn, vt, 2.0, pid, seed, st, 1000 * step)
             a.fx_step(2, step == 1)
             b.fx_step(2, step == 1)
             ra, ja = a.fx_download_accum()

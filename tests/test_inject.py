@@ -88,6 +88,31 @@ def test_inflow_faces(axis, front):
         assert np.array_equal(z.view(np.uint8), rec.view(np.uint8))
 
 
+@pytest.mark.parametrize("nemd", [1, -1, 2, -2, 3, -3])
+def test_emit_plane_geometry(nemd):
+    """Plane emission (emit_from_rectangular_surf, psuper2.F90:554-576):
+    one record per particle with preside 0 and pid of the body; the normal
+    coordinate grd + vnorm * injctisw * u3 on the side of nemd, the tangential
+    ones uniform on the plane plus vtang * injctisw * u3."""
+    vn_t = inject.flux_table(0.01, 0.0, 256)
+    vt_t = inject.maxwell_table(0.01, 0.0, 256)
+    u = inject.hash_uniforms(5, 6, 0, 500, 6)
+    b1, b2 = (8.0, 16.0), (14.0, 18.0)
+    rec = inject.emit_plane(nemd, 16.0, b1, b2, 500, vn_t, vt_t, 2.0, None, spec=1, pid=3, uniforms=u)
+    assert rec.size == 500 and np.all(rec["preside"] == 0) and np.all(rec["pid"] == 3)
+    ax = inject._ORDER[abs(nemd)]
+    names = "xyz"
+    n0, t1, t2 = (names[a] for a in ax)
+    sgn = 1.0 if nemd > 0 else -1.0
+    a0 = (256 * u[:, 0]).astype(np.int64)
+    assert np.array_equal(rec["v" + n0], sgn * vn_t[a0])
+    assert np.all(sgn * (rec[n0] - 16.0) >= 0)
+    assert np.allclose(rec[n0], 16.0 + rec["v" + n0] * 2.0 * u[:, 3])
+    for t, (lo, hi), c in ((t1, b1, 4), (t2, b2, 5)):
+        on_plane = rec[t] - rec["v" + t] * 2.0 * u[:, 3]
+        assert np.allclose(on_plane, lo + (hi - lo) * u[:, c])
+
+
 def _box_cfg():
     c = case(n=(24, 24, 32))
     c.bodies = [dict(geotype=0, ncond=1, xlpc=8.0, xupc=16.0, ylpc=8.0, yupc=16.0, zlpc=14.0, zupc=18.0,
