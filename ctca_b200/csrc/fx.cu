@@ -1532,11 +1532,11 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
       if (fx_box_tile(tmax) == 4) {
         EMSESG_ADJ(check_cuda(ctx, cudaFuncSetAttribute(k_fx_adjoint<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                         asmem), "adjoint smem"));
-        EMSESG_LAUNCH(ctx, "fx_adjoint", k_fx_adjoint<4>, grid, PUSH_THREADS, asmem, a);
+        EMSESG_LAUNCH(ctx, "fx_adjoint", k_fx_adjoint<4>, grid, ADJ_THREADS, asmem, a);
       } else {
         EMSESG_ADJ(check_cuda(ctx, cudaFuncSetAttribute(k_fx_adjoint<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                         asmem), "adjoint smem"));
-        EMSESG_LAUNCH(ctx, "fx_adjoint", k_fx_adjoint<8>, grid, PUSH_THREADS, asmem, a);
+        EMSESG_LAUNCH(ctx, "fx_adjoint", k_fx_adjoint<8>, grid, ADJ_THREADS, asmem, a);
       }
     }
   }

@@ -134,8 +134,13 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
   return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 
+// Threads of a reverse-step CTA: a row of more than 512 slots is taken in
+// two column passes by half as many threads (whole warps), so that the
+// reverse step keeps its registers (the push's wide rows cap them at 80).
+constexpr int ADJ_THREADS = PUSH_THREADS > 512 ? (PUSH_THREADS / 2 + 31) / 32 * 32 : PUSH_THREADS;
+
 template <int T>
-__global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
+__global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
   constexpr int B = T + 2 * PG + 1;
   constexpr int NF = B * B * B;
   extern __shared__ __align__(16) float4 adj_smem[];
@@ -154,7 +159,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
   const int o[3] = {tx * G.t[0] - PG, ty * G.t[1] - PG, tz * G.t[2] - PG};
   const int64_t sy = G.nx + 1, sz = (int64_t)(G.nx + 1) * (G.ny + 1);
   bool anyg = false;
-  for (int e = tid; e < NF; e += PUSH_THREADS) {
+  for (int e = tid; e < NF; e += ADJ_THREADS) {
     const int li = e % B, lj = (e / B) % B, lk = e / (B * B);
     const int gi = o[0] + li, gj = o[1] + lj, gk = o[2] + lk;
     float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p;
@@ -198,8 +203,10 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
     }
   };
   const float qmp = a.qmp[is], qq = a.q[is], us = a.us, rustep = a.rustep;
+  // the thread's columns, one pass each (a run never spans two columns)
+  for (int col = tid; col < PUSH_THREADS; col += ADJ_THREADS) {
   for (int r = 0; r < L; r++) {
-    const int64_t m = slot0 + (int64_t)r * PUSH_THREADS + tid;
+    const int64_t m = slot0 + (int64_t)r * PUSH_THREADS + col;
     const float4 ps = a.pos[m];
     const uint32_t cell = (uint32_t)__float_as_int(ps.w);
     if (cell == DEAD) continue;
@@ -309,8 +316,10 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_fx_adjoint(AdjArgs a) {
     a.lvz[m] = lu.z;
   }
   flush();
+  runbase = -1;
+  }  // column passes
   __syncthreads();
-  for (int e = tid; e < NF; e += PUSH_THREADS) {
+  for (int e = tid; e < NF; e += ADJ_THREADS) {
     const int li = e % B, lj = (e / B) % B, lk = e / (B * B);
     const int gi = o[0] + li, gj = o[1] + lj, gk = o[2] + lk;
     if (gi < 0 || gj < 0 || gk < 0 || gi > G.nx || gj > G.ny || gk > G.nz) continue;

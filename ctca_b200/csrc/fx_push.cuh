@@ -7,8 +7,8 @@
 // thread t's contiguous run of the cell-sorted order, and row r is one
 // coalesced stretch of PUSH_THREADS records.  Empty slots hold DEAD cells.
 //
-// One CTA pushes one region with 480 threads; a 16th warp streams the rows
-// into a 4-stage shared-memory ring with cp.async.bulk (TMA 1-D copies
+// One CTA pushes one region with 736 threads; a 24th warp streams the rows
+// into a 3-stage shared-memory ring with cp.async.bulk (TMA 1-D copies
 // completing on mbarriers) and never computes, so a warp busy with its
 // queues never holds up the stream; pushing warps release a stage through an
 // "empty" mbarrier once they hold their particle.  The
@@ -33,20 +33,23 @@
 // every conversion to fixed point is of one value; integer atomics commute.
 // Two runs on the same input give the same bits.
 
-// 15 pushing warps + 1 streaming warp: 16 warps, so that each SM sub-partition
-// holds 4 of them and the kernel keeps 128 registers a thread.
-constexpr int PUSH_THREADS = 480;           // pushing threads = slots per row
+// 23 pushing warps + 1 streaming warp: 24 warps, 6 on each SM sub-partition,
+// at 80 registers a thread (a few values spill).  The kernel is bound by
+// latency more than by issue or memory: at 128^3 x 64 ppc it pushed in
+// 8.16 ms with 480-slot rows (16 warps, 128 registers), 7.53 with 608 (20
+// warps, 96 registers), 7.20 with 736.
+constexpr int PUSH_THREADS = 736;           // pushing threads = slots per row
 constexpr int PUSH_WARPS = PUSH_THREADS / 32;
 constexpr int PUSH_BLOCK = PUSH_THREADS + 32;  // + one warp that streams the rows
 constexpr int PG = 1;           // guard cells around the tile
-constexpr int NSTAGE = 5;       // row ring stages (up to NSTAGE - 1 rows in flight)
+constexpr int NSTAGE = 3;       // row ring stages (up to NSTAGE - 1 rows in flight)
 constexpr int NJ = 12;          // zigzag node values of one cell
 constexpr int NR = 8;           // CIC node values of one cell
 constexpr int RQW = NJ + NR + 1;  // run-queue entry: 20 sums + box index of the cell
 constexpr int RQ_DRAIN = 8;     // drain the run queue at this many entries
 constexpr int RQCAP = RQ_DRAIN + 32;
 constexpr int XQW = 8;          // general-path entry: slot, cell, 3 offsets, 3 velocities
-constexpr int XLCAP = 512;      // per-warp list of cross slots
+constexpr int XLCAP = 128;      // per-warp list of cross slots (emptied when nearly full)
 constexpr int CHUNK_ROWS = 256;  // rows of a tile region per CTA (crowded tiles take several)
 constexpr uint32_t ROW_BYTES = PUSH_THREADS * (16 + 3 * 4);
 static_assert(PUSH_THREADS == EMSESG_FX_ROW_SLOTS, "row width of the thread-major layout");

@@ -20,7 +20,7 @@
 //           warp (rows in order, lanes in order, __match_any_sync) gives its
 //           slot in the thread-major region of its new tile: inv[slot] = old
 //           slot (4-byte scattered writes);
-//   move    per destination tile, in groups of 32 to 480 columns: a window
+//   move    per destination tile, in groups of 32 columns or of the whole row: a window
 //           of the tile's old region and the group's inv are staged in
 //           shared memory (cp.async, double-buffered) and every slot takes
 //           its particle from the window or, for particles from other tiles
@@ -397,8 +397,9 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restr
 // (coalesced).  The window and the group's columns of inv are staged in
 // shared memory with cp.async, double-buffered: group g+1's copies are in
 // flight while group g is written.  The group width is the widest of 32,
-// 96, 160 and 480 columns whose group fits the staged slots at the tile's
-// row count, so that a tile of few rows is moved in few groups.
+// 96, 160 columns and the whole row (those that divide the row) whose group
+// fits the staged slots at the tile's row count, so that a tile of few rows
+// is moved in few groups.
 //
 // Two shapes (MoveBig, MoveSmall), picked per sort by the mean rows per
 // tile: tiles of many rows need big windows (80 rows: 200 KB of shared
@@ -422,7 +423,7 @@ constexpr int MOVE_SMALL_ROWS = 32;           // mean rows per tile up to which 
 constexpr int MOVE_MAXGROUPS = PUSH_THREADS / 32;
 template <class Cfg>
 inline int move_smem() { return 2 * Cfg::BUF; }
-static_assert(PUSH_THREADS == 480, "the group widths 32, 96, 160 and 480 divide the row");
+static_assert(PUSH_THREADS % 32 == 0, "32-column groups divide the row");
 
 template <bool CA>
 __device__ __forceinline__ void cpa16(void* dst, const void* src) {
@@ -584,14 +585,23 @@ __global__ void __launch_bounds__(PUSH_THREADS, 1) k_lcs_move(const float4* __re
   const int64_t ns = ts[t + 1] - ts[t];
   const int Ls = (int)((ns + PUSH_THREADS - 1) / PUSH_THREADS);
   const int R = max(Ls, Ld);
-  if (R * 480 <= Cfg::SLOTS)
-    move_tile<Cfg, 480>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
-  else if (R * 160 <= Cfg::SLOTS)
-    move_tile<Cfg, 160>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
-  else if (R * 96 <= Cfg::SLOTS)
-    move_tile<Cfg, 96>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
-  else
-    move_tile<Cfg, 32>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
+  if (R * PUSH_THREADS <= Cfg::SLOTS) {
+    move_tile<Cfg, PUSH_THREADS>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
+    return;
+  }
+  if constexpr (PUSH_THREADS % 160 == 0) {
+    if (R * 160 <= Cfg::SLOTS) {
+      move_tile<Cfg, 160>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
+      return;
+    }
+  }
+  if constexpr (PUSH_THREADS % 96 == 0) {
+    if (R * 96 <= Cfg::SLOTS) {
+      move_tile<Cfg, 96>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
+      return;
+    }
+  }
+  move_tile<Cfg, 32>(pos, vx, vy, vz, inv, pos2, vx2, vy2, vz2, Ld, Ls, tp[t], tp2[t], ns > 0, msm, wlo);
 }
 
 // Inside a CUDA graph the host cannot switch to the radix sort when a

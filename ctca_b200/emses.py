@@ -41,7 +41,7 @@ PCL_TO_BE_ACCUMULATED = -1
 PCL_TO_BE_ACCUMULATED_AS_ANTIPCL = -2
 
 # Slots per row of the FP32 form's thread-major tile regions (EMSESG_FX_ROW_SLOTS).
-FX_ROW_SLOTS = 480
+FX_ROW_SLOTS = 736
 
 FIELDS = {"eb": 0, "wrk": 1, "aj": 2, "ajdg": 3, "rho": 4, "rhodg": 5, "rhobk": 6, "rhobksp": 7}
 

@@ -13,7 +13,7 @@ run.
 
 The tile shape and the sort interval S of each grid-size class come from an
 autotuner that times the candidates on a batch of copies of the class's
-first run (the push block is fixed at 512 threads by the 480-slot rows of
+first run (the push block is fixed at 768 threads by the 736-slot rows of
 the layout).  Runs that do not fit in device memory together go in waves.
 
 Runs are drawn as stated for the ensemble workload: cubic periodic grids of

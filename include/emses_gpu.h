@@ -252,7 +252,7 @@ int emsesg_energy(emsesg_ctx* ctx, double* engk);
 /* Slots per row of the FP32 form's thread-major tile regions: after a sort
  * the particle of sorted rank q of a tile of n particles sits in row q % L,
  * column q / L of its region, L = ceil(n / EMSESG_FX_ROW_SLOTS). */
-#define EMSESG_FX_ROW_SLOTS 480
+#define EMSESG_FX_ROW_SLOTS 736
 int emsesg_fx_load(emsesg_ctx* ctx);
 /* Converts the FP32 form back into the FP64 pbuf mirror (for download), in
  * the current buffer order; particles that died since the last sort come

@@ -141,12 +141,14 @@ def _tile_key(cfg, tile, p):
 @pytest.mark.parametrize("npbnd,tile,ppc", [
     ((0, 0, 0), (8, 8, 8), (8, 8)),
     ((1, 2, 0), (8, 4, 8), (8, 8)),
-    # tiles of 43 rows: the move's large shape with 40-column windows; and
-    # of 1 row: one group of all 480 columns
+    # tiles of 28 rows: the move's small shape, 40-column windows; of 1
+    # row: one group of the whole row
     ((0, 0, 0), (8, 8, 8), (40, 1)),
-    # tiles of 103 rows: no window, inv read from global memory, several
-    # batches of slots per group
+    # tiles of 67 rows: the large shape with windows
     ((0, 0, 0), (8, 8, 8), (96, 4)),
+    # tiles of 98 rows: no window, inv read from global memory, several
+    # batches of slots per group
+    ((0, 0, 0), (8, 8, 8), (140, 4)),
 ])
 def test_fx_local_sort_is_a_stable_cell_sort(gpu, npbnd, tile, ppc):
     """The re-sort after a step (the tile-local counting sort) orders the
