@@ -522,7 +522,7 @@ int fx_local_sort(emsesg_ctx* ctx, bool* done) {
   FxState& f = ctx->fx;
   const emsesg_config& c = ctx->cfg;
   Geo g = make_geo(ctx);
-  LcsGeo G[EMSESG_ISPEC];
+  LcsGeo G[EMSESG_ISPEC] = {};
   const int n[3] = {c.nx, c.ny, c.nz};
   for (int is = 0; is < c.nspec; is++) {
     G[is].nbc = 1;
