@@ -13,9 +13,9 @@ struct SlabArgs {
   int64_t count;  // depth * extent_a * extent_b * nc
 };
 
-// Element t of one slab operation.
+// Element t of one slab operation (also run on the host by a test).
 template <typename T>
-__device__ __forceinline__ void slab_apply(T* __restrict__ a, const SlabArgs& s, int64_t t) {
+__host__ __device__ __forceinline__ void slab_apply(T* __restrict__ a, const SlabArgs& s, int64_t t) {
   const SlabOp& o = s.o;
   int ax = o.axis, ea = ax == 0 ? 1 : 0, eb = ax == 2 ? 1 : 2;
   int na = o.hi[ea] - o.lo[ea] + 1, nb = o.hi[eb] - o.lo[eb] + 1;
@@ -114,24 +114,27 @@ inline bool slab_independent(const SlabOp& x, const SlabOp& y) {
   return !boxes_meet(wx, wy) && !boxes_meet(wx, ry) && !boxes_meet(wy, rx);
 }
 
+// Consecutive operations of a list grouped into stages of at most
+// SLAB_MULTI / 2 pairwise independent ones, in list order.
+inline std::vector<std::vector<SlabOp>> slab_stages(const std::vector<SlabOp>& ops) {
+  std::vector<std::vector<SlabOp>> st;
+  for (const SlabOp& o : ops) {
+    bool join = !st.empty() && st.back().size() < SLAB_MULTI / 2;
+    if (join)
+      for (const SlabOp& p : st.back()) join = join && slab_independent(p, o);
+    if (join) st.back().push_back(o);
+    else st.push_back({o});
+  }
+  return st;
+}
+
 // Runs two operation lists on two arrays (each list in its order; the
-// lists are unrelated) in few launches: consecutive independent operations
-// of a list share a stage, and the k-th stages of both lists one launch.
+// lists are unrelated) in few launches: the k-th stages of both lists share
+// one launch.
 template <typename T>
 int run_slab_ops2(emsesg_ctx* ctx, T* a1, const FieldDesc& f1, const std::vector<SlabOp>& ops1, T* a2,
                   const FieldDesc& f2, const std::vector<SlabOp>& ops2, const char* name) {
-  auto stages = [](const std::vector<SlabOp>& ops) {
-    std::vector<std::vector<SlabOp>> st;
-    for (const SlabOp& o : ops) {
-      bool join = !st.empty() && st.back().size() < SLAB_MULTI / 2;
-      if (join)
-        for (const SlabOp& p : st.back()) join = join && slab_independent(p, o);
-      if (join) st.back().push_back(o);
-      else st.push_back({o});
-    }
-    return st;
-  };
-  const auto s1 = stages(ops1), s2 = stages(ops2);
+  const auto s1 = slab_stages(ops1), s2 = slab_stages(ops2);
   const size_t ns = std::max(s1.size(), s2.size());
   for (size_t k = 0; k < ns; k++) {
     SlabMulti<T> m{};
