@@ -595,7 +595,7 @@ class Frame:
 
 
 INTRINSICS = {
-    "int": lambda x: int(x) if not is_int(x) else int(x),
+    "int": lambda x, *kind: int(x),  # truncation toward zero; the kind argument changes no value here
     "floor": lambda x: int(math.floor(x)),
     "nint": lambda x: int(round(x)),
     "dble": float, "real": lambda x, *k: float(x),
@@ -673,6 +673,7 @@ class Interpreter:
             self.run_block(unit.body, fr)
         except _Return:
             pass
+        self.last_frame = fr
         if unit.kind == "function":
             return fr.vars[unit.result or unit.name]
         return None
@@ -781,7 +782,17 @@ class Interpreter:
         if len(parts) == 1:
             name, args = parts[0]
             vals = [self.eval_arg(a, fr) for a in (args or [])]
+            self.last_frame = None
             self.call(name, vals, fr)
+            callee = self.last_frame
+            # arguments pass by reference: a scalar variable or component
+            # given to an interpreted subroutine gets the dummy's final value
+            if callee is not None and callee.unit.name == name:
+                for a, v, dummy in zip(args or [], vals, callee.unit.args):
+                    if isinstance(a, tuple) and a[0] == "des" and not isinstance(v, (FArray, np.ndarray, DerivedObj)):
+                        nv = callee.vars.get(dummy, v)
+                        if nv is not v:
+                            self.assign(a, nv, fr)
             return
         # obj%method(args): type-bound call
         obj = self.eval(("des", parts[:-1]), fr)

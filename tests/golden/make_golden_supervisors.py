@@ -1,0 +1,166 @@
+"""Golden vectors of the injection supervisors, made by EXECUTING THE
+REFERENCE'S OWN FORTRAN SOURCE TEXT (fortran_subset.py, as make_golden.py
+does for the particle path).
+
+psuper2.F90 as a whole uses statements the small interpreter does not run
+(print, array sections, the OhHelp mapping calls of the inner-boundary
+branch), so the pieces on this path are cut out of the file verbatim and
+run on their own:
+
+  * the six outer-boundary inflow blocks (x-bottom .. z-top,
+    src/pcl/psuper2.F90:114-292), wrapped in a subroutine whose variables
+    are the module state the blocks read;
+  * the rectangular-plane emission dispatch on nemd (psuper2.F90:333-362)
+    and the contained emit_from_rectangular_surf (:554-576) it calls.
+
+RANU0 hands out a fixed list of uniforms; oh2_inject_particle collects the
+records.  The fixture holds the tables, the uniforms each piece consumed,
+the counts and the records; tests/test_golden_supervisors.py checks
+ctca_b200/inject.py (and so, through the device tests, the device
+supervisors) against it.
+
+Run from the repository root:
+
+    python tests/golden/make_golden_supervisors.py [--reference DIR]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
+sys.path.insert(0, str(HERE.parent.parent))
+
+from fortran_subset import DerivedObj, FArray, Interpreter, parse_source  # noqa: E402
+
+from ctca_b200 import inject  # noqa: E402
+from ctca_b200.emses import PARTICLE_DTYPE  # noqa: E402
+
+FIELDS = ("x", "y", "z", "vx", "vy", "vz", "pid", "preside", "nid", "spec")
+
+
+def cut(lines, start_pat, stop_pat, include_stop=False):
+    """Lines from the first one containing start_pat up to the first later
+    one containing stop_pat."""
+    i0 = next(i for i, l in enumerate(lines) if start_pat in l)
+    i1 = next(i for i in range(i0 + 1, len(lines)) if stop_pat in lines[i])
+    return lines[i0:i1 + (1 if include_stop else 0)]
+
+
+def pieces(ref: Path) -> str:
+    lines = (ref / "src/pcl/psuper2.F90").read_text().splitlines()
+    inflow = cut(lines, "!-------------------- x-bottom", "!============================== from inner boundary")
+    assert any("narrzb(is)" in l for l in inflow) and sum("oh2_inject_particle" in l for l in inflow) == 6
+    # the dispatch on nemd of the rectangular surfaces, up to its end if
+    i0 = next(i for i, l in enumerate(lines) if "if(nemd(iepl).eq. 1) then" in l)
+    i1 = next(i for i in range(i0, len(lines)) if lines[i].strip() == "end if")
+    emit = lines[i0:i1 + 1]
+    assert sum("call emit_from_rectangular_surf" in l for l in emit) == 6
+    surf = cut(lines, "subroutine emit_from_rectangular_surf &", "end subroutine emit_from_rectangular_surf",
+               include_stop=True)
+    text = ["subroutine golden_inflow(ustep)",
+            "  integer(kind=4) :: m, iran, addr1, addr2, icon, ustep"] + inflow + [
+            "end subroutine golden_inflow", "",
+            "subroutine golden_emit(m)",
+            "  integer(kind=4) :: m"] + emit + ["end subroutine golden_emit", ""] + surf
+    return "\n".join(text) + "\n"
+
+
+def record_of(p) -> tuple:
+    return tuple(p[f] for f in FIELDS)
+
+
+def make(ref: Path) -> dict:
+    units = parse_source(pieces(ref))
+    rng = np.random.default_rng(20251203)
+    npr = 64
+    ext = (24, 20, 32)
+    uniforms = rng.random(200000)
+    pos = [0]
+    injected = []
+
+    def ranu0(dranu, n, icon):
+        for i in range(int(n)):
+            dranu.data[i] = uniforms[pos[0]]
+            pos[0] += 1
+
+    def inject_rec(p):
+        injected.append(record_of(p))
+
+    tab = lambda a: FArray(np.asarray(a, dtype=np.float64).copy(), [1])  # noqa: E731
+    # tables of one species (nprs = 1): normal speeds per face, tangential ones
+    vth, vd = 0.05, 0.02
+    t = {"vxf": inject.flux_table(vth, vd, npr, 1.0), "vxb": inject.flux_table(vth, vd, npr, -1.0),
+         "vyf": inject.flux_table(vth, -vd, npr, 1.0), "vyb": inject.flux_table(vth, -vd, npr, -1.0),
+         "vzf": inject.flux_table(vth, 0.0, npr, 1.0), "vzb": inject.flux_table(vth, 0.0, npr, -1.0),
+         "vxr": inject.maxwell_table(vth, vd, npr), "vyr": inject.maxwell_table(vth, -vd, npr),
+         "vzr": inject.maxwell_table(vth, 0.0, npr)}
+    ustep, injct, istep, lstep = 2, 1, 7, 0
+    arr = {"arrxf": 13.7, "arrxb": 9.2, "arryf": 11.4, "arryb": 8.9, "arrzf": 15.3, "arrzb": 12.1}
+    zssurf = 0.004  # some z-bottom particles stay below: dropped (psuper2.F90 `cycle`)
+    pinj = FArray(np.zeros(1, dtype=PARTICLE_DTYPE), [1])
+    g = {"is": 1, "nprs": 1, "npr": FArray(np.array([npr], dtype=np.int64), [1]),
+         "npbnd": FArray(np.full((3, 1), 2, dtype=np.int64), [1, 1]),
+         "bared": FArray(np.ones((2, 3, 1), dtype=np.int64), [1, 1, 1]),
+         "sdid": FArray(np.array([0], dtype=np.int64), [1]),
+         "istep": istep, "lstep": lstep, "injct": FArray(np.array([injct], dtype=np.int64), [1]),
+         "injctisw": FArray(np.array([injct * ustep], dtype=np.int64), [1]),
+         "xl": 0, "xu": ext[0], "yl": 0, "yu": ext[1], "zl": 0, "zu": ext[2],
+         "zssurf": zssurf, "ubhole": -1.0e30, "dranu": FArray(np.zeros(200000), [1]), "pinj": pinj}
+    for k, v in t.items():
+        g[k] = tab(v)
+    for k, v in arr.items():
+        g[k] = FArray(np.array([v]), [1])
+        g["n" + k] = FArray(np.zeros(1, dtype=np.int64), [1])
+    it = Interpreter(units, g, {"ranu0": ranu0, "oh2_inject_particle": inject_rec})
+    it.call("golden_inflow", [ustep])
+    out = {"npr": np.int64(npr), "ext": np.array(ext, dtype=np.int64), "ustep": np.int64(ustep),
+           "injct": np.int64(injct), "istep": np.int64(istep), "lstep": np.int64(lstep), "zssurf": np.float64(zssurf),
+           "uniforms": uniforms[:pos[0]].copy(), "inflow_records": np.array(injected, dtype=PARTICLE_DTYPE)}
+    for k, v in t.items():
+        out["tab_" + k] = v
+    for k in arr:
+        out["arr_" + k] = np.float64(arr[k])
+        out["count_" + k] = np.int64(g["n" + k].data[0])
+    used_inflow = pos[0]
+    # plane emission: per face, n particles with RANU0(dranu, n*6) first
+    vnormf, vtangf = inject.flux_table(0.01, 0.0, npr), inject.maxwell_table(0.01, 0.0, npr)
+    g.update(vnormf=tab(vnormf), vtangf=tab(vtangf), iepl=1)
+    faces = [(1, 16.0), (-1, 8.0), (2, 12.5), (-2, 7.0), (3, 18.0), (-3, 14.0)]
+    bounds = {"xl": 4.0, "xu": 20.0, "yl": 3.0, "yu": 17.0, "zl": 6.0, "zu": 26.0}
+    emitted = []
+    for nemd, grd in faces:
+        n = 40
+        g["nemd"] = FArray(np.array([nemd], dtype=np.int64), [1])
+        g["peject"] = FArray(np.array([DerivedObj(grd=grd, **bounds)], dtype=object), [1])
+        ranu0(g["dranu"], n * 6, 0)
+        for m in range(1, n + 1):
+            pinj.data[0] = np.zeros(1, dtype=PARTICLE_DTYPE)[0]
+            it.call("golden_emit", [m])
+            emitted.append(record_of(pinj.data[0]))
+    out["emit_faces"] = np.array(faces, dtype=np.float64)
+    out["emit_bounds"] = np.array([bounds[k] for k in ("xl", "xu", "yl", "yu", "zl", "zu")])
+    out["emit_n"] = np.int64(40)
+    out["emit_uniforms"] = uniforms[used_inflow:pos[0]].copy()
+    out["emit_vnormf"] = vnormf
+    out["emit_vtangf"] = vtangf
+    out["emit_records"] = np.array(emitted, dtype=PARTICLE_DTYPE)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("EMSES_REFERENCE", "/root/reference"))
+    args = ap.parse_args()
+    out = make(Path(args.reference))
+    np.savez_compressed(HERE / "supervisors.npz", **out)
+    print(f"inflow records {out['inflow_records'].size}, emitted {out['emit_records'].size}")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,73 @@
+"""The host injection supervisors (ctca_b200/inject.py) against golden
+vectors made by executing the reference's own psuper2.F90 text
+(tests/golden/make_golden_supervisors.py): the inflow counts and records of
+all six outer faces (psuper2.F90:114-292, with the z-surface drop) and the
+rectangular-plane emission of every face orientation (:333-362, 554-576),
+bit for bit on the same uniforms.  The device supervisors are checked
+against these host ones by tests/test_gpu_supervisors.py."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from ctca_b200 import inject
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "supervisors.npz"
+KIN = ("x", "y", "z", "vx", "vy", "vz")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    if not GOLDEN.exists():
+        pytest.skip("supervisors.npz not generated")
+    return dict(np.load(GOLDEN))
+
+
+def test_inflow_counts_and_records(gold):
+    nx, ny, nz = (int(v) for v in gold["ext"])
+    ustep, injct = int(gold["ustep"]), int(gold["injct"])
+    istep, lstep = int(gold["istep"]), int(gold["lstep"])
+    t = {k[4:]: gold[k] for k in gold if k.startswith("tab_")}
+    # face order of psuper2: x-bottom, x-top, y-bottom, y-top, z-bottom, z-top
+    faces = [("arrxf", 0, True, t["vxf"], t["vyr"], t["vzr"]), ("arrxb", 0, False, t["vxb"], t["vyr"], t["vzr"]),
+             ("arryf", 1, True, t["vyf"], t["vxr"], t["vzr"]), ("arryb", 1, False, t["vyb"], t["vxr"], t["vzr"]),
+             ("arrzf", 2, True, t["vzf"], t["vxr"], t["vyr"]), ("arrzb", 2, False, t["vzb"], t["vxr"], t["vyr"])]
+    u = gold["uniforms"]
+    pos = 0
+    recs = []
+    for key, axis, front, vn, va, vb in faces:
+        n = inject.inflow_count(istep, lstep, float(gold["arr_" + key]), injct, ustep)
+        assert n == int(gold["count_" + key]), key
+        uu = u[pos:pos + 5 * n].reshape(n, 5)
+        pos += 5 * n
+        recs.append(inject.inflow(axis, front, n, nx, ny, nz, vn, va, vb, float(injct * ustep), None, spec=1,
+                                  zssurf=float(gold["zssurf"]), uniforms=uu))
+    assert pos == u.size
+    got = np.concatenate(recs)
+    want = gold["inflow_records"]
+    assert got.size == want.size and got.size > 0
+    assert want.size < sum(int(gold["count_" + f[0]]) for f in faces)  # the surface drop happened
+    for f in KIN:
+        assert np.array_equal(got[f], want[f]), f
+    assert np.array_equal(got["preside"], want["preside"])
+    assert np.array_equal(got["spec"], want["spec"])
+
+
+def test_plane_emission_records(gold):
+    n = int(gold["emit_n"])
+    xl, xu, yl, yu, zl, zu = gold["emit_bounds"]
+    tang = {1: ((yl, yu), (zl, zu)), 2: ((zl, zu), (xl, xu)), 3: ((xl, xu), (yl, yu))}
+    injctisw = float(int(gold["injct"]) * int(gold["ustep"]))
+    u = gold["emit_uniforms"]
+    out = []
+    for k, (nemd, grd) in enumerate(gold["emit_faces"]):
+        nemd = int(nemd)
+        b1, b2 = tang[abs(nemd)]
+        uu = u[k * 6 * n:(k + 1) * 6 * n].reshape(n, 6)
+        out.append(inject.emit_plane(nemd, float(grd), b1, b2, n, gold["emit_vnormf"], gold["emit_vtangf"], injctisw,
+                                     None, spec=1, uniforms=uu))
+    got = np.concatenate(out)
+    want = gold["emit_records"]
+    assert got.size == want.size
+    for f in KIN:
+        assert np.array_equal(got[f], want[f]), f
