@@ -1016,7 +1016,9 @@ __device__ __forceinline__ double lin(double lo, double hi, double u) {
 }
 
 // Emitted pairs (psuper3.F90:142-208): pair k -> records 2k (anti-particle
-// on the face) and 2k+1 (its twin 1e-5 off the face, preside 1).
+// on the face) and 2k+1 (its twin 1e-5 off the face, preside 1; the
+// reference adds 1e-5 as a single precision literal, so the offset is
+// (double)1e-5f).
 __global__ void k_gen_emit(emsesg_particle* out, int32_t* ord, int64_t n, int nemd, double grd, double b1lo,
                            double b1hi, double b2lo, double b2hi, const double* __restrict__ vnorm,
                            const double* __restrict__ vtang, int npr, uint64_t seed, uint64_t stream,
@@ -1040,7 +1042,7 @@ __global__ void k_gen_emit(emsesg_particle* out, int32_t* ord, int64_t n, int ne
   p.preside = EMSESG_PCL_TO_BE_ACCUMULATED_AS_ANTIPCL;
   out[2 * k] = p;
   ord[2 * k] = 0;
-  r[ax0] = __dadd_rn(grd, __dmul_rn(ud, 1e-5));
+  r[ax0] = __dadd_rn(grd, __dmul_rn(ud, (double)1e-5f));
   p.preside = EMSESG_PCL_INJECTED;
   out[2 * k + 1] = p;
   ord[2 * k + 1] = (int32_t)(pending + k + 1);

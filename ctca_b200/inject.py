@@ -90,6 +90,11 @@ def emission_count(istep: int, lstep: int, fluxf: float, injct: int, ustep: int)
 _ORDER = {1: (0, 1, 2), 2: (1, 2, 0), 3: (2, 0, 1)}
 
 
+# The twin's offset from the face: psuper3.F90:196-206 adds the literal 1e-5,
+# a default (single precision) real in the reference's build, to a double.
+TWIN_OFFSET = float(np.float32(1e-5))
+
+
 def emit_rectangle(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int, vnormf: np.ndarray,
                    vtangf: np.ndarray, rng: np.random.Generator | None, spec: int,
                    uniforms: np.ndarray | None = None) -> np.ndarray:
@@ -118,7 +123,7 @@ def emit_rectangle(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int
         c, v = coords[ax]
         r2 = np.repeat(val_r, 2)
         if ax == axis[0]:
-            r2[1::2] += ud * 1e-5
+            r2[1::2] += ud * TWIN_OFFSET
         out[c] = r2
         out[v] = np.repeat(val_v, 2)
     out["preside"] = np.tile(np.array([PCL_ANTI, PCL_INJECTED], dtype=np.int32), n)

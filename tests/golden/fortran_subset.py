@@ -152,8 +152,10 @@ def tokenize(s: str):
             body = re.sub(r"_\w+$", "", txt)
             if re.fullmatch(r"\d+", body):
                 toks.append(("num", int(body)))
+            elif "d" in body or body != txt:
+                toks.append(("num", float(body.replace("d", "e"))))  # double precision (d exponent or kind)
             else:
-                toks.append(("num", float(body.replace("d", "e"))))
+                toks.append(("num", float(np.float32(float(body)))))  # default real: single precision
             continue
         if c.isalpha() or c == "_":
             m = re.match(r"[a-z_][a-z0-9_]*", s[i:])

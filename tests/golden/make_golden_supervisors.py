@@ -11,7 +11,11 @@ run on their own:
     src/pcl/psuper2.F90:114-292), wrapped in a subroutine whose variables
     are the module state the blocks read;
   * the rectangular-plane emission dispatch on nemd (psuper2.F90:333-362)
-    and the contained emit_from_rectangular_surf (:554-576) it calls.
+    and the contained emit_from_rectangular_surf (:554-576) it calls;
+  * the emission pairs of psuper3 (emit_from_rectangle, psuper3.F90:142-208,
+    with its own emit_from_rectangular_surf, :210-240; the BLOCK construct
+    around three local declarations is unwrapped), oh3_map_particle_to_
+    subdomain answering this rank.
 
 RANU0 hands out a fixed list of uniforms; oh2_inject_particle collects the
 records.  The fixture holds the tables, the uniforms each piece consumed,
@@ -69,6 +73,17 @@ def pieces(ref: Path) -> str:
             "subroutine golden_emit(m)",
             "  integer(kind=4) :: m"] + emit + ["end subroutine golden_emit", ""] + surf
     return "\n".join(text) + "\n"
+
+
+def pieces3(ref: Path) -> str:
+    lines = (ref / "src/pcl/psuper3.F90").read_text().splitlines()
+    rect = cut(lines, "subroutine emit_from_rectangle", "end subroutine", include_stop=True)
+    rect[0] = rect[0].replace("subroutine emit_from_rectangle", "subroutine emit_from_rectangle()")  # empty list
+    surf = cut(lines, "subroutine emit_from_rectangular_surf(", "end subroutine emit_from_rectangular_surf",
+               include_stop=True)
+    surf = [l for l in surf if not (l.strip().startswith("block") or l.strip().startswith("end block"))]
+    assert sum("oh2_inject_particle" in l for l in rect) == 2
+    return "\n".join(rect + [""] + surf) + "\n"
 
 
 def record_of(p) -> tuple:
@@ -150,6 +165,23 @@ def make(ref: Path) -> dict:
     out["emit_vnormf"] = vnormf
     out["emit_vtangf"] = vtangf
     out["emit_records"] = np.array(emitted, dtype=PARTICLE_DTYPE)
+    # psuper3 emission pairs: nemit(iepl) pairs per face
+    used_plane = pos[0]
+    units3 = parse_source(pieces3(ref))
+    pinj2 = FArray(np.zeros(2, dtype=PARTICLE_DTYPE), [1])
+    injected.clear()
+    g3 = dict(g)
+    g3.update(pinj=pinj2, m=0, xl=0, xu=ext[0], yl=0, yu=ext[1], zl=0, zu=ext[2])
+    it3 = Interpreter(units3, g3, {"ranu0": ranu0, "oh2_inject_particle": inject_rec,
+                                   "oh3_map_particle_to_subdomain": lambda *a: 0})
+    for nemd, grd in faces:
+        g3["nemd"] = FArray(np.array([nemd], dtype=np.int64), [1])
+        g3["nemit"] = FArray(np.array([40], dtype=np.int64), [1])
+        g3["peject"] = FArray(np.array([DerivedObj(grd=grd, **bounds)], dtype=object), [1])
+        ranu0(g3["dranu"], 40 * 6, 0)
+        it3.call("emit_from_rectangle", [])
+    out["pair_uniforms"] = uniforms[used_plane:pos[0]].copy()
+    out["pair_records"] = np.array(injected, dtype=PARTICLE_DTYPE)
     return out
 
 
@@ -159,7 +191,8 @@ def main():
     args = ap.parse_args()
     out = make(Path(args.reference))
     np.savez_compressed(HERE / "supervisors.npz", **out)
-    print(f"inflow records {out['inflow_records'].size}, emitted {out['emit_records'].size}")
+    print(f"inflow records {out['inflow_records'].size}, emitted {out['emit_records'].size}, "
+          f"pair records {out['pair_records'].size}")
 
 
 if __name__ == "__main__":

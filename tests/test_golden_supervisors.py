@@ -71,3 +71,24 @@ def test_plane_emission_records(gold):
     assert got.size == want.size
     for f in KIN:
         assert np.array_equal(got[f], want[f]), f
+
+
+def test_emission_pairs(gold):
+    """psuper3's emission pairs (emit_from_rectangle, psuper3.F90:142-208):
+    an anti-particle on the face and its twin 1e-5 off it, per face."""
+    n = int(gold["emit_n"])
+    xl, xu, yl, yu, zl, zu = gold["emit_bounds"]
+    tang = {1: ((yl, yu), (zl, zu)), 2: ((zl, zu), (xl, xu)), 3: ((xl, xu), (yl, yu))}
+    u = gold["pair_uniforms"]
+    out = []
+    for k, (nemd, grd) in enumerate(gold["emit_faces"]):
+        nemd = int(nemd)
+        b1, b2 = tang[abs(nemd)]
+        uu = u[k * 6 * n:(k + 1) * 6 * n].reshape(n, 6)
+        out.append(inject.emit_rectangle(nemd, float(grd), b1, b2, n, gold["emit_vnormf"], gold["emit_vtangf"], None,
+                                         spec=1, uniforms=uu))
+    got = np.concatenate(out)
+    want = gold["pair_records"]
+    assert got.size == want.size == 2 * n * len(gold["emit_faces"])
+    for f in KIN + ("preside", "spec", "pid"):
+        assert np.array_equal(got[f], want[f]), f
