@@ -12,6 +12,8 @@ run on their own:
     are the module state the blocks read;
   * the rectangular-plane emission dispatch on nemd (psuper2.F90:333-362)
     and the contained emit_from_rectangular_surf (:554-576) it calls;
+  * the emission count of psuper3 (psuper3.F90:68-69), over a grid of
+    steps and fluxes;
   * the emission pairs of psuper3 (emit_from_rectangle, psuper3.F90:142-208,
     with its own emit_from_rectangular_surf, :210-240; the BLOCK construct
     around three local declarations is unwrapped), oh3_map_particle_to_
@@ -181,6 +183,24 @@ def make(ref: Path) -> dict:
         ranu0(g3["dranu"], 40 * 6, 0)
         it3.call("emit_from_rectangle", [])
     out["pair_uniforms"] = uniforms[used_plane:pos[0]].copy()
+    # the emission count statement, cut out of psuper3.F90
+    lines = (ref / "src/pcl/psuper3.F90").read_text().splitlines()
+    cnt = cut(lines, "nemit(iepl) = (int((istep + lstep)*fluxf(iepl), 8)", "ipcplane = ipcpl(iepl)")
+    units_c = parse_source("\n".join(["subroutine golden_count(ustep)", "  integer(kind=4) :: ustep"] + cnt +
+                                     ["end subroutine golden_count", ""]))
+    rows = []
+    for istep in (0, 1, 7, 123):
+        for lstep in (0, 5):
+            for injct in (1, 3):
+                for fluxf in (0.37, 2.5, 1048576.0, 13.09):
+                    for ustep in (1, 2):
+                        gc = {"istep": istep, "lstep": lstep, "iepl": 1, "is": 1,
+                              "injct": FArray(np.array([injct], dtype=np.int64), [1]),
+                              "fluxf": FArray(np.array([fluxf]), [1]),
+                              "nemit": FArray(np.zeros(1, dtype=np.int64), [1])}
+                        Interpreter(units_c, gc, {}).call("golden_count", [ustep])
+                        rows.append((istep, lstep, injct, fluxf, ustep, int(gc["nemit"].data[0])))
+    out["count_rows"] = np.array(rows, dtype=np.float64)
     out["pair_records"] = np.array(injected, dtype=PARTICLE_DTYPE)
     return out
 

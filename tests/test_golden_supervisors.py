@@ -92,3 +92,10 @@ def test_emission_pairs(gold):
     assert got.size == want.size == 2 * n * len(gold["emit_faces"])
     for f in KIN + ("preside", "spec", "pid"):
         assert np.array_equal(got[f], want[f]), f
+
+
+def test_emission_count(gold):
+    """nemit of psuper3.F90:68-69 over steps, step offsets, intervals,
+    fluxes and ustep."""
+    for istep, lstep, injct, fluxf, ustep, n in gold["count_rows"]:
+        assert inject.emission_count(int(istep), int(lstep), fluxf, int(injct), int(ustep)) == int(n)
