@@ -372,8 +372,8 @@ class Unit:
 
 
 DECL_TYPES = ("integer", "real", "double precision", "logical", "type(", "type (", "character")
-HEADER = re.compile(r"^(?:pure\s+|elemental\s+|recursive\s+)*(subroutine|function)\s+(\w+)\s*\(([^)]*)\)\s*"
-                    r"(?:result\s*\((\w+)\))?")
+HEADER = re.compile(r"^(?:pure\s+|elemental\s+|recursive\s+)*(subroutine|function)\s+(\w+)\s*(?:\(([^)]*)\))?\s*"
+                    r"(?:result\s*\((\w+)\))?$")
 END_UNIT = re.compile(r"^end(\s*(subroutine|function)\b.*)?$")
 
 
@@ -450,7 +450,7 @@ class SourceParser:
 
     def unit(self):
         m = HEADER.match(self.lines[self.i])
-        u = Unit(m.group(1), m.group(2), [a.strip() for a in m.group(3).split(",") if a.strip()], m.group(4))
+        u = Unit(m.group(1), m.group(2), [a.strip() for a in (m.group(3) or "").split(",") if a.strip()], m.group(4))
         self.i += 1
         stmts = self.block(lambda l: l == "contains" or END_UNIT.match(l) is not None)
         for st in stmts:

@@ -15,6 +15,7 @@ these files use) runs them from the text of
     src/pcl/positn.F90           positn
     src/field/bfield.F90         bfield
     src/field/efield.F90         efield
+    src/etc/energy.F90           energy (MPI_Reduce of one rank: a no-op)
 
 with IEEE double arithmetic in source order (Python floats: no fused
 multiply-add, no reassociation), Fortran integer division and int()
@@ -62,7 +63,7 @@ from ctca_b200.emses import INPC, ISPEC, PARTICLE_DTYPE, Body, Config, field_sha
 
 SOURCES = ["src/field/grdcrt.F90", "src/pcl2field/psolve2.F90", "src/pcl2field/psolve1.F90",
            "src/pcl2field/charge.F90", "src/field/rhoupd.F90", "src/pcl/positn.F90",
-           "src/field/bfield.F90", "src/field/efield.F90"]
+           "src/field/bfield.F90", "src/field/efield.F90", "src/etc/energy.F90"]
 # tcs of efield (src/main/inital.F90:78, rescal.F90:132) for the field-step
 # fixtures: 2 (c dt)^2 in internal units with c dt / dx = 0.5
 TCS = 0.125
@@ -372,6 +373,13 @@ def run_case(units, name, c, ustep, opts):
     out["positn_nranu"] = np.int64(pos[0])
     for k, v in counters(gc).items():
         out["positn_" + k] = v
+    # energy of the initial state (kinetic per species and axis)
+    g.update(engk=FArray(np.zeros((3, cfg.nspec))), engeb=FArray(np.zeros(2)), cs=1.0,
+             rm=FArray(np.array([cfg.rm[i] for i in range(cfg.nspec)], dtype=np.float64)),
+             engkg=FArray(np.zeros((3, cfg.nspec))), engebg=FArray(np.zeros(2)), mpi_real8=0, mpi_sum=0, mcw=0)
+    ext["mpi_reduce"] = lambda *a: None
+    it.call("energy", [])
+    out["energy_engk"] = g["engk"].data.copy()
     # grdcrt + psolve1(func=1): zigzag current, then the J border reduction
     f = fields()
     pb = p0.copy()

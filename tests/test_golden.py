@@ -122,3 +122,14 @@ def test_field_step(path):
     assert same(o.eb, d["efield_eb"]), first_diff(o.eb, d["efield_eb"])
     o.exchange_eb()
     assert same(o.eb, d["exchange_eb"]), first_diff(o.eb, d["exchange_eb"])
+
+
+@pytest.mark.parametrize("path", CASES, ids=lambda p: p.stem)
+def test_energy(path):
+    """Kinetic energy per species and axis (energy.F90:29-47) of the state
+    after positn, bit for bit."""
+    d, cfg = load(path)
+    o = oracle_for(d, cfg, d["positn_pbuf"].copy())
+    e = o.energy().reshape(cfg.nspec, 3).T
+    want = d["energy_engk"]
+    assert same(e, want), first_diff(e, want)
