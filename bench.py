@@ -147,48 +147,100 @@ def max_over_ranks(world, x: float) -> float:
 
 
 # --------------------------------------------------------------- CPU baseline
-def cpu_sample(seconds: float, threads: int):
-    """The oracle's psolve1 + charge on the 128^3 grid with 1 particle per
-    cell per species (4.19 M particles): a bounded sample of the workload."""
+def headline_case(cells: int = 0, ppc: int = 0):
+    """The headline workload (128^3, 2 species x 64 ppc, mass ratio 1836,
+    ion drift, 8 E and 8 dB modes), or a smaller copy for profiler captures."""
+    from ctca_b200 import inputs
+    case = inputs.workload_case(2)
+    if cells:
+        case.n = (cells, cells, cells)
+        case.kmax = 4 * 2 * math.pi / cells
+        for sp in case.species:
+            sp.ppc = ppc or sp.ppc
+    return case
+
+
+def headline_config(case, npart: int, world: int) -> dict:
+    return {"workload": f"{case.n[0]}^3 periodic, 2 species x {case.species[0].ppc} ppc ({npart:,} particles), "
+                        "mass ratio 1836, sort every 4; FP32 cell+offset particles, int64 rho/J at 2^40",
+            "l2": f"inputs larger than L2 ({npart * 28 / 1e9:.2f} GB particle state)",
+            "parallelism": f"replicas x{world}"}
+
+
+def cpu_blocks(case, layers: int | None, threads: int, seconds: float, min_steps: int, max_steps: int,
+               restore: bool = True, warmup: int = 1) -> dict:
+    """Times the oracle's psolve1 + charge in the reference's one rank per
+    core (oracle.Blocks) on the first `layers` z layers of `case` (all of it
+    when None): particle-steps per second over the timed steps, after
+    `warmup` untimed ones (with `restore`)."""
     from ctca_b200 import inputs
     from oracle import oracle as O
-    case = inputs.workload_case(2)
-    for s in case.species:
-        s.ppc = 1
     cfg = inputs.make_config(case)
     eb = inputs.make_fields(case)
-    pl = inputs.plasma(case)
-    pbuf, tp = O.load_plasma(cfg, pl)
-    o = O.Oracle(cfg, pbuf[:0], [0, 0], eb)
+    cells = None if layers is None else case.n[0] * case.n[1] * layers
+    p, tp = inputs.make_particles(case, cells=cells)
+    o = O.Oracle(cfg, p[:0], [0] * cfg.nspec, eb)
     o.grdcrt()
-    wrk = o.f["wrk"]
-    n = int(tp.sum())
-    t_total, steps = 0.0, 0
-    while t_total < seconds or steps < 1:
-        dt, _, _ = O.step_timed(cfg, 2, wrk, pbuf, tp, threads)
-        t_total += dt
-        steps += 1
-    return n * steps / t_total, f"128^3 grid, 2 species x 1 ppc ({n} particles), psolve1+charge, {steps} steps", steps
+    b = O.Blocks(cfg, o.f["wrk"], p, tp, threads)
+    del p, o
+    for _ in range(warmup if restore else 0):
+        b.step(2)  # untimed
+    ts = []
+    while len(ts) < max_steps and (len(ts) < min_steps or sum(ts) < seconds):
+        ts.append(b.step(2, restore))
+    out = {"value": b.particles * len(ts) / sum(ts), "threads": b.threads, "particles": b.particles,
+           "steps": len(ts), "s_per_step": sum(ts) / len(ts)}
+    b.close()
+    return out
+
+
+def cpu_baseline(threads: int) -> dict:
+    """The reference's CPU path, timed on the host cores: the headline
+    workload's plasma (a sample of its z layers at the full 64 ppc) on one
+    thread and on all threads, and the 32^3 x 16 ppc case for 10 steps."""
+    from ctca_b200 import inputs
+    allt = cpu_blocks(headline_case(), 8, threads, 3.0, 3, 20)
+    one = cpu_blocks(headline_case(), 1, 1, 2.0, 2, 10)
+    c1 = inputs.workload_case(1)
+    c1_one = cpu_blocks(c1, None, 1, 0.0, 10, 10, restore=False)
+    c1_all = cpu_blocks(c1, None, threads, 0.0, 10, 10, restore=False)
+    return {
+        "value": allt["value"], "unit": UNIT, "cores": allt["threads"], "kind": "port",
+        "sample": (f"first 8 z layers of the 128^3 x 2 species x 64 ppc workload ({allt['particles']:,} particles, "
+                   "the same plasma drawn on the host), the oracle's psolve1 + charge (FP64, g++ -O3), one block "
+                   f"of x rows per thread as one rank per core, {allt['steps']} steps each from the same particles"),
+        "single_thread": {"value": one["value"], "unit": UNIT, "cores": 1,
+                          "sample": f"first z layer ({one['particles']:,} particles), {one['steps']} steps"},
+        "config_32cube_16ppc": {"workload": "32^3 periodic, 2 species x 16 ppc (1,048,576 particles), mass ratio "
+                                            "100, B0 (0,0,0.2), E0 + 4 modes, 10 steps",
+                                "threads_1": c1_one["value"], "threads_all": c1_all["value"],
+                                "cores": c1_all["threads"], "unit": UNIT},
+    }
 
 
 def run_reference(args, world, rank):
+    """The reference's CPU path on the host cores (rank 0 only): the oracle's
+    psolve1 + charge, one block of x rows per thread, on the first 8 z layers
+    of the headline workload at its full 64 ppc; every timed step is one step
+    of that sample from the same particles."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    secs = max(1.0, 3.0 * args.steps / max(args.steps, 1))
-    for _ in range(max(args.warmup, 0) and 1):
-        cpu_sample(0.1, threads)
-    value, sample, steps = cpu_sample(min(60.0, 2.0 * args.steps), threads)
+    case = headline_case()
+    total = sum(sp.ppc for sp in case.species) * case.n[0] * case.n[1] * case.n[2]
+    r = cpu_blocks(case, 8, threads, 0.0, args.steps, args.steps, warmup=max(args.warmup, 0))
+    sample = (f"first 8 z layers of the workload ({r['particles']:,} particles, the same plasma drawn on the host), "
+              "the oracle's psolve1 + charge (FP64 restatement of the reference; the Fortran reference is not "
+              "buildable: no Fortran/MPI/HDF5/FFTW toolchain), one block of x rows per thread as one rank per core; "
+              "each step from the same particles")
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 268435456 / value * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "impl": "reference",
-        "config": {"workload": "128^3 periodic, 2 species x 64 ppc (268M particles), sort every 4",
-                   "sample": sample, "note": "oracle restatement of psolve1+charge (Fortran reference not "
-                                             "buildable: no Fortran/MPI/HDF5/FFTW toolchain)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": r["steps"],
+        "warmup": args.warmup, "ms_per_step": r["s_per_step"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": headline_config(case, total, 1),
+        "sample": sample,
+        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "port", "sample": sample},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -265,14 +317,8 @@ def run_ours(args, world, rank, local):
 
     torch.cuda.set_device(local)
     select_device(local)
-    case = inputs.workload_case(2)
-    if args.cells:
-        # smaller copy of the workload for profiler captures (not the headline)
-        n = args.cells
-        case.n = (n, n, n)
-        case.kmax = 4 * 2 * math.pi / n
-        for sp in case.species:
-            sp.ppc = args.ppc or sp.ppc
+    # args.cells: a smaller copy of the workload for profiler captures (not the headline)
+    case = headline_case(args.cells, args.ppc)
     cfg = inputs.make_config(case)
     eb = inputs.make_fields(case)
     npart = sum(cfg.capacity[i] for i in range(cfg.nspec))
@@ -366,10 +412,7 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_time * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+i64", "data": "synthetic",
-        "config": {"workload": f"{case.n[0]}^3 periodic, 2 species x {case.species[0].ppc} ppc ({npart:,} particles), "
-                               "mass ratio 1836, sort every 4; FP32 cell+offset particles, int64 rho/J at 2^40",
-                   "l2": f"inputs larger than L2 ({npart * 28 / 1e9:.2f} GB particle state)",
-                   "parallelism": f"replicas x{world}"},
+        "config": headline_config(case, npart, world),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                      "kernel": "fx_push", "peak_kind": peak_kind,
@@ -388,9 +431,7 @@ def run_ours(args, world, rank, local):
         out["adjoint"] = time_adjoint()
         out["ensemble"] = ensemble_sample(args.ensemble_runs, args.ensemble_steps)
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, sample, _ = cpu_sample(args.cpu_seconds, os.cpu_count() or 1)
-        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-                               "sample": sample}
+        out["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
     g.close()
     if rank == 0:
         print(json.dumps(out), flush=True)

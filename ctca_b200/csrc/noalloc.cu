@@ -15,7 +15,8 @@
 // contents.  Every entry a call reads is written by the same call first, so
 // nothing has to start at zero.  Two calls whose kernels overlap on the GPU
 // (different streams, or different host threads) use the same scratch and
-// race: the caller must order them, e.g. on one stream.
+// race: the caller must order them, e.g. on one stream.  The input, the
+// output and the survivor count must not share a byte (EMSESG_ERR_ARG).
 #include <mutex>
 
 #include "common.cuh"
@@ -98,23 +99,35 @@ __global__ void k_na_scatter(const emsesg_particle* __restrict__ in, int64_t n, 
   if (in[m].nid != -1) out[tile_sum[m / NA_TILE] + local[m]] = in[m];
 }
 
-// Device address of the scratch, looked up once per device (host code may
-// not use the symbol itself as a device pointer).
+// Device address of the scratch per device.  Host code may not use the
+// symbol itself as a device pointer.  Outside a stream capture every call
+// looks the address up again (cheap), so a device reset, after which the
+// module is loaded anew, leaves no stale pointer; inside a capture the address
+// of the last call outside it is used.
 constexpr int NA_MAX_DEVICES = 64;
 uint32_t* g_scratch_ptr[NA_MAX_DEVICES] = {nullptr};
 std::mutex g_scratch_mu;
 
-int scratch_for_current_device(uint32_t** out) {
+int scratch_for_current_device(cudaStream_t st, uint32_t** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return EMSESG_ERR_CUDA;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) return EMSESG_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_compact_scratch) != cudaSuccess || !p) return EMSESG_ERR_CUDA;
     g_scratch_ptr[dev] = (uint32_t*)p;
   }
+  if (!g_scratch_ptr[dev]) return EMSESG_ERR_CUDA;  // first call on this device inside a capture
   *out = g_scratch_ptr[dev];
   return EMSESG_OK;
+}
+
+// [a, a + na) and [b, b + nb) share a byte.
+bool overlap(const void* a, size_t na, const void* b, size_t nb) {
+  const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+  return na > 0 && nb > 0 && x < y + nb && y < x + na;
 }
 
 }  // namespace
@@ -122,16 +135,34 @@ int scratch_for_current_device(uint32_t** out) {
 extern "C" int emsesg_compact_noalloc(const emsesg_particle* d_in, int64_t n, emsesg_particle* d_out,
                                       int64_t* d_kept, void* stream) {
   if (n < 0 || n > NA_MAX || (n > 0 && (!d_in || !d_out)) || !d_kept) return EMSESG_ERR_ARG;
-  if (d_in == d_out && n > 0) return EMSESG_ERR_ARG;
-  uint32_t* scratch = nullptr;
-  int rc = scratch_for_current_device(&scratch);
-  if (rc) return rc;
+  const size_t bytes = (size_t)n * sizeof(emsesg_particle);
+  if (overlap(d_in, bytes, d_out, bytes) || overlap(d_kept, sizeof(int64_t), d_in, bytes) ||
+      overlap(d_kept, sizeof(int64_t), d_out, bytes))
+    return EMSESG_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
+  uint32_t* scratch = nullptr;
+  int rc = scratch_for_current_device(st, &scratch);
+  if (rc) return rc;
   uint32_t* local = scratch;
   uint32_t* tile_sum = scratch + NA_MAX;
   int ntiles = (int)((n + NA_TILE - 1) / NA_TILE);
-  if (ntiles > 0) k_na_tile<<<ntiles, NA_TILE_THREADS, 0, st>>>(d_in, n, local, tile_sum);
-  k_na_tiles<<<1, (int)NA_TILES, 0, st>>>(tile_sum, ntiles, d_kept);
-  if (n > 0) k_na_scatter<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_in, n, local, tile_sum, d_out);
-  return cudaGetLastError() == cudaSuccess ? EMSESG_OK : EMSESG_ERR_CUDA;
+  // Each launch reports its own status; an error left pending by earlier
+  // work of the caller is neither cleared nor reported here.
+  if (ntiles > 0) {
+    void* args[] = {(void*)&d_in, (void*)&n, (void*)&local, (void*)&tile_sum};
+    if (cudaLaunchKernel((const void*)k_na_tile, dim3(ntiles), dim3(NA_TILE_THREADS), args, 0, st) != cudaSuccess)
+      return EMSESG_ERR_CUDA;
+  }
+  {
+    void* args[] = {(void*)&tile_sum, (void*)&ntiles, (void*)&d_kept};
+    if (cudaLaunchKernel((const void*)k_na_tiles, dim3(1), dim3((unsigned)NA_TILES), args, 0, st) != cudaSuccess)
+      return EMSESG_ERR_CUDA;
+  }
+  if (n > 0) {
+    void* args[] = {(void*)&d_in, (void*)&n, (void*)&local, (void*)&tile_sum, (void*)&d_out};
+    if (cudaLaunchKernel((const void*)k_na_scatter, dim3((unsigned)((n + 255) / 256)), dim3(256), args, 0, st) !=
+        cudaSuccess)
+      return EMSESG_ERR_CUDA;
+  }
+  return EMSESG_OK;
 }

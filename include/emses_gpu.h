@@ -216,13 +216,15 @@ int emsesg_rhoupd(emsesg_ctx* ctx, int ps);
  * hosts that cannot call cudaMalloc (device memory owned by their own pool or
  * framework): copies the particles of d_in[0..n) with nid != -1, in buffer
  * order, into d_out and writes their number to *d_kept; all three are device
- * pointers owned by the caller, d_out distinct from d_in.  No context is
- * needed.  Scratch is a fixed file-scope device array, so
+ * pointers owned by the caller and must not overlap (EMSESG_ERR_ARG).  No
+ * context is needed.  Scratch is a fixed file-scope device array, so
  * n <= EMSESG_NOALLOC_MAX_PARTICLES (else EMSESG_ERR_ARG), every GPU that
  * loads the library holds it (about 4 MB) until exit, and calls whose kernels
- * overlap on a GPU race on it: order them on one stream.  The first call on a
- * device looks up the scratch address; make that call before any stream
- * capture.  Asynchronous on `stream` (a cudaStream_t, NULL = default). */
+ * overlap on a GPU race on it: order them on one stream.  Each call outside a
+ * stream capture looks up the scratch address of the current device; a call
+ * inside a capture reuses the last one, so make the first call on a device
+ * before any stream capture.  A CUDA error left pending by earlier work is
+ * not consumed.  Asynchronous on `stream` (a cudaStream_t, NULL = default). */
 #define EMSESG_NOALLOC_MAX_PARTICLES (1 << 20)
 int emsesg_compact_noalloc(const emsesg_particle* d_in, int64_t n, emsesg_particle* d_out, int64_t* d_kept,
                            void* stream);

@@ -1211,53 +1211,4 @@ void orc_load_plasma(const emsesg_config* c, const emsesg_plasma* pl,
   }
 }
 
-// Timed CPU baseline: psolve1 (zigzag) followed by charge(func 0) for the
-// whole buffer on `threads` host threads, each owning a contiguous slice of
-// every species segment with private wrk-TJ, aj and rho arrays that are
-// summed at the end (one MPI rank per core in the reference).  The
-// per-particle arithmetic is the restatement above.
-double orc_step_timed(const emsesg_config* c, int ustep, const double* wrk,
-                      emsesg_particle* pbuf, const int64_t* totalp, double* aj,
-                      double* rho, int threads) {
-  int64_t wsz = orc_field_size(c, EMSESG_FIELD_WRK), asz = orc_field_size(c, EMSESG_FIELD_AJ);
-  int64_t rsz = orc_field_size(c, EMSESG_FIELD_RHO);
-  if (threads < 1) threads = 1;
-  std::vector<std::vector<double>> A(threads), R(threads);
-  auto work = [&](int tid) {
-    std::vector<double> w(wrk, wrk + wsz);
-    std::vector<double>& a = A[tid];
-    std::vector<double>& r = R[tid];
-    a.assign(asz, 0.0);
-    r.assign(rsz, 0.0);
-    emsesg_counter gc;
-    std::memset(&gc, 0, sizeof(gc));
-    std::vector<int64_t> tp(c->nspec);
-    int64_t base = 0;
-    for (int is = 0; is < c->nspec; is++) {
-      int64_t n = totalp[is];
-      int64_t lo = n * tid / threads, hi = n * (tid + 1) / threads;
-      for (int js = 0; js < c->nspec; js++) tp[js] = 0;
-      tp[is] = hi - lo;
-      int64_t pos = 0;
-      orc_psolve1(c, ustep, 0, w.data(), pbuf + base + lo, tp.data(), nullptr, 0, &pos, 0,
-                  a.data(), nullptr, &gc, nullptr);
-      std::vector<double> rr(rsz, 0.0);
-      orc_charge(c, 0, pbuf + base + lo, tp.data(), rr.data(), nullptr, nullptr, nullptr);
-      for (int64_t x = 0; x < rsz; x++) r[x] += rr[x];
-      base += n;
-    }
-  };
-  auto t0 = std::chrono::steady_clock::now();
-  std::vector<std::thread> pool;
-  for (int t = 1; t < threads; t++) pool.emplace_back(work, t);
-  work(0);
-  for (auto& th : pool) th.join();
-  for (int t = 0; t < threads; t++) {
-    for (int64_t x = 0; x < asz; x++) aj[x] += A[t][x];
-    for (int64_t x = 0; x < rsz; x++) rho[x] += R[t][x];
-  }
-  auto t1 = std::chrono::steady_clock::now();
-  return std::chrono::duration<double>(t1 - t0).count();
-}
-
 }  // extern "C"

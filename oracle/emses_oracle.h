@@ -86,12 +86,21 @@ double orc_hash_u01(uint64_t seed, uint64_t stream, uint64_t index);
 void orc_load_plasma(const emsesg_config* c, const emsesg_plasma* pl,
                      emsesg_particle* pbuf, int64_t* totalp);
 
-/* Timed CPU baseline: one step psolve1 (zigzag J) + charge(func 0) on
- * `threads` OpenMP threads with private rho/aj per thread.  Returns the
- * wall time in seconds. */
-double orc_step_timed(const emsesg_config* c, int ustep, const double* wrk,
-                      emsesg_particle* pbuf, const int64_t* totalp, double* aj,
-                      double* rho, int threads);
+/* Timed CPU baseline in the reference's one-rank-per-core model
+ * (baseline.cpp): the particles are split into blocks of x rows (y rows x z
+ * layers), one per thread, each with its own sub-grid (margin cells on its
+ * split sides), wrk, aj and rho; a step runs orc_psolve1 + orc_charge on
+ * every block in parallel (from the blocks' initial particles when
+ * `restore`) and returns the wall time.  orc_blocks_result sums the blocks' aj / rho into the global
+ * periodic arrays (interior nodes). */
+typedef struct orc_blocks orc_blocks;
+orc_blocks* orc_blocks_create(const emsesg_config* c, const double* wrk, const emsesg_particle* p,
+                              const int64_t* totalp, int threads, int margin);
+int orc_blocks_threads(const orc_blocks* h);
+int64_t orc_blocks_particles(const orc_blocks* h);
+double orc_blocks_step(orc_blocks* h, int ustep, int restore);
+void orc_blocks_result(const orc_blocks* h, double* aj, double* rho);
+void orc_blocks_destroy(orc_blocks* h);
 
 /* Loss sum_steps sum_probe Jx^2 of K periodic steps and, when gE is not
  * NULL, its gradients with respect to the node fields (gE, gB: [n^3][3],

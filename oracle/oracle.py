@@ -11,6 +11,7 @@ this path (MT19937 of lib/mtarm, particle_sort_ of lib/psort) when built.
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from pathlib import Path
 
@@ -27,11 +28,18 @@ _P = ctypes.c_void_p
 _lib = None
 
 
+def reference_dir() -> Path:
+    """The reference's source tree: $EMSES_REFERENCE, else a `reference`
+    directory beside this repository."""
+    env = os.environ.get("EMSES_REFERENCE")
+    return Path(env) if env else HERE.parent.parent / "reference"
+
+
 def build(reference: str | None = None):
     """Builds liboracle.so (and _ref/ when the reference sources exist)."""
     args = ["make", "-C", str(HERE), "liboracle.so"]
     subprocess.run(args, check=True, capture_output=True)
-    ref = Path(reference or "/root/reference")
+    ref = Path(reference) if reference else reference_dir()
     if (ref / "lib" / "mtarm" / "mt19937arm.c").exists():
         subprocess.run(["make", "-C", str(HERE), "ref", f"REFERENCE={ref}"], check=True, capture_output=True)
 
@@ -73,7 +81,12 @@ def lib() -> ctypes.CDLL:
         "orc_load_plasma": (None, [cfgp, ctypes.POINTER(Plasma), _P, i64p]),
         "orc_adjoint": (ctypes.c_double, [cfgp, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, ctypes.c_int64, _P, _P,
                                           _P, _P, _P, _P]),
-        "orc_step_timed": (ctypes.c_double, [cfgp, ctypes.c_int, _P, _P, i64p, _P, _P, ctypes.c_int]),
+        "orc_blocks_create": (_P, [cfgp, _P, _P, i64p, ctypes.c_int, ctypes.c_int]),
+        "orc_blocks_threads": (ctypes.c_int, [_P]),
+        "orc_blocks_particles": (ctypes.c_int64, [_P]),
+        "orc_blocks_step": (ctypes.c_double, [_P, ctypes.c_int, ctypes.c_int]),
+        "orc_blocks_result": (None, [_P, _P, _P]),
+        "orc_blocks_destroy": (None, [_P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -217,12 +230,40 @@ def load_plasma(cfg: Config, pl: Plasma):
     return pbuf, np.array(tp[: cfg.nspec], dtype=np.int64)
 
 
-def step_timed(cfg: Config, ustep: int, wrk: np.ndarray, pbuf: np.ndarray, totalp, threads: int):
-    """One psolve1 + charge step on `threads` host threads; returns seconds."""
-    aj = zeros(cfg, "aj")
-    rho = zeros(cfg, "rho")
-    return lib().orc_step_timed(ctypes.byref(cfg), ustep, wrk.ctypes.data, pbuf.ctypes.data, _tp(totalp),
-                                aj.ctypes.data, rho.ctypes.data, threads), aj, rho
+class Blocks:
+    """The timed CPU baseline (baseline.cpp): the reference's one rank per
+    core, each owning a block of x rows of the grid with its own sub-grid
+    arrays, running psolve1 + charge on its particles.  `wrk` is the global
+    node field (grdcrt output)."""
+
+    def __init__(self, cfg: Config, wrk: np.ndarray, pbuf: np.ndarray, totalp, threads: int, margin: int = 3):
+        self.cfg = cfg
+        self.L = lib()
+        p = np.ascontiguousarray(pbuf, dtype=PARTICLE_DTYPE)
+        w = np.ascontiguousarray(wrk, dtype=np.float64)
+        self.h = self.L.orc_blocks_create(ctypes.byref(cfg), w.ctypes.data, p.ctypes.data, _tp(totalp), threads,
+                                          margin)
+        self.threads = int(self.L.orc_blocks_threads(self.h))
+        self.particles = int(self.L.orc_blocks_particles(self.h))
+
+    def step(self, ustep: int = 2, restore: bool = True) -> float:
+        """One step of every block (from the initial particles when
+        `restore`); returns the wall seconds of psolve1 + charge."""
+        return float(self.L.orc_blocks_step(self.h, ustep, int(restore)))
+
+    def result(self):
+        """aj and rho of the last step, folded periodically (interior nodes)."""
+        aj, rho = zeros(self.cfg, "aj"), zeros(self.cfg, "rho")
+        self.L.orc_blocks_result(self.h, aj.ctypes.data, rho.ctypes.data)
+        return aj, rho
+
+    def close(self):
+        if self.h:
+            self.L.orc_blocks_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 # -- the reference's own C code (oracle/_ref) --------------------------------

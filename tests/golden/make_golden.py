@@ -446,7 +446,9 @@ def run_case(units, name, c, ustep, opts):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("EMSES_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("EMSES_REFERENCE", str(HERE.parents[2] / "reference")),
+                    help="the reference source tree ($EMSES_REFERENCE, else a `reference` directory beside "
+                         "this repository)")
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
     units = load_units(Path(a.reference))

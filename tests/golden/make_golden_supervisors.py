@@ -207,7 +207,9 @@ def make(ref: Path) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("EMSES_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("EMSES_REFERENCE", str(HERE.parents[2] / "reference")),
+                    help="the reference source tree ($EMSES_REFERENCE, else a `reference` directory beside "
+                         "this repository)")
     args = ap.parse_args()
     out = make(Path(args.reference))
     np.savez_compressed(HERE / "supervisors.npz", **out)
