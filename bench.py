@@ -245,6 +245,100 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------- accuracy (checker)
+def accuracy_report(steps: int = 4) -> dict:
+    """Errors of the FP32 form against the FP64 oracle on the headline
+    workload's physics at 32^3 x 64 ppc (4,194,304 particles), the oracle
+    started every step from the FP32 form's own state, with the re-sort after
+    the 4th step: worst case over the steps of every quantity."""
+    from ctca_b200 import inputs
+    from ctca_b200.emses import FX_ROW_SLOTS, Emses
+    from oracle import compare as C
+    from oracle import oracle as O
+
+    case = inputs.workload_case(2, scale=0.25)
+    cfg = inputs.make_config(case)
+    eb = inputs.make_fields(case)
+    p, tp = inputs.make_particles(case)
+    worst = {"pos_max_abs": 0.0, "pos_rms": 0.0, "vel_max_rel": 0.0, "vel_l2_rel": 0.0, "rho_l2_rel": 0.0,
+             "rho_max_rel": 0.0, "j_l2_rel": 0.0, "j_max_rel": 0.0, "cell_mismatch": 0, "cell_mismatch_off_band": 0,
+             "near_face": 0, "alive_mismatch": 0, "sort_count_mismatch_cells": 0, "permutation_mismatch": 0,
+             "energy_rel": 0.0, "energy_fp64_reproducible": True, "continuity_residual": 0.0,
+             "continuity_residual_oracle": 0.0, "continuity_max_rho": 0.0}
+    with Emses(cfg) as g:
+        g.upload_particles(p, tp)
+        g.upload_field("eb", eb)
+        g.fx_load()
+        g.fx_store()
+        cur, tpc = g.download_particles()
+        g.fx_load()
+        last_sorted = cur
+        for step in range(steps):
+            o = O.Oracle(cfg, cur, tpc, eb)
+            o.charge(0)
+            o.reduce_rho("rho")
+            rho_o_old = o.f["rho"].copy()
+            o.grdcrt()
+            o.f["aj"][...] = 0.0
+            o.psolve1(2, 0)
+            o.reduce_aj()
+            o.charge(0)
+            o.reduce_rho("rho")
+            g.fx_step(2, False)
+            g.fx_store()
+            after, _ = g.download_particles()
+            rep = C.particle_errors(cfg, after, o.pbuf)
+            for k in ("pos_max_abs", "pos_rms", "vel_max_rel", "vel_l2_rel"):
+                worst[k] = max(worst[k], rep[k])
+            for k in ("cell_mismatch", "cell_mismatch_off_band", "near_face", "alive_mismatch"):
+                worst[k] += rep[k]
+            for name, key in (("rho", "rho"), ("aj", "j")):
+                fe = C.field_errors(g.download_field(name), o.f[name])
+                worst[key + "_l2_rel"] = max(worst[key + "_l2_rel"], fe["l2_rel"])
+                worst[key + "_max_rel"] = max(worst[key + "_max_rel"], fe["max_rel"])
+            eg = g.fx_energy()
+            worst["energy_rel"] = max(worst["energy_rel"], C.rel_l2(eg, o.energy()))
+            worst["energy_fp64_reproducible"] &= bool(np.array_equal(eg, g.fx_energy()))
+            res, rmax = g.fx_continuity()
+            if not math.isnan(res):
+                worst["continuity_residual"] = max(worst["continuity_residual"], res)
+                worst["continuity_max_rho"] = max(worst["continuity_max_rho"], rmax)
+                worst["continuity_residual_oracle"] = max(
+                    worst["continuity_residual_oracle"],
+                    C.continuity_residual(cfg, rho_o_old, o.f["rho"], o.f["aj"]))
+            if step % SORT_EVERY == SORT_EVERY - 1:
+                g.fx_sort()
+                g.fx_store()
+                srt, tps = g.download_particles()
+                worst["sort_count_mismatch_cells"] += int(np.sum(C.cell_histogram(cfg, srt)
+                                                                 != C.cell_histogram(cfg, o.pbuf)))
+                b0 = np.concatenate([[0], np.cumsum(tpc)])
+                b1 = np.concatenate([[0], np.cumsum(tps)])
+                for sp in range(cfg.nspec):
+                    before, moved = last_sorted[b0[sp]:b0[sp + 1]], after[b0[sp]:b0[sp + 1]]
+                    okeys = C.tile_key(cfg, case.sort_tile, o.pbuf[b0[sp]:b0[sp + 1]])[0]
+                    exp = C.sort_order(cfg, case.sort_tile, FX_ROW_SLOTS, before, moved, keys=okeys)
+                    got = srt[b1[sp]:b1[sp + 1]]
+                    if got.size != exp.size:
+                        worst["permutation_mismatch"] += abs(got.size - exp.size)
+                        continue
+                    same = np.all(np.stack([got[f] == moved[exp][f] for f in ("x", "y", "z", "vx", "vy", "vz")]), 0)
+                    worst["permutation_mismatch"] += int((~same).sum())
+                cur, tpc, last_sorted = srt, tps, srt
+            else:
+                cur = after
+    worst["workload"] = (f"the headline physics (mass ratio 1836, ion drift, 8 E and 8 dB modes) on 32^3 x 64 ppc "
+                         f"({int(tp.sum()):,} particles), {steps} steps with the re-sort after step {SORT_EVERY}; the "
+                         "FP64 oracle started every step from the FP32 form's state; worst step (max) or total over "
+                         "the steps (counts)")
+    worst["definitions"] = ("pos in cells, vel relative to the largest |v|, rho/J relative L2 and max; cell "
+                            "mismatches counted, those farther than 4 FP32 ulps from every face must be 0; "
+                            "permutation against the tile sort's definition with the oracle's cells; energy = FP64 "
+                            "kinetic energy of the FP32 state vs the oracle's; continuity = max |rho_new - rho_old + "
+                            "2 div J| in FP64 (the 3-D zigzag's cubic remainder)")
+    return worst
+
+
 # --------------------------------------------------------------- GPU arm
 def time_adjoint(K: int = 256, ckpt: int = 16, sort_every: int = SORT_EVERY) -> dict:
     """Forward K steps vs the reverse mode through them (emsesg_fx_adjoint)
@@ -432,6 +526,7 @@ def run_ours(args, world, rank, local):
         out["ensemble"] = ensemble_sample(args.ensemble_runs, args.ensemble_steps)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
+        out["accuracy"] = accuracy_report()
     g.close()
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -125,6 +125,9 @@ struct FxState {
   emsesg_config g_cfg{};
   AdjWork* adj = nullptr;
   int64_t* accum = nullptr;         // int64 (rho, jx, jy, jz) on the rho layout
+  double* diag = nullptr;           // FP64 checks: energy partials, sums, continuity maxima
+  bool rho_prev = false;            // the rho field holds the deposit of the step before
+  bool cont_valid = false;          // ... so the last step's continuity residual is meaningful
   float4* fnode = nullptr;          // node field {ex, ey, ez, bx} over (n+1)^3 nodes
   float4* fnode2 = nullptr;         // {by, bz, 0, 0}
   int bits[3] = {0, 0, 0};          // packed cell bit widths

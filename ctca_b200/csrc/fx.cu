@@ -323,6 +323,7 @@ __global__ void k_fx_gather_tm(const float4* __restrict__ pos, const float* __re
 
 #include "fx_sort.cuh"
 #include "fx_adjoint.cuh"
+#include "fx_diag.cuh"
 
 inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
 
@@ -448,6 +449,9 @@ int fx_alloc(emsesg_ctx* ctx) {
   EMSESG_CUDA(ctx, cudaMalloc(&f.chunk_start, (int64_t)c.nspec * (f.ntiles + 1) * sizeof(int64_t)));
   FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
   EMSESG_CUDA(ctx, cudaMalloc(&f.accum, (fr.size() + fj.size()) * sizeof(int64_t)));
+  // FP64 checks: energy partials and sums, the continuity maxima
+  EMSESG_CUDA(ctx, cudaMalloc(&f.diag, (3 * DIAG_GRID + 3 + 2) * sizeof(double)));
+  EMSESG_CUDA(ctx, cudaMemsetAsync(f.diag, 0, (3 * DIAG_GRID + 3 + 2) * sizeof(double), ctx->stream));
   int64_t nn = (int64_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
   EMSESG_CUDA(ctx, cudaMalloc(&f.fnode, nn * sizeof(float4)));
   EMSESG_CUDA(ctx, cudaMalloc(&f.fnode2, nn * sizeof(float4)));
@@ -491,6 +495,7 @@ void fx_free(emsesg_ctx* ctx) {
   cudaFree(f.count_d); cudaFree(f.slots_d); cudaFree(f.tile_start); cudaFree(f.tile_pad); cudaFree(f.accum);
   cudaFree(f.chunk_start);
   cudaFree(f.fnode); cudaFree(f.fnode2);
+  cudaFree(f.diag);
   cudaFree(f.tile_start2); cudaFree(f.tile_pad2); cudaFree(f.lcs_cnt); cudaFree(f.lcs_base); cudaFree(f.lcs_wcnt);
   cudaFree(f.lcs_celltot); cudaFree(f.lcs_tiletot); cudaFree(f.lcs_stray); cudaFree(f.lcs_inv);
   cudaFree(f.surf); cudaFree(f.tailord); cudaFree(f.stage); cudaFree(f.stage_ord);
@@ -709,6 +714,7 @@ extern "C" int emsesg_fx_load(emsesg_ctx* ctx) {
                                    ctx->stream));
   f.loaded = true;
   f.tiled = false;  // buffer order: the first sort is the radix path
+  f.rho_prev = false;
   rc = emsesg_fx_sort(ctx);
   if (rc) return rc;
   return emsesg_synchronize(ctx);
@@ -795,6 +801,7 @@ extern "C" int emsesg_fx_load_plasma(emsesg_ctx* ctx, const emsesg_plasma* pl) {
                                    ctx->stream));
   f.loaded = true;
   f.tiled = false;
+  f.rho_prev = false;
   rc = emsesg_fx_sort(ctx);
   if (rc) return rc;
   return emsesg_synchronize(ctx);
@@ -941,10 +948,16 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   if ((rc = run_slab_ops2(ctx, (long long*)acc_rho, fr, fold_ops(c, 0, 1), (long long*)acc_j, fj,
                           fold_ops(c, 1, 3), "fx_fold")))
     return rc;
-  EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_double, nblk(fr.size()), 256, 0, (const long long*)acc_rho,
-                ctx->field[EMSESG_FIELD_RHO], fr.size());
+  // J first: the conversion of rho takes the continuity residual of the step
+  // against the rho field of the step before (still in place) and this J
   EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_double, nblk(fj.size()), 256, 0, (const long long*)acc_j,
                 ctx->field[EMSESG_FIELD_AJ], fj.size());
+  unsigned long long* cres = (unsigned long long*)(f.diag + 3 * DIAG_GRID + 3);
+  EMSESG_CUDA(ctx, cudaMemsetAsync(cres, 0, 2 * sizeof(double), ctx->stream));
+  EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_rho, nblk(fr.size()), 256, 0, (const long long*)acc_rho,
+                ctx->field[EMSESG_FIELD_RHO], ctx->field[EMSESG_FIELD_AJ], fr, fj, c.nx, c.ny, c.nz, cres);
+  f.cont_valid = f.rho_prev;
+  f.rho_prev = true;
   ctx->rng_stream++;
   // the re-sort after the push (so that injected particles take their
   // first, partial step before they join the tile regions)
@@ -1237,6 +1250,62 @@ extern "C" int emsesg_fx_surface(emsesg_ctx* ctx, int64_t* counts, int64_t* nsur
                                      cudaMemcpyDeviceToHost, ctx->stream));
     EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_fx_energy(emsesg_ctx* ctx, double* engk) {
+  if (!ctx || !engk) return EMSESG_ERR_ARG;
+  if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded");
+  FxState& f = ctx->fx;
+  const emsesg_config& c = ctx->cfg;
+  double* part = f.diag;
+  double* sum = f.diag + 3 * DIAG_GRID;
+  const double vol = (double)c.nx * (double)c.ny * (double)c.nz;
+  for (int is = 0; is < c.nspec; is++) {
+    const int64_t off = f.base[is];
+    const int64_t* tile_end = f.tile_pad + (int64_t)is * (f.ntiles + 1) + f.ntiles;
+    EMSESG_LAUNCH(ctx, "fx_energy", k_fx_energy_part, DIAG_GRID, DIAG_BLOCK, 0, f.pos + off, f.vx + off, f.vy + off,
+                  f.vz + off, tile_end, f.tail0[is], f.ntail[is], part);
+    EMSESG_LAUNCH(ctx, "fx_energy", k_fx_energy_sum, 1, 32, 0, part, DIAG_GRID, sum);
+    double t[3];
+    EMSESG_CUDA(ctx, cudaMemcpyAsync(t, sum, sizeof(t), cudaMemcpyDeviceToHost, ctx->stream));
+    EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    // engk(d,is) = 0.5*rm(is)*t(d)/(slx*sly*slz), energy.F90:44-46
+    for (int d = 0; d < 3; d++) engk[3 * is + d] = 0.5 * c.rm[is] * t[d] / vol;
+  }
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_fx_continuity(emsesg_ctx* ctx, double* res) {
+  if (!ctx || !res) return EMSESG_ERR_ARG;
+  if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded");
+  FxState& f = ctx->fx;
+  double r[2];
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(r, f.diag + 3 * DIAG_GRID + 3, sizeof(r), cudaMemcpyDeviceToHost, ctx->stream));
+  EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  res[0] = f.cont_valid ? r[0] : std::nan("");
+  res[1] = f.rho_prev ? r[1] : std::nan("");
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_fx_background(emsesg_ctx* ctx, int replace) {
+  if (!ctx) return EMSESG_ERR_ARG;
+  if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded");
+  const emsesg_config& c = ctx->cfg;
+  FxState& f = ctx->fx;
+  const FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO);
+  double* rhobk = ctx->field[EMSESG_FIELD_RHOBK];
+  EMSESG_CUDA(ctx, cudaMemsetAsync(rhobk, 0, fr.size() * sizeof(double), ctx->stream));
+  const Bodies bd = make_bodies(c);
+  for (int is = 0; is < c.nspec; is++)
+    for (int q = 0; q < bd.n; q++) {
+      const int64_t nodes =
+          (int64_t)(bd.hi[q][0] - bd.lo[q][0] + 1) * (bd.hi[q][1] - bd.lo[q][1] + 1) * (bd.hi[q][2] - bd.lo[q][2] + 1);
+      EMSESG_LAUNCH(ctx, "fx_background", k_fx_background, nblk(nodes), 256, 0, f.surf + (int64_t)is * f.nsurf, bd,
+                    q, c.q[is], rhobk, fr);
+    }
+  EMSESG_LAUNCH(ctx, "fx_background", k_add_background, nblk(fr.size()), 256, 0, ctx->field[EMSESG_FIELD_RHO],
+                rhobk, fr, c.nx, c.ny, c.nz, replace ? 1 : 0);
   return EMSESG_OK;
 }
 

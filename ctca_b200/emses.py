@@ -141,6 +141,9 @@ _SIGS = {
     "emsesg_fx_download_accum": (_I, [_P, _P]),
     "emsesg_fx_inject": (_I, [_P, _I, _P, ctypes.c_int64]),
     "emsesg_fx_surface": (_I, [_P, _P, ctypes.POINTER(ctypes.c_int64)]),
+    "emsesg_fx_background": (_I, [_P, _I]),
+    "emsesg_fx_energy": (_I, [_P, ctypes.POINTER(ctypes.c_double)]),
+    "emsesg_fx_continuity": (_I, [_P, ctypes.POINTER(ctypes.c_double)]),
     "emsesg_fx_emit": (_I, [_P, _I, _I, ctypes.c_double, _P, _P, ctypes.c_int64, _P, _P, _I, ctypes.c_uint64,
                             ctypes.c_uint64, ctypes.c_uint64]),
     "emsesg_fx_inflow_z": (_I, [_P, _I, _I, ctypes.c_int64, _P, _P, _P, _I, ctypes.c_double, ctypes.c_uint64,
@@ -458,6 +461,23 @@ class Emses:
         if n.value:
             self._check(self.lib.emsesg_fx_surface(self.h, out.ctypes.data, ctypes.byref(n)))
         return out
+
+    def fx_background(self, replace: bool = False):
+        """add_background_charge of the FP32 form: rhobk from the surface
+        counts, added into rho (or replacing it)."""
+        self._check(self.lib.emsesg_fx_background(self.h, 1 if replace else 0))
+
+    def fx_energy(self) -> np.ndarray:
+        """Kinetic energy of the FP32 state in FP64, [nspec, 3] (energy)."""
+        e = (ctypes.c_double * (3 * ISPEC))()
+        self._check(self.lib.emsesg_fx_energy(self.h, e))
+        return np.array(e[: 3 * self.cfg.nspec]).reshape(self.cfg.nspec, 3)
+
+    def fx_continuity(self) -> tuple[float, float]:
+        """(max |rho_new - rho_old + 2 div J|, max |rho_new|) of the last step."""
+        r = (ctypes.c_double * 2)()
+        self._check(self.lib.emsesg_fx_continuity(self.h, r))
+        return float(r[0]), float(r[1])
 
     def fx_adjoint(self, K: int, ustep: int, ckpt: int, sort_every: int, probe_lo, probe_hi, nparticles: int):
         """Loss sum_steps sum_probe aj_x^2 over K steps and its gradients:

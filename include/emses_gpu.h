@@ -366,6 +366,27 @@ int emsesg_fx_emit_plane(emsesg_ctx* ctx, int spec, int nemd, double grd, const 
  * crossed last, in the cell holding its end point.  counts may be NULL to
  * query nsurf. */
 int emsesg_fx_surface(emsesg_ctx* ctx, int64_t* counts, int64_t* nsurf);
+/* Background charge from the surface counts (replaces add_background_charge,
+ * src/pcl2field/charge.F90:414-449, with rhobk(...,3) += rhobk(...,1) of
+ * src/main/emses.F90:249-251): the field EMSESG_FIELD_RHOBK becomes the
+ * cumulative absorbed minus emitted charge of the box bodies as node values
+ * -- a surface cell's charge q(is) * count goes in equal quarters to the four
+ * nodes of its face cell, the counts meeting at a node summed in int64 per
+ * species, then scaled once in FP64 -- and rho(0:nx,0:ny,0:nz) += rhobk, or
+ * = rhobk with replace != 0 (the reference's nflag_testp == 1).  Call it
+ * after a step, as the reference calls add_background_charge after charge. */
+int emsesg_fx_background(emsesg_ctx* ctx, int replace);
+/* Kinetic energy of the FP32 state in FP64 (replaces energy,
+ * src/etc/energy.F90:29-47): engk[is*3 + d] = 0.5*rm(is)*sum(v_d^2)/(nx*ny*nz)
+ * over the live particles, the sums in a fixed order (reproducible bit for
+ * bit).  Works with EMSESG_FLAG_FP32_ONLY. */
+int emsesg_fx_energy(emsesg_ctx* ctx, double* engk);
+/* Charge continuity of the last FP32 step in FP64 (the check of rhoupd,
+ * src/field/rhoupd.F90:41-49): res[0] = max over the nodes 0..n of
+ * |rho_new - rho_old + 2 (div J)|, rho_old the rho field the step before
+ * left; res[1] = max |rho_new|.  res[0] is NaN when no step deposited rho
+ * before the last one (after a load).  Works with EMSESG_FLAG_FP32_ONLY. */
+int emsesg_fx_continuity(emsesg_ctx* ctx, double* res);
 /* Reverse mode through K steps of the FP32 form on a periodic grid (no
  * bodies, no injection): runs the K forward steps (re-sort every sort_every
  * steps), then the adjoint sweep with the particle state checkpointed every

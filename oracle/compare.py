@@ -1,0 +1,148 @@
+"""TEST INFRASTRUCTURE ONLY: per-quantity errors of the FP32 / fixed-point
+form against the FP64 oracle.
+
+Used by tests/ and by bench.py's accuracy report, always as the checker.
+The FP32 form and the oracle start a step from the same state (the FP32
+form's own particles as FP64 records, emsesg_fx_store), so a difference in
+a particle's cell after the step can only come from FP32 rounding of a
+position that ends next to a cell face.  Such particles are counted, and a
+cell difference of any particle farther than `band` from every face counts
+as a failure of exactness.
+
+The sort permutation is the definition of the FP32 tile sort: live particles
+ordered by the tile-major cell key, equal cells in the order (source tile,
+warp, row, lane) of the thread-major layout of the previous sort (the sorted
+rank q of a tile of n particles sits in row q % L, column q / L,
+L = ceil(n / row slots); a warp is 32 consecutive columns).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+FP32_ULP = 2.0 ** -23   # one FP32 ulp of an in-cell offset in [0.5, 1)
+BAND = 4 * FP32_ULP     # "next to a face": within four ulps
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def max_rel(a, b) -> float:
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    mb = np.max(np.abs(b)) if b.size else 0.0
+    return float(np.max(np.abs(a - b)) / (mb if mb > 0 else 1.0)) if b.size else 0.0
+
+
+def _cells(cfg, p):
+    return np.stack([np.floor(p[f]).astype(np.int64) for f in "xyz"], 1)
+
+
+def particle_errors(cfg, pg, po, band: float = BAND) -> dict:
+    """Errors of the FP32 form's records pg against the oracle's po (same
+    particles, same order, after the same step from the same state)."""
+    ext = np.array([cfg.nx, cfg.ny, cfg.nz], dtype=np.float64)
+    alive_g, alive_o = pg["nid"] != -1, po["nid"] != -1
+    m = alive_g & alive_o
+    a, b = pg[m], po[m]
+    out = {"particles": int(po.size), "alive": int(alive_o.sum()),
+           "alive_mismatch": int((alive_g != alive_o).sum())}
+    dpos = np.stack([a[f] - b[f] for f in "xyz"], 1)
+    dpos = dpos - ext * np.round(dpos / ext)  # a periodic wrap is no error
+    out["pos_max_abs"] = float(np.max(np.abs(dpos))) if dpos.size else 0.0
+    out["pos_rms"] = float(np.sqrt(np.mean(np.sum(dpos ** 2, 1)))) if dpos.size else 0.0
+    vg = np.stack([a[f] for f in ("vx", "vy", "vz")], 1)
+    vo = np.stack([b[f] for f in ("vx", "vy", "vz")], 1)
+    out["vel_max_rel"] = max_rel(vg, vo)
+    out["vel_l2_rel"] = rel_l2(vg, vo)
+    cg = _cells(cfg, a) % ext.astype(np.int64)
+    co = _cells(cfg, b) % ext.astype(np.int64)
+    mis = np.any(cg != co, 1)
+    frac = np.stack([b[f] - np.floor(b[f]) for f in "xyz"], 1)
+    near = np.any((frac < band) | (frac > 1.0 - band), 1)
+    out["cell_mismatch"] = int(mis.sum())
+    out["cell_mismatch_off_band"] = int((mis & ~near).sum())
+    out["near_face"] = int(near.sum())
+    out["band"] = band
+    return out
+
+
+def field_errors(g, o) -> dict:
+    return {"l2_rel": rel_l2(g, o), "max_rel": max_rel(g, o)}
+
+
+def tile_key(cfg, tile, p):
+    """Tile-major cell key and tile index of records p (tile: cells a side)."""
+    i, j, k = (np.floor(p[f]).astype(np.int64) % n for f, n in zip("xyz", (cfg.nx, cfg.ny, cfg.nz)))
+    nt = [-(-n // t) for n, t in zip((cfg.nx, cfg.ny, cfg.nz), tile)]
+    tid = i // tile[0] + nt[0] * (j // tile[1] + nt[1] * (k // tile[2]))
+    lin = i % tile[0] + tile[0] * (j % tile[1] + tile[1] * (k % tile[2]))
+    return tid * (tile[0] * tile[1] * tile[2]) + lin, tid
+
+
+def sort_order(cfg, tile, row_slots, before, after, keys=None):
+    """The permutation of one species' tile sort: `before` are its records
+    in the order of the previous sort (cells of that sort), `after` the same
+    particles moved by the steps since; returns the indices of the live
+    particles of `after` in sorted order.  `keys` overrides the cell keys of
+    `after` (e.g. the oracle's)."""
+    _, t0 = tile_key(cfg, tile, before)
+    ntile = int(t0.max()) + 1 if t0.size else 0
+    counts = np.bincount(t0, minlength=ntile)
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    q = np.arange(before.size) - starts[t0]
+    L = -(-counts[t0] // row_slots)
+    col, row = q // L, q % L
+    src = np.lexsort((col % 32, row, col // 32, t0))  # (tile, warp, row, lane)
+    order_pos = np.empty(before.size, dtype=np.int64)
+    order_pos[src] = np.arange(before.size)
+    live = after["nid"] != -1
+    key1 = tile_key(cfg, tile, after)[0] if keys is None else keys
+    idx = np.flatnonzero(live)
+    return idx[np.lexsort((order_pos[idx], key1[idx]))]
+
+
+def cell_histogram(cfg, p) -> np.ndarray:
+    c = _cells(cfg, p[p["nid"] != -1]) % np.array([cfg.nx, cfg.ny, cfg.nz])
+    lin = c[:, 0] + cfg.nx * (c[:, 1] + cfg.ny * c[:, 2])
+    return np.bincount(lin, minlength=cfg.nx * cfg.ny * cfg.nz)
+
+
+def continuity_residual(cfg, rho_old, rho_new, aj) -> float:
+    """max over the nodes 0..n of |rho_new - rho_old + 2 div J| (rhoupd.F90:
+    41-49), FP64; rho arrays of the rho layout (guard 1), aj of the aj layout
+    (guard 4), numpy shape (z, y, x[, c])."""
+    nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
+    r0 = rho_old.reshape(nz + 3, ny + 3, nx + 3)[1:nz + 2, 1:ny + 2, 1:nx + 2]
+    r1 = rho_new.reshape(nz + 3, ny + 3, nx + 3)[1:nz + 2, 1:ny + 2, 1:nx + 2]
+    j = aj.reshape(nz + 9, ny + 9, nx + 9, 3)
+    jx = j[4:nz + 5, 4:ny + 5, 4:nx + 5, 0] - j[4:nz + 5, 4:ny + 5, 3:nx + 4, 0]
+    jy = j[4:nz + 5, 4:ny + 5, 4:nx + 5, 1] - j[4:nz + 5, 3:ny + 4, 4:nx + 5, 1]
+    jz = j[4:nz + 5, 4:ny + 5, 4:nx + 5, 2] - j[3:nz + 4, 4:ny + 5, 4:nx + 5, 2]
+    return float(np.max(np.abs(r1 - (r0 - ((jx + jy) + jz) * 2.0))))
+
+
+def near_faces(cfg, start, end, bodies=(), band: float = BAND, tie: float = 1e-5) -> np.ndarray:
+    """Particles whose FP64 move start -> end comes within `band` of a
+    decision that FP32 rounding can flip: an end point within `band` of an
+    integer plane on any axis (cell faces, the faces of box bodies with
+    integer bounds, the outer faces), or, for an end point inside a box (the
+    absorption test, inclusive bounds), two face entry times within `tie` of
+    each other (the face crossed last picks the surface cell).  bodies:
+    (lo[3], hi[3]) integer boxes."""
+    e = np.stack([end[f] for f in "xyz"], 1)
+    s = np.stack([start[f] for f in "xyz"], 1)
+    frac = e - np.floor(e)
+    near = np.any((frac < band) | (frac > 1.0 - band), 1)
+    for lo, hi in bodies:
+        lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+        inside = np.all((e >= lo) & (e <= hi), 1)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t = np.where(s < lo, (lo - s) / (e - s), np.where(s > hi, (hi - s) / (e - s), -1.0))
+        ts = np.sort(t, 1)
+        close = (ts[:, 1] >= 0) & (ts[:, 2] - ts[:, 1] < tie)
+        near |= inside & close
+    return near

@@ -214,6 +214,56 @@ extern "C" int64_t orc_surface_cell(const emsesg_config* c, int ipc, const doubl
   return off[ipc * 6 + 2 * best + side] + face_index(lo, hi, best, ap);
 }
 
+// Background charge of the box bodies from the per-surface-cell counts
+// surf[nspec][nsurf] (absorbed minus emitted particles): the node field
+// rhobk(...,3) with a surface cell's charge q(is) * count in equal quarters
+// on the four nodes of its face cell (the counts meeting at a node summed as
+// integers per species, then scaled), species by species and body by body;
+// then add_background_charge, charge.F90:440-448: rho(0:n) += rhobk, or
+// rho(0:n) = rhobk with `replace` (nflag_testp == 1).  rhobk and rho have the
+// rho layout.  The counts-to-nodes rule is the project's: the reference
+// deposits absorbed charge into rhobk only along the finbound route.
+extern "C" void orc_background(const emsesg_config* c, const int64_t* surf, double* rhobk, double* rho,
+                               int replace) {
+  const FD fr = fd_of(c, EMSESG_FIELD_RHO);
+  for (int64_t x = 0; x < fr.size(); x++) rhobk[x] = 0.0;
+  int64_t off[6 * EMSESG_INPC];
+  const int64_t nsurf = orc_surface_layout(c, off);
+  for (int is = 0; is < c->nspec; is++)
+    for (int ipc = 0; ipc < c->npc; ipc++) {
+      const emsesg_body& b = c->body[ipc];
+      if (!box_surface(b)) continue;
+      int lo[3], hi[3];
+      body_bounds(b, lo, hi);
+      for (int k = lo[2]; k <= hi[2]; k++)
+        for (int j = lo[1]; j <= hi[1]; j++)
+          for (int i = lo[0]; i <= hi[0]; i++) {
+            const int nd[3] = {i, j, k};
+            int64_t sum = 0;
+            for (int f = 0; f < 6; f++) {
+              const int d = f / 2, e1 = TAN1[d], e2 = TAN2[d];
+              if (nd[d] != ((f & 1) ? hi[d] : lo[d])) continue;
+              const int ext1 = hi[e1] - lo[e1], ext2 = hi[e2] - lo[e2];
+              const int a = nd[e1] - lo[e1], bb = nd[e2] - lo[e2];
+              for (int v = bb - 1; v <= bb; v++)
+                for (int u = a - 1; u <= a; u++)
+                  if (u >= 0 && v >= 0 && u < ext1 && v < ext2)
+                    sum += surf[is * nsurf + off[ipc * 6 + f] + u + (int64_t)ext1 * v];
+            }
+            if (sum != 0) {
+              const int64_t x = fr.at(0, i, j, k);
+              rhobk[x] = rhobk[x] + c->q[is] * 0.25 * (double)sum;
+            }
+          }
+    }
+  for (int k = 0; k <= c->nz; k++)
+    for (int j = 0; j <= c->ny; j++)
+      for (int i = 0; i <= c->nx; i++) {
+        const int64_t x = fr.at(0, i, j, k);
+        rho[x] = replace ? rhobk[x] : rho[x] + rhobk[x];
+      }
+}
+
 // Face cell of a point lying on a box face (an emitted particle's
 // anti-particle), or -1.
 extern "C" int64_t orc_surface_point(const emsesg_config* c, int ipc, const double* p) {

@@ -60,6 +60,10 @@ int orc_psolve1(const emsesg_config* c, int ustep, int func, double* wrk,
 int64_t orc_surface_layout(const emsesg_config* c, int64_t* offsets);
 int64_t orc_surface_cell(const emsesg_config* c, int ipc, const double* b, const double* a);
 int64_t orc_surface_point(const emsesg_config* c, int ipc, const double* p);
+/* Background charge from the surface counts surf[nspec][nsurf]: rhobk
+ * (node field, rho layout) and rho(0:n) += rhobk, or = rhobk with
+ * `replace` (add_background_charge, charge.F90:414-449). */
+void orc_background(const emsesg_config* c, const int64_t* surf, double* rhobk, double* rho, int replace);
 void orc_charge(const emsesg_config* c, int func, emsesg_particle* pbuf,
                 const int64_t* totalp, double* rho, double* rhodg, double* rhobk,
                 double* rhobksp);

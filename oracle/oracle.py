@@ -68,6 +68,7 @@ def lib() -> ctypes.CDLL:
         "orc_surface_layout": (ctypes.c_int64, [cfgp, _P]),
         "orc_surface_cell": (ctypes.c_int64, [cfgp, ctypes.c_int, _P, _P]),
         "orc_surface_point": (ctypes.c_int64, [cfgp, ctypes.c_int, _P]),
+        "orc_background": (None, [cfgp, _P, _P, _P, ctypes.c_int]),
         "orc_charge": (None, [cfgp, ctypes.c_int, _P, i64p, _P, _P, _P, _P]),
         "orc_reduce_rho": (None, [cfgp, _P, ctypes.c_int]),
         "orc_reduce_aj": (None, [cfgp, _P]),
@@ -192,6 +193,13 @@ class Oracle:
 
     def rhoupd(self):
         self.L.orc_rhoupd(self._c(), self.f["rho"].ctypes.data, self.f["aj"].ctypes.data)
+
+    def background(self, surf=None, replace: bool = False):
+        """rhobk from the surface counts (the oracle's own, or `surf`), added
+        into rho (add_background_charge)."""
+        s = np.ascontiguousarray(self.surf if surf is None else surf, dtype=np.int64)
+        self.L.orc_background(self._c(), s.ctypes.data, self.f["rhobk"].ctypes.data, self.f["rho"].ctypes.data,
+                              int(replace))
 
     def energy(self) -> np.ndarray:
         e = np.zeros(3 * ISPEC)

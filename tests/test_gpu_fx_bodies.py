@@ -1,27 +1,35 @@
 """The FP32 / fixed-point form with a conducting box body, an open z axis
 with inflow through the back face, and photoelectron emission from the box's
-+x face: a small copy of the body + inflow + emission workload, against the
-FP64 oracle run on the same FP32-rounded start state and the same injected
-particles (ctca_b200/inject.py) and random numbers.
++x face (a small copy of the body + inflow + emission workload), step by
+step against the FP64 oracle started every step from the FP32 form's own
+state with the same injected particles and random numbers
+(ctca_b200/inject.py).
 
-Checked every step: rho and J within 1e-5 relative L2.  At the end: the
-absorbed counts per body (influx), the escape counts (nesc) and the
-per-surface-cell counts (absorbed minus emitted) agree, up to one particle
-that FP32 rounding may put on the other side of a face."""
+Every step: rho and J within 1e-5 relative L2, and the step's absorbed
+counts per body (influx), escapes (nesc) and per-surface-cell counts
+(absorbed minus emitted) equal to the oracle's.  A count may differ only by
+particles this test lists as next to a decision FP32 rounding can flip: an
+FP64 end point within four FP32 ulps of an integer plane (a cell, body or
+outer face), or two body-face entry times within 1e-5 (the face crossed
+last).  With none listed in a step, the counts must be equal.  At the end the
+background charge from the surface counts (emsesg_fx_background) equals the
+oracle's conversion of the same counts bit for bit."""
 import ctypes
 
 import numpy as np
 import pytest
 
 from ctca_b200 import inject, inputs
-from ctca_b200.emses import PARTICLE_DTYPE, Counter, Emses
+from ctca_b200.emses import PARTICLE_DTYPE, Emses
+from oracle import compare as C
 from oracle import oracle as O
 
-from helpers import build, case, rel_l2
+from helpers import build, case
 
 pytestmark = pytest.mark.gpu
 
 BOX = dict(geotype=0, ncond=1, xlpc=8.0, xupc=16.0, ylpc=8.0, yupc=16.0, zlpc=14.0, zupc=18.0, sqdscaled=1.0)
+BOUNDS = ((8, 8, 14), (16, 16, 18))
 
 
 def inside(p):
@@ -29,14 +37,20 @@ def inside(p):
             & (p["z"] >= BOX["zlpc"]) & (p["z"] <= BOX["zupc"]))
 
 
-def oracle_inject(o, spec, rec):
-    base = np.concatenate([[0], np.cumsum(o.totalp)])
-    end = int(base[spec])
-    o.pbuf = np.concatenate([o.pbuf[:end], rec, o.pbuf[end:]]).astype(PARTICLE_DTYPE)
-    o.totalp[spec - 1] += rec.size
+def with_injected(p, tp, batches):
+    """The records p (species segments tp) with each species' injected
+    records appended to its segment."""
+    base = np.concatenate([[0], np.cumsum(tp)])
+    parts, counts = [], []
+    for s in range(len(tp)):
+        seg = p[base[s]:base[s + 1]]
+        rec = batches.get(s + 1)
+        parts += [seg] + ([rec] if rec is not None else [])
+        counts.append(seg.size + (rec.size if rec is not None else 0))
+    return np.concatenate(parts).astype(PARTICLE_DTYPE), np.array(counts, dtype=np.int64)
 
 
-def test_fx_box_inflow_emission_vs_oracle(gpu):
+def test_fx_box_inflow_emission_per_step(gpu):
     c = case(n=(24, 24, 32), ppc=(4, 4), npbnd=(0, 0, 2), nfbnd=(0, 0, 1), vth_scale=3.0, tile=(8, 8, 8))
     for s in c.species:
         s.drift = (0.0, 0.0, -0.08)
@@ -58,13 +72,12 @@ def test_fx_box_inflow_emission_vs_oracle(gpu):
     g.upload_field("eb", eb)
     g.fx_load()
     g.fx_store()
-    p32, tp32 = g.download_particles()
+    cur, tp_cur = g.download_particles()
     g.fx_load()
-    o = O.Oracle(cfg, p32, tp32, eb)
     rng = np.random.default_rng(77)
     uni = rng.random(200000)
     g.set_randoms(uni)
-    o.set_randoms(uni)
+    drawn = 0
 
     renv = inputs.units()["renv"]
     vth = [s.vth * renv for s in c.species]
@@ -72,43 +85,83 @@ def test_fx_box_inflow_emission_vs_oracle(gpu):
     vt = inject.maxwell_table(0.01 * renv, 0.0, 1024)
     inflow_tabs = [(inject.flux_table(vth[s], -0.08 * renv, 1024, sign=-1.0), inject.maxwell_table(vth[s], 0.0, 1024))
                    for s in range(2)]
-    emitted = np.zeros_like(o.surf)
     L = O.lib()
-    for step in range(3):
+    surf_prev = g.fx_surface()
+    gc_prev = g.get_counters().as_dict()
+    totals = {"influx": 0, "nesc": 0, "emitted": 0, "listed": 0}
+    for step in range(4):
         batches = {1: [], 2: []}
         batches[1].append(inject.emit_rectangle(1, 16.0, (8.0, 16.0), (14.0, 18.0), 40, vn, vt, rng, spec=1))
         for s in (1, 2):
             vz, vxy = inflow_tabs[s - 1]
             batches[s].append(inject.inflow_z(False, 60, cfg.nx, cfg.ny, cfg.nz, vz, vxy, vxy, 1.0, rng, spec=s))
-        for s in (1, 2):
-            rec = np.concatenate(batches[s])
+        batches = {s: np.concatenate(b) for s, b in batches.items()}
+        emitted = np.zeros_like(surf_prev)
+        listed_anti = 0
+        for s, rec in batches.items():
             g.fx_inject(s, rec)
-            oracle_inject(o, s, rec)
             for r in rec[rec["preside"] == -2]:
                 pt = (ctypes.c_double * 3)(r["x"], r["y"], r["z"])
                 sc = L.orc_surface_point(ctypes.byref(cfg), 0, pt)
                 assert sc >= 0
                 emitted[s - 1, sc] += 1
-        g.fx_step(2, step == 1)
+                # an anti-particle next to a face-cell edge may count in the next cell
+                fr = np.array([r["y"], r["z"]]) - np.floor([r["y"], r["z"]])
+                listed_anti += int(np.any((fr < C.BAND) | (fr > 1 - C.BAND)))
+        # the oracle starts from the FP32 form's state plus the same records
+        start, tp_start = with_injected(cur, tp_cur, batches)
+        o = O.Oracle(cfg, start, tp_start, eb)
+        o.set_randoms(uni[drawn:])
+        drawn += sum(int((r["preside"] == 1).sum()) for r in batches.values())
         o.grdcrt()
         o.f["aj"][...] = 0.0
         o.psolve1(2, 0)
         o.reduce_aj()
         o.charge(0)
         o.reduce_rho("rho")
-        assert rel_l2(g.download_field("rho"), o.f["rho"]) < 1e-5, step
-        assert rel_l2(g.download_field("aj"), o.f["aj"]) < 1e-5, step
-
-    gc = g.get_counters().as_dict()
-    og = o.gc.as_dict()
-    assert og["influx"][:2, 0].sum() > 20          # the box absorbed particles
-    assert np.all(np.abs(gc["influx"] - og["influx"]) <= 1)
-    assert np.all(np.abs(gc["nesc"] - og["nesc"]) <= 1)
-    assert og["nesc"][:2].sum() > 10               # particles left through the open z faces
-    surf = g.fx_surface()
-    want = o.surf[:, :surf.shape[1]] - emitted[:, :surf.shape[1]]
-    assert surf.shape == (2, o.nsurf)
-    assert np.abs(surf - want).sum() <= 2
-    assert abs(surf.sum() - want.sum()) <= 1
-    assert (emitted.sum() == 3 * 40)
+        g.fx_step(2, True)  # the re-sort merges the injected particles
+        assert C.rel_l2(g.download_field("rho"), o.f["rho"]) < 1e-5, step
+        assert C.rel_l2(g.download_field("aj"), o.f["aj"]) < 1e-5, step
+        # the step's counts
+        near = C.near_faces(cfg, start, o.pbuf, bodies=[BOUNDS])
+        listed = np.flatnonzero(near)
+        for m in listed:
+            print(f"step {step}: listed particle {m} start ({start[m]['x']:.9f}, {start[m]['y']:.9f}, "
+                  f"{start[m]['z']:.9f}) end ({o.pbuf[m]['x']:.9f}, {o.pbuf[m]['y']:.9f}, {o.pbuf[m]['z']:.9f})")
+        nl = listed.size + listed_anti
+        gc = g.get_counters().as_dict()
+        og = o.gc.as_dict()
+        d_influx = gc["influx"][:2, 0] - gc_prev["influx"][:2, 0]
+        d_nesc = gc["nesc"][:2] - gc_prev["nesc"][:2]
+        surf = g.fx_surface()
+        d_surf = surf - surf_prev
+        want_surf = o.surf[:, :surf.shape[1]] - emitted
+        diff = (int(np.abs(d_influx - og["influx"][:2, 0]).sum()), int(np.abs(d_nesc - og["nesc"][:2]).sum()),
+                int(np.abs(d_surf - want_surf).sum()))
+        print(f"step {step}: influx {d_influx} (oracle {og['influx'][:2, 0]}), nesc {d_nesc} "
+              f"(oracle {og['nesc'][:2]}), surface-count difference {diff[2]}, listed {nl}")
+        assert diff[0] <= nl and diff[1] <= nl and diff[2] <= 2 * nl, (step, diff, nl)
+        if nl == 0:
+            assert diff == (0, 0, 0)
+        totals["influx"] += int(og["influx"][:2, 0].sum())
+        totals["nesc"] += int(og["nesc"][:2].sum())
+        totals["emitted"] += int(emitted.sum())
+        totals["listed"] += nl
+        surf_prev, gc_prev = surf, gc
+        g.fx_store()
+        cur, tp_cur = g.download_particles()
+    print("totals", totals)
+    assert totals["influx"] > 20          # the box absorbed particles
+    assert totals["nesc"] > 10            # particles left through the open z faces
+    assert totals["emitted"] == 4 * 40
+    # background charge from the counts, against the oracle's conversion
+    rho = g.download_field("rho")
+    g.fx_background(False)
+    o2 = O.Oracle(cfg, cur[:0], [0, 0], eb)
+    o2.f["rho"][...] = rho
+    o2.background(surf=g.fx_surface())
+    assert np.array_equal(g.download_field("rhobk"), o2.f["rhobk"])
+    assert np.array_equal(g.download_field("rho"), o2.f["rho"])
+    net = g.fx_surface().sum(1)
+    assert abs(o2.f["rhobk"].sum() - sum(cfg.q[s] * net[s] for s in range(2))) < 1e-9 * abs(cfg.q[0]) * np.abs(net).sum()
     g.close()

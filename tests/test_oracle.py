@@ -209,3 +209,40 @@ def test_compact_keeps_order():
 def test_hash_uniforms():
     u = np.array([O.hash_u01(1, 2, i) for i in range(4000)])
     assert (u >= 0).all() and (u < 1).all() and abs(u.mean() - 0.5) < 0.02
+
+
+def test_background_charge_from_surface_counts():
+    """orc_background: one count on a face cell puts q/4 on each of the
+    four nodes of that face cell; any counts give total charge sum(q * count);
+    rho(0:n) gets rhobk added, or replaced with replace."""
+    case = small_case(n=(12, 10, 14))
+    box = dict(geotype=0, ncond=1, xlpc=3.0, xupc=7.0, ylpc=2.0, yupc=5.0, zlpc=4.0, zupc=9.0, sqdscaled=1.0)
+    case.bodies = [box]
+    cfg = inputs.make_config(case)
+    p, tp = inputs.make_particles(case)
+    o = O.Oracle(cfg, p[:0], [0, 0], inputs.make_fields(case))
+    off = np.zeros(6 * 4, dtype=np.int64)
+    nsurf = int(O.lib().orc_surface_layout(ctypes.byref(cfg), off.ctypes.data))
+    assert nsurf == 2 * (3 * 5 + 4 * 5 + 4 * 3)
+    lo, hi = (3, 2, 4), (7, 5, 9)
+    # +y face (f = 3), cell (u, v) = (1, 2): x in [4, 5], z in [6, 7], y = 5
+    surf = np.zeros((cfg.nspec, nsurf), dtype=np.int64)
+    surf[0, off[3] + 1 + 4 * 2] = 1
+    o.background(surf=surf)
+    rb = o.f["rhobk"][..., 0]
+    nz_idx = np.argwhere(rb != 0)
+    got = {(int(k) - 1, int(j) - 1, int(i) - 1) for k, j, i in nz_idx}
+    assert got == {(6, 5, 4), (6, 5, 5), (7, 5, 4), (7, 5, 5)}  # (k, j, i)
+    assert np.all(rb[rb != 0] == cfg.q[0] * 0.25)
+    # random counts: the total charge, and rho += rhobk on the nodes 0..n
+    rng = np.random.default_rng(3)
+    surf = rng.integers(-3, 9, size=(cfg.nspec, nsurf))
+    o.f["rho"][...] = rng.random(o.f["rho"].shape)
+    rho0 = o.f["rho"].copy()
+    o.background(surf=surf)
+    want = sum(cfg.q[s] * surf[s].sum() for s in range(cfg.nspec))
+    assert abs(o.f["rhobk"].sum() - want) <= 1e-12 * np.abs(cfg.q[:2]).sum() * np.abs(surf).sum()
+    inner = (slice(1, cfg.nz + 2), slice(1, cfg.ny + 2), slice(1, cfg.nx + 2))
+    assert np.array_equal(o.f["rho"][inner], rho0[inner] + o.f["rhobk"][inner])
+    o.background(surf=surf, replace=True)
+    assert np.array_equal(o.f["rho"][inner], o.f["rhobk"][inner])
