@@ -293,7 +293,7 @@ def accuracy_report(steps: int = 4) -> dict:
             for k in ("cell_mismatch", "cell_mismatch_off_band", "near_face", "alive_mismatch"):
                 worst[k] += rep[k]
             for name, key in (("rho", "rho"), ("aj", "j")):
-                fe = C.field_errors(g.download_field(name), o.f[name])
+                fe = C.field_errors(g.download_field(name), o.f[name], cfg)
                 worst[key + "_l2_rel"] = max(worst[key + "_l2_rel"], fe["l2_rel"])
                 worst[key + "_max_rel"] = max(worst[key + "_max_rel"], fe["max_rel"])
             eg = g.fx_energy()
@@ -331,7 +331,8 @@ def accuracy_report(steps: int = 4) -> dict:
                          f"({int(tp.sum()):,} particles), {steps} steps with the re-sort after step {SORT_EVERY}; the "
                          "FP64 oracle started every step from the FP32 form's state; worst step (max) or total over "
                          "the steps (counts)")
-    worst["definitions"] = ("pos in cells, vel relative to the largest |v|, rho/J relative L2 and max; cell "
+    worst["definitions"] = ("pos in cells, vel relative to the largest |v|, rho/J relative L2 and max on the "
+                            "nodes 0..n; cell "
                             "mismatches counted, those farther than 4 FP32 ulps from every face must be 0; "
                             "permutation against the tile sort's definition with the oracle's cells; energy = FP64 "
                             "kinetic energy of the FP32 state vs the oracle's; continuity = max |rho_new - rho_old + "
@@ -533,9 +534,9 @@ def run_ours(args, world, rank, local):
 
 
 def run_ensemble_line(args, world, rank, local):
-    """The ensemble workload: runs split across ranks (round robin), each
-    rank's runs in one graph per wave; value = all runs' particle-steps over
-    the slowest rank's device time."""
+    """The ensemble workload: runs split across ranks by particle count
+    (ensemble.split_runs), each rank's runs in one graph per wave; value =
+    all runs' particle-steps over the slowest rank's device time."""
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no ensemble runner: each "
@@ -547,7 +548,7 @@ def run_ensemble_line(args, world, rank, local):
     torch.cuda.set_device(local)
     select_device(local)
     cases = ensemble.ensemble_cases(args.ensemble_runs)
-    mine = cases[rank::world]
+    mine = [cases[i] for i in ensemble.split_runs(cases, world, rank)]
     tuner = ensemble.Autotuner()
     with Clocks(local) as clk:
         out = ensemble.run_ensemble(mine, args.ensemble_steps, tuner, modes=("batch", "each"))

@@ -65,6 +65,21 @@ def particles(case: inputs.Case) -> int:
     return sum(s.ppc for s in case.species) * ncell
 
 
+def split_runs(cases: list[inputs.Case], world: int, rank: int) -> list[int]:
+    """Indices of the runs rank `rank` of `world` takes: the runs go, largest
+    first, to the rank with the fewest particles so far (ties to the lower
+    rank), so that every rank gets about the same particle-steps; no run is
+    split and no data moves between ranks."""
+    load = [0] * world
+    mine = []
+    for i in sorted(range(len(cases)), key=lambda i: (-particles(cases[i]), i)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += particles(cases[i])
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
 def run_bytes(case: inputs.Case) -> int:
     """Device memory of one run (context + FP32 form + sort scratch), with margin."""
     g = (case.n[0] + 9) * (case.n[1] + 9) * (case.n[2] + 9)

@@ -11,7 +11,9 @@
  *
  * Loss: sum over steps and over the probe nodes of Jx(node)^2.
  *
- * Reverse sweep by hand, step by step from the last: the J-loss gradient
+ * Reverse sweep by hand, step by step from the last (orc_adjoint_ckpt keeps
+ * the state every ckpt steps and recomputes each segment's states, moves
+ * only, before its reverse steps; orc_adjoint keeps every state): the J-loss gradient
  * g = 2 Jx on the probe nodes gives dS/da and dS/db of each particle's
  * deposit S = sum_nodes g . J; the move gives lambda_v += lambda_a*ustep and
  * lambda_b += lambda_a; the Boris rotation is transposed term by term; the
@@ -23,6 +25,7 @@
  */
 #include <cmath>
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -172,56 +175,83 @@ double wrap(double x, int n) {
 
 }  // namespace
 
-extern "C" double orc_adjoint(const emsesg_config* c, int K, int ustep, const double* enode, const double* bnode,
-                              const double* e0b0, emsesg_particle* p, int64_t np, const int* probe_lo,
-                              const int* probe_hi, double* gE, double* gB, double* g0, double* gv) {
+extern "C" double orc_adjoint_ckpt(const emsesg_config* c, int K, int ckpt, int ustep, const double* enode,
+                                   const double* bnode, const double* e0b0, emsesg_particle* p, int64_t np,
+                                   const int* probe_lo, const int* probe_hi, double* gE, double* gB, double* g0,
+                                   double* gv) {
   const Grid G{{c->nx, c->ny, c->nz}};
   const int64_t nn = (int64_t)c->nx * c->ny * c->nz;
   const double rustep = 1.0 / ustep;
   const bool grad = gE != nullptr;
-  std::vector<double> xs((size_t)(grad ? (K + 1) * np * 3 : 0)), vs((size_t)(grad ? (K + 1) * np * 3 : 0));
+  if (ckpt < 1 || ckpt > K || K % ckpt != 0) ckpt = K;
+  const int nseg = K / ckpt;
+  // checkpoints (state before steps 0, ckpt, 2 ckpt, ...) and the states of
+  // one segment, recomputed from its checkpoint in the reverse sweep
+  std::vector<double> ckx((size_t)(grad ? nseg * np * 3 : 0)), ckv((size_t)(grad ? nseg * np * 3 : 0));
+  std::vector<double> xs((size_t)(grad ? ckpt * np * 3 : 0)), vs((size_t)(grad ? ckpt * np * 3 : 0));
   std::vector<double> J((size_t)(3 * nn)), Jx((size_t)(grad ? K * nn : 0));
   auto probe = [&](int64_t node) {
     const int i = (int)(node % c->nx), j = (int)((node / c->nx) % c->ny), k = (int)(node / ((int64_t)c->nx * c->ny));
     return i >= probe_lo[0] && i < probe_hi[0] && j >= probe_lo[1] && j < probe_hi[1] && k >= probe_lo[2] &&
            k < probe_hi[2];
   };
-  double loss = 0.0;
-  for (int n = 0; n < K; n++) {
-    std::memset(J.data(), 0, J.size() * sizeof(double));
+  // one forward step of every particle of p in place; the states before it
+  // go to (sx, sv) when given, the current into J when `deposit`
+  auto step = [&](double* sx, double* sv, bool deposit) {
+    if (deposit) std::memset(J.data(), 0, J.size() * sizeof(double));
     for (int64_t m = 0; m < np; m++) {
       emsesg_particle& q = p[m];
       const int is = q.spec - 1;
       const double x[3] = {q.x, q.y, q.z};
-      if (grad) {
-        for (int k = 0; k < 3; k++) xs[(size_t)((n * np + m) * 3 + k)] = x[k];
-        vs[(size_t)((n * np + m) * 3 + 0)] = q.vx;
-        vs[(size_t)((n * np + m) * 3 + 1)] = q.vy;
-        vs[(size_t)((n * np + m) * 3 + 2)] = q.vz;
+      if (sx) {
+        for (int k = 0; k < 3; k++) sx[3 * m + k] = x[k];
+        sv[3 * m + 0] = q.vx;
+        sv[3 * m + 1] = q.vy;
+        sv[3 * m + 2] = q.vz;
       }
       const Fwd f = forward(G, enode, bnode, e0b0, x, V3{q.vx, q.vy, q.vz}, c->qm[is] * ustep * 0.5);
       const double a[3] = {x[0] + f.vnew.x * ustep, x[1] + f.vnew.y * ustep, x[2] + f.vnew.z * ustep};
-      const Seg ax[3] = {relay(x[0], a[0]), relay(x[1], a[1]), relay(x[2], a[2])};
-      zigzag(G, ax, x, a, c->q[is], rustep, J.data(), nullptr, nullptr, nullptr);
+      if (deposit) {
+        const Seg ax[3] = {relay(x[0], a[0]), relay(x[1], a[1]), relay(x[2], a[2])};
+        zigzag(G, ax, x, a, c->q[is], rustep, J.data(), nullptr, nullptr, nullptr);
+      }
       q.vx = f.vnew.x; q.vy = f.vnew.y; q.vz = f.vnew.z;
       q.x = wrap(a[0], c->nx); q.y = wrap(a[1], c->ny); q.z = wrap(a[2], c->nz);
     }
+  };
+  double loss = 0.0;
+  for (int n = 0; n < K; n++) {
+    double* sx = (grad && n % ckpt == 0) ? &ckx[(size_t)((n / ckpt) * np * 3)] : nullptr;
+    double* sv = (grad && n % ckpt == 0) ? &ckv[(size_t)((n / ckpt) * np * 3)] : nullptr;
+    step(sx, sv, true);
     for (int64_t node = 0; node < nn; node++)
       if (probe(node)) loss += J[3 * node] * J[3 * node];
     if (grad)
       for (int64_t node = 0; node < nn; node++) Jx[(size_t)(n * nn + node)] = J[3 * node];
   }
   if (!grad) return loss;
+  // the state after K steps is given back at the end
+  std::vector<emsesg_particle> pend(p, p + np);
   std::memset(gE, 0, 3 * nn * sizeof(double));
   std::memset(gB, 0, 3 * nn * sizeof(double));
   std::memset(g0, 0, 6 * sizeof(double));
   std::vector<double> lx((size_t)(3 * np), 0.0), lv((size_t)(3 * np), 0.0), gJ((size_t)(3 * nn), 0.0);
-  for (int n = K - 1; n >= 0; n--) {
+  for (int sg = nseg - 1; sg >= 0; sg--) {
+    // recompute the segment's states from its checkpoint (moves only)
+    for (int64_t m = 0; m < np; m++) {
+      const double* x = &ckx[(size_t)((sg * np + m) * 3)];
+      const double* v = &ckv[(size_t)((sg * np + m) * 3)];
+      p[m].x = x[0]; p[m].y = x[1]; p[m].z = x[2];
+      p[m].vx = v[0]; p[m].vy = v[1]; p[m].vz = v[2];
+    }
+    for (int j = 0; j < ckpt; j++) step(&xs[(size_t)(j * np * 3)], &vs[(size_t)(j * np * 3)], false);
+  for (int j = ckpt - 1; j >= 0; j--) {
+    const int n = sg * ckpt + j;
     for (int64_t node = 0; node < nn; node++) gJ[3 * node] = probe(node) ? 2.0 * Jx[(size_t)(n * nn + node)] : 0.0;
     for (int64_t m = 0; m < np; m++) {
       const int is = p[m].spec - 1;
-      const double* x = &xs[(size_t)((n * np + m) * 3)];
-      const double* v = &vs[(size_t)((n * np + m) * 3)];
+      const double* x = &xs[(size_t)((j * np + m) * 3)];
+      const double* v = &vs[(size_t)((j * np + m) * 3)];
       const Fwd f = forward(G, enode, bnode, e0b0, x, V3{v[0], v[1], v[2]}, c->qm[is] * ustep * 0.5);
       const double a[3] = {x[0] + f.vnew.x * ustep, x[1] + f.vnew.y * ustep, x[2] + f.vnew.z * ustep};
       const Seg ax[3] = {relay(x[0], a[0]), relay(x[1], a[1]), relay(x[2], a[2])};
@@ -265,7 +295,15 @@ extern "C" double orc_adjoint(const emsesg_config* c, int K, int ustep, const do
       LV[0] = lvold.x; LV[1] = lvold.y; LV[2] = lvold.z;
     }
   }
+  }
   for (int64_t m = 0; m < np; m++)
     for (int k = 0; k < 3; k++) gv[3 * m + k] = lv[(size_t)(3 * m + k)];
+  std::copy(pend.begin(), pend.end(), p);
   return loss;
+}
+
+extern "C" double orc_adjoint(const emsesg_config* c, int K, int ustep, const double* enode, const double* bnode,
+                              const double* e0b0, emsesg_particle* p, int64_t np, const int* probe_lo,
+                              const int* probe_hi, double* gE, double* gB, double* g0, double* gv) {
+  return orc_adjoint_ckpt(c, K, K, ustep, enode, bnode, e0b0, p, np, probe_lo, probe_hi, gE, gB, g0, gv);
 }

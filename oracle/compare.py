@@ -70,7 +70,23 @@ def particle_errors(cfg, pg, po, band: float = BAND) -> dict:
     return out
 
 
-def field_errors(g, o) -> dict:
+def nodes(cfg, a):
+    """The nodes 0..n of every axis of a rho-layout (guard 1) or aj-layout
+    (guard 4) array, numpy shape (z, y, x[, c]): the field the reference's
+    solver and rhoupd use.  The guard layers are left out: after a periodic
+    fold they keep partial sums that depend on which side of a periodic face
+    a particle is stored, and a particle that ends within an FP32 ulp of that
+    face is stored on one side by the FP32 form and on the other by FP64."""
+    nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
+    lo = (a.shape[0] - nz - 1) // 2  # 1 for rho, 4 for aj
+    return a[lo:lo + nz + 1, lo:lo + ny + 1, lo:lo + nx + 1]
+
+
+def field_errors(g, o, cfg=None) -> dict:
+    """Relative L2 and max errors of a field, on the nodes 0..n when cfg is
+    given (see nodes), else over the whole array."""
+    if cfg is not None:
+        g, o = nodes(cfg, g), nodes(cfg, o)
     return {"l2_rel": rel_l2(g, o), "max_rel": max_rel(g, o)}
 
 

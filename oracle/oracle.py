@@ -82,6 +82,8 @@ def lib() -> ctypes.CDLL:
         "orc_load_plasma": (None, [cfgp, ctypes.POINTER(Plasma), _P, i64p]),
         "orc_adjoint": (ctypes.c_double, [cfgp, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, ctypes.c_int64, _P, _P,
                                           _P, _P, _P, _P]),
+        "orc_adjoint_ckpt": (ctypes.c_double, [cfgp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P,
+                                               ctypes.c_int64, _P, _P, _P, _P, _P, _P]),
         "orc_blocks_create": (_P, [cfgp, _P, _P, i64p, ctypes.c_int, ctypes.c_int]),
         "orc_blocks_threads": (ctypes.c_int, [_P]),
         "orc_blocks_particles": (ctypes.c_int64, [_P]),
@@ -307,10 +309,11 @@ def ranu0_stream(seed: int, n: int) -> np.ndarray:
 
 
 def adjoint(cfg: Config, K: int, ustep: int, enode: np.ndarray, bnode: np.ndarray, e0b0, pbuf: np.ndarray,
-            probe_lo, probe_hi, grad: bool = True):
+            probe_lo, probe_hi, grad: bool = True, ckpt: int = 0):
     """FP64 loss sum_steps sum_probe Jx^2 of K periodic steps and its
     gradients (adjoint.cpp): returns (loss, gE, gB, g0, gv); node fields are
-    [n^3][3] with x fastest and exclude e0 / b0."""
+    [n^3][3] with x fastest and exclude e0 / b0.  ckpt: keep the state every
+    ckpt steps and recompute in between (0: keep every state)."""
     p = np.ascontiguousarray(pbuf, dtype=PARTICLE_DTYPE).copy()
     en = np.ascontiguousarray(enode, dtype=np.float64)
     bn = np.ascontiguousarray(bnode, dtype=np.float64)
@@ -323,6 +326,6 @@ def adjoint(cfg: Config, K: int, ustep: int, enode: np.ndarray, bnode: np.ndarra
     g0 = np.zeros(6) if grad else None
     gv = np.zeros((p.size, 3)) if grad else None
     ptr = (lambda a: a.ctypes.data if a is not None else None)
-    loss = lib().orc_adjoint(ctypes.byref(cfg), K, ustep, en.ctypes.data, bn.ctypes.data, e0.ctypes.data,
-                             p.ctypes.data, p.size, lo, hi, ptr(gE), ptr(gB), ptr(g0), ptr(gv))
+    loss = lib().orc_adjoint_ckpt(ctypes.byref(cfg), K, ckpt or K, ustep, en.ctypes.data, bn.ctypes.data,
+                                  e0.ctypes.data, p.ctypes.data, p.size, lo, hi, ptr(gE), ptr(gB), ptr(g0), ptr(gv))
     return loss, gE, gB, g0, gv

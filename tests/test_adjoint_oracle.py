@@ -81,3 +81,13 @@ def test_initial_velocity_gradients(problem):
             b[f][m] -= h
             fd = (L(cfg, args, en, bn, e0, a) - L(cfg, args, en, bn, e0, b)) / (2 * h)
             assert abs(gv[m, comp] - fd) <= 1e-4 * abs(fd) + 1e-16 * loss / h * 50, (m, comp)
+
+
+def test_checkpointed_adjoint_equals_the_full_one(problem):
+    """Keeping the state every 2 steps and recomputing in between gives the
+    same loss and gradients, bit for bit."""
+    cfg, p, en, bn, e0, args, (loss, gE, gB, g0, gv) = problem
+    r = O.adjoint(cfg, args["K"], 2, en, bn, e0, p, args["lo"], args["hi"], ckpt=2)
+    assert r[0] == loss
+    for a, b in zip(r[1:], (gE, gB, g0, gv)):
+        assert np.array_equal(a, b)
