@@ -59,6 +59,9 @@ SORT_EVERY = 4
 # per cell): 2*28 (push read+write) + (2*28+8)/4 (sort) + (24+32)/128 (grid).
 B_ALG_STEP = 2 * 28 + (2 * 28 + 8) / SORT_EVERY + (24 + 32) / 128
 B_ALG_PUSH = 2 * 28  # the fused push + deposit kernel, per particle
+# The plain FP64 drop-in (64-byte records): push read + write 128, charge read
+# 64, sort (128 + 8)/S, grid (48 + 32)/128.
+B_ALG_FP64 = 2 * 64 + 64 + (2 * 64 + 8) / SORT_EVERY + (48 + 32) / 128
 
 
 def peaks() -> tuple[float, str]:
@@ -245,6 +248,16 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def fx_fp64_checks(g) -> dict:
+    """The FP64 checks of the FP32 state after the last step: kinetic energy
+    per species and component (energy.F90), and the continuity residual
+    max |rho_new - rho_old + 2 div J| of the last step with max |rho|."""
+    e = g.fx_energy()
+    res, rmax = g.fx_continuity()
+    return {"kinetic_energy": [[float(x) for x in row] for row in e], "continuity_residual": res,
+            "max_rho": rmax, "note": "FP64 over the FP32 state of the last timed step"}
+
+
 # --------------------------------------------------------------- accuracy (checker)
 def accuracy_report(steps: int = 4) -> dict:
     """Errors of the FP32 form against the FP64 oracle on the headline
@@ -261,7 +274,7 @@ def accuracy_report(steps: int = 4) -> dict:
     eb = inputs.make_fields(case)
     p, tp = inputs.make_particles(case)
     worst = {"pos_max_abs": 0.0, "pos_rms": 0.0, "vel_max_rel": 0.0, "vel_l2_rel": 0.0, "rho_l2_rel": 0.0,
-             "rho_max_rel": 0.0, "j_l2_rel": 0.0, "j_max_rel": 0.0, "cell_mismatch": 0, "cell_mismatch_off_band": 0,
+             "rho_max_rel": 0.0, "j_l2_rel": 0.0, "j_max_rel": 0.0, "j_l2_rel_same_cells": 0.0, "cell_mismatch": 0, "cell_mismatch_off_band": 0,
              "near_face": 0, "alive_mismatch": 0, "sort_count_mismatch_cells": 0, "permutation_mismatch": 0,
              "energy_rel": 0.0, "energy_fp64_reproducible": True, "continuity_residual": 0.0,
              "continuity_residual_oracle": 0.0, "continuity_max_rho": 0.0}
@@ -296,6 +309,9 @@ def accuracy_report(steps: int = 4) -> dict:
                 fe = C.field_errors(g.download_field(name), o.f[name], cfg)
                 worst[key + "_l2_rel"] = max(worst[key + "_l2_rel"], fe["l2_rel"])
                 worst[key + "_max_rel"] = max(worst[key + "_max_rel"], fe["max_rel"])
+            _, same = C.j_error_corrected(cfg, g.download_field("aj"), o.f["aj"], cur, after, o.pbuf,
+                                          rep["mismatched"])
+            worst["j_l2_rel_same_cells"] = max(worst["j_l2_rel_same_cells"], same)
             eg = g.fx_energy()
             worst["energy_rel"] = max(worst["energy_rel"], C.rel_l2(eg, o.energy()))
             worst["energy_fp64_reproducible"] &= bool(np.array_equal(eg, g.fx_energy()))
@@ -332,7 +348,8 @@ def accuracy_report(steps: int = 4) -> dict:
                          "FP64 oracle started every step from the FP32 form's state; worst step (max) or total over "
                          "the steps (counts)")
     worst["definitions"] = ("pos in cells, vel relative to the largest |v|, rho/J relative L2 and max on the "
-                            "nodes 0..n; cell "
+                            "nodes 0..n (j_l2_rel_same_cells: with the oracle's zigzag current moved to the "
+                            "cells the FP32 form took for the particles FP32 rounding put across a face); cell "
                             "mismatches counted, those farther than 4 FP32 ulps from every face must be 0; "
                             "permutation against the tile sort's definition with the oracle's cells; energy = FP64 "
                             "kinetic energy of the FP32 state vs the oracle's; continuity = max |rho_new - rho_old + "
@@ -470,6 +487,7 @@ def run_ours(args, world, rank, local):
         t = timed(fx_step, args.steps)
     prof = g.profile()
     g.set_profiling(False)
+    fp64_checks = fx_fp64_checks(g)
 
     # ---- end to end through the C ABI with host buffers
     eb_host = torch.empty(eb.size, dtype=torch.float64, pin_memory=True)
@@ -517,7 +535,10 @@ def run_ours(args, world, rank, local):
                 "h2d_bytes_per_step": int(eb.size * 8), "d2h_bytes_per_step": int((nr + na) * 8)},
         "fp64_dropin": {"value": world * npart * k64 / t64, "unit": UNIT, "steps": k64,
                         "ms_per_step": t64 / k64 * 1e3,
-                        "fp32_over_fp64": (value / (world * npart * k64 / t64))},
+                        "fp32_over_fp64": (value / (world * npart * k64 / t64)),
+                        "bytes_per_particle_step_alg": B_ALG_FP64,
+                        "roofline_frac": B_ALG_FP64 * npart / (t64 / k64) / 1e9 / hbm},
+        "fp64_checks": fp64_checks,
         "gpu_launches": int(sum(n for _, n in prof.values())),
         "kernels_ms": {k: round(v[0], 3) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
         "clocks": clk.summary(),
@@ -741,6 +762,9 @@ def run_body_line(args, world, rank, local):
     prof = g.profile()
     g.set_profiling(False)
     n1 = int(g.fx_counts().sum())
+    body_checks = fx_fp64_checks(g)
+    g.fx_background(False)  # add_background_charge from the surface counts
+    body_checks["background_charge_total"] = float(g.download_field("rhobk").sum())
     inj_bytes = (sum(int(r.nbytes) for st in inj[warm:warm + steps] for r in st) if args.host_inject
                  else 0)
     # end to end: the same steps plus rho and J to host after each one
@@ -783,6 +807,7 @@ def run_body_line(args, world, rank, local):
         "e2e": {"value": world * 0.5 * (ne0 + ne1) * ke / te, "unit": UNIT, "steps": ke,
                 "h2d_bytes_per_step": int(inj_bytes / steps), "d2h_bytes_per_step": int((nr + na) * 8)},
         "particles": {"start": n0, "end": n1},
+        "fp64_checks": body_checks,
         "absorbed": {"influx_e": int(counters["influx"][0].sum()), "influx_i": int(counters["influx"][1].sum()),
                      "surface_net_e": int(surf[0].sum()), "surface_net_i": int(surf[1].sum()),
                      "escaped_e": int(counters["nesc"][0]), "escaped_i": int(counters["nesc"][1])},

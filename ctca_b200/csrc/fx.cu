@@ -954,7 +954,7 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
                 ctx->field[EMSESG_FIELD_AJ], fj.size());
   unsigned long long* cres = (unsigned long long*)(f.diag + 3 * DIAG_GRID + 3);
   EMSESG_CUDA(ctx, cudaMemsetAsync(cres, 0, 2 * sizeof(double), ctx->stream));
-  EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_rho, nblk(fr.size()), 256, 0, (const long long*)acc_rho,
+  EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_rho, nblk(fr.size(), RHO_BLOCK), RHO_BLOCK, 0, (const long long*)acc_rho,
                 ctx->field[EMSESG_FIELD_RHO], ctx->field[EMSESG_FIELD_AJ], fr, fj, c.nx, c.ny, c.nz, cres);
   f.cont_valid = f.rho_prev;
   f.rho_prev = true;
@@ -1359,7 +1359,8 @@ struct emsesg::AdjWork {
   int64_t cap = 0, nl = 0, nn = 0;
   std::vector<FxSnap> ck, seg;     // checkpoints; the states of one segment
   std::vector<uint32_t*> inv;      // sort maps of one segment
-  float *lam = nullptr, *lam2 = nullptr, *gd = nullptr, *gEd = nullptr, *gBd = nullptr;
+  float *lam = nullptr, *lam2 = nullptr, *gd = nullptr;
+  double *gEd = nullptr, *gBd = nullptr;  // node-field gradients, FP64 sums
   float* jx = nullptr;             // probe Jx of each step
   int jx_steps = 0;
   double* lossd = nullptr;
@@ -1402,8 +1403,8 @@ int adj_reserve(emsesg_ctx* ctx, AdjWork& w, int nseg, int ckpt, int jsteps, int
   if (!w.lam) EMSESG_CUDA(ctx, cudaMalloc(&w.lam, 6 * cap * sizeof(float)));
   if (!w.lam2) EMSESG_CUDA(ctx, cudaMalloc(&w.lam2, 6 * cap * sizeof(float)));
   if (!w.gd) EMSESG_CUDA(ctx, cudaMalloc(&w.gd, 3 * nn * sizeof(float)));
-  if (!w.gEd) EMSESG_CUDA(ctx, cudaMalloc(&w.gEd, 3 * nn * sizeof(float)));
-  if (!w.gBd) EMSESG_CUDA(ctx, cudaMalloc(&w.gBd, 3 * nn * sizeof(float)));
+  if (!w.gEd) EMSESG_CUDA(ctx, cudaMalloc(&w.gEd, 3 * nn * sizeof(double)));
+  if (!w.gBd) EMSESG_CUDA(ctx, cudaMalloc(&w.gBd, 3 * nn * sizeof(double)));
   if (!w.lossd) EMSESG_CUDA(ctx, cudaMalloc(&w.lossd, sizeof(double)));
   if (w.jx_steps < jsteps) {
     cudaFree(w.jx);
@@ -1518,8 +1519,8 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
   float* lam2 = w.lam2;
   float* const jx = w.jx;
   float* const gd = w.gd;
-  float* const gEd = w.gEd;
-  float* const gBd = w.gBd;
+  double* const gEd = w.gEd;
+  double* const gBd = w.gBd;
   double* const lossd = w.lossd;
   ArrayOwners owners(f, seg);
 #define EMSESG_ADJ(call) do { rc = (call); if (rc) return rc; } while (0)
@@ -1535,8 +1536,8 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
   // backward
   float* lx = lam;
   EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(lam, 0, 6 * cap * sizeof(float), ctx->stream), "adjoint lambda"));
-  EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(gEd, 0, 3 * nn * sizeof(float), ctx->stream), "adjoint gE"));
-  EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(gBd, 0, 3 * nn * sizeof(float), ctx->stream), "adjoint gB"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(gEd, 0, 3 * nn * sizeof(double), ctx->stream), "adjoint gE"));
+  EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(gBd, 0, 3 * nn * sizeof(double), ctx->stream), "adjoint gB"));
   AdjArgs a{};
   for (int is = 0; is < c.nspec; is++) {
     a.off[is] = f.base[is];
@@ -1636,10 +1637,10 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
     EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(gv, gvd, ntot * 3 * sizeof(double), cudaMemcpyDeviceToHost,
                                                ctx->stream), "gv"));
   }
-  std::vector<float> hE((size_t)(3 * nn)), hB((size_t)(3 * nn));
-  EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(hE.data(), gEd, 3 * nn * sizeof(float), cudaMemcpyDeviceToHost,
+  std::vector<double> hE((size_t)(3 * nn)), hB((size_t)(3 * nn));
+  EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(hE.data(), gEd, 3 * nn * sizeof(double), cudaMemcpyDeviceToHost,
                                              ctx->stream), "gE"));
-  EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(hB.data(), gBd, 3 * nn * sizeof(float), cudaMemcpyDeviceToHost,
+  EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(hB.data(), gBd, 3 * nn * sizeof(double), cudaMemcpyDeviceToHost,
                                              ctx->stream), "gB"));
   EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(loss, lossd, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
                         "loss"));

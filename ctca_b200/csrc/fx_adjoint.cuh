@@ -13,8 +13,10 @@
 //   Boris      the rotation transposed term by term -> lambda_v_n,
 //              lambda_E, lambda_B at the particle
 //   gather     w_c lambda_E, w_c lambda_B added to the node-field gradients
-//              (per-thread run sums in registers, added into a shared-memory
-//              box when the thread's cell changes, then global float atomics);
+//              (per-thread FP32 run sums in registers, added into an FP64
+//              shared-memory box when the thread's cell changes, then FP64
+//              global atomics: the gradient sums over particles and steps run
+//              in FP64);
 //              sum_c grad(w_c) (E_c . lambda_E + B_c . lambda_B) added to
 //              lambda_x
 // The same formulas in FP64 are the CPU checker (oracle/adjoint.cpp).
@@ -38,8 +40,8 @@ struct AdjArgs {
   const float4* __restrict__ f0;  // node fields (nodes 0..n per axis)
   const float4* __restrict__ f1;
   const float* __restrict__ g;    // dL/dJ per unique node, 3 components
-  float* gE;                      // node-field gradients per unique node, 3 + 3
-  float* gB;
+  double* gE;                     // node-field gradients per unique node, 3 + 3 (FP64 sums)
+  double* gB;
   Geo geo;
   int64_t ntiles;
 };
@@ -146,8 +148,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
   extern __shared__ __align__(16) float4 adj_smem[];
   float4* sf0 = adj_smem;
   float4* sf1 = sf0 + NF;
-  float* sg = reinterpret_cast<float*>(sf1 + NF);  // 3 per node
-  float* sgr = sg + 3 * NF;                        // 6 per node: dE (3), dB (3)
+  double* sgr = reinterpret_cast<double*>(sf1 + NF);  // 6 per node: dE (3), dB (3), FP64
+  float* sg = reinterpret_cast<float*>(sgr + 6 * NF);  // 3 per node
   const Geo& G = a.geo;
   const int is = blockIdx.y, t = blockIdx.x, tid = threadIdx.x;
   const int64_t* ts = a.tile_start + (int64_t)is * (a.ntiles + 1);
@@ -177,7 +179,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
       anyg = anyg || sg[3 * e + c] != 0.f;
     }
 #pragma unroll
-    for (int c = 0; c < 6; c++) sgr[6 * e + c] = 0.f;
+    for (int c = 0; c < 6; c++) sgr[6 * e + c] = 0.0;
   }
   // dL/dJ is zero on every node of most boxes (the loss sees a probe region
   // only): their particles' zigzag terms are zero and are skipped
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
       const int e = runbase + (c >> 2) * B * B + ((c >> 1) & 1) * B + (c & 1);
 #pragma unroll
       for (int q = 0; q < 6; q++) {
-        if (pacc[6 * c + q] != 0.f) atomicAdd(&sgr[6 * e + q], pacc[6 * c + q]);
+        if (pacc[6 * c + q] != 0.f) atomicAdd(&sgr[6 * e + q], (double)pacc[6 * c + q]);
         pacc[6 * c + q] = 0.f;
       }
     }
@@ -303,8 +305,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
         const int64_t un = unique_node(G, cb[0] + di, cb[1] + dj, cb[2] + dk);
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-          atomicAdd(&a.gE[3 * un + q], gv[q]);
-          atomicAdd(&a.gB[3 * un + q], gv[3 + q]);
+          atomicAdd(&a.gE[3 * un + q], (double)gv[q]);
+          atomicAdd(&a.gB[3 * un + q], (double)gv[3 + q]);
         }
       }
     }
@@ -326,9 +328,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
     const int64_t un = unique_node(G, gi, gj, gk);
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      const float vE = sgr[6 * e + q], vB = sgr[6 * e + 3 + q];
-      if (vE != 0.f) atomicAdd(&a.gE[3 * un + q], vE);
-      if (vB != 0.f) atomicAdd(&a.gB[3 * un + q], vB);
+      const double vE = sgr[6 * e + q], vB = sgr[6 * e + 3 + q];
+      if (vE != 0.0) atomicAdd(&a.gE[3 * un + q], vE);
+      if (vB != 0.0) atomicAdd(&a.gB[3 * un + q], vB);
     }
   }
 }
@@ -336,7 +338,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
 inline int fx_adjoint_smem(int tmax) {
   const int B = fx_box_tile(tmax) + 2 * PG + 1;
   const int nf = B * B * B;
-  return nf * (int)(2 * sizeof(float4) + 9 * sizeof(float));
+  return nf * (int)(2 * sizeof(float4) + 6 * sizeof(double) + 3 * sizeof(float));
 }
 
 // lambda through a sort: the adjoint of S_{n+1} (new layout) back to the

@@ -78,24 +78,44 @@ __device__ __forceinline__ void max_nonneg(unsigned long long* p, double v) {
 // rho (FP64) from the folded int64 accumulator (scale 2^-40), and over the
 // nodes 0..n the continuity residual of the step: res[0] = max |rho_new -
 // rho_old + 2 (div J)|, res[1] = max |rho_new| (rhoupd.F90:41-49 gives
-// rho_old - 2 div J as the prediction of rho_new).
-__global__ void k_fix_to_rho(const long long* __restrict__ acc, double* __restrict__ rho,
-                             const double* __restrict__ aj, FieldDesc fr, FieldDesc fj, int nx, int ny, int nz,
-                             unsigned long long* res) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= fr.size()) return;
-  const double v = (double)acc[e] * (1.0 / 1099511627776.0);
-  const int64_t ex = fr.ex, ey = fr.ey;
-  const int i = (int)(e % ex) + fr.lo, j = (int)((e / ex) % ey) + fr.lo, k = (int)(e / (ex * ey)) + fr.lo;
-  if (i >= 0 && j >= 0 && k >= 0 && i <= nx && j <= ny && k <= nz) {
-    const double div = (aj[fj.at(0, i, j, k)] - aj[fj.at(0, i - 1, j, k)]) +
-                       (aj[fj.at(1, i, j, k)] - aj[fj.at(1, i, j - 1, k)]) +
-                       (aj[fj.at(2, i, j, k)] - aj[fj.at(2, i, j, k - 1)]);
-    const double r = fabs(v - (rho[e] - div * 2.0));
-    max_nonneg(&res[0], r);
-    max_nonneg(&res[1], fabs(v));
+// rho_old - 2 div J as the prediction of rho_new).  The maxima are taken per
+// block (warp shuffles, then the block's warps) before one atomic per block.
+constexpr int RHO_BLOCK = 256;
+__global__ void __launch_bounds__(RHO_BLOCK) k_fix_to_rho(const long long* __restrict__ acc, double* __restrict__ rho,
+                                                          const double* __restrict__ aj, FieldDesc fr, FieldDesc fj,
+                                                          int nx, int ny, int nz, unsigned long long* res) {
+  __shared__ double wmax[2][RHO_BLOCK / 32];
+  const int64_t e = (int64_t)blockIdx.x * RHO_BLOCK + threadIdx.x;
+  double r = 0.0, m = 0.0;
+  if (e < fr.size()) {
+    const double v = (double)acc[e] * (1.0 / 1099511627776.0);
+    const int64_t ex = fr.ex, ey = fr.ey;
+    const int i = (int)(e % ex) + fr.lo, j = (int)((e / ex) % ey) + fr.lo, k = (int)(e / (ex * ey)) + fr.lo;
+    if (i >= 0 && j >= 0 && k >= 0 && i <= nx && j <= ny && k <= nz) {
+      const double div = (aj[fj.at(0, i, j, k)] - aj[fj.at(0, i - 1, j, k)]) +
+                         (aj[fj.at(1, i, j, k)] - aj[fj.at(1, i, j - 1, k)]) +
+                         (aj[fj.at(2, i, j, k)] - aj[fj.at(2, i, j, k - 1)]);
+      r = fabs(v - (rho[e] - div * 2.0));
+      m = fabs(v);
+    }
+    rho[e] = v;
   }
-  rho[e] = v;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+    m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    wmax[0][warp] = r;
+    wmax[1][warp] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    double v = 0.0;
+    for (int w = 0; w < RHO_BLOCK / 32; w++) v = fmax(v, wmax[threadIdx.x][w]);
+    if (v > 0.0) max_nonneg(&res[threadIdx.x], v);
+  }
 }
 
 // One body's background charge: for every node of its bounding box (one

@@ -377,3 +377,32 @@ def read_esdat(path) -> dict:
     out["pbuf"] = p
     out["totalp"] = totalp
     return out
+
+
+def save(g, path, rens, fx: bool = True, rank: int = 0, nnode: int | None = 1) -> None:
+    """Writes the particles of the context g (with fx, the FP32 form's state
+    as FP64 records) with its background charge rhobk on the nodes 0..n and
+    the bodies' chgacm as esdat; rens = (renr, renv, renrho, renq) of the
+    run's units."""
+    cfg = g.cfg
+    if fx:
+        g.fx_store()
+    p, tp = g.download_particles()
+    rb = g.download_field("rhobk")[1:cfg.nz + 2, 1:cfg.ny + 2, 1:cfg.nx + 2, 0]
+    chg = g.get_counters().as_dict()["chgacm"][:cfg.npc, 0]
+    sd = [[0, cfg.nx], [0, cfg.ny], [0, cfg.nz]]
+    write_esdat(path, p, tp[:cfg.nspec], rens, sdoms=sd, rhobk=rb, chgacm=chg, nnode=nnode if rank == 0 else None)
+
+
+def load(g, path, fx: bool = True) -> dict:
+    """Starts the context g from an esdat file (inipcl's restart read): its
+    particles become g's, converted into the FP32 form when fx; returns the
+    file's datasets."""
+    d = read_esdat(path)
+    p = d["pbuf"].copy()
+    p["nid"] = 0
+    p["pid"] = 0
+    g.upload_particles(p, d["totalp"])
+    if fx:
+        g.fx_load()
+    return d

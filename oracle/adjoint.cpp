@@ -175,6 +175,17 @@ double wrap(double x, int n) {
 
 }  // namespace
 
+// The zigzag current q * J(b -> a) of one segment on the periodic grid, added
+// into J[nn][3] (node index i + nx*(j + ny*k)): b the start point, a the
+// unwrapped end point.  The checker uses it to follow a particle that FP32
+// rounding put on the other side of a cell face.
+extern "C" void orc_zigzag_one(const emsesg_config* c, int ustep, double q, const double* b, const double* a,
+                               double* J) {
+  const Grid G{{c->nx, c->ny, c->nz}};
+  const Seg ax[3] = {relay(b[0], a[0]), relay(b[1], a[1]), relay(b[2], a[2])};
+  zigzag(G, ax, b, a, q, 1.0 / ustep, J, nullptr, nullptr, nullptr);
+}
+
 extern "C" double orc_adjoint_ckpt(const emsesg_config* c, int K, int ckpt, int ustep, const double* enode,
                                    const double* bnode, const double* e0b0, emsesg_particle* p, int64_t np,
                                    const int* probe_lo, const int* probe_hi, double* gE, double* gB, double* g0,

@@ -114,6 +114,9 @@ void orc_blocks_destroy(orc_blocks* h);
 double orc_adjoint(const emsesg_config* c, int K, int ustep, const double* enode, const double* bnode,
                    const double* e0b0, emsesg_particle* p, int64_t np, const int* probe_lo,
                    const int* probe_hi, double* gE, double* gB, double* g0, double* gv);
+/* q * the zigzag current of one segment b -> a (a unwrapped) on the periodic
+ * grid, added into J[nn][3] (x fastest). */
+void orc_zigzag_one(const emsesg_config* c, int ustep, double q, const double* b, const double* a, double* J);
 /* The same with the state kept every ckpt steps (K a multiple of ckpt) and
  * each segment recomputed in the reverse sweep; same result. */
 double orc_adjoint_ckpt(const emsesg_config* c, int K, int ckpt, int ustep, const double* enode,

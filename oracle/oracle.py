@@ -84,6 +84,7 @@ def lib() -> ctypes.CDLL:
                                           _P, _P, _P, _P]),
         "orc_adjoint_ckpt": (ctypes.c_double, [cfgp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P,
                                                ctypes.c_int64, _P, _P, _P, _P, _P, _P]),
+        "orc_zigzag_one": (None, [cfgp, ctypes.c_int, ctypes.c_double, _P, _P, _P]),
         "orc_blocks_create": (_P, [cfgp, _P, _P, i64p, ctypes.c_int, ctypes.c_int]),
         "orc_blocks_threads": (ctypes.c_int, [_P]),
         "orc_blocks_particles": (ctypes.c_int64, [_P]),

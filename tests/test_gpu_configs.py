@@ -17,8 +17,12 @@
   continuity residual of the FP32 state checked.
 Tolerances: rho / J 1e-5 relative L2 (the FP32 form's stated bound) on the
 nodes 0..n (the guard layers of a periodic fold depend on which side of a
-periodic face a particle is stored; see oracle.compare.nodes); positions
-within 1e-6 cell; velocities within 1e-5 relative."""
+periodic face a particle is stored; see oracle.compare.nodes).  The 3-D
+zigzag current is discontinuous where an end point crosses a face, so J is
+compared with the oracle's current moved to the cells the FP32 form took
+for the particles that FP32 rounding put on the other side of a face (each
+listed; compare.j_error_corrected); the error before that move is printed.
+Positions within 1e-6 cell; velocities within 1e-5 relative."""
 import numpy as np
 import pytest
 
@@ -90,22 +94,25 @@ def fx_start(cfg, eb, p, tp):
     return g, p32, tp32
 
 
-def check_step(cfg, g, o, label):
+def check_step(cfg, g, o, start, label):
     """The FP32 form's state and fields after a step against the oracle's
     (same start): returns the error report, asserting the bounds."""
     g.fx_store()
     pg, tpg = g.download_particles()
     rep = C.particle_errors(cfg, pg, o.pbuf)
+    jg = g.download_field("aj")
     rep["rho"] = C.field_errors(g.download_field("rho"), o.f["rho"], cfg)
-    rep["aj"] = C.field_errors(g.download_field("aj"), o.f["aj"], cfg)
-    print(label, rep)
+    rep["aj"] = C.field_errors(jg, o.f["aj"], cfg)
+    raw, same = C.j_error_corrected(cfg, jg, o.f["aj"], start, pg, o.pbuf, rep["mismatched"])
+    rep["aj"]["l2_rel_same_cells"] = same
+    print(label, {k: v for k, v in rep.items() if k != "mismatched"})
     assert np.array_equal(tpg, o.totalp)
     assert rep["alive_mismatch"] == 0
     assert rep["cell_mismatch_off_band"] == 0, label
     assert rep["pos_max_abs"] < POS_TOL, label
     assert rep["vel_max_rel"] < VEL_TOL, label
     assert rep["rho"]["l2_rel"] < RHOJ_TOL, label
-    assert rep["aj"]["l2_rel"] < RHOJ_TOL, label
+    assert same < RHOJ_TOL, label
     return rep, pg
 
 
@@ -119,11 +126,21 @@ def test_config_32cube_fp32_form_ten_steps(gpu):
     for step in range(10):
         o = O.Oracle(cfg, cur, tp32, eb)  # re-seeded from the FP32 state
         oracle_step(o)
+        free_start = free.pbuf.copy()
         oracle_step(free)
         g.fx_step(2, False)
-        _, cur = check_step(cfg, g, o, f"32^3 step {step}")
+        _, after = check_step(cfg, g, o, cur, f"32^3 step {step}")
+        # the free-running oracle: its cells differ from the FP32 form's only
+        # next to faces, and J by the zigzag jumps of those particles
+        rf = C.particle_errors(cfg, after, free.pbuf)
+        assert rf["cell_mismatch_off_band"] == 0
         assert C.field_errors(g.download_field("rho"), free.f["rho"], cfg)["l2_rel"] < RHOJ_TOL
-        assert C.field_errors(g.download_field("aj"), free.f["aj"], cfg)["l2_rel"] < RHOJ_TOL
+        raw, same = C.j_error_corrected(cfg, g.download_field("aj"), free.f["aj"], free_start, after, free.pbuf,
+                                        rf["mismatched"])
+        print(f"free-running step {step}: J {raw:.2e} ({same:.2e} with the FP32 form's cells), cells differing "
+              f"{rf['cell_mismatch']}")
+        assert same < RHOJ_TOL
+        cur = after
     g.close()
 
 
@@ -146,7 +163,7 @@ def test_config_headline_physics_32cube_64ppc(gpu):
         rho_o_old = o.f["rho"].copy()
         oracle_step(o)
         g.fx_step(2, False)
-        rep, after = check_step(cfg, g, o, f"headline physics step {step}")
+        rep, after = check_step(cfg, g, o, cur, f"headline physics step {step}")
         # FP64 checks on the FP32 state: the kinetic energy of the FP32 form's
         # own particles, and against the oracle's FP64 particles
         eg = g.fx_energy()

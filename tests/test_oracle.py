@@ -246,3 +246,32 @@ def test_background_charge_from_surface_counts():
     assert np.array_equal(o.f["rho"][inner], rho0[inner] + o.f["rhobk"][inner])
     o.background(surf=surf, replace=True)
     assert np.array_equal(o.f["rho"][inner], o.f["rhobk"][inner])
+
+
+def test_zigzag_one_sums_to_psolve1():
+    """orc_zigzag_one (the checker's per-particle zigzag) summed over every
+    particle equals psolve1's folded current on the nodes 0..n-1 of a
+    periodic grid with no fields (so a = b + v ustep), many particles
+    crossing faces."""
+    case = small_case(n=(8, 6, 5), e=False, b0=(0.0, 0.0, 0.0))
+    case.species[0].vth *= 8
+    cfg = inputs.make_config(case)
+    p, tp = inputs.make_particles(case)
+    o = O.Oracle(cfg, p, tp, inputs.make_fields(case) * 0.0)
+    o.grdcrt()
+    o.f["aj"][...] = 0.0
+    o.psolve1(2, 0)
+    o.reduce_aj()
+    J = np.zeros((cfg.nx * cfg.ny * cfg.nz, 3))
+    L = O.lib()
+    for m in range(p.size):
+        b = np.array([p[f][m] for f in "xyz"])
+        a = b + 2.0 * np.array([p[f][m] for f in ("vx", "vy", "vz")])
+        L.orc_zigzag_one(ctypes.byref(cfg), 2, cfg.q[int(p["spec"][m]) - 1], b.ctypes.data, a.ctypes.data,
+                         J.ctypes.data)
+    got = J.reshape(cfg.nz, cfg.ny, cfg.nx, 3)
+    want = o.f["aj"][4:4 + cfg.nz, 4:4 + cfg.ny, 4:4 + cfg.nx]
+    crossing = np.any(np.floor(np.stack([p[f] for f in "xyz"], 1)) != np.floor(np.stack(
+        [p[f] + 2 * p[v] for f, v in zip("xyz", ("vx", "vy", "vz"))], 1)), 1)
+    assert crossing.sum() > 50
+    assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.norm(want)
