@@ -71,6 +71,77 @@ def particle_errors(cfg, pg, po, band: float = BAND) -> dict:
     return out
 
 
+def nodes(cfg, a):
+    """The nodes 0..n of every axis of a rho-layout (guard 1) or aj-layout
+    (guard 4) array, numpy shape (z, y, x[, c]): the field the reference's
+    solver and rhoupd use.  The guard layers are left out: after a periodic
+    fold they keep partial sums that depend on which side of a periodic face
+    a particle is stored, and a particle that ends within an FP32 ulp of that
+    face is stored on one side by the FP32 form and on the other by FP64."""
+    nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
+    lo = (a.shape[0] - nz - 1) // 2  # 1 for rho, 4 for aj
+    return a[lo:lo + nz + 1, lo:lo + ny + 1, lo:lo + nx + 1]
+
+
+def field_errors(g, o, cfg=None) -> dict:
+    """Relative L2 and max errors of a field, on the nodes 0..n when cfg is
+    given (see nodes), else over the whole array."""
+    if cfg is not None:
+        g, o = nodes(cfg, g), nodes(cfg, o)
+    return {"l2_rel": rel_l2(g, o), "max_rel": max_rel(g, o)}
+
+
+def tile_key(cfg, tile, p):
+    """Tile-major cell key and tile index of records p (tile: cells a side)."""
+    i, j, k = (np.floor(p[f]).astype(np.int64) % n for f, n in zip("xyz", (cfg.nx, cfg.ny, cfg.nz)))
+    nt = [-(-n // t) for n, t in zip((cfg.nx, cfg.ny, cfg.nz), tile)]
+    tid = i // tile[0] + nt[0] * (j // tile[1] + nt[1] * (k // tile[2]))
+    lin = i % tile[0] + tile[0] * (j % tile[1] + tile[1] * (k % tile[2]))
+    return tid * (tile[0] * tile[1] * tile[2]) + lin, tid
+
+
+def sort_order(cfg, tile, row_slots, before, after, keys=None):
+    """The permutation of one species' tile sort: `before` are its records
+    in the order of the previous sort (cells of that sort), `after` the same
+    particles moved by the steps since; returns the indices of the live
+    particles of `after` in sorted order.  `keys` overrides the cell keys of
+    `after` (e.g. the oracle's)."""
+    _, t0 = tile_key(cfg, tile, before)
+    ntile = int(t0.max()) + 1 if t0.size else 0
+    counts = np.bincount(t0, minlength=ntile)
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    q = np.arange(before.size) - starts[t0]
+    L = -(-counts[t0] // row_slots)
+    col, row = q // L, q % L
+    src = np.lexsort((col % 32, row, col // 32, t0))  # (tile, warp, row, lane)
+    order_pos = np.empty(before.size, dtype=np.int64)
+    order_pos[src] = np.arange(before.size)
+    live = after["nid"] != -1
+    key1 = tile_key(cfg, tile, after)[0] if keys is None else keys
+    idx = np.flatnonzero(live)
+    return idx[np.lexsort((order_pos[idx], key1[idx]))]
+
+
+def cell_histogram(cfg, p) -> np.ndarray:
+    c = _cells(cfg, p[p["nid"] != -1]) % np.array([cfg.nx, cfg.ny, cfg.nz])
+    lin = c[:, 0] + cfg.nx * (c[:, 1] + cfg.ny * c[:, 2])
+    return np.bincount(lin, minlength=cfg.nx * cfg.ny * cfg.nz)
+
+
+def continuity_residual(cfg, rho_old, rho_new, aj) -> float:
+    """max over the nodes 0..n of |rho_new - rho_old + 2 div J| (rhoupd.F90:
+    41-49), FP64; rho arrays of the rho layout (guard 1), aj of the aj layout
+    (guard 4), numpy shape (z, y, x[, c])."""
+    nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
+    r0 = rho_old.reshape(nz + 3, ny + 3, nx + 3)[1:nz + 2, 1:ny + 2, 1:nx + 2]
+    r1 = rho_new.reshape(nz + 3, ny + 3, nx + 3)[1:nz + 2, 1:ny + 2, 1:nx + 2]
+    j = aj.reshape(nz + 9, ny + 9, nx + 9, 3)
+    jx = j[4:nz + 5, 4:ny + 5, 4:nx + 5, 0] - j[4:nz + 5, 4:ny + 5, 3:nx + 4, 0]
+    jy = j[4:nz + 5, 4:ny + 5, 4:nx + 5, 1] - j[4:nz + 5, 3:ny + 4, 4:nx + 5, 1]
+    jz = j[4:nz + 5, 4:ny + 5, 4:nx + 5, 2] - j[3:nz + 4, 4:ny + 5, 4:nx + 5, 2]
+    return float(np.max(np.abs(r1 - (r0 - ((jx + jy) + jz) * 2.0))))
+
+
 def zigzag_correction(cfg, start, g_end, o_end, idx, ustep: int = 2) -> np.ndarray:
     """The current that particles `idx` deposit with the FP32 form's end
     point (g_end) minus the current with the oracle's (o_end), from the same
