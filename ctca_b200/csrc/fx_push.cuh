@@ -387,7 +387,9 @@ __device__ __forceinline__ void gather8_smem(const float4* f0, const float2* f1,
 
 // Trilinear gather of E and B at the particle (from the tile's shared nodes
 // when its cell lies in the box, gb >= 0, else from the global node field)
-// and the Buneman-Boris velocity update (psolve1.F90:186-272).
+// and the Buneman-Boris velocity update (psolve1.F90:186-272).  The shared
+// nodes hold the fields already multiplied by the species' qmp; the global
+// ones are multiplied here.
 template <int B>
 __device__ __forceinline__ void kick(const FxPushArgs& a, const float4* sf0, const float2* sf1, int gb, int ib, int jb,
                                      int kb, const float4& ps, float qmp, float& vx, float& vy, float& vz) {
@@ -403,9 +405,14 @@ __device__ __forceinline__ void kick(const FxPushArgs& a, const float4* sf0, con
   } else {
     const int64_t sy = a.g.nx + 1, sz = (int64_t)(a.g.nx + 1) * (a.g.ny + 1);
     gather8<false>(a.f0, a.f1, ib + sy * jb + sz * kb, sy, sz, wv, fe, fb);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      fe[d] *= qmp;
+      fb[d] *= qmp;
+    }
   }
-  const float eex = fe[0] * qmp, eey = fe[1] * qmp, eez = fe[2] * qmp;
-  const float bbx = fb[0] * qmp, bby = fb[1] * qmp, bbz = fb[2] * qmp;
+  const float eex = fe[0], eey = fe[1], eez = fe[2];
+  const float bbx = fb[0], bby = fb[1], bbz = fb[2];
   const float boris = __fdividef(2.0f, 1.0f + bbx * bbx + bby * bby + bbz * bbz);
   vx += eex; vy += eey; vz += eez;
   const float vxt = vx + vy * bbz - vz * bby;
@@ -688,6 +695,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   if (DEP)
     for (int e = tid; e < NBOX; e += PUSH_BLOCK) box[e] = 0ull;
   const int64_t sy = g.nx + 1, sz = (int64_t)(g.nx + 1) * (g.ny + 1);
+  const float sq = a.qmp[is];  // the tile's fields times the species' qmp
   for (int e = tid; e < NF; e += PUSH_BLOCK) {
     int li = e % B, lj = (e / B) % B, lk = e / (B * B);
     int gi = o[0] + li, gj = o[1] + lj, gk = o[2] + lk;
@@ -697,8 +705,8 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       p = __ldg(&a.f0[gn]);
       q = __ldg(&a.f1[gn]);
     }
-    sf0[e] = p;
-    sf1[e] = make_float2(q.x, q.y);
+    sf0[e] = make_float4(p.x * sq, p.y * sq, p.z * sq, p.w * sq);
+    sf1[e] = make_float2(q.x * sq, q.y * sq);
   }
   __syncthreads();
 
@@ -751,13 +759,15 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
 
   int r = 0;
   for (;;) {
+  // the stage of row r and the parity of its use, kept as running counters
+  int s = r % NSTAGE;
+  uint32_t ph = (uint32_t)((r / NSTAGE) & 1);
   for (; r < L && !failed; r++) {
-    const int s = r % NSTAGE;
+    const int s1 = s + 1 == NSTAGE ? 0 : s + 1;
+    const uint32_t par1 = s1 == 0 ? ph ^ 1u : ph;
     uint32_t nextcell = DEAD;
     bool oknext = false;
     if (r + 1 < L) {
-      const int s1 = (r + 1) % NSTAGE;
-      const uint32_t par1 = (uint32_t)(((r + 1) / NSTAGE) & 1);
       oknext = mbar_wait(&full_bar[s1], par1);
       if (!__any_sync(0xffffffffu, oknext)) {
         failed = true;
@@ -805,9 +815,10 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
         }
       }
     }
+    // a new run starts from zero: folded into this particle's accumulate
+    // below, or (rarely: the particle itself leaves the run's cell) cleared
+    const float keep = newrun ? 0.f : 1.f;
     if (newrun) {
-#pragma unroll
-      for (int q = 0; q < NJ + NR; q++) acc[q] = 0.f;
       runcell = cell;
       runbase = box_base<B>(o, ib, jb, kb);
     }
@@ -859,8 +870,12 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
         oen[NJ + NR] = __int_as_float(gb);
       } else {
 #pragma unroll
-        for (int q = 0; q < NJ + NR; q++) acc[q] += cv[q];
+        for (int q = 0; q < NJ + NR; q++) acc[q] = fmaf(acc[q], keep, cv[q]);
       }
+    }
+    if (newrun && !simple) {
+#pragma unroll
+      for (int q = 0; q < NJ + NR; q++) acc[q] = 0.f;
     }
     // the new velocity of every particle (a cell-crossing one keeps its old
     // position until the general path writes the whole record)
@@ -898,6 +913,8 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
         break;
       }
     }
+    s = s1;
+    ph = par1;
   }
   if (xqn) {
     nesc += cross_list<B, DEP>(a, is, slot0, box, o, xl, xqn, lane);
