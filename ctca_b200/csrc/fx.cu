@@ -1360,6 +1360,7 @@ struct emsesg::AdjWork {
   std::vector<FxSnap> ck, seg;     // checkpoints; the states of one segment
   std::vector<uint32_t*> inv;      // sort maps of one segment
   float *lam = nullptr, *lam2 = nullptr, *gd = nullptr;
+  uint32_t* fwd = nullptr;  // a sort's old slot -> new slot
   double *gEd = nullptr, *gBd = nullptr;  // node-field gradients, FP64 sums
   float* jx = nullptr;             // probe Jx of each step
   int jx_steps = 0;
@@ -1370,7 +1371,7 @@ struct emsesg::AdjWork {
     for (auto& sn : ck) snap_free(sn);
     for (auto& sn : seg) snap_free(sn);
     for (auto* q : inv) cudaFree(q);
-    cudaFree(lam); cudaFree(lam2); cudaFree(gd); cudaFree(gEd); cudaFree(gBd); cudaFree(jx);
+    cudaFree(lam); cudaFree(lam2); cudaFree(fwd); cudaFree(gd); cudaFree(gEd); cudaFree(gBd); cudaFree(jx);
     cudaFree(lossd); cudaFree(gvd);
     *this = AdjWork();
   }
@@ -1402,6 +1403,7 @@ int adj_reserve(emsesg_ctx* ctx, AdjWork& w, int nseg, int ckpt, int jsteps, int
   if ((int)w.inv.size() < ckpt) w.inv.resize((size_t)ckpt, nullptr);
   if (!w.lam) EMSESG_CUDA(ctx, cudaMalloc(&w.lam, 6 * cap * sizeof(float)));
   if (!w.lam2) EMSESG_CUDA(ctx, cudaMalloc(&w.lam2, 6 * cap * sizeof(float)));
+  if (!w.fwd) EMSESG_CUDA(ctx, cudaMalloc(&w.fwd, cap * sizeof(uint32_t)));
   if (!w.gd) EMSESG_CUDA(ctx, cudaMalloc(&w.gd, 3 * nn * sizeof(float)));
   if (!w.gEd) EMSESG_CUDA(ctx, cudaMalloc(&w.gEd, 3 * nn * sizeof(double)));
   if (!w.gBd) EMSESG_CUDA(ctx, cudaMalloc(&w.gBd, 3 * nn * sizeof(double)));
@@ -1583,24 +1585,26 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
       }
     }
     for (int j = ckpt - 1; j >= 0; j--) {
-      if (j < 64 && sorted[j]) {
-        // lambda of S_{n+1} (sorted layout) back to the layout of S_n
-        EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(lam2, 0, 6 * cap * sizeof(float), ctx->stream), "lambda"));
+      // lambda of S_{n+1}: in place, or across a re-sort after step n read
+      // through the sort's forward map and written in the layout of S_n
+      const bool across = j < 64 && sorted[j];
+      float* lsrc = lx;
+      if (across) {
         for (int is = 0; is < c.nspec; is++) {
           const int64_t off = f.base[is];
-          EMSESG_LAUNCH(ctx, "adj_unsort", k_adj_unsort, nblk(f.cap[is]), 256, 0, inv[(size_t)j] + off, f.cap[is],
-                        lx + off, lx + cap + off, lx + 2 * cap + off, lx + 3 * cap + off, lx + 4 * cap + off,
-                        lx + 5 * cap + off, lam2 + off, lam2 + cap + off, lam2 + 2 * cap + off, lam2 + 3 * cap + off,
-                        lam2 + 4 * cap + off, lam2 + 5 * cap + off);
+          EMSESG_LAUNCH(ctx, "adj_fwd", k_adj_fwd, nblk(f.cap[is]), 256, 0, inv[(size_t)j] + off, f.cap[is],
+                        w.fwd + off);
         }
-        std::swap(lam, lam2);
-        lx = lam;
+        lx = lam2;
       }
       EMSESG_LAUNCH(ctx, "adj_g", k_adj_g, nblk(nn), 256, 0, jx + (int64_t)(sgi * ckpt + j) * nn, nn, gd);
       const FxSnap& sn = seg[(size_t)j];
       a.pos = sn.pos; a.vx = sn.vx; a.vy = sn.vy; a.vz = sn.vz;
       a.tile_start = sn.ts; a.tile_pad = sn.tp;
       a.lx = lx; a.ly = lx + cap; a.lz = lx + 2 * cap; a.lvx = lx + 3 * cap; a.lvy = lx + 4 * cap; a.lvz = lx + 5 * cap;
+      a.slx = lsrc; a.sly = lsrc + cap; a.slz = lsrc + 2 * cap;
+      a.slvx = lsrc + 3 * cap; a.slvy = lsrc + 4 * cap; a.slvz = lsrc + 5 * cap;
+      a.fwd = across ? w.fwd : nullptr;
       if (fx_box_tile(tmax) == 4) {
         EMSESG_ADJ(check_cuda(ctx, cudaFuncSetAttribute(k_fx_adjoint<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                         asmem), "adjoint smem"));
@@ -1609,6 +1613,10 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
         EMSESG_ADJ(check_cuda(ctx, cudaFuncSetAttribute(k_fx_adjoint<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                         asmem), "adjoint smem"));
         EMSESG_LAUNCH(ctx, "fx_adjoint", k_fx_adjoint<8>, grid, ADJ_THREADS, asmem, a);
+      }
+      if (across) {  // lambda_n went to lam2: it is the current lambda now
+        std::swap(lam, lam2);
+        lx = lam;
       }
     }
   }

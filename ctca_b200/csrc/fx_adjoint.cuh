@@ -26,12 +26,22 @@ struct AdjArgs {
   const float* vx;
   const float* vy;
   const float* vz;
-  float* lx;                    // adjoint of the position (x, y, z)
+  float* lx;                    // adjoint of the position (x, y, z), written
   float* ly;
   float* lz;
-  float* lvx;                   // adjoint of the velocity
+  float* lvx;                   // adjoint of the velocity, written
   float* lvy;
   float* lvz;
+  // lambda of the next state, read: the arrays above (in place) or, across
+  // a re-sort, the next state's arrays at slot off + fwd[slot - off] (fwd:
+  // the sort's old slot -> new slot, per species region)
+  const float* slx;
+  const float* sly;
+  const float* slz;
+  const float* slvx;
+  const float* slvy;
+  const float* slvz;
+  const uint32_t* fwd;
   const int64_t* tile_start;
   const int64_t* tile_pad;
   int64_t off[EMSESG_ISPEC];
@@ -263,8 +273,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
                      (unsigned)(ca[2] - o[2]) < (unsigned)(B - 1);
     if (anyg || !inb || !ina) zigzag_adj<B>(bx, cb, ca, bl, al, qq, rustep, dSda, dSdb);
     // move: a = b + vnew * ustep
-    const float3 la = f3(a.lx[m] + dSda[0], a.ly[m] + dSda[1], a.lz[m] + dSda[2]);
-    const float3 lvn = add3(f3(a.lvx[m], a.lvy[m], a.lvz[m]), mul3(us, la));
+    const int64_t mn = a.fwd ? a.off[is] + (int64_t)a.fwd[m] : m;  // the slot of the next state
+    const float3 la = f3(a.slx[mn] + dSda[0], a.sly[mn] + dSda[1], a.slz[mn] + dSda[2]);
+    const float3 lvn = add3(f3(a.slvx[mn], a.slvy[mn], a.slvz[mn]), mul3(us, la));
     float3 lb = add3(f3(dSdb[0], dSdb[1], dSdb[2]), la);
     // Boris, reversed
     float3 le = lvn;
@@ -341,19 +352,15 @@ inline int fx_adjoint_smem(int tmax) {
   return nf * (int)(2 * sizeof(float4) + 6 * sizeof(double) + 3 * sizeof(float));
 }
 
-// lambda through a sort: the adjoint of S_{n+1} (new layout) back to the
-// layout before the sort (inv[new slot] = old slot).
-__global__ void k_adj_unsort(const uint32_t* __restrict__ inv, int64_t n, const float* __restrict__ src0,
-                             const float* __restrict__ src1, const float* __restrict__ src2,
-                             const float* __restrict__ src3, const float* __restrict__ src4,
-                             const float* __restrict__ src5, float* d0, float* d1, float* d2, float* d3, float* d4,
-                             float* d5) {
+// The forward map of a sort from its inverse (inv[new slot] = old slot,
+// region-relative, DEAD for empty slots): fwd[old slot] = new slot, so that
+// the reverse step of S_n (old layout) reads the lambda of S_{n+1} (new
+// layout) in place of a separate unsort of lambda.
+__global__ void k_adj_fwd(const uint32_t* __restrict__ inv, int64_t n, uint32_t* fwd) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n) return;
   const uint32_t s = inv[m];
-  if (s == DEAD) return;
-  d0[s] = src0[m]; d1[s] = src1[m]; d2[s] = src2[m];
-  d3[s] = src3[m]; d4[s] = src4[m]; d5[s] = src5[m];
+  if (s != DEAD) fwd[s] = (uint32_t)m;
 }
 
 __device__ __forceinline__ bool in_probe(const Geo& G, int64_t un, int3 lo, int3 hi, int& i, int& j, int& k) {

@@ -479,15 +479,23 @@ class Emses:
         self._check(self.lib.emsesg_fx_continuity(self.h, r))
         return float(r[0]), float(r[1])
 
-    def fx_adjoint(self, K: int, ustep: int, ckpt: int, sort_every: int, probe_lo, probe_hi, nparticles: int):
+    def fx_adjoint(self, K: int, ustep: int, ckpt: int, sort_every: int, probe_lo, probe_hi, nparticles: int,
+                   gv_out: np.ndarray | None = None):
         """Loss sum_steps sum_probe aj_x^2 over K steps and its gradients:
         returns (loss, gE, gB, g0, gv) with node gradients [n^3, 3] and gv
-        [nparticles, 3] in emsesg_fx_store order."""
+        [nparticles, 3] in emsesg_fx_store order.  gv_out: a float64
+        [nparticles, 3] buffer for gv (e.g. pinned host memory, so that its
+        copy from the device runs at full speed)."""
         nn = self.cfg.nx * self.cfg.ny * self.cfg.nz
         gE = np.zeros((nn, 3))
         gB = np.zeros((nn, 3))
         g0 = np.zeros(6)
-        gv = np.zeros((nparticles, 3))
+        if gv_out is not None:
+            if gv_out.dtype != np.float64 or gv_out.shape != (nparticles, 3) or not gv_out.flags.c_contiguous:
+                raise ValueError("gv_out must be a C-contiguous float64 array of shape (nparticles, 3)")
+            gv = gv_out
+        else:
+            gv = np.zeros((nparticles, 3))
         loss = ctypes.c_double(0.0)
         lo = (ctypes.c_int32 * 3)(*probe_lo)
         hi = (ctypes.c_int32 * 3)(*probe_hi)
