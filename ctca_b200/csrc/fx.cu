@@ -1359,6 +1359,11 @@ struct emsesg::AdjWork {
   int64_t cap = 0, nl = 0, nn = 0;
   std::vector<FxSnap> ck, seg;     // checkpoints; the states of one segment
   std::vector<uint32_t*> inv;      // sort maps of one segment
+  // the map of every sort of the forward pass, with the tile starts, tile
+  // pads and counts after it (when they fit in memory): the recompute of a
+  // segment applies them instead of sorting again
+  std::vector<uint32_t*> maps;
+  std::vector<int64_t*> meta;
   float *lam = nullptr, *lam2 = nullptr, *gd = nullptr;
   uint32_t* fwd = nullptr;  // a sort's old slot -> new slot
   double *gEd = nullptr, *gBd = nullptr;  // node-field gradients, FP64 sums
@@ -1371,6 +1376,8 @@ struct emsesg::AdjWork {
     for (auto& sn : ck) snap_free(sn);
     for (auto& sn : seg) snap_free(sn);
     for (auto* q : inv) cudaFree(q);
+    for (auto* q : maps) cudaFree(q);
+    for (auto* q : meta) cudaFree(q);
     cudaFree(lam); cudaFree(lam2); cudaFree(fwd); cudaFree(gd); cudaFree(gEd); cudaFree(gBd); cudaFree(jx);
     cudaFree(lossd); cudaFree(gvd);
     *this = AdjWork();
@@ -1415,6 +1422,37 @@ int adj_reserve(emsesg_ctx* ctx, AdjWork& w, int nseg, int ckpt, int jsteps, int
     EMSESG_CUDA(ctx, cudaMalloc(&w.jx, (size_t)jsteps * nn * sizeof(float)));
     w.jx_steps = jsteps;
   }
+  return EMSESG_OK;
+}
+
+// Room for the maps of nsort sorts: taken when what is still to allocate
+// is at most half of the free device memory (*keep), else the recompute
+// sorts again.
+int adj_reserve_maps(emsesg_ctx* ctx, AdjWork& w, int nsort, int64_t cap, int64_t nl, bool* keep) {
+  *keep = false;
+  const size_t mb = (size_t)cap * sizeof(uint32_t);
+  const size_t tb = (size_t)(2 * nl + 2 * EMSESG_ISPEC) * sizeof(int64_t);
+  const int have = (int)w.maps.size();
+  if (have < nsort) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+      return EMSESG_OK;
+    }
+    if ((size_t)(nsort - have) * (mb + tb) > fr / 2) return EMSESG_OK;
+  }
+  while ((int)w.maps.size() < nsort) {
+    uint32_t* m = nullptr;
+    int64_t* t = nullptr;
+    EMSESG_CUDA(ctx, cudaMalloc(&m, mb));
+    if (cudaMalloc(&t, tb) != cudaSuccess) {
+      cudaFree(m);
+      return check_cuda(ctx, cudaGetLastError(), "adjoint sort maps");
+    }
+    w.maps.push_back(m);
+    w.meta.push_back(t);
+  }
+  *keep = true;
   return EMSESG_OK;
 }
 
@@ -1524,13 +1562,42 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
   double* const gEd = w.gEd;
   double* const gBd = w.gBd;
   double* const lossd = w.lossd;
+  bool keep_maps = false;
+  rc = adj_reserve_maps(ctx, w, K / sort_every, cap, nl, &keep_maps);
+  if (rc) return rc;
   ArrayOwners owners(f, seg);
+  // the sort writes its map where f.lcs_inv points: a kept map for the
+  // sorts of the forward pass, the context's own buffer again on every way out
+  struct InvOwner {
+    uint32_t*& p;
+    uint32_t* const own;
+    ~InvOwner() { p = own; }
+  } inv_owner{f.lcs_inv, f.lcs_inv};
 #define EMSESG_ADJ(call) do { rc = (call); if (rc) return rc; } while (0)
   EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(lossd, 0, sizeof(double), ctx->stream), "adjoint loss"));
   // forward: K steps with a checkpoint every ckpt steps, the loss on the way
   for (int n = 0; n < K; n++) {
     if (n % ckpt == 0) EMSESG_ADJ(snap_copy(ctx, true, ck[(size_t)(n / ckpt)], cap, nl));
-    EMSESG_ADJ(emsesg_fx_step(ctx, ustep, (n + 1) % sort_every == 0 ? 1 : 0));
+    const bool srt = (n + 1) % sort_every == 0;
+    const int ks = (n + 1) / sort_every - 1;
+    if (srt && keep_maps) {
+      // slots past the new regions keep no map
+      EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(w.maps[(size_t)ks], 0xFF, cap * sizeof(uint32_t), ctx->stream),
+                            "adjoint sort map"));
+      f.lcs_inv = w.maps[(size_t)ks];
+    }
+    rc = emsesg_fx_step(ctx, ustep, srt ? 1 : 0);
+    f.lcs_inv = inv_owner.own;
+    if (rc) return rc;
+    if (srt && keep_maps) {
+      int64_t* t = w.meta[(size_t)ks];
+      const cudaMemcpyKind dd = cudaMemcpyDeviceToDevice;
+      EMSESG_CUDA(ctx, cudaMemcpyAsync(t, f.tile_start, nl * sizeof(int64_t), dd, ctx->stream));
+      EMSESG_CUDA(ctx, cudaMemcpyAsync(t + nl, f.tile_pad, nl * sizeof(int64_t), dd, ctx->stream));
+      EMSESG_CUDA(ctx, cudaMemcpyAsync(t + 2 * nl, f.count_d, EMSESG_ISPEC * sizeof(int64_t), dd, ctx->stream));
+      EMSESG_CUDA(ctx, cudaMemcpyAsync(t + 2 * nl + EMSESG_ISPEC, f.slots_d, EMSESG_ISPEC * sizeof(int64_t), dd,
+                                       ctx->stream));
+    }
     EMSESG_LAUNCH(ctx, "adj_probe", k_adj_probe, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_AJ], fj, g, lo, hi,
                   lossd, jx + (int64_t)n * nn);
   }
@@ -1560,6 +1627,7 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
   for (int sgi = nseg - 1; sgi >= 0; sgi--) {
     EMSESG_ADJ(snap_copy(ctx, false, ck[(size_t)sgi], cap, nl));
     bool sorted[64] = {false};
+    uint32_t* smap[64] = {nullptr};  // the map of the sort after step j
     for (int j = 0; j < ckpt; j++) {
       const int n = sgi * ckpt + j;
       // the state before step n is kept in seg[j]: its particle arrays take
@@ -1571,17 +1639,48 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
       std::swap(f.vx, sj.vx);
       std::swap(f.vy, sj.vy);
       std::swap(f.vz, sj.vz);
-      f.move_src = FxSrc{sj.pos, sj.vx, sj.vy, sj.vz};
       const bool srt = (n + 1) % sort_every == 0;
+      const int ks = (n + 1) / sort_every - 1;
+      const bool apply = srt && keep_maps;
+      if (apply) {
+        sorted[j] = true;
+        smap[j] = w.maps[(size_t)ks];
+      }
+      // the state after the segment is not needed (only the map of a sort
+      // after its last step, which is kept or made below)
+      if (j == ckpt - 1 && (!srt || apply)) break;
+      f.move_src = FxSrc{sj.pos, sj.vx, sj.vy, sj.vz};
       // slots past the new regions keep no map from an earlier sort
-      if (srt) EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(f.lcs_inv, 0xFF, cap * sizeof(uint32_t), ctx->stream), "inv"));
-      EMSESG_ADJ(fx_step_impl(ctx, ustep, srt ? 1 : 0, false));
+      if (srt && !apply)
+        EMSESG_ADJ(check_cuda(ctx, cudaMemsetAsync(f.lcs_inv, 0xFF, cap * sizeof(uint32_t), ctx->stream), "inv"));
+      EMSESG_ADJ(fx_step_impl(ctx, ustep, srt && !apply ? 1 : 0, false));
       f.move_src = FxSrc{};
-      if (srt && j < 64) {
+      if (apply) {
+        // the forward pass's sort again: gathered through its map, then its
+        // tile starts, pads and counts
+        for (int is = 0; is < c.nspec; is++) {
+          const int64_t off = f.base[is];
+          EMSESG_LAUNCH(ctx, "adj_apply", k_adj_apply, nblk(f.cap[is]), 256, 0, smap[j] + off, f.cap[is],
+                        f.pos + off, f.vx + off, f.vy + off, f.vz + off, f.pos2 + off, f.vx2 + off, f.vy2 + off,
+                        f.vz2 + off);
+        }
+        std::swap(f.pos, f.pos2);
+        std::swap(f.vx, f.vx2);
+        std::swap(f.vy, f.vy2);
+        std::swap(f.vz, f.vz2);
+        const int64_t* t = w.meta[(size_t)ks];
+        const cudaMemcpyKind dd = cudaMemcpyDeviceToDevice;
+        EMSESG_CUDA(ctx, cudaMemcpyAsync(f.tile_start, t, nl * sizeof(int64_t), dd, ctx->stream));
+        EMSESG_CUDA(ctx, cudaMemcpyAsync(f.tile_pad, t + nl, nl * sizeof(int64_t), dd, ctx->stream));
+        EMSESG_CUDA(ctx, cudaMemcpyAsync(f.count_d, t + 2 * nl, EMSESG_ISPEC * sizeof(int64_t), dd, ctx->stream));
+        EMSESG_CUDA(ctx, cudaMemcpyAsync(f.slots_d, t + 2 * nl + EMSESG_ISPEC, EMSESG_ISPEC * sizeof(int64_t), dd,
+                                         ctx->stream));
+      } else if (srt && j < 64) {
         if (!inv[(size_t)j]) EMSESG_ADJ(check_cuda(ctx, cudaMalloc(&inv[(size_t)j], cap * sizeof(uint32_t)), "inv"));
         EMSESG_ADJ(check_cuda(ctx, cudaMemcpyAsync(inv[(size_t)j], f.lcs_inv, cap * sizeof(uint32_t),
                                                    cudaMemcpyDeviceToDevice, ctx->stream), "inv"));
         sorted[j] = true;
+        smap[j] = inv[(size_t)j];
       }
     }
     for (int j = ckpt - 1; j >= 0; j--) {
@@ -1592,7 +1691,7 @@ extern "C" int emsesg_fx_adjoint(emsesg_ctx* ctx, int K, int ustep, int ckpt, in
       if (across) {
         for (int is = 0; is < c.nspec; is++) {
           const int64_t off = f.base[is];
-          EMSESG_LAUNCH(ctx, "adj_fwd", k_adj_fwd, nblk(f.cap[is]), 256, 0, inv[(size_t)j] + off, f.cap[is],
+          EMSESG_LAUNCH(ctx, "adj_fwd", k_adj_fwd, nblk(f.cap[is]), 256, 0, smap[j] + off, f.cap[is],
                         w.fwd + off);
         }
         lx = lam2;

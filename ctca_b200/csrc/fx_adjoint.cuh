@@ -222,36 +222,47 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
     const float4 ps = a.pos[m];
     const uint32_t cell = (uint32_t)__float_as_int(ps.w);
     if (cell == DEAD) continue;
+    // lambda of the next state, loaded first: its latency hides behind the
+    // recompute
+    const int64_t mn = a.fwd ? a.off[is] + (int64_t)a.fwd[m] : m;  // the slot of the next state
+    const float lnx = a.slx[mn], lny = a.sly[mn], lnz = a.slz[mn];
+    const float lnvx = a.slvx[mn], lnvy = a.slvy[mn], lnvz = a.slvz[mn];
     int cb[3];
     unpack(G, cell, cb[0], cb[1], cb[2]);
     const float bl[3] = {ps.x, ps.y, ps.z};
     const float3 v0 = f3(a.vx[m], a.vy[m], a.vz[m]);
-    // forward recompute: gather (corner c = di + 2 dj + 4 dk)
-    float3 E = f3(0.f, 0.f, 0.f), Bf = E;
     const int li = cb[0] - o[0], lj = cb[1] - o[1], lk = cb[2] - o[2];
     const bool inb = (unsigned)li < (unsigned)(B - 1) && (unsigned)lj < (unsigned)(B - 1) && (unsigned)lk < (unsigned)(B - 1);
-    // corner c's node fields (read again by the reversed gather)
-    auto corner = [&](int c, float4& cp, float4& cq) {
-      const int di = c & 1, dj = (c >> 1) & 1, dk = c >> 2;
-      if (inb) {
-        const int e = ((lk + dk) * B + (lj + dj)) * B + (li + di);
-        cp = sf0[e];
-        cq = sf1[e];
-      } else {
-        const int64_t gn = (cb[0] + di) + sy * (cb[1] + dj) + sz * (cb[2] + dk);
-        cp = __ldg(&a.f0[gn]);
-        cq = __ldg(&a.f1[gn]);
-      }
-    };
+    const int e0 = (lk * B + lj) * B + li;  // box index of corner 0 (in the box)
+    // trilinear weights, corner c = di + 2 dj + 4 dk
+    float wc[8];
 #pragma unroll
     for (int c = 0; c < 8; c++) {
       const int di = c & 1, dj = (c >> 1) & 1, dk = c >> 2;
-      float4 cp, cq;
-      corner(c, cp, cq);
       const float X = di ? bl[0] : 1.0f - bl[0], Y = dj ? bl[1] : 1.0f - bl[1], Z = dk ? bl[2] : 1.0f - bl[2];
-      const float w = X * Y * Z;
-      E = add3(E, mul3(w, f3(cp.x, cp.y, cp.z)));
-      Bf = add3(Bf, mul3(w, f3(cp.w, cq.x, cq.y)));
+      wc[c] = X * Y * Z;
+    }
+    // forward recompute: gather
+    float3 E = f3(0.f, 0.f, 0.f), Bf = E;
+    if (inb) {
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        const int e = e0 + (c >> 2) * B * B + ((c >> 1) & 1) * B + (c & 1);
+        const float4 cp = sf0[e], cq = sf1[e];
+        E = add3(E, mul3(wc[c], f3(cp.x, cp.y, cp.z)));
+        Bf = add3(Bf, mul3(wc[c], f3(cp.w, cq.x, cq.y)));
+      }
+    } else {
+#pragma unroll 1
+      for (int c = 0; c < 8; c++) {
+        const int di = c & 1, dj = (c >> 1) & 1, dk = c >> 2;
+        const float X = di ? bl[0] : 1.0f - bl[0], Y = dj ? bl[1] : 1.0f - bl[1], Z = dk ? bl[2] : 1.0f - bl[2];
+        const float w = X * Y * Z;
+        const int64_t gn = (cb[0] + di) + sy * (cb[1] + dj) + sz * (cb[2] + dk);
+        const float4 cp = __ldg(&a.f0[gn]), cq = __ldg(&a.f1[gn]);
+        E = add3(E, mul3(w, f3(cp.x, cp.y, cp.z)));
+        Bf = add3(Bf, mul3(w, f3(cp.w, cq.x, cq.y)));
+      }
     }
     const float3 ee = mul3(qmp, E), tt = mul3(qmp, Bf);
     const float sfac = 2.0f / (1.0f + dot3(tt, tt));
@@ -273,9 +284,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
                      (unsigned)(ca[2] - o[2]) < (unsigned)(B - 1);
     if (anyg || !inb || !ina) zigzag_adj<B>(bx, cb, ca, bl, al, qq, rustep, dSda, dSdb);
     // move: a = b + vnew * ustep
-    const int64_t mn = a.fwd ? a.off[is] + (int64_t)a.fwd[m] : m;  // the slot of the next state
-    const float3 la = f3(a.slx[mn] + dSda[0], a.sly[mn] + dSda[1], a.slz[mn] + dSda[2]);
-    const float3 lvn = add3(f3(a.slvx[mn], a.slvy[mn], a.slvz[mn]), mul3(us, la));
+    const float3 la = f3(lnx + dSda[0], lny + dSda[1], lnz + dSda[2]);
+    const float3 lvn = add3(f3(lnvx, lnvy, lnvz), mul3(us, la));
     float3 lb = add3(f3(dSdb[0], dSdb[1], dSdb[2]), la);
     // Boris, reversed
     float3 le = lvn;
@@ -290,29 +300,53 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) k_fx_adjoint(AdjArgs a) {
     lt = add3(lt, mul3(-ls * sfac * sfac, tt));
     le = add3(le, lu);
     const float3 lE = mul3(qmp, le), lB = mul3(qmp, lt);
+    // gather, reversed: the node-field gradients w_c lambda, and to lambda_b
+    // the gradient of sum_c w_c s_c, s_c = (E_c, B_c) . (lambda_E, lambda_B)
     if (inb) {
-      const int base = (lk * B + lj) * B + li;
-      if (base != runbase) {
+      if (e0 != runbase) {
         flush();
-        runbase = base;
+        runbase = e0;
       }
-    }
-    // gather, reversed
+      float sc[8];
 #pragma unroll
-    for (int c = 0; c < 8; c++) {
-      const int di = c & 1, dj = (c >> 1) & 1, dk = c >> 2;
-      const float X = di ? bl[0] : 1.0f - bl[0], Y = dj ? bl[1] : 1.0f - bl[1], Z = dk ? bl[2] : 1.0f - bl[2];
-      const float dX = di ? 1.0f : -1.0f, dY = dj ? 1.0f : -1.0f, dZ = dk ? 1.0f : -1.0f;
-      const float w = X * Y * Z;
-      float4 cp, cq;
-      corner(c, cp, cq);
-      const float sdot = cp.x * lE.x + cp.y * lE.y + cp.z * lE.z + cp.w * lB.x + cq.x * lB.y + cq.y * lB.z;
-      lb = add3(lb, mul3(sdot, f3(dX * Y * Z, X * dY * Z, X * Y * dZ)));
-      const float gv[6] = {w * lE.x, w * lE.y, w * lE.z, w * lB.x, w * lB.y, w * lB.z};
-      if (inb) {
+      for (int c = 0; c < 8; c++) {
+        const int e = e0 + (c >> 2) * B * B + ((c >> 1) & 1) * B + (c & 1);
+        const float4 cp = sf0[e], cq = sf1[e];
+        sc[c] = cp.x * lE.x + cp.y * lE.y + cp.z * lE.z + cp.w * lB.x + cq.x * lB.y + cq.y * lB.z;
+        const float gv[6] = {lE.x, lE.y, lE.z, lB.x, lB.y, lB.z};
 #pragma unroll
-        for (int q = 0; q < 6; q++) pacc[6 * c + q] += gv[q];
-      } else {
+        for (int q = 0; q < 6; q++) pacc[6 * c + q] = fmaf(wc[c], gv[q], pacc[6 * c + q]);
+      }
+      // trilinear interpolation of sc in x, then y, then z, with the
+      // derivatives carried along
+      float dx[4], ax[4];
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        dx[h] = sc[2 * h + 1] - sc[2 * h];
+        ax[h] = fmaf(bl[0], dx[h], sc[2 * h]);
+      }
+      float ey[2], cy[2], bxy[2];
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        ey[k] = ax[2 * k + 1] - ax[2 * k];
+        cy[k] = fmaf(bl[1], ey[k], ax[2 * k]);
+        bxy[k] = fmaf(bl[1], dx[2 * k + 1] - dx[2 * k], dx[2 * k]);
+      }
+      lb.x += fmaf(bl[2], bxy[1] - bxy[0], bxy[0]);
+      lb.y += fmaf(bl[2], ey[1] - ey[0], ey[0]);
+      lb.z += cy[1] - cy[0];
+    } else {
+#pragma unroll 1
+      for (int c = 0; c < 8; c++) {
+        const int di = c & 1, dj = (c >> 1) & 1, dk = c >> 2;
+        const float X = di ? bl[0] : 1.0f - bl[0], Y = dj ? bl[1] : 1.0f - bl[1], Z = dk ? bl[2] : 1.0f - bl[2];
+        const float dX = di ? 1.0f : -1.0f, dY = dj ? 1.0f : -1.0f, dZ = dk ? 1.0f : -1.0f;
+        const float w = X * Y * Z;
+        const int64_t gn = (cb[0] + di) + sy * (cb[1] + dj) + sz * (cb[2] + dk);
+        const float4 cp = __ldg(&a.f0[gn]), cq = __ldg(&a.f1[gn]);
+        const float sdot = cp.x * lE.x + cp.y * lE.y + cp.z * lE.z + cp.w * lB.x + cq.x * lB.y + cq.y * lB.z;
+        lb = add3(lb, mul3(sdot, f3(dX * Y * Z, X * dY * Z, X * Y * dZ)));
+        const float gv[6] = {w * lE.x, w * lE.y, w * lE.z, w * lB.x, w * lB.y, w * lB.z};
         const int64_t un = unique_node(G, cb[0] + di, cb[1] + dj, cb[2] + dk);
 #pragma unroll
         for (int q = 0; q < 3; q++) {
@@ -361,6 +395,31 @@ __global__ void k_adj_fwd(const uint32_t* __restrict__ inv, int64_t n, uint32_t*
   if (m >= n) return;
   const uint32_t s = inv[m];
   if (s != DEAD) fwd[s] = (uint32_t)m;
+}
+
+// A sort of the forward pass applied again from its kept map (inv[new slot]
+// = old slot, region-relative, DEAD for an empty slot): the records of the
+// new layout gathered from the old one, empty slots as the sort leaves them.
+// The recompute of a segment repeats its sorts this way instead of sorting.
+__global__ void k_adj_apply(const uint32_t* __restrict__ inv, int64_t n, const float4* __restrict__ pos,
+                            const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz,
+                            float4* __restrict__ pos2, float* __restrict__ vx2, float* __restrict__ vy2,
+                            float* __restrict__ vz2) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const uint32_t s = inv[m];
+  float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float((int)DEAD));
+  float a = 0.f, b = 0.f, c = 0.f;
+  if (s != DEAD) {
+    p = pos[s];
+    a = vx[s];
+    b = vy[s];
+    c = vz[s];
+  }
+  pos2[m] = p;
+  vx2[m] = a;
+  vy2[m] = b;
+  vz2[m] = c;
 }
 
 __device__ __forceinline__ bool in_probe(const Geo& G, int64_t un, int3 lo, int3 hi, int& i, int& j, int& k) {
