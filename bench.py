@@ -600,25 +600,48 @@ def run_ensemble_line(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+BODY_NPR = 4096  # entries of each velocity table of the body workload
+
+
+_BODY_TABLES = {}
+
+
+def body_tables(case) -> dict:
+    """The velocity tables of the body workload, built by the reference's
+    own table code (ctca_b200/tables.py) from one random stream seeded with
+    the case's seed: per species the open-boundary tables (flux through the
+    z faces of the drifting Maxwellian, Maxwellian x / y), then the emission
+    tables of the photoelectrons (flux and tangential Maxwellian of
+    vth = 0.01)."""
+    key = (case.seed, tuple((s.vth, s.drift[2]) for s in case.species))
+    if key not in _BODY_TABLES:
+        from ctca_b200 import inputs, tables
+        renv = inputs.units()["renv"]
+        rng = tables.Ranu0(case.seed)
+        out = {"species": []}
+        for s in case.species:
+            t = tables.inflow_tables(BODY_NPR, 1, (0.0, 0.0, s.drift[2] * renv), s.vth * renv, s.vth * renv, rng)
+            out["species"].append({"vzf": t["vzf"], "vzb": t["vzb"], "vxr": t["vxr"], "vyr": t["vyr"]})
+        em = tables.emission_tables(BODY_NPR, BODY_NPR, 0.0, 0.01 * renv, 0.01 * renv, 0.0, rng)
+        out["vn"], out["vt"] = em["vnormf"], em["vtangf"]
+        _BODY_TABLES[key] = out
+    return _BODY_TABLES[key]
+
+
 def body_plan(case, scale: float) -> dict:
     """Per-step injection of the body workload drawn on the device: tables
     and counts (the rates of body_injection)."""
-    from ctca_b200 import inject, inputs
-    renv = inputs.units()["renv"]
     nx, ny, nz = case.n
-    plan = {"nemit": int(round((1 << 20) * scale ** 3)),
-            "vn": inject.flux_table(0.01 * renv, 0.0, 4096), "vt": inject.maxwell_table(0.01 * renv, 0.0, 4096),
-            "inflow": []}
+    tb = body_tables(case)
+    plan = {"nemit": int(round((1 << 20) * scale ** 3)), "vn": tb["vn"], "vt": tb["vt"], "inflow": []}
     counts = [0, 0]
     for isp, s in enumerate(case.species):
         vd = s.drift[2]
-        vxt = inject.maxwell_table(s.vth * renv, 0.0, 4096)
-        vyt = np.random.default_rng([case.seed, 99, isp]).permutation(vxt)
+        st = tb["species"][isp]
         for front, sgn in ((True, +1.0), (False, -1.0)):
             n = int(round(s.ppc * nx * ny * _flux(vd, s.vth, sgn) * case.dt))
             if n:
-                plan["inflow"].append((isp + 1, front, n, inject.flux_table(s.vth * renv, vd * renv, 4096, sign=sgn),
-                                       vxt, vyt))
+                plan["inflow"].append((isp + 1, front, n, st["vzf"] if front else st["vzb"], st["vxr"], st["vyr"]))
                 counts[isp] += n
     counts[0] += 2 * plan["nemit"]
     plan["counts"] = counts
@@ -646,29 +669,26 @@ def _body_step(job):
     """The injected records of one step of the body workload (see
     body_injection); runs in a worker process."""
     case, scale, seed, step = job
-    from ctca_b200 import inject, inputs
-    renv = inputs.units()["renv"]
+    from ctca_b200 import inject
     nx, ny, nz = case.n
     rng = np.random.default_rng([seed, step])
     body = case.bodies[0]
     nemit = int(round((1 << 20) * scale ** 3))
+    tb = body_tables(case)
     recs = []
     for isp, s in enumerate(case.species):
         vd = s.drift[2]
-        vxt = inject.maxwell_table(s.vth * renv, 0.0, 4096)
-        vyt = np.random.default_rng([seed, 99, isp]).permutation(vxt)  # tables drawn apart, as vxr / vyr
+        st = tb["species"][isp]
         parts = []
         for front, sgn in ((True, +1.0), (False, -1.0)):
             cnt = s.ppc * nx * ny * _flux(vd, s.vth, sgn) * case.dt
             n = int(cnt) + (1 if rng.random() < cnt - int(cnt) else 0)
             if n:
-                vz = inject.flux_table(s.vth * renv, vd * renv, 4096, sign=sgn)
-                parts.append(inject.inflow_z(front, n, nx, ny, nz, vz, vxt, vyt, 2.0, rng, spec=isp + 1))
+                parts.append(inject.inflow_z(front, n, nx, ny, nz, st["vzf"] if front else st["vzb"], st["vxr"],
+                                             st["vyr"], 2.0, rng, spec=isp + 1))
         if isp == 0 and nemit:
-            vn = inject.flux_table(0.01 * renv, 0.0, 4096)
-            vt = inject.maxwell_table(0.01 * renv, 0.0, 4096)
             parts.append(inject.emit_rectangle(1, body["xupc"], (body["ylpc"], body["yupc"]),
-                                               (body["zlpc"], body["zupc"]), nemit, vn, vt, rng, spec=1))
+                                               (body["zlpc"], body["zupc"]), nemit, tb["vn"], tb["vt"], rng, spec=1))
         recs.append(np.concatenate(parts))
     return recs
 

@@ -5,12 +5,10 @@ Emses.fx_inject (emsesg_fx_inject); the reference's supervisors also run on
 the host and hand each new particle to oh2_inject_particle.
 
 Velocity tables.  The reference fills vnormf / vtangf / vzf / vzb / vxr / vyr
-at initialisation (src/main/inipin.F90:476-583) with npr samples of the flux
-distributions and draws table entries with addr = nprs + npr*U.  Here the
-tables hold the npr quantiles (k + 1/2)/npr of the same distributions:
-
-  tangential   Maxwellian N(drift, vth^2)
-  normal flux  v * exp(-(v - vd)^2 / (2 vth^2)) on v > 0 (flux through a face)
+at initialisation (src/main/inipin.F90:476-660, 996-1097) and the
+supervisors draw table entries with addr = nprs + npr*U; the tables are
+built by the reference's own table code, restated in ctca_b200/tables.py
+(vflux / RANN0 / rexch on the reference's Mersenne Twister stream).
 
 Random numbers come from a numpy Generator (the reference uses MT19937
 through RANU0), or, with `uniforms=`, from a given array; the number and
@@ -21,10 +19,8 @@ produce the same records.
 """
 from __future__ import annotations
 
-import math
 
 import numpy as np
-from scipy.special import erfinv
 
 from .emses import PARTICLE_DTYPE
 
@@ -54,30 +50,6 @@ def hash_uniforms(seed: int, stream: int, index0: int, n: int, per: int) -> np.n
             np.arange(per, dtype=np.uint64)[None, :]
         b = _mix64(a ^ (idx * np.uint64(0xD1B54A32D192ED03)))
     return (b >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
-
-
-def maxwell_table(vth: float, drift: float, npr: int) -> np.ndarray:
-    """npr quantiles of N(drift, vth^2)."""
-    p = (np.arange(npr) + 0.5) / npr
-    return drift + vth * math.sqrt(2.0) * erfinv(2.0 * p - 1.0)
-
-
-def flux_table(vth: float, vd: float, npr: int, sign: float = 1.0) -> np.ndarray:
-    """npr quantiles of the one-sided flux distribution along an axis:
-    f(v) ~ |v| exp(-(v - vd)^2 / (2 vth^2)) for sign*v > 0, with vd the
-    signed drift along the axis and sign the side of the flux (+1: v > 0,
-    -1: v < 0).  With vd = 0 it is the Rayleigh distribution
-    sign*vth*sqrt(-2 ln(1-p))."""
-    p = (np.arange(npr) + 0.5) / npr
-    vd = sign * vd
-    if vd == 0.0:
-        return sign * vth * np.sqrt(-2.0 * np.log1p(-p))
-    hi = max(vd, 0.0) + 12.0 * vth
-    v = np.linspace(0.0, hi, 200001)
-    f = v * np.exp(-0.5 * ((v - vd) / vth) ** 2)
-    cdf = np.concatenate([[0.0], np.cumsum(0.5 * (f[1:] + f[:-1]) * np.diff(v))])
-    cdf /= cdf[-1]
-    return sign * np.interp(p, cdf, v)
 
 
 def emission_count(istep: int, lstep: int, fluxf: float, injct: int, ustep: int) -> int:

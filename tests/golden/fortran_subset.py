@@ -100,6 +100,11 @@ def binop(op, a, b):
             if op == "*": return a * b
             if op == "/": return fdiv(a, b)
             return a ** b if b >= 0 else fdiv(1, a ** -b)
+        if op == "**" and is_int(b) and 0 <= int(b) <= 4:
+            # a real base to a small integer power is multiplied out, as
+            # gfortran does: x**2 = x*x, x**3 = (x*x)*x, x**4 = (x*x)*(x*x)
+            a, n = float(a), int(b)
+            return [1.0, a, a * a, (a * a) * a, (a * a) * (a * a)][n]
         a, b = float(a), float(b)
         if op == "+": return a + b
         if op == "-": return a - b
@@ -481,6 +486,16 @@ class SourceParser:
         return self.stmt_text(ln)
 
     def stmt_text(self, ln):
+        m = re.match(r"^(\d+)\s+(.*)$", ln)
+        if m:  # numeric statement label (the target of a GO TO)
+            return ("label", int(m.group(1)), self.stmt_text(m.group(2)))
+        if ln == "continue":
+            return ("nop",)
+        m = re.match(r"^go\s*to\s+(\d+)$", ln)
+        if m:
+            return ("goto", int(m.group(1)))
+        if re.match(r"^(print|write)\b", ln):
+            return ("nop",)  # output statements change no value
         label = None
         m = re.match(r"^(\w+)\s*:\s*(do\b.*)$", ln)
         if m:
@@ -577,6 +592,11 @@ class _Return(Exception):
     pass
 
 
+class _Goto(Exception):
+    def __init__(self, label):
+        self.label = label
+
+
 class Frame:
     def __init__(self, interp, unit, parent=None):
         self.interp = interp
@@ -584,6 +604,7 @@ class Frame:
         self.vars = {}
         self.types = {}
         self.parent = parent  # host scope for contained procedures
+        self.absent = set()   # optional dummy arguments not given
 
     def lookup(self, name):
         f = self
@@ -596,12 +617,25 @@ class Frame:
         raise FortranError(f"unknown name {name}")
 
 
+def _libm_tgamma(x):
+    """GAMMA: the C library's tgamma (what gfortran calls; Python's
+    math.gamma is a different implementation)."""
+    import ctypes
+    import ctypes.util
+    f = ctypes.CDLL(ctypes.util.find_library("m")).tgamma
+    f.restype, f.argtypes = ctypes.c_double, [ctypes.c_double]
+    return f(float(x))
+
+
 INTRINSICS = {
     "int": lambda x, *kind: int(x),  # truncation toward zero; the kind argument changes no value here
     "floor": lambda x: int(math.floor(x)),
-    "nint": lambda x: int(round(x)),
+    "nint": lambda x: int(math.floor(x + 0.5)) if x >= 0 else -int(math.floor(-x + 0.5)),  # half away from 0
     "dble": float, "real": lambda x, *k: float(x),
     "abs": abs, "sqrt": math.sqrt, "exp": math.exp, "cos": math.cos, "sin": math.sin,
+    "dabs": abs, "dsqrt": math.sqrt, "dexp": math.exp, "dcos": math.cos, "dsin": math.sin,
+    "log": math.log, "dlog": math.log, "erf": math.erf,  # math.erf is the C library's erf
+    "gamma": lambda x: _libm_tgamma(x),
     "mod": lambda a, b: (a - int(a / b) * b) if not (is_int(a) and is_int(b)) else int(math.fmod(a, b)),
 }
 
@@ -632,7 +666,7 @@ class Interpreter:
         self.externals = externals or {}
 
     # -- calls
-    def call(self, name, args, frame=None):
+    def call(self, name, args, frame=None, kw=None):
         unit = None
         if frame is not None:
             f = frame
@@ -643,7 +677,7 @@ class Interpreter:
             unit = self.units.get(name)
         if unit is None:
             if name in self.externals:
-                return self.externals[name](*args)
+                return self.externals[name](*args, **(kw or {}))
             raise FortranError(f"unknown procedure {name}")
         host = None
         if frame is not None and name not in self.units:
@@ -656,7 +690,15 @@ class Interpreter:
             fr.types[nm] = ty
         for a, v in zip(unit.args, args):
             fr.vars[a] = v
+        for a, v in (kw or {}).items():
+            if a not in unit.args:
+                raise FortranError(f"{name}: no dummy argument {a}")
+            fr.vars[a] = v
+        # dummies not given: absent optional arguments (present() is false)
+        fr.absent = {a for a in unit.args if a not in fr.vars}
         for (ty, nm, dims, init, is_param) in unit.decls:
+            if nm in fr.absent:
+                continue
             if nm in fr.vars:
                 if dims is not None and isinstance(fr.vars[nm], FArray):
                     # explicit-shape dummy: rebind bounds
@@ -714,8 +756,20 @@ class Interpreter:
 
     # -- statements
     def run_block(self, stmts, fr):
-        for st in stmts:
-            self.exec(st, fr)
+        i = 0
+        while i < len(stmts):
+            try:
+                self.exec(stmts[i], fr)
+                i += 1
+            except _Goto as g:
+                # a GO TO resumes at the labelled statement of this block, or
+                # leaves the block for an enclosing one
+                for j, st in enumerate(stmts):
+                    if st[0] == "label" and st[1] == g.label:
+                        i = j
+                        break
+                else:
+                    raise
 
     def exec(self, st, fr):
         k = st[0]
@@ -774,6 +828,10 @@ class Interpreter:
             self.do_call(st[1], fr)
         elif k == "nop":
             pass
+        elif k == "label":
+            self.exec(st[2], fr)
+        elif k == "goto":
+            raise _Goto(st[1])
         elif k == "decl":
             pass
         else:
@@ -783,14 +841,34 @@ class Interpreter:
         parts = des[1]
         if len(parts) == 1:
             name, args = parts[0]
-            vals = [self.eval_arg(a, fr) for a in (args or [])]
+            pos = [a for a in (args or []) if not (isinstance(a, tuple) and a[0] == "kw")]
+            vals = [self.eval(a, fr) for a in pos]
+            # an element of a 1-D array given for an array dummy: sequence
+            # association, the dummy starts at that element
+            unit = self.units.get(name)
+            if unit is not None:
+                arr_dummies = {nm for (ty, nm, dims, init, is_param) in unit.decls if dims is not None}
+                for q, (a, dummy) in enumerate(zip(pos, unit.args)):
+                    if dummy not in arr_dummies or not (isinstance(a, tuple) and a[0] == "des"):
+                        continue
+                    parts = a[1]
+                    if len(parts) != 1 or parts[0][1] is None or len(parts[0][1]) != 1:
+                        continue
+                    scope, nm, ty = self.resolve(parts[0][0], fr)
+                    arr = scope[nm] if scope is not None else None
+                    sub = parts[0][1][0]
+                    if isinstance(arr, FArray) and arr.data.ndim == 1 and not (isinstance(sub, tuple) and
+                                                                              sub[0] == "range"):
+                        k0 = int(self.eval(sub, fr)) - arr.lb[0]
+                        vals[q] = FArray(arr.data[k0:], [1])
+            kw = {a[1]: self.eval(a[2], fr) for a in (args or []) if isinstance(a, tuple) and a[0] == "kw"}
             self.last_frame = None
-            self.call(name, vals, fr)
+            self.call(name, vals, fr, kw)
             callee = self.last_frame
             # arguments pass by reference: a scalar variable or component
             # given to an interpreted subroutine gets the dummy's final value
             if callee is not None and callee.unit.name == name:
-                for a, v, dummy in zip(args or [], vals, callee.unit.args):
+                for a, v, dummy in zip(pos, vals, callee.unit.args):
                     if isinstance(a, tuple) and a[0] == "des" and not isinstance(v, (FArray, np.ndarray, DerivedObj)):
                         nv = callee.vars.get(dummy, v)
                         if nv is not v:
@@ -837,7 +915,7 @@ class Interpreter:
             return e[1]
         if k == "neg":
             v = self.eval(e[1], fr)
-            return -v
+            return FArray(-v.data, v.lb) if isinstance(v, FArray) else -v
         if k == "not":
             return not self.eval(e[1], fr)
         if k == "bin":
@@ -857,6 +935,8 @@ class Interpreter:
     def eval_des(self, parts, fr):
         name, args = parts[0]
         scope, nm, ty = self.resolve(name, fr)
+        if scope is None and name == "present":
+            return args[0][1][0][0] not in fr.absent
         if scope is None:
             # function / intrinsic
             vals = [self.eval_arg(a, fr) for a in (args or [])]

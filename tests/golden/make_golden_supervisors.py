@@ -44,7 +44,7 @@ sys.path.insert(0, str(HERE.parent.parent))
 
 from fortran_subset import DerivedObj, FArray, Interpreter, parse_source  # noqa: E402
 
-from ctca_b200 import inject  # noqa: E402
+from ctca_b200 import tables  # noqa: E402
 from ctca_b200.emses import PARTICLE_DTYPE  # noqa: E402
 
 FIELDS = ("x", "y", "z", "vx", "vy", "vz", "pid", "preside", "nid", "spec")
@@ -111,12 +111,12 @@ def make(ref: Path) -> dict:
 
     tab = lambda a: FArray(np.asarray(a, dtype=np.float64).copy(), [1])  # noqa: E731
     # tables of one species (nprs = 1): normal speeds per face, tangential ones
+    # (the reference's own table builders, ctca_b200/tables.py, pinned by
+    # make_golden_tables.py)
     vth, vd = 0.05, 0.02
-    t = {"vxf": inject.flux_table(vth, vd, npr, 1.0), "vxb": inject.flux_table(vth, vd, npr, -1.0),
-         "vyf": inject.flux_table(vth, -vd, npr, 1.0), "vyb": inject.flux_table(vth, -vd, npr, -1.0),
-         "vzf": inject.flux_table(vth, 0.0, npr, 1.0), "vzb": inject.flux_table(vth, 0.0, npr, -1.0),
-         "vxr": inject.maxwell_table(vth, vd, npr), "vyr": inject.maxwell_table(vth, -vd, npr),
-         "vzr": inject.maxwell_table(vth, 0.0, npr)}
+    stream = tables.Ranu0(900)
+    built = tables.inflow_tables(npr, 1, (vd, -vd, 0.0), vth, vth, stream)
+    t = {k: built[k] for k in ("vxf", "vxb", "vyf", "vyb", "vzf", "vzb", "vxr", "vyr", "vzr")}
     ustep, injct, istep, lstep = 2, 1, 7, 0
     arr = {"arrxf": 13.7, "arrxb": 9.2, "arryf": 11.4, "arryb": 8.9, "arrzf": 15.3, "arrzb": 12.1}
     zssurf = 0.004  # some z-bottom particles stay below: dropped (psuper2.F90 `cycle`)
@@ -146,7 +146,8 @@ def make(ref: Path) -> dict:
         out["count_" + k] = np.int64(g["n" + k].data[0])
     used_inflow = pos[0]
     # plane emission: per face, n particles with RANU0(dranu, n*6) first
-    vnormf, vtangf = inject.flux_table(0.01, 0.0, npr), inject.maxwell_table(0.01, 0.0, npr)
+    em = tables.emission_tables(npr, npr, 0.0, 0.01, 0.01, 0.0, stream)
+    vnormf, vtangf = em["vnormf"], em["vtangf"]
     g.update(vnormf=tab(vnormf), vtangf=tab(vtangf), iepl=1)
     faces = [(1, 16.0), (-1, 8.0), (2, 12.5), (-2, 7.0), (3, 18.0), (-3, 14.0)]
     bounds = {"xl": 4.0, "xu": 20.0, "yl": 3.0, "yu": 17.0, "zl": 6.0, "zu": 26.0}

@@ -15,9 +15,10 @@ import pytest
 from ctca_b200.emses import Config
 from oracle import oracle as O
 
-# the particle-path fixtures of make_golden.py (supervisors.npz, of
-# make_golden_supervisors.py, has its own test)
-CASES = sorted(p for p in (Path(__file__).parent / "golden").glob("*.npz") if p.stem != "supervisors")
+# the particle-path fixtures of make_golden.py (supervisors.npz and
+# tables.npz, of make_golden_supervisors.py and make_golden_tables.py, have
+# their own tests)
+CASES = sorted(p for p in (Path(__file__).parent / "golden").glob("*.npz") if p.stem not in ("supervisors", "tables"))
 
 
 def load(path):

@@ -19,12 +19,18 @@ import ctypes
 import numpy as np
 import pytest
 
-from ctca_b200 import inject, inputs
+from ctca_b200 import inject, inputs, tables
 from ctca_b200.emses import PARTICLE_DTYPE, Emses
 from oracle import compare as C
 from oracle import oracle as O
 
 from helpers import build, case
+
+
+@pytest.fixture
+def trng():
+    """The reference's random stream for the velocity tables of a test."""
+    return tables.Ranu0(4357)
 
 pytestmark = pytest.mark.gpu
 
@@ -50,7 +56,7 @@ def with_injected(p, tp, batches):
     return np.concatenate(parts).astype(PARTICLE_DTYPE), np.array(counts, dtype=np.int64)
 
 
-def test_fx_box_inflow_emission_per_step(gpu):
+def test_fx_box_inflow_emission_per_step(gpu, trng):
     c = case(n=(24, 24, 32), ppc=(4, 4), npbnd=(0, 0, 2), nfbnd=(0, 0, 1), vth_scale=3.0, tile=(8, 8, 8))
     for s in c.species:
         s.drift = (0.0, 0.0, -0.08)
@@ -81,9 +87,9 @@ def test_fx_box_inflow_emission_per_step(gpu):
 
     renv = inputs.units()["renv"]
     vth = [s.vth * renv for s in c.species]
-    vn = inject.flux_table(0.01 * renv, 0.0, 1024)
-    vt = inject.maxwell_table(0.01 * renv, 0.0, 1024)
-    inflow_tabs = [(inject.flux_table(vth[s], -0.08 * renv, 1024, sign=-1.0), inject.maxwell_table(vth[s], 0.0, 1024))
+    vn = tables.signed_flux(1024, 0.0, 0.01 * renv, 1, trng)[0]
+    vt = tables.rann0(0.0, 0.01 * renv, 1024, trng)
+    inflow_tabs = [(tables.signed_flux(1024, -0.08 * renv, vth[s], -1, trng)[0], tables.rann0(0.0, vth[s], 1024, trng))
                    for s in range(2)]
     L = O.lib()
     surf_prev = g.fx_surface()

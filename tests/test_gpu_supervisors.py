@@ -6,10 +6,16 @@ counts, the particle records after the sort), are bit-identical."""
 import numpy as np
 import pytest
 
-from ctca_b200 import inject, inputs
+from ctca_b200 import inject, inputs, tables
 from ctca_b200.emses import Emses
 
 from helpers import build, case
+
+
+@pytest.fixture
+def trng():
+    """The reference's random stream for the velocity tables of a test."""
+    return tables.Ranu0(4357)
 
 pytestmark = pytest.mark.gpu
 
@@ -32,14 +38,14 @@ def loaded(c, cfg, eb):
     return g
 
 
-def test_device_supervisors_match_host(gpu):
+def test_device_supervisors_match_host(gpu, trng):
     c, cfg, eb = setup()
     renv = inputs.units()["renv"]
-    vn = inject.flux_table(0.01 * renv, 0.0, 512)
-    vt = inject.maxwell_table(0.01 * renv, 0.0, 512)
+    vn = tables.signed_flux(512, 0.0, 0.01 * renv, 1, trng)[0]
+    vt = tables.rann0(0.0, 0.01 * renv, 512, trng)
     s0 = c.species[0]
-    vz = inject.flux_table(s0.vth * renv, -0.08 * renv, 512, sign=-1.0)
-    vx = inject.maxwell_table(s0.vth * renv, 0.0, 512)
+    vz = tables.signed_flux(512, -0.08 * renv, s0.vth * renv, -1, trng)[0]
+    vx = tables.rann0(0.0, s0.vth * renv, 512, trng)
     vy = vx[::-1].copy()
     seed = 99
     with loaded(c, cfg, eb) as a, loaded(c, cfg, eb) as b:
@@ -74,7 +80,7 @@ def test_device_supervisors_match_host(gpu):
 
 
 @pytest.mark.parametrize("axis", [0, 1])
-def test_device_inflow_x_y_faces_match_host(gpu, axis):
+def test_device_inflow_x_y_faces_match_host(gpu, axis, trng):
     """Inflow through both faces of x or y (open along that axis): device
     records against the host supervisor on the same draws, through a step
     and a sort."""
@@ -86,14 +92,14 @@ def test_device_inflow_x_y_faces_match_host(gpu, axis):
     cfg, eb, p, tp = build(c, capacity_factor=1.5)
     renv = inputs.units()["renv"]
     s0 = c.species[0]
-    va = inject.maxwell_table(s0.vth * renv, 0.0, 512)
+    va = tables.rann0(0.0, s0.vth * renv, 512, trng)
     vb = va[::-1].copy()
     ext = (cfg.nx, cfg.ny, cfg.nz)
     seed = 7
     with loaded(c, cfg, eb) as a, loaded(c, cfg, eb) as b:
         for step in range(2):
             for q, front in enumerate((True, False)):
-                vn = inject.flux_table(s0.vth * renv, 0.0, 512, sign=1.0 if front else -1.0)
+                vn = tables.signed_flux(512, 0.0, s0.vth * renv, 1 if front else -1, trng)[0]
                 n = 50 + 7 * step + q
                 st = 10 + q
                 u = inject.hash_uniforms(seed, st, 1000 * step, n, 5)
@@ -116,15 +122,15 @@ def test_device_inflow_x_y_faces_match_host(gpu, axis):
         assert np.array_equal(pa.view(np.uint8), pb.view(np.uint8))
 
 
-def test_device_plane_emission_matches_host(gpu):
+def test_device_plane_emission_matches_host(gpu, trng):
     """Plane emission (psuper2) from two planes inside a periodic box:
     device records against the host supervisor on the same draws, through
     steps and a sort."""
     c = case(n=(24, 24, 24), ppc=(3, 3), vth_scale=3.0, tile=(8, 8, 8))
     cfg, eb, p, tp = build(c, capacity_factor=1.5)
     renv = inputs.units()["renv"]
-    vn = inject.flux_table(0.01 * renv, 0.0, 512)
-    vt = inject.maxwell_table(0.01 * renv, 0.0, 512)
+    vn = tables.signed_flux(512, 0.0, 0.01 * renv, 1, trng)[0]
+    vt = tables.rann0(0.0, 0.01 * renv, 512, trng)
     seed = 31
     planes = [(1, 12.0, (4.0, 20.0), (6.0, 18.0), 1), (-3, 9.5, (2.0, 22.0), (3.0, 21.0), 2)]
     with loaded(c, cfg, eb) as a, loaded(c, cfg, eb) as b:
