@@ -108,6 +108,7 @@ struct FxState {
   int32_t* tailord = nullptr;          // per tail slot: 1 + ordinal of a pending random step, or 0
   int64_t tailord_base[EMSESG_ISPEC] = {};  // offset of each species' tail in tailord
   int64_t pending[EMSESG_ISPEC] = {};  // injected particles still to take their random step
+  bool inj_j_pending = false;          // the J accumulator holds injection currents for the next step
   emsesg_particle* stage = nullptr;    // device staging of injected records
   int32_t* stage_ord = nullptr;
   int64_t stage_cap = 0;

@@ -878,8 +878,13 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
   unsigned long long* acc_rho = (unsigned long long*)f.accum;
   unsigned long long* acc_j = acc_rho + fr.size();
-  if (deposit)
-    EMSESG_CUDA(ctx, cudaMemsetAsync(f.accum, 0, (fr.size() + fj.size()) * sizeof(int64_t), ctx->stream));
+  // rho and J start from zero; J keeps the injection currents of the
+  // supervisors called since the last step (emsesg_fx_inflow_current)
+  if (deposit) {
+    EMSESG_CUDA(ctx, cudaMemsetAsync(f.accum, 0, (fr.size() + (f.inj_j_pending ? 0 : fj.size())) * sizeof(int64_t),
+                                     ctx->stream));
+    f.inj_j_pending = false;
+  }
   int tmax = std::max(f.tile[0], std::max(f.tile[1], f.tile[2]));
   int smem = fx_push_smem(tmax);
   FxPushArgs a{};
@@ -1061,6 +1066,104 @@ __global__ void k_gen_emit(emsesg_particle* out, int32_t* ord, int64_t n, int ne
   ord[2 * k + 1] = (int32_t)(pending + k + 1);
 }
 
+// Particles emitted from a cylindrical body (psuper3.F90:241-528), each a
+// record with preside 1 and, with `anti`, its anti-particle (preside -2) at
+// the same place.  The uniforms of particle k are entries per*k + c of the
+// call's flat array of 6n (per = 5 for a side of radius < 1 with omni 0,
+// else 6), entry j the hash of index0*6 + j.  An end cap (|nemd| = align):
+// normal ud * vnormf, tangential vtangf, the point at grd, radius *
+// runiform from the axis at the angle 2 pi u4.  A side: vnormc / vtangc
+// turned by psicos + psi (radius >= 1), by psi (radius < 1: the point where
+// the velocity's direction meets the circle) or by 2 pi u2 (omni 1), the
+// coordinate along the axis hl + (hu - hl) u.  The records match the host's
+// (ctca_b200/inject.emit_cylinder) up to the last bits of the device's
+// cos / sin.
+struct CylTabs {
+  const double *vnormf, *vtangf, *runiform, *vnormc, *vtangc, *psicos;
+};
+__global__ void k_gen_emit_cyl(emsesg_particle* out, int32_t* ord, int64_t n, int nemd, int align, double radius,
+                               double axis0, double axis1, int omni, double grd, double hl, double hu, double psi,
+                               CylTabs t, int npr, int anti, uint64_t seed, uint64_t stream, uint64_t index0,
+                               int spec, int64_t pending) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const bool cap = abs(nemd) == align;
+  const int per = (!cap && omni == 0 && radius < 1.0) ? 5 : 6;
+  double u[6];
+  for (int c = 0; c < per; c++) u[c] = hash_u01(seed, stream, index0 * 6 + (uint64_t)(per * k + c));
+  int ad[4];
+  for (int c = 0; c < 4; c++) ad[c] = (int)(npr * u[c]);
+  const double pi2 = 6.283185307179586;  // 2 acos(-1)
+  int p0, p1, p2;
+  double vn, vt1, vt2, rn, rt1, rt2;
+  if (cap) {
+    const int an = abs(nemd);
+    p0 = an - 1; p1 = an % 3; p2 = (an + 1) % 3;
+    vn = nemd > 0 ? t.vnormf[ad[0]] : -t.vnormf[ad[0]];
+    vt1 = t.vtangf[ad[1]];
+    vt2 = t.vtangf[ad[2]];
+    const double radial = __dmul_rn(radius, t.runiform[ad[3]]);
+    const double ang = __dmul_rn(pi2, u[4]);
+    rn = grd;
+    rt1 = __dadd_rn(axis0, __dmul_rn(radial, cos(ang)));
+    rt2 = __dadd_rn(axis1, __dmul_rn(radial, sin(ang)));
+  } else {
+    double a1 = axis0, a2 = axis1;
+    if (align == 1) {
+      p0 = 2; p1 = 1; p2 = 0;
+      a1 = axis1; a2 = axis0;
+    } else if (align == 2) {
+      p0 = 2; p1 = 0; p2 = 1;
+    } else {
+      p0 = 0; p1 = 1; p2 = 2;
+    }
+    const double nc = t.vnormc[ad[0]], tc = t.vtangc[ad[1]];
+    if (omni == 0 && radius >= 1.0) {
+      const double ang = __dadd_rn(t.psicos[ad[2]], psi);
+      const double ca = cos(ang), sa = sin(ang);
+      vn = __dsub_rn(__dmul_rn(nc, ca), __dmul_rn(tc, sa));
+      vt1 = __dadd_rn(__dmul_rn(nc, sa), __dmul_rn(tc, ca));
+      rn = __dadd_rn(a1, __dmul_rn(radius, ca));
+      rt1 = __dadd_rn(a2, __dmul_rn(radius, sa));
+      vt2 = t.vtangf[ad[3]];
+      rt2 = lin(hl, hu, u[5]);
+    } else if (omni == 0) {
+      const double ca = cos(psi), sa = sin(psi);
+      vn = __dsub_rn(__dmul_rn(nc, ca), __dmul_rn(tc, sa));
+      vt1 = __dadd_rn(__dmul_rn(nc, sa), __dmul_rn(tc, ca));
+      vt2 = t.vtangf[ad[2]];
+      const double v2normi = __ddiv_rn(radius, __dsqrt_rn(__dadd_rn(__dmul_rn(vn, vn), __dmul_rn(vt1, vt1))));
+      rn = __dadd_rn(a1, __dmul_rn(vn, v2normi));
+      rt1 = __dadd_rn(a2, __dmul_rn(vt1, v2normi));
+      rt2 = lin(hl, hu, u[4]);
+    } else {
+      const double eaz = __dmul_rn(pi2, u[2]);
+      const double ca = cos(eaz), sa = sin(eaz);
+      vn = __dsub_rn(__dmul_rn(nc, ca), __dmul_rn(tc, sa));
+      vt1 = __dadd_rn(__dmul_rn(nc, sa), __dmul_rn(tc, ca));
+      vt2 = t.vtangf[ad[3]];
+      rn = __dadd_rn(a1, __dmul_rn(radius, ca));
+      rt1 = __dadd_rn(a2, __dmul_rn(radius, sa));
+      rt2 = lin(hl, hu, u[5]);
+    }
+  }
+  emsesg_particle p;
+  double* r = &p.x;
+  double* v = &p.vx;
+  r[p0] = rn; r[p1] = rt1; r[p2] = rt2;
+  v[p0] = vn; v[p1] = vt1; v[p2] = vt2;
+  p.pid = 0; p.nid = 0; p.spec = spec;
+  p.preside = EMSESG_PCL_INJECTED;
+  const int64_t o = anti ? 2 * k : k;
+  out[o] = p;
+  ord[o] = (int32_t)(pending + k + 1);
+  if (anti) {
+    p.preside = EMSESG_PCL_TO_BE_ACCUMULATED_AS_ANTIPCL;
+    out[o + 1] = p;
+    ord[o + 1] = 0;
+  }
+}
+
 // Particles emitted from a rectangular plane (psuper2.F90:330-360,
 // 554-576): the normal coordinate grd + vn * injctisw * u3, the tangential
 // ones uniform on the plane plus vt * injctisw * u3; preside 0, pid = the
@@ -1095,10 +1198,78 @@ __global__ void k_gen_emit_plane(emsesg_particle* out, int32_t* ord, int64_t n, 
 // along the tangential axes; along the normal the distance vn * injctisw * u
 // from the face.  vnt: normal speeds [int(npr*u0)]; vat / vbt: the
 // tangential ones of the two other axes in increasing order [int(npr*u1)].
+// The injection current of psuper1 (psuper1.F90:120-323 with
+// current_deposition, :859-988) for a particle injected through the face
+// (axis, front) at a: the zigzag current of the path from b outside the face
+// (-1 below the lower face, n + 0.99999999 above the upper one, along the
+// normal; a - v ustep along the others) to a, times q, into the int64 J
+// accumulator (scale 2^40), each of the 24 contributions rounded on its own.
+// A node outside the accumulator's guard layers is reported, not written.
+struct InjCurrent {
+  long long* acc;  // J accumulator; null: no current
+  FieldDesc fj;
+  double qfix;     // q * 2^40
+  int ustep;
+  double rustep;
+};
+
+__device__ __forceinline__ void inj_zigzag(const InjCurrent& c, const double (&b)[3], const double (&a)[3], int* status,
+                                           long long* diag) {
+  int ib[3], ia[3];
+  double r[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    ib[d] = (int)floor(b[d]);
+    ia[d] = (int)floor(a[d]);
+    r[d] = ib[d] == ia[d] ? __dmul_rn(__dadd_rn(b[d], a[d]), 0.5) : fmax((double)ib[d], (double)ia[d]);
+  }
+  const int ext[3] = {c.fj.ex, c.fj.ey, c.fj.ez};
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    double dd[3], vv[3];
+    int cell[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      if (s == 0) {
+        cell[d] = ib[d];
+        dd[d] = __dsub_rn(__dmul_rn(__dadd_rn(r[d], b[d]), 0.5), (double)ib[d]);
+        vv[d] = __dmul_rn(__dsub_rn(r[d], b[d]), c.rustep);
+      } else {
+        cell[d] = ia[d];
+        dd[d] = __dsub_rn(__dmul_rn(__dadd_rn(a[d], r[d]), 0.5), (double)ia[d]);
+        vv[d] = __dmul_rn(__dsub_rn(a[d], r[d]), c.rustep);
+      }
+    }
+#pragma unroll
+    for (int comp = 0; comp < 3; comp++) {
+      const int e1 = comp == 0 ? 1 : 0, e2 = comp == 2 ? 1 : 2;
+      const double w4 = __dmul_rn(dd[e1], dd[e2]);
+      const double w[4] = {__dsub_rn(__dsub_rn(1.0, dd[e1]), __dsub_rn(dd[e2], w4)), __dsub_rn(dd[e1], w4),
+                           __dsub_rn(dd[e2], w4), w4};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        int n3[3] = {cell[0], cell[1], cell[2]};
+        if (q & 1) n3[e1]++;
+        if (q & 2) n3[e2]++;
+        bool in = true;
+#pragma unroll
+        for (int d = 0; d < 3; d++) in = in && n3[d] >= c.fj.lo && n3[d] - c.fj.lo < ext[d];
+        if (!in) {
+          report_bad(status, diag, SITE_FX_DEPOSIT, -5, n3[0] + 100000LL * n3[1] + 10000000000LL * n3[2]);
+          continue;
+        }
+        const long long v = __double2ll_rn(__dmul_rn(__dmul_rn(vv[comp], w[q]), c.qfix));
+        if (v) atomicAdd((unsigned long long*)&c.acc[c.fj.at(comp, n3[0], n3[1], n3[2])], (unsigned long long)v);
+      }
+    }
+  }
+}
+
 __global__ void k_gen_inflow(emsesg_particle* out, int32_t* ord, int64_t n, int axis, int front, int nx, int ny,
                              int nz, const double* __restrict__ vnt, const double* __restrict__ vat,
                              const double* __restrict__ vbt, int npr, double injctisw, uint64_t seed,
-                             uint64_t stream, uint64_t index0, int spec) {
+                             uint64_t stream, uint64_t index0, int spec, InjCurrent cur, int* status,
+                             long long* diag) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   double u[5];
@@ -1119,6 +1290,17 @@ __global__ void k_gen_inflow(emsesg_particle* out, int32_t* ord, int64_t n, int 
   p.pid = 0; p.preside = 0; p.nid = 0; p.spec = spec;
   out[k] = p;
   ord[k] = 0;
+  if (cur.acc) {
+    // the point outside the face, component by component (no array index
+    // chosen at run time)
+    const double us = (double)cur.ustep;
+    const double out_n = front ? -1.0 : __dadd_rn((double)ext[axis], 0.99999999);
+    const double b[3] = {axis == 0 ? out_n : __dsub_rn(p.x, __dmul_rn(p.vx, us)),
+                         axis == 1 ? out_n : __dsub_rn(p.y, __dmul_rn(p.vy, us)),
+                         axis == 2 ? out_n : __dsub_rn(p.z, __dmul_rn(p.vz, us))};
+    const double at[3] = {p.x, p.y, p.z};
+    inj_zigzag(cur, b, at, status, diag);
+  }
 }
 
 int inject_tables(emsesg_ctx* ctx, int ntab, int npr, const double* const* tabs) {
@@ -1216,12 +1398,39 @@ extern "C" int emsesg_fx_emit_plane(emsesg_ctx* ctx, int spec, int nemd, double 
   return inject_staged(ctx, is, n, f.pending[is]);
 }
 
-extern "C" int emsesg_fx_inflow(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n, const double* vn_t,
-                                const double* va_t, const double* vb_t, int npr, double injctisw, uint64_t seed,
-                                uint64_t stream, uint64_t index0) {
+extern "C" int emsesg_fx_emit_cylinder(emsesg_ctx* ctx, int spec, int nemd, int align, double radius,
+                                       const double* axis, int omni, double grd, double hl, double hu, double psi,
+                                       int64_t n, const double* vnormf, const double* vtangf, const double* runiform,
+                                       const double* vnormc, const double* vtangc, const double* psicos, int npr,
+                                       int anti, uint64_t seed, uint64_t stream, uint64_t index0) {
+  int rc = inject_check(ctx, spec, n, npr, vnormf, vtangf, runiform);
+  if (rc) return rc;
+  if (!axis || !vnormc || !vtangc || !psicos) return EMSESG_ERR_ARG;
+  if (nemd == 0 || nemd < -3 || nemd > 3 || align < 1 || align > 3 || !(radius > 0.0) || (omni != 0 && omni != 1))
+    return set_error(ctx, EMSESG_ERR_ARG, "bad cylinder emission (nemd %d, align %d, omni %d)", nemd, align, omni);
+  if (n == 0) return EMSESG_OK;
+  const int is = spec - 1;
+  FxState& f = ctx->fx;
+  const int64_t nrec = anti ? 2 * n : n;
+  if ((rc = inject_reserve(ctx, is, nrec))) return rc;
+  const double* tabs[6] = {vnormf, vtangf, runiform, vnormc, vtangc, psicos};
+  if ((rc = inject_tables(ctx, 6, npr, tabs))) return rc;
+  CylTabs t{f.inj_tab, f.inj_tab + npr, f.inj_tab + 2 * npr, f.inj_tab + 3 * npr, f.inj_tab + 4 * npr,
+            f.inj_tab + 5 * npr};
+  const int64_t pending = f.pending[is];
+  EMSESG_LAUNCH(ctx, "fx_gen_emit_cyl", k_gen_emit_cyl, nblk(n), 256, 0, f.stage, f.stage_ord, n, nemd, align, radius,
+                axis[0], axis[1], omni, grd, hl, hu, psi, t, npr, anti ? 1 : 0, seed, stream, index0, spec, pending);
+  return inject_staged(ctx, is, nrec, pending + n);
+}
+
+namespace {
+int inflow_impl(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n, const double* vn_t, const double* va_t,
+                const double* vb_t, int npr, double injctisw, uint64_t seed, uint64_t stream, uint64_t index0,
+                int ustep) {
   int rc = inject_check(ctx, spec, n, npr, vn_t, va_t, vb_t);
   if (rc) return rc;
   if (axis < 0 || axis > 2) return set_error(ctx, EMSESG_ERR_ARG, "inflow axis %d (0, 1 or 2)", axis);
+  if (ustep < 0) return set_error(ctx, EMSESG_ERR_ARG, "ustep must be >= 1");
   if (n == 0) return EMSESG_OK;
   const int is = spec - 1;
   FxState& f = ctx->fx;
@@ -1229,10 +1438,40 @@ extern "C" int emsesg_fx_inflow(emsesg_ctx* ctx, int spec, int axis, int front, 
   const double* tabs[3] = {vn_t, va_t, vb_t};
   if ((rc = inject_tables(ctx, 3, npr, tabs))) return rc;
   const emsesg_config& c = ctx->cfg;
+  InjCurrent cur{};
+  if (ustep > 0) {
+    // the J accumulator: cleared before the first current after a step,
+    // then kept by that step
+    FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO);
+    cur.fj = field_desc(c, EMSESG_FIELD_AJ);
+    cur.acc = (long long*)f.accum + fr.size();
+    if (!f.inj_j_pending) {
+      EMSESG_CUDA(ctx, cudaMemsetAsync(cur.acc, 0, cur.fj.size() * sizeof(int64_t), ctx->stream));
+      f.inj_j_pending = true;
+    }
+    cur.qfix = c.q[is] * 1099511627776.0;
+    cur.ustep = ustep;
+    cur.rustep = 1.0 / ustep;
+  }
   EMSESG_LAUNCH(ctx, "fx_gen_inflow", k_gen_inflow, nblk(n), 256, 0, f.stage, f.stage_ord, n, axis, front, c.nx,
                 c.ny, c.nz, f.inj_tab, f.inj_tab + npr, f.inj_tab + 2 * npr, npr, injctisw, seed, stream, index0,
-                spec);
+                spec, cur, ctx->d_status, ctx->d_diag);
   return inject_staged(ctx, is, n, f.pending[is]);
+}
+}  // namespace
+
+extern "C" int emsesg_fx_inflow(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n, const double* vn_t,
+                                const double* va_t, const double* vb_t, int npr, double injctisw, uint64_t seed,
+                                uint64_t stream, uint64_t index0) {
+  return inflow_impl(ctx, spec, axis, front, n, vn_t, va_t, vb_t, npr, injctisw, seed, stream, index0, 0);
+}
+
+extern "C" int emsesg_fx_inflow_current(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n,
+                                        const double* vn_t, const double* va_t, const double* vb_t, int npr,
+                                        double injctisw, int ustep, uint64_t seed, uint64_t stream,
+                                        uint64_t index0) {
+  if (ustep < 1) return ctx ? set_error(ctx, EMSESG_ERR_ARG, "ustep must be >= 1") : EMSESG_ERR_ARG;
+  return inflow_impl(ctx, spec, axis, front, n, vn_t, va_t, vb_t, npr, injctisw, seed, stream, index0, ustep);
 }
 
 extern "C" int emsesg_fx_inflow_z(emsesg_ctx* ctx, int spec, int front, int64_t n, const double* vz_t,
@@ -1811,7 +2050,7 @@ bool graph_ready(const emsesg_ctx* ctx) {
   const FxState& f = ctx->fx;
   bool tail = false;
   for (int is = 0; is < ctx->cfg.nspec; is++) tail = tail || f.ntail[is] > 0 || f.pending[is] > 0;
-  return f.tiled && !tail;
+  return f.tiled && !tail && !f.inj_j_pending;
 }
 
 }  // namespace

@@ -152,6 +152,11 @@ _SIGS = {
                               ctypes.c_uint64, ctypes.c_uint64]),
     "emsesg_fx_emit_plane": (_I, [_P, _I, _I, ctypes.c_double, _P, _P, ctypes.c_int64, _P, _P, _I, ctypes.c_double,
                                   _I, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+    "emsesg_fx_inflow_current": (_I, [_P, _I, _I, _I, ctypes.c_int64, _P, _P, _P, _I, ctypes.c_double, _I,
+                                      ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+    "emsesg_fx_emit_cylinder": (_I, [_P, _I, _I, _I, ctypes.c_double, _P, _I, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_int64, _P, _P, _P, _P, _P, _P, _I, _I,
+                                     ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
     "emsesg_fx_adjoint": (_I, [_P, _I, _I, _I, _I, _P, _P, ctypes.POINTER(ctypes.c_double), _P, _P, _P, _P]),
     "emsesg_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
     "emsesg_fx_load_plasma": (_I, [_P, ctypes.POINTER(Plasma)]),
@@ -442,6 +447,21 @@ class Emses:
         self._check(self.lib.emsesg_fx_emit_plane(self.h, spec, nemd, grd, cb1, cb2, n, vn.ctypes.data,
                                                   vt.ctypes.data, vn.size, injctisw, pid, seed, stream, index0))
 
+    def fx_emit_cylinder(self, spec: int, nemd: int, align: int, radius: float, axis, omni: int, grd: float,
+                         hl: float, hu: float, psi: float, n: int, tabs: dict, anti: bool, seed: int, stream: int,
+                         index0: int = 0):
+        """n particles emitted from a face of a cylindrical body, drawn on the
+        device (inject.emit_cylinder with hash_uniforms(seed, stream, index0,
+        n, 6) flattened); tabs: vnormf, vtangf, runiform, vnormc, vtangc,
+        psicos."""
+        t = [np.ascontiguousarray(tabs[k], dtype=np.float64)
+             for k in ("vnormf", "vtangf", "runiform", "vnormc", "vtangc", "psicos")]
+        assert all(x.size == t[0].size for x in t)
+        ax = (ctypes.c_double * 2)(*axis)
+        self._check(self.lib.emsesg_fx_emit_cylinder(self.h, spec, nemd, align, radius, ax, omni, grd, hl, hu, psi, n,
+                                                     *[x.ctypes.data for x in t], t[0].size, 1 if anti else 0, seed,
+                                                     stream, index0))
+
     def fx_inflow(self, spec: int, axis: int, front: bool, n: int, vn_table, va_table, vb_table, injctisw: float,
                   seed: int, stream: int, index0: int = 0):
         """n inflow particles through a face of `axis` (0 x, 1 y, 2 z) drawn
@@ -452,6 +472,16 @@ class Emses:
         self._check(self.lib.emsesg_fx_inflow(self.h, spec, axis, 1 if front else 0, n, t[0].ctypes.data,
                                               t[1].ctypes.data, t[2].ctypes.data, t[0].size, injctisw, seed,
                                               stream, index0))
+
+    def fx_inflow_current(self, spec: int, axis: int, front: bool, n: int, vn_table, va_table, vb_table,
+                          injctisw: float, ustep: int, seed: int, stream: int, index0: int = 0):
+        """fx_inflow that also deposits psuper1's injection current into the
+        J of the next step (inject.inflow_current times the charge)."""
+        t = [np.ascontiguousarray(x, dtype=np.float64) for x in (vn_table, va_table, vb_table)]
+        assert t[0].size == t[1].size == t[2].size
+        self._check(self.lib.emsesg_fx_inflow_current(self.h, spec, axis, 1 if front else 0, n, t[0].ctypes.data,
+                                                      t[1].ctypes.data, t[2].ctypes.data, t[0].size, injctisw,
+                                                      ustep, seed, stream, index0))
 
     def fx_surface(self) -> np.ndarray:
         """Absorbed minus emitted particles per surface cell, [nspec, nsurf]."""

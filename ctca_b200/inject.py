@@ -103,6 +103,98 @@ def emit_rectangle(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int
     return out
 
 
+def _flat_uniforms(n: int, rng, uniforms) -> np.ndarray:
+    """The 6n numbers of one emission call (RANU0(dranu, n*6)), flat."""
+    if uniforms is not None:
+        return np.asarray(uniforms, dtype=np.float64).ravel()
+    return rng.random(6 * n)
+
+
+# The side surface of a cylinder of axis `align`: the emission routine's
+# (normal, first tangential, second tangential) axes and which of the
+# cylinder's two axis coordinates give the first two (psuper3.F90:301-346).
+_CYL_SIDE = {1: ((2, 1, 0), (1, 0)), 2: ((2, 0, 1), (0, 1)), 3: ((0, 1, 2), (0, 1))}
+
+
+def emit_cylinder(nemd: int, align: int, radius: float, axis: tuple, omni: int, grd: float, hl: float, hu: float,
+                  psi: float, n: int, tabs: dict, rng: np.random.Generator | None, spec: int,
+                  uniforms: np.ndarray | None = None, anti: bool = True) -> np.ndarray:
+    """n particles emitted from a cylindrical body (emit_from_cylinder,
+    psuper3.F90:241-371) from 6n uniforms u (the flat RANU0 array of the
+    call).  A face nemd along the cylinder's axis (|nemd| = align) is an end
+    cap (emit_from_circular_surf, :373-410): normal speed ud *
+    vnormf[int(npr u0)], tangential vtangf[int(npr u1)], vtangf[int(npr u2)];
+    the point at grd on the normal axis and radius * runiform[int(npr u3)]
+    from the axis (axis[0], axis[1]) at the angle 2 pi u4.  Any other face is
+    the side surface, by omni and radius (:412-528): radius >= 1
+    (emit_from_cylindrical_surf1) turns vnormc / vtangc by psicos + psi and
+    puts the point on the circle at that angle; radius < 1 (surf2, five
+    uniforms a particle) turns them by psi and puts the point where the
+    velocity's direction meets the circle; omni = 1 (surf3) turns them by an
+    azimuth 2 pi u2; the coordinate along the axis is hl + (hu - hl) u5 (u4
+    for surf2).  Each particle gives a record with preside 1 and, with
+    `anti` (ncond <= 0), its anti-particle (preside -2) at the same place.
+    tabs: vnormf, vtangf, runiform, vnormc, vtangc, psicos (one species,
+    tables.emission_tables).  The trigonometry is the C library's."""
+    import math
+    u = _flat_uniforms(n, rng, uniforms)
+    vnormf, vtangf, runiform = tabs["vnormf"], tabs["vtangf"], tabs["runiform"]
+    vnormc, vtangc, psicos = tabs["vnormc"], tabs["vtangc"], tabs["psicos"]
+    npr = vnormf.size
+    pi2 = math.pi * 2.0
+    cap = abs(nemd) == align
+    ud = 1.0 if nemd > 0 else -1.0
+    per = 5 if (not cap and omni == 0 and radius < 1.0) else 6
+    out = np.zeros(2 * n if anti else n, dtype=PARTICLE_DTYPE)
+    coords = (("x", "vx"), ("y", "vy"), ("z", "vz"))
+    for m in range(n):
+        ir = per * m
+        ad = [int(npr * float(u[ir + c])) for c in range(4)]
+        if cap:
+            perm = _ORDER[abs(nemd)]
+            vn, vt1, vt2 = ud * vnormf[ad[0]], vtangf[ad[1]], vtangf[ad[2]]
+            radial = radius * runiform[ad[3]]
+            angular = pi2 * float(u[ir + 4])
+            rn, rt1, rt2 = grd, axis[0] + radial * math.cos(angular), axis[1] + radial * math.sin(angular)
+        else:
+            perm, (k1, k2) = _CYL_SIDE[align]
+            a1, a2 = axis[k1], axis[k2]
+            if omni == 0 and radius >= 1.0:
+                ang = psicos[ad[2]] + psi
+                vn = vnormc[ad[0]] * math.cos(ang) - vtangc[ad[1]] * math.sin(ang)
+                vt1 = vnormc[ad[0]] * math.sin(ang) + vtangc[ad[1]] * math.cos(ang)
+                rn, rt1 = a1 + radius * math.cos(ang), a2 + radius * math.sin(ang)
+                vt2 = vtangf[ad[3]]
+                rt2 = hl + (hu - hl) * float(u[ir + 5])
+            elif omni == 0:
+                vn = vnormc[ad[0]] * math.cos(psi) - vtangc[ad[1]] * math.sin(psi)
+                vt1 = vnormc[ad[0]] * math.sin(psi) + vtangc[ad[1]] * math.cos(psi)
+                vt2 = vtangf[ad[2]]
+                v2normi = radius / math.sqrt(vn * vn + vt1 * vt1)
+                rn, rt1 = a1 + vn * v2normi, a2 + vt1 * v2normi
+                rt2 = hl + (hu - hl) * float(u[ir + 4])
+            else:
+                eaz = pi2 * float(u[ir + 2])
+                vn = vnormc[ad[0]] * math.cos(eaz) - vtangc[ad[1]] * math.sin(eaz)
+                vt1 = vnormc[ad[0]] * math.sin(eaz) + vtangc[ad[1]] * math.cos(eaz)
+                vt2 = vtangf[ad[3]]
+                rn, rt1 = a1 + radius * math.cos(eaz), a2 + radius * math.sin(eaz)
+                rt2 = hl + (hu - hl) * float(u[ir + 5])
+        k = 2 * m if anti else m
+        for val_r, val_v, ax in ((rn, vn, perm[0]), (rt1, vt1, perm[1]), (rt2, vt2, perm[2])):
+            c, v = coords[ax]
+            out[c][k] = val_r
+            out[v][k] = val_v
+            if anti:
+                out[c][k + 1] = val_r
+                out[v][k + 1] = val_v
+        out["preside"][k] = PCL_INJECTED
+        if anti:
+            out["preside"][k + 1] = PCL_ANTI
+    out["spec"] = spec
+    return out
+
+
 def emit_plane(nemd: int, grd: float, bounds1: tuple, bounds2: tuple, n: int, vnormf: np.ndarray,
                vtangf: np.ndarray, injctisw: float, rng: np.random.Generator | None, spec: int, pid: int = 0,
                uniforms: np.ndarray | None = None) -> np.ndarray:
@@ -175,6 +267,67 @@ def inflow(axis: int, front: bool, n: int, nx: int, ny: int, nz: int, vn_table: 
     out["spec"] = spec
     keep = out["z"] > zssurf
     return out[keep]
+
+
+# (normal, first, second) axes of the zigzag weights of J along each axis:
+# Jx is spread over (j, k), Jy over (i, k), Jz over (i, j)
+_ZZ_SPREAD = ((1, 2), (0, 2), (0, 1))
+
+
+def _zigzag_add(wrk: np.ndarray, b: list, a: list, rustep: float) -> None:
+    """One particle's zigzag current from b to a (psuper1.F90:859-988,
+    current_deposition) added into wrk[k + 4, j + 4, i + 4, comp] in the
+    reference's order (segment b -> relay point, then relay point -> a; per
+    segment the weights 1..4, each for x, y, z)."""
+    import math
+    ib = [math.floor(v) for v in b]
+    ia = [math.floor(v) for v in a]
+    r = [(b[d] + a[d]) * 0.5 if ib[d] == ia[d] else max(float(ib[d]), float(ia[d])) for d in range(3)]
+    for cell, dd, vv in ((ib, [(r[d] + b[d]) * 0.5 - float(ib[d]) for d in range(3)],
+                          [(r[d] - b[d]) * rustep for d in range(3)]),
+                         (ia, [(a[d] + r[d]) * 0.5 - float(ia[d]) for d in range(3)],
+                          [(a[d] - r[d]) * rustep for d in range(3)])):
+        w = []
+        for comp in range(3):
+            e1, e2 = _ZZ_SPREAD[comp]
+            w4 = dd[e1] * dd[e2]
+            w2 = dd[e1] - w4
+            w3 = dd[e2] - w4
+            w1 = 1.0 - dd[e1] - w3
+            w.append((w1, w2, w3, w4))
+        for q in range(4):
+            for comp in range(3):
+                e1, e2 = _ZZ_SPREAD[comp]
+                n = list(cell)
+                if q & 1:
+                    n[e1] += 1
+                if q & 2:
+                    n[e2] += 1
+                wrk[n[2] + 4, n[1] + 4, n[0] + 4, comp] += vv[comp] * w[comp][q]
+
+
+def inflow_current(axis: int, front: bool, rec: np.ndarray, ustep: int, ext: tuple,
+                   wrk: np.ndarray | None = None) -> np.ndarray:
+    """The injection current of psuper1 (psuper1.F90:120-323 with
+    current_deposition, :859-988) for records `rec` injected through the
+    lower (front) or upper face of `axis`, in order: the zigzag current of
+    the path from b to the injection point a, b outside the face (-1 below
+    the lower face, n + 0.99999999 above the upper one, along the normal;
+    a - v * ustep along the other axes), without the charge factor (the
+    reference's wrk(TJX:TJZ), added to aj times q).  Returns (or adds into)
+    wrk, numpy (nz + 9, ny + 9, nx + 9, 3) over the nodes -4..n+4 of each
+    axis."""
+    nx, ny, nz = ext
+    if wrk is None:
+        wrk = np.zeros((nz + 9, ny + 9, nx + 9, 3))
+    rustep = 1.0 / ustep
+    names = ("x", "y", "z")
+    for p in rec:
+        a = [float(p[c]) for c in names]
+        b = [a[d] - float(p["v" + names[d]]) * ustep for d in range(3)]
+        b[axis] = -1.0 if front else ext[axis] + 0.99999999
+        _zigzag_add(wrk, b, a, rustep)
+    return wrk
 
 
 def inflow_z(front: bool, n: int, nx: int, ny: int, nz: int, vz_table: np.ndarray, vx_table: np.ndarray,

@@ -348,6 +348,19 @@ int emsesg_fx_inflow_z(emsesg_ctx* ctx, int spec, int front, int64_t n, const do
  * emsesg_fx_inflow(..., 2, ..., vz_t, vx_t, vy_t, ...). */
 int emsesg_fx_inflow(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n, const double* vn_t, const double* va_t,
                      const double* vb_t, int npr, double injctisw, uint64_t seed, uint64_t stream, uint64_t index0);
+/* emsesg_fx_inflow_current: emsesg_fx_inflow with the injection current of
+ * psuper1 (replaces psuper1's outer-face blocks, src/pcl/psuper1.F90:120-323,
+ * and current_deposition, :859-988): each particle also deposits, times its
+ * species' charge, the zigzag current of its path from b outside the face
+ * (-1 below the lower face, n + 0.99999999 above the upper one, along the
+ * normal; its position minus v * ustep along the other axes) to its
+ * injection point, into the J of the next emsesg_fx_step (the step adds its
+ * own deposit to these currents instead of starting J from zero; the
+ * reference zeroes aj, runs psuper1, then psolve1).  Contributions are
+ * rounded to the int64 accumulator (scale 2^40) one by one. */
+int emsesg_fx_inflow_current(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n, const double* vn_t,
+                             const double* va_t, const double* vb_t, int npr, double injctisw, int ustep,
+                             uint64_t seed, uint64_t stream, uint64_t index0);
 /* emsesg_fx_emit_plane: n particles from a rectangular plane of body pid
  * (psuper2.F90:330-360 with emit_from_rectangular_surf, :554-576): six
  * uniforms each; normal speed ud * vnorm[int(npr*u0)], tangential
@@ -358,6 +371,32 @@ int emsesg_fx_inflow(emsesg_ctx* ctx, int spec, int axis, int front, int64_t n, 
 int emsesg_fx_emit_plane(emsesg_ctx* ctx, int spec, int nemd, double grd, const double* b1, const double* b2,
                          int64_t n, const double* vnorm, const double* vtang, int npr, double injctisw, int pid,
                          uint64_t seed, uint64_t stream, uint64_t index0);
+/* emsesg_fx_emit_cylinder: n particles from a face of a cylindrical body
+ * (replaces emit_from_cylinder with emit_from_circular_surf and
+ * emit_from_cylindrical_surf1/2/3, src/pcl/psuper3.F90:241-528).  align:
+ * the cylinder's axis (1..3); axis: its two axis coordinates as the
+ * reference's cylinder%axis; radius; omni: the reference's omniemit.
+ * |nemd| = align: the end cap at grd (normal ud * vnormf[int(npr u0)],
+ * tangential vtangf[int(npr u1)], vtangf[int(npr u2)], the point radius *
+ * runiform[int(npr u3)] from the axis at the angle 2 pi u4).  Other nemd:
+ * the side, between hl and hu along the axis: omni 0 and radius >= 1
+ * turns vnormc / vtangc by psicos[int(npr u2)] + psi, omni 0 and radius < 1
+ * by psi (five uniforms a particle), omni 1 by the azimuth 2 pi u2; psi is
+ * the reference's psizy / psizx / psixy for align 1 / 2 / 3.  Uniform c of
+ * particle k is the hash of index0 * 6 + per * k + c (per: 5 or 6), the
+ * flat RANU0(dranu, 6n) of the reference.  Each particle gives a record
+ * with preside 1 and, with anti (the reference's ncond <= 0), its
+ * anti-particle (preside -2) at the same place; the FP32 form counts
+ * anti-particles on box-body face cells only, so these are dropped.  The
+ * tables (npr entries each) are the species' vnormf, vtangf, runiform,
+ * vnormc, vtangc, psicos (inipin.F90:996-1097).  ctca_b200/inject.py
+ * (emit_cylinder) computes the same records on the host; they agree to the
+ * last bits of cos / sin. */
+int emsesg_fx_emit_cylinder(emsesg_ctx* ctx, int spec, int nemd, int align, double radius, const double* axis,
+                            int omni, double grd, double hl, double hu, double psi, int64_t n, const double* vnormf,
+                            const double* vtangf, const double* runiform, const double* vnormc,
+                            const double* vtangc, const double* psicos, int npr, int anti, uint64_t seed,
+                            uint64_t stream, uint64_t index0);
 /* Absorbed minus emitted particles per surface cell of the box bodies
  * (geotype 0/1, integer bounds), int64 [nspec][nsurf]: body by body, faces
  * -x,+x,-y,+y,-z,+z, each face's cells with its first tangential axis

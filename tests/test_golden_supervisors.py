@@ -99,3 +99,63 @@ def test_emission_count(gold):
     fluxes and ustep."""
     for istep, lstep, injct, fluxf, ustep, n in gold["count_rows"]:
         assert inject.emission_count(int(istep), int(lstep), fluxf, int(injct), int(ustep)) == int(n)
+
+
+def test_cylinder_emission(gold):
+    """psuper3's emission from cylinders (emit_from_cylinder with
+    emit_from_circular_surf and emit_from_cylindrical_surf1/2/3,
+    psuper3.F90:241-528): end caps and side surfaces of cylinders along x, y
+    and z, the three side kinds (radius >= 1, radius < 1 with five uniforms a
+    particle, omnidirectional), with and without anti-particles."""
+    n = int(gold["cyl_n"])
+    xl, xu, yl, yu, zl, zu = gold["cyl_bounds"]
+    psixy, psizx, psizy = gold["cyl_psi"]
+    along = {1: (xl, xu, psizy), 2: (yl, yu, psizx), 3: (zl, zu, psixy)}
+    tabs = {k: gold["cyl_" + k] for k in ("vnormf", "vtangf", "runiform", "vnormc", "vtangc", "psicos")}
+    u = gold["cyl_uniforms"]
+    out = []
+    for k, (align, radius, omni, ncond, nemd, grd) in enumerate(gold["cyl_cases"]):
+        hl, hu, psi = along[int(align)]
+        out.append(inject.emit_cylinder(int(nemd), int(align), radius, tuple(gold["cyl_axis"]), int(omni), grd, hl,
+                                        hu, psi, n, tabs, None, spec=1, uniforms=u[k * 6 * n:(k + 1) * 6 * n],
+                                        anti=int(ncond) <= 0))
+    got = np.concatenate(out)
+    want = gold["cyl_records"]
+    assert got.size == want.size
+    for f in KIN + ("preside", "spec", "pid", "nid"):
+        assert np.array_equal(got[f], want[f]), f
+
+
+def test_psuper1_inflow_current(gold):
+    """psuper1's outer-face inflow with its injection current
+    (psuper1.F90:120-323, current_deposition :859-988): the records of the
+    six faces and the zigzag current of every particle's path from outside
+    the face to its injection point, bit for bit."""
+    nx, ny, nz = (int(v) for v in gold["p1_ext"])
+    npr, ustep, injct, istep, lstep = (int(v) for v in gold["p1_setup"])
+    t = {k[7:]: gold[k] for k in gold if k.startswith("p1_tab_")}
+    faces = [("arrxf", 0, True, t["vxf"], t["vyr"], t["vzr"]), ("arrxb", 0, False, t["vxb"], t["vyr"], t["vzr"]),
+             ("arryf", 1, True, t["vyf"], t["vxr"], t["vzr"]), ("arryb", 1, False, t["vyb"], t["vxr"], t["vzr"]),
+             ("arrzf", 2, True, t["vzf"], t["vxr"], t["vyr"]), ("arrzb", 2, False, t["vzb"], t["vxr"], t["vyr"])]
+    u = gold["p1_uniforms"]
+    pos = 0
+    recs = []
+    wrk = np.zeros((nz + 9, ny + 9, nx + 9, 3))
+    for key, axis, front, vn, va, vb in faces:
+        n = inject.inflow_count(istep, lstep, float(gold["p1_arr_" + key]), injct, ustep)
+        assert n == int(gold["p1_count_" + key]), key
+        r = inject.inflow(axis, front, n, nx, ny, nz, vn, va, vb, float(injct * ustep), None, spec=1,
+                          uniforms=u[pos:pos + 5 * n].reshape(n, 5))
+        pos += 5 * n
+        inject.inflow_current(axis, front, r, ustep, (nx, ny, nz), wrk)
+        recs.append(r)
+    assert pos == u.size
+    got = np.concatenate(recs)
+    want = gold["p1_records"]
+    assert got.size == want.size > 0
+    for f in KIN + ("preside", "spec"):
+        assert np.array_equal(got[f], want[f]), f
+    # the fixture's wrk is (3, x, y, z) over the nodes -4..n+4
+    ref = np.transpose(gold["p1_wrk"], (3, 2, 1, 0))
+    assert np.count_nonzero(ref) > 0
+    assert np.array_equal(wrk.view(np.uint64), np.ascontiguousarray(ref).view(np.uint64))
