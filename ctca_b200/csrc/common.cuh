@@ -109,6 +109,14 @@ struct FxState {
   int64_t tailord_base[EMSESG_ISPEC] = {};  // offset of each species' tail in tailord
   int64_t pending[EMSESG_ISPEC] = {};  // injected particles still to take their random step
   bool inj_j_pending = false;          // the J accumulator holds injection currents for the next step
+  // slab mode (emsesg_fx_slab): records of the particles leaving through the
+  // z faces, [2 nspec][outbox_cap], and their counts
+  bool slab = false;
+  bool slab_open = false;              // between emsesg_fx_slab_begin and emsesg_fx_slab_end
+  emsesg_particle* outbox = nullptr;
+  emsesg_particle* outbox2 = nullptr;  // the sort of a region by source slot
+  unsigned long long* outbox_n = nullptr;
+  int64_t outbox_cap = 0;
   emsesg_particle* stage = nullptr;    // device staging of injected records
   int32_t* stage_ord = nullptr;
   int64_t stage_cap = 0;

@@ -502,6 +502,7 @@ void fx_free(emsesg_ctx* ctx) {
   cudaFreeHost(f.ord_host);
   if (f.ord_ev) cudaEventDestroy(f.ord_ev);
   cudaFree(f.inj_tab);
+  cudaFree(f.outbox); cudaFree(f.outbox2); cudaFree(f.outbox_n);
   if (f.gexec) cudaGraphExecDestroy(f.gexec);
   adj_free(f);
   f = FxState();
@@ -859,16 +860,19 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
 }
 
 namespace {
-// One step; without `deposit` the move only (no rho / J): for recomputing
-// particle states on a grid without bodies or injected particles.
-int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
+// The push of one step: grdcrt, the particles of the tile regions and of the
+// tail zones, into the zeroed int64 accumulators (the J of injection
+// currents kept); without `deposit` the move only (no rho / J), for
+// recomputing particle states on a grid without bodies or injected
+// particles.  In slab mode the particles leaving through the z faces go to
+// the outbox.
+int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit) {
   if (!ctx) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
   if (ustep < 1) return set_error(ctx, EMSESG_ERR_ARG, "ustep must be >= 1");
   const emsesg_config& c = ctx->cfg;
   std::string why;
   if (!bodies_supported(c, &why)) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "%s", why.c_str());
-  int rc;
   FxState& f = ctx->fx;
   Geo g = make_geo(ctx);
   int64_t nn = (int64_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
@@ -916,6 +920,10 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   a.bd = make_bodies(c);
   a.status = ctx->d_status;
   a.diag = ctx->d_diag;
+  if (f.slab && deposit) {
+    EMSESG_CUDA(ctx, cudaMemsetAsync(f.outbox_n, 0, 2 * EMSESG_ISPEC * sizeof(unsigned long long), ctx->stream));
+    a.ob = Outbox{f.outbox, f.outbox_n, f.outbox_cap};
+  }
   // row chunks of the tile regions: at most ntiles + rows / CHUNK_ROWS
   int64_t rows = 0;
   for (int is = 0; is < c.nspec; is++) rows = std::max(rows, (f.cap[is] + PUSH_THREADS - 1) / PUSH_THREADS);
@@ -929,8 +937,6 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
       EMSESG_LAUNCH(ctx, "fx_move", (k_fx_push<4, false>), grid, PUSH_BLOCK, smem, a);
     else
       EMSESG_LAUNCH(ctx, "fx_move", (k_fx_push<8, false>), grid, PUSH_BLOCK, smem, a);
-    ctx->rng_stream++;
-    if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
     return EMSESG_OK;
   }
   if (fx_box_tile(tmax) == 4)
@@ -949,12 +955,50 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   }
   if (drawn && c.rng_mode == 1) EMSESG_LAUNCH(ctx, "fx_rand_advance", k_add_i64, 1, 1, 0, ctx->d_rand_pos, drawn);
   if (a.bd.n > 0) EMSESG_LAUNCH(ctx, "fx_chgacm", k_fx_chgacm, 1, 32, 0, ctx->d_cfg, ctx->d_counter);
-  // guard folding on the exact integers, then FP64 outputs
-  if ((rc = run_slab_ops2(ctx, (long long*)acc_rho, fr, fold_ops(c, 0, 1), (long long*)acc_j, fj,
-                          fold_ops(c, 1, 3), "fx_fold")))
-    return rc;
-  // J first: the conversion of rho takes the continuity residual of the step
-  // against the rho field of the step before (still in place) and this J
+  return EMSESG_OK;
+}
+
+// The fold lists of rho and J split for slab mode: the border exchange of
+// the x and y axes (run by emsesg_fx_slab_begin, before the ranks exchange
+// their z border planes) and the rest (run by emsesg_fx_slab_end).  Without
+// slab mode the whole lists.
+void fold_lists(const emsesg_config& c, bool slab, int part, std::vector<SlabOp>* rho, std::vector<SlabOp>* j) {
+  for (int kind = 0; kind < 2; kind++) {
+    std::vector<SlabOp> all = fold_ops(c, kind, kind == 0 ? 1 : 3);
+    std::vector<SlabOp>& out = kind == 0 ? *rho : *j;
+    out.clear();
+    if (!slab) {
+      out = all;
+      continue;
+    }
+    int nex = 0;  // the exchange copies come first, two per periodic axis
+    for (int d = 0; d < 3; d++)
+      if (c.nfbnd[d] == 0) nex += 2;
+    for (int q = 0; q < (int)all.size(); q++) {
+      const bool exchange = q < nex;
+      if (part == 0 && exchange && all[q].axis != 2) out.push_back(all[q]);
+      if (part == 1 && !exchange) out.push_back(all[q]);
+    }
+  }
+}
+
+// The rest of a step after its push (and, in slab mode, the exchange of the
+// z border planes and the arrivals): guard folds on the exact integers,
+// FP64 rho and J (J first: the conversion of rho takes the continuity
+// residual of the step against the rho field of the step before, still in
+// place, and this J), then the re-sort after the push (so that injected
+// particles take their first, partial step before they join the tile
+// regions).
+int fx_finish_phase(emsesg_ctx* ctx, int do_sort) {
+  FxState& f = ctx->fx;
+  const emsesg_config& c = ctx->cfg;
+  FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
+  unsigned long long* acc_rho = (unsigned long long*)f.accum;
+  unsigned long long* acc_j = acc_rho + fr.size();
+  std::vector<SlabOp> orho, oj;
+  fold_lists(c, f.slab, 1, &orho, &oj);
+  int rc;
+  if ((rc = run_slab_ops2(ctx, (long long*)acc_rho, fr, orho, (long long*)acc_j, fj, oj, "fx_fold"))) return rc;
   EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_double, nblk(fj.size()), 256, 0, (const long long*)acc_j,
                 ctx->field[EMSESG_FIELD_AJ], fj.size());
   unsigned long long* cres = (unsigned long long*)(f.diag + 3 * DIAG_GRID + 3);
@@ -964,10 +1008,23 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   f.cont_valid = f.rho_prev;
   f.rho_prev = true;
   ctx->rng_stream++;
-  // the re-sort after the push (so that injected particles take their
-  // first, partial step before they join the tile regions)
   if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
   return EMSESG_OK;
+}
+
+// One step; without `deposit` the move only (no rho / J): for recomputing
+// particle states on a grid without bodies or injected particles.
+int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
+  if (ctx && ctx->fx.slab && deposit)
+    return set_error(ctx, EMSESG_ERR_STATE, "slab mode: steps are emsesg_fx_slab_begin / _arrive / _end");
+  int rc = fx_push_phase(ctx, ustep, deposit);
+  if (rc) return rc;
+  if (!deposit) {
+    ctx->rng_stream++;
+    if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
+    return EMSESG_OK;
+  }
+  return fx_finish_phase(ctx, do_sort);
 }
 }  // namespace
 
@@ -1329,6 +1386,194 @@ int inject_check(emsesg_ctx* ctx, int spec, int64_t n, int npr, const void* t0, 
 
 }  // namespace
 }  // namespace emsesg
+
+namespace emsesg {
+namespace {
+// The charge of particles that arrived from a neighbouring slab (tail slots
+// s0 .. s0 + n - 1 of a species region): the CIC weights of the push
+// (charge.F90:152-210) at their FP32 offsets, into the int64 rho.
+__global__ void k_fx_rho_arrivals(const float4* __restrict__ pos, int64_t s0, int64_t n, Sink sk, Geo g,
+                                  float qfix) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const float4 ps = pos[s0 + k];
+  const uint32_t cell = (uint32_t)__float_as_int(ps.w);
+  if (cell == DEAD) return;
+  int i, j, kk;
+  unpack(g, cell, i, j, kk);
+  const float X = ps.x, Y = ps.y, Z = ps.z;
+  const float XY = X * Y, XZ = X * Z, YZ = Y * Z, Z2 = 1.0f - Z, XZ2 = X * Z2, YZ2 = Y * Z2;
+  V8 R;
+  R.v[2] = XY * Z; R.v[1] = XZ - R.v[2]; R.v[3] = YZ - R.v[2]; R.v[0] = Z - XZ - R.v[3];
+  R.v[6] = XY * Z2; R.v[5] = XZ2 - R.v[6]; R.v[7] = YZ2 - R.v[6]; R.v[4] = Z2 - XZ2 - R.v[7];
+  put_r_global(sk, i, j, kk, R, qfix);
+}
+
+// keys = source slot (pid), vals = record index, of one outbox region.
+__global__ void k_outbox_keys(const emsesg_particle* __restrict__ rec, int64_t n, uint32_t* keys, uint32_t* vals) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  keys[k] = (uint32_t)rec[k].pid;
+  vals[k] = (uint32_t)k;
+}
+
+__global__ void k_outbox_gather(const emsesg_particle* __restrict__ rec, const uint32_t* __restrict__ idx, int64_t n,
+                                emsesg_particle* out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  out[k] = rec[idx[k]];
+}
+
+// The z border planes of rho (kind 0) and J (kind 1) that slab mode
+// exchanges, as the border exchange of oh3_exchange_borders for the types of
+// src/wrapper/ohinit.F90:113-118 (rho: from 0 / to n+1 and from n / to -1,
+// one plane each way; J: from -1..1 / to n+2..n+4 and from n-1..n+1 /
+// to -4..-2): which 0 the planes sent down, 1 sent up, 2 received from
+// below, 3 received from above.
+void slab_plane_range(int kind, int which, int nz, int* k0, int* depth) {
+  const int fromL = kind == 0 ? 0 : -1, toL = kind == 0 ? 1 : 2, sizeL = kind == 0 ? 1 : 3;
+  const int fromU = kind == 0 ? 0 : -1, toU = kind == 0 ? -1 : -4, sizeU = kind == 0 ? 1 : 3;
+  if (which == 0) { *k0 = fromL; *depth = sizeL; }
+  else if (which == 1) { *k0 = nz + fromU; *depth = sizeU; }
+  else if (which == 2) { *k0 = toU; *depth = sizeU; }
+  else { *k0 = nz + toL; *depth = sizeL; }
+}
+}  // namespace
+}  // namespace emsesg
+
+extern "C" int emsesg_fx_slab(emsesg_ctx* ctx, int on, int64_t outbox_cap) {
+  if (!ctx || (on && outbox_cap < 1)) return EMSESG_ERR_ARG;
+  FxState& f = ctx->fx;
+  if (!f.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
+  if (f.slab_open) return set_error(ctx, EMSESG_ERR_STATE, "slab step open (emsesg_fx_slab_end first)");
+  const emsesg_config& c = ctx->cfg;
+  cudaFree(f.outbox); cudaFree(f.outbox2); cudaFree(f.outbox_n);
+  f.outbox = f.outbox2 = nullptr;
+  f.outbox_n = nullptr;
+  f.outbox_cap = 0;
+  f.slab = false;
+  if (!on) return EMSESG_OK;
+  for (int is = 0; is < c.nspec; is++)
+    if (c.npbnd[is][2] != 0) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "slab mode: periodic z particles only");
+  if (c.nfbnd[2] != 0) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "slab mode: periodic z fields only");
+  if (c.npc > 0 && c.line_mode != 1) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "slab mode: no bodies");
+  EMSESG_CUDA(ctx, cudaMalloc(&f.outbox, (size_t)2 * c.nspec * outbox_cap * sizeof(emsesg_particle)));
+  EMSESG_CUDA(ctx, cudaMalloc(&f.outbox2, (size_t)outbox_cap * sizeof(emsesg_particle)));
+  EMSESG_CUDA(ctx, cudaMalloc(&f.outbox_n, 2 * EMSESG_ISPEC * sizeof(unsigned long long)));
+  f.outbox_cap = outbox_cap;
+  f.slab = true;
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_fx_slab_begin(emsesg_ctx* ctx, int ustep, int64_t* counts) {
+  if (!ctx || !counts) return EMSESG_ERR_ARG;
+  FxState& f = ctx->fx;
+  if (!f.slab) return set_error(ctx, EMSESG_ERR_STATE, "not in slab mode (emsesg_fx_slab)");
+  if (f.slab_open) return set_error(ctx, EMSESG_ERR_STATE, "slab step already open");
+  const emsesg_config& c = ctx->cfg;
+  int rc = fx_push_phase(ctx, ustep, true);
+  if (rc) return rc;
+  unsigned long long n[2 * EMSESG_ISPEC];
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(n, f.outbox_n, sizeof(n), cudaMemcpyDeviceToHost, ctx->stream));
+  EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int q = 0; q < 2 * c.nspec; q++)
+    if ((int64_t)n[q] > f.outbox_cap)
+      return set_error(ctx, EMSESG_ERR_OVERFLOW, "slab outbox %d: %llu particles left, room for %lld", q,
+                       (unsigned long long)n[q], (long long)f.outbox_cap);
+  // each region in the order of the particles' slots (the atomics of the
+  // push leave it in any order)
+  int64_t slots = 1;
+  for (int is = 0; is < c.nspec; is++) slots = std::max(slots, f.base[is] + f.cap[is]);
+  int bits = 1;
+  while (bits < 32 && (1LL << bits) < slots) bits++;
+  for (int q = 0; q < 2 * c.nspec; q++) {
+    counts[q] = (int64_t)n[q];
+    if (n[q] < 2) continue;
+    emsesg_particle* reg = f.outbox + (int64_t)q * f.outbox_cap;
+    if ((rc = ensure_sort_scratch(ctx, (int64_t)n[q]))) return rc;
+    EMSESG_LAUNCH(ctx, "slab_keys", k_outbox_keys, nblk((int64_t)n[q]), 256, 0, reg, (int64_t)n[q],
+                  ctx->sort.keys[0], ctx->sort.vals[0]);
+    uint32_t *ko, *vo;
+    if ((rc = sort_pairs(ctx, ctx->sort.keys[0], ctx->sort.vals[0], (int64_t)n[q], bits, &ko, &vo))) return rc;
+    EMSESG_LAUNCH(ctx, "slab_gather", k_outbox_gather, nblk((int64_t)n[q]), 256, 0, reg, vo, (int64_t)n[q],
+                  f.outbox2);
+    EMSESG_CUDA(ctx, cudaMemcpyAsync(reg, f.outbox2, n[q] * sizeof(emsesg_particle), cudaMemcpyDeviceToDevice,
+                                     ctx->stream));
+  }
+  EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  f.slab_open = true;
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_fx_slab_outbox(emsesg_ctx* ctx, int spec, int dir, emsesg_particle** dev) {
+  if (!ctx || !dev || dir < 0 || dir > 1) return EMSESG_ERR_ARG;
+  FxState& f = ctx->fx;
+  if (!f.slab) return set_error(ctx, EMSESG_ERR_STATE, "not in slab mode (emsesg_fx_slab)");
+  if (spec < 1 || spec > ctx->cfg.nspec) return set_error(ctx, EMSESG_ERR_ARG, "species %d out of range", spec);
+  *dev = f.outbox + (int64_t)(2 * (spec - 1) + dir) * f.outbox_cap;
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_fx_slab_planes(emsesg_ctx* ctx, int which, int64_t** rho, int64_t* nrho, int64_t** j,
+                                     int64_t* nj) {
+  if (!ctx || !rho || !nrho || !j || !nj || which < 0 || which > 3) return EMSESG_ERR_ARG;
+  FxState& f = ctx->fx;
+  if (!f.slab) return set_error(ctx, EMSESG_ERR_STATE, "not in slab mode (emsesg_fx_slab)");
+  const emsesg_config& c = ctx->cfg;
+  FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
+  int k0, depth;
+  slab_plane_range(0, which, c.nz, &k0, &depth);
+  *rho = f.accum + fr.at(0, fr.lo, fr.lo, k0);
+  *nrho = (int64_t)depth * fr.nc * fr.ex * fr.ey;
+  slab_plane_range(1, which, c.nz, &k0, &depth);
+  *j = f.accum + fr.size() + fj.at(0, fj.lo, fj.lo, k0);
+  *nj = (int64_t)depth * fj.nc * fj.ex * fj.ey;
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_fx_slab_arrive(emsesg_ctx* ctx, int spec, const emsesg_particle* dev, int64_t n) {
+  if (!ctx || n < 0 || (n > 0 && !dev)) return EMSESG_ERR_ARG;
+  FxState& f = ctx->fx;
+  if (!f.slab_open) return set_error(ctx, EMSESG_ERR_STATE, "no slab step open (emsesg_fx_slab_begin)");
+  const int is = spec - 1;
+  if (is < 0 || is >= ctx->cfg.nspec) return set_error(ctx, EMSESG_ERR_ARG, "species %d out of range", spec);
+  if (n == 0) return EMSESG_OK;
+  int rc = inject_reserve(ctx, is, n);
+  if (rc) return rc;
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(f.stage, dev, n * sizeof(emsesg_particle), cudaMemcpyDeviceToDevice, ctx->stream));
+  EMSESG_CUDA(ctx, cudaMemsetAsync(f.stage_ord, 0, n * sizeof(int32_t), ctx->stream));
+  const int64_t s0 = f.base[is] + f.tail0[is] + f.ntail[is];
+  if ((rc = inject_staged(ctx, is, n, f.pending[is]))) return rc;
+  const emsesg_config& c = ctx->cfg;
+  FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
+  unsigned long long* acc_rho = (unsigned long long*)f.accum;
+  const Sink sk{acc_rho, acc_rho + fr.size(), fr, fj, c.nx, c.ny, c.nz, ctx->d_status, ctx->d_diag};
+  EMSESG_LAUNCH(ctx, "slab_rho_arrivals", k_fx_rho_arrivals, nblk(n), 256, 0, f.pos, s0, n, sk, make_geo(ctx),
+                (float)(c.q[is] * 1099511627776.0));
+  return EMSESG_OK;
+}
+
+extern "C" int emsesg_fx_slab_border(emsesg_ctx* ctx) {
+  if (!ctx) return EMSESG_ERR_ARG;
+  FxState& f = ctx->fx;
+  if (!f.slab_open) return set_error(ctx, EMSESG_ERR_STATE, "no slab step open (emsesg_fx_slab_begin)");
+  const emsesg_config& c = ctx->cfg;
+  FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
+  unsigned long long* acc_rho = (unsigned long long*)f.accum;
+  std::vector<SlabOp> orho, oj;
+  fold_lists(c, true, 0, &orho, &oj);
+  int rc = run_slab_ops2(ctx, (long long*)acc_rho, fr, orho, (long long*)(acc_rho + fr.size()), fj, oj, "fx_fold");
+  if (rc) return rc;
+  return emsesg_synchronize(ctx);
+}
+
+extern "C" int emsesg_fx_slab_end(emsesg_ctx* ctx, int do_sort) {
+  if (!ctx) return EMSESG_ERR_ARG;
+  FxState& f = ctx->fx;
+  if (!f.slab_open) return set_error(ctx, EMSESG_ERR_STATE, "no slab step open (emsesg_fx_slab_begin)");
+  f.slab_open = false;
+  return fx_finish_phase(ctx, do_sort);
+}
 
 extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int64_t n) {
   if (!ctx || n < 0 || (n > 0 && !host)) return EMSESG_ERR_ARG;

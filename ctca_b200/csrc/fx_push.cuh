@@ -67,6 +67,19 @@ struct Bodies {
   int64_t nsurf;                // surface cells of all bodies
 };
 
+// Slab mode (the grid is one z slab of a larger grid, periodic in z, cut
+// into slabs of equal thickness): particles that leave through a z face go
+// to the neighbouring slab's rank.  Their records, in that rank's frame (the
+// periodic wrap of this slab), per species and direction: region
+// (2 is + dir) of cap records, dir 0 through z = 0, 1 through z = nz.  pid
+// holds the particle's slot here (the order of the records is then made
+// independent of the atomics).
+struct Outbox {
+  emsesg_particle* rec;         // null: not in slab mode
+  unsigned long long* count;    // [2 nspec]
+  int64_t cap;
+};
+
 struct FxPushArgs {
   float4* pos;                  // all species regions (the step's result)
   float* vx;
@@ -94,6 +107,7 @@ struct FxPushArgs {
   emsesg_counter* gc;           // influx / infhist of the body absorption
   unsigned long long* surf;     // [nspec][nsurf] absorbed - emitted counts
   Bodies bd;
+  Outbox ob;
   int* status;
   long long* diag;
 };
@@ -461,6 +475,9 @@ struct CrossCtx {
   emsesg_counter* gc;
   unsigned long long* surf;     // this species' surface counts
   int is;
+  int64_t slot_base;            // slot of gpos[0] in the particle arrays
+  const Outbox* ob;
+  int* status;
 };
 
 // Box absorption of the end point a = (ac, af) per axis (psolve1.F90:
@@ -541,7 +558,28 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
     const Axis a3[3] = {ax, ay, az};
     absorbed = body_absorb(c, ib3, ob3, a3);
   }
-  const bool dead = escaped || absorbed;
+  // slab mode: a particle leaving through a z face moves to the neighbouring
+  // slab (its stored position, the slab's periodic wrap, is its position
+  // there); its current stays here, in the guard planes that the ranks
+  // exchange and fold, and its charge is deposited by the receiver
+  const bool migrant = c.ob != nullptr && az.crossed && !escaped && !absorbed;
+  if (migrant) {
+    const int dir = az.ac < 0 ? 0 : 1;
+    const unsigned long long q = atomicAdd(&c.ob->count[2 * c.is + dir], 1ull);
+    if (q < (unsigned long long)c.ob->cap) {
+      emsesg_particle r;
+      r.x = (double)ax.nc + (double)ax.nf;
+      r.y = (double)ay.nc + (double)ay.nf;
+      r.z = (double)az.nc + (double)az.nf;
+      r.vx = vx; r.vy = vy; r.vz = vz;
+      r.pid = (int32_t)(c.slot_base + loc);
+      r.preside = 0; r.nid = 0; r.spec = c.is + 1;
+      c.ob->rec[(int64_t)(2 * c.is + dir) * c.ob->cap + (int64_t)q] = r;
+    } else {
+      atomicOr(c.status, ST_OVERFLOW);
+    }
+  }
+  const bool dead = escaped || absorbed || migrant;
   const uint32_t nc = dead ? DEAD : pack(g, ax.nc, ay.nc, az.nc);
   c.gpos[loc] = make_float4(ax.nf, ay.nf, az.nf, __int_as_float((int)nc));
   c.gvx[loc] = vx;
@@ -611,7 +649,7 @@ __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t s
   const Sink sk{a.acc_rho, a.acc_j, a.fr, a.fj, g.nx, g.ny, g.nz, a.status, a.diag};
   const CrossCtx c{a.pos + slot0, a.vx + slot0, a.vy + slot0, a.vz + slot0, a.gustep, a.rustep, a.qfix[is],
                    {a.npbnd[is][0], a.npbnd[is][1], a.npbnd[is][2]}, &a.bd, a.gc,
-                   a.surf + (int64_t)is * a.bd.nsurf, is};
+                   a.surf + (int64_t)is * a.bd.nsurf, is, slot0, a.ob.rec ? &a.ob : nullptr, a.status};
   int dead = 0;
   for (int e = lane; e < xn; e += 32) {
     const int loc = xl[e];
@@ -1064,7 +1102,7 @@ __global__ void k_fx_tail(FxPushArgs a, int is, int64_t tail0, int64_t ntail, in
   const Sink sk{a.acc_rho, a.acc_j, a.fr, a.fj, g.nx, g.ny, g.nz, a.status, a.diag};
   const CrossCtx c{a.pos + base, a.vx + base, a.vy + base, a.vz + base, gus, a.rustep, a.qfix[is],
                    {a.npbnd[is][0], a.npbnd[is][1], a.npbnd[is][2]}, &a.bd, a.gc,
-                   a.surf + (int64_t)is * a.bd.nsurf, is};
+                   a.surf + (int64_t)is * a.bd.nsurf, is, base, a.ob.rec ? &a.ob : nullptr, a.status};
   const float en[XQW] = {__int_as_float((int)slot), ps.w, ps.x, ps.y, ps.z, vx, vy, vz};
   const int far[3] = {-(1 << 28), -(1 << 28), -(1 << 28)};  // no box: global deposits
   const int esc = cross_one<11>(g, nullptr, far, sk, c, en);

@@ -132,6 +132,14 @@ _SIGS = {
     "emsesg_fx_step": (_I, [_P, _I, _I]),
     "emsesg_fx_sort": (_I, [_P]),
     "emsesg_fx_run": (_I, [_P, _I, _I, _I, _I]),
+    "emsesg_fx_slab": (_I, [_P, _I, ctypes.c_int64]),
+    "emsesg_fx_slab_begin": (_I, [_P, _I, _P]),
+    "emsesg_fx_slab_outbox": (_I, [_P, _I, _I, ctypes.POINTER(ctypes.c_void_p)]),
+    "emsesg_fx_slab_planes": (_I, [_P, _I, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64),
+                                   ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64)]),
+    "emsesg_fx_slab_arrive": (_I, [_P, _I, ctypes.c_void_p, ctypes.c_int64]),
+    "emsesg_fx_slab_border": (_I, [_P]),
+    "emsesg_fx_slab_end": (_I, [_P, _I]),
     "emsesg_batch_create": (_I, [_P, _I, _I, _I, _P, ctypes.POINTER(_P)]),
     "emsesg_batch_launch": (_I, [_P, _I]),
     "emsesg_batch_stream": (_P, [_P]),
@@ -382,6 +390,46 @@ class Emses:
 
     def fx_step(self, ustep: int = 2, do_sort: bool = False):
         self._check(self.lib.emsesg_fx_step(self.h, ustep, 1 if do_sort else 0))
+
+    # -- slab mode (a z slab of a decomposed grid; ctca_b200/slabs.py)
+    def fx_slab(self, on: bool, outbox_cap: int = 0):
+        self._check(self.lib.emsesg_fx_slab(self.h, 1 if on else 0, outbox_cap))
+
+    def fx_slab_begin(self, ustep: int = 2) -> np.ndarray:
+        """The push of a slab step; returns the particles leaving, [spec, dir]."""
+        out = np.zeros(2 * ISPEC, dtype=np.int64)
+        self._check(self.lib.emsesg_fx_slab_begin(self.h, ustep, out.ctypes.data))
+        return out[:2 * self.cfg.nspec].reshape(self.cfg.nspec, 2)
+
+    def fx_slab_outbox(self, spec: int, direction: int) -> int:
+        """Device address of the outbox records of species spec, direction 0
+        (through z = 0) or 1 (through z = nz)."""
+        ptr = ctypes.c_void_p(0)
+        self._check(self.lib.emsesg_fx_slab_outbox(self.h, spec, direction, ctypes.byref(ptr)))
+        return ptr.value or 0
+
+    def fx_slab_planes(self, which: int) -> tuple[int, int, int, int]:
+        """(rho address, rho int64 count, J address, J int64 count) of the z
+        border planes: which 0 sent down, 1 sent up, 2 received from below,
+        3 received from above."""
+        pr, pj = ctypes.c_void_p(0), ctypes.c_void_p(0)
+        nr, nj = ctypes.c_int64(0), ctypes.c_int64(0)
+        self._check(self.lib.emsesg_fx_slab_planes(self.h, which, ctypes.byref(pr), ctypes.byref(nr),
+                                                   ctypes.byref(pj), ctypes.byref(nj)))
+        return pr.value or 0, nr.value, pj.value or 0, nj.value
+
+    def fx_slab_arrive(self, spec: int, dev_ptr: int, n: int):
+        """Particles of species spec arriving from a neighbouring slab
+        (n records at a device address)."""
+        self._check(self.lib.emsesg_fx_slab_arrive(self.h, spec, ctypes.c_void_p(dev_ptr), n))
+
+    def fx_slab_border(self):
+        """The x / y border exchange of a slab step (after the arrivals,
+        before the z border planes go to the neighbours)."""
+        self._check(self.lib.emsesg_fx_slab_border(self.h))
+
+    def fx_slab_end(self, do_sort: bool = False):
+        self._check(self.lib.emsesg_fx_slab_end(self.h, 1 if do_sort else 0))
 
     def fx_run(self, ustep: int, nsteps: int, sort_every: int, use_graph: bool = True):
         """nsteps steps, re-sort every sort_every, replayed from a CUDA graph."""

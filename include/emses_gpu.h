@@ -260,9 +260,6 @@ int emsesg_fx_load(emsesg_ctx* ctx);
  * the current buffer order; particles that died since the last sort come
  * out in place with nid = -1. */
 int emsesg_fx_store(emsesg_ctx* ctx);
-/* One step: FP32 field relocation (grdcrt), push, zigzag J and CIC rho into
- * the fixed-point accumulators, guard folding, FP64 rho/aj outputs.  Sorts
- * (and compacts) first when do_sort != 0. */
 /* One step of the FP32 form: push of the tile regions and of the tail zone,
  * zigzag J and CIC rho into int64 fixed point, guard folds, FP64 rho / aj;
  * with do_sort, the re-sort after the push. */
@@ -280,6 +277,44 @@ int emsesg_fx_sort(emsesg_ctx* ctx);
  * tail zone, or an unsorted layout, make it run step by step.  Asynchronous
  * on the context's stream. */
 int emsesg_fx_run(emsesg_ctx* ctx, int ustep, int nsteps, int sort_every, int use_graph);
+
+/* Domain decomposition in z slabs (replaces, for slabs of one periodic z
+ * axis, OhHelp's particle migration, oh2_transbound / exchange_particles,
+ * lib/ohhelp/ohhelp-1.1.1/ohhelp2.c:103-123, 333-384, and the border
+ * exchange of oh3_exchange_borders, ohhelp3.c:959-1046, between ranks).
+ * The context's grid is one slab of nz cells of a grid cut into slabs of
+ * equal thickness; its eb holds the slab's field with its guards.
+ * emsesg_fx_slab(ctx, 1, cap) turns slab mode on (periodic z particles and
+ * fields, no bodies; cap: room for the particles leaving a slab through one
+ * face per species and step).  A step is then
+ *   emsesg_fx_slab_begin(ctx, ustep, counts): the push; particles leaving
+ *     through z = 0 / z = nz go to the outbox of direction 0 / 1 (their
+ *     positions in the neighbour's frame, their current in this slab's
+ *     guard planes), counts[2 (spec - 1) + dir] of them, in the order of
+ *     their slots; synchronous;
+ *   the exchange of particles: the outbox of direction 1 of a rank goes to
+ *     the rank above, direction 0 to the rank below (emsesg_fx_slab_outbox
+ *     gives its device address);
+ *   emsesg_fx_slab_arrive(ctx, spec, dev, n), for the particles from below,
+ *     then from above: into the tail zone, their charge into rho;
+ *   emsesg_fx_slab_border(ctx): the x / y border exchange of rho and J (the
+ *     z border planes then hold what goes to the neighbours); synchronous;
+ *   the exchange of planes: the z border planes of the int64 rho and J
+ *     accumulators (emsesg_fx_slab_planes: which 0 / 1 the planes sent
+ *     down / up, 2 / 3 the planes that receive them from below / above,
+ *     device addresses and counts of int64) are copied from the sending
+ *     planes of the neighbours;
+ *   emsesg_fx_slab_end(ctx, do_sort): the guard folds (z, y, x), FP64 rho
+ *     and aj, with do_sort the re-sort.
+ * The nodes 0..nz of each slab then hold what one grid of all slabs holds
+ * on them (rho and J as sums of the same int64 contributions). */
+int emsesg_fx_slab(emsesg_ctx* ctx, int on, int64_t outbox_cap);
+int emsesg_fx_slab_begin(emsesg_ctx* ctx, int ustep, int64_t* counts);
+int emsesg_fx_slab_outbox(emsesg_ctx* ctx, int spec, int dir, emsesg_particle** dev);
+int emsesg_fx_slab_planes(emsesg_ctx* ctx, int which, int64_t** rho, int64_t* nrho, int64_t** j, int64_t* nj);
+int emsesg_fx_slab_arrive(emsesg_ctx* ctx, int spec, const emsesg_particle* dev, int64_t n);
+int emsesg_fx_slab_border(emsesg_ctx* ctx);
+int emsesg_fx_slab_end(emsesg_ctx* ctx, int do_sort);
 
 /* Ensembles (no counterpart in the reference, which runs one job per run):
  * one CUDA graph holding `block` steps of each of n independent runs
