@@ -30,6 +30,12 @@ of side 16..64 in one CUDA graph) against the same runs launched one after
 the other.  --workload ensemble prints the full ensemble line instead
 (512 runs x 200 steps by default).
 
+--workload slabs runs the headline plasma on a grid cut into z slabs
+(ctca_b200/slabs.py): with torchrun and N GPUs one 128^3 slab per GPU
+(128 x 128 x 128N cells, weak scaling) exchanging the particles that change
+slab and the border planes of rho and J over NCCL every step; on one GPU two
+slabs of half the grid in one process against the grid as one context.
+
 --impl reference times the reference's CPU path (the oracle restatement of
 psolve1 + charge; the Fortran reference cannot be built here) on the host
 cores, on a bounded sample of the same workload.
@@ -556,6 +562,124 @@ def run_ours(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
+def run_slabs_line(args, world, rank, local):
+    """The headline plasma on a grid cut into z slabs (ctca_b200/slabs.py):
+    with N GPUs one 128^3 slab per GPU, a grid of 128 x 128 x 128N (weak
+    scaling), the particles that change slab and the z border planes of rho
+    and J exchanged every step over NCCL (device to device); on one GPU two
+    slabs of 128 x 128 x 64 in one process, against the same grid as one
+    context (what the decomposition itself costs).  Each slab draws its
+    plasma on its device (its own seed)."""
+    import torch
+    from ctca_b200 import inputs, slabs
+    from ctca_b200.emses import Emses, select_device
+    torch.cuda.set_device(local)
+    select_device(local)
+    case = headline_case(args.cells, args.ppc)
+    nslab = max(world, 2)
+    nzs = case.n[2] if world > 1 else case.n[2] // 2
+    gcase = headline_case(args.cells, args.ppc)
+    gcase.n = (case.n[0], case.n[1], nzs * nslab)
+    cfg = inputs.make_config(gcase)
+    eb = inputs.make_fields(gcase)
+    sub = slabs.slab_config(cfg, nslab)
+    ppc = sum(s.ppc for s in case.species)
+    outbox = max(1 << 16, case.n[0] * case.n[1] * ppc // 4)
+    steps, warm = args.steps, max(3, args.warmup)
+
+    def slab_plasma(r):
+        scase = headline_case(args.cells, args.ppc)
+        scase.n = (case.n[0], case.n[1], nzs)
+        return inputs.plasma(scase, seed=case.seed + 7919 * (r + 1))
+
+    if world == 1:
+        grp = slabs.SlabGroup(cfg, eb, None, None, nslab, outbox, plasmas=[slab_plasma(r) for r in range(nslab)])
+        npart = int(grp.counts().sum())
+        for s in range(warm):
+            grp.step(2, s % SORT_EVERY == SORT_EVERY - 1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for s in range(steps):
+            grp.step(2, (warm + s) % SORT_EVERY == SORT_EVERY - 1)
+        torch.cuda.synchronize()
+        e1.record()
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        moved = grp.migrated
+        grp.close()
+        # the same grid as one context
+        w = Emses(cfg)
+        w.load_plasma(inputs.plasma(gcase, seed=case.seed + 7919))
+        w.upload_field("eb", eb)
+        w.fx_load()
+        for s in range(warm):
+            w.fx_step(2, s % SORT_EVERY == SORT_EVERY - 1)
+        st = torch.cuda.ExternalStream(w.stream)
+        w.synchronize()
+        e0.record(st)
+        for s in range(steps):
+            w.fx_step(2, (warm + s) % SORT_EVERY == SORT_EVERY - 1)
+        e1.record(st)
+        e1.synchronize()
+        tw = e0.elapsed_time(e1) / 1e3
+        nw = int(w.fx_counts().sum())
+        w.close()
+        value = npart * steps / t
+        line = {"metric": "slab decomposition particle-steps/s", "value": value, "unit": UNIT, "n_gpus": 1,
+                "steps": steps, "warmup": warm, "ms_per_step": t / steps * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64", "data": "synthetic",
+                "config": {"workload": f"{gcase.n[0]}x{gcase.n[1]}x{gcase.n[2]} periodic cut into {nslab} z "
+                                       f"slabs on one GPU, 2 species x {case.species[0].ppc} ppc "
+                                       f"({npart:,} particles), sort every 4",
+                           "parallelism": f"{nslab} slabs, one process"},
+                "whole_grid": {"value": nw * steps / tw, "ms_per_step": tw / steps * 1e3},
+                "decomposed_over_whole": (value / (nw * steps / tw)),
+                "changed_slab_per_step": (moved / (steps + warm))}
+        print(json.dumps(line), flush=True)
+        return
+    import torch.distributed as dist
+    nccl = dist.new_group(backend="nccl")
+    g = Emses(sub)
+    g.load_plasma(slab_plasma(rank))
+    g.upload_field("eb", slabs.slab_field(cfg, eb, "eb", rank, nslab))
+    g.fx_load()
+    g.fx_slab(True, outbox)
+    io = slabs.ContextIO(g)
+    n_local = int(g.fx_counts().sum())
+    for s in range(warm):
+        slabs.exchange_step(io, dist, nccl, rank, world, 2, s % SORT_EVERY == SORT_EVERY - 1)
+    st = torch.cuda.ExternalStream(g.stream)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    moved = 0
+    for s in range(steps):
+        moved += int(slabs.exchange_step(io, dist, nccl, rank, world, 2,
+                                         (warm + s) % SORT_EVERY == SORT_EVERY - 1).sum())
+    e1.record(st)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    t = max_over_ranks(world, e0.elapsed_time(e1) / 1e3)
+    cnt = torch.tensor([float(n_local), float(moved)], dtype=torch.float64)
+    dist.all_reduce(cnt)
+    g.close()
+    dist.destroy_process_group(nccl)
+    if rank == 0:
+        npart, moved_all = int(cnt[0].item()), int(cnt[1].item())
+        print(json.dumps({"metric": "slab decomposition particle-steps/s", "value": npart * steps / t, "unit": UNIT,
+                          "n_gpus": world, "steps": steps, "warmup": warm, "ms_per_step": t / steps * 1e3,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64",
+                          "data": "synthetic",
+                          "config": {"workload": f"{gcase.n[0]}x{gcase.n[1]}x{gcase.n[2]} periodic, one "
+                                                 f"{case.n[0]}x{case.n[1]}x{nzs} z slab per GPU, 2 species x "
+                                                 f"{case.species[0].ppc} ppc ({npart:,} particles), sort every 4",
+                                     "parallelism": f"z slabs x{world}, NCCL point-to-point"},
+                          "changed_slab_per_step": moved_all / steps}), flush=True)
+
+
 def run_ensemble_line(args, world, rank, local):
     """The ensemble workload: runs split across ranks by particle count
     (ensemble.split_runs), each rank's runs in one graph per wave; value =
@@ -920,7 +1044,8 @@ def main():
     ap.add_argument("--cells", type=int, default=0, help="grid side of a smaller profiling case (default 128)")
     ap.add_argument("--ppc", type=int, default=0, help="particles per cell per species with --cells")
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and ensemble sections")
-    ap.add_argument("--workload", default="particle_step", choices=["particle_step", "ensemble", "body", "em"])
+    ap.add_argument("--workload", default="particle_step",
+                    choices=["particle_step", "ensemble", "body", "em", "slabs"])
     ap.add_argument("--body-scale", type=float, default=1.0, help="grid scale of the body workload (1: 256x256x512)")
     ap.add_argument("--host-inject", action="store_true",
                     help="body workload: draw the injected records on the host (else on the device)")
@@ -933,6 +1058,8 @@ def main():
             run_body_line(args, world, rank, local)
         elif args.workload == "em":
             run_em_line(args, world, rank, local)
+        elif args.workload == "slabs":
+            run_slabs_line(args, world, rank, local)
         elif args.workload == "ensemble":
             args.ensemble_runs = args.ensemble_runs or 512
             args.ensemble_steps = args.ensemble_steps or 200

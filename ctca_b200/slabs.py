@@ -114,8 +114,11 @@ class SlabGroup:
     """All slabs of a z decomposition in this process: contexts (on one GPU
     or several) stepped together, the exchange done by device copies."""
 
-    def __init__(self, cfg: Config, eb: np.ndarray, p: np.ndarray, tp, nslab: int, outbox_cap: int,
-                 capacity_factor: float = 1.25, devices=None):
+    def __init__(self, cfg: Config, eb: np.ndarray, p: np.ndarray | None, tp, nslab: int, outbox_cap: int,
+                 capacity_factor: float = 1.25, devices=None, plasmas=None):
+        """The particles of the whole grid as records (p, tp), or per slab a
+        plasma description drawn on its device (plasmas[r], emsesg_load_plasma
+        on the slab's grid; p None)."""
         self.cfg = cfg
         self.nslab = nslab
         self.sub = slab_config(cfg, nslab, capacity_factor)
@@ -125,8 +128,11 @@ class SlabGroup:
                 import torch
                 torch.cuda.set_device(devices[r])
             g = Emses(self.sub)
-            pr, tpr = slab_particles(cfg, p, tp, r, nslab)
-            g.upload_particles(pr, tpr)
+            if plasmas is not None:
+                g.load_plasma(plasmas[r])
+            else:
+                pr, tpr = slab_particles(cfg, p, tp, r, nslab)
+                g.upload_particles(pr, tpr)
             g.upload_field("eb", slab_field(cfg, eb, "eb", r, nslab))
             g.fx_load()
             g.fx_slab(True, outbox_cap)
