@@ -141,6 +141,7 @@ struct FxState {
   float4* fnode2 = nullptr;         // {by, bz, 0, 0}
   int bits[3] = {0, 0, 0};          // packed cell bit widths
   int tile[3] = {8, 8, 8};
+  int chunk_rows = 256;             // rows of a tile region per push CTA (emsesg_fx_chunk_rows)
   int ntile[3] = {0, 0, 0};
   int64_t ntiles = 0;
 };

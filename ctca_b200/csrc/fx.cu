@@ -901,6 +901,7 @@ int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit) {
   a.tile_pad = f.tile_pad;
   a.chunk_start = f.chunk_start;
   a.ntiles = f.ntiles;
+  a.chunk_rows = f.chunk_rows;
   double gustep = ustep;
   a.gustep = (float)gustep;
   a.rustep = (float)(1.0 / ustep);
@@ -924,11 +925,12 @@ int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit) {
     EMSESG_CUDA(ctx, cudaMemsetAsync(f.outbox_n, 0, 2 * EMSESG_ISPEC * sizeof(unsigned long long), ctx->stream));
     a.ob = Outbox{f.outbox, f.outbox_n, f.outbox_cap};
   }
-  // row chunks of the tile regions: at most ntiles + rows / CHUNK_ROWS
+  // row chunks of the tile regions: at most ntiles + rows / chunk_rows
   int64_t rows = 0;
   for (int is = 0; is < c.nspec; is++) rows = std::max(rows, (f.cap[is] + PUSH_THREADS - 1) / PUSH_THREADS);
-  EMSESG_LAUNCH(ctx, "fx_chunks", k_push_chunks, (unsigned)c.nspec, 1024, 0, f.tile_start, f.ntiles, f.chunk_start);
-  dim3 grid((unsigned)(f.ntiles + rows / CHUNK_ROWS + 1), (unsigned)c.nspec);
+  EMSESG_LAUNCH(ctx, "fx_chunks", k_push_chunks, (unsigned)c.nspec, 1024, 0, f.tile_start, f.ntiles, f.chunk_start,
+                f.chunk_rows);
+  dim3 grid((unsigned)(f.ntiles + rows / f.chunk_rows + 1), (unsigned)c.nspec);
   if (!deposit) {
     for (int is = 0; is < c.nspec; is++)
       if (f.ntail[is]) return set_error(ctx, EMSESG_ERR_STATE, "move-only step with injected particles");
@@ -1440,6 +1442,18 @@ void slab_plane_range(int kind, int which, int nz, int* k0, int* depth) {
 }
 }  // namespace
 }  // namespace emsesg
+
+extern "C" int emsesg_fx_chunk_rows(emsesg_ctx* ctx, int rows) {
+  if (!ctx || rows < 1 || rows > 1 << 20) return EMSESG_ERR_ARG;
+  FxState& f = ctx->fx;
+  if (f.slab_open) return set_error(ctx, EMSESG_ERR_STATE, "slab step open");
+  if (f.chunk_rows != rows && f.gexec) {  // a captured block holds the old grid
+    cudaGraphExecDestroy(f.gexec);
+    f.gexec = nullptr;
+  }
+  f.chunk_rows = rows;
+  return EMSESG_OK;
+}
 
 extern "C" int emsesg_fx_slab(emsesg_ctx* ctx, int on, int64_t outbox_cap) {
   if (!ctx || (on && outbox_cap < 1)) return EMSESG_ERR_ARG;

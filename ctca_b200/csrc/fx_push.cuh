@@ -50,7 +50,6 @@ constexpr int RQ_DRAIN = 8;     // drain the run queue at this many entries
 constexpr int RQCAP = RQ_DRAIN + 32;
 constexpr int XQW = 8;          // general-path entry: slot, cell, 3 offsets, 3 velocities
 constexpr int XLCAP = 128;      // per-warp list of cross slots (emptied when nearly full)
-constexpr int CHUNK_ROWS = 256;  // rows of a tile region per CTA (crowded tiles take several)
 constexpr uint32_t ROW_BYTES = PUSH_THREADS * (16 + 3 * 4);
 static_assert(PUSH_THREADS == EMSESG_FX_ROW_SLOTS, "row width of the thread-major layout");
 static_assert(ROW_BYTES % 16 == 0 && (PUSH_THREADS * 4) % 16 == 0, "bulk copies move whole 16-byte units");
@@ -103,6 +102,7 @@ struct FxPushArgs {
   FieldDesc fr, fj;
   Geo g;
   int64_t ntiles;
+  int chunk_rows;               // rows of a tile region per CTA
   int* nesc;                    // counter nesc(is), one int per species
   emsesg_counter* gc;           // influx / infhist of the body absorption
   unsigned long long* surf;     // [nspec][nsurf] absorbed - emitted counts
@@ -696,8 +696,8 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   const int t = (int)tlo;
   const int64_t n = ts[t + 1] - ts[t];
   if (n <= 0) return;
-  const int r0 = (int)(b - cs[t]) * CHUNK_ROWS;
-  const int L = min((int)((n + PUSH_THREADS - 1) / PUSH_THREADS) - r0, CHUNK_ROWS);
+  const int r0 = (int)(b - cs[t]) * a.chunk_rows;
+  const int L = min((int)((n + PUSH_THREADS - 1) / PUSH_THREADS) - r0, a.chunk_rows);
   if (L <= 0) return;
   const int64_t slot0 = a.off[is] + a.tile_pad[(int64_t)is * (a.ntiles + 1) + t] + (int64_t)r0 * PUSH_THREADS;
 
@@ -1008,7 +1008,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
 // The row chunks of every tile region: cs[t] = first chunk of tile t,
 // cs[ntiles] = the number of chunks (one block of 1024 threads per species).
 __global__ void __launch_bounds__(1024) k_push_chunks(const int64_t* __restrict__ tile_start, int64_t ntiles,
-                                                      int64_t* chunk_start) {
+                                                      int64_t* chunk_start, int chunk_rows) {
   __shared__ int64_t pa[1024];
   const int64_t* ts = tile_start + (int64_t)blockIdx.x * (ntiles + 1);
   int64_t* cs = chunk_start + (int64_t)blockIdx.x * (ntiles + 1);
@@ -1017,7 +1017,7 @@ __global__ void __launch_bounds__(1024) k_push_chunks(const int64_t* __restrict_
   const int64_t t0 = tid * per, t1 = min(ntiles, t0 + per);
   auto chunks = [&](int64_t t) {
     const int64_t rows = (ts[t + 1] - ts[t] + PUSH_THREADS - 1) / PUSH_THREADS;
-    return (rows + CHUNK_ROWS - 1) / CHUNK_ROWS;
+    return (rows + chunk_rows - 1) / chunk_rows;
   };
   int64_t sa = 0;
   for (int64_t t = t0; t < t1; t++) sa += chunks(t);

@@ -132,6 +132,7 @@ _SIGS = {
     "emsesg_fx_step": (_I, [_P, _I, _I]),
     "emsesg_fx_sort": (_I, [_P]),
     "emsesg_fx_run": (_I, [_P, _I, _I, _I, _I]),
+    "emsesg_fx_chunk_rows": (_I, [_P, _I]),
     "emsesg_fx_slab": (_I, [_P, _I, ctypes.c_int64]),
     "emsesg_fx_slab_begin": (_I, [_P, _I, _P]),
     "emsesg_fx_slab_outbox": (_I, [_P, _I, _I, ctypes.POINTER(ctypes.c_void_p)]),
@@ -390,6 +391,10 @@ class Emses:
 
     def fx_step(self, ustep: int = 2, do_sort: bool = False):
         self._check(self.lib.emsesg_fx_step(self.h, ustep, 1 if do_sort else 0))
+
+    def fx_chunk_rows(self, rows: int):
+        """Rows of a tile region per push CTA (default 256)."""
+        self._check(self.lib.emsesg_fx_chunk_rows(self.h, rows))
 
     # -- slab mode (a z slab of a decomposed grid; ctca_b200/slabs.py)
     def fx_slab(self, on: bool, outbox_cap: int = 0):

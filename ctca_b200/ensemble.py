@@ -11,10 +11,13 @@ taken their steps.  Small runs (16^3 cells fill 16 CTAs) leave most of the
 the CPU launches one graph instead of about fifteen kernels per step and
 run.
 
-The tile shape and the sort interval S of each grid-size class come from an
-autotuner that times the candidates on a batch of copies of the class's
-first run (the push block is fixed at 768 threads by the 736-slot rows of
-the layout).  Runs that do not fit in device memory together go in waves.
+The tile shape, the sort interval S and the push CTA's share of a tile
+region (rows per CTA: with fewer, a small grid's tiles spread over more
+SMs) of each grid-size class come from an autotuner that times the
+candidates on a batch of copies of the class's first run: tile and sort
+interval first, then the rows per CTA for the best of those (the CTA itself
+is fixed at 768 threads by the 736-slot rows of the layout).  Runs that do
+not fit in device memory together go in waves.
 
 Runs are drawn as stated for the ensemble workload: cubic periodic grids of
 side 16, 24, 32, 48 or 64, electrons and ions (mass ratio 100, equal
@@ -38,6 +41,7 @@ from .emses import Batch, Emses
 SIDES = (16, 24, 32, 48, 64)
 TILES = (4, 8)
 SORTS = (1, 2, 4, 8)
+CHUNKS = (256, 48, 16)  # rows of a tile region per push CTA
 USTEP = 2
 
 
@@ -86,13 +90,14 @@ def run_bytes(case: inputs.Case) -> int:
     return int(particles(case) * 260 + g * 480 + (48 << 20))
 
 
-def open_run(case: inputs.Case, tile: int) -> Emses:
+def open_run(case: inputs.Case, tile: int, chunk_rows: int = CHUNKS[0]) -> Emses:
     """A loaded run: context, fields, device-seeded plasma, FP32 form."""
     case = replace(case, sort_tile=(tile, tile, tile))
     g = Emses(inputs.make_config(case))
     g.upload_field("eb", inputs.make_fields(case))
     g.load_plasma(inputs.plasma(case))
     g.fx_load()
+    g.fx_chunk_rows(chunk_rows)
     return g
 
 
@@ -168,20 +173,23 @@ class Choice:
     tile: int
     sort_every: int
     ns_per_particle_step: float
+    chunk_rows: int = CHUNKS[0]
 
 
 class Autotuner:
-    """Tile shape and sort interval per grid-size class (cubic side),
-    timed on a batch of copies of the class's first run; results are kept
-    in memory and, with `cache`, in a JSON file keyed by side."""
+    """Tile shape, sort interval and rows per push CTA per grid-size class
+    (cubic side), timed on a batch of copies of the class's first run;
+    results are kept in memory and, with `cache`, in a JSON file keyed by
+    side."""
 
     def __init__(self, cache: str | Path | None = None, steps: int = 8, trial_particles: int = 32 << 20,
-                 tiles=TILES, sorts=SORTS):
+                 tiles=TILES, sorts=SORTS, chunks=CHUNKS):
         self.cache = Path(cache) if cache else None
         self.steps = steps
         self.trial_particles = trial_particles
         self.tiles = tiles
         self.sorts = sorts
+        self.chunks = chunks
         self.table: dict[str, Choice] = {}
         self.trials: dict[str, list] = {}
         if self.cache and self.cache.exists():
@@ -213,9 +221,25 @@ class Autotuner:
                     steps = max(self.steps, block_steps([s]))
                     t = run_batch(runs, [s] * copies, steps)
                     ns = t / (copies * particles(case) * steps) * 1e9
-                    trials.append((tile, s, ns))
+                    trials.append((tile, s, self.chunks[0], ns))
                     if best is None or ns < best.ns_per_particle_step:
-                        best = Choice(tile, s, ns)
+                        best = Choice(tile, s, ns, self.chunks[0])
+            finally:
+                for g in runs:
+                    g.close()
+        # the rows per CTA, for the best tile and sort interval
+        if best is not None and len(self.chunks) > 1:
+            runs = [open_run(replace(case, seed=case.seed + c), best.tile) for c in range(copies)]
+            try:
+                steps = max(self.steps, block_steps([best.sort_every]))
+                for rows in self.chunks[1:]:
+                    for g in runs:
+                        g.fx_chunk_rows(rows)
+                    t = run_batch(runs, [best.sort_every] * copies, steps)
+                    ns = t / (copies * particles(case) * steps) * 1e9
+                    trials.append((best.tile, best.sort_every, rows, ns))
+                    if ns < best.ns_per_particle_step:
+                        best = Choice(best.tile, best.sort_every, ns, rows)
             finally:
                 for g in runs:
                     g.close()
@@ -262,7 +286,7 @@ def run_ensemble(cases: list[inputs.Case], steps: int, tuner: Autotuner, modes=(
     for w in plan:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        runs = [open_run(cases[i], choice[i].tile) for i in w]
+        runs = [open_run(cases[i], choice[i].tile, choice[i].chunk_rows) for i in w]
         sorts = [choice[i].sort_every for i in w]
         torch.cuda.synchronize()
         e2e += time.perf_counter() - t0

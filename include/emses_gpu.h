@@ -278,6 +278,13 @@ int emsesg_fx_sort(emsesg_ctx* ctx);
  * on the context's stream. */
 int emsesg_fx_run(emsesg_ctx* ctx, int ustep, int nsteps, int sort_every, int use_graph);
 
+/* Rows of a tile region that one push CTA takes (default 256; a tile of
+ * more rows is pushed by several CTAs that add their sums into the same
+ * accumulators).  Fewer rows per CTA spread a small grid over more SMs at
+ * the cost of more field-tile loads and accumulator flushes; the ensemble's
+ * autotuner picks it per grid size.  Kept until the FP32 form is released. */
+int emsesg_fx_chunk_rows(emsesg_ctx* ctx, int rows);
+
 /* Domain decomposition in z slabs (replaces, for slabs of one periodic z
  * axis, OhHelp's particle migration, oh2_transbound / exchange_particles,
  * lib/ohhelp/ohhelp-1.1.1/ohhelp2.c:103-123, 333-384, and the border

@@ -142,3 +142,22 @@ def test_small_ensemble_runs_and_tunes(gpu):
     assert set(out["choices"]) <= {"side16", "side24"}
     for ch in out["choices"].values():
         assert ch["tile"] in ensemble.TILES and ch["sort_every"] in ensemble.SORTS
+        assert ch["chunk_rows"] in ensemble.CHUNKS
+
+
+@pytest.mark.parametrize("rows", [1, 16, 48])
+def test_rows_per_cta_change_no_particle(gpu, rows):
+    """Fewer rows of a tile region per push CTA (the autotuner's block
+    knob): several CTAs share a tile, so a thread's run sums split at the
+    chunk edges; the particles stay bit-identical and rho / J agree to FP32
+    summation order."""
+    c = case(n=(16, 16, 16), ppc=(24, 24), vth_scale=2.0, tile=(8, 8, 8))
+    with loaded(c) as a, loaded(c) as b:
+        b.fx_chunk_rows(rows)
+        a.fx_run(2, 8, 4, use_graph=False)
+        b.fx_run(2, 8, 4, use_graph=False)
+        ra, ja, pa, ta = state(a)
+        rb, jb, pb, tb = state(b)
+        assert np.array_equal(ta, tb)
+        assert np.array_equal(pa.view(np.uint8), pb.view(np.uint8))
+        assert rel_l2(rb, ra) < 1e-6 and rel_l2(jb, ja) < 1e-6
