@@ -78,12 +78,15 @@ def peaks() -> tuple[float, str]:
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (read only)."""
+    """nvidia-smi sampling (every 50 ms) during the timed region (read only):
+    the sampler is running before the region starts, and only the samples
+    taken inside it are summarised."""
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
+        self.samples = []  # (host time, fields)
         self.proc = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -91,19 +94,24 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.reader = threading.Thread(target=self._read, daemon=True)
             self.reader.start()
+            deadline = time.time() + 3.0
+            while not self.samples and time.time() < deadline:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t0 = time.time()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.samples.append([x.strip() for x in line.split(",")])
+            self.samples.append((time.time(), [x.strip() for x in line.split(",")]))
 
     def __exit__(self, *exc):
+        self.t1 = time.time()
         if self.proc:
             self.proc.terminate()
             try:
@@ -115,7 +123,8 @@ class Clocks:
     def summary(self) -> dict:
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for s in self.samples:
+        inside = [f for t, f in self.samples if self.t0 is not None and self.t0 <= t <= (self.t1 or t)]
+        for s in inside or [f for _, f in self.samples[-1:]]:
             try:
                 sm.append(float(s[1]))
                 mx = float(s[2])
