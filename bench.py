@@ -515,11 +515,16 @@ def run_ours(args, world, rank, local):
     aj_host = torch.empty(na, dtype=torch.float64, pin_memory=True)
     lib = g.lib
 
+    # per step: this step's eb up (copied beside the previous step's sort,
+    # after its rho / J reached the host), the step, rho and J down (beside
+    # this step's sort); the host has rho and J before it uploads the next eb
     def e2e_step(s):
-        lib.emsesg_upload_field(g.h, 0, eb_host.data_ptr())
-        fx_step(s)
-        lib.emsesg_download_field(g.h, 4, rho_host.data_ptr())
-        lib.emsesg_download_field(g.h, 2, aj_host.data_ptr())
+        lib.emsesg_upload_field_async(g.h, 0, eb_host.data_ptr())
+        rc = lib.emsesg_fx_step_download(g.h, 2, 1 if (step_i[0] % SORT_EVERY) == SORT_EVERY - 1 else 0,
+                                         rho_host.data_ptr(), aj_host.data_ptr())
+        step_i[0] += 1
+        if rc:
+            raise RuntimeError(f"emsesg_fx_step_download: {rc}")
 
     ke2e = max(1, min(args.steps, args.e2e_steps))
     te2e = timed(e2e_step, ke2e)

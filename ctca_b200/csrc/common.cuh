@@ -153,6 +153,14 @@ struct emsesg_ctx {
   emsesg_config* d_cfg = nullptr;      // device copy of cfg for the kernels
   int device = 0;
   cudaStream_t stream = nullptr;
+  // host transfers beside the step (emsesg_fx_step_download,
+  // emsesg_upload_field_async): a side stream, the event after a step's
+  // field phase, the next eb (double buffer) and its copy event
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fields = nullptr;
+  cudaEvent_t ev_eb = nullptr;
+  double* eb_next = nullptr;
+  bool eb_next_pending = false;
   std::string err;
   emsesg::Segments seg;
   int64_t totalp[EMSESG_ISPEC] = {0};  // host mirror of the species counts
@@ -179,6 +187,11 @@ struct emsesg_ctx {
 namespace emsesg {
 
 int set_error(emsesg_ctx* ctx, int code, const char* fmt, ...);
+// The side stream of host transfers (created on first use), and the eb of
+// an asynchronous upload put in place (the context's stream waits for its
+// copy) before the work that reads eb.
+int side_stream(emsesg_ctx* ctx);
+int apply_pending_eb(emsesg_ctx* ctx);
 // Records m0 .. m0+n-1 of species `is` of the seeded plasma of
 // emsesg_load_plasma, into the device array dst (n records).
 int plasma_records(emsesg_ctx* ctx, emsesg_particle* dst, int is, int64_t m0, int64_t n, const emsesg_plasma* pl);

@@ -189,6 +189,11 @@ extern "C" int emsesg_destroy(emsesg_ctx* ctx) {
   cudaFree(ctx->sort.scan_tmp);
   fx_free(ctx);
   for (auto e : ctx->timer.pool) cudaEventDestroy(e);
+  if (ctx->side) cudaStreamSynchronize(ctx->side);
+  cudaFree(ctx->eb_next);
+  if (ctx->ev_fields) cudaEventDestroy(ctx->ev_fields);
+  if (ctx->ev_eb) cudaEventDestroy(ctx->ev_eb);
+  if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return EMSESG_OK;
@@ -288,8 +293,47 @@ extern "C" int emsesg_download_particles(emsesg_ctx* ctx, int ps, emsesg_particl
 extern "C" int emsesg_upload_field(emsesg_ctx* ctx, int field, const double* host) {
   if (!ctx || !host || field < 0 || field >= EMSESG_NFIELDS) return set_error(ctx, EMSESG_ERR_ARG, "bad field");
   if (field == EMSESG_FIELD_WRK) return set_error(ctx, EMSESG_ERR_ARG, "wrk is produced by grdcrt");
+  if (field == EMSESG_FIELD_EB && ctx->eb_next_pending) {  // this upload replaces a pending one
+    EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->side));
+    ctx->eb_next_pending = false;
+  }
   int64_t n = field_doubles(ctx->cfg, field);
   EMSESG_CUDA(ctx, cudaMemcpyAsync(ctx->field[field], host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  return EMSESG_OK;
+}
+
+namespace emsesg {
+int side_stream(emsesg_ctx* ctx) {
+  if (ctx->side) return EMSESG_OK;
+  EMSESG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+  EMSESG_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_fields, cudaEventDisableTiming));
+  EMSESG_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_eb, cudaEventDisableTiming));
+  // no step yet: the first copy waits for the work queued so far
+  EMSESG_CUDA(ctx, cudaEventRecord(ctx->ev_fields, ctx->stream));
+  return EMSESG_OK;
+}
+
+int apply_pending_eb(emsesg_ctx* ctx) {
+  if (!ctx->eb_next_pending) return EMSESG_OK;
+  EMSESG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_eb, 0));
+  std::swap(ctx->field[EMSESG_FIELD_EB], ctx->eb_next);
+  ctx->eb_next_pending = false;
+  return EMSESG_OK;
+}
+}  // namespace emsesg
+
+extern "C" int emsesg_upload_field_async(emsesg_ctx* ctx, int field, const double* host) {
+  if (!ctx || !host) return EMSESG_ERR_ARG;
+  if (field != EMSESG_FIELD_EB) return set_error(ctx, EMSESG_ERR_ARG, "asynchronous upload: eb only");
+  int rc = side_stream(ctx);
+  if (rc) return rc;
+  const int64_t n = field_doubles(ctx->cfg, field);
+  if (!ctx->eb_next) EMSESG_CUDA(ctx, cudaMalloc(&ctx->eb_next, n * sizeof(double)));
+  // the buffer was last read before the last step's field phase ended
+  EMSESG_CUDA(ctx, cudaStreamWaitEvent(ctx->side, ctx->ev_fields, 0));
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(ctx->eb_next, host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->side));
+  EMSESG_CUDA(ctx, cudaEventRecord(ctx->ev_eb, ctx->side));
+  ctx->eb_next_pending = true;
   return EMSESG_OK;
 }
 
@@ -306,6 +350,10 @@ int download_wrk(emsesg_ctx* ctx, double* host);  // dropin.cu
 
 extern "C" int emsesg_download_field(emsesg_ctx* ctx, int field, double* host) {
   if (!ctx || !host || field < 0 || field >= EMSESG_NFIELDS) return set_error(ctx, EMSESG_ERR_ARG, "bad field");
+  if (field == EMSESG_FIELD_EB) {
+    int rc = apply_pending_eb(ctx);
+    if (rc) return rc;
+  }
   if (field == EMSESG_FIELD_WRK) return download_wrk(ctx, host);
   int64_t n = field_doubles(ctx->cfg, field);
   EMSESG_CUDA(ctx, cudaMemcpyAsync(host, ctx->field[field], n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

@@ -860,6 +860,7 @@ PushArgs push_args(emsesg_ctx* ctx, int is, int ustep) {
 extern "C" int emsesg_grdcrt(emsesg_ctx* ctx, int ps) {
   int rc = check_ps(ctx, ps);
   if (rc) return rc;
+  if ((rc = apply_pending_eb(ctx))) return rc;
   const emsesg_config& c = ctx->cfg;
   int64_t nn = (int64_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
   EMSESG_LAUNCH(ctx, "grdcrt", k_grdcrt, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_EB], ctx->node64,
@@ -1017,6 +1018,7 @@ extern "C" int emsesg_rhoupd(emsesg_ctx* ctx, int ps) {
 extern "C" int emsesg_bfield(emsesg_ctx* ctx, int ps) {
   int rc = check_ps(ctx, ps);
   if (rc) return rc;
+  if ((rc = apply_pending_eb(ctx))) return rc;
   const emsesg_config& c = ctx->cfg;
   const int64_t nn = (int64_t)(c.nx + 2) * (c.ny + 2) * (c.nz + 2);
   EMSESG_LAUNCH(ctx, "bfield", k_bfield, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_EB],
@@ -1027,6 +1029,7 @@ extern "C" int emsesg_bfield(emsesg_ctx* ctx, int ps) {
 extern "C" int emsesg_efield(emsesg_ctx* ctx, int ps, double tcs, double dlt) {
   int rc = check_ps(ctx, ps);
   if (rc) return rc;
+  if ((rc = apply_pending_eb(ctx))) return rc;
   const emsesg_config& c = ctx->cfg;
   const int64_t nn = (int64_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
   EMSESG_LAUNCH(ctx, "efield", k_efield, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_EB], ctx->field[EMSESG_FIELD_AJ],
@@ -1036,6 +1039,8 @@ extern "C" int emsesg_efield(emsesg_ctx* ctx, int ps, double tcs, double dlt) {
 
 extern "C" int emsesg_exchange_eb(emsesg_ctx* ctx) {
   if (!ctx) return EMSESG_ERR_ARG;
+  int rc = apply_pending_eb(ctx);
+  if (rc) return rc;
   const FieldDesc f = field_desc(ctx->cfg, EMSESG_FIELD_EB);
   return run_slab_ops(ctx, ctx->field[EMSESG_FIELD_EB], f, fold_ops(ctx->cfg, 2, 6), "exchange_eb");
 }

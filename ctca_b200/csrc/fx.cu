@@ -874,6 +874,8 @@ int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit) {
   std::string why;
   if (!bodies_supported(c, &why)) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "%s", why.c_str());
   FxState& f = ctx->fx;
+  int rc0 = apply_pending_eb(ctx);
+  if (rc0) return rc0;
   Geo g = make_geo(ctx);
   int64_t nn = (int64_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
   EMSESG_LAUNCH(ctx, "fx_grdcrt", k_grdcrt32, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_EB], f.fnode, f.fnode2,
@@ -991,7 +993,7 @@ void fold_lists(const emsesg_config& c, bool slab, int part, std::vector<SlabOp>
 // place, and this J), then the re-sort after the push (so that injected
 // particles take their first, partial step before they join the tile
 // regions).
-int fx_finish_phase(emsesg_ctx* ctx, int do_sort) {
+int fx_fields_phase(emsesg_ctx* ctx) {
   FxState& f = ctx->fx;
   const emsesg_config& c = ctx->cfg;
   FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
@@ -1009,6 +1011,15 @@ int fx_finish_phase(emsesg_ctx* ctx, int do_sort) {
                 ctx->field[EMSESG_FIELD_RHO], ctx->field[EMSESG_FIELD_AJ], fr, fj, c.nx, c.ny, c.nz, cres);
   f.cont_valid = f.rho_prev;
   f.rho_prev = true;
+  // the step's reads of eb are over: an asynchronous upload of the next eb
+  // may start
+  if (ctx->ev_fields) EMSESG_CUDA(ctx, cudaEventRecord(ctx->ev_fields, ctx->stream));
+  return EMSESG_OK;
+}
+
+int fx_finish_phase(emsesg_ctx* ctx, int do_sort) {
+  int rc = fx_fields_phase(ctx);
+  if (rc) return rc;
   ctx->rng_stream++;
   if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
   return EMSESG_OK;
@@ -1029,6 +1040,28 @@ int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   return fx_finish_phase(ctx, do_sort);
 }
 }  // namespace
+
+extern "C" int emsesg_fx_step_download(emsesg_ctx* ctx, int ustep, int do_sort, double* rho, double* aj) {
+  if (!ctx || !rho || !aj) return EMSESG_ERR_ARG;
+  if (ctx->fx.slab) return set_error(ctx, EMSESG_ERR_STATE, "slab mode: steps are emsesg_fx_slab_begin / _arrive / _end");
+  int rc = side_stream(ctx);
+  if (rc) return rc;
+  if ((rc = fx_push_phase(ctx, ustep, true))) return rc;
+  if ((rc = fx_fields_phase(ctx))) return rc;
+  // rho and aj are final: copied to the host on the side stream while the
+  // context's stream goes on with the sort
+  const emsesg_config& c = ctx->cfg;
+  const int64_t nr = field_desc(c, EMSESG_FIELD_RHO).size(), na = field_desc(c, EMSESG_FIELD_AJ).size();
+  EMSESG_CUDA(ctx, cudaStreamWaitEvent(ctx->side, ctx->ev_fields, 0));
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(rho, ctx->field[EMSESG_FIELD_RHO], nr * sizeof(double), cudaMemcpyDeviceToHost,
+                                   ctx->side));
+  EMSESG_CUDA(ctx, cudaMemcpyAsync(aj, ctx->field[EMSESG_FIELD_AJ], na * sizeof(double), cudaMemcpyDeviceToHost,
+                                   ctx->side));
+  ctx->rng_stream++;
+  if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
+  EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->side));
+  return EMSESG_OK;
+}
 
 extern "C" int emsesg_fx_em_step(emsesg_ctx* ctx, int ustep, int do_sort, double tcs) {
   if (!ctx) return EMSESG_ERR_ARG;

@@ -133,6 +133,8 @@ _SIGS = {
     "emsesg_fx_sort": (_I, [_P]),
     "emsesg_fx_run": (_I, [_P, _I, _I, _I, _I]),
     "emsesg_fx_chunk_rows": (_I, [_P, _I]),
+    "emsesg_fx_step_download": (_I, [_P, _I, _I, _P, _P]),
+    "emsesg_upload_field_async": (_I, [_P, _I, _P]),
     "emsesg_fx_slab": (_I, [_P, _I, ctypes.c_int64]),
     "emsesg_fx_slab_begin": (_I, [_P, _I, _P]),
     "emsesg_fx_slab_outbox": (_I, [_P, _I, _I, ctypes.POINTER(ctypes.c_void_p)]),
@@ -391,6 +393,20 @@ class Emses:
 
     def fx_step(self, ustep: int = 2, do_sort: bool = False):
         self._check(self.lib.emsesg_fx_step(self.h, ustep, 1 if do_sort else 0))
+
+    def fx_step_download(self, ustep: int, do_sort: bool, rho: np.ndarray, aj: np.ndarray):
+        """A step with rho and aj copied into the given host arrays (float64,
+        contiguous, the fields' sizes) while the sort runs."""
+        assert rho.dtype == np.float64 and aj.dtype == np.float64
+        assert rho.size == self.field_size("rho") and aj.size == self.field_size("aj")
+        self._check(self.lib.emsesg_fx_step_download(self.h, ustep, 1 if do_sort else 0, rho.ctypes.data,
+                                                     aj.ctypes.data))
+
+    def upload_eb_async(self, eb: np.ndarray):
+        """The eb of the next step, copied beside the current step's sort
+        (keep the array unchanged until the next step has started)."""
+        assert eb.dtype == np.float64 and eb.size == self.field_size("eb") and eb.flags["C_CONTIGUOUS"]
+        self._check(self.lib.emsesg_upload_field_async(self.h, FIELDS["eb"], eb.ctypes.data))
 
     def fx_chunk_rows(self, rows: int):
         """Rows of a tile region per push CTA (default 256)."""

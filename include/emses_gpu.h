@@ -265,6 +265,18 @@ int emsesg_fx_store(emsesg_ctx* ctx);
  * with do_sort, the re-sort after the push. */
 int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort);
 int emsesg_fx_sort(emsesg_ctx* ctx);
+/* emsesg_fx_step followed by the downloads of rho and aj (the arrays a field
+ * solver takes), made on a side stream as soon as the step's fields are
+ * final, so that they overlap with the re-sort; returns once rho and aj are
+ * in host memory (pinned memory for the overlap), the sort may still run.
+ * emsesg_upload_field_async(ctx, EMSESG_FIELD_EB, host) copies the eb of
+ * the next step on the side stream into a second buffer, which replaces the
+ * field before the next work that reads eb (an FP32 step, grdcrt, the field
+ * step, a download of eb); the copy starts once the last step has read eb,
+ * so it overlaps with that step's sort.  A synchronous emsesg_upload_field
+ * of eb replaces a pending asynchronous one. */
+int emsesg_fx_step_download(emsesg_ctx* ctx, int ustep, int do_sort, double* rho, double* aj);
+int emsesg_upload_field_async(emsesg_ctx* ctx, int field, const double* host);
 /* nsteps steps of the FP32 form, re-sorting every sort_every steps
  * (emsesg_fx_step with do_sort on every sort_every-th step).  With use_graph,
  * a block of 2*sort_every steps is captured once into a CUDA graph (cached

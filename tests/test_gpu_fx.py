@@ -278,3 +278,38 @@ def test_fx_stray_particles_fall_back_to_the_radix_sort(gpu):
     assert rel_l2(g.download_field("rho"), o.f["rho"]) < RHOJ_TOL
     assert rel_l2(g.download_field("aj"), o.f["aj"]) < RHOJ_TOL
     g.close()
+
+
+def test_step_download_overlap_matches_plain_io(gpu):
+    """emsesg_fx_step_download with the next eb uploaded asynchronously (a
+    different eb every step, so that the double buffer must hand over the
+    right one) gives the rho / aj and the particles of the plain sequence
+    upload_field, fx_step, download_field, bit for bit, through sorts."""
+    import torch
+    c = case(n=(16, 16, 16), ppc=(8, 8), vth_scale=2.0, tile=(8, 8, 8))
+    cfg, eb, p, tp = build(c, 1.2)
+    ebs = [np.ascontiguousarray(eb * (1.0 + 0.05 * k)) for k in range(6)]
+    pinned = [torch.from_numpy(e.reshape(-1)).pin_memory().numpy() for e in ebs]
+    with Emses(cfg) as a, Emses(cfg) as b:
+        for g in (a, b):
+            g.upload_particles(p, tp)
+            g.upload_field("eb", ebs[0])
+            g.fx_load()
+        rho_b = torch.empty(b.field_size("rho"), dtype=torch.float64).pin_memory().numpy()
+        aj_b = torch.empty(b.field_size("aj"), dtype=torch.float64).pin_memory().numpy()
+        for k in range(6):
+            srt = k % 3 == 2
+            a.upload_field("eb", ebs[k])
+            a.fx_step(2, srt)
+            ra, ja = a.download_field("rho"), a.download_field("aj")
+            if k > 0:
+                b.upload_eb_async(pinned[k])
+            b.fx_step_download(2, srt, rho_b, aj_b)
+            assert np.array_equal(ra.reshape(-1), rho_b), k
+            assert np.array_equal(ja.reshape(-1), aj_b), k
+        a.fx_store()
+        b.fx_store()
+        pa, ta = a.download_particles()
+        pb, tb = b.download_particles()
+        assert np.array_equal(ta, tb)
+        assert np.array_equal(pa.view(np.uint8), pb.view(np.uint8))
