@@ -138,6 +138,7 @@ __global__ void k_fx_inject(const emsesg_particle* __restrict__ q, const int32_t
   if (r.preside == EMSESG_PCL_TO_BE_ACCUMULATED_AS_ANTIPCL) {
     const double p3[3] = {r.x, r.y, r.z};
     for (int b = 0; b < bd.n; b++) {
+      if (bd.kind[b] != 0) continue;  // surface cells of box bodies only
       int64_t hit = -1;
       for (int d = 0; d < 3 && hit < 0; d++) {
         const int e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;
@@ -347,14 +348,22 @@ Geo make_geo(emsesg_ctx* ctx) {
 
 }  // namespace
 
-// Box bodies usable by the FP32 form: geotype 0/1 with integer bounds.
-// Returns false (with the reason) when a body cannot be handled.
+// Bodies usable by the FP32 form: boxes (geotype 0/1) with integer bounds,
+// cylinders (geotype 2, axis 1..3) and spheres (geotype 3) of positive
+// radius.  Returns false (with the reason) when a body cannot be handled.
 bool bodies_supported(const emsesg_config& c, std::string* why) {
   if (c.npc <= 0 || c.line_mode == 1) return true;
   for (int ipc = 0; ipc < c.npc; ipc++) {
     const emsesg_body& b = c.body[ipc];
+    if (b.geotype == 2 || b.geotype == 3) {
+      if (!(b.radius > 0.0) || (b.geotype == 2 && (b.cyl_align < 1 || b.cyl_align > 3))) {
+        if (why) *why = "cylinder or sphere body without a positive radius or a valid axis";
+        return false;
+      }
+      continue;
+    }
     if (!(b.geotype == 0 || b.geotype == 1)) {
-      if (why) *why = "the FP32 form handles box bodies (geotype 0/1) only";
+      if (why) *why = "the FP32 form handles box, cylinder and sphere bodies (geotype 0..3) only";
       return false;
     }
     const double v[6] = {b.xlpc, b.xupc, b.ylpc, b.yupc, b.zlpc, b.zupc};
@@ -380,6 +389,38 @@ Bodies make_bodies(const emsesg_config& c) {
     const emsesg_body& b = c.body[ipc];
     const int q = bd.n++;
     bd.ipc[q] = ipc;
+    if (b.geotype == 2 || b.geotype == 3) {
+      // the cells a point inside may lie in, with one cell of margin
+      double lo[3], hi[3];
+      if (b.geotype == 3) {
+        for (int d = 0; d < 3; d++) {
+          bd.cen[q][d] = (float)b.sph_center[d];
+          lo[d] = b.sph_center[d] - b.radius;
+          hi[d] = b.sph_center[d] + b.radius;
+        }
+      } else {
+        const int a0 = b.cyl_align - 1, a1 = (a0 + 1) % 3, a2 = (a0 + 2) % 3;
+        bd.cax[q] = a0;
+        bd.cen[q][a0] = 0.f;
+        bd.cen[q][a1] = (float)b.cyl_axis[0];
+        bd.cen[q][a2] = (float)b.cyl_axis[1];
+        bd.edge[q][0] = (float)b.cyl_edge[0];
+        bd.edge[q][1] = (float)b.cyl_edge[1];
+        lo[a0] = b.cyl_edge[0]; hi[a0] = b.cyl_edge[1];
+        lo[a1] = b.cyl_axis[0] - b.radius; hi[a1] = b.cyl_axis[0] + b.radius;
+        lo[a2] = b.cyl_axis[1] - b.radius; hi[a2] = b.cyl_axis[1] + b.radius;
+      }
+      bd.kind[q] = b.geotype;
+      bd.r2[q] = (float)(b.radius * b.radius);
+      for (int d = 0; d < 3; d++) {
+        bd.lo[q][d] = (int)std::max(-2.0, std::floor(lo[d]) - 1.0);
+        bd.hi[q][d] = (int)std::min(1e9, std::floor(hi[d]) + 1.0);
+      }
+      for (int f = 0; f < 6; f++) bd.off[q][f] = -1;
+      bd.ncurved++;
+      continue;
+    }
+    bd.kind[q] = 0;
     bd.lo[q][0] = (int)b.xlpc; bd.hi[q][0] = (int)b.xupc;
     bd.lo[q][1] = (int)b.ylpc; bd.hi[q][1] = (int)b.yupc;
     bd.lo[q][2] = (int)b.zlpc; bd.hi[q][2] = (int)b.zupc;
@@ -484,6 +525,10 @@ int fx_alloc(emsesg_ctx* ctx) {
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         fx_push_smem(4)));
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        fx_push_smem(8)));
+  EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<4, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        fx_push_smem(4)));
+  EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<8, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         fx_push_smem(8)));
   return EMSESG_OK;
 }
@@ -723,8 +768,9 @@ extern "C" int emsesg_fx_load(emsesg_ctx* ctx) {
 
 namespace emsesg {
 namespace {
-// Particles whose start point lies inside a box body (inclusive bounds, the
-// absorption test of the push) are not placed: DEAD.
+// Particles whose start point lies inside a body (the absorption test of
+// the push: a box with inclusive bounds, a cylinder or a sphere) are not
+// placed: DEAD.
 __global__ void k_fx_clear_bodies(float4* pos, int64_t n, Geo g, Bodies bd) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n) return;
@@ -735,6 +781,13 @@ __global__ void k_fx_clear_bodies(float4* pos, int64_t n, Geo g, Bodies bd) {
   unpack(g, cell, c3[0], c3[1], c3[2]);
   const float f3v[3] = {p.x, p.y, p.z};
   for (int q = 0; q < bd.n; q++) {
+    if (bd.kind[q] != 0) {
+      if (in_curved(bd, q, c3, f3v)) {
+        pos[m].w = __int_as_float((int)DEAD);
+        return;
+      }
+      continue;
+    }
     bool in = true;
     for (int d = 0; d < 3; d++)
       in = in && c3[d] >= bd.lo[q][d] && (c3[d] < bd.hi[q][d] || (c3[d] == bd.hi[q][d] && f3v[d] == 0.0f));
@@ -750,7 +803,7 @@ __global__ void k_fx_clear_bodies(float4* pos, int64_t n, Geo g, Bodies bd) {
 // The records come through a bounded device scratch in chunks and are
 // converted by the same kernel as emsesg_fx_load, so the state is the one
 // emsesg_load_plasma + emsesg_fx_load give (without bodies: particles that
-// start inside a box body are left out here).
+// start inside a body are left out here).
 extern "C" int emsesg_fx_load_plasma(emsesg_ctx* ctx, const emsesg_plasma* pl) {
   if (!ctx || !pl) return EMSESG_ERR_ARG;
   const emsesg_config& c = ctx->cfg;
@@ -943,10 +996,14 @@ int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit) {
       EMSESG_LAUNCH(ctx, "fx_move", (k_fx_push<8, false>), grid, PUSH_BLOCK, smem, a);
     return EMSESG_OK;
   }
-  if (fx_box_tile(tmax) == 4)
-    EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<4>, grid, PUSH_BLOCK, smem, a);
-  else
-    EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<8>, grid, PUSH_BLOCK, smem, a);
+  const bool curved = a.bd.ncurved > 0;
+  if (fx_box_tile(tmax) == 4) {
+    if (curved) EMSESG_LAUNCH(ctx, "fx_push", (k_fx_push<4, true, true>), grid, PUSH_BLOCK, smem, a);
+    else EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<4>, grid, PUSH_BLOCK, smem, a);
+  } else {
+    if (curved) EMSESG_LAUNCH(ctx, "fx_push", (k_fx_push<8, true, true>), grid, PUSH_BLOCK, smem, a);
+    else EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<8>, grid, PUSH_BLOCK, smem, a);
+  }
   // injected particles of the tail zones (general path, global deposits)
   int64_t drawn = 0;
   for (int is = 0; is < c.nspec; is++) {
@@ -1830,6 +1887,7 @@ extern "C" int emsesg_fx_background(emsesg_ctx* ctx, int replace) {
   const Bodies bd = make_bodies(c);
   for (int is = 0; is < c.nspec; is++)
     for (int q = 0; q < bd.n; q++) {
+      if (bd.kind[q] != 0) continue;  // the counts of box bodies only
       const int64_t nodes =
           (int64_t)(bd.hi[q][0] - bd.lo[q][0] + 1) * (bd.hi[q][1] - bd.lo[q][1] + 1) * (bd.hi[q][2] - bd.lo[q][2] + 1);
       EMSESG_LAUNCH(ctx, "fx_background", k_fx_background, nblk(nodes), 256, 0, f.surf + (int64_t)is * f.nsurf, bd,

@@ -54,17 +54,50 @@ constexpr uint32_t ROW_BYTES = PUSH_THREADS * (16 + 3 * 4);
 static_assert(PUSH_THREADS == EMSESG_FX_ROW_SLOTS, "row width of the thread-major layout");
 static_assert(ROW_BYTES % 16 == 0 && (PUSH_THREADS * 4) % 16 == 0, "bulk copies move whole 16-byte units");
 
-// Box bodies of the FP32 form (geotype 0/1 with integer bounds): the
-// absorption test and the per-surface-cell counts.  Faces -x,+x,-y,+y,-z,+z;
-// a face's cells with its first tangential axis fastest (x faces: y then z;
-// y faces: x then z; z faces: x then y).
+// Bodies of the FP32 form, in the order of cfg.body.  Box bodies (geotype
+// 0/1 with integer bounds): the absorption test and the per-surface-cell
+// counts; faces -x,+x,-y,+y,-z,+z, a face's cells with its first tangential
+// axis fastest (x faces: y then z; y faces: x then z; z faces: x then y).
+// Cylinders (geotype 2) and spheres (3): the absorption test of the end
+// point (psolve1.F90:684-712) and the body's influx; lo / hi are then the
+// cells their bounding box touches, and they have no surface cells.
 struct Bodies {
-  int n;                        // box bodies
+  int n;                        // bodies
   int ipc[EMSESG_INPC];         // their index in cfg.body
+  int kind[EMSESG_INPC];        // 0 box, 2 cylinder, 3 sphere
   int lo[EMSESG_INPC][3], hi[EMSESG_INPC][3];
-  int64_t off[EMSESG_INPC][6];  // first surface cell of each face
-  int64_t nsurf;                // surface cells of all bodies
+  int64_t off[EMSESG_INPC][6];  // first surface cell of each face (boxes)
+  int64_t nsurf;                // surface cells of all box bodies
+  int ncurved;                  // cylinders and spheres
+  int cax[EMSESG_INPC];         // cylinder axis 0..2; its transverse axes are cax+1, cax+2 (mod 3)
+  float cen[EMSESG_INPC][3];    // sphere centre; cylinder: cyl_axis(1:2) in [cax+1], [cax+2]
+  float edge[EMSESG_INPC][2];   // cylinder extent along its axis (inclusive)
+  float r2[EMSESG_INPC];        // radius squared (strict inside)
 };
+
+// Whether the point (cell ac, offset af per axis) lies inside curved body q
+// (psolve1.F90:684-712: d1^2 + d2^2 < r^2 with the axial coordinate within
+// the cylinder's edges, inclusive; |x - c|^2 < r^2 for a sphere).  Each
+// difference is taken from the integer cell first, so it keeps the offset's
+// precision.
+__device__ __forceinline__ bool in_curved(const Bodies& bd, int q, const int (&ac)[3], const float (&af)[3]) {
+  if (bd.kind[q] == 3) {
+    float s = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const float x = ((float)ac[d] - bd.cen[q][d]) + af[d];
+      s = fmaf(x, x, s);
+    }
+    return s < bd.r2[q];
+  }
+  const int c0 = bd.cax[q], c1 = c0 == 2 ? 0 : c0 + 1, c2 = c0 == 0 ? 2 : c0 - 1;
+  const float xl = ((float)ac[c0] - bd.edge[q][0]) + af[c0];
+  const float xu = ((float)ac[c0] - bd.edge[q][1]) + af[c0];
+  if (!(xl >= 0.f && xu <= 0.f)) return false;
+  const float d1 = ((float)ac[c1] - bd.cen[q][c1]) + af[c1];
+  const float d2 = ((float)ac[c2] - bd.cen[q][c2]) + af[c2];
+  return fmaf(d1, d1, d2 * d2) < bd.r2[q];
+}
 
 // Slab mode (the grid is one z slab of a larger grid, periodic in z, cut
 // into slabs of equal thickness): particles that leave through a z face go
@@ -480,14 +513,28 @@ struct CrossCtx {
   int* status;
 };
 
-// Box absorption of the end point a = (ac, af) per axis (psolve1.F90:
-// 644-662, inclusive bounds); counts influx, infhist and the surface cell of
-// the face crossed last on the way from b = (ib, ob) (the rule of the oracle's
-// orc_surface_cell).  Returns true when the particle was absorbed.
-__device__ __forceinline__ bool body_absorb(const CrossCtx& c, const int (&ib)[3], const float (&ob)[3],
-                                            const Axis* a3) {
+// Absorption of the end point by the bodies in their order, the first that
+// holds it taking it (psolve1.F90:639-715).  A box tests a = (ac, af) per
+// axis (:644-662, inclusive bounds) and counts influx, infhist and the
+// surface cell of the face crossed last on the way from b = (ib, ob) (the
+// rule of the oracle's orc_surface_cell); a cylinder or sphere tests the
+// stored position (nc, nf) and counts influx and infhist.  Returns 0 (not
+// absorbed), ABS_BOX (the particle stops at the relay point: no second
+// zigzag segment, :660-662) or ABS_CURVED (both segments deposited).
+constexpr int ABS_BOX = 1, ABS_CURVED = 2;
+template <bool CURV>
+__device__ __forceinline__ int body_absorb(const CrossCtx& c, const int (&ib)[3], const float (&ob)[3],
+                                           const Axis* a3) {
   const Bodies& bd = *c.bd;
   for (int q = 0; q < bd.n; q++) {
+    if (CURV && bd.kind[q] != 0) {
+      const int nc3[3] = {a3[0].nc, a3[1].nc, a3[2].nc};
+      const float nf3[3] = {a3[0].nf, a3[1].nf, a3[2].nf};
+      if (!in_curved(bd, q, nc3, nf3)) continue;
+      atomicAdd(&c.gc->influx[c.is][bd.ipc[q]], 1);
+      atomicAdd(&c.gc->infhist[c.is][bd.ipc[q]][0], 1);
+      return ABS_CURVED;
+    }
     bool in = true;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -527,15 +574,16 @@ __device__ __forceinline__ bool body_absorb(const CrossCtx& c, const int (&ib)[3
     const int v = min(max(c2, bd.lo[q][e2]), bd.hi[q][e2] - 1) - bd.lo[q][e2];
     const int64_t cellx = bd.off[q][2 * best + side] + u + (int64_t)(bd.hi[q][e1] - bd.lo[q][e1]) * v;
     atomicAdd(&c.surf[cellx], 1ull);
-    return true;
+    return ABS_BOX;
   }
-  return false;
+  return 0;
 }
 
 // General path for one particle that left its cell (or whose cell lies
 // outside the box): boundary rules, zigzag with relay point, charge at the
-// stored cell; the final record is written here.
-template <int B, bool DEP = true>
+// stored cell; the final record is written here.  CURV = false: the run has
+// box bodies only.
+template <int B, bool DEP = true, bool CURV = true>
 __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, const int (&o)[3], const Sink& sk,
                                          const CrossCtx& c, const float* en) {
   const int loc = __float_as_int(en[0]);
@@ -551,13 +599,14 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
   if (ay.flip) vy = -vy;
   if (az.flip) vz = -vz;
   const bool escaped = ax.dead || ay.dead || az.dead;
-  bool absorbed = false;
+  int absorbed = 0;
   if (!escaped && c.bd->n > 0) {
     const int ib3[3] = {ib, jb, kb};
     const float ob3[3] = {bx, by, bz};
     const Axis a3[3] = {ax, ay, az};
-    absorbed = body_absorb(c, ib3, ob3, a3);
+    absorbed = body_absorb<CURV>(c, ib3, ob3, a3);
   }
+  const bool stop = absorbed == ABS_BOX;
   // slab mode: a particle leaving through a z face moves to the neighbouring
   // slab (its stored position, the slab's periodic wrap, is its position
   // there); its current stays here, in the guard planes that the ranks
@@ -601,11 +650,11 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
     w = xd * yd; J[11] = vvz * w; J[9] = vvz * (xd - w); J[10] = vvz * (yd - w); J[8] = vvz * (1.0f - xd - (yd - w));
   }
   // both segments in the cell of the start point (a particle that did not
-  // change cell): one set of node values.  An absorbed particle stops at the
-  // relay point (psolve1.F90:660-662): no second segment.
-  const bool one = !absorbed && ax.ia == ib && ay.ia == jb && az.ia == kb;
+  // change cell): one set of node values.  A particle absorbed by a box
+  // stops at the relay point (psolve1.F90:660-662): no second segment.
+  const bool one = !stop && ax.ia == ib && ay.ia == jb && az.ia == kb;
   if (!one) put_j<B>(box, o, sk, ib, jb, kb, J, c.qfix);
-  if (!absorbed) {
+  if (!stop) {
     float J2[NJ];
     float xd = ((float)(ax.ac - ax.ia) + ax.af + (float)(ax.rc - ax.ia) + ax.rf) * 0.5f;
     float yd = ((float)(ay.ac - ay.ia) + ay.af + (float)(ay.rc - ay.ia) + ay.rf) * 0.5f;
@@ -639,7 +688,7 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
 // holding their position before this step and the velocity the row loop
 // gave them): each lane takes one and runs the general path.  Returns the
 // number of this lane's particles that escaped.
-template <int B, bool DEP>
+template <int B, bool DEP, bool CURV>
 __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t slot0, unsigned long long* box,
                                           const int (&o)[3], const int* xl, int xn, int lane) {
   __syncwarp();
@@ -656,15 +705,18 @@ __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t s
     const float4 ps = a.rpos[slot0 + loc];  // the position before the step
     const float vx = c.gvx[loc], vy = c.gvy[loc], vz = c.gvz[loc];
     const float en[XQW] = {__int_as_float(loc), ps.w, ps.x, ps.y, ps.z, vx, vy, vz};
-    dead += cross_one<B, DEP>(g, box, o, sk, c, en);
+    dead += cross_one<B, DEP, CURV>(g, box, o, sk, c, en);
   }
   __syncwarp();
   return dead;
 }
 
 // DEP = false: the move only (positions, velocities, boundary rules; no
-// current, no charge), for recomputing particle states.
-template <int T, bool DEP = true>
+// current, no charge), for recomputing particle states.  CURV = true: the
+// run has cylinders or spheres (tile regions next to one push every
+// particle on the general path); without them the in-cell test keeps its
+// constant bound.
+template <int T, bool DEP = true, bool CURV = false>
 __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   constexpr int B = T + 2 * PG + 1;  // box and field tile edge (nodes)
   constexpr int NBOX = 4 * B * B * B;
@@ -773,6 +825,18 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
 
   const float qmp = a.qmp[is], qfix = a.qfix[is];
   const float gustep = a.gustep, hr = 0.5f * a.rustep;
+  // A particle can enter a cylinder or a sphere without leaving its cell: in
+  // a tile region whose box touches one, every particle takes the general
+  // path (the in-cell test below then fails for all).
+  float flo = 0.f;
+  if (CURV)
+    for (int q = 0; q < a.bd.n; q++) {
+      if (a.bd.kind[q] == 0) continue;
+      bool hit = true;
+#pragma unroll
+      for (int d = 0; d < 3; d++) hit = hit && o[d] + B - 2 >= a.bd.lo[q][d] && o[d] <= a.bd.hi[q][d];
+      if (hit) flo = 2.0f;
+    }
 
   float acc[NJ + NR];
 #pragma unroll
@@ -873,7 +937,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       szz = ps.z + vz * gustep;
       // an end point exactly on a cell face takes the general path (it may
       // lie on a body face: inclusive bounds)
-      const bool incell = sx > 0.f && sx < 1.0f && syy > 0.f && syy < 1.0f && szz > 0.f && szz < 1.0f;
+      const bool incell = sx > flo && sx < 1.0f && syy > 0.f && syy < 1.0f && szz > 0.f && szz < 1.0f;
       simple = incell && (!DEP || (cell == runcell && runbase >= 0));
       // a particle that stays in its cell but is out of place in the thread's
       // run (it changed cell since the sort): its 20 sums go to the run queue
@@ -955,7 +1019,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     ph = par1;
   }
   if (xqn) {
-    nesc += cross_list<B, DEP>(a, is, slot0, box, o, xl, xqn, lane);
+    nesc += cross_list<B, DEP, CURV>(a, is, slot0, box, o, xl, xqn, lane);
     xqn = 0;
   }
   if (r >= L || failed) break;

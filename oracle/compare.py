@@ -196,3 +196,31 @@ def near_faces(cfg, start, end, bodies=(), band: float = BAND, tie: float = 1e-5
         close = (ts[:, 1] >= 0) & (ts[:, 2] - ts[:, 1] < tie)
         near |= inside & close
     return near
+
+
+def near_curved(end, bodies, band: float = 1e-5) -> np.ndarray:
+    """Particles whose FP64 end point lies within `band` (cells) of the
+    surface of a cylinder or a sphere, where FP32 rounding of the position
+    or of the squared distance can flip the absorption test of
+    psolve1.F90:684-712.  bodies: emsesg_body-like dicts (geotype 2 with
+    cyl_align, cyl_axis, cyl_edge, radius; geotype 3 with sph_center,
+    radius); other geotypes are skipped."""
+    e = np.stack([end[f] for f in "xyz"], 1)
+    near = np.zeros(e.shape[0], dtype=bool)
+    for b in bodies:
+        if b["geotype"] not in (2, 3):
+            continue
+        r = float(b["radius"])
+        if b["geotype"] == 3:
+            d = np.sqrt(((e - np.asarray(b["sph_center"], float)) ** 2).sum(1))
+            near |= np.abs(d - r) < band
+        elif b["geotype"] == 2:
+            a0 = int(b["cyl_align"]) - 1
+            a1, a2 = (a0 + 1) % 3, (a0 + 2) % 3
+            d = np.hypot(e[:, a1] - b["cyl_axis"][0], e[:, a2] - b["cyl_axis"][1])
+            lo, hi = b["cyl_edge"]
+            ax = e[:, a0]
+            within = (ax >= lo - band) & (ax <= hi + band)
+            near |= within & (np.abs(d - r) < band)
+            near |= (d < r + band) & ((np.abs(ax - lo) < band) | (np.abs(ax - hi) < band))
+    return near

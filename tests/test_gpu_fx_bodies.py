@@ -173,3 +173,127 @@ def test_fx_box_inflow_emission_per_step(gpu, trng):
     net = g.fx_surface().sum(1)
     assert abs(o2.f["rhobk"].sum() - sum(cfg.q[s] * net[s] for s in range(2))) < 1e-9 * abs(cfg.q[0]) * np.abs(net).sum()
     g.close()
+
+
+# a box, a cylinder along x and a sphere, apart from each other, on a
+# periodic 24^3 grid (the cylinder's axis and the sphere's centre off the
+# cell nodes)
+CURVED = [dict(geotype=0, ncond=1, xlpc=3.0, xupc=7.0, ylpc=3.0, yupc=7.0, zlpc=3.0, zupc=7.0, sqdscaled=1.0),
+          dict(geotype=2, ncond=1, cyl_align=1, cyl_axis=(16.5, 8.25), cyl_edge=(2.0, 21.5), radius=3.3,
+               sqdscaled=1.0),
+          dict(geotype=3, ncond=0, sph_center=(15.3, 16.7, 17.1), radius=4.2)]
+
+
+def inside_any(p, bodies):
+    e = np.stack([p[f] for f in "xyz"], 1)
+    m = np.zeros(p.size, dtype=bool)
+    for b in bodies:
+        if b["geotype"] in (0, 1):
+            lo = np.array([b["xlpc"], b["ylpc"], b["zlpc"]])
+            hi = np.array([b["xupc"], b["yupc"], b["zupc"]])
+            m |= np.all((e >= lo) & (e <= hi), 1)
+        elif b["geotype"] == 3:
+            m |= ((e - np.asarray(b["sph_center"])) ** 2).sum(1) < b["radius"] ** 2
+        else:
+            a0 = b["cyl_align"] - 1
+            a1, a2 = (a0 + 1) % 3, (a0 + 2) % 3
+            d2 = (e[:, a1] - b["cyl_axis"][0]) ** 2 + (e[:, a2] - b["cyl_axis"][1]) ** 2
+            m |= (e[:, a0] >= b["cyl_edge"][0]) & (e[:, a0] <= b["cyl_edge"][1]) & (d2 < b["radius"] ** 2)
+    return m
+
+
+def test_fx_cylinder_sphere_per_step(gpu):
+    """Cylinders and spheres in the FP32 form: every step from the FP32
+    form's own state against the oracle, rho and J within 1e-5 relative L2
+    and the absorbed counts of each body equal, except for particles listed
+    as next to a decision FP32 rounding can flip (an end point within 1e-5
+    cell of a curved surface, or next to an integer plane)."""
+    c = case(n=(24, 24, 24), ppc=(6, 6), vth_scale=3.0, tile=(8, 8, 8))
+    c.bodies = CURVED
+    cfg, eb, p, tp = build(c, capacity_factor=1.5)
+    parts, counts = [], []
+    base = np.concatenate([[0], np.cumsum(tp)])
+    for s in range(cfg.nspec):
+        seg = p[base[s]:base[s + 1]]
+        seg = seg[~inside_any(seg, CURVED)]
+        parts.append(seg)
+        counts.append(seg.size)
+    p, tp = np.concatenate(parts), np.array(counts, dtype=np.int64)
+    g = Emses(cfg)
+    g.upload_particles(p, tp)
+    g.upload_field("eb", eb)
+    g.fx_load()
+    g.fx_store()
+    cur, tp_cur = g.download_particles()
+    gc_prev = g.get_counters().as_dict()
+    totals = np.zeros(3, dtype=np.int64)
+    listed_all = 0
+    for step in range(4):
+        o = O.Oracle(cfg, cur, tp_cur, eb)
+        o.grdcrt()
+        o.f["aj"][...] = 0.0
+        o.psolve1(2, 0)
+        o.reduce_aj()
+        o.charge(0)
+        o.reduce_rho("rho")
+        g.fx_step(2, step % 2 == 1)
+        er = C.field_errors(g.download_field("rho"), o.f["rho"], cfg)["l2_rel"]
+        ej = C.field_errors(g.download_field("aj"), o.f["aj"], cfg)["l2_rel"]
+        live = cur["nid"] != -1  # records of particles that died since the last sort stay in place
+        near = live & (C.near_faces(cfg, cur, o.pbuf, bodies=[((3, 3, 3), (7, 7, 7))])
+                       | C.near_curved(o.pbuf, CURVED))
+        nl = int(near.sum())
+        gc = g.get_counters().as_dict()
+        og = o.gc.as_dict()
+        d_influx = gc["influx"][:2, :3] - gc_prev["influx"][:2, :3]
+        diff = np.abs(d_influx - og["influx"][:2, :3])
+        print(f"step {step}: rho {er:.2e}, J {ej:.2e}, influx {d_influx.sum(0)} (oracle {og['influx'][:2, :3].sum(0)}), "
+              f"difference {int(diff.sum())}, listed {nl}")
+        assert er < 1e-5 and ej < 1e-5, step
+        assert int(diff.sum()) <= nl, step
+        if nl == 0:
+            assert int(diff.sum()) == 0
+        # escapes: periodic, none
+        assert int((gc["nesc"][:2] - gc_prev["nesc"][:2]).sum()) == 0
+        totals += og["influx"][:2, :3].sum(0)
+        listed_all += nl
+        gc_prev = gc
+        g.fx_store()
+        cur, tp_cur = g.download_particles()
+        # the absorbed particles are gone: what is left lies outside every body
+        # (up to the listed band)
+        left = (inside_any(cur, CURVED) & (cur["nid"] != -1) & ~C.near_curved(cur, CURVED)
+                & ~C.near_faces(cfg, cur, cur))
+        assert not left.any(), step
+    print("absorbed per body", totals, "listed", listed_all)
+    assert np.all(totals > 10)   # every body absorbed particles
+    g.close()
+
+
+def test_fx_load_plasma_leaves_out_curved_bodies(gpu):
+    """The FP32 plasma loader places no particle inside a body (the push's
+    absorption test), and places the same particles as the loader of the
+    FP64 records outside them."""
+    from ctca_b200 import inputs as I
+    c = case(n=(24, 24, 24), ppc=(5, 5), tile=(8, 8, 8))
+    c.bodies = CURVED
+    cfg = I.make_config(c)
+    eb = I.make_fields(c)
+    pl = I.plasma(c, seed=9)
+    with Emses(cfg) as a, Emses(cfg) as b:
+        for g in (a, b):
+            g.upload_field("eb", eb)
+        a.load_plasma(pl)
+        a.fx_load()
+        a.fx_store()
+        pa, ta = a.download_particles()
+        b.fx_load_plasma(pl)
+        b.fx_store()
+        pb, tb = b.download_particles()
+    pb = pb[pb["nid"] != -1]
+    keep = ~inside_any(pa, CURVED)
+    edge = C.near_curved(pa, CURVED) | C.near_faces(cfg, pa, pa)
+    assert not (inside_any(pb, CURVED) & ~C.near_curved(pb, CURVED) & ~C.near_faces(cfg, pb, pb)).any()
+    # the same particles outside the bodies (up to those on a surface)
+    assert abs(int(pb.size) - int(keep.sum())) <= int(edge.sum())
+    assert pb.size < pa.size
