@@ -185,16 +185,17 @@ def near_faces(cfg, start, end, bodies=(), band: float = BAND, tie: float = 1e-5
     (lo[3], hi[3]) integer boxes."""
     e = np.stack([end[f] for f in "xyz"], 1)
     s = np.stack([start[f] for f in "xyz"], 1)
-    frac = e - np.floor(e)
-    near = np.any((frac < band) | (frac > 1.0 - band), 1)
-    for lo, hi in bodies:
-        lo, hi = np.asarray(lo, float), np.asarray(hi, float)
-        inside = np.all((e >= lo) & (e <= hi), 1)
-        with np.errstate(divide="ignore", invalid="ignore"):
+    # (records of dead particles may hold no number: they compare false)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        frac = e - np.floor(e)
+        near = np.any((frac < band) | (frac > 1.0 - band), 1)
+        for lo, hi in bodies:
+            lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+            inside = np.all((e >= lo) & (e <= hi), 1)
             t = np.where(s < lo, (lo - s) / (e - s), np.where(s > hi, (hi - s) / (e - s), -1.0))
-        ts = np.sort(t, 1)
-        close = (ts[:, 1] >= 0) & (ts[:, 2] - ts[:, 1] < tie)
-        near |= inside & close
+            ts = np.sort(t, 1)
+            close = (ts[:, 1] >= 0) & (ts[:, 2] - ts[:, 1] < tie)
+            near |= inside & close
     return near
 
 
