@@ -519,6 +519,8 @@ int fx_alloc(emsesg_ctx* ctx) {
                                           move_smem<MoveBig>()));
     EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_move<MoveSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           move_smem<MoveSmall>()));
+    EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_move<MoveMid>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          move_smem<MoveMid>()));
   }
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(4)));
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(8)));
@@ -661,6 +663,10 @@ int fx_local_sort(emsesg_ctx* ctx, bool* done) {
     // upper bound between synchronisations: escapes are not in it)
     if (ctx->totalp[is] + nt <= (int64_t)MOVE_SMALL_ROWS * PUSH_THREADS * f.ntiles)
       EMSESG_LAUNCH(ctx, "lcs_move", k_lcs_move<MoveSmall>, (unsigned)f.ntiles, PUSH_THREADS, move_smem<MoveSmall>(),
+                    f.pos + off, f.vx + off, f.vy + off, f.vz + off, f.tile_start + is * T1, f.tile_pad + is * T1, ts2,
+                    tp2, f.lcs_inv + off, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off, stray);
+    else if (ctx->totalp[is] + nt <= (int64_t)MOVE_MID_ROWS * PUSH_THREADS * f.ntiles)
+      EMSESG_LAUNCH(ctx, "lcs_move", k_lcs_move<MoveMid>, (unsigned)f.ntiles, PUSH_THREADS, move_smem<MoveMid>(),
                     f.pos + off, f.vx + off, f.vy + off, f.vz + off, f.tile_start + is * T1, f.tile_pad + is * T1, ts2,
                     tp2, f.lcs_inv + off, f.pos2 + off, f.vx2 + off, f.vy2 + off, f.vz2 + off, stray);
     else

@@ -407,22 +407,28 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restr
 // take half that, and the copies go through L1, which then holds the
 // recent columns of the old region: the particles that changed cell along
 // z (whose rank moves by a z-layer, tens of columns) are found there.
+// A third shape (MoveMid) for tiles of up to 56 rows keeps two groups'
+// copies in flight (three buffers) while one group is written.
 // grid = ntiles, block = PUSH_THREADS (one CTA per SM), shared =
-// 2 * Cfg::BUF.
-template <int WIN_, int SLOTS_, bool CA_>
+// Cfg::NBUF * Cfg::BUF.
+template <int WIN_, int SLOTS_, bool CA_, int NBUF_ = 2>
 struct MoveCfg {
   static constexpr int WIN = WIN_;      // window particles of one buffer
   static constexpr int SLOTS = SLOTS_;  // slots of one group (staged inv)
   static constexpr bool CA = CA_;       // copies cached in L1
+  static constexpr int NBUF = NBUF_;    // buffers: NBUF - 1 groups in flight while one is written
   static constexpr int K = (SLOTS + PUSH_THREADS - 1) / PUSH_THREADS;  // slots of a thread per group
   static constexpr int BUF = WIN * (16 + 3 * 4) + SLOTS * 4;          // bytes of one buffer
+  static_assert(NBUF == 2 || NBUF == 3, "double or triple buffering");
 };
-using MoveBig = MoveCfg<3200, 2560, false>;   // up to 80 rows of 40 columns
-using MoveSmall = MoveCfg<1600, 1280, true>;  // up to 40 rows of 40 columns
-constexpr int MOVE_SMALL_ROWS = 32;           // mean rows per tile up to which MoveSmall is used
+using MoveBig = MoveCfg<3200, 2560, false>;      // up to 80 rows of 40 columns
+using MoveMid = MoveCfg<2240, 1792, false, 3>;   // up to 56 rows of 40 columns, two groups in flight
+using MoveSmall = MoveCfg<1600, 1280, true>;     // up to 40 rows of 40 columns
+constexpr int MOVE_SMALL_ROWS = 32;              // mean rows per tile up to which MoveSmall is used
+constexpr int MOVE_MID_ROWS = 48;                // then MoveMid up to this mean
 constexpr int MOVE_MAXGROUPS = PUSH_THREADS / 32;
 template <class Cfg>
-inline int move_smem() { return 2 * Cfg::BUF; }
+inline int move_smem() { return Cfg::NBUF * Cfg::BUF; }
 static_assert(PUSH_THREADS % 32 == 0, "32-column groups divide the row");
 
 template <bool CA>
@@ -468,7 +474,7 @@ __device__ __forceinline__ void move_tile(const float4* __restrict__ pos, const 
   }
   __syncthreads();
   auto stage = [&](int grp) {
-    char* buf = reinterpret_cast<char*>(msm) + (grp & 1) * MOVE_BUF;
+    char* buf = reinterpret_cast<char*>(msm) + (grp % Cfg::NBUF) * MOVE_BUF;
     float4* wpos = reinterpret_cast<float4*>(buf);
     float* wv = reinterpret_cast<float*>(wpos + MOVE_WIN);
     uint32_t* winv = reinterpret_cast<uint32_t*>(wv + 3 * MOVE_WIN);
@@ -497,15 +503,25 @@ __device__ __forceinline__ void move_tile(const float4* __restrict__ pos, const 
     cpa_commit();
   };
   stage(0);
+  if (Cfg::NBUF == 3 && NG > 1) stage(1);
   for (int grp = 0; grp < NG; grp++) {
-    if (grp + 1 < NG) {
+    if (Cfg::NBUF == 3) {
+      if (grp + 2 < NG) {
+        stage(grp + 2);
+        cpa_wait<2>();
+      } else if (grp + 1 < NG) {
+        cpa_wait<1>();
+      } else {
+        cpa_wait<0>();
+      }
+    } else if (grp + 1 < NG) {
       stage(grp + 1);
       cpa_wait<1>();
     } else {
       cpa_wait<0>();
     }
     __syncthreads();
-    const char* buf = reinterpret_cast<const char*>(msm) + (grp & 1) * MOVE_BUF;
+    const char* buf = reinterpret_cast<const char*>(msm) + (grp % Cfg::NBUF) * MOVE_BUF;
     const float4* wpos = reinterpret_cast<const float4*>(buf);
     const float* wvx = reinterpret_cast<const float*>(wpos + MOVE_WIN);
     const float* wvy = wvx + MOVE_WIN;
@@ -559,7 +575,7 @@ __device__ __forceinline__ void move_tile(const float4* __restrict__ pos, const 
         }
       }
     }
-    __syncthreads();  // this buffer is staged again for group grp + 2
+    __syncthreads();  // this buffer is staged again for group grp + NBUF
   }
 }
 

@@ -144,6 +144,8 @@ def _tile_key(cfg, tile, p):
     # tiles of 28 rows: the move's small shape, 40-column windows; of 1
     # row: one group of the whole row
     ((0, 0, 0), (8, 8, 8), (40, 1)),
+    # tiles of 45 rows: the mid shape, three buffers
+    ((0, 0, 0), (8, 8, 8), (64, 4)),
     # tiles of 67 rows: the large shape with windows
     ((0, 0, 0), (8, 8, 8), (96, 4)),
     # tiles of 98 rows: no window, inv read from global memory, several
