@@ -131,6 +131,7 @@ struct FxState {
   int g_ustep = 0, g_sort = 0;
   const float4* g_pos = nullptr;       // buffers and configuration it was captured with
   const int64_t* g_ts = nullptr;
+  const double* g_eb = nullptr;        // (an asynchronous eb upload swaps the eb buffer)
   emsesg_config g_cfg{};
   AdjWork* adj = nullptr;
   int64_t* accum = nullptr;         // int64 (rho, jx, jy, jz) on the rho layout

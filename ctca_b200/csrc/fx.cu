@@ -1075,8 +1075,9 @@ int fx_fields_phase(emsesg_ctx* ctx) {
   f.cont_valid = f.rho_prev;
   f.rho_prev = true;
   // the step's reads of eb are over: an asynchronous upload of the next eb
-  // may start
-  if (ctx->ev_fields) EMSESG_CUDA(ctx, cudaEventRecord(ctx->ev_fields, ctx->stream));
+  // may start (inside a stream capture the event is recorded after the
+  // graph's launch instead)
+  if (ctx->ev_fields && !f.capture) EMSESG_CUDA(ctx, cudaEventRecord(ctx->ev_fields, ctx->stream));
   return EMSESG_OK;
 }
 
@@ -2419,7 +2420,9 @@ extern "C" int emsesg_fx_run(emsesg_ctx* ctx, int ustep, int nsteps, int sort_ev
   if (!ctx || nsteps < 0 || sort_every < 1) return EMSESG_ERR_ARG;
   FxState& f = ctx->fx;
   if (!f.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
-  int rc;
+  // a pending asynchronous eb upload is taken now, outside any capture
+  int rc = apply_pending_eb(ctx);
+  if (rc) return rc;
   const int block = 2 * sort_every;
   if (!use_graph || !graph_ready(ctx) || nsteps < block) {
     for (int s = 0; s < nsteps; s++)
@@ -2427,7 +2430,7 @@ extern "C" int emsesg_fx_run(emsesg_ctx* ctx, int ustep, int nsteps, int sort_ev
     return EMSESG_OK;
   }
   if (f.gexec && (f.g_ustep != ustep || f.g_sort != sort_every || f.g_pos != f.pos || f.g_ts != f.tile_start ||
-                  memcmp(&f.g_cfg, &ctx->cfg, sizeof(emsesg_config)) != 0)) {
+                  f.g_eb != ctx->field[EMSESG_FIELD_EB] || memcmp(&f.g_cfg, &ctx->cfg, sizeof(emsesg_config)) != 0)) {
     cudaGraphExecDestroy(f.gexec);
     f.gexec = nullptr;
   }
@@ -2444,10 +2447,12 @@ extern "C" int emsesg_fx_run(emsesg_ctx* ctx, int ustep, int nsteps, int sort_ev
     f.g_sort = sort_every;
     f.g_pos = f.pos;
     f.g_ts = f.tile_start;
+    f.g_eb = ctx->field[EMSESG_FIELD_EB];
     f.g_cfg = ctx->cfg;
   }
   const int nblock = nsteps / block;
   for (int b = 0; b < nblock; b++) EMSESG_CUDA(ctx, cudaGraphLaunch(f.gexec, ctx->stream));
+  if (ctx->ev_fields) EMSESG_CUDA(ctx, cudaEventRecord(ctx->ev_fields, ctx->stream));
   ctx->rng_stream += (uint64_t)nblock * block;
   for (int s = 0; s < nsteps - nblock * block; s++)
     if ((rc = emsesg_fx_step(ctx, ustep, (s + 1) % sort_every == 0))) return rc;
@@ -2464,6 +2469,7 @@ struct emsesg_batch {
   std::vector<cudaEvent_t> ev;      // one per context: its stream's last work
   std::vector<float4*> pos;         // buffers each run was captured with
   std::vector<const int64_t*> ts;
+  std::vector<const double*> eb;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -2498,6 +2504,9 @@ extern "C" int emsesg_batch_create(emsesg_ctx* const* ctxs, int n, int ustep, in
       return set_error(c, EMSESG_ERR_ARG, "block %d is not a multiple of 2*sort_every (%d)", block, sort_every[r]);
     if (!c->fx.loaded) return set_error(c, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
     if (!graph_ready(c)) return set_error(c, EMSESG_ERR_STATE, "run is not tile-sorted or has injected particles");
+    // a pending asynchronous eb upload is taken before the capture
+    int rc0 = apply_pending_eb(c);
+    if (rc0) return rc0;
   }
   emsesg_batch* b = new emsesg_batch();
   b->ctxs.assign(ctxs, ctxs + n);
@@ -2533,6 +2542,7 @@ extern "C" int emsesg_batch_create(emsesg_ctx* const* ctxs, int n, int ustep, in
     if (e != cudaSuccess) rc = check_cuda(ctxs[r], e, "cudaGraphAddChildGraphNode");
     b->pos.push_back(ctxs[r]->fx.pos);
     b->ts.push_back(ctxs[r]->fx.tile_start);
+    b->eb.push_back(ctxs[r]->field[EMSESG_FIELD_EB]);
   }
   if (!rc) {
     e = cudaGraphInstantiate(&b->exec, parent, 0);
@@ -2558,6 +2568,10 @@ extern "C" int emsesg_batch_launch(emsesg_batch* b, int nrep) {
     emsesg_ctx* c = b->ctxs[r];
     if (c->fx.pos != b->pos[r] || c->fx.tile_start != b->ts[r] || graph_ready(c) == false)
       return set_error(c, EMSESG_ERR_STATE, "run changed since the batch was captured");
+    // the graph reads the eb buffer it was captured with; an asynchronous
+    // upload goes to the other one
+    if (c->eb_next_pending || c->field[EMSESG_FIELD_EB] != b->eb[r])
+      return set_error(c, EMSESG_ERR_STATE, "eb uploaded asynchronously since the batch was captured");
   }
   // the graph starts after each run's earlier work ...
   for (int r = 0; r < n; r++) {
@@ -2570,6 +2584,8 @@ extern "C" int emsesg_batch_launch(emsesg_batch* b, int nrep) {
   for (int r = 0; r < n; r++) {
     EMSESG_CUDA(c0, cudaStreamWaitEvent(b->ctxs[r]->stream, b->done, 0));
     b->ctxs[r]->rng_stream += (uint64_t)nrep * b->block;
+    // the graph's reads of eb are over once the run's stream gets here
+    if (b->ctxs[r]->ev_fields) EMSESG_CUDA(c0, cudaEventRecord(b->ctxs[r]->ev_fields, b->ctxs[r]->stream));
   }
   return EMSESG_OK;
 }

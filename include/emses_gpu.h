@@ -274,7 +274,12 @@ int emsesg_fx_sort(emsesg_ctx* ctx);
  * field before the next work that reads eb (an FP32 step, grdcrt, the field
  * step, a download of eb); the copy starts once the last step has read eb,
  * so it overlaps with that step's sort.  A synchronous emsesg_upload_field
- * of eb replaces a pending asynchronous one. */
+ * of eb replaces a pending asynchronous one.  The two buffers change roles
+ * with every asynchronous upload: emsesg_fx_run takes a pending upload
+ * before it captures or replays its graph and captures again when the eb
+ * buffer changed; a batch (emsesg_batch_create) takes pending uploads before
+ * its capture, and emsesg_batch_launch refuses (EMSESG_ERR_STATE) a run whose
+ * eb was uploaded asynchronously since. */
 int emsesg_fx_step_download(emsesg_ctx* ctx, int ustep, int do_sort, double* rho, double* aj);
 int emsesg_upload_field_async(emsesg_ctx* ctx, int field, const double* host);
 /* nsteps steps of the FP32 form, re-sorting every sort_every steps

@@ -315,3 +315,45 @@ def test_step_download_overlap_matches_plain_io(gpu):
         pb, tb = b.download_particles()
         assert np.array_equal(ta, tb)
         assert np.array_equal(pa.view(np.uint8), pb.view(np.uint8))
+
+
+def test_async_eb_upload_with_graph_runs(gpu):
+    """An asynchronous eb upload between graph runs (emsesg_fx_run) takes
+    effect at the next run, whose graph is captured again for the other eb
+    buffer: the same particles and rho / aj, bit for bit, as synchronous
+    uploads and step-by-step runs; a batch refuses to launch after an
+    asynchronous upload of one of its runs."""
+    import torch
+    from ctca_b200.emses import Batch, EmsesError
+    c = case(n=(16, 16, 16), ppc=(6, 6), vth_scale=2.0, tile=(8, 8, 8))
+    cfg, eb, p, tp = build(c, 1.2)
+    ebs = [np.ascontiguousarray(eb * (1.0 + 0.07 * k)) for k in range(3)]
+    pinned = [torch.from_numpy(e.reshape(-1)).pin_memory().numpy() for e in ebs]
+    with Emses(cfg) as a, Emses(cfg) as b:
+        for g in (a, b):
+            g.upload_particles(p, tp)
+            g.upload_field("eb", ebs[0])
+            g.fx_load()
+        for k in range(3):
+            if k > 0:
+                a.upload_field("eb", ebs[k])
+                b.upload_eb_async(pinned[k])
+            a.fx_run(2, 8, 4, use_graph=False)
+            b.fx_run(2, 8, 4, use_graph=True)
+            a.synchronize()
+            b.synchronize()
+            assert np.array_equal(a.download_field("rho"), b.download_field("rho")), k
+            assert np.array_equal(a.download_field("aj"), b.download_field("aj")), k
+        a.fx_store()
+        b.fx_store()
+        pa, _ = a.download_particles()
+        pb, _ = b.download_particles()
+        assert np.array_equal(pa.view(np.uint8), pb.view(np.uint8))
+        b.fx_load()
+        batch = Batch([b], 2, 8, [4])
+        batch.launch(1)
+        b.synchronize()
+        b.upload_eb_async(pinned[0])
+        with pytest.raises(EmsesError, match="asynchronously"):
+            batch.launch(1)
+        batch.close()
