@@ -30,6 +30,11 @@ of side 16..64 in one CUDA graph) against the same runs launched one after
 the other.  --workload ensemble prints the full ensemble line instead
 (512 runs x 200 steps by default).
 
+--workload em and --workload es run the headline plasma self-consistently
+with the field solve on the device every step: the EM leapfrog (bfield,
+push, bfield, efield, border exchange) or the electrostatic loop (push, rho,
+FFT Poisson solve, E from phi).
+
 --workload slabs runs the headline plasma on a grid cut into z slabs
 (ctca_b200/slabs.py): with torchrun and N GPUs one 128^3 slab per GPU
 (128 x 128 x 128N cells, weak scaling) exchanging the particles that change
@@ -980,11 +985,13 @@ def run_body_line(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
-def run_em_line(args, world, rank, local):
+def run_em_line(args, world, rank, local, es=False):
     """The headline workload run self-consistently with the fields on the
     device: each step is bfield, push + J + rho, bfield, efield and the eb
     border exchange (emsesg_fx_em_step; tcs = 2 (c dt)^2 = 0.125 in internal
-    units for c dt / dx = 0.5); sort every 4 steps."""
+    units for c dt / dx = 0.5); sort every 4 steps.  With es (--workload es)
+    the electrostatic loop instead: push + J + rho, then E from rho by the
+    FFT Poisson solve (emsesg_esfield)."""
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the reference's field solver is not built (no "
@@ -1006,7 +1013,11 @@ def run_em_line(args, world, rank, local):
     k = [0]
 
     def step():
-        g.fx_em_step(2, k[0] % SORT_EVERY == SORT_EVERY - 1, 0.125)
+        if es:
+            g.fx_step(2, k[0] % SORT_EVERY == SORT_EVERY - 1)
+            g.esfield(1, check=False)
+        else:
+            g.fx_em_step(2, k[0] % SORT_EVERY == SORT_EVERY - 1, 0.125)
         k[0] += 1
 
     for _ in range(args.warmup):
@@ -1027,14 +1038,17 @@ def run_em_line(args, world, rank, local):
     barrier(world)
     t = max_over_ranks(world, e0.elapsed_time(e1) / 1e3)
     prof = g.profile()
-    field_ms = sum(prof.get(n, (0.0, 0))[0] for n in ("bfield", "efield", "exchange_eb"))
+    fields = ("es_pack", "es_fft", "es_divide", "es_unpack", "es_efield") if es else ("bfield", "efield", "exchange_eb")
+    field_ms = sum(prof.get(n, (0.0, 0))[0] for n in fields)
     out = {"metric": METRIC, "value": world * npart * args.steps / t, "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64 (fields f64)",
            "data": "synthetic",
            "config": {"workload": f"{case.n[0]}^3 periodic, 2 species x {case.species[0].ppc} ppc ({npart:,} "
-                                  "particles), EM fields advanced on the device each step (bfield, push, bfield, "
-                                  "efield, border exchange), sort every 4",
+                                  "particles), " + ("electrostatic field solved on the device each step (push, "
+                                  "rho, FFT Poisson solve, E from phi)" if es else "EM fields advanced on the "
+                                  "device each step (bfield, push, bfield, efield, border exchange)") +
+                                  ", sort every 4",
                       "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
            "field_step_ms": field_ms / args.steps,
            "gpu_launches": int(sum(n for _, n in prof.values())),
@@ -1059,7 +1073,7 @@ def main():
     ap.add_argument("--ppc", type=int, default=0, help="particles per cell per species with --cells")
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and ensemble sections")
     ap.add_argument("--workload", default="particle_step",
-                    choices=["particle_step", "ensemble", "body", "em", "slabs"])
+                    choices=["particle_step", "ensemble", "body", "em", "es", "slabs"])
     ap.add_argument("--body-scale", type=float, default=1.0, help="grid scale of the body workload (1: 256x256x512)")
     ap.add_argument("--host-inject", action="store_true",
                     help="body workload: draw the injected records on the host (else on the device)")
@@ -1070,8 +1084,8 @@ def main():
     try:
         if args.workload == "body":
             run_body_line(args, world, rank, local)
-        elif args.workload == "em":
-            run_em_line(args, world, rank, local)
+        elif args.workload in ("em", "es"):
+            run_em_line(args, world, rank, local, es=args.workload == "es")
         elif args.workload == "slabs":
             run_slabs_line(args, world, rank, local)
         elif args.workload == "ensemble":

@@ -28,7 +28,9 @@ SOURCES = {
     "sort.cu": [],
     "fx.cu": [],
     "noalloc.cu": [],
+    "esfield.cu": [],
 }
+LIBS = ["-lcufft"]  # the electrostatic field step's FFTs
 
 
 def nvcc() -> str:
@@ -59,7 +61,7 @@ def build(verbose: bool = False, force: bool = False, extra: list[str] | None = 
             subprocess.run(cmd, check=True)
     if force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         tmp = LIB.with_suffix(".so.tmp")
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs)]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), *LIBS]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -149,6 +149,19 @@ struct FxState {
 
 }  // namespace emsesg
 
+// Electrostatic field step (esfield.cu): cuFFT plans (cufftHandle values),
+// the dense rho / phi of the nodes 0..n-1, its spectrum, the eigenvalues of
+// the three axes and the residual sum.
+struct EsState {
+  int fwd = 0, inv = 0;
+  bool has_fwd = false, has_inv = false;
+  double* r = nullptr;
+  void* c = nullptr;
+  double* lam = nullptr;
+  double* sum = nullptr;
+  bool ready = false;
+};
+
 struct emsesg_ctx {
   emsesg_config cfg;
   emsesg_config* d_cfg = nullptr;      // device copy of cfg for the kernels
@@ -169,6 +182,7 @@ struct emsesg_ctx {
   emsesg_particle* pbuf = nullptr;     // device pbuf, one region per species
   emsesg_particle* pbuf2 = nullptr;    // scratch for sort / compaction
   double* field[EMSESG_NFIELDS] = {nullptr};
+  EsState es;
   double* node64 = nullptr;            // drop-in node field: 8 doubles / node
   double* tj = nullptr;                // per-species zigzag scratch (aj layout)
   emsesg_counter* d_counter = nullptr;
@@ -241,6 +255,7 @@ int ensure_sort_scratch(emsesg_ctx* ctx, int64_t n);
 
 int fx_alloc(emsesg_ctx* ctx);
 void fx_free(emsesg_ctx* ctx);
+void es_free(emsesg_ctx* ctx);
 
 }  // namespace emsesg
 

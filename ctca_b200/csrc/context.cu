@@ -18,6 +18,7 @@ FieldDesc field_desc(const emsesg_config& c, int field) {
     case EMSESG_FIELD_RHODG: return {2 * c.nspec + 1, -1, nx + 3, ny + 3, nz + 3};
     case EMSESG_FIELD_RHOBK: return {1, -1, nx + 3, ny + 3, nz + 3};
     case EMSESG_FIELD_RHOBKSP: return {1, -1, nx + 3, ny + 3, nz + 3};
+    case EMSESG_FIELD_PHI: return {1, -1, nx + 3, ny + 3, nz + 3};
   }
   return {0, 0, 0, 0, 0};
 }
@@ -188,6 +189,7 @@ extern "C" int emsesg_destroy(emsesg_ctx* ctx) {
   cudaFree(ctx->sort.hist);
   cudaFree(ctx->sort.scan_tmp);
   fx_free(ctx);
+  es_free(ctx);
   for (auto e : ctx->timer.pool) cudaEventDestroy(e);
   if (ctx->side) cudaStreamSynchronize(ctx->side);
   cudaFree(ctx->eb_next);

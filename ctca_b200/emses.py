@@ -43,7 +43,7 @@ PCL_TO_BE_ACCUMULATED_AS_ANTIPCL = -2
 # Slots per row of the FP32 form's thread-major tile regions (EMSESG_FX_ROW_SLOTS).
 FX_ROW_SLOTS = 736
 
-FIELDS = {"eb": 0, "wrk": 1, "aj": 2, "ajdg": 3, "rho": 4, "rhodg": 5, "rhobk": 6, "rhobksp": 7}
+FIELDS = {"eb": 0, "wrk": 1, "aj": 2, "ajdg": 3, "rho": 4, "rhodg": 5, "rhobk": 6, "rhobksp": 7, "phi": 8}
 
 # oh_particle (lib/ohhelp/ohhelp-1.1.1/oh_type.F90:15-28): 64 bytes.
 PARTICLE_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("vx", "<f8"), ("vy", "<f8"),
@@ -126,6 +126,7 @@ _SIGS = {
     "emsesg_efield": (_I, [_P, _I, ctypes.c_double, ctypes.c_double]),
     "emsesg_exchange_eb": (_I, [_P]),
     "emsesg_fx_em_step": (_I, [_P, _I, _I, ctypes.c_double]),
+    "emsesg_esfield": (_I, [_P, _I, _P]),
     "emsesg_energy": (_I, [_P, ctypes.POINTER(ctypes.c_double)]),
     "emsesg_fx_load": (_I, [_P]),
     "emsesg_fx_store": (_I, [_P]),
@@ -230,6 +231,7 @@ def field_extents(cfg: Config, name: str) -> tuple[int, int, int, int, int]:
         "rhodg": (2 * ns + 1, -1, nx + 3, ny + 3, nz + 3),
         "rhobk": (1, -1, nx + 3, ny + 3, nz + 3),
         "rhobksp": (1, -1, nx + 3, ny + 3, nz + 3),
+        "phi": (1, -1, nx + 3, ny + 3, nz + 3),
     }[name]
 
 
@@ -378,6 +380,14 @@ class Emses:
     def fx_em_step(self, ustep: int, do_sort: bool, tcs: float):
         """bfield, fx_step, bfield, efield, exchange_eb (the main loop's order)."""
         self._check(self.lib.emsesg_fx_em_step(self.h, ustep, 1 if do_sort else 0, tcs))
+
+    def esfield(self, mltstp: int = 1, check: bool = True):
+        """The electrostatic field from rho (esfld1(0) + poisson + esfld2,
+        periodic fields): phi and EX..EZ of eb on the device.  With check,
+        returns poichk's residual."""
+        r = ctypes.c_double()
+        self._check(self.lib.emsesg_esfield(self.h, int(mltstp), ctypes.byref(r) if check else None))
+        return r.value if check else None
 
     def energy(self) -> np.ndarray:
         e = (ctypes.c_double * (3 * ISPEC))()

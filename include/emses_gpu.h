@@ -47,6 +47,7 @@
  *   rhodg  (2*nspec+1,-1:nx+1, -1:ny+1, -1:nz+1)   EMSESG_FIELD_RHODG
  *   rhobk  (1,        -1:nx+1, -1:ny+1, -1:nz+1)   EMSESG_FIELD_RHOBK
  *   rhobksp(1,        -1:nx+1, -1:ny+1, -1:nz+1, nspec) EMSESG_FIELD_RHOBKSP
+ *   phi    (1,        -1:nx+1, -1:ny+1, -1:nz+1)   EMSESG_FIELD_PHI
  *
  * Error convention: every function returns an int status (EMSESG_OK == 0);
  * none of them exits, aborts or traps.  emsesg_last_error() gives the text.
@@ -92,7 +93,8 @@ extern "C" {
 #define EMSESG_FIELD_RHODG 5
 #define EMSESG_FIELD_RHOBK 6
 #define EMSESG_FIELD_RHOBKSP 7
-#define EMSESG_NFIELDS 8
+#define EMSESG_FIELD_PHI 8
+#define EMSESG_NFIELDS 9
 
 /* The OhHelp particle record oh_particle (oh_type.F90:15-28, oh_part.h:23-28,
  * OH_BIG_SPACE off): 64 bytes. */
@@ -242,6 +244,23 @@ int emsesg_exchange_eb(emsesg_ctx* ctx);
  * fields, no bodies): bfield, emsesg_fx_step (push, J, rho), bfield,
  * efield, exchange_eb -- the order of the reference's main loop. */
 int emsesg_fx_em_step(emsesg_ctx* ctx, int ustep, int do_sort, double tcs);
+
+/* emsesg_esfield: the electrostatic field from rho on the device, for
+ * periodic fields (nfbnd 0 on every axis; else EMSESG_ERR_UNSUPPORTED).
+ * Replaces esfld1(0) with poisson(3) (src/field/esfild.F90:5-236,
+ * src/field/poisson/poissn.F90:4-890, the periodic set-up of
+ * src/field/poisson/inifft.F90:389-470), the periodic guards of phi and
+ * esfld2 (src/field/esfild.F90:351-366): phi (EMSESG_FIELD_PHI, nodes
+ * -1..n+1) is the zero-mean solution of
+ * rho + (sum of the six neighbours of phi) - 6 phi = mean(rho) on the nodes
+ * 0..n-1, by a real-to-complex FFT (cuFFT) divided by the reference's
+ * eigenvalues (2 sin(pi m / n))^2 and nx ny nz; EX..EZ of eb become
+ * (phi(i) - phi(i+1)) * mltstp on their staggered positions and zero
+ * elsewhere; BX..BZ are left as they are.  FP64.  With resid non-null it
+ * also returns poichk's residual (src/field/poisson/poissn.F90:921-961):
+ * sqrt(sum over the nodes 0..n-1 of (rho + sum of neighbours - 6 phi)^2)
+ * divided by their count (synchronises).  Asynchronous otherwise. */
+int emsesg_esfield(emsesg_ctx* ctx, int mltstp, double* resid);
 /* engk[is*3 + d] = 0.5*rm(is)*sum(v_d^2)/(slx*sly*slz), FP64. */
 int emsesg_energy(emsesg_ctx* ctx, double* engk);
 
