@@ -256,6 +256,25 @@ class SlabRank:
     def step(self, ustep: int = 2, do_sort: bool = False) -> np.ndarray:
         return exchange_step(self.io, self.dist, self.group, self.rank, self.size, ustep, do_sort)
 
+    def totals(self) -> dict:
+        """The run's global counters, summed over the ranks by one
+        all-reduce: particles per species and escapes per species."""
+        ns = self.sub.nspec
+        local = np.concatenate([self.g.fx_counts()[:ns], self.g.get_counters().as_dict()["nesc"][:ns]])
+        tot = reduce_counts(local, self.dist, self.group, self.io.device)
+        return {"particles": tot[:ns], "nesc": tot[ns:]}
+
+
+def reduce_counts(counts, dist, group=None, device=None) -> np.ndarray:
+    """int64 counters summed over the ranks of `group` by one all-reduce
+    (the global counts the reference reduces over its ranks: OhHelp's
+    per-species totals, the escape counts)."""
+    import torch
+    a = np.asarray(counts, dtype=np.int64)
+    t = torch.as_tensor(a.ravel().copy()).to(device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.cpu().numpy().reshape(a.shape)
+
 
 def exchange_step(io, dist, group, rank: int, size: int, ustep: int, do_sort: bool) -> np.ndarray:
     """One slab step of rank `rank` of `size` (size >= 2) with the exchange

@@ -137,7 +137,9 @@ def _rank(rank, world, port, nz, steps, q):
         moved = 0
         for _ in range(steps):
             moved += int(slabs.exchange_step(t, dist, None, rank, world, 1, False).sum())
-        q.put((rank, t.rho[1:nzl + 2].copy(), t.j[4:nzl + 5].copy(), np.sort(t.z + rank * nzl), moved))
+        # the global counters: one all-reduce over the ranks
+        tot = slabs.reduce_counts(np.array([[t.z.size, moved]]), dist)
+        q.put((rank, t.rho[1:nzl + 2].copy(), t.j[4:nzl + 5].copy(), np.sort(t.z + rank * nzl), moved, tot))
     finally:
         dist.destroy_process_group()
 
@@ -159,8 +161,10 @@ def test_slab_exchange_over_gloo_ranks(world):
     nzl = nz // world
     rho = np.zeros(nz + 1, dtype=np.int64)
     j = np.zeros(nz + 1, dtype=np.int64)
-    for r, rr, jr, zr, moved in out:
+    moved_all = sum(o[4] for o in out)
+    for r, rr, jr, zr, moved, tot in out:
         assert moved > 0
+        assert tot.shape == (1, 2) and tot[0, 0] == ref.z.size and tot[0, 1] == moved_all
         rho[r * nzl:(r + 1) * nzl + 1] = rr
         j[r * nzl:(r + 1) * nzl + 1] = jr
         # the shared node of two slabs holds the same value on both
