@@ -160,6 +160,15 @@ struct EsState {
   double* lam = nullptr;
   double* sum = nullptr;
   bool ready = false;
+  // any field boundary (axis by axis): the mtd_vbnd it was set up for, one
+  // batched complex plan per axis, the solved nodes, the complex lines and
+  // the eigenvalues over the solved nodes
+  int gt[3] = {-1, -1, -1};
+  int gplan[3] = {0, 0, 0};
+  bool has_gplan[3] = {false, false, false};
+  double* w = nullptr;
+  void* z = nullptr;
+  double* glam = nullptr;
 };
 
 struct emsesg_ctx {

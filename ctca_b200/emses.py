@@ -126,7 +126,7 @@ _SIGS = {
     "emsesg_efield": (_I, [_P, _I, ctypes.c_double, ctypes.c_double]),
     "emsesg_exchange_eb": (_I, [_P]),
     "emsesg_fx_em_step": (_I, [_P, _I, _I, ctypes.c_double]),
-    "emsesg_esfield": (_I, [_P, _I, _P]),
+    "emsesg_esfield": (_I, [_P, _P, _P, _I, _P]),
     "emsesg_energy": (_I, [_P, ctypes.POINTER(ctypes.c_double)]),
     "emsesg_fx_load": (_I, [_P]),
     "emsesg_fx_store": (_I, [_P]),
@@ -381,12 +381,17 @@ class Emses:
         """bfield, fx_step, bfield, efield, exchange_eb (the main loop's order)."""
         self._check(self.lib.emsesg_fx_em_step(self.h, ustep, 1 if do_sort else 0, tcs))
 
-    def esfield(self, mltstp: int = 1, check: bool = True):
-        """The electrostatic field from rho (esfld1(0) + poisson + esfld2,
-        periodic fields): phi and EX..EZ of eb on the device.  With check,
-        returns poichk's residual."""
+    def esfield(self, mltstp: int = 1, check: bool = True, mtd_vbnd=(0, 0, 0), bc=None):
+        """The electrostatic field from rho (esfld1(0) + poisson + esfld2):
+        phi and EX..EZ of eb on the device.  mtd_vbnd per axis (0 periodic,
+        1 phi = 0 on the faces, 2 Neumann); bc[axis][side] the Neumann values
+        (boundary_conditions * rene).  With check, returns poichk's residual."""
         r = ctypes.c_double()
-        self._check(self.lib.emsesg_esfield(self.h, int(mltstp), ctypes.byref(r) if check else None))
+        t = (ctypes.c_int * 3)(*[int(x) for x in mtd_vbnd])
+        b = None
+        if bc is not None:
+            b = (ctypes.c_double * 6)(*[float(bc[d][s]) for d in range(3) for s in range(2)])
+        self._check(self.lib.emsesg_esfield(self.h, t, b, int(mltstp), ctypes.byref(r) if check else None))
         return r.value if check else None
 
     def energy(self) -> np.ndarray:

@@ -245,22 +245,30 @@ int emsesg_exchange_eb(emsesg_ctx* ctx);
  * efield, exchange_eb -- the order of the reference's main loop. */
 int emsesg_fx_em_step(emsesg_ctx* ctx, int ustep, int do_sort, double tcs);
 
-/* emsesg_esfield: the electrostatic field from rho on the device, for
- * periodic fields (nfbnd 0 on every axis; else EMSESG_ERR_UNSUPPORTED).
+/* emsesg_esfield: the electrostatic field from rho on the device.
  * Replaces esfld1(0) with poisson(3) (src/field/esfild.F90:5-236,
- * src/field/poisson/poissn.F90:4-890, the periodic set-up of
- * src/field/poisson/inifft.F90:389-470), the periodic guards of phi and
- * esfld2 (src/field/esfild.F90:351-366): phi (EMSESG_FIELD_PHI, nodes
- * -1..n+1) is the zero-mean solution of
- * rho + (sum of the six neighbours of phi) - 6 phi = mean(rho) on the nodes
- * 0..n-1, by a real-to-complex FFT (cuFFT) divided by the reference's
- * eigenvalues (2 sin(pi m / n))^2 and nx ny nz; EX..EZ of eb become
- * (phi(i) - phi(i+1)) * mltstp on their staggered positions and zero
- * elsewhere; BX..BZ are left as they are.  FP64.  With resid non-null it
- * also returns poichk's residual (src/field/poisson/poissn.F90:921-961):
- * sqrt(sum over the nodes 0..n-1 of (rho + sum of neighbours - 6 phi)^2)
- * divided by their count (synchronises).  Asynchronous otherwise. */
-int emsesg_esfield(emsesg_ctx* ctx, int mltstp, double* resid);
+ * src/field/poisson/poissn.F90:4-890 with the set-up of
+ * src/field/poisson/inifft.F90:389-470), the guards of phi and esfld2
+ * (src/field/esfild.F90:351-435).  mtd_vbnd[3] (x, y, z; NULL: all 0) is the
+ * reference's Poisson boundary per axis: 0 periodic (nodes 0..n-1 solved),
+ * 1 phi = 0 on the faces (nodes 1..n-1), 2 Neumann (nodes 0..n, with
+ * bcond[2 axis + side] = boundary_conditions(side+1, axis+1) * rene added as
+ * -2 bcond on the node-0 plane and +2 bcond on the node-n plane of rho;
+ * bcond NULL: zeros).  phi (EMSESG_FIELD_PHI, nodes -1..n+1) solves
+ * rho + (sum of the six neighbours of phi) - 6 phi = 0 on the solved nodes
+ * (less the mean when no axis has a face), by cuFFT transforms divided by
+ * the reference's eigenvalues -- (2 sin(pi m / n))^2 on periodic axes,
+ * 2 (1 - cos(i pi / n)) on the others -- and mfactor (n per periodic axis,
+ * 2n per other); it is zero outside the solved nodes and keeps the periodic
+ * copies on periodic axes.  EX..EZ of eb become (phi(i) - phi(i+1)) * mltstp
+ * on their staggered positions and zero elsewhere, the normal component at
+ * -1 and n copied from 0 and n-1 on a mtd_vbnd 1 axis and negated on a 2
+ * axis; BX..BZ are left as they are.  FP64.  With resid non-null it also
+ * returns poichk's residual (src/field/poisson/poissn.F90:921-961):
+ * sqrt(sum of (rho + sum of neighbours - 6 phi)^2 over its nodes -- the
+ * solved ones up to n-1 -- ) divided by their count (synchronises).
+ * Asynchronous otherwise. */
+int emsesg_esfield(emsesg_ctx* ctx, const int* mtd_vbnd, const double* bcond, int mltstp, double* resid);
 /* engk[is*3 + d] = 0.5*rm(is)*sum(v_d^2)/(slx*sly*slz), FP64. */
 int emsesg_energy(emsesg_ctx* ctx, double* engk);
 

@@ -10,7 +10,11 @@ what the reference's algorithm must give, without a GPU:
 * for any rho the result satisfies the reference's own check (poichk's
   stencil, poissn.F90:937-943): rho + sum of the six neighbours - 6 phi =
   mean(rho) on every node, with mean(phi) = 0;
-* esfld2's staggered differences and the periodic guards."""
+* esfld2's staggered differences and the periodic guards;
+* the other field boundaries (mtd_vbnd 1: phi = 0 on the faces, DST-I;
+  2: Neumann, DCT-I): one eigenfunction per axis divided by its eigenvalue,
+  the Dirichlet solution exact under poichk's stencil, the Neumann boundary
+  values added as the reference adds them, and esfld2's boundary copies."""
 import numpy as np
 import pytest
 
@@ -93,3 +97,90 @@ def test_esfld2_differences_and_guards():
            + (ey[1:nz + 1, 1:ny + 1, 1:nx + 1] - ey[1:nz + 1, 0:ny, 1:nx + 1])
            + (ez[1:nz + 1, 1:ny + 1, 1:nx + 1] - ez[0:nz, 1:ny + 1, 1:nx + 1]))
     assert np.allclose(div, 3.0 * rho, atol=1e-12 * np.abs(rho).max())
+
+
+# ---- other field boundaries (mtd_vbnd 1: phi = 0 on the faces, 2: Neumann)
+
+def nodes_grid(nz, ny, nx):
+    return np.meshgrid(np.arange(-1, nz + 2), np.arange(-1, ny + 2), np.arange(-1, nx + 2), indexing="ij")
+
+
+@pytest.mark.parametrize("mtd,shape,mode", [((1, 0, 0), (8, 9, 10), (3, 2, 1)), ((0, 1, 2), (10, 8, 9), (2, 3, 4)),
+                                            ((1, 1, 1), (8, 8, 8), (1, 5, 7)), ((2, 2, 0), (9, 10, 8), (2, 0, 3))])
+def test_eigenmodes_of_each_boundary(mtd, shape, mode):
+    """A product of one eigenfunction per axis -- cos / sin of 2 pi a i / n
+    (periodic), sin(pi a i / n) (phi = 0), cos(pi a i / n) (Neumann) -- is
+    divided by its eigenvalue sum_d lambda_d, lambda = (2 sin(pi a / n))^2
+    periodic and 2 (1 - cos(pi a / n)) otherwise."""
+    nz, ny, nx = shape
+    k, j, i = nodes_grid(nz, ny, nx)
+    n = (nx, ny, nz)
+    idx = (i, j, k)
+    f, lam = np.ones_like(i, dtype=float), 0.0
+    for d in range(3):
+        a = mode[d]
+        if mtd[d] == 0:
+            f = f * np.cos(2 * np.pi * a * idx[d] / n[d])
+            lam += (2 * np.sin(np.pi * a / n[d])) ** 2
+        elif mtd[d] == 1:
+            f = f * np.sin(np.pi * a * idx[d] / n[d])
+            lam += 2 * (1 - np.cos(np.pi * a / n[d]))
+        else:
+            f = f * np.cos(np.pi * a * idx[d] / n[d])
+            lam += 2 * (1 - np.cos(np.pi * a / n[d]))
+    rho = f[..., None]
+    phi = E.poisson_general(rho, mtd)
+    rng = [E.solve_range(n[d], mtd[d]) for d in range(3)]
+    sl = tuple(slice(rng[d][0] + 1, rng[d][1] + 2) for d in (2, 1, 0))
+    assert np.allclose(phi[sl][..., 0], f[sl] / lam, rtol=0, atol=1e-12 / lam)
+
+
+def test_dirichlet_solution_satisfies_the_reference_check():
+    """phi = 0 on the faces: the solved interior satisfies poichk's stencil
+    exactly (no mean to remove), with phi on the faces and guards zero."""
+    rng = np.random.default_rng(3)
+    nz, ny, nx = 9, 8, 10
+    rho = rng.standard_normal((nz + 3, ny + 3, nx + 3, 1))
+    phi = E.poisson_general(rho, (1, 1, 1))
+    assert E.poichk_general(rho, phi, (1, 1, 1)) < 1e-14 * np.abs(rho).max()
+    p = phi[..., 0]
+    for face in (p[0], p[1], p[nz + 1], p[nz + 2], p[:, 1], p[:, :, nx + 1]):
+        assert np.all(face == 0.0)
+
+
+def test_neumann_boundary_values_enter_as_the_reference_adds_them():
+    """mtd_vbnd 2 with boundary values: the same as the solve of rho_tilde
+    (rho - 2 bc(1) on the node-0 plane, + 2 bc(2) on the node-n plane,
+    poissn.F90:76-127) without them; guards outside the solved nodes zero."""
+    rng = np.random.default_rng(4)
+    nz, ny, nx = 8, 9, 10
+    rho = rng.standard_normal((nz + 3, ny + 3, nx + 3, 1))
+    bc = [(0.0, 0.0), (0.0, 0.0), (0.3, -0.7)]
+    a = E.poisson_general(rho, (0, 0, 2), bc)
+    rt = rho.copy()
+    rt[1] -= 2 * 0.3
+    rt[nz + 1] += 2 * -0.7
+    b = E.poisson_general(rt, (0, 0, 2))
+    assert np.array_equal(a, b)
+    assert np.all(a[0] == 0.0) and np.all(a[nz + 2] == 0.0)
+
+
+@pytest.mark.parametrize("mtd", [(1, 2, 0), (2, 1, 1)])
+def test_esfld2_boundary_components(mtd):
+    """The normal E component at -1 and n: a copy of the one at 0 and n-1
+    with mtd_vbnd 1, its negative with 2 (esfild.F90:368-435)."""
+    rng = np.random.default_rng(6)
+    nz, ny, nx = 7, 8, 9
+    n = (nx, ny, nz)
+    rho = rng.standard_normal((nz + 3, ny + 3, nx + 3, 1))
+    eb0 = rng.standard_normal((nz + 3, ny + 3, nx + 3, 6))
+    phi, eb = E.esfield_general(rho, eb0, mtd, mltstp=2)
+    assert np.array_equal(eb[..., 3:], eb0[..., 3:])
+    for d in range(3):
+        if mtd[d] == 0:
+            continue
+        s = 1.0 if mtd[d] == 1 else -1.0
+        comp = np.moveaxis(eb[..., d], 2 - d, 0)   # the axis first
+        inner = tuple(slice(1, n[e] + 2) for e in (2, 1, 0) if e != d)
+        assert np.array_equal(comp[(0,) + inner], s * comp[(1,) + inner])
+        assert np.array_equal(comp[(n[d] + 1,) + inner], s * comp[(n[d],) + inner])

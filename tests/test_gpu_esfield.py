@@ -1,4 +1,4 @@
-"""emsesg_esfield (the electrostatic field step, periodic fields) against the
+"""emsesg_esfield (the electrostatic field step) against the
 oracle's restatement of poisson(3) + esfld2 (oracle/esfield.py), through the
 C ABI.
 
@@ -6,7 +6,10 @@ phi and EX..EZ agree with the oracle to 1e-12 relative (the two FFTs round
 differently; the eigenvalues are the same doubles), BX..BZ are left
 bit-identical, the guards of phi are the periodic copies, and poichk's
 residual is at rounding level for a zero-mean rho and |mean| / sqrt(N)
-otherwise -- on cubic grids, even and odd sizes, and with mltstp > 1.  Then
+otherwise -- on cubic grids, even and odd sizes, and with mltstp > 1; the
+same against the oracle's general solve for every mix of field boundaries
+(phi = 0 faces by a type-1 DST, Neumann faces with boundary values by a
+type-1 DCT, periodic axes by the halfcomplex transform).  Then
 the field goes into the FP32 push: an ES loop (fx_step, esfield, fx_step)
 runs and keeps the discrete Gauss law div E = rho - mean(rho)."""
 import numpy as np
@@ -80,3 +83,31 @@ def test_es_loop_keeps_gauss_law(gpu):
             err = np.max(np.abs(div - (r - r.mean()))) / np.abs(r).max()
             print(f"step {step}: poichk {res:.3e}, div E - rho {err:.2e}")
             assert err < 1e-12
+
+
+@pytest.mark.parametrize("mtd,n", [((1, 1, 1), (16, 16, 16)), ((0, 0, 1), (16, 12, 20)), ((2, 0, 0), (10, 12, 14)),
+                                   ((1, 2, 0), (13, 16, 9)), ((2, 2, 2), (12, 12, 12)), ((0, 1, 2), (15, 10, 17))])
+def test_esfield_faces_match_oracle(gpu, mtd, n):
+    c = case(n=n, ppc=(1, 1))
+    cfg, eb, p, tp = build(c)
+    rng = np.random.default_rng(sum(n) + 10 * sum(mtd))
+    bc = [tuple(rng.uniform(-0.5, 0.5, 2)) if mtd[d] == 2 else (0.0, 0.0) for d in range(3)]
+    with Emses(cfg) as g:
+        rho = rng.standard_normal(field_shape(cfg, "rho"))
+        eb0 = rng.standard_normal(field_shape(cfg, "eb"))
+        g.upload_field("rho", rho)
+        g.upload_field("eb", eb0)
+        res = g.esfield(2, mtd_vbnd=mtd, bc=bc)
+        phi = g.download_field("phi").reshape(field_shape(cfg, "phi"))
+        ebg = g.download_field("eb").reshape(field_shape(cfg, "eb"))
+        phi_o, eb_o = E.esfield_general(rho, eb0, mtd, bc, mltstp=2)
+        res_o = E.poichk_general(rho, phi_o, mtd)
+        e_phi = rel_l2(phi, phi_o)
+        e_e = rel_l2(ebg[..., :3], eb_o[..., :3])
+        print(f"{mtd} {n}: phi {e_phi:.2e}, E {e_e:.2e}, poichk {res:.3e} (oracle {res_o:.3e})")
+        assert e_phi < 1e-12 and e_e < 1e-12
+        assert np.max(np.abs(phi - phi_o)) < 1e-12 * np.abs(phi_o).max()
+        # zeros outside the solved nodes are exact
+        assert np.array_equal(phi == 0.0, phi_o == 0.0)
+        assert np.array_equal(ebg[..., 3:], eb0[..., 3:])
+        assert abs(res - res_o) <= 1e-9 * max(res_o, 1e-300) + 1e-15
