@@ -990,8 +990,9 @@ def run_em_line(args, world, rank, local, es=False):
     device: each step is bfield, push + J + rho, bfield, efield and the eb
     border exchange (emsesg_fx_em_step; tcs = 2 (c dt)^2 = 0.125 in internal
     units for c dt / dx = 0.5); sort every 4 steps.  With es (--workload es)
-    the electrostatic loop instead: push + J + rho, then E from rho by the
-    FFT Poisson solve (emsesg_esfield)."""
+    the electrostatic loop instead: push + rho without the current
+    (emsesg_fx_step_es, psolve2 + charge), then E from rho by the FFT
+    Poisson solve (emsesg_esfield)."""
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the reference's field solver is not built (no "
@@ -1014,7 +1015,7 @@ def run_em_line(args, world, rank, local, es=False):
 
     def step():
         if es:
-            g.fx_step(2, k[0] % SORT_EVERY == SORT_EVERY - 1)
+            g.fx_step_es(2, k[0] % SORT_EVERY == SORT_EVERY - 1)
             g.esfield(1, check=False)
         else:
             g.fx_em_step(2, k[0] % SORT_EVERY == SORT_EVERY - 1, 0.125)
@@ -1045,8 +1046,8 @@ def run_em_line(args, world, rank, local, es=False):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64 (fields f64)",
            "data": "synthetic",
            "config": {"workload": f"{case.n[0]}^3 periodic, 2 species x {case.species[0].ppc} ppc ({npart:,} "
-                                  "particles), " + ("electrostatic field solved on the device each step (push, "
-                                  "rho, FFT Poisson solve, E from phi)" if es else "EM fields advanced on the "
+                                  "particles), " + ("electrostatic loop on the device each step (push and "
+                                  "rho without the current, FFT Poisson solve, E from phi)" if es else "EM fields advanced on the "
                                   "device each step (bfield, push, bfield, efield, border exchange)") +
                                   ", sort every 4",
                       "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},

@@ -522,16 +522,15 @@ int fx_alloc(emsesg_ctx* ctx) {
     EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_lcs_move<MoveMid>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           move_smem<MoveMid>()));
   }
-  EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(4)));
-  EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(8)));
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         fx_push_smem(4)));
   EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         fx_push_smem(8)));
-  EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<4, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        fx_push_smem(4)));
-  EMSESG_CUDA(ctx, cudaFuncSetAttribute(k_fx_push<8, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        fx_push_smem(8)));
+  for (int box : {4, 8})
+    for (int curved = 0; curved < 2; curved++)
+      for (int jd = 0; jd < 2; jd++)
+        EMSESG_CUDA(ctx, cudaFuncSetAttribute(push_kernel(box, curved != 0, jd != 0),
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(box, jd != 0)));
   return EMSESG_OK;
 }
 
@@ -925,7 +924,7 @@ namespace {
 // recomputing particle states on a grid without bodies or injected
 // particles.  In slab mode the particles leaving through the z faces go to
 // the outbox.
-int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit) {
+int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit, bool jd) {
   if (!ctx) return EMSESG_ERR_ARG;
   if (!ctx->fx.loaded) return set_error(ctx, EMSESG_ERR_STATE, "FP32 form not loaded (emsesg_fx_load)");
   if (ustep < 1) return set_error(ctx, EMSESG_ERR_ARG, "ustep must be >= 1");
@@ -944,14 +943,15 @@ int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit) {
   unsigned long long* acc_rho = (unsigned long long*)f.accum;
   unsigned long long* acc_j = acc_rho + fr.size();
   // rho and J start from zero; J keeps the injection currents of the
-  // supervisors called since the last step (emsesg_fx_inflow_current)
+  // supervisors called since the last step (emsesg_fx_inflow_current).  A
+  // step without the current (jd false) leaves J's accumulator alone.
   if (deposit) {
-    EMSESG_CUDA(ctx, cudaMemsetAsync(f.accum, 0, (fr.size() + (f.inj_j_pending ? 0 : fj.size())) * sizeof(int64_t),
-                                     ctx->stream));
-    f.inj_j_pending = false;
+    const int64_t nz = fr.size() + (jd && !f.inj_j_pending ? fj.size() : 0);
+    EMSESG_CUDA(ctx, cudaMemsetAsync(f.accum, 0, nz * sizeof(int64_t), ctx->stream));
+    if (jd) f.inj_j_pending = false;
   }
   int tmax = std::max(f.tile[0], std::max(f.tile[1], f.tile[2]));
-  int smem = fx_push_smem(tmax);
+  int smem = fx_push_smem(tmax, !deposit || jd);
   FxPushArgs a{};
   a.pos = f.pos; a.vx = f.vx; a.vy = f.vy; a.vz = f.vz;
   a.rpos = f.pos; a.rvx = f.vx; a.rvy = f.vy; a.rvz = f.vz;
@@ -1002,19 +1002,14 @@ int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit) {
       EMSESG_LAUNCH(ctx, "fx_move", (k_fx_push<8, false>), grid, PUSH_BLOCK, smem, a);
     return EMSESG_OK;
   }
-  const bool curved = a.bd.ncurved > 0;
-  if (fx_box_tile(tmax) == 4) {
-    if (curved) EMSESG_LAUNCH(ctx, "fx_push", (k_fx_push<4, true, true>), grid, PUSH_BLOCK, smem, a);
-    else EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<4>, grid, PUSH_BLOCK, smem, a);
-  } else {
-    if (curved) EMSESG_LAUNCH(ctx, "fx_push", (k_fx_push<8, true, true>), grid, PUSH_BLOCK, smem, a);
-    else EMSESG_LAUNCH(ctx, "fx_push", k_fx_push<8>, grid, PUSH_BLOCK, smem, a);
-  }
+  const PushKernel kern = push_kernel(fx_box_tile(tmax), a.bd.ncurved > 0, jd);
+  EMSESG_LAUNCH(ctx, "fx_push", kern, grid, PUSH_BLOCK, smem, a);
   // injected particles of the tail zones (general path, global deposits)
   int64_t drawn = 0;
   for (int is = 0; is < c.nspec; is++) {
     if (f.ntail[is] == 0) continue;
-    EMSESG_LAUNCH(ctx, "fx_tail", k_fx_tail, nblk(f.ntail[is]), 256, 0, a, is, f.tail0[is], f.ntail[is],
+    EMSESG_LAUNCH(ctx, "fx_tail", (jd ? k_fx_tail<true> : k_fx_tail<false>), nblk(f.ntail[is]), 256, 0, a, is,
+                  f.tail0[is], f.ntail[is],
                   f.tailord + f.tailord_base[is], ustep, c.rng_mode == 1 ? ctx->d_randoms : nullptr, ctx->n_randoms,
                   ctx->d_rand_pos, drawn, c.rng_seed, ctx->rng_stream, ctx->d_counter->nesc + is);
     drawn += f.pending[is];
@@ -1056,7 +1051,7 @@ void fold_lists(const emsesg_config& c, bool slab, int part, std::vector<SlabOp>
 // place, and this J), then the re-sort after the push (so that injected
 // particles take their first, partial step before they join the tile
 // regions).
-int fx_fields_phase(emsesg_ctx* ctx) {
+int fx_fields_phase(emsesg_ctx* ctx, bool jd) {
   FxState& f = ctx->fx;
   const emsesg_config& c = ctx->cfg;
   FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
@@ -1064,15 +1059,19 @@ int fx_fields_phase(emsesg_ctx* ctx) {
   unsigned long long* acc_j = acc_rho + fr.size();
   std::vector<SlabOp> orho, oj;
   fold_lists(c, f.slab, 1, &orho, &oj);
+  if (!jd) oj.clear();
   int rc;
   if ((rc = run_slab_ops2(ctx, (long long*)acc_rho, fr, orho, (long long*)acc_j, fj, oj, "fx_fold"))) return rc;
-  EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_double, nblk(fj.size()), 256, 0, (const long long*)acc_j,
-                ctx->field[EMSESG_FIELD_AJ], fj.size());
+  if (jd)
+    EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_double, nblk(fj.size()), 256, 0, (const long long*)acc_j,
+                  ctx->field[EMSESG_FIELD_AJ], fj.size());
   unsigned long long* cres = (unsigned long long*)(f.diag + 3 * DIAG_GRID + 3);
   EMSESG_CUDA(ctx, cudaMemsetAsync(cres, 0, 2 * sizeof(double), ctx->stream));
   EMSESG_LAUNCH(ctx, "fx_to_double", k_fix_to_rho, nblk(fr.size(), RHO_BLOCK), RHO_BLOCK, 0, (const long long*)acc_rho,
-                ctx->field[EMSESG_FIELD_RHO], ctx->field[EMSESG_FIELD_AJ], fr, fj, c.nx, c.ny, c.nz, cres);
-  f.cont_valid = f.rho_prev;
+                ctx->field[EMSESG_FIELD_RHO], jd ? ctx->field[EMSESG_FIELD_AJ] : nullptr, fr, fj, c.nx, c.ny, c.nz,
+                cres);
+  // the continuity residual needs the step's current
+  f.cont_valid = jd && f.rho_prev;
   f.rho_prev = true;
   // the step's reads of eb are over: an asynchronous upload of the next eb
   // may start (inside a stream capture the event is recorded after the
@@ -1081,8 +1080,8 @@ int fx_fields_phase(emsesg_ctx* ctx) {
   return EMSESG_OK;
 }
 
-int fx_finish_phase(emsesg_ctx* ctx, int do_sort) {
-  int rc = fx_fields_phase(ctx);
+int fx_finish_phase(emsesg_ctx* ctx, int do_sort, bool jd) {
+  int rc = fx_fields_phase(ctx, jd);
   if (rc) return rc;
   ctx->rng_stream++;
   if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
@@ -1094,24 +1093,36 @@ int fx_finish_phase(emsesg_ctx* ctx, int do_sort) {
 int fx_step_impl(emsesg_ctx* ctx, int ustep, int do_sort, bool deposit) {
   if (ctx && ctx->fx.slab && deposit)
     return set_error(ctx, EMSESG_ERR_STATE, "slab mode: steps are emsesg_fx_slab_begin / _arrive / _end");
-  int rc = fx_push_phase(ctx, ustep, deposit);
+  int rc = fx_push_phase(ctx, ustep, deposit, true);
   if (rc) return rc;
   if (!deposit) {
     ctx->rng_stream++;
     if (do_sort && (rc = emsesg_fx_sort(ctx))) return rc;
     return EMSESG_OK;
   }
-  return fx_finish_phase(ctx, do_sort);
+  return fx_finish_phase(ctx, do_sort, true);
 }
 }  // namespace
+
+// The electrostatic step of the FP32 form: psolve2 + charge (push, boundary
+// rules and bodies, rho; no current), the folds of rho and its conversion,
+// then the re-sort on a sort step.  The J accumulator and the aj field are
+// left as they are.
+extern "C" int emsesg_fx_step_es(emsesg_ctx* ctx, int ustep, int do_sort) {
+  if (!ctx) return EMSESG_ERR_ARG;
+  if (ctx->fx.slab) return set_error(ctx, EMSESG_ERR_STATE, "slab mode: the electrostatic step is not built for slabs");
+  int rc = fx_push_phase(ctx, ustep, true, false);
+  if (rc) return rc;
+  return fx_finish_phase(ctx, do_sort, false);
+}
 
 extern "C" int emsesg_fx_step_download(emsesg_ctx* ctx, int ustep, int do_sort, double* rho, double* aj) {
   if (!ctx || !rho || !aj) return EMSESG_ERR_ARG;
   if (ctx->fx.slab) return set_error(ctx, EMSESG_ERR_STATE, "slab mode: steps are emsesg_fx_slab_begin / _arrive / _end");
   int rc = side_stream(ctx);
   if (rc) return rc;
-  if ((rc = fx_push_phase(ctx, ustep, true))) return rc;
-  if ((rc = fx_fields_phase(ctx))) return rc;
+  if ((rc = fx_push_phase(ctx, ustep, true, true))) return rc;
+  if ((rc = fx_fields_phase(ctx, true))) return rc;
   // rho and aj are final: copied to the host on the side stream while the
   // context's stream goes on with the sort
   const emsesg_config& c = ctx->cfg;
@@ -1582,7 +1593,7 @@ extern "C" int emsesg_fx_slab_begin(emsesg_ctx* ctx, int ustep, int64_t* counts)
   if (!f.slab) return set_error(ctx, EMSESG_ERR_STATE, "not in slab mode (emsesg_fx_slab)");
   if (f.slab_open) return set_error(ctx, EMSESG_ERR_STATE, "slab step already open");
   const emsesg_config& c = ctx->cfg;
-  int rc = fx_push_phase(ctx, ustep, true);
+  int rc = fx_push_phase(ctx, ustep, true, true);
   if (rc) return rc;
   unsigned long long n[2 * EMSESG_ISPEC];
   EMSESG_CUDA(ctx, cudaMemcpyAsync(n, f.outbox_n, sizeof(n), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1683,7 +1694,7 @@ extern "C" int emsesg_fx_slab_end(emsesg_ctx* ctx, int do_sort) {
   FxState& f = ctx->fx;
   if (!f.slab_open) return set_error(ctx, EMSESG_ERR_STATE, "no slab step open (emsesg_fx_slab_begin)");
   f.slab_open = false;
-  return fx_finish_phase(ctx, do_sort);
+  return fx_finish_phase(ctx, do_sort, true);
 }
 
 extern "C" int emsesg_fx_inject(emsesg_ctx* ctx, int spec, const emsesg_particle* host, int64_t n) {

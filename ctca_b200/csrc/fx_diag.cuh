@@ -92,10 +92,12 @@ __global__ void __launch_bounds__(RHO_BLOCK) k_fix_to_rho(const long long* __res
     const int64_t ex = fr.ex, ey = fr.ey;
     const int i = (int)(e % ex) + fr.lo, j = (int)((e / ex) % ey) + fr.lo, k = (int)(e / (ex * ey)) + fr.lo;
     if (i >= 0 && j >= 0 && k >= 0 && i <= nx && j <= ny && k <= nz) {
-      const double div = (aj[fj.at(0, i, j, k)] - aj[fj.at(0, i - 1, j, k)]) +
-                         (aj[fj.at(1, i, j, k)] - aj[fj.at(1, i, j - 1, k)]) +
-                         (aj[fj.at(2, i, j, k)] - aj[fj.at(2, i, j, k - 1)]);
-      r = fabs(v - (rho[e] - div * 2.0));
+      if (aj) {  // without the step's current (the electrostatic step) no residual
+        const double div = (aj[fj.at(0, i, j, k)] - aj[fj.at(0, i - 1, j, k)]) +
+                           (aj[fj.at(1, i, j, k)] - aj[fj.at(1, i, j - 1, k)]) +
+                           (aj[fj.at(2, i, j, k)] - aj[fj.at(2, i, j, k - 1)]);
+        r = fabs(v - (rho[e] - div * 2.0));
+      }
       m = fabs(v);
     }
     rho[e] = v;

@@ -45,7 +45,7 @@ constexpr int PG = 1;           // guard cells around the tile
 constexpr int NSTAGE = 3;       // row ring stages (up to NSTAGE - 1 rows in flight)
 constexpr int NJ = 12;          // zigzag node values of one cell
 constexpr int NR = 8;           // CIC node values of one cell
-constexpr int RQW = NJ + NR + 1;  // run-queue entry: 20 sums + box index of the cell
+constexpr int RQW = NJ + NR + 1;  // run-queue entry: 20 sums + box index of the cell (charge only: 8 + 1)
 constexpr int RQ_DRAIN = 8;     // drain the run queue at this many entries
 constexpr int RQCAP = RQ_DRAIN + 32;
 constexpr int XQW = 8;          // general-path entry: slot, cell, 3 offsets, 3 velocities
@@ -476,21 +476,24 @@ __device__ __forceinline__ void kick(const FxPushArgs& a, const float4* sf0, con
 // 32 lanes busy however few entries are queued; the items of one entry go
 // to 20 different nodes.  An entry holds its 20 sums and the box index of
 // its cell (only cells inside the box are queued).
+template <int NC>
 __device__ __forceinline__ void drain_runs(unsigned long long* box, const int* slot_off, const float* q, int qn,
                                            float qfix, int lane) {
+  static_assert(NC > 0 && NC <= 32, "an entry's sums fit one pass");
+  constexpr int QW = NC + 1;
   __syncwarp();
-  const int items = qn * (NJ + NR);
-  int e = lane / (NJ + NR), sl = lane % (NJ + NR);
+  const int items = qn * NC;
+  int e = lane / NC, sl = lane % NC;
   for (int m = lane; m < items; m += 32) {
-    const float* en = q + e * RQW;
-    const int base = __float_as_int(en[NJ + NR]);
+    const float* en = q + e * QW;
+    const int base = __float_as_int(en[NC]);
     const long long f = to_fix(en[sl], qfix);
     if (f) box_add(&box[base + slot_off[sl]], (unsigned long long)f);
-    // m += 32: 32 = 1 * 20 + 12
-    sl += 32 - (NJ + NR);
-    e += 1;
-    if (sl >= NJ + NR) {
-      sl -= NJ + NR;
+    // m += 32: 32 = (32 / NC) * NC + 32 % NC
+    sl += 32 % NC;
+    e += 32 / NC;
+    if (sl >= NC) {
+      sl -= NC;
       e += 1;
     }
   }
@@ -582,8 +585,8 @@ __device__ __forceinline__ int body_absorb(const CrossCtx& c, const int (&ib)[3]
 // General path for one particle that left its cell (or whose cell lies
 // outside the box): boundary rules, zigzag with relay point, charge at the
 // stored cell; the final record is written here.  CURV = false: the run has
-// box bodies only.
-template <int B, bool DEP = true, bool CURV = true>
+// box bodies only.  JD = false: charge only (no zigzag current).
+template <int B, bool DEP = true, bool CURV = true, bool JD = true>
 __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, const int (&o)[3], const Sink& sk,
                                          const CrossCtx& c, const float* en) {
   const int loc = __float_as_int(en[0]);
@@ -635,6 +638,7 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
   c.gvy[loc] = vy;
   c.gvz[loc] = vz;
   if (!DEP) return escaped ? 1 : 0;
+  if (JD) {
   // zigzag (psolve1.F90:717-757), integer parts first
   float J[NJ];
   {
@@ -672,6 +676,7 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
     }
     put_j<B>(box, o, sk, ax.ia, ay.ia, az.ia, J2, c.qfix);
   }
+  }  // JD
   if (!dead) {
     // charge.F90:152-210 at the stored (wrapped / reflected) position
     float X = ax.nf, Y = ay.nf, Z = az.nf;
@@ -688,7 +693,7 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
 // holding their position before this step and the velocity the row loop
 // gave them): each lane takes one and runs the general path.  Returns the
 // number of this lane's particles that escaped.
-template <int B, bool DEP, bool CURV>
+template <int B, bool DEP, bool CURV, bool JD>
 __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t slot0, unsigned long long* box,
                                           const int (&o)[3], const int* xl, int xn, int lane) {
   __syncwarp();
@@ -705,7 +710,7 @@ __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t s
     const float4 ps = a.rpos[slot0 + loc];  // the position before the step
     const float vx = c.gvx[loc], vy = c.gvy[loc], vz = c.gvz[loc];
     const float en[XQW] = {__int_as_float(loc), ps.w, ps.x, ps.y, ps.z, vx, vy, vz};
-    dead += cross_one<B, DEP, CURV>(g, box, o, sk, c, en);
+    dead += cross_one<B, DEP, CURV, JD>(g, box, o, sk, c, en);
   }
   __syncwarp();
   return dead;
@@ -715,16 +720,25 @@ __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t s
 // current, no charge), for recomputing particle states.  CURV = true: the
 // run has cylinders or spheres (tile regions next to one push every
 // particle on the general path); without them the in-cell test keeps its
-// constant bound.
-template <int T, bool DEP = true, bool CURV = false>
+// constant bound.  JD = false (the electrostatic step, psolve2 + charge):
+// the charge only -- runs of 8 CIC sums, an accumulator of rho alone, no
+// zigzag current.
+template <int T, bool DEP = true, bool CURV = false, bool JD = true>
 __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   constexpr int B = T + 2 * PG + 1;  // box and field tile edge (nodes)
-  constexpr int NBOX = 4 * B * B * B;
+  constexpr int NC = JD ? NJ + NR : NR;  // sums of a run: zigzag J and CIC rho, or rho alone
+  constexpr int RO = JD ? NJ : 0;        // first rho sum
+  constexpr int QW = NC + 1;             // run-queue entry: the sums and the cell's box index
+  constexpr int NACC = (JD ? 4 : 1) * B * B * B;  // accumulator entries (rho, then Jx, Jy, Jz)
+  constexpr int NBOX = (NACC + 1) & ~1;           // their 8-byte words, padded so that the ring after them
+                                                  // starts on a 16-byte boundary (bulk copies, float4)
   constexpr int NF = B * B * B;
+  static_assert((NBOX * 8) % 16 == 0 && (NBOX * 8 + NSTAGE * ROW_BYTES) % 16 == 0,
+                "the row ring and the field tile start on 16-byte boundaries");
   extern __shared__ __align__(128) unsigned long long smem[];
   __shared__ __align__(8) uint64_t full_bar[NSTAGE];
   __shared__ __align__(8) uint64_t empty_bar[NSTAGE];
-  __shared__ int slot_off[NJ + NR];
+  __shared__ int slot_off[NC];
   __shared__ int rows_seen;
   const Geo& g = a.g;
   const int is = blockIdx.y;
@@ -762,8 +776,8 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   float* stvz = stvy + NSTAGE * PUSH_THREADS;
   float4* sf0 = reinterpret_cast<float4*>(stvz + NSTAGE * PUSH_THREADS);
   float2* sf1 = reinterpret_cast<float2*>(sf0 + NF);
-  float* rq = reinterpret_cast<float*>(sf1 + NF) + warp * RQCAP * RQW;
-  int* xl = reinterpret_cast<int*>(reinterpret_cast<float*>(sf1 + NF) + PUSH_WARPS * RQCAP * RQW) + warp * XLCAP;
+  float* rq = reinterpret_cast<float*>(sf1 + NF) + warp * RQCAP * QW;
+  int* xl = reinterpret_cast<int*>(reinterpret_cast<float*>(sf1 + NF) + PUSH_WARPS * RQCAP * QW) + warp * XLCAP;
 
   float4* gpos = a.pos + slot0;
   float* gvx = a.vx + slot0;
@@ -781,7 +795,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     }
     mbar_fence_init();
   }
-  if (tid < NJ + NR) slot_off[tid] = tid < NJ ? BoxT<B>::joff(tid) : BoxT<B>::roff(tid - NJ);
+  if (tid < NC) slot_off[tid] = tid < RO ? BoxT<B>::joff(tid) : BoxT<B>::roff(tid - RO);
   if (DEP)
     for (int e = tid; e < NBOX; e += PUSH_BLOCK) box[e] = 0ull;
   const int64_t sy = g.nx + 1, sz = (int64_t)(g.nx + 1) * (g.ny + 1);
@@ -838,9 +852,9 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       if (hit) flo = 2.0f;
     }
 
-  float acc[NJ + NR];
+  float acc[NC];
 #pragma unroll
-  for (int s = 0; s < NJ + NR; s++) acc[s] = 0.f;
+  for (int s = 0; s < NC; s++) acc[s] = 0.f;
   uint32_t runcell = DEAD;
   int runbase = -1;
   int nesc = 0;
@@ -905,14 +919,14 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       const unsigned mk = __ballot_sync(0xffffffffu, evict);
       if (mk) {
         if (evict) {
-          float* en = rq + (rqn + __popc(mk & lt)) * RQW;
+          float* en = rq + (rqn + __popc(mk & lt)) * QW;
 #pragma unroll
-          for (int q = 0; q < NJ + NR; q++) en[q] = acc[q];
-          en[NJ + NR] = __int_as_float(runbase);
+          for (int q = 0; q < NC; q++) en[q] = acc[q];
+          en[NC] = __int_as_float(runbase);
         }
         rqn += __popc(mk);
         if (rqn >= RQ_DRAIN) {
-          drain_runs(box, slot_off, rq, rqn, qfix, lane);
+          drain_runs<NC>(box, slot_off, rq, rqn, qfix, lane);
           rqn = 0;
         }
       }
@@ -944,40 +958,43 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
       oop = DEP && incell && !simple && gb >= 0;
     }
     const unsigned om = DEP ? __ballot_sync(0xffffffffu, oop) : 0u;
-    float* oen = oop ? rq + (rqn + __popc(om & lt)) * RQW : nullptr;
+    float* oen = oop ? rq + (rqn + __popc(om & lt)) * QW : nullptr;
     if (DEP && (simple || oop)) {
       // both zigzag segments in the same cell: relay point at the midpoint,
       // equal segment fluxes h = (a-b)/2/ustep, mid-points m -+ (a-b)/4; the
       // sum of the two bilinear weight sets is written with S = a+b, D = a-b
-      const float Sx = sx + ps.x, Sy = syy + ps.y, Sz = szz + ps.z;
-      const float Dx = sx - ps.x, Dy = syy - ps.y, Dz = szz - ps.z;
-      const float hx = Dx * hr, hy = Dy * hr, hz = Dz * hr;
-      float cv[NJ + NR];
-      float P;
-      P = 0.5f * Sy * Sz + 0.125f * Dy * Dz;
-      cv[3] = hx * P; cv[1] = hx * (Sy - P); cv[2] = hx * (Sz - P); cv[0] = hx * (2.0f - Sy - Sz + P);
-      P = 0.5f * Sx * Sz + 0.125f * Dx * Dz;
-      cv[7] = hy * P; cv[5] = hy * (Sx - P); cv[6] = hy * (Sz - P); cv[4] = hy * (2.0f - Sx - Sz + P);
-      P = 0.5f * Sx * Sy + 0.125f * Dx * Dy;
-      cv[11] = hz * P; cv[9] = hz * (Sx - P); cv[10] = hz * (Sy - P); cv[8] = hz * (2.0f - Sx - Sy + P);
+      float cv[NC];
+      if (JD) {
+        const float Sx = sx + ps.x, Sy = syy + ps.y, Sz = szz + ps.z;
+        const float Dx = sx - ps.x, Dy = syy - ps.y, Dz = szz - ps.z;
+        const float hx = Dx * hr, hy = Dy * hr, hz = Dz * hr;
+        float P;
+        P = 0.5f * Sy * Sz + 0.125f * Dy * Dz;
+        cv[3] = hx * P; cv[1] = hx * (Sy - P); cv[2] = hx * (Sz - P); cv[0] = hx * (2.0f - Sy - Sz + P);
+        P = 0.5f * Sx * Sz + 0.125f * Dx * Dz;
+        cv[7] = hy * P; cv[5] = hy * (Sx - P); cv[6] = hy * (Sz - P); cv[4] = hy * (2.0f - Sx - Sz + P);
+        P = 0.5f * Sx * Sy + 0.125f * Dx * Dy;
+        cv[11 % NC] = hz * P; cv[9 % NC] = hz * (Sx - P); cv[10 % NC] = hz * (Sy - P);
+        cv[8 % NC] = hz * (2.0f - Sx - Sy + P);
+      }
       // CIC charge at the new position (charge.F90:152-210)
       const float XY = sx * syy, XZ = sx * szz, YZ = syy * szz, Z2 = 1.0f - szz, XZ2 = sx * Z2, YZ2 = syy * Z2;
       const float r2 = XY * szz, r6 = XY * Z2;
       const float r3 = YZ - r2, r7 = YZ2 - r6;
-      cv[NJ + 2] = r2; cv[NJ + 1] = XZ - r2; cv[NJ + 3] = r3; cv[NJ + 0] = szz - XZ - r3;
-      cv[NJ + 6] = r6; cv[NJ + 5] = XZ2 - r6; cv[NJ + 7] = r7; cv[NJ + 4] = Z2 - XZ2 - r7;
+      cv[RO + 2] = r2; cv[RO + 1] = XZ - r2; cv[RO + 3] = r3; cv[RO + 0] = szz - XZ - r3;
+      cv[RO + 6] = r6; cv[RO + 5] = XZ2 - r6; cv[RO + 7] = r7; cv[RO + 4] = Z2 - XZ2 - r7;
       if (oop) {
 #pragma unroll
-        for (int q = 0; q < NJ + NR; q++) oen[q] = cv[q];
-        oen[NJ + NR] = __int_as_float(gb);
+        for (int q = 0; q < NC; q++) oen[q] = cv[q];
+        oen[NC] = __int_as_float(gb);
       } else {
 #pragma unroll
-        for (int q = 0; q < NJ + NR; q++) acc[q] = fmaf(acc[q], keep, cv[q]);
+        for (int q = 0; q < NC; q++) acc[q] = fmaf(acc[q], keep, cv[q]);
       }
     }
     if (newrun && !simple) {
 #pragma unroll
-      for (int q = 0; q < NJ + NR; q++) acc[q] = 0.f;
+      for (int q = 0; q < NC; q++) acc[q] = 0.f;
     }
     // the new velocity of every particle (a cell-crossing one keeps its old
     // position until the general path writes the whole record)
@@ -999,7 +1016,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     if (om) {
       rqn += __popc(om);
       if (rqn >= RQ_DRAIN) {
-        drain_runs(box, slot_off, rq, rqn, qfix, lane);
+        drain_runs<NC>(box, slot_off, rq, rqn, qfix, lane);
         rqn = 0;
       }
     }
@@ -1019,7 +1036,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     ph = par1;
   }
   if (xqn) {
-    nesc += cross_list<B, DEP, CURV>(a, is, slot0, box, o, xl, xqn, lane);
+    nesc += cross_list<B, DEP, CURV, JD>(a, is, slot0, box, o, xl, xqn, lane);
     xqn = 0;
   }
   if (r >= L || failed) break;
@@ -1030,13 +1047,13 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     const bool has = runbase >= 0;
     const unsigned mk = __ballot_sync(0xffffffffu, has);
     if (has) {
-      float* en = rq + (rqn + __popc(mk & lt)) * RQW;
+      float* en = rq + (rqn + __popc(mk & lt)) * QW;
 #pragma unroll
-      for (int q = 0; q < NJ + NR; q++) en[q] = acc[q];
-      en[NJ + NR] = __int_as_float(runbase);
+      for (int q = 0; q < NC; q++) en[q] = acc[q];
+      en[NC] = __int_as_float(runbase);
     }
     rqn += __popc(mk);
-    if (rqn) drain_runs(box, slot_off, rq, rqn, qfix, lane);
+    if (rqn) drain_runs<NC>(box, slot_off, rq, rqn, qfix, lane);
   }
   if (nesc) atomicAdd(&a.nesc[is], nesc);
   if (tid == 0) rows_seen = seen;
@@ -1047,7 +1064,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     for (int r = rows_seen; r < issued; r++) (void)mbar_wait(&full_bar[r % NSTAGE], (uint32_t)((r / NSTAGE) & 1));
   // add the tile accumulator into the global int64 arrays
   if (DEP) {
-    for (int e = tid; e < NBOX; e += PUSH_BLOCK) {
+    for (int e = tid; e < NACC; e += PUSH_BLOCK) {
       unsigned long long v = box[e];
       if (v == 0ull) continue;
       int li = e % B, lj = (e / B) % B, lk = (e / (B * B)) % B, comp = e / (B * B * B);
@@ -1105,6 +1122,7 @@ __global__ void __launch_bounds__(1024) k_push_chunks(const int64_t* __restrict_
 // random fraction of the step for a particle injected since the last push
 // (psolve1.F90:150-156: gustep = ustep * U), gather from the global node
 // field, Buneman-Boris, and the general path with global deposits.
+template <bool JD>
 __global__ void k_fx_tail(FxPushArgs a, int is, int64_t tail0, int64_t ntail, int32_t* ord, int ustep,
                           const double* randoms, int64_t nrand, const int64_t* rand_pos, int64_t ord_base,
                           uint64_t seed, uint64_t stream, int* nesc_out) {
@@ -1169,17 +1187,34 @@ __global__ void k_fx_tail(FxPushArgs a, int is, int64_t tail0, int64_t ntail, in
                    a.surf + (int64_t)is * a.bd.nsurf, is, base, a.ob.rec ? &a.ob : nullptr, a.status};
   const float en[XQW] = {__int_as_float((int)slot), ps.w, ps.x, ps.y, ps.z, vx, vy, vz};
   const int far[3] = {-(1 << 28), -(1 << 28), -(1 << 28)};  // no box: global deposits
-  const int esc = cross_one<11>(g, nullptr, far, sk, c, en);
+  const int esc = cross_one<11, true, true, JD>(g, nullptr, far, sk, c, en);
   if (esc) atomicAdd(nesc_out, esc);
 }
 
 // The compiled box edge for the largest tile edge tmax (<= 8).
 inline int fx_box_tile(int tmax) { return tmax <= 4 ? 4 : 8; }
 
-inline int fx_push_smem(int tmax) {
+// Dynamic shared memory of the push: int64 accumulator (4 components, or
+// rho alone without the current), row ring, field tile, run queues and cross
+// lists.
+inline int fx_push_smem(int tmax, bool jd = true) {
   int B = fx_box_tile(tmax) + 2 * PG + 1;
   int nf = B * B * B;
-  return 4 * nf * (int)sizeof(unsigned long long) + NSTAGE * (int)ROW_BYTES +
+  const int qw = (jd ? NJ + NR : NR) + 1;
+  const int nbox = ((jd ? 4 : 1) * nf + 1) & ~1;  // as NBOX in k_fx_push
+  return nbox * (int)sizeof(unsigned long long) + NSTAGE * (int)ROW_BYTES +
          nf * (int)(sizeof(float4) + sizeof(float2)) +
-         PUSH_WARPS * (RQCAP * RQW * (int)sizeof(float) + XLCAP * (int)sizeof(int));
+         PUSH_WARPS * (RQCAP * qw * (int)sizeof(float) + XLCAP * (int)sizeof(int));
+}
+
+// The pushing kernel (DEP = true) for a compiled box tile (4 or 8), runs
+// with cylinders or spheres, and with (jd) or without the current.
+using PushKernel = void (*)(FxPushArgs);
+inline PushKernel push_kernel(int box, bool curved, bool jd) {
+  if (box == 4) {
+    if (curved) return jd ? k_fx_push<4, true, true, true> : k_fx_push<4, true, true, false>;
+    return jd ? k_fx_push<4, true, false, true> : k_fx_push<4, true, false, false>;
+  }
+  if (curved) return jd ? k_fx_push<8, true, true, true> : k_fx_push<8, true, true, false>;
+  return jd ? k_fx_push<8, true, false, true> : k_fx_push<8, true, false, false>;
 }

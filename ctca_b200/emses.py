@@ -127,6 +127,7 @@ _SIGS = {
     "emsesg_exchange_eb": (_I, [_P]),
     "emsesg_fx_em_step": (_I, [_P, _I, _I, ctypes.c_double]),
     "emsesg_esfield": (_I, [_P, _P, _P, _I, _P]),
+    "emsesg_fx_step_es": (_I, [_P, _I, _I]),
     "emsesg_energy": (_I, [_P, ctypes.POINTER(ctypes.c_double)]),
     "emsesg_fx_load": (_I, [_P]),
     "emsesg_fx_store": (_I, [_P]),
@@ -376,6 +377,10 @@ class Emses:
 
     def exchange_eb(self):
         self._check(self.lib.emsesg_exchange_eb(self.h))
+
+    def fx_step_es(self, ustep: int, do_sort: bool):
+        """The electrostatic step (psolve2 + charge): push and rho, no J."""
+        self._check(self.lib.emsesg_fx_step_es(self.h, ustep, 1 if do_sort else 0))
 
     def fx_em_step(self, ustep: int, do_sort: bool, tcs: float):
         """bfield, fx_step, bfield, efield, exchange_eb (the main loop's order)."""

@@ -308,6 +308,16 @@ int emsesg_fx_sort(emsesg_ctx* ctx);
  * its capture, and emsesg_batch_launch refuses (EMSESG_ERR_STATE) a run whose
  * eb was uploaded asynchronously since. */
 int emsesg_fx_step_download(emsesg_ctx* ctx, int ustep, int do_sort, double* rho, double* aj);
+/* emsesg_fx_step_es: the electrostatic step of the FP32 form, the
+ * reference's psolve2 + charge (src/pcl2field/psolve2.F90:4-548,
+ * src/pcl2field/charge.F90:4-212, as its ES main loop calls them,
+ * src/main/esses.F90:341-367,530-560): the push with the outer boundary
+ * rules, bodies and injected particles of emsesg_fx_step, rho deposited
+ * and folded, no current (J's accumulator and the aj field are left as
+ * they are, and the step has no continuity residual); then the re-sort when
+ * do_sort.  rho is the one emsesg_fx_step deposits for the same particles.
+ * Not in slab mode.  Asynchronous. */
+int emsesg_fx_step_es(emsesg_ctx* ctx, int ustep, int do_sort);
 int emsesg_upload_field_async(emsesg_ctx* ctx, int field, const double* host);
 /* nsteps steps of the FP32 form, re-sorting every sort_every steps
  * (emsesg_fx_step with do_sort on every sort_every-th step).  With use_graph,

@@ -357,3 +357,58 @@ def test_async_eb_upload_with_graph_runs(gpu):
         with pytest.raises(EmsesError, match="asynchronously"):
             batch.launch(1)
         batch.close()
+
+
+@pytest.mark.parametrize("npbnd,nfbnd,bodies", [((0, 0, 0), (0, 0, 0), False), ((0, 0, 2), (0, 0, 1), True)])
+def test_es_step_is_the_step_without_current(gpu, npbnd, nfbnd, bodies):
+    """emsesg_fx_step_es (psolve2 + charge on the FP32 form): the same
+    particles, counts and rho, bit for bit, as emsesg_fx_step from the same
+    state, over steps with re-sorts, escapes and (with bodies) absorption by
+    a box, a cylinder and a sphere; aj is left as it was.  Against the
+    oracle's psolve2 + charge from the same state: rho within 1e-5."""
+    c = case(n=(16, 16, 24), ppc=(8, 8), npbnd=npbnd, nfbnd=nfbnd, vth_scale=3.0, tile=(8, 8, 8))
+    if bodies:
+        c.bodies = [dict(geotype=0, ncond=1, xlpc=3.0, xupc=7.0, ylpc=3.0, yupc=7.0, zlpc=4.0, zupc=9.0,
+                         sqdscaled=1.0),
+                    dict(geotype=2, ncond=1, cyl_align=3, cyl_axis=(11.5, 11.25), cyl_edge=(2.0, 20.0), radius=2.2,
+                         sqdscaled=1.0),
+                    dict(geotype=3, ncond=0, sph_center=(5.3, 11.7, 16.1), radius=2.4)]
+    cfg, eb, p, tp = build(c, 1.2)
+    with Emses(cfg) as a, Emses(cfg) as b:
+        for g in (a, b):
+            g.upload_particles(p, tp)
+            g.upload_field("eb", eb)
+            g.fx_load()
+        aj0 = b.download_field("aj")
+        for k in range(5):
+            srt = k % 2 == 1
+            if k == 2:
+                # the oracle from the ES step's state: psolve2 + charge
+                b.fx_store()
+                pb, tpb = b.download_particles()
+                b.fx_load()
+                a.fx_store()
+                a.fx_load()
+                o = O.Oracle(cfg, pb, tpb, eb)
+                o.grdcrt()
+                o.psolve2(2)
+                o.charge(0)
+                o.reduce_rho("rho")
+            a.fx_step(2, srt)
+            b.fx_step_es(2, srt)
+            assert np.array_equal(a.download_field("rho"), b.download_field("rho")), k
+            assert np.array_equal(a.fx_counts(), b.fx_counts()), k
+            if k == 2:
+                err = rel_l2(b.download_field("rho"), o.f["rho"])
+                print(f"rho against psolve2 + charge: {err:.2e}")
+                assert err < RHOJ_TOL
+        assert np.array_equal(b.download_field("aj"), aj0)
+        ca, cb = a.get_counters().as_dict(), b.get_counters().as_dict()
+        assert np.array_equal(ca["influx"], cb["influx"]) and np.array_equal(ca["nesc"], cb["nesc"])
+        if bodies:
+            assert int(cb["influx"][:2].sum()) > 0
+        a.fx_store()
+        b.fx_store()
+        pa, _ = a.download_particles()
+        pb, _ = b.download_particles()
+        assert np.array_equal(pa.view(np.uint8), pb.view(np.uint8))
