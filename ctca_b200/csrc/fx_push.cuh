@@ -43,6 +43,9 @@ constexpr int PUSH_WARPS = PUSH_THREADS / 32;
 constexpr int PUSH_BLOCK = PUSH_THREADS + 32;  // + one warp that streams the rows
 constexpr int PG = 1;           // guard cells around the tile
 constexpr int NSTAGE = 3;       // row ring stages (up to NSTAGE - 1 rows in flight)
+// Stages of the push's ring: the charge-only push (no current) has the
+// shared memory for one more.
+__host__ __device__ constexpr int push_stages(bool jd) { return jd ? NSTAGE : NSTAGE + 1; }
 constexpr int NJ = 12;          // zigzag node values of one cell
 constexpr int NR = 8;           // CIC node values of one cell
 constexpr int RQW = NJ + NR + 1;  // run-queue entry: 20 sums + box index of the cell (charge only: 8 + 1)
@@ -733,11 +736,12 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   constexpr int NBOX = (NACC + 1) & ~1;           // their 8-byte words, padded so that the ring after them
                                                   // starts on a 16-byte boundary (bulk copies, float4)
   constexpr int NF = B * B * B;
-  static_assert((NBOX * 8) % 16 == 0 && (NBOX * 8 + NSTAGE * ROW_BYTES) % 16 == 0,
+  constexpr int NS = push_stages(JD);  // row ring stages
+  static_assert((NBOX * 8) % 16 == 0 && (NBOX * 8 + NS * ROW_BYTES) % 16 == 0,
                 "the row ring and the field tile start on 16-byte boundaries");
   extern __shared__ __align__(128) unsigned long long smem[];
-  __shared__ __align__(8) uint64_t full_bar[NSTAGE];
-  __shared__ __align__(8) uint64_t empty_bar[NSTAGE];
+  __shared__ __align__(8) uint64_t full_bar[NS];
+  __shared__ __align__(8) uint64_t empty_bar[NS];
   __shared__ int slot_off[NC];
   __shared__ int rows_seen;
   const Geo& g = a.g;
@@ -771,10 +775,10 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   const int o[3] = {tx * g.t[0] - PG, ty * g.t[1] - PG, tz * g.t[2] - PG};
   unsigned long long* box = smem;
   float4* stpos = reinterpret_cast<float4*>(smem + NBOX);
-  float* stvx = reinterpret_cast<float*>(stpos + NSTAGE * PUSH_THREADS);
-  float* stvy = stvx + NSTAGE * PUSH_THREADS;
-  float* stvz = stvy + NSTAGE * PUSH_THREADS;
-  float4* sf0 = reinterpret_cast<float4*>(stvz + NSTAGE * PUSH_THREADS);
+  float* stvx = reinterpret_cast<float*>(stpos + NS * PUSH_THREADS);
+  float* stvy = stvx + NS * PUSH_THREADS;
+  float* stvz = stvy + NS * PUSH_THREADS;
+  float4* sf0 = reinterpret_cast<float4*>(stvz + NS * PUSH_THREADS);
   float2* sf1 = reinterpret_cast<float2*>(sf0 + NF);
   float* rq = reinterpret_cast<float*>(sf1 + NF) + warp * RQCAP * QW;
   int* xl = reinterpret_cast<int*>(reinterpret_cast<float*>(sf1 + NF) + PUSH_WARPS * RQCAP * QW) + warp * XLCAP;
@@ -789,7 +793,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   const float* rgvz = a.rvz + slot0;
 
   if (tid == 0) {
-    for (int s = 0; s < NSTAGE; s++) {
+    for (int s = 0; s < NS; s++) {
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], PUSH_WARPS);
     }
@@ -816,12 +820,12 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
 
   int issued = 0;  // rows issued (producer lane 0)
   if (warp == PUSH_WARPS) {
-    // Row producer: row r goes to stage r % NSTAGE once every pushing warp
+    // Row producer: row r goes to stage r % NS once every pushing warp
     // released the row that used that stage before.
     if (lane == 0) {
       for (int r = 0; r < L; r++) {
-        const int s = r % NSTAGE;
-        if (r >= NSTAGE && !mbar_wait(&empty_bar[s], (uint32_t)((r / NSTAGE - 1) & 1))) {
+        const int s = r % NS;
+        if (r >= NS && !mbar_wait(&empty_bar[s], (uint32_t)((r / NS - 1) & 1))) {
           report_bad(a.status, a.diag, SITE_FX_PUSH, -4, t);
           break;
         }
@@ -876,10 +880,10 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   int r = 0;
   for (;;) {
   // the stage of row r and the parity of its use, kept as running counters
-  int s = r % NSTAGE;
-  uint32_t ph = (uint32_t)((r / NSTAGE) & 1);
+  int s = r % NS;
+  uint32_t ph = (uint32_t)((r / NS) & 1);
   for (; r < L && !failed; r++) {
-    const int s1 = s + 1 == NSTAGE ? 0 : s + 1;
+    const int s1 = s + 1 == NS ? 0 : s + 1;
     const uint32_t par1 = s1 == 0 ? ph ^ 1u : ph;
     uint32_t nextcell = DEAD;
     bool oknext = false;
@@ -1061,7 +1065,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   __syncthreads();
   // copies still in flight after a failed wait complete before the CTA exits
   if (warp == PUSH_WARPS && lane == 0)
-    for (int r = rows_seen; r < issued; r++) (void)mbar_wait(&full_bar[r % NSTAGE], (uint32_t)((r / NSTAGE) & 1));
+    for (int r = rows_seen; r < issued; r++) (void)mbar_wait(&full_bar[r % NS], (uint32_t)((r / NS) & 1));
   // add the tile accumulator into the global int64 arrays
   if (DEP) {
     for (int e = tid; e < NACC; e += PUSH_BLOCK) {
@@ -1202,7 +1206,7 @@ inline int fx_push_smem(int tmax, bool jd = true) {
   int nf = B * B * B;
   const int qw = (jd ? NJ + NR : NR) + 1;
   const int nbox = ((jd ? 4 : 1) * nf + 1) & ~1;  // as NBOX in k_fx_push
-  return nbox * (int)sizeof(unsigned long long) + NSTAGE * (int)ROW_BYTES +
+  return nbox * (int)sizeof(unsigned long long) + push_stages(jd) * (int)ROW_BYTES +
          nf * (int)(sizeof(float4) + sizeof(float2)) +
          PUSH_WARPS * (RQCAP * qw * (int)sizeof(float) + XLCAP * (int)sizeof(int));
 }
