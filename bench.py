@@ -1004,7 +1004,7 @@ def run_em_line(args, world, rank, local, es=False):
     from ctca_b200.emses import Emses, select_device
     torch.cuda.set_device(local)
     select_device(local)
-    case = inputs.workload_case(2)
+    case = headline_case(args.cells, args.ppc)
     cfg = inputs.make_config(case)
     g = Emses(cfg)
     g.upload_field("eb", inputs.make_fields(case))
