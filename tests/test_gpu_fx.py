@@ -363,9 +363,11 @@ def test_async_eb_upload_with_graph_runs(gpu):
 def test_es_step_is_the_step_without_current(gpu, npbnd, nfbnd, bodies):
     """emsesg_fx_step_es (psolve2 + charge on the FP32 form): the same
     particles, counts and rho, bit for bit, as emsesg_fx_step from the same
-    state, over steps with re-sorts, escapes and (with bodies) absorption by
-    a box, a cylinder and a sphere; aj is left as it was.  Against the
-    oracle's psolve2 + charge from the same state: rho within 1e-5."""
+    state, over steps with re-sorts, escapes, injected particles (inflow
+    through the open z face, their first push on the tail path) and (with
+    bodies) absorption by a box, a cylinder and a sphere; aj is left as it
+    was.  Against the oracle's psolve2 + charge from the same state: rho
+    within 1e-5."""
     c = case(n=(16, 16, 24), ppc=(8, 8), npbnd=npbnd, nfbnd=nfbnd, vth_scale=3.0, tile=(8, 8, 8))
     if bodies:
         c.bodies = [dict(geotype=0, ncond=1, xlpc=3.0, xupc=7.0, ylpc=3.0, yupc=7.0, zlpc=4.0, zupc=9.0,
@@ -380,8 +382,24 @@ def test_es_step_is_the_step_without_current(gpu, npbnd, nfbnd, bodies):
             g.upload_field("eb", eb)
             g.fx_load()
         aj0 = b.download_field("aj")
+        if npbnd[2] == 2:
+            # inflow through the back z face before every step (the tail
+            # zone's first push, with the random fractions of the step)
+            from ctca_b200 import inject
+            rng = np.random.default_rng(12)
+            vz = np.sort(rng.uniform(-0.2, -0.01, 256))
+            vxy = rng.normal(0.0, 0.05, 256)
+            uni = rng.random(100000)
+            for g in (a, b):
+                g.set_randoms(uni)
         for k in range(5):
             srt = k % 2 == 1
+            if npbnd[2] == 2 and k != 2:  # (step 2 is the one compared with the oracle)
+                for s in (1, 2):
+                    rec = inject.inflow_z(False, 50, cfg.nx, cfg.ny, cfg.nz, vz, vxy, vxy, 1.0,
+                                          np.random.default_rng(100 * k + s), spec=s)
+                    a.fx_inject(s, rec)
+                    b.fx_inject(s, rec)
             if k == 2:
                 # the oracle from the ES step's state: psolve2 + charge
                 b.fx_store()
