@@ -87,6 +87,7 @@ struct FxState {
   int64_t base[EMSESG_ISPEC] = {};  // species region offsets in pos / vx / vy / vz
   int64_t cap[EMSESG_ISPEC] = {};   // species region sizes (capacity + tile padding)
   bool tiled = false;               // regions hold the thread-major layout of a sort
+  bool box_inside = false;          // loaded particles start inside a box body (until the next push)
   // tile-local counting sort (fx_sort.cuh): per species
   int64_t* tile_start2 = nullptr;   // the new tile_start / tile_pad, swapped in after
   int64_t* tile_pad2 = nullptr;

@@ -743,6 +743,34 @@ extern "C" int emsesg_fx_sort(emsesg_ctx* ctx) {
   return EMSESG_OK;
 }
 
+namespace emsesg {
+namespace {
+// Live particles inside a box body (the push's end-point test, inclusive
+// bounds), counted: records loaded from a caller may start inside one.
+__global__ void k_fx_count_in_boxes(const float4* __restrict__ pos, int64_t n, Geo g, Bodies bd,
+                                    unsigned long long* cnt) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const float4 p = pos[m];
+  const uint32_t cell = (uint32_t)__float_as_int(p.w);
+  if (cell == DEAD) return;
+  int c3[3];
+  unpack(g, cell, c3[0], c3[1], c3[2]);
+  const float f3v[3] = {p.x, p.y, p.z};
+  for (int q = 0; q < bd.n; q++) {
+    if (bd.kind[q] != 0) continue;
+    bool in = true;
+    for (int d = 0; d < 3; d++)
+      in = in && c3[d] >= bd.lo[q][d] && (c3[d] < bd.hi[q][d] || (c3[d] == bd.hi[q][d] && f3v[d] == 0.0f));
+    if (in) {
+      atomicAdd(cnt, 1ull);
+      return;
+    }
+  }
+}
+}  // namespace
+}  // namespace emsesg
+
 extern "C" int emsesg_fx_load(emsesg_ctx* ctx) {
   if (!ctx) return EMSESG_ERR_ARG;
   if (ctx->cfg.flags & EMSESG_FLAG_FP32_ONLY)
@@ -757,6 +785,24 @@ extern "C" int emsesg_fx_load(emsesg_ctx* ctx) {
     EMSESG_LAUNCH(ctx, "fx_from_aos", k_fx_from_aos, nblk(n), 256, 0, ctx->pbuf + ctx->seg.base[is], n, g,
                   f.pos + f.base[is], f.vx + f.base[is], f.vy + f.base[is], f.vz + f.base[is], ctx->d_status,
                   ctx->d_diag);
+  }
+  // particles that start inside a box body: the next push sends the tile
+  // regions next to a body down its general path, whose end-point test
+  // absorbs them as the reference's push does (a particle entering a box
+  // always crosses a cell face, so no later step needs it)
+  f.box_inside = false;
+  const Bodies bd = make_bodies(ctx->cfg);
+  if (bd.n > bd.ncurved) {
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(ctx->d_scratch64);
+    EMSESG_CUDA(ctx, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), ctx->stream));
+    for (int is = 0; is < ctx->cfg.nspec; is++)
+      if (ctx->totalp[is])
+        EMSESG_LAUNCH(ctx, "fx_in_boxes", k_fx_count_in_boxes, nblk(ctx->totalp[is]), 256, 0, f.pos + f.base[is],
+                      ctx->totalp[is], g, bd, cnt);
+    unsigned long long inside = 0;
+    EMSESG_CUDA(ctx, cudaMemcpyAsync(&inside, cnt, sizeof(inside), cudaMemcpyDeviceToHost, ctx->stream));
+    EMSESG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    f.box_inside = inside > 0;
   }
   // before the first sort the regions hold the records in buffer order
   EMSESG_CUDA(ctx, cudaMemcpyAsync(f.count_d, ctx->totalp, EMSESG_ISPEC * sizeof(int64_t), cudaMemcpyHostToDevice,
@@ -861,6 +907,7 @@ extern "C" int emsesg_fx_load_plasma(emsesg_ctx* ctx, const emsesg_plasma* pl) {
   f.loaded = true;
   f.tiled = false;
   f.rho_prev = false;
+  f.box_inside = false;  // cleared above
   rc = emsesg_fx_sort(ctx);
   if (rc) return rc;
   return emsesg_synchronize(ctx);
@@ -1002,8 +1049,12 @@ int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit, bool jd) {
       EMSESG_LAUNCH(ctx, "fx_move", (k_fx_push<8, false>), grid, PUSH_BLOCK, smem, a);
     return EMSESG_OK;
   }
-  const PushKernel kern = push_kernel(fx_box_tile(tmax), a.bd.ncurved > 0, jd);
+  // tile regions next to a body take the general path when a particle can
+  // end inside one without leaving its cell: always with cylinders or
+  // spheres, with boxes only while loaded particles may start inside one
+  const PushKernel kern = push_kernel(fx_box_tile(tmax), a.bd.ncurved > 0 || f.box_inside, jd);
   EMSESG_LAUNCH(ctx, "fx_push", kern, grid, PUSH_BLOCK, smem, a);
+  f.box_inside = false;
   // injected particles of the tail zones (general path, global deposits)
   int64_t drawn = 0;
   for (int is = 0; is < c.nspec; is++) {

@@ -587,8 +587,8 @@ __device__ __forceinline__ int body_absorb(const CrossCtx& c, const int (&ib)[3]
 
 // General path for one particle that left its cell (or whose cell lies
 // outside the box): boundary rules, zigzag with relay point, charge at the
-// stored cell; the final record is written here.  CURV = false: the run has
-// box bodies only.  JD = false: charge only (no zigzag current).
+// stored cell; the final record is written here.  CURV = false: no
+// cylinder or sphere to test.  JD = false: charge only (no zigzag current).
 template <int B, bool DEP = true, bool CURV = true, bool JD = true>
 __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, const int (&o)[3], const Sink& sk,
                                          const CrossCtx& c, const float* en) {
@@ -656,6 +656,26 @@ __device__ __forceinline__ int cross_one(const Geo& g, unsigned long long* box, 
     w = xd * zd; J[7] = vvy * w; J[5] = vvy * (xd - w); J[6] = vvy * (zd - w); J[4] = vvy * (1.0f - xd - (zd - w));
     w = xd * yd; J[11] = vvz * w; J[9] = vvz * (xd - w); J[10] = vvz * (yd - w); J[8] = vvz * (1.0f - xd - (yd - w));
   }
+  // a start point inside a box body moves to the relay point
+  // (psolve1.F90:648-651): no first segment
+  if (CURV && !escaped) {
+    const Bodies& bd = *c.bd;
+    const int ib3[3] = {ib, jb, kb};
+    const float ob3[3] = {bx, by, bz};
+    bool start_in = false;
+    for (int q = 0; q < bd.n && !start_in; q++) {
+      if (bd.kind[q] != 0) continue;
+      bool in = true;
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+        in = in && ib3[d] >= bd.lo[q][d] && (ib3[d] < bd.hi[q][d] || (ib3[d] == bd.hi[q][d] && ob3[d] == 0.0f));
+      start_in = in;
+    }
+    if (start_in) {
+#pragma unroll
+      for (int q = 0; q < NJ; q++) J[q] = 0.f;
+    }
+  }
   // both segments in the cell of the start point (a particle that did not
   // change cell): one set of node values.  A particle absorbed by a box
   // stops at the relay point (psolve1.F90:660-662): no second segment.
@@ -720,10 +740,12 @@ __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t s
 }
 
 // DEP = false: the move only (positions, velocities, boundary rules; no
-// current, no charge), for recomputing particle states.  CURV = true: the
-// run has cylinders or spheres (tile regions next to one push every
-// particle on the general path); without them the in-cell test keeps its
-// constant bound.  JD = false (the electrostatic step, psolve2 + charge):
+// current, no charge), for recomputing particle states.  CURV = true: a
+// particle may end inside a body without leaving its cell (cylinders or
+// spheres; boxes after a load of particles that start inside one): tile
+// regions next to a body push every particle on the general path; without
+// that the in-cell test keeps its constant bound.
+// JD = false (the electrostatic step, psolve2 + charge):
 // the charge only -- runs of 8 CIC sums, an accumulator of rho alone, no
 // zigzag current.
 template <int T, bool DEP = true, bool CURV = false, bool JD = true>
@@ -843,13 +865,15 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
 
   const float qmp = a.qmp[is], qfix = a.qfix[is];
   const float gustep = a.gustep, hr = 0.5f * a.rustep;
-  // A particle can enter a cylinder or a sphere without leaving its cell: in
-  // a tile region whose box touches one, every particle takes the general
-  // path (the in-cell test below then fails for all).
+  // A particle can end inside a body without leaving its cell (entering a
+  // cylinder or a sphere, or starting inside any body, where the reference's
+  // end-point test absorbs it): in a tile region whose box touches a body's
+  // cells (a box's lo..hi, its faces included; a curved body's bounding
+  // cells), every particle takes the general path, whose absorption test is
+  // the reference's (the in-cell test below then fails for all).
   float flo = 0.f;
   if (CURV)
     for (int q = 0; q < a.bd.n; q++) {
-      if (a.bd.kind[q] == 0) continue;
       bool hit = true;
 #pragma unroll
       for (int d = 0; d < 3; d++) hit = hit && o[d] + B - 2 >= a.bd.lo[q][d] && o[d] <= a.bd.hi[q][d];

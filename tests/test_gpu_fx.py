@@ -359,8 +359,10 @@ def test_async_eb_upload_with_graph_runs(gpu):
         batch.close()
 
 
-@pytest.mark.parametrize("npbnd,nfbnd,bodies", [((0, 0, 0), (0, 0, 0), False), ((0, 0, 2), (0, 0, 1), True)])
-def test_es_step_is_the_step_without_current(gpu, npbnd, nfbnd, bodies):
+@pytest.mark.parametrize("npbnd,nfbnd,bodies,tile", [((0, 0, 0), (0, 0, 0), False, (8, 8, 8)),
+                                                     ((0, 0, 2), (0, 0, 1), True, (8, 8, 8)),
+                                                     ((1, 0, 2), (1, 0, 1), True, (4, 4, 4))])
+def test_es_step_is_the_step_without_current(gpu, npbnd, nfbnd, bodies, tile):
     """emsesg_fx_step_es (psolve2 + charge on the FP32 form): the same
     particles, counts and rho, bit for bit, as emsesg_fx_step from the same
     state, over steps with re-sorts, escapes, injected particles (inflow
@@ -368,7 +370,7 @@ def test_es_step_is_the_step_without_current(gpu, npbnd, nfbnd, bodies):
     bodies) absorption by a box, a cylinder and a sphere; aj is left as it
     was.  Against the oracle's psolve2 + charge from the same state: rho
     within 1e-5."""
-    c = case(n=(16, 16, 24), ppc=(8, 8), npbnd=npbnd, nfbnd=nfbnd, vth_scale=3.0, tile=(8, 8, 8))
+    c = case(n=(16, 16, 24), ppc=(8, 8), npbnd=npbnd, nfbnd=nfbnd, vth_scale=3.0, tile=tile)
     if bodies:
         c.bodies = [dict(geotype=0, ncond=1, xlpc=3.0, xupc=7.0, ylpc=3.0, yupc=7.0, zlpc=4.0, zupc=9.0,
                          sqdscaled=1.0),
@@ -430,3 +432,28 @@ def test_es_step_is_the_step_without_current(gpu, npbnd, nfbnd, bodies):
         pa, _ = a.download_particles()
         pb, _ = b.download_particles()
         assert np.array_equal(pa.view(np.uint8), pb.view(np.uint8))
+
+
+def test_es_entry_points_refuse_bad_arguments(gpu):
+    """The electrostatic entry points: a Poisson boundary other than 0, 1, 2
+    and mltstp < 1 are argument errors; the step without the current is
+    refused in slab mode; the context stays usable after each refusal."""
+    from ctca_b200.emses import ERR_ARG, ERR_STATE, EmsesError
+    c = case(n=(16, 16, 16), ppc=(2, 2), tile=(8, 8, 8))
+    cfg, eb, p, tp = build(c, 1.2)
+    with Emses(cfg) as g:
+        g.upload_particles(p, tp)
+        g.upload_field("eb", eb)
+        g.fx_load()
+        with pytest.raises(EmsesError) as e:
+            g.esfield(1, mtd_vbnd=(0, 3, 0))
+        assert e.value.code == ERR_ARG
+        with pytest.raises(EmsesError) as e:
+            g.esfield(0)
+        assert e.value.code == ERR_ARG
+        g.fx_step_es(2, False)
+        assert g.esfield(1) >= 0.0
+        g.fx_slab(True, 1000)
+        with pytest.raises(EmsesError) as e:
+            g.fx_step_es(2, False)
+        assert e.value.code == ERR_STATE

@@ -297,3 +297,45 @@ def test_fx_load_plasma_leaves_out_curved_bodies(gpu):
     # the same particles outside the bodies (up to those on a surface)
     assert abs(int(pb.size) - int(keep.sum())) <= int(edge.sum())
     assert pb.size < pa.size
+
+
+@pytest.mark.parametrize("es", [False, True])
+def test_fx_particles_loaded_inside_a_box(gpu, es):
+    """Records loaded with particles inside a box body (the reference's push
+    absorbs every particle whose end point is inside, leaving its cell or
+    not; a start point inside moves to the relay point, so the first zigzag
+    segment carries no current): the first step of the FP32 form, with and
+    without the current, absorbs the same particles as the oracle's
+    psolve1 / psolve2 -- influx equal -- with rho and J within 1e-5."""
+    c = case(n=(16, 16, 24), ppc=(8, 8), npbnd=(1, 0, 2), nfbnd=(1, 0, 1), vth_scale=3.0, tile=(8, 8, 8))
+    c.bodies = [dict(geotype=0, ncond=1, xlpc=3.0, xupc=7.0, ylpc=3.0, yupc=7.0, zlpc=4.0, zupc=9.0, sqdscaled=1.0)]
+    cfg, eb, p, tp = build(c, 1.2)
+    g = Emses(cfg)
+    g.upload_particles(p, tp)
+    g.upload_field("eb", eb)
+    g.fx_load()
+    g.fx_store()
+    p32, tp32 = g.download_particles()
+    g.fx_load()
+    o = O.Oracle(cfg, p32, tp32, eb)
+    o.grdcrt()
+    if es:
+        o.psolve2(2)
+    else:
+        o.f["aj"][...] = 0.0
+        o.psolve1(2, 0)
+        o.reduce_aj()
+    o.charge(0)
+    o.reduce_rho("rho")
+    if es:
+        g.fx_step_es(2, False)
+    else:
+        g.fx_step(2, False)
+    gi = g.get_counters().as_dict()["influx"][:2, 0]
+    oi = o.gc.as_dict()["influx"][:2, 0]
+    print("influx", gi, "oracle", oi)
+    assert oi.sum() > 100 and np.array_equal(gi, oi)
+    assert C.field_errors(g.download_field("rho"), o.f["rho"], cfg)["l2_rel"] < 1e-5
+    if not es:
+        assert C.field_errors(g.download_field("aj"), o.f["aj"], cfg)["l2_rel"] < 1e-5
+    g.close()
