@@ -457,3 +457,19 @@ def test_es_entry_points_refuse_bad_arguments(gpu):
         with pytest.raises(EmsesError) as e:
             g.fx_step_es(2, False)
         assert e.value.code == ERR_STATE
+
+
+@pytest.mark.parametrize("ustep", [1, 4])
+def test_fx_one_step_other_usteps(gpu, ustep):
+    """The push with ustep other than 2 (the time step in units of dth: the
+    kick E * qm * ustep / 2, the move v * ustep, the current (a - b) / ustep)
+    against the oracle's psolve1 + charge from the same state."""
+    c = case(n=(16, 16, 16), ppc=(8, 8), npbnd=(0, 0, 0), nfbnd=(0, 0, 0), vth_scale=2.0, tile=(8, 8, 8))
+    cfg, g, o, p32, tp32 = fx_pair(c)
+    g.fx_step(ustep, False)
+    oracle_step(o, ustep)
+    rho_err = rel_l2(g.download_field("rho"), o.f["rho"])
+    aj_err = rel_l2(g.download_field("aj"), o.f["aj"])
+    print(f"ustep {ustep}: rho {rho_err:.2e}, J {aj_err:.2e}")
+    assert rho_err < RHOJ_TOL and aj_err < RHOJ_TOL
+    g.close()
