@@ -473,3 +473,28 @@ def test_fx_one_step_other_usteps(gpu, ustep):
     print(f"ustep {ustep}: rho {rho_err:.2e}, J {aj_err:.2e}")
     assert rho_err < RHOJ_TOL and aj_err < RHOJ_TOL
     g.close()
+
+
+def test_fx_species_with_their_own_boundaries(gpu):
+    """npbnd per species (electrons periodic in x and escaping in z, ions
+    reflecting in x and periodic in z): two steps with a re-sort against
+    the oracle started from the FP32 state before each."""
+    c = case(n=(16, 16, 16), ppc=(8, 8), nfbnd=(0, 0, 1), vth_scale=3.0, tile=(8, 8, 8))
+    c.species[0].npbnd = (0, 0, 2)
+    c.species[1].npbnd = (1, 0, 0)
+    cfg, g, o, p32, tp32 = fx_pair(c, 1.2)
+    for k in range(2):
+        if k:
+            g.fx_store()
+            p32, tp32 = g.download_particles()
+            g.fx_load()
+            o = O.Oracle(cfg, p32, tp32, o.eb)
+        g.fx_step(2, k == 0)
+        oracle_step(o)
+        rho_err = rel_l2(g.download_field("rho"), o.f["rho"])
+        aj_err = rel_l2(g.download_field("aj"), o.f["aj"])
+        print(f"step {k}: rho {rho_err:.2e}, J {aj_err:.2e}")
+        assert rho_err < RHOJ_TOL and aj_err < RHOJ_TOL
+    nesc = g.get_counters().as_dict()["nesc"]
+    assert nesc[0] > 0 and nesc[1] == 0
+    g.close()
