@@ -498,3 +498,47 @@ def test_fx_species_with_their_own_boundaries(gpu):
     nesc = g.get_counters().as_dict()["nesc"]
     assert nesc[0] > 0 and nesc[1] == 0
     g.close()
+
+
+@pytest.mark.parametrize("nspec", [1, 3])
+def test_fx_other_species_counts(gpu, nspec):
+    """One species (electrons alone) and three (a second, heavier ion
+    population with its own density): two steps with a re-sort against the
+    oracle, with and without the current -- the per-species regions, launch
+    rows and counters of the FP32 form for species counts other than two."""
+    from ctca_b200.inputs import Species
+    c = case(n=(16, 16, 16), ppc=(8, 8), vth_scale=2.0, tile=(8, 8, 8))
+    if nspec == 1:
+        c.species = c.species[:1]
+    else:
+        c.species.append(Species(ppc=4, qm=1.0 / 400.0, vth=c.species[1].vth * 0.5, drift=(0.0, 0.01, 0.0)))
+    cfg, g, o, p32, tp32 = fx_pair(c, 1.2)
+    assert cfg.nspec == nspec
+    for k in range(3):
+        if k:
+            g.fx_store()
+            p32, tp32 = g.download_particles()
+            g.fx_load()
+            o = O.Oracle(cfg, p32, tp32, o.eb)
+        es = k == 2
+        if es:
+            g.fx_step_es(2, False)
+            o.grdcrt()
+            o.psolve2(2)
+            o.charge(0)
+            o.reduce_rho("rho")
+        else:
+            g.fx_step(2, k == 0)
+            oracle_step(o)
+        rho_err = rel_l2(g.download_field("rho"), o.f["rho"])
+        msg = f"nspec {nspec} step {k}: rho {rho_err:.2e}"
+        assert rho_err < RHOJ_TOL, msg
+        if not es:
+            aj_err = rel_l2(g.download_field("aj"), o.f["aj"])
+            msg += f", J {aj_err:.2e}"
+            assert aj_err < RHOJ_TOL, msg
+        print(msg)
+        assert np.array_equal(g.fx_counts(), o.totalp[:nspec]), k
+    e = g.fx_energy()
+    assert e.shape[0] == nspec and np.all(e > 0)
+    g.close()
