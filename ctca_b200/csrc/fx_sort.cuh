@@ -347,6 +347,13 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restr
   const int L = (int)((n + PUSH_THREADS - 1) / PUSH_THREADS);
   const int64_t s0 = tp[t];
   uint32_t* mywb = wb + warp * G.nbc;
+  // the tile's own cells per axis (the last tile of an axis whose length is
+  // not a multiple of the tile is shorter; on a periodic axis its sort box
+  // then reaches past the grid's end onto the next tile's cells): box
+  // position 0 is the tile below, 1..ext its own cells, beyond them the tile
+  // above
+  const int ext0 = min(G.t[0], G.n[0] - tx * G.t[0]), ext1 = min(G.t[1], G.n[1] - ty * G.t[1]),
+            ext2 = min(G.t[2], G.n[2] - tz * G.t[2]);
   // the cells of the next rows are loaded ahead
   constexpr int AHEAD = 4;
   uint32_t cr[AHEAD];
@@ -366,8 +373,8 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_lcs_rank(const float4* __restr
       const int a = lcs_axis(G, 0, tx, i), b = lcs_axis(G, 1, ty, j), c = lcs_axis(G, 2, tz, k);
       if ((a | b | c) >= 0) {  // else a stray: the radix path sorts
         bc = a + G.bc[0] * (b + G.bc[1] * c);
-        nb = (a == 0 ? 0 : (a == G.bc[0] - 1 ? 2 : 1)) + 3 * (b == 0 ? 0 : (b == G.bc[1] - 1 ? 2 : 1)) +
-             9 * (c == 0 ? 0 : (c == G.bc[2] - 1 ? 2 : 1));
+        nb = (a == 0 ? 0 : (a <= ext0 ? 1 : 2)) + 3 * (b == 0 ? 0 : (b <= ext1 ? 1 : 2)) +
+             9 * (c == 0 ? 0 : (c <= ext2 ? 1 : 2));
       }
     }
     const unsigned peers = __match_any_sync(0xffffffffu, bc);

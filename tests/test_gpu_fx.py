@@ -138,27 +138,31 @@ def _tile_key(cfg, tile, p):
     return tid * (tile[0] * tile[1] * tile[2]) + lin, tid
 
 
-@pytest.mark.parametrize("npbnd,tile,ppc", [
-    ((0, 0, 0), (8, 8, 8), (8, 8)),
-    ((1, 2, 0), (8, 4, 8), (8, 8)),
+@pytest.mark.parametrize("npbnd,tile,ppc,n", [
+    ((0, 0, 0), (8, 8, 8), (8, 8), (16, 16, 16)),
+    ((1, 2, 0), (8, 4, 8), (8, 8), (16, 16, 16)),
     # tiles of 28 rows: the move's small shape, 40-column windows; of 1
     # row: one group of the whole row
-    ((0, 0, 0), (8, 8, 8), (40, 1)),
+    ((0, 0, 0), (8, 8, 8), (40, 1), (16, 16, 16)),
     # tiles of 45 rows: the mid shape, three buffers
-    ((0, 0, 0), (8, 8, 8), (64, 4)),
+    ((0, 0, 0), (8, 8, 8), (64, 4), (16, 16, 16)),
     # tiles of 67 rows: the large shape with windows
-    ((0, 0, 0), (8, 8, 8), (96, 4)),
+    ((0, 0, 0), (8, 8, 8), (96, 4), (16, 16, 16)),
     # tiles of 98 rows: no window, inv read from global memory, several
     # batches of slots per group
-    ((0, 0, 0), (8, 8, 8), (140, 4)),
+    ((0, 0, 0), (8, 8, 8), (140, 4), (16, 16, 16)),
+    # partial tiles: grid sizes that are not multiples of the tile, periodic
+    # (the last tile's sort box wraps onto the first tile) and not
+    ((0, 0, 0), (8, 8, 8), (8, 8), (20, 12, 18)),
+    ((1, 2, 0), (8, 8, 8), (8, 8), (13, 22, 9)),
 ])
-def test_fx_local_sort_is_a_stable_cell_sort(gpu, npbnd, tile, ppc):
+def test_fx_local_sort_is_a_stable_cell_sort(gpu, npbnd, tile, ppc, n):
     """The re-sort after a step (the tile-local counting sort) orders the
     live particles by the tile-major cell key; equal cells keep the order
     (source tile, warp, row, lane) of the thread-major layout of the last
     sort, computed here from the tile sizes of that sort."""
     threads = FX_ROW_SLOTS
-    c = case(n=(16, 16, 16), ppc=ppc, npbnd=npbnd, vth_scale=6.0, tile=tile)
+    c = case(n=n, ppc=ppc, npbnd=npbnd, vth_scale=6.0, tile=tile)
     cfg, eb, p, tp = build(c)
     g = Emses(cfg)
     g.upload_particles(p, tp)
@@ -541,4 +545,32 @@ def test_fx_other_species_counts(gpu, nspec):
         assert np.array_equal(g.fx_counts(), o.totalp[:nspec]), k
     e = g.fx_energy()
     assert e.shape[0] == nspec and np.all(e > 0)
+    g.close()
+
+
+@pytest.mark.parametrize("n,npbnd,nfbnd", [((20, 12, 18), (0, 0, 0), (0, 0, 0)), ((13, 22, 9), (1, 0, 2), (1, 0, 1))])
+def test_fx_partial_tiles(gpu, n, npbnd, nfbnd):
+    """Grid sizes that are not multiples of the 8-cell sort tile (partial
+    tiles on every axis, odd sizes): steps with re-sorts against the oracle,
+    and the tile-local sort's order against its definition."""
+    c = case(n=n, ppc=(6, 6), npbnd=npbnd, nfbnd=nfbnd, vth_scale=3.0, tile=(8, 8, 8))
+    cfg, g, o, p32, tp32 = fx_pair(c, 1.2)
+    for k in range(3):
+        if k:
+            g.fx_store()
+            p32, tp32 = g.download_particles()
+            g.fx_load()
+            o = O.Oracle(cfg, p32, tp32, o.eb)
+        g.fx_step(2, k == 1)
+        oracle_step(o)
+        rho_err = rel_l2(g.download_field("rho"), o.f["rho"])
+        aj_err = rel_l2(g.download_field("aj"), o.f["aj"])
+        print(f"{n} step {k}: rho {rho_err:.2e}, J {aj_err:.2e}")
+        assert rho_err < RHOJ_TOL and aj_err < RHOJ_TOL
+        # live particles per species (the re-sort drops the dead ones; the
+        # oracle keeps them in place until a compaction)
+        base = np.concatenate([[0], np.cumsum(o.totalp[:cfg.nspec])])
+        live = [int((o.pbuf["nid"][base[s]:base[s + 1]] != -1).sum()) for s in range(cfg.nspec)]
+        if k == 1:
+            assert list(g.fx_counts()) == live, k
     g.close()
