@@ -202,12 +202,14 @@ def inside_any(p, bodies):
     return m
 
 
-def test_fx_cylinder_sphere_per_step(gpu):
+@pytest.mark.parametrize("es", [False, True])
+def test_fx_cylinder_sphere_per_step(gpu, es):
     """Cylinders and spheres in the FP32 form: every step from the FP32
     form's own state against the oracle, rho and J within 1e-5 relative L2
     and the absorbed counts of each body equal, except for particles listed
     as next to a decision FP32 rounding can flip (an end point within 1e-5
-    cell of a curved surface, or next to an integer plane)."""
+    cell of a curved surface, or next to an integer plane).  With `es` the
+    step without the current against psolve2 + charge."""
     c = case(n=(24, 24, 24), ppc=(6, 6), vth_scale=3.0, tile=(8, 8, 8))
     c.bodies = CURVED
     cfg, eb, p, tp = build(c, capacity_factor=1.5)
@@ -231,14 +233,20 @@ def test_fx_cylinder_sphere_per_step(gpu):
     for step in range(4):
         o = O.Oracle(cfg, cur, tp_cur, eb)
         o.grdcrt()
-        o.f["aj"][...] = 0.0
-        o.psolve1(2, 0)
-        o.reduce_aj()
+        if es:
+            o.psolve2(2)
+        else:
+            o.f["aj"][...] = 0.0
+            o.psolve1(2, 0)
+            o.reduce_aj()
         o.charge(0)
         o.reduce_rho("rho")
-        g.fx_step(2, step % 2 == 1)
+        if es:
+            g.fx_step_es(2, step % 2 == 1)
+        else:
+            g.fx_step(2, step % 2 == 1)
         er = C.field_errors(g.download_field("rho"), o.f["rho"], cfg)["l2_rel"]
-        ej = C.field_errors(g.download_field("aj"), o.f["aj"], cfg)["l2_rel"]
+        ej = 0.0 if es else C.field_errors(g.download_field("aj"), o.f["aj"], cfg)["l2_rel"]
         live = cur["nid"] != -1  # records of particles that died since the last sort stay in place
         near = live & (C.near_faces(cfg, cur, o.pbuf, bodies=[((3, 3, 3), (7, 7, 7))])
                        | C.near_curved(o.pbuf, CURVED))
