@@ -11,6 +11,9 @@
 
 #include "../../include/emses_gpu.h"
 
+// z chunks of an asynchronous eb upload for the FP32 step (parts of its push)
+constexpr int EMSESG_EB_PARTS = 4;
+
 namespace emsesg {
 
 // Fortran-layout field descriptor (nc, lo:n+hi per axis), component fastest.
@@ -135,6 +138,8 @@ struct FxState {
   const double* g_eb = nullptr;        // (an asynchronous eb upload swaps the eb buffer)
   emsesg_config g_cfg{};
   AdjWork* adj = nullptr;
+  uint32_t* defer = nullptr;        // one bit per slot: left for k_fx_deferred by the parts of a step
+  int64_t defer_words = 0;
   int64_t* accum = nullptr;         // int64 (rho, jx, jy, jz) on the rho layout
   double* diag = nullptr;           // FP64 checks: energy partials, sums, continuity maxima
   bool rho_prev = false;            // the rho field holds the deposit of the step before
@@ -185,6 +190,13 @@ struct emsesg_ctx {
   cudaEvent_t ev_eb = nullptr;
   double* eb_next = nullptr;
   bool eb_next_pending = false;
+  // the pending eb copied in z chunks for the FP32 step (eb_parts > 1):
+  // chunk p holds what the node planes 0..eb_zready[p] read, and part p of
+  // the push (tiles eb_tile[p] .. eb_tile[p+1] - 1) runs once it is there
+  int eb_parts = 0;
+  int eb_zready[EMSESG_EB_PARTS] = {0};
+  int64_t eb_tile[EMSESG_EB_PARTS + 1] = {0};
+  cudaEvent_t ev_ebp[EMSESG_EB_PARTS] = {nullptr};
   std::string err;
   emsesg::Segments seg;
   int64_t totalp[EMSESG_ISPEC] = {0};  // host mirror of the species counts
@@ -217,6 +229,10 @@ int set_error(emsesg_ctx* ctx, int code, const char* fmt, ...);
 // copy) before the work that reads eb.
 int side_stream(emsesg_ctx* ctx);
 int apply_pending_eb(emsesg_ctx* ctx);
+// The z chunks of an eb upload for the FP32 step (fx.cu): per part the last
+// node plane it needs and its first tile; returns the number of parts (0:
+// one copy).
+int fx_eb_plan(const emsesg_ctx* ctx, int* zready, int64_t* tile);
 // Records m0 .. m0+n-1 of species `is` of the seeded plasma of
 // emsesg_load_plasma, into the device array dst (n records).
 int plasma_records(emsesg_ctx* ctx, emsesg_particle* dst, int is, int64_t m0, int64_t n, const emsesg_plasma* pl);

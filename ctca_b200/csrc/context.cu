@@ -195,6 +195,8 @@ extern "C" int emsesg_destroy(emsesg_ctx* ctx) {
   cudaFree(ctx->eb_next);
   if (ctx->ev_fields) cudaEventDestroy(ctx->ev_fields);
   if (ctx->ev_eb) cudaEventDestroy(ctx->ev_eb);
+  for (auto e : ctx->ev_ebp)
+    if (e) cudaEventDestroy(e);
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -333,7 +335,28 @@ extern "C" int emsesg_upload_field_async(emsesg_ctx* ctx, int field, const doubl
   if (!ctx->eb_next) EMSESG_CUDA(ctx, cudaMalloc(&ctx->eb_next, n * sizeof(double)));
   // the buffer was last read before the last step's field phase ended
   EMSESG_CUDA(ctx, cudaStreamWaitEvent(ctx->side, ctx->ev_fields, 0));
-  EMSESG_CUDA(ctx, cudaMemcpyAsync(ctx->eb_next, host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->side));
+  // for the FP32 step: in z chunks, each with its event, so that the push's
+  // parts start while the later planes are still on their way
+  ctx->eb_parts = emsesg::fx_eb_plan(ctx, ctx->eb_zready, ctx->eb_tile);
+  if (ctx->eb_parts > 1) {
+    const emsesg::FieldDesc fe = emsesg::field_desc(ctx->cfg, EMSESG_FIELD_EB);
+    const int64_t plane = (int64_t)fe.nc * fe.ex * fe.ey;  // doubles of one z plane
+    int64_t done = 0;
+    for (int p = 0; p < ctx->eb_parts; p++) {
+      if (!ctx->ev_ebp[p]) EMSESG_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_ebp[p], cudaEventDisableTiming));
+      // node plane k reads the eb planes k - 1 and k
+      const int64_t upto =
+          p + 1 == ctx->eb_parts ? n : std::min(n, (int64_t)(ctx->eb_zready[p] - fe.lo + 1) * plane);
+      if (upto > done) {
+        EMSESG_CUDA(ctx, cudaMemcpyAsync(ctx->eb_next + done, host + done, (upto - done) * sizeof(double),
+                                         cudaMemcpyHostToDevice, ctx->side));
+        done = upto;
+      }
+      EMSESG_CUDA(ctx, cudaEventRecord(ctx->ev_ebp[p], ctx->side));
+    }
+  } else {
+    EMSESG_CUDA(ctx, cudaMemcpyAsync(ctx->eb_next, host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->side));
+  }
   EMSESG_CUDA(ctx, cudaEventRecord(ctx->ev_eb, ctx->side));
   ctx->eb_next_pending = true;
   return EMSESG_OK;

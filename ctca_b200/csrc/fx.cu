@@ -56,14 +56,16 @@ __device__ __forceinline__ uint32_t pack(const Geo& g, int i, int j, int k) {
 
 // ---------------------------------------------------------------- fields
 // FP32 node field from the staggered FP64 eb (grdcrt.F90:156-169, 214-230),
-// nodes 0..n on every axis.
+// nodes 0..n on the x and y axes, node planes k0 .. k0 + nk - 1 on z (node
+// plane k reads the eb planes k - 1 and k).
 __global__ void k_grdcrt32(const double* __restrict__ eb, float4* __restrict__ f0, float4* __restrict__ f1,
-                           FieldDesc fe, int nx, int ny, int nz, double e0x, double e0y, double e0z, double b0x,
-                           double b0y, double b0z) {
+                           FieldDesc fe, int nx, int ny, int k0, int nk, double e0x, double e0y, double e0z,
+                           double b0x, double b0y, double b0z) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int64_t ex = nx + 1, ey = ny + 1, ez = nz + 1;
-  if (t >= ex * ey * ez) return;
-  int i = (int)(t % ex), j = (int)((t / ex) % ey), k = (int)(t / (ex * ey));
+  int64_t ex = nx + 1, ey = ny + 1;
+  if (t >= ex * ey * nk) return;
+  int i = (int)(t % ex), j = (int)((t / ex) % ey), k = k0 + (int)(t / (ex * ey));
+  t += (int64_t)k0 * ex * ey;
   double wex = 0.5 * (eb[fe.at(0, i, j, k)] + eb[fe.at(0, i - 1, j, k)]) + e0x;
   double wey = 0.5 * (eb[fe.at(1, i, j, k)] + eb[fe.at(1, i, j - 1, k)]) + e0y;
   double wez = 0.5 * (eb[fe.at(2, i, j, k)] + eb[fe.at(2, i, j, k - 1)]) + e0z;
@@ -490,6 +492,10 @@ int fx_alloc(emsesg_ctx* ctx) {
   EMSESG_CUDA(ctx, cudaMalloc(&f.chunk_start, (int64_t)c.nspec * (f.ntiles + 1) * sizeof(int64_t)));
   FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
   EMSESG_CUDA(ctx, cudaMalloc(&f.accum, (fr.size() + fj.size()) * sizeof(int64_t)));
+  // one bit per slot: the particles the parts of a step leave for k_fx_deferred
+  f.defer_words = (cap + 31) / 32;
+  EMSESG_CUDA(ctx, cudaMalloc(&f.defer, f.defer_words * sizeof(uint32_t)));
+  EMSESG_CUDA(ctx, cudaMemsetAsync(f.defer, 0, f.defer_words * sizeof(uint32_t), ctx->stream));
   // FP64 checks: energy partials and sums, the continuity maxima
   EMSESG_CUDA(ctx, cudaMalloc(&f.diag, (3 * DIAG_GRID + 3 + 2) * sizeof(double)));
   EMSESG_CUDA(ctx, cudaMemsetAsync(f.diag, 0, (3 * DIAG_GRID + 3 + 2) * sizeof(double), ctx->stream));
@@ -529,8 +535,10 @@ int fx_alloc(emsesg_ctx* ctx) {
   for (int box : {4, 8})
     for (int curved = 0; curved < 2; curved++)
       for (int jd = 0; jd < 2; jd++)
-        EMSESG_CUDA(ctx, cudaFuncSetAttribute(push_kernel(box, curved != 0, jd != 0),
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize, fx_push_smem(box, jd != 0)));
+        for (int parts = 0; parts < 2; parts++)
+          EMSESG_CUDA(ctx, cudaFuncSetAttribute(push_kernel(box, curved != 0, jd != 0, parts != 0),
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                fx_push_smem(box, jd != 0)));
   return EMSESG_OK;
 }
 
@@ -539,7 +547,7 @@ void fx_free(emsesg_ctx* ctx) {
   cudaFree(f.pos); cudaFree(f.vx); cudaFree(f.vy); cudaFree(f.vz);
   cudaFree(f.pos2); cudaFree(f.vx2); cudaFree(f.vy2); cudaFree(f.vz2);
   cudaFree(f.count_d); cudaFree(f.slots_d); cudaFree(f.tile_start); cudaFree(f.tile_pad); cudaFree(f.accum);
-  cudaFree(f.chunk_start);
+  cudaFree(f.chunk_start); cudaFree(f.defer);
   cudaFree(f.fnode); cudaFree(f.fnode2);
   cudaFree(f.diag);
   cudaFree(f.tile_start2); cudaFree(f.tile_pad2); cudaFree(f.lcs_cnt); cudaFree(f.lcs_base); cudaFree(f.lcs_wcnt);
@@ -964,6 +972,29 @@ extern "C" int emsesg_fx_step(emsesg_ctx* ctx, int ustep, int do_sort) {
   return fx_step_impl(ctx, ustep, do_sort, true);
 }
 
+namespace emsesg {
+// The parts of a push whose eb arrives in z chunks: part p takes the tile
+// layers tz0 .. tz1 - 1 (tiles tile[p] .. tile[p+1] - 1) and needs the node
+// planes 0..zready[p] (its tiles' boxes: tz1 - 1 times the tile edge plus
+// the compiled box).  Returns the number of parts, 0 where the step does not
+// run in parts (FP32 form not loaded, slab mode, one tile layer).
+int fx_eb_plan(const emsesg_ctx* ctx, int* zready, int64_t* tile) {
+  const FxState& f = ctx->fx;
+  if (!f.loaded || f.slab || f.ntile[2] < 2) return 0;
+  const int nz = ctx->cfg.nz;
+  const int parts = std::min(EMSESG_EB_PARTS, f.ntile[2]);
+  const int tmax = std::max(f.tile[0], std::max(f.tile[1], f.tile[2]));
+  const int64_t layer = (int64_t)f.ntile[0] * f.ntile[1];
+  for (int p = 0; p < parts; p++) {
+    const int tz0 = p * f.ntile[2] / parts, tz1 = (p + 1) * f.ntile[2] / parts;
+    tile[p] = tz0 * layer;
+    zready[p] = p == parts - 1 ? nz : std::min(nz, (tz1 - 1) * f.tile[2] + fx_box_tile(tmax) + PG);
+  }
+  tile[parts] = f.ntiles;
+  return parts;
+}
+}  // namespace emsesg
+
 namespace {
 // The push of one step: grdcrt, the particles of the tile regions and of the
 // tail zones, into the zeroed int64 accumulators (the J of injection
@@ -979,13 +1010,30 @@ int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit, bool jd) {
   std::string why;
   if (!bodies_supported(c, &why)) return set_error(ctx, EMSESG_ERR_UNSUPPORTED, "%s", why.c_str());
   FxState& f = ctx->fx;
-  int rc0 = apply_pending_eb(ctx);
-  if (rc0) return rc0;
+  // an eb copied in z chunks: the push runs in parts, part p once chunk p is
+  // there (the plan it was copied with still holds, no graph capture)
+  int zready[EMSESG_EB_PARTS];
+  int64_t ptile[EMSESG_EB_PARTS + 1];
+  int parts = 0;
+  if (deposit && ctx->eb_next_pending && ctx->eb_parts > 1 && !f.capture) {
+    parts = fx_eb_plan(ctx, zready, ptile);
+    for (int p = 0; parts && p < parts; p++)
+      if (zready[p] != ctx->eb_zready[p] || ptile[p + 1] != ctx->eb_tile[p + 1]) parts = 0;
+    if (parts != ctx->eb_parts) parts = 0;
+  }
+  if (parts) {
+    std::swap(ctx->field[EMSESG_FIELD_EB], ctx->eb_next);
+    ctx->eb_next_pending = false;
+  } else {
+    int rc0 = apply_pending_eb(ctx);
+    if (rc0) return rc0;
+  }
   Geo g = make_geo(ctx);
-  int64_t nn = (int64_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1);
-  EMSESG_LAUNCH(ctx, "fx_grdcrt", k_grdcrt32, nblk(nn), 256, 0, ctx->field[EMSESG_FIELD_EB], f.fnode, f.fnode2,
-                field_desc(c, EMSESG_FIELD_EB), c.nx, c.ny, c.nz, c.e0[0], c.e0[1], c.e0[2], c.b0[0], c.b0[1],
-                c.b0[2]);
+  const int64_t nplane = (int64_t)(c.nx + 1) * (c.ny + 1);
+  if (!parts)
+    EMSESG_LAUNCH(ctx, "fx_grdcrt", k_grdcrt32, nblk(nplane * (c.nz + 1)), 256, 0, ctx->field[EMSESG_FIELD_EB],
+                  f.fnode, f.fnode2, field_desc(c, EMSESG_FIELD_EB), c.nx, c.ny, 0, c.nz + 1, c.e0[0], c.e0[1],
+                  c.e0[2], c.b0[0], c.b0[1], c.b0[2]);
   FieldDesc fr = field_desc(c, EMSESG_FIELD_RHO), fj = field_desc(c, EMSESG_FIELD_AJ);
   unsigned long long* acc_rho = (unsigned long long*)f.accum;
   unsigned long long* acc_j = acc_rho + fr.size();
@@ -1029,6 +1077,8 @@ int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit, bool jd) {
   a.bd = make_bodies(c);
   a.status = ctx->d_status;
   a.diag = ctx->d_diag;
+  a.zready = c.nz;
+  a.defer = f.defer;
   if (f.slab && deposit) {
     EMSESG_CUDA(ctx, cudaMemsetAsync(f.outbox_n, 0, 2 * EMSESG_ISPEC * sizeof(unsigned long long), ctx->stream));
     a.ob = Outbox{f.outbox, f.outbox_n, f.outbox_cap};
@@ -1052,8 +1102,34 @@ int fx_push_phase(emsesg_ctx* ctx, int ustep, bool deposit, bool jd) {
   // tile regions next to a body take the general path when a particle can
   // end inside one without leaving its cell: always with cylinders or
   // spheres, with boxes only while loaded particles may start inside one
-  const PushKernel kern = push_kernel(fx_box_tile(tmax), a.bd.ncurved > 0 || f.box_inside, jd);
-  EMSESG_LAUNCH(ctx, "fx_push", kern, grid, PUSH_BLOCK, smem, a);
+  const bool curv = a.bd.ncurved > 0 || f.box_inside;
+  const PushKernel kern = push_kernel(fx_box_tile(tmax), curv, jd);
+  if (!parts) {
+    EMSESG_LAUNCH(ctx, "fx_push", kern, grid, PUSH_BLOCK, smem, a);
+  } else {
+    const PushKernel pkern = push_kernel(fx_box_tile(tmax), curv, jd, true);
+    // part p: the node planes its chunk completes (its tiles' boxes), then
+    // its tiles
+    int k0 = 0;
+    for (int p = 0; p < parts; p++) {
+      EMSESG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_ebp[p], 0));
+      const int nk = zready[p] + 1 - k0;
+      if (nk > 0)
+        EMSESG_LAUNCH(ctx, "fx_grdcrt", k_grdcrt32, nblk(nplane * nk), 256, 0, ctx->field[EMSESG_FIELD_EB], f.fnode,
+                      f.fnode2, field_desc(c, EMSESG_FIELD_EB), c.nx, c.ny, k0, nk, c.e0[0], c.e0[1], c.e0[2],
+                      c.b0[0], c.b0[1], c.b0[2]);
+      k0 = std::max(k0, zready[p] + 1);
+      FxPushArgs ap = a;
+      ap.t_lo = ptile[p];
+      ap.t_n = ptile[p + 1] - ptile[p];
+      ap.zready = zready[p];
+      dim3 pgrid((unsigned)(ap.t_n + rows / f.chunk_rows + 1), (unsigned)c.nspec);
+      EMSESG_LAUNCH(ctx, "fx_push_part", pkern, pgrid, PUSH_BLOCK, smem, ap);
+    }
+    // the particles the parts left, every node plane converted
+    EMSESG_LAUNCH(ctx, "fx_deferred", deferred_kernel(fx_box_tile(tmax), curv, jd), nblk(f.defer_words), 256, 0,
+                  a, f.defer, f.defer_words, c.nspec);
+  }
   f.box_inside = false;
   // injected particles of the tail zones (general path, global deposits)
   int64_t drawn = 0;

@@ -146,6 +146,14 @@ struct FxPushArgs {
   Outbox ob;
   int* status;
   long long* diag;
+  // the tiles of this launch: t_lo .. t_lo + t_n - 1 (t_n = 0: every tile;
+  // a step whose eb arrives in z chunks pushes its tile layers in parts)
+  int64_t t_lo, t_n;
+  // a part (PARTS) holds the node planes 0..zready; it marks here (one bit
+  // per slot) a particle that would gather from a higher plane, which
+  // k_fx_deferred pushes after the last part
+  int zready;
+  uint32_t* defer;
 };
 
 // ---------------------------------------------------------------- PTX
@@ -748,7 +756,7 @@ __device__ __forceinline__ int cross_list(const FxPushArgs& a, int is, int64_t s
 // JD = false (the electrostatic step, psolve2 + charge):
 // the charge only -- runs of 8 CIC sums, an accumulator of rho alone, no
 // zigzag current.
-template <int T, bool DEP = true, bool CURV = false, bool JD = true>
+template <int T, bool DEP = true, bool CURV = false, bool JD = true, bool PARTS = false>
 __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   constexpr int B = T + 2 * PG + 1;  // box and field tile edge (nodes)
   constexpr int NC = JD ? NJ + NR : NR;  // sums of a run: zigzag J and CIC rho, or rho alone
@@ -777,9 +785,10 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
   // sums into the same global arrays)
   const int64_t* ts = a.tile_start + (int64_t)is * (a.ntiles + 1);
   const int64_t* cs = a.chunk_start + (int64_t)is * (a.ntiles + 1);
-  const int64_t b = blockIdx.x;
-  if (b >= cs[a.ntiles]) return;
-  int64_t tlo = 0, thi = a.ntiles;  // the last tile with cs[t] <= b
+  const int64_t t_end = a.t_n > 0 ? a.t_lo + a.t_n : a.ntiles;
+  const int64_t b = cs[a.t_lo] + blockIdx.x;
+  if (b >= cs[t_end]) return;
+  int64_t tlo = a.t_lo, thi = t_end;  // the last tile with cs[t] <= b
   while (thi - tlo > 1) {
     const int64_t mid = (tlo + thi) >> 1;
     if (cs[mid] <= b) tlo = mid;
@@ -968,22 +977,32 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     }
 
     // ---- gather + Buneman-Boris (psolve1.F90:186-272)
-    bool simple = false, oop = false;
+    bool simple = false, oop = false, defer = false;
     int gb = -1;
     float sx = 0.f, syy = 0.f, szz = 0.f;
     if (act) {
       gb = cell == runcell ? runbase : box_base<B>(o, ib, jb, kb);
-      kick<B>(a, sf0, sf1, gb, ib, jb, kb, ps, qmp, vx, vy, vz);
-      sx = ps.x + vx * gustep;
-      syy = ps.y + vy * gustep;
-      szz = ps.z + vz * gustep;
-      // an end point exactly on a cell face takes the general path (it may
-      // lie on a body face: inclusive bounds)
-      const bool incell = sx > flo && sx < 1.0f && syy > 0.f && syy < 1.0f && szz > 0.f && szz < 1.0f;
-      simple = incell && (!DEP || (cell == runcell && runbase >= 0));
-      // a particle that stays in its cell but is out of place in the thread's
-      // run (it changed cell since the sort): its 20 sums go to the run queue
-      oop = DEP && incell && !simple && gb >= 0;
+      // a part of a step whose eb arrives in z chunks: a cell outside the box
+      // (a particle that crossed a periodic face or left the box since the
+      // sort) whose node planes are not converted yet is left as it is for
+      // k_fx_deferred
+      defer = PARTS && gb < 0 && kb + 1 > a.zready;
+      if (defer) {
+        const int64_t m = slot0 + (int64_t)r * PUSH_THREADS + tid;
+        atomicOr(a.defer + (m >> 5), 1u << (m & 31));
+      } else {
+        kick<B>(a, sf0, sf1, gb, ib, jb, kb, ps, qmp, vx, vy, vz);
+        sx = ps.x + vx * gustep;
+        syy = ps.y + vy * gustep;
+        szz = ps.z + vz * gustep;
+        // an end point exactly on a cell face takes the general path (it may
+        // lie on a body face: inclusive bounds)
+        const bool incell = sx > flo && sx < 1.0f && syy > 0.f && syy < 1.0f && szz > 0.f && szz < 1.0f;
+        simple = incell && (!DEP || (cell == runcell && runbase >= 0));
+        // a particle that stays in its cell but is out of place in the thread's
+        // run (it changed cell since the sort): its 20 sums go to the run queue
+        oop = DEP && incell && !simple && gb >= 0;
+      }
     }
     const unsigned om = DEP ? __ballot_sync(0xffffffffu, oop) : 0u;
     float* oen = oop ? rq + (rqn + __popc(om & lt)) * QW : nullptr;
@@ -1026,7 +1045,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     }
     // the new velocity of every particle (a cell-crossing one keeps its old
     // position until the general path writes the whole record)
-    if (act) {
+    if (act && !defer) {
       const int m = r * PUSH_THREADS + tid;
       if (simple || oop) gpos[m] = make_float4(sx, syy, szz, ps.w);
       gvx[m] = vx;
@@ -1050,7 +1069,7 @@ __global__ void __launch_bounds__(PUSH_BLOCK, 1) k_fx_push(FxPushArgs a) {
     }
     // ---- cell-crossing particles: the warp's cross list (their positions
     // stay as they were; the general path after the row loop moves them)
-    const bool cross = act && !simple && !oop;
+    const bool cross = act && !simple && !oop && !defer;
     const unsigned xm = __ballot_sync(0xffffffffu, cross);
     if (xm) {
       if (cross) xl[xqn + __popc(xm & lt)] = r * PUSH_THREADS + tid;
@@ -1219,6 +1238,56 @@ __global__ void k_fx_tail(FxPushArgs a, int is, int64_t tail0, int64_t ntail, in
   if (esc) atomicAdd(nesc_out, esc);
 }
 
+// The particles the parts of a step left for later (FxPushArgs::defer: a
+// gather from node planes converted after their part ran), once every plane
+// is converted: what the row loop and the general path do for a particle
+// whose cell lies outside its tile's box -- the global gather and the kick,
+// then the general path with global deposits (a deposit takes the same
+// int64 value per node as through a tile's box).  The compiler may round
+// this kernel's kick otherwise than the row loop's (where it fuses a
+// multiply with an add), so such a particle can differ in the last bit from
+// the same step pushed in one launch.  One thread per 32-slot word of the
+// bitmap, which it clears.
+template <int T, bool CURV, bool JD>
+__global__ void k_fx_deferred(FxPushArgs a, uint32_t* __restrict__ bits, int64_t nwords, int nspec) {
+  constexpr int B = T + 2 * PG + 1;
+  const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nwords) return;
+  uint32_t m = bits[w];
+  if (m == 0u) return;
+  bits[w] = 0u;
+  const Geo& g = a.g;
+  const Sink sk{a.acc_rho, a.acc_j, a.fr, a.fj, g.nx, g.ny, g.nz, a.status, a.diag};
+  const int far[3] = {-(1 << 28), -(1 << 28), -(1 << 28)};  // no box: global deposits
+  while (m) {
+    const int64_t slot = w * 32 + (__ffs(m) - 1);
+    m &= m - 1u;
+    int is = 0;
+    for (int s = 1; s < nspec; s++)
+      if (slot >= a.off[s]) is = s;
+    const int64_t base = a.off[is];
+    const float4 ps = a.pos[slot];
+    const uint32_t cell = (uint32_t)__float_as_int(ps.w);
+    int ib, jb, kb;
+    unpack(g, cell, ib, jb, kb);
+    if (cell == DEAD || ib >= g.nx || jb >= g.ny || kb >= g.nz) {
+      report_bad(a.status, a.diag, SITE_FX_PUSH, slot, (long long)cell);
+      continue;
+    }
+    float vx = a.vx[slot], vy = a.vy[slot], vz = a.vz[slot];
+    kick<B>(a, nullptr, nullptr, -1, ib, jb, kb, ps, a.qmp[is], vx, vy, vz);
+    a.vx[slot] = vx;
+    a.vy[slot] = vy;
+    a.vz[slot] = vz;
+    const CrossCtx c{a.pos + base, a.vx + base, a.vy + base, a.vz + base, a.gustep, a.rustep, a.qfix[is],
+                     {a.npbnd[is][0], a.npbnd[is][1], a.npbnd[is][2]}, &a.bd, a.gc,
+                     a.surf + (int64_t)is * a.bd.nsurf, is, base, a.ob.rec ? &a.ob : nullptr, a.status};
+    const float en[XQW] = {__int_as_float((int)(slot - base)), ps.w, ps.x, ps.y, ps.z, vx, vy, vz};
+    const int esc = cross_one<B, true, CURV, JD>(g, nullptr, far, sk, c, en);
+    if (esc) atomicAdd(&a.nesc[is], esc);
+  }
+}
+
 // The compiled box edge for the largest tile edge tmax (<= 8).
 inline int fx_box_tile(int tmax) { return tmax <= 4 ? 4 : 8; }
 
@@ -1238,11 +1307,25 @@ inline int fx_push_smem(int tmax, bool jd = true) {
 // The pushing kernel (DEP = true) for a compiled box tile (4 or 8), runs
 // with cylinders or spheres, and with (jd) or without the current.
 using PushKernel = void (*)(FxPushArgs);
-inline PushKernel push_kernel(int box, bool curved, bool jd) {
+using DeferredKernel = void (*)(FxPushArgs, uint32_t*, int64_t, int);
+inline DeferredKernel deferred_kernel(int box, bool curved, bool jd) {
   if (box == 4) {
-    if (curved) return jd ? k_fx_push<4, true, true, true> : k_fx_push<4, true, true, false>;
-    return jd ? k_fx_push<4, true, false, true> : k_fx_push<4, true, false, false>;
+    if (curved) return jd ? k_fx_deferred<4, true, true> : k_fx_deferred<4, true, false>;
+    return jd ? k_fx_deferred<4, false, true> : k_fx_deferred<4, false, false>;
   }
-  if (curved) return jd ? k_fx_push<8, true, true, true> : k_fx_push<8, true, true, false>;
-  return jd ? k_fx_push<8, true, false, true> : k_fx_push<8, true, false, false>;
+  if (curved) return jd ? k_fx_deferred<8, true, true> : k_fx_deferred<8, true, false>;
+  return jd ? k_fx_deferred<8, false, true> : k_fx_deferred<8, false, false>;
+}
+
+template <bool PARTS>
+inline PushKernel push_kernel_t(int box, bool curved, bool jd) {
+  if (box == 4) {
+    if (curved) return jd ? k_fx_push<4, true, true, true, PARTS> : k_fx_push<4, true, true, false, PARTS>;
+    return jd ? k_fx_push<4, true, false, true, PARTS> : k_fx_push<4, true, false, false, PARTS>;
+  }
+  if (curved) return jd ? k_fx_push<8, true, true, true, PARTS> : k_fx_push<8, true, true, false, PARTS>;
+  return jd ? k_fx_push<8, true, false, true, PARTS> : k_fx_push<8, true, false, false, PARTS>;
+}
+inline PushKernel push_kernel(int box, bool curved, bool jd, bool parts = false) {
+  return parts ? push_kernel_t<true>(box, curved, jd) : push_kernel_t<false>(box, curved, jd);
 }
