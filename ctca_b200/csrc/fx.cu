@@ -976,19 +976,28 @@ namespace emsesg {
 // The parts of a push whose eb arrives in z chunks: part p takes the tile
 // layers tz0 .. tz1 - 1 (tiles tile[p] .. tile[p+1] - 1) and needs the node
 // planes 0..zready[p] (its tiles' boxes: tz1 - 1 times the tile edge plus
-// the compiled box).  Returns the number of parts, 0 where the step does not
-// run in parts (FP32 form not loaded, slab mode, one tile layer).
+// the compiled box).  The parts grow (1/16, 3/16, 3/8 and 3/8 of the
+// layers, at least one each): the first starts after a small chunk, and
+// each later chunk arrives while the parts before it push.  Returns the
+// number of parts, 0 where the step does not run in parts (FP32 form not
+// loaded, slab mode, one tile layer).
 int fx_eb_plan(const emsesg_ctx* ctx, int* zready, int64_t* tile) {
   const FxState& f = ctx->fx;
   if (!f.loaded || f.slab || f.ntile[2] < 2) return 0;
-  const int nz = ctx->cfg.nz;
-  const int parts = std::min(EMSESG_EB_PARTS, f.ntile[2]);
+  static_assert(EMSESG_EB_PARTS == 4, "one cumulative share per part");
+  constexpr double share[EMSESG_EB_PARTS] = {1.0 / 16, 4.0 / 16, 10.0 / 16, 1.0};
+  const int nz = ctx->cfg.nz, ntz = f.ntile[2];
+  const int parts = std::min(EMSESG_EB_PARTS, ntz);
   const int tmax = std::max(f.tile[0], std::max(f.tile[1], f.tile[2]));
   const int64_t layer = (int64_t)f.ntile[0] * f.ntile[1];
+  int tz0 = 0;
   for (int p = 0; p < parts; p++) {
-    const int tz0 = p * f.ntile[2] / parts, tz1 = (p + 1) * f.ntile[2] / parts;
+    // at least one layer, and one left for each later part
+    int tz1 = p == parts - 1 ? ntz : (int)(ntz * share[EMSESG_EB_PARTS - parts + p] + 0.5);
+    tz1 = std::min(std::max(tz1, tz0 + 1), ntz - (parts - 1 - p));
     tile[p] = tz0 * layer;
     zready[p] = p == parts - 1 ? nz : std::min(nz, (tz1 - 1) * f.tile[2] + fx_box_tile(tmax) + PG);
+    tz0 = tz1;
   }
   tile[parts] = f.ntiles;
   return parts;
