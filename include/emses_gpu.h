@@ -300,7 +300,13 @@ int emsesg_fx_sort(emsesg_ctx* ctx);
  * the next step on the side stream into a second buffer, which replaces the
  * field before the next work that reads eb (an FP32 step, grdcrt, the field
  * step, a download of eb); the copy starts once the last step has read eb,
- * so it overlaps with that step's sort.  A synchronous emsesg_upload_field
+ * so it overlaps with that step's sort.  With the FP32 form loaded the copy
+ * goes in z chunks and the next FP32 step pushes its tile layers in parts,
+ * each once its chunk is there; a particle outside its tile's box whose
+ * node planes are not there yet is pushed after the last part, by a kernel
+ * that may round its kick otherwise in the last bit (such a step agrees
+ * with the step after a synchronous upload in counts, cells and liveness,
+ * and up to those particles' last bits).  A synchronous emsesg_upload_field
  * of eb replaces a pending asynchronous one.  The two buffers change roles
  * with every asynchronous upload: emsesg_fx_run takes a pending upload
  * before it captures or replays its graph and captures again when the eb
