@@ -21,14 +21,15 @@ no data exchange on one rank: weak scaling, replicas only).
 --cells N [--ppc P] shrinks the grid (and particles per cell) for profiler
 captures; the headline line is the default 128^3 x 64 workload.
 
-Two more workloads ride on the headline line (skip them with --no-extras):
+Four more workloads ride on the headline line (skip them with --no-extras):
 `adjoint` times the reverse mode through K = 256 steps of a 64^3 periodic
 grid with 32 particles per cell per species (checkpoints every 16 steps,
 loss = sum of Jx^2 over an 8^3 probe) against the same K forward steps;
 `ensemble` runs a bounded sample of the ensemble workload (independent runs
 of side 16..64 in one CUDA graph) against the same runs launched one after
-the other.  --workload ensemble prints the full ensemble line instead
-(512 runs x 200 steps by default).
+the other; `em_loop` and `es_loop` are 12 steps of the --workload em and es
+loops below on the headline grid.  --workload ensemble prints the full
+ensemble line instead (512 runs x 200 steps by default).
 
 --workload em and --workload es run the headline plasma self-consistently
 with the field solve on the device every step: the EM leapfrog (bfield,
@@ -573,6 +574,8 @@ def run_ours(args, world, rank, local):
     if world == 1 and not args.no_extras and not args.cells:
         out["adjoint"] = time_adjoint()
         out["ensemble"] = ensemble_sample(args.ensemble_runs, args.ensemble_steps)
+        out["em_loop"] = loop_section(local, es=False)
+        out["es_loop"] = loop_section(local, es=True)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
         out["accuracy"] = accuracy_report()
@@ -999,12 +1002,20 @@ def run_em_line(args, world, rank, local, es=False):
                               "Fortran toolchain); its CPU particle path is timed by the default workload"}),
                   flush=True)
         return
+    out = field_loop(args.cells, args.ppc, args.steps, args.warmup, world, rank, local, es)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def field_loop(cells, ppc, steps, warmup, world, rank, local, es):
+    """One timed run of the EM (or, with es, the electrostatic) loop of
+    run_em_line; returns its line."""
     import torch
     from ctca_b200 import inputs
     from ctca_b200.emses import Emses, select_device
     torch.cuda.set_device(local)
     select_device(local)
-    case = headline_case(args.cells, args.ppc)
+    case = headline_case(cells, ppc)
     cfg = inputs.make_config(case)
     g = Emses(cfg)
     g.upload_field("eb", inputs.make_fields(case))
@@ -1021,7 +1032,7 @@ def run_em_line(args, world, rank, local, es=False):
             g.fx_em_step(2, k[0] % SORT_EVERY == SORT_EVERY - 1, 0.125)
         k[0] += 1
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     g.synchronize()
     g.set_profiling(True)
@@ -1031,7 +1042,7 @@ def run_em_line(args, world, rank, local, es=False):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clk:
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             step()
         e1.record(stream)
         e1.synchronize()
@@ -1041,8 +1052,8 @@ def run_em_line(args, world, rank, local, es=False):
     prof = g.profile()
     fields = ("es_pack", "es_fft", "es_divide", "es_unpack", "es_efield") if es else ("bfield", "efield", "exchange_eb")
     field_ms = sum(prof.get(n, (0.0, 0))[0] for n in fields)
-    out = {"metric": METRIC, "value": world * npart * args.steps / t, "unit": UNIT, "n_gpus": world,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
+    out = {"metric": METRIC, "value": world * npart * steps / t, "unit": UNIT, "n_gpus": world,
+           "steps": steps, "warmup": warmup, "ms_per_step": t / steps * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64 (fields f64)",
            "data": "synthetic",
            "config": {"workload": f"{case.n[0]}^3 periodic, 2 species x {case.species[0].ppc} ppc ({npart:,} "
@@ -1051,13 +1062,20 @@ def run_em_line(args, world, rank, local, es=False):
                                   "device each step (bfield, push, bfield, efield, border exchange)") +
                                   ", sort every 4",
                       "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
-           "field_step_ms": field_ms / args.steps,
+           "field_step_ms": field_ms / steps,
            "gpu_launches": int(sum(n for _, n in prof.values())),
            "kernels_ms": {kk: round(v[0], 3) for kk, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
            "clocks": clk.summary()}
     g.close()
-    if rank == 0:
-        print(json.dumps(out), flush=True)
+    return out
+
+
+def loop_section(local, es):
+    """The EM / electrostatic loop on the headline grid for the default line
+    (12 timed steps after 3 warm-up steps, three sorts)."""
+    o = field_loop(0, 0, 12, 3, 1, 0, local, es)
+    return {k: o[k] for k in ("value", "unit", "ms_per_step", "steps", "warmup", "field_step_ms", "config",
+                              "gpu_launches", "clocks")}
 
 
 def main():
@@ -1072,7 +1090,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cells", type=int, default=0, help="grid side of a smaller profiling case (default 128)")
     ap.add_argument("--ppc", type=int, default=0, help="particles per cell per species with --cells")
-    ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and ensemble sections")
+    ap.add_argument("--no-extras", action="store_true", help="skip the adjoint, ensemble and loop sections")
     ap.add_argument("--workload", default="particle_step",
                     choices=["particle_step", "ensemble", "body", "em", "es", "slabs"])
     ap.add_argument("--body-scale", type=float, default=1.0, help="grid scale of the body workload (1: 256x256x512)")
