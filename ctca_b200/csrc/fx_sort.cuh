@@ -70,8 +70,8 @@ __device__ __forceinline__ int lcs_box_cell(const LcsGeo& G, int tx, int ty, int
   return a + G.bc[0] * (b + G.bc[1] * c);
 }
 
-// Tiles along one axis whose sort box may hold cell index i, ascending,
-// without repeats.
+// Tiles along one axis whose sort box holds cell index i, ascending,
+// without repeats (the tile of i, and a neighbour when i lies in its guard).
 __device__ __forceinline__ int lcs_cand(const LcsGeo& G, int d, int i, int (&out)[3]) {
   const int c = i / G.t[d];
   int m = 0;
@@ -83,6 +83,7 @@ __device__ __forceinline__ int lcs_cand(const LcsGeo& G, int d, int i, int (&out
       if (!G.wrap[d]) continue;
       x = (x + G.nt[d]) % G.nt[d];
     }
+    if (lcs_axis(G, d, x, i) < 0) continue;
     w[m++] = x;
   }
   // sort the (at most 3) entries and drop repeats
